@@ -1,0 +1,302 @@
+"""Benchmark: parallel-tempering Monte Carlo of the pyrochlore Heisenberg
+antiferromagnet, L=32 (524,288 sites), 64 replicas on a geometric ladder
+T in [0.02, 2.0], 1 cone-Metropolis + 4 over-relaxation sweeps per exchange
+attempt, FP64 energies and swap test. One step = one such cycle over all
+replicas; metric = spin updates per nanosecond (whole job).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Under torchrun (N > 1) every rank holds 64 replicas of one global ladder of
+64 N temperatures; energies are all-gathered over NCCL each cycle and every
+rank applies the identical exchange (weak scaling).
+
+``--impl reference`` times the reference algorithm's CPU implementation (the
+C++/OpenMP port in oracle/, the reference itself does not build) on the host
+cores for the same workload, on a bounded sample of replicas per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L = 32
+R_PER_GPU = 64
+T_MIN, T_MAX = 0.02, 2.0
+N_METRO, N_OR = 1, 4
+SEED = 12345 + 1
+METRIC = "spin-updates/ns"
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+BYTES_PER_UPDATE_PASS = 80  # float4 spins, J1 4-colour pass: 16 N/4 own + 48 N/4 nbr + 16 N/4 write
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons with nvidia-smi during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline_sample(threads: int | None = None, replicas: int = 4, cycles: int = 3):
+    """The reference algorithm's CPU path (oracle port) on a bounded sample."""
+    from cudacode_b200.engine import System, geometric_ladder
+    from oracle.binding import Oracle
+
+    temps = geometric_ladder(T_MIN, T_MAX, R_PER_GPU)
+    o = Oracle([System(L=L, temperatures=temps, n_replicas=replicas)], seed=SEED,
+               threads=threads or os.cpu_count())
+    o.init_random()
+    o.set_cone(np.full(R_PER_GPU, 0.3, dtype=np.float32))
+    o.metropolis_sweep(1)  # warm caches / threads
+    t0 = time.perf_counter()
+    for _ in range(cycles):
+        o.metropolis_sweep(N_METRO)
+        o.overrelax_sweep(N_OR)
+        o.observables()
+    dt = time.perf_counter() - t0
+    updates = replicas * 16 * L ** 3 * (N_METRO + N_OR) * cycles
+    n_threads = o.lib.orc_set_threads(0)
+    return updates / (dt * 1e9), n_threads, dt, f"{replicas} of {R_PER_GPU} replicas, {cycles} cycles"
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    vals = []
+    n_threads = None
+    for _ in range(args.warmup):
+        cpu_baseline_sample(cycles=1)
+    for _ in range(args.steps):
+        v, n_threads, dt, sample = cpu_baseline_sample(cycles=1)
+        vals.append(v)
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "updates/ns",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (random unit spins from Philox seed)",
+        "config": workload_config(args.gpus),
+        "cpu_baseline": {"value": value, "unit": "updates/ns", "cores": n_threads, "kind": "port",
+                         "sample": "per step: 4 of 64 replicas of L=32, 1 cycle (1 M + 4 OR "
+                                   "sweeps + FP64 energies)"},
+        "e2e": {"value": value, "unit": "updates/ns", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(n_gpus):
+    return {"workload": "pyrochlore Heisenberg AFM PT: L=32 (524,288 sites), J1=1, "
+                        f"{R_PER_GPU} replicas per GPU on a geometric ladder T in [0.02, 2.0], "
+                        "1 Metropolis + 4 over-relaxation sweeps + FP64 energies + swap per step",
+            "L": L, "replicas_per_gpu": R_PER_GPU, "global_replicas": R_PER_GPU * n_gpus,
+            "sweeps_per_step": N_METRO + N_OR, "parallelism": f"replicas sharded over {n_gpus} GPU",
+            "l2": "inputs larger than L2 (537 MB of spins per GPU > 126 MB)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+
+    from cudacode_b200.engine import Engine, System, geometric_ladder
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    n_gpus = world
+
+    temps = geometric_ladder(T_MIN, T_MAX, R_PER_GPU * n_gpus)
+    sysd = System(L=L, temperatures=temps, n_replicas=R_PER_GPU, replica_offset=R_PER_GPU * rank)
+    eng = Engine([sysd], seed=SEED, device=local)
+    stream = torch.cuda.Stream(device=local)
+    eng.set_stream(stream.cuda_stream)
+    eng.init_random()
+    cones = np.full(len(temps), 0.3, dtype=np.float32)
+    eng.set_cone(cones)
+    e_all = torch.zeros(R_PER_GPU * n_gpus, dtype=torch.float64, device=f"cuda:{local}")
+    e_loc = torch.zeros(R_PER_GPU, dtype=torch.float64, device=f"cuda:{local}")
+
+    def step():
+        if world == 1:
+            eng.cycle(N_METRO, N_OR, True, 1)
+        else:
+            eng.cycle(N_METRO, N_OR, False, 1)
+            eng.observables_device(e_loc.data_ptr())
+            with torch.cuda.stream(stream):
+                dist.all_gather_into_tensor(e_all, e_loc)
+            eng.pt_swap_global(e_all.data_ptr(), -1)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            torch.cuda.synchronize()
+            start.record(stream)
+            for _ in range(args.steps):
+                step()
+            stop.record(stream)
+            torch.cuda.synchronize()
+        ms = start.elapsed_time(stop)
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    updates = R_PER_GPU * n_gpus * 16 * L ** 3 * (N_METRO + N_OR) * args.steps
+    value = updates / (ms * 1e6)
+
+    # Dominant kernel: the over-relaxation colour pass (16 of 20 passes per step).
+    n_or_timed = 20
+    with torch.cuda.stream(stream):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        eng.overrelax_sweep(2)
+        a.record(stream)
+        eng.overrelax_sweep(n_or_timed)
+        b.record(stream)
+        torch.cuda.synchronize()
+        or_ms = a.elapsed_time(b) / (n_or_timed * 4)  # per colour pass
+    pass_updates = R_PER_GPU * 16 * L ** 3 // 4
+    achieved = pass_updates * BYTES_PER_UPDATE_PASS / (or_ms * 1e-3) / 1e9
+    peak, peak_kind = hbm_peak()
+
+    # End to end through the C-ABI with host buffers: each step uploads the cone
+    # widths from pinned host memory, runs the cycle, and reads the FP64
+    # energies and magnetisations back to host memory (synchronous).
+    e2e_steps = max(10, args.steps // 4)
+    cones_h = torch.from_numpy(cones).pin_memory()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        eng.set_cone(cones_h.numpy())
+        step()
+        E, M = eng.observables()
+    e2e_s = time.perf_counter() - t0
+    e2e_value = R_PER_GPU * n_gpus * 16 * L ** 3 * (N_METRO + N_OR) * e2e_steps / (e2e_s * 1e9)
+    if world > 1:
+        t = torch.tensor([e2e_value], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MIN)
+        e2e_value = float(t.item()) * 1.0
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, nt, dt, sample = cpu_baseline_sample()
+        cpu = {"value": v, "unit": "updates/ns", "cores": nt, "kind": "port",
+               "sample": sample + f" ({dt:.1f} s)"}
+
+    passes_per_step = 4 * (N_METRO + N_OR)
+    launches_per_step = passes_per_step + 3  # + observables, finalise, exchange
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "updates/ns", "n_gpus": n_gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (random unit spins from Philox seed)",
+            "config": workload_config(n_gpus),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "kernel": "colour_pass_kernel<J1, over-relaxation>",
+                         "bytes_per_update": BYTES_PER_UPDATE_PASS,
+                         "updates_per_launch": pass_updates, "ms_per_launch": or_ms,
+                         "traffic": None},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "updates/ns",
+                    "h2d_bytes_per_step": 4 * len(temps),
+                    "d2h_bytes_per_step": 8 * R_PER_GPU + 24 * R_PER_GPU},
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,91 @@
+"""Builds the engine's shared library in-tree (sm_100a) and, for the tests,
+the host oracle.
+
+    python -m cudacode_b200.build            # engine + oracle
+    python -m cudacode_b200.build --engine   # engine only
+
+The engine library ``cudacode_b200/libpyro.so`` is built with nvcc for
+``sm_100a`` only; device code is compiled with ``--fmad=false`` so that every
+fused multiply-add is the explicit ``fmaf`` of ``include/pyro_math.h`` and the
+kernels round exactly like the host oracle.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+LIB = os.path.join(PKG, "libpyro.so")
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+
+ENGINE_SOURCES = ["kernels.cu", "capi.cu", "lattice.cpp"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(cand):
+        raise RuntimeError("nvcc not found; the engine needs the CUDA 12.9 toolkit")
+    return cand
+
+
+def _newer(target: str, sources: list[str]) -> bool:
+    if not os.path.exists(target):
+        return False
+    t = os.path.getmtime(target)
+    return all(os.path.getmtime(s) <= t for s in sources)
+
+
+def _deps() -> list[str]:
+    out = []
+    for d in (CSRC, os.path.join(ROOT, "include")):
+        for f in os.listdir(d):
+            if f.endswith((".cu", ".cuh", ".h", ".cpp", ".hpp")):
+                out.append(os.path.join(d, f))
+    return out
+
+
+def build_engine(force: bool = False, verbose: bool = False) -> str:
+    deps = _deps()
+    if not force and _newer(LIB, deps):
+        return LIB
+    objs = []
+    build_dir = os.path.join(PKG, "_build")
+    os.makedirs(build_dir, exist_ok=True)
+    common = [nvcc(), *ARCH, "-lineinfo", "-O3", "--fmad=false", "-std=c++17",
+              "-Xcompiler", "-fPIC,-O3,-ffp-contract=off", "-I", os.path.join(ROOT, "include")]
+    for src in ENGINE_SOURCES:
+        obj = os.path.join(build_dir, src.rsplit(".", 1)[0] + ".o")
+        cmd = [*common, "-c", os.path.join(CSRC, src), "-o", obj]
+        if src.endswith(".cpp"):
+            cmd = [*common, "-x", "cu", "-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        objs.append(obj)
+    tmp = LIB + ".tmp"
+    subprocess.run([nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"], check=True)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+def build_oracle(force: bool = False) -> str:
+    """Compiles the host oracle (test infrastructure) with make."""
+    subprocess.run(["make", "-s", "-C", ORACLE_DIR] + (["-B"] if force else []), check=True)
+    return os.path.join(ORACLE_DIR, "liboracle.so")
+
+
+def main(argv: list[str]) -> int:
+    force = "--force" in argv
+    build_engine(force=force, verbose="-v" in argv)
+    if "--engine" not in argv:
+        build_oracle(force=force)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv[1:]))

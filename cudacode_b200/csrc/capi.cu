@@ -1,0 +1,919 @@
+// C-ABI implementation: context, memory layout, pass schedules, CUDA graph of
+// the sweep + exchange cycle, and the host-side wrappers of include/pyro.h.
+//
+// The reference keeps this state in `struct dev` (fields used at
+// MonteCarlo.cu:15-245, Pyrochlore.cu:74-133) and drives it from one pthread
+// per GPU; here one context owns one GPU's memory and all calls are
+// stream-ordered on the context's stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/pyro.h"
+#include "kernels.cuh"
+#include "lattice.h"
+
+using namespace pyro;
+
+struct pyro_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+  uint64_t seed = 0;
+  int renorm_every = 0;
+  NbrTable tab;
+  bool j1_only = true;
+
+  std::vector<SysDev> sys;
+  std::vector<std::vector<double>> ladders;
+  SysDev* d_sys = nullptr;
+  int total_temps = 0;
+  int total_reps = 0;  // replicas held
+
+  float4* d_spins = nullptr;
+  long long n_spins = 0;
+
+  int* d_temp_of_rep = nullptr;
+  int* d_rep_of_temp = nullptr;
+  float* d_beta = nullptr;
+  double* d_beta64 = nullptr;
+  float* d_cosmax = nullptr;
+  unsigned long long* d_accepted = nullptr;
+  unsigned long long* d_swap_acc = nullptr;
+  unsigned long long* d_swap_try = nullptr;
+  unsigned long long* d_swap_count = nullptr;
+  int* d_last_accepted = nullptr;
+
+  double* d_energy = nullptr;
+  double* d_mag = nullptr;
+  int* d_rep_sys = nullptr;
+  int* d_rep_local = nullptr;
+
+  std::vector<ObsSeg> obs_segs;
+  ObsSeg* d_obs_segs = nullptr;
+  int obs_blocks = 0;
+  double4* d_partials = nullptr;
+
+  int n_passes = 4;
+  std::vector<std::vector<PassSeg>> pass_segs;
+  std::vector<PassSeg*> d_pass_segs;
+  std::vector<int> pass_blocks;
+
+  unsigned long long* d_sweep = nullptr;
+  unsigned long long h_sweep = 0;
+  unsigned long long metro_sweeps_since_reset = 0;
+  unsigned long long* d_scratch_u64 = nullptr;
+
+  double* d_history = nullptr;
+  int history_cap = 0;
+  unsigned long long* d_history_count = nullptr;
+
+  std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;
+};
+
+namespace {
+
+int fail(pyro_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+#define PYRO_CK(call)                                                                   \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return fail(ctx, PYRO_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define PYRO_CK_LAUNCH()                                                                \
+  do {                                                                                  \
+    cudaError_t e_ = cudaGetLastError();                                                \
+    if (e_ != cudaSuccess)                                                              \
+      return fail(ctx, PYRO_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <typename T>
+cudaError_t alloc(T** p, size_t n) {
+  return cudaMalloc((void**)p, sizeof(T) * std::max<size_t>(n, 1));
+}
+
+PassParams pass_params(pyro_ctx* ctx, int pass) {
+  PassParams p;
+  p.segs = ctx->d_pass_segs[pass];
+  p.nseg = (int)ctx->pass_segs[pass].size();
+  p.sys = ctx->d_sys;
+  p.spins = ctx->d_spins;
+  p.temp_of_rep = ctx->d_temp_of_rep;
+  p.beta = ctx->d_beta;
+  p.cosmax = ctx->d_cosmax;
+  p.accepted = ctx->d_accepted;
+  p.sweep_ctr = ctx->d_sweep;
+  p.sweep_off = 0;
+  p.seed_lo = (uint32_t)(ctx->seed & 0xffffffffu);
+  p.seed_hi = (uint32_t)(ctx->seed >> 32);
+  p.renorm_every = ctx->renorm_every;
+  return p;
+}
+
+// Queues one sweep (all colour passes) with the given offset from *d_sweep.
+int queue_sweep(pyro_ctx* ctx, bool metro, unsigned long long off) {
+  for (int pass = 0; pass < ctx->n_passes; ++pass) {
+    if (ctx->pass_blocks[pass] == 0) continue;
+    PassParams p = pass_params(ctx, pass);
+    p.sweep_off = off;
+    launch_colour_pass(p, ctx->tab, ctx->pass_blocks[pass], metro, ctx->j1_only, ctx->stream);
+    PYRO_CK_LAUNCH();
+  }
+  return PYRO_OK;
+}
+
+int queue_observables(pyro_ctx* ctx) {
+  ObsParams op;
+  op.segs = ctx->d_obs_segs;
+  op.nseg = (int)ctx->obs_segs.size();
+  op.sys = ctx->d_sys;
+  op.spins = ctx->d_spins;
+  op.partials = ctx->d_partials;
+  launch_observables(op, ctx->tab, ctx->obs_blocks, ctx->stream);
+  PYRO_CK_LAUNCH();
+  launch_obs_finalise(ctx->d_partials, ctx->d_obs_segs, (int)ctx->obs_segs.size(), ctx->d_sys,
+                      ctx->total_reps, ctx->d_rep_sys, ctx->d_rep_local, ctx->d_energy, ctx->d_mag,
+                      ctx->stream);
+  PYRO_CK_LAUNCH();
+  return PYRO_OK;
+}
+
+ExchangeParams exchange_params(pyro_ctx* ctx) {
+  ExchangeParams x;
+  std::memset(&x, 0, sizeof(x));
+  x.sys = ctx->d_sys;
+  x.n_sys = (int)ctx->sys.size();
+  x.sys_first = 0;
+  x.energy = ctx->d_energy;
+  x.energy_is_global = 0;
+  x.beta64 = ctx->d_beta64;
+  x.temp_of_rep = ctx->d_temp_of_rep;
+  x.rep_of_temp = ctx->d_rep_of_temp;
+  x.swap_count = ctx->d_swap_count;
+  x.swap_acc = ctx->d_swap_acc;
+  x.swap_try = ctx->d_swap_try;
+  x.last_accepted = ctx->d_last_accepted;
+  x.parity = -1;
+  x.seed_lo = (uint32_t)(ctx->seed & 0xffffffffu);
+  x.seed_hi = (uint32_t)(ctx->seed >> 32);
+  x.history = nullptr;
+  x.history_count = ctx->d_history_count;
+  x.history_cap = ctx->history_cap;
+  x.total_temps = ctx->total_temps;
+  x.sweep_ctr = nullptr;
+  x.sweep_advance = 0;
+  x.do_swap = 1;
+  return x;
+}
+
+int max_pairs(const pyro_ctx* ctx) {
+  int m = 1;
+  for (const auto& s : ctx->sys) m = std::max(m, (s.n_temp + 1) / 2);
+  return m;
+}
+
+bool sharded(const pyro_ctx* ctx) {
+  for (const auto& s : ctx->sys)
+    if (s.n_rep != s.n_temp) return true;
+  return false;
+}
+
+void free_all(pyro_ctx* c) {
+  for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+  c->graphs.clear();
+  void* ptrs[] = {c->d_sys,         c->d_spins,        c->d_temp_of_rep, c->d_rep_of_temp,
+                  c->d_beta,        c->d_beta64,       c->d_cosmax,      c->d_accepted,
+                  c->d_swap_acc,    c->d_swap_try,     c->d_swap_count,  c->d_last_accepted,
+                  c->d_energy,      c->d_mag,          c->d_rep_sys,     c->d_rep_local,
+                  c->d_obs_segs,    c->d_partials,     c->d_sweep,       c->d_scratch_u64,
+                  c->d_history,     c->d_history_count};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  for (auto* p : c->d_pass_segs)
+    if (p) cudaFree(p);
+  c->d_pass_segs.clear();
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  c->stream = nullptr;
+}
+
+int validate(const pyro_config* cfg, std::string* why) {
+  if (!cfg || cfg->n_systems <= 0 || !cfg->systems) {
+    *why = "config: need n_systems >= 1 and a systems array";
+    return PYRO_ERR_ARG;
+  }
+  for (int i = 0; i < cfg->n_systems; ++i) {
+    const pyro_system_desc& d = cfg->systems[i];
+    char buf[160];
+    if (d.L < 2 || d.L > 256) {
+      snprintf(buf, sizeof buf, "system %d: L=%d out of range [2, 256]", i, d.L);
+      *why = buf;
+      return PYRO_ERR_ARG;
+    }
+    if (d.n_temperatures < 1 || d.n_replicas < 1 || d.replica_offset < 0 ||
+        d.replica_offset + d.n_replicas > d.n_temperatures) {
+      snprintf(buf, sizeof buf, "system %d: replicas [%d, %d) not inside the ladder of %d", i,
+               d.replica_offset, d.replica_offset + d.n_replicas, d.n_temperatures);
+      *why = buf;
+      return PYRO_ERR_ARG;
+    }
+    if (!d.temperatures) {
+      snprintf(buf, sizeof buf, "system %d: temperatures is NULL", i);
+      *why = buf;
+      return PYRO_ERR_ARG;
+    }
+    for (int t = 0; t < d.n_temperatures; ++t) {
+      const double T = d.temperatures[t];
+      if (!(T > 0.0) || !std::isfinite(T) || (t > 0 && !(T > d.temperatures[t - 1]))) {
+        snprintf(buf, sizeof buf, "system %d: temperatures must be finite, > 0, increasing", i);
+        *why = buf;
+        return PYRO_ERR_ARG;
+      }
+    }
+    const double J[4] = {d.J1, d.J2, d.J3, d.J3b};
+    for (double j : J)
+      if (!std::isfinite(j)) {
+        snprintf(buf, sizeof buf, "system %d: couplings must be finite", i);
+        *why = buf;
+        return PYRO_ERR_ARG;
+      }
+    // A 16-colour class holds sites that are a lattice vector apart; with
+    // L = 2 the J2/J3 shells would reach a periodic image of the same site.
+    if ((d.J2 != 0.0 || d.J3 != 0.0 || d.J3b != 0.0) && d.L < 3) {
+      snprintf(buf, sizeof buf, "system %d: J2/J3 need L >= 3", i);
+      *why = buf;
+      return PYRO_ERR_ARG;
+    }
+  }
+  if (cfg->renorm_every < 0) {
+    *why = "renorm_every must be >= 0";
+    return PYRO_ERR_ARG;
+  }
+  return PYRO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pyro_version(void) { return 1; }
+
+int pyro_neighbour_table(int site, int* out120) {
+  if (site < 0 || site >= kSitesPerCell || !out120) return PYRO_ERR_ARG;
+  NbrTable tab;
+  if (!build_neighbour_table(&tab)) return PYRO_ERR_STATE;
+  for (int k = 0; k < kMaxNbr; ++k) {
+    const NbrEntry e = tab.e[site][k];
+    out120[4 * k] = e.dx;
+    out120[4 * k + 1] = e.dy;
+    out120[4 * k + 2] = e.dz;
+    out120[4 * k + 3] = e.t;
+  }
+  return PYRO_OK;
+}
+
+const char* pyro_last_error(const pyro_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int pyro_create(const pyro_config* cfg, pyro_ctx** out) {
+  if (!out) return PYRO_ERR_ARG;
+  *out = nullptr;
+  std::string why;
+  int rc = validate(cfg, &why);
+  if (rc != PYRO_OK) {
+    fprintf(stderr, "pyro_create: %s\n", why.c_str());
+    return rc;
+  }
+  pyro_ctx* ctx = new pyro_ctx();
+  ctx->device = cfg->device;
+  ctx->seed = cfg->seed;
+  ctx->renorm_every = cfg->renorm_every;
+  if (!build_neighbour_table(&ctx->tab)) {
+    delete ctx;
+    return PYRO_ERR_STATE;
+  }
+  cudaError_t e = cudaSetDevice(cfg->device);
+  if (e != cudaSuccess) {
+    fprintf(stderr, "pyro_create: cudaSetDevice(%d): %s\n", cfg->device, cudaGetErrorString(e));
+    delete ctx;
+    return PYRO_ERR_CUDA;
+  }
+  auto bail = [&](int code) {
+    fprintf(stderr, "pyro_create: %s\n", ctx->err.c_str());
+    free_all(ctx);
+    delete ctx;
+    return code;
+  };
+#define CREATE_CK(call)                                                              \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess) {                                                         \
+      ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);                 \
+      return bail(e_ == cudaErrorMemoryAllocation ? PYRO_ERR_NOMEM : PYRO_ERR_CUDA); \
+    }                                                                                \
+  } while (0)
+  CREATE_CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  ctx->own_stream = true;
+
+  // Systems, temperature slots and replica maps.
+  long long spin_off = 0;
+  int temp_base = 0, rep_ctx = 0;
+  int max_colours = 4;
+  std::vector<int> h_temp_of_rep, h_rep_of_temp;
+  std::vector<float> h_beta, h_cos;
+  std::vector<double> h_beta64;
+  std::vector<int> h_rep_sys, h_rep_local;
+  for (int i = 0; i < cfg->n_systems; ++i) {
+    const pyro_system_desc& d = cfg->systems[i];
+    SysDev s;
+    std::memset(&s, 0, sizeof s);
+    s.L = d.L;
+    s.L3 = d.L * d.L * d.L;
+    const bool far = d.J2 != 0.0 || d.J3 != 0.0 || d.J3b != 0.0;
+    s.n_colours = far ? 16 : 4;
+    if (far) ctx->j1_only = false;
+    max_colours = std::max(max_colours, s.n_colours);
+    s.units_per_colour = 16 * s.L3 / s.n_colours;
+    s.n_rep = d.n_replicas;
+    s.rep_global = d.replica_offset;
+    s.rep_key = temp_base + d.replica_offset;
+    s.rep_ctx_base = rep_ctx;
+    s.temp_base = temp_base;
+    s.n_temp = d.n_temperatures;
+    s.spin_off = spin_off;
+    s.J1 = (float)d.J1;
+    s.J2 = (float)d.J2;
+    s.J3a = (float)d.J3;
+    s.J3b = (float)d.J3b;
+    s.shells = (d.J1 != 0.0 ? 1 : 0) | (d.J2 != 0.0 ? 2 : 0) | (d.J3 != 0.0 ? 4 : 0) |
+               (d.J3b != 0.0 ? 8 : 0);
+    ctx->sys.push_back(s);
+    ctx->ladders.emplace_back(d.temperatures, d.temperatures + d.n_temperatures);
+    for (int t = 0; t < d.n_temperatures; ++t) {
+      h_temp_of_rep.push_back(t);
+      h_rep_of_temp.push_back(t);
+      h_beta.push_back((float)(1.0 / d.temperatures[t]));
+      h_beta64.push_back(1.0 / d.temperatures[t]);
+      h_cos.push_back(-1.0f);
+    }
+    for (int r = 0; r < d.n_replicas; ++r) {
+      h_rep_sys.push_back(i);
+      h_rep_local.push_back(r);
+    }
+    spin_off += (long long)d.n_replicas * 16 * s.L3;
+    temp_base += d.n_temperatures;
+    rep_ctx += d.n_replicas;
+  }
+  ctx->total_temps = temp_base;
+  ctx->total_reps = rep_ctx;
+  ctx->n_spins = spin_off;
+  ctx->n_passes = max_colours;
+
+  // Pass schedules: pass p runs colour p of 16-colour systems, and colour p/4
+  // of 4-colour systems when p % 4 == 0 (or every pass if all use 4 colours).
+  ctx->pass_segs.assign(ctx->n_passes, {});
+  ctx->pass_blocks.assign(ctx->n_passes, 0);
+  for (int pass = 0; pass < ctx->n_passes; ++pass) {
+    int blocks = 0;
+    for (int i = 0; i < (int)ctx->sys.size(); ++i) {
+      const SysDev& s = ctx->sys[i];
+      int colour = -1;
+      if (s.n_colours == ctx->n_passes) colour = pass;
+      else if (pass % 4 == 0) colour = pass / 4;
+      if (colour < 0) continue;
+      PassSeg g;
+      g.sys = i;
+      g.colour = colour;
+      g.blocks_per_rep = (s.units_per_colour + kPassThreads - 1) / kPassThreads;
+      g.block_begin = blocks;
+      blocks += g.blocks_per_rep * s.n_rep;
+      ctx->pass_segs[pass].push_back(g);
+    }
+    ctx->pass_blocks[pass] = blocks;
+  }
+  // Observable segments.
+  {
+    int blocks = 0;
+    for (int i = 0; i < (int)ctx->sys.size(); ++i) {
+      const SysDev& s = ctx->sys[i];
+      ObsSeg g;
+      g.sys = i;
+      g.blocks_per_rep = (16 * s.L3 + kObsThreads * kObsSitesPerThread - 1) /
+                         (kObsThreads * kObsSitesPerThread);
+      g.block_begin = blocks;
+      g.partial_begin = blocks;
+      blocks += g.blocks_per_rep * s.n_rep;
+      ctx->obs_segs.push_back(g);
+    }
+    ctx->obs_blocks = blocks;
+  }
+
+  const int nS = (int)ctx->sys.size(), nT = ctx->total_temps, nR = ctx->total_reps;
+  CREATE_CK(alloc(&ctx->d_sys, nS));
+  CREATE_CK(alloc(&ctx->d_spins, ctx->n_spins));
+  CREATE_CK(alloc(&ctx->d_temp_of_rep, nT));
+  CREATE_CK(alloc(&ctx->d_rep_of_temp, nT));
+  CREATE_CK(alloc(&ctx->d_beta, nT));
+  CREATE_CK(alloc(&ctx->d_beta64, nT));
+  CREATE_CK(alloc(&ctx->d_cosmax, nT));
+  CREATE_CK(alloc(&ctx->d_accepted, nT));
+  CREATE_CK(alloc(&ctx->d_swap_acc, nT));
+  CREATE_CK(alloc(&ctx->d_swap_try, nT));
+  CREATE_CK(alloc(&ctx->d_swap_count, nS));
+  CREATE_CK(alloc(&ctx->d_last_accepted, nS));
+  CREATE_CK(alloc(&ctx->d_energy, nR));
+  CREATE_CK(alloc(&ctx->d_mag, 3 * nR));
+  CREATE_CK(alloc(&ctx->d_rep_sys, nR));
+  CREATE_CK(alloc(&ctx->d_rep_local, nR));
+  CREATE_CK(alloc(&ctx->d_obs_segs, ctx->obs_segs.size()));
+  CREATE_CK(alloc(&ctx->d_partials, ctx->obs_blocks));
+  CREATE_CK(alloc(&ctx->d_sweep, 1));
+  CREATE_CK(alloc(&ctx->d_scratch_u64, 4));
+  CREATE_CK(alloc(&ctx->d_history_count, 1));
+  ctx->d_pass_segs.assign(ctx->n_passes, nullptr);
+  for (int pass = 0; pass < ctx->n_passes; ++pass) {
+    CREATE_CK(alloc(&ctx->d_pass_segs[pass], ctx->pass_segs[pass].size()));
+    if (!ctx->pass_segs[pass].empty())
+      CREATE_CK(cudaMemcpy(ctx->d_pass_segs[pass], ctx->pass_segs[pass].data(),
+                           sizeof(PassSeg) * ctx->pass_segs[pass].size(), cudaMemcpyHostToDevice));
+  }
+  CREATE_CK(cudaMemcpy(ctx->d_sys, ctx->sys.data(), sizeof(SysDev) * nS, cudaMemcpyHostToDevice));
+  CREATE_CK(cudaMemcpy(ctx->d_temp_of_rep, h_temp_of_rep.data(), sizeof(int) * nT,
+                       cudaMemcpyHostToDevice));
+  CREATE_CK(cudaMemcpy(ctx->d_rep_of_temp, h_rep_of_temp.data(), sizeof(int) * nT,
+                       cudaMemcpyHostToDevice));
+  CREATE_CK(cudaMemcpy(ctx->d_beta, h_beta.data(), sizeof(float) * nT, cudaMemcpyHostToDevice));
+  CREATE_CK(cudaMemcpy(ctx->d_beta64, h_beta64.data(), sizeof(double) * nT, cudaMemcpyHostToDevice));
+  CREATE_CK(cudaMemcpy(ctx->d_cosmax, h_cos.data(), sizeof(float) * nT, cudaMemcpyHostToDevice));
+  CREATE_CK(cudaMemcpy(ctx->d_rep_sys, h_rep_sys.data(), sizeof(int) * nR, cudaMemcpyHostToDevice));
+  CREATE_CK(cudaMemcpy(ctx->d_rep_local, h_rep_local.data(), sizeof(int) * nR,
+                       cudaMemcpyHostToDevice));
+  CREATE_CK(cudaMemcpy(ctx->d_obs_segs, ctx->obs_segs.data(), sizeof(ObsSeg) * ctx->obs_segs.size(),
+                       cudaMemcpyHostToDevice));
+  CREATE_CK(cudaMemset(ctx->d_accepted, 0, sizeof(unsigned long long) * nT));
+  CREATE_CK(cudaMemset(ctx->d_swap_acc, 0, sizeof(unsigned long long) * nT));
+  CREATE_CK(cudaMemset(ctx->d_swap_try, 0, sizeof(unsigned long long) * nT));
+  CREATE_CK(cudaMemset(ctx->d_swap_count, 0, sizeof(unsigned long long) * nS));
+  CREATE_CK(cudaMemset(ctx->d_last_accepted, 0, sizeof(int) * nS));
+  CREATE_CK(cudaMemset(ctx->d_sweep, 0, sizeof(unsigned long long)));
+  CREATE_CK(cudaMemset(ctx->d_history_count, 0, sizeof(unsigned long long)));
+  CREATE_CK(cudaMemset(ctx->d_spins, 0, sizeof(float4) * ctx->n_spins));
+#undef CREATE_CK
+  *out = ctx;
+  return PYRO_OK;
+}
+
+int pyro_destroy(pyro_ctx* ctx) {
+  if (!ctx) return PYRO_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  free_all(ctx);
+  delete ctx;
+  return PYRO_OK;
+}
+
+int pyro_set_stream(pyro_ctx* ctx, void* cuda_stream) {
+  if (!ctx) return PYRO_ERR_ARG;
+  PYRO_CK(cudaSetDevice(ctx->device));
+  for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+  ctx->graphs.clear();
+  if (ctx->own_stream && ctx->stream) {
+    PYRO_CK(cudaStreamSynchronize(ctx->stream));
+    cudaStreamDestroy(ctx->stream);
+  }
+  ctx->stream = (cudaStream_t)cuda_stream;
+  ctx->own_stream = false;
+  return PYRO_OK;
+}
+
+void* pyro_get_stream(const pyro_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int pyro_synchronize(pyro_ctx* ctx) {
+  if (!ctx) return PYRO_ERR_ARG;
+  PYRO_CK(cudaSetDevice(ctx->device));
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  return PYRO_OK;
+}
+
+int pyro_system_info(const pyro_ctx* ctx, int system, int* L, int* n_sites, int* n_replicas,
+                     int* n_colours) {
+  if (!ctx || system < 0 || system >= (int)ctx->sys.size()) return PYRO_ERR_ARG;
+  const SysDev& s = ctx->sys[system];
+  if (L) *L = s.L;
+  if (n_sites) *n_sites = 16 * s.L3;
+  if (n_replicas) *n_replicas = s.n_rep;
+  if (n_colours) *n_colours = s.n_colours;
+  return PYRO_OK;
+}
+
+int pyro_init_random(pyro_ctx* ctx) {
+  if (!ctx) return PYRO_ERR_ARG;
+  PYRO_CK(cudaSetDevice(ctx->device));
+  launch_init_random(ctx->d_spins, ctx->sys.data(), ctx->d_sys, (int)ctx->sys.size(),
+                     (uint32_t)(ctx->seed & 0xffffffffu), (uint32_t)(ctx->seed >> 32), ctx->stream);
+  PYRO_CK_LAUNCH();
+  return PYRO_OK;
+}
+
+static int spin_copy(pyro_ctx* ctx, int system, void* dst, const void* src, cudaMemcpyKind kind,
+                     bool to_device, bool sync) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (system < 0 || system >= (int)ctx->sys.size() || (!dst && !src))
+    return fail(ctx, PYRO_ERR_ARG, "spin copy: bad system or null pointer");
+  PYRO_CK(cudaSetDevice(ctx->device));
+  const SysDev& s = ctx->sys[system];
+  const size_t bytes = sizeof(float4) * (size_t)s.n_rep * 16 * s.L3;
+  float4* dev = ctx->d_spins + s.spin_off;
+  if (to_device) PYRO_CK(cudaMemcpyAsync(dev, src, bytes, kind, ctx->stream));
+  else PYRO_CK(cudaMemcpyAsync(dst, dev, bytes, kind, ctx->stream));
+  if (sync) PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  return PYRO_OK;
+}
+
+int pyro_set_spins(pyro_ctx* ctx, int system, const float* host_xyzw) {
+  if (!host_xyzw) return fail(ctx, PYRO_ERR_ARG, "set_spins: null pointer");
+  return spin_copy(ctx, system, nullptr, host_xyzw, cudaMemcpyHostToDevice, true, true);
+}
+int pyro_get_spins(pyro_ctx* ctx, int system, float* host_xyzw) {
+  if (!host_xyzw) return fail(ctx, PYRO_ERR_ARG, "get_spins: null pointer");
+  return spin_copy(ctx, system, host_xyzw, nullptr, cudaMemcpyDeviceToHost, false, true);
+}
+int pyro_set_spins_device(pyro_ctx* ctx, int system, const float* dev_xyzw) {
+  if (!dev_xyzw) return fail(ctx, PYRO_ERR_ARG, "set_spins_device: null pointer");
+  return spin_copy(ctx, system, nullptr, dev_xyzw, cudaMemcpyDeviceToDevice, true, false);
+}
+int pyro_get_spins_device(pyro_ctx* ctx, int system, float* dev_xyzw) {
+  if (!dev_xyzw) return fail(ctx, PYRO_ERR_ARG, "get_spins_device: null pointer");
+  return spin_copy(ctx, system, dev_xyzw, nullptr, cudaMemcpyDeviceToDevice, false, false);
+}
+
+static int run_sweeps(pyro_ctx* ctx, int n, bool metro) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (n < 0) return fail(ctx, PYRO_ERR_ARG, "n_sweeps must be >= 0");
+  if (n == 0) return PYRO_OK;
+  PYRO_CK(cudaSetDevice(ctx->device));
+  for (int i = 0; i < n; ++i) {
+    int rc = queue_sweep(ctx, metro, (unsigned long long)i);
+    if (rc != PYRO_OK) return rc;
+  }
+  launch_advance(ctx->d_sweep, (unsigned long long)n, ctx->stream);
+  PYRO_CK_LAUNCH();
+  ctx->h_sweep += (unsigned long long)n;
+  if (metro) ctx->metro_sweeps_since_reset += (unsigned long long)n;
+  return PYRO_OK;
+}
+
+int pyro_metropolis_sweep(pyro_ctx* ctx, int n_sweeps) { return run_sweeps(ctx, n_sweeps, true); }
+int pyro_overrelax_sweep(pyro_ctx* ctx, int n_sweeps) { return run_sweeps(ctx, n_sweeps, false); }
+
+int pyro_set_cone(pyro_ctx* ctx, int system, const float* cosmax) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (system < 0 || system >= (int)ctx->sys.size() || !cosmax)
+    return fail(ctx, PYRO_ERR_ARG, "set_cone: bad system or null pointer");
+  const SysDev& s = ctx->sys[system];
+  for (int t = 0; t < s.n_temp; ++t)
+    if (!(cosmax[t] >= -1.0f && cosmax[t] < 1.0f))
+      return fail(ctx, PYRO_ERR_ARG, "set_cone: cos(theta_max) must lie in [-1, 1)");
+  PYRO_CK(cudaSetDevice(ctx->device));
+  PYRO_CK(cudaMemcpyAsync(ctx->d_cosmax + s.temp_base, cosmax, sizeof(float) * s.n_temp,
+                          cudaMemcpyHostToDevice, ctx->stream));
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  return PYRO_OK;
+}
+
+int pyro_get_cone(pyro_ctx* ctx, int system, float* cosmax) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (system < 0 || system >= (int)ctx->sys.size() || !cosmax)
+    return fail(ctx, PYRO_ERR_ARG, "get_cone: bad system or null pointer");
+  const SysDev& s = ctx->sys[system];
+  PYRO_CK(cudaSetDevice(ctx->device));
+  PYRO_CK(cudaMemcpyAsync(cosmax, ctx->d_cosmax + s.temp_base, sizeof(float) * s.n_temp,
+                          cudaMemcpyDeviceToHost, ctx->stream));
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  return PYRO_OK;
+}
+
+int pyro_get_acceptance(pyro_ctx* ctx, int system, uint64_t* accepted, uint64_t* proposed) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (system < 0 || system >= (int)ctx->sys.size() || !accepted)
+    return fail(ctx, PYRO_ERR_ARG, "get_acceptance: bad system or null pointer");
+  const SysDev& s = ctx->sys[system];
+  PYRO_CK(cudaSetDevice(ctx->device));
+  PYRO_CK(cudaMemcpyAsync(accepted, ctx->d_accepted + s.temp_base,
+                          sizeof(unsigned long long) * s.n_temp, cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  if (proposed) {
+    // Each temperature slot holds exactly one replica during every sweep;
+    // in a sharded context only the slots of held replicas are counted here.
+    const uint64_t per = (uint64_t)16 * s.L3 * ctx->metro_sweeps_since_reset;
+    for (int t = 0; t < s.n_temp; ++t) proposed[t] = s.n_rep == s.n_temp ? per : 0;
+  }
+  return PYRO_OK;
+}
+
+int pyro_reset_acceptance(pyro_ctx* ctx) {
+  if (!ctx) return PYRO_ERR_ARG;
+  PYRO_CK(cudaSetDevice(ctx->device));
+  PYRO_CK(cudaMemsetAsync(ctx->d_accepted, 0, sizeof(unsigned long long) * ctx->total_temps,
+                          ctx->stream));
+  ctx->metro_sweeps_since_reset = 0;
+  return PYRO_OK;
+}
+
+int pyro_tune_cone(pyro_ctx* ctx, double target, int iterations, int sweeps_per_iteration,
+                   int n_or) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (!(target > 0.0 && target < 1.0) || iterations < 0 || sweeps_per_iteration < 1 || n_or < 0)
+    return fail(ctx, PYRO_ERR_ARG, "tune_cone: need 0 < target < 1, iterations >= 0, sweeps >= 1");
+  if (sharded(ctx))
+    return fail(ctx, PYRO_ERR_STATE, "tune_cone: needs every replica of the ladder in one context");
+  std::vector<float> cosv;
+  std::vector<uint64_t> acc, prop;
+  for (int it = 0; it < iterations; ++it) {
+    int rc = pyro_reset_acceptance(ctx);
+    if (rc) return rc;
+    for (int k = 0; k < sweeps_per_iteration; ++k) {
+      if ((rc = pyro_metropolis_sweep(ctx, 1))) return rc;
+      if (n_or > 0 && (rc = pyro_overrelax_sweep(ctx, n_or))) return rc;
+    }
+    bool done = true;
+    for (int si = 0; si < (int)ctx->sys.size(); ++si) {
+      const SysDev& s = ctx->sys[si];
+      cosv.resize(s.n_temp);
+      acc.resize(s.n_temp);
+      prop.resize(s.n_temp);
+      if ((rc = pyro_get_acceptance(ctx, si, acc.data(), prop.data()))) return rc;
+      if ((rc = pyro_get_cone(ctx, si, cosv.data()))) return rc;
+      for (int t = 0; t < s.n_temp; ++t) {
+        const double ratio = prop[t] ? (double)acc[t] / (double)prop[t] : target;
+        if (std::fabs(ratio - target) > 0.02) done = false;
+        double theta = std::acos(std::max(-1.0, std::min(1.0, (double)cosv[t])));
+        const double f = std::max(0.5, std::min(2.0, ratio / target));
+        theta = std::max(1e-4, std::min(M_PI, theta * f));
+        float c = (float)std::cos(theta);
+        if (c >= 1.0f) c = std::nextafter(1.0f, 0.0f);
+        if (c < -1.0f) c = -1.0f;
+        cosv[t] = c;
+      }
+      if ((rc = pyro_set_cone(ctx, si, cosv.data()))) return rc;
+    }
+    if (done) break;
+  }
+  return pyro_reset_acceptance(ctx);
+}
+
+int pyro_observables_device(pyro_ctx* ctx, int system, double* dev_energy,
+                            double* dev_magnetisation3) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (system < 0 || system >= (int)ctx->sys.size())
+    return fail(ctx, PYRO_ERR_ARG, "observables: bad system");
+  PYRO_CK(cudaSetDevice(ctx->device));
+  int rc = queue_observables(ctx);
+  if (rc) return rc;
+  const SysDev& s = ctx->sys[system];
+  if (dev_energy)
+    PYRO_CK(cudaMemcpyAsync(dev_energy, ctx->d_energy + s.rep_ctx_base, sizeof(double) * s.n_rep,
+                            cudaMemcpyDeviceToDevice, ctx->stream));
+  if (dev_magnetisation3)
+    PYRO_CK(cudaMemcpyAsync(dev_magnetisation3, ctx->d_mag + 3 * s.rep_ctx_base,
+                            sizeof(double) * 3 * s.n_rep, cudaMemcpyDeviceToDevice, ctx->stream));
+  return PYRO_OK;
+}
+
+int pyro_observables(pyro_ctx* ctx, int system, double* energy, double* magnetisation3) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (system < 0 || system >= (int)ctx->sys.size())
+    return fail(ctx, PYRO_ERR_ARG, "observables: bad system");
+  PYRO_CK(cudaSetDevice(ctx->device));
+  int rc = queue_observables(ctx);
+  if (rc) return rc;
+  const SysDev& s = ctx->sys[system];
+  if (energy)
+    PYRO_CK(cudaMemcpyAsync(energy, ctx->d_energy + s.rep_ctx_base, sizeof(double) * s.n_rep,
+                            cudaMemcpyDeviceToHost, ctx->stream));
+  if (magnetisation3)
+    PYRO_CK(cudaMemcpyAsync(magnetisation3, ctx->d_mag + 3 * s.rep_ctx_base,
+                            sizeof(double) * 3 * s.n_rep, cudaMemcpyDeviceToHost, ctx->stream));
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  return PYRO_OK;
+}
+
+int pyro_get_temperatures(pyro_ctx* ctx, int system, double* temperature_of_replica) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (system < 0 || system >= (int)ctx->sys.size() || !temperature_of_replica)
+    return fail(ctx, PYRO_ERR_ARG, "get_temperatures: bad system or null pointer");
+  const SysDev& s = ctx->sys[system];
+  std::vector<int> t(s.n_temp);
+  PYRO_CK(cudaSetDevice(ctx->device));
+  PYRO_CK(cudaMemcpyAsync(t.data(), ctx->d_temp_of_rep + s.temp_base, sizeof(int) * s.n_temp,
+                          cudaMemcpyDeviceToHost, ctx->stream));
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  for (int g = 0; g < s.n_temp; ++g) temperature_of_replica[g] = ctx->ladders[system][t[g]];
+  return PYRO_OK;
+}
+
+int pyro_get_permutation(pyro_ctx* ctx, int system, int* replica_of_temperature) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (system < 0 || system >= (int)ctx->sys.size() || !replica_of_temperature)
+    return fail(ctx, PYRO_ERR_ARG, "get_permutation: bad system or null pointer");
+  const SysDev& s = ctx->sys[system];
+  PYRO_CK(cudaSetDevice(ctx->device));
+  PYRO_CK(cudaMemcpyAsync(replica_of_temperature, ctx->d_rep_of_temp + s.temp_base,
+                          sizeof(int) * s.n_temp, cudaMemcpyDeviceToHost, ctx->stream));
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  return PYRO_OK;
+}
+
+int pyro_pt_swap(pyro_ctx* ctx, int parity, int* n_accepted) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (parity > 1) return fail(ctx, PYRO_ERR_ARG, "pt_swap: parity must be 0, 1 or < 0 (auto)");
+  if (sharded(ctx))
+    return fail(ctx, PYRO_ERR_STATE,
+                "pt_swap: context holds part of the ladder; use pyro_pt_swap_global");
+  PYRO_CK(cudaSetDevice(ctx->device));
+  int rc = queue_observables(ctx);
+  if (rc) return rc;
+  ExchangeParams x = exchange_params(ctx);
+  x.parity = parity < 0 ? -1 : parity;
+  launch_exchange(x, (int)ctx->sys.size(), max_pairs(ctx), ctx->stream);
+  PYRO_CK_LAUNCH();
+  if (n_accepted) {
+    std::vector<int> a(ctx->sys.size());
+    PYRO_CK(cudaMemcpyAsync(a.data(), ctx->d_last_accepted, sizeof(int) * a.size(),
+                            cudaMemcpyDeviceToHost, ctx->stream));
+    PYRO_CK(cudaStreamSynchronize(ctx->stream));
+    int sum = 0;
+    for (int v : a) sum += v;
+    *n_accepted = sum;
+  }
+  return PYRO_OK;
+}
+
+int pyro_pt_swap_global(pyro_ctx* ctx, int system, const double* dev_energy_all, int parity) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (system < 0 || system >= (int)ctx->sys.size() || !dev_energy_all)
+    return fail(ctx, PYRO_ERR_ARG, "pt_swap_global: bad system or null pointer");
+  if (parity > 1) return fail(ctx, PYRO_ERR_ARG, "pt_swap_global: parity must be 0, 1 or < 0");
+  PYRO_CK(cudaSetDevice(ctx->device));
+  ExchangeParams x = exchange_params(ctx);
+  x.sys_first = system;
+  x.energy = dev_energy_all;
+  x.energy_is_global = 1;
+  x.parity = parity < 0 ? -1 : parity;
+  x.history_count = nullptr;
+  launch_exchange(x, 1, (ctx->sys[system].n_temp + 1) / 2, ctx->stream);
+  PYRO_CK_LAUNCH();
+  return PYRO_OK;
+}
+
+int pyro_get_swap_stats(pyro_ctx* ctx, int system, uint64_t* accepted, uint64_t* attempted) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (system < 0 || system >= (int)ctx->sys.size())
+    return fail(ctx, PYRO_ERR_ARG, "get_swap_stats: bad system");
+  const SysDev& s = ctx->sys[system];
+  PYRO_CK(cudaSetDevice(ctx->device));
+  if (accepted)
+    PYRO_CK(cudaMemcpyAsync(accepted, ctx->d_swap_acc + s.temp_base, 8 * s.n_temp,
+                            cudaMemcpyDeviceToHost, ctx->stream));
+  if (attempted)
+    PYRO_CK(cudaMemcpyAsync(attempted, ctx->d_swap_try + s.temp_base, 8 * s.n_temp,
+                            cudaMemcpyDeviceToHost, ctx->stream));
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  return PYRO_OK;
+}
+
+int pyro_enable_history(pyro_ctx* ctx, int capacity_cycles) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (capacity_cycles < 0) return fail(ctx, PYRO_ERR_ARG, "history capacity must be >= 0");
+  PYRO_CK(cudaSetDevice(ctx->device));
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+  ctx->graphs.clear();
+  if (ctx->d_history) cudaFree(ctx->d_history);
+  ctx->d_history = nullptr;
+  ctx->history_cap = capacity_cycles;
+  if (capacity_cycles > 0)
+    PYRO_CK(alloc(&ctx->d_history, (size_t)capacity_cycles * ctx->total_temps));
+  PYRO_CK(cudaMemset(ctx->d_history_count, 0, sizeof(unsigned long long)));
+  return PYRO_OK;
+}
+
+int pyro_get_history(pyro_ctx* ctx, int system, double* out, int* n_cycles) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (system < 0 || system >= (int)ctx->sys.size() || !out || !n_cycles)
+    return fail(ctx, PYRO_ERR_ARG, "get_history: bad system or null pointer");
+  if (!ctx->d_history) return fail(ctx, PYRO_ERR_STATE, "get_history: history not enabled");
+  PYRO_CK(cudaSetDevice(ctx->device));
+  unsigned long long count = 0;
+  PYRO_CK(cudaMemcpyAsync(&count, ctx->d_history_count, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  const int n = (int)std::min<unsigned long long>(count, (unsigned long long)ctx->history_cap);
+  std::vector<double> all((size_t)ctx->history_cap * ctx->total_temps);
+  PYRO_CK(cudaMemcpy(all.data(), ctx->d_history, sizeof(double) * all.size(),
+                     cudaMemcpyDeviceToHost));
+  const SysDev& s = ctx->sys[system];
+  // Oldest first: when the ring wrapped, start at the oldest slot.
+  const unsigned long long first = count > (unsigned long long)ctx->history_cap
+                                       ? count % (unsigned long long)ctx->history_cap
+                                       : 0ull;
+  for (int c = 0; c < n; ++c) {
+    const size_t slot = (size_t)((first + c) % ctx->history_cap);
+    for (int t = 0; t < s.n_temp; ++t)
+      out[(size_t)c * s.n_temp + t] = all[slot * ctx->total_temps + s.temp_base + t];
+  }
+  *n_cycles = n;
+  return PYRO_OK;
+}
+
+int pyro_cycle(pyro_ctx* ctx, int n_metro, int n_or, int do_swap, int n_cycles) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (n_metro < 0 || n_or < 0 || n_cycles < 0)
+    return fail(ctx, PYRO_ERR_ARG, "cycle: counts must be >= 0");
+  if (do_swap && sharded(ctx))
+    return fail(ctx, PYRO_ERR_STATE,
+                "cycle: a sharded context exchanges through pyro_pt_swap_global");
+  if (n_cycles == 0) return PYRO_OK;
+  PYRO_CK(cudaSetDevice(ctx->device));
+  const auto key = std::make_tuple(n_metro, n_or, do_swap ? 1 : 0);
+  auto it = ctx->graphs.find(key);
+  if (it == ctx->graphs.end()) {
+    cudaGraph_t g;
+    PYRO_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = PYRO_OK;
+    for (int i = 0; i < n_metro && rc == PYRO_OK; ++i) rc = queue_sweep(ctx, true, i);
+    for (int i = 0; i < n_or && rc == PYRO_OK; ++i) rc = queue_sweep(ctx, false, n_metro + i);
+    if (rc == PYRO_OK) rc = queue_observables(ctx);
+    if (rc == PYRO_OK) {
+      ExchangeParams x = exchange_params(ctx);
+      x.do_swap = do_swap ? 1 : 0;
+      x.parity = -1;
+      x.history = ctx->d_history;
+      x.sweep_ctr = ctx->d_sweep;
+      x.sweep_advance = (unsigned long long)(n_metro + n_or);
+      launch_exchange(x, (int)ctx->sys.size(), max_pairs(ctx), ctx->stream);
+      if (cudaGetLastError() != cudaSuccess) rc = PYRO_ERR_CUDA;
+    }
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (rc != PYRO_OK) return fail(ctx, rc, "cycle: capture failed: " + ctx->err);
+    if (e != cudaSuccess)
+      return fail(ctx, PYRO_ERR_CUDA, std::string("cycle: end capture: ") + cudaGetErrorString(e));
+    cudaGraphExec_t ge;
+    e = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess)
+      return fail(ctx, PYRO_ERR_CUDA, std::string("cycle: instantiate: ") + cudaGetErrorString(e));
+    it = ctx->graphs.emplace(key, ge).first;
+  }
+  for (int c = 0; c < n_cycles; ++c) PYRO_CK(cudaGraphLaunch(it->second, ctx->stream));
+  ctx->h_sweep += (unsigned long long)(n_metro + n_or) * n_cycles;
+  ctx->metro_sweeps_since_reset += (unsigned long long)n_metro * n_cycles;
+  return PYRO_OK;
+}
+
+int pyro_get_sweep_count(pyro_ctx* ctx, uint64_t* sweeps) {
+  if (!ctx || !sweeps) return PYRO_ERR_ARG;
+  PYRO_CK(cudaSetDevice(ctx->device));
+  unsigned long long v = 0;
+  PYRO_CK(cudaMemcpyAsync(&v, ctx->d_sweep, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  *sweeps = v;
+  return PYRO_OK;
+}
+
+int pyro_check_spins(pyro_ctx* ctx, float tol, long long* first_bad) {
+  if (!ctx) return PYRO_ERR_ARG;
+  PYRO_CK(cudaSetDevice(ctx->device));
+  const unsigned long long none = ~0ull;
+  PYRO_CK(cudaMemcpyAsync(ctx->d_scratch_u64, &none, 8, cudaMemcpyHostToDevice, ctx->stream));
+  launch_check_spins(ctx->d_spins, ctx->n_spins, tol, ctx->d_scratch_u64, ctx->stream);
+  PYRO_CK_LAUNCH();
+  unsigned long long v = none;
+  PYRO_CK(cudaMemcpyAsync(&v, ctx->d_scratch_u64, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  if (first_bad) *first_bad = v == none ? -1 : (long long)v;
+  if (v != none) return fail(ctx, PYRO_ERR_NAN, "check_spins: non-finite or non-unit spin");
+  return PYRO_OK;
+}
+
+int pyro_structure_factor(pyro_ctx* ctx, int system, int replica, int G, int stride, double* out) {
+  (void)system;
+  (void)replica;
+  (void)G;
+  (void)stride;
+  (void)out;
+  return fail(ctx, PYRO_ERR_STATE, "structure_factor: not available in this build");
+}
+
+}  // extern "C"

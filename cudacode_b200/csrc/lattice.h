@@ -1,0 +1,80 @@
+// Pyrochlore geometry, colour schedules and the per-pass work description.
+//
+// Geometry (taillefu/cudacode Pyrochlore.cu:1339-1401, atom positions; 16-site
+// conventional cubic cell = 4 FCC corners x 4-site basis, Pyrochlore.cu:29-30):
+// site s = 4 f + b sits at F[f] + B[b], with the FCC corners
+// F = (0,0,0), (1/2,1/2,0), (0,1/2,1/2), (1/2,0,1/2) and the basis B = F/2.
+// b is the pyrochlore sublattice; {4f..4f+3} is one up-tetrahedron.
+//
+// The neighbour table is not copied from links16 (Pyrochlore.cu:152-167): it
+// is generated from the positions by distance shell,
+//   J1  : |r|^2 = 2/16  (6 neighbours)   J2 : 6/16 (12)
+//   J3a : 8/16 through a shared neighbour (r = 2 x a J1 bond vector; 6)
+//   J3b : 8/16 across a hexagon (the other 6),
+// in the canonical order (shell, target site, dx, dy, dz). The oracle sums a
+// site's neighbours in exactly this order, which the bit-exact parity needs.
+#pragma once
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define PYRO_HOSTDEV __host__ __device__
+#else
+#define PYRO_HOSTDEV
+#endif
+
+namespace pyro {
+
+constexpr int kSitesPerCell = 16;
+constexpr int kMaxNbr = 30;
+constexpr int kShellBegin[5] = {0, 6, 18, 24, 30};  // J1, J2, J3a, J3b, end
+
+struct NbrEntry {
+  int8_t dx, dy, dz, t;  // neighbour cell offset and its site in the cell
+};
+
+struct NbrTable {
+  NbrEntry e[kSitesPerCell][kMaxNbr];
+};
+
+// Positions in units of a/4.
+inline void site_pos4(int s, int p[3]) {
+  static const int F[4][3] = {{0, 0, 0}, {2, 2, 0}, {0, 2, 2}, {2, 0, 2}};
+  const int f = s >> 2, b = s & 3;
+  for (int k = 0; k < 3; ++k) p[k] = F[f][k] + F[b][k] / 2;
+}
+
+// Builds the canonical table; returns false if a shell count is off.
+bool build_neighbour_table(NbrTable* tab);
+
+// Work description of one colour pass over one (system, colour) pair.
+struct PassSeg {
+  int sys;             // system index
+  int colour;          // colour class
+  int blocks_per_rep;  // CTAs per replica
+  int block_begin;     // first CTA of the segment in the launch
+};
+
+// Per-system constants in device memory.
+struct SysDev {
+  int L, L3;
+  int n_colours;       // 4 (J1 only) or 16
+  int units_per_colour;  // sites per colour class per replica
+  int n_rep;           // replicas held
+  int rep_global;      // global replica id of replica 0 within the system's ladder
+  int rep_key;         // Philox replica word of replica 0 (unique across systems)
+  int rep_ctx_base;    // index of replica 0 in the context-wide per-replica arrays
+  int temp_base;       // offset of this system's temperature arrays
+  int n_temp;          // ladder size
+  long long spin_off;  // float4 offset of replica 0
+  float J1, J2, J3a, J3b;
+  int shells;          // bitmask of non-zero shells: 1 J1, 2 J2, 4 J3a, 8 J3b
+};
+
+// Sites of colour class c: for the 4-colour schedule colour b holds sites
+// {b, 4+b, 8+b, 12+b} (the pyrochlore sublattices, Pyrochlore.cu:36-43
+// groups {0,4,8,12}...{3,7,11,15}); for 16 colours colour c is site c.
+PYRO_HOSTDEV inline int colour_site(int n_colours, int colour, int k) {
+  return n_colours == 4 ? 4 * k + colour : colour;
+}
+
+}  // namespace pyro

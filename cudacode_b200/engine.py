@@ -1,0 +1,359 @@
+"""Python binding of the C-ABI in ``include/pyro.h`` (ctypes).
+
+The engine runs only on the GPU: loading fails loudly when ``libpyro.so`` is
+missing, and every call raises :class:`PyroError` when the library returns a
+negative status. Host arrays are numpy arrays owned by the caller.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import Sequence
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libpyro.so")
+
+PYRO_OK = 0
+ERRORS = {
+    -1: "PYRO_ERR_ARG",
+    -2: "PYRO_ERR_CUDA",
+    -3: "PYRO_ERR_TIMEOUT",
+    -4: "PYRO_ERR_NAN",
+    -5: "PYRO_ERR_IO",
+    -6: "PYRO_ERR_STATE",
+    -7: "PYRO_ERR_NOMEM",
+}
+
+
+class PyroError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {message}")
+        self.code = code
+
+
+class SystemDesc(C.Structure):
+    _fields_ = [
+        ("L", C.c_int),
+        ("n_replicas", C.c_int),
+        ("replica_offset", C.c_int),
+        ("n_temperatures", C.c_int),
+        ("temperatures", C.POINTER(C.c_double)),
+        ("J1", C.c_double),
+        ("J2", C.c_double),
+        ("J3", C.c_double),
+        ("J3b", C.c_double),
+    ]
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("n_systems", C.c_int),
+        ("systems", C.POINTER(SystemDesc)),
+        ("seed", C.c_uint64),
+        ("device", C.c_int),
+        ("renorm_every", C.c_int),
+    ]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Loads libpyro.so (built in-tree by ``python -m cudacode_b200.build``)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(
+            f"{path} is missing: build it with `python -m cudacode_b200.build`; "
+            "the engine has no CPU fallback")
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    i, d, f = C.c_int, C.c_double, C.c_float
+    pd, pf, pi = C.POINTER(C.c_double), C.POINTER(C.c_float), C.POINTER(C.c_int)
+    pu64 = C.POINTER(C.c_uint64)
+    sig = {
+        "pyro_create": (i, [C.POINTER(Config), C.POINTER(P)]),
+        "pyro_destroy": (i, [P]),
+        "pyro_last_error": (C.c_char_p, [P]),
+        "pyro_version": (i, []),
+        "pyro_neighbour_table": (i, [i, pi]),
+        "pyro_set_stream": (i, [P, P]),
+        "pyro_get_stream": (P, [P]),
+        "pyro_synchronize": (i, [P]),
+        "pyro_system_info": (i, [P, i, pi, pi, pi, pi]),
+        "pyro_init_random": (i, [P]),
+        "pyro_set_spins": (i, [P, i, pf]),
+        "pyro_get_spins": (i, [P, i, pf]),
+        "pyro_set_spins_device": (i, [P, i, P]),
+        "pyro_get_spins_device": (i, [P, i, P]),
+        "pyro_metropolis_sweep": (i, [P, i]),
+        "pyro_overrelax_sweep": (i, [P, i]),
+        "pyro_set_cone": (i, [P, i, pf]),
+        "pyro_get_cone": (i, [P, i, pf]),
+        "pyro_get_acceptance": (i, [P, i, pu64, pu64]),
+        "pyro_reset_acceptance": (i, [P]),
+        "pyro_tune_cone": (i, [P, d, i, i, i]),
+        "pyro_observables": (i, [P, i, pd, pd]),
+        "pyro_observables_device": (i, [P, i, P, P]),
+        "pyro_get_temperatures": (i, [P, i, pd]),
+        "pyro_get_permutation": (i, [P, i, pi]),
+        "pyro_pt_swap": (i, [P, i, pi]),
+        "pyro_pt_swap_global": (i, [P, i, P, i]),
+        "pyro_get_swap_stats": (i, [P, i, pu64, pu64]),
+        "pyro_cycle": (i, [P, i, i, i, i]),
+        "pyro_enable_history": (i, [P, i]),
+        "pyro_get_history": (i, [P, i, pd, pi]),
+        "pyro_get_sweep_count": (i, [P, pu64]),
+        "pyro_check_spins": (i, [P, f, C.POINTER(C.c_longlong)]),
+        "pyro_structure_factor": (i, [P, i, i, i, i, pd]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _ptr(a: np.ndarray, ctype):
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+@dataclass
+class System:
+    """One pyrochlore lattice: L^3 cubic cells (16 L^3 sites) and a ladder."""
+
+    L: int
+    temperatures: Sequence[float]
+    J1: float = 1.0
+    J2: float = 0.0
+    J3: float = 0.0
+    J3b: float = 0.0
+    n_replicas: int | None = None  # default: the whole ladder
+    replica_offset: int = 0
+
+    @property
+    def n_sites(self) -> int:
+        return 16 * self.L ** 3
+
+    @property
+    def n_colours(self) -> int:
+        return 16 if (self.J2 or self.J3 or self.J3b) else 4
+
+    def replicas(self) -> int:
+        return len(self.temperatures) if self.n_replicas is None else self.n_replicas
+
+
+def neighbour_table(site: int) -> np.ndarray:
+    """(30, 4) array of (dx, dy, dz, target site) for cubic-cell site `site`."""
+    lib = load_library()
+    out = np.empty(120, dtype=np.int32)
+    rc = lib.pyro_neighbour_table(site, _ptr(out, C.c_int))
+    if rc != PYRO_OK:
+        raise PyroError(rc, "pyro_neighbour_table")
+    return out.reshape(30, 4)
+
+
+def geometric_ladder(t_min: float, t_max: float, n: int) -> list[float]:
+    if n == 1:
+        return [float(t_min)]
+    r = (t_max / t_min) ** (1.0 / (n - 1))
+    return [float(t_min * r ** k) for k in range(n)]
+
+
+class Engine:
+    """One GPU context over one or more systems (``pyro_ctx``)."""
+
+    def __init__(self, systems: Sequence[System], seed: int = 12345, device: int = 0,
+                 renorm_every: int = 0):
+        self.lib = load_library()
+        self.systems = list(systems)
+        self._temps = [np.ascontiguousarray(s.temperatures, dtype=np.float64) for s in systems]
+        descs = (SystemDesc * len(systems))()
+        for k, s in enumerate(systems):
+            descs[k].L = s.L
+            descs[k].n_replicas = s.replicas()
+            descs[k].replica_offset = s.replica_offset
+            descs[k].n_temperatures = len(s.temperatures)
+            descs[k].temperatures = _ptr(self._temps[k], C.c_double)
+            descs[k].J1, descs[k].J2, descs[k].J3, descs[k].J3b = s.J1, s.J2, s.J3, s.J3b
+        cfg = Config(len(systems), descs, seed, device, renorm_every)
+        h = C.c_void_p()
+        rc = self.lib.pyro_create(C.byref(cfg), C.byref(h))
+        if rc != PYRO_OK:
+            raise PyroError(rc, "pyro_create failed (see stderr)")
+        self.ctx = h
+        self.seed = seed
+
+    # -- plumbing ---------------------------------------------------------
+    def _ck(self, rc: int) -> int:
+        if rc < 0:
+            raise PyroError(rc, self.lib.pyro_last_error(self.ctx).decode())
+        return rc
+
+    def close(self) -> None:
+        if getattr(self, "ctx", None):
+            self.lib.pyro_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_stream(self, stream_handle: int) -> None:
+        self._ck(self.lib.pyro_set_stream(self.ctx, C.c_void_p(stream_handle)))
+
+    def synchronize(self) -> None:
+        self._ck(self.lib.pyro_synchronize(self.ctx))
+
+    def info(self, system: int = 0) -> dict:
+        L, n, r, c = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        self._ck(self.lib.pyro_system_info(self.ctx, system, C.byref(L), C.byref(n), C.byref(r),
+                                           C.byref(c)))
+        return {"L": L.value, "n_sites": n.value, "n_replicas": r.value, "n_colours": c.value}
+
+    # -- spins ------------------------------------------------------------
+    def init_random(self) -> None:
+        self._ck(self.lib.pyro_init_random(self.ctx))
+
+    def spin_shape(self, system: int = 0) -> tuple:
+        s = self.systems[system]
+        return (s.replicas(), 16, s.L ** 3, 4)
+
+    def get_spins(self, system: int = 0) -> np.ndarray:
+        out = np.empty(self.spin_shape(system), dtype=np.float32)
+        self._ck(self.lib.pyro_get_spins(self.ctx, system, _ptr(out, C.c_float)))
+        return out
+
+    def set_spins(self, spins: np.ndarray, system: int = 0) -> None:
+        a = np.ascontiguousarray(spins, dtype=np.float32)
+        if a.size != int(np.prod(self.spin_shape(system))):
+            raise ValueError(f"expected {self.spin_shape(system)} spins, got {a.shape}")
+        self._ck(self.lib.pyro_set_spins(self.ctx, system, _ptr(a, C.c_float)))
+
+    def set_spins_device(self, ptr: int, system: int = 0) -> None:
+        self._ck(self.lib.pyro_set_spins_device(self.ctx, system, C.c_void_p(ptr)))
+
+    def get_spins_device(self, ptr: int, system: int = 0) -> None:
+        self._ck(self.lib.pyro_get_spins_device(self.ctx, system, C.c_void_p(ptr)))
+
+    def check_spins(self, tol: float = 1e-3) -> int:
+        bad = C.c_longlong(-1)
+        rc = self.lib.pyro_check_spins(self.ctx, tol, C.byref(bad))
+        if rc == -4:
+            return bad.value
+        self._ck(rc)
+        return -1
+
+    # -- sweeps -----------------------------------------------------------
+    def metropolis_sweep(self, n: int = 1) -> None:
+        self._ck(self.lib.pyro_metropolis_sweep(self.ctx, n))
+
+    def overrelax_sweep(self, n: int = 1) -> None:
+        self._ck(self.lib.pyro_overrelax_sweep(self.ctx, n))
+
+    def cycle(self, n_metro: int, n_or: int, do_swap: bool = True, n_cycles: int = 1) -> None:
+        self._ck(self.lib.pyro_cycle(self.ctx, n_metro, n_or, int(bool(do_swap)), n_cycles))
+
+    def sweep_count(self) -> int:
+        v = C.c_uint64()
+        self._ck(self.lib.pyro_get_sweep_count(self.ctx, C.byref(v)))
+        return v.value
+
+    # -- cone -------------------------------------------------------------
+    def set_cone(self, cosmax, system: int = 0) -> None:
+        a = np.ascontiguousarray(cosmax, dtype=np.float32)
+        self._ck(self.lib.pyro_set_cone(self.ctx, system, _ptr(a, C.c_float)))
+
+    def get_cone(self, system: int = 0) -> np.ndarray:
+        out = np.empty(len(self.systems[system].temperatures), dtype=np.float32)
+        self._ck(self.lib.pyro_get_cone(self.ctx, system, _ptr(out, C.c_float)))
+        return out
+
+    def acceptance(self, system: int = 0) -> tuple[np.ndarray, np.ndarray]:
+        n = len(self.systems[system].temperatures)
+        acc = np.zeros(n, dtype=np.uint64)
+        prop = np.zeros(n, dtype=np.uint64)
+        self._ck(self.lib.pyro_get_acceptance(self.ctx, system, _ptr(acc, C.c_uint64),
+                                              _ptr(prop, C.c_uint64)))
+        return acc, prop
+
+    def reset_acceptance(self) -> None:
+        self._ck(self.lib.pyro_reset_acceptance(self.ctx))
+
+    def tune_cone(self, target: float = 0.5, iterations: int = 20, sweeps: int = 10,
+                  n_or: int = 0) -> None:
+        self._ck(self.lib.pyro_tune_cone(self.ctx, target, iterations, sweeps, n_or))
+
+    # -- observables and exchange ----------------------------------------
+    def observables(self, system: int = 0) -> tuple[np.ndarray, np.ndarray]:
+        r = self.systems[system].replicas()
+        e = np.empty(r, dtype=np.float64)
+        m = np.empty((r, 3), dtype=np.float64)
+        self._ck(self.lib.pyro_observables(self.ctx, system, _ptr(e, C.c_double),
+                                           _ptr(m, C.c_double)))
+        return e, m
+
+    def observables_device(self, e_ptr: int, m_ptr: int = 0, system: int = 0) -> None:
+        self._ck(self.lib.pyro_observables_device(self.ctx, system, C.c_void_p(e_ptr),
+                                                  C.c_void_p(m_ptr or None)))
+
+    def temperatures_of_replicas(self, system: int = 0) -> np.ndarray:
+        out = np.empty(len(self.systems[system].temperatures), dtype=np.float64)
+        self._ck(self.lib.pyro_get_temperatures(self.ctx, system, _ptr(out, C.c_double)))
+        return out
+
+    def permutation(self, system: int = 0) -> np.ndarray:
+        out = np.empty(len(self.systems[system].temperatures), dtype=np.int32)
+        self._ck(self.lib.pyro_get_permutation(self.ctx, system, _ptr(out, C.c_int)))
+        return out
+
+    def pt_swap(self, parity: int = -1) -> int:
+        n = C.c_int()
+        self._ck(self.lib.pyro_pt_swap(self.ctx, parity, C.byref(n)))
+        return n.value
+
+    def pt_swap_global(self, e_all_ptr: int, parity: int = -1, system: int = 0) -> None:
+        self._ck(self.lib.pyro_pt_swap_global(self.ctx, system, C.c_void_p(e_all_ptr), parity))
+
+    def swap_stats(self, system: int = 0) -> tuple[np.ndarray, np.ndarray]:
+        n = len(self.systems[system].temperatures)
+        a = np.zeros(n, dtype=np.uint64)
+        t = np.zeros(n, dtype=np.uint64)
+        self._ck(self.lib.pyro_get_swap_stats(self.ctx, system, _ptr(a, C.c_uint64),
+                                              _ptr(t, C.c_uint64)))
+        return a, t
+
+    def enable_history(self, capacity: int) -> None:
+        self._ck(self.lib.pyro_enable_history(self.ctx, capacity))
+        self._history_cap = capacity
+
+    def history(self, system: int = 0) -> np.ndarray:
+        """Energy of every temperature slot per recorded cycle, oldest first."""
+        nT = len(self.systems[system].temperatures)
+        cap = getattr(self, "_history_cap", 0)
+        if cap <= 0:
+            raise PyroError(-6, "history not enabled")
+        out = np.empty((cap, nT), dtype=np.float64)
+        n = C.c_int()
+        self._ck(self.lib.pyro_get_history(self.ctx, system, _ptr(out, C.c_double), C.byref(n)))
+        return out[: n.value].copy()
+
+    def structure_factor(self, G: int, stride: int = 1, replica: int = -1,
+                         system: int = 0) -> np.ndarray:
+        out = np.empty((G, G, G), dtype=np.float64)
+        self._ck(self.lib.pyro_structure_factor(self.ctx, system, replica, G, stride,
+                                                _ptr(out, C.c_double)))
+        return out

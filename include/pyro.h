@@ -1,0 +1,172 @@
+/*
+ * pyro.h — C-ABI of the B200 Monte Carlo engine for classical O(3)
+ * Heisenberg spins on the pyrochlore lattice (16 L^3 sites, 6 nearest
+ * neighbours; H = J1 sum_<ij> S_i.S_j + J2 sum_<<ij>> + J3 sum_<<<ij>>>).
+ *
+ * It replaces the host interface of taillefu/cudacode, whose functions all
+ * return void, print and exit() on error, and keep their state in a
+ * `std::vector<dev>`. Here every call returns an int status (PYRO_OK or a
+ * negative PYRO_ERR_* code, with a message from pyro_last_error()), all device
+ * state lives in an opaque pyro_ctx (one per GPU), and the caller owns every
+ * host array it passes. Calls are stream-ordered on the context's stream and
+ * return without waiting, except those that copy results to host memory.
+ * A context is not thread-safe; use one context per GPU and per thread.
+ *
+ * Spin layout (device and host): per system, per replica, 16 planes (one per
+ * site of the conventional cubic cell, s = 4 f + b with f the FCC corner and b
+ * the pyrochlore sublattice), each plane L^3 cells with cell = (z L + y) L + x;
+ * one float4 (x, y, z, 0) per spin.
+ */
+#ifndef PYRO_H
+#define PYRO_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PYRO_OK 0
+#define PYRO_ERR_ARG -1      /* invalid argument or configuration        */
+#define PYRO_ERR_CUDA -2     /* a CUDA runtime call failed               */
+#define PYRO_ERR_TIMEOUT -3  /* a bounded device wait ran out            */
+#define PYRO_ERR_NAN -4      /* non-finite or non-unit spins detected    */
+#define PYRO_ERR_IO -5       /* checkpoint file missing, short or corrupt */
+#define PYRO_ERR_STATE -6    /* call not valid in the current state       */
+#define PYRO_ERR_NOMEM -7    /* device allocation failed                 */
+
+/* One lattice with its own size, couplings and temperature ladder. */
+typedef struct {
+  int L;                      /* cubic cells per edge (>= 2)                       */
+  int n_replicas;             /* replicas held by this context                     */
+  int replica_offset;         /* global index of the first one (sharding over GPUs) */
+  int n_temperatures;         /* full ladder size; == n_replicas when not sharded   */
+  const double* temperatures; /* n_temperatures values, strictly increasing          */
+  double J1;                  /* nearest neighbour (distance sqrt(2)/4 a)            */
+  double J2;                  /* second neighbour (sqrt(6)/4 a)                      */
+  double J3;                  /* third neighbour through a site (sqrt(2)/2 a, J3a)   */
+  double J3b;                 /* third neighbour across a hexagon (sqrt(2)/2 a)      */
+} pyro_system_desc;
+
+typedef struct {
+  int n_systems;
+  const pyro_system_desc* systems;
+  uint64_t seed;     /* Philox key; all randomness is a function of (seed, counters) */
+  int device;        /* CUDA device ordinal                                         */
+  int renorm_every;  /* renormalise spins every this many sweeps (0 = never)        */
+} pyro_config;
+
+typedef struct pyro_ctx pyro_ctx;
+
+/* Context life cycle. Replaces InitializeDevice + InitializeCouplings3D
+ * (Pyrochlore.cu:643-711, 1251-1267). */
+int pyro_create(const pyro_config* cfg, pyro_ctx** out);
+int pyro_destroy(pyro_ctx* ctx);
+const char* pyro_last_error(const pyro_ctx* ctx);
+int pyro_version(void);
+/* Host-only: the neighbour table of cubic-cell site `site` (0..15) in the
+ * canonical order (J1 6, J2 12, J3a 6, J3b 6): out[4k..4k+3] = dx, dy, dz,
+ * target site. Replaces the packed links16 table of InitializeCouplings3D
+ * (Pyrochlore.cu:152-167, 643-711). Needs no GPU. */
+int pyro_neighbour_table(int site, int* out120);
+
+/* Stream used by every call (default: a stream the context creates). */
+int pyro_set_stream(pyro_ctx* ctx, void* cuda_stream);
+void* pyro_get_stream(const pyro_ctx* ctx);
+/* Wait for all work queued by the context. Replaces SynchronizeJobs
+ * (MonteCarlo.cu:230-245). */
+int pyro_synchronize(pyro_ctx* ctx);
+
+/* Sizes of one system, and the number of colour classes its sweep uses
+ * (4 for J1 only, 16 when J2/J3 are present). */
+int pyro_system_info(const pyro_ctx* ctx, int system, int* L, int* n_sites,
+                     int* n_replicas, int* n_colours);
+
+/* Spins. Uniform random unit vectors from Philox(seed; site, replica):
+ * replaces GenerateRandomVectorsOnDevice / Generate3DVectorList
+ * (MonteCarlo.cu:257-293, Math.cu:132-143). set/get copy one system's
+ * replicas in the float4 layout above; replace the configuration transfers
+ * of Save/ReadConfigurations (Math.cu:618-701). */
+int pyro_init_random(pyro_ctx* ctx);
+int pyro_set_spins(pyro_ctx* ctx, int system, const float* host_xyzw);
+int pyro_get_spins(pyro_ctx* ctx, int system, float* host_xyzw);
+/* Device-pointer variants (stream-ordered; the pointer must hold one system). */
+int pyro_set_spins_device(pyro_ctx* ctx, int system, const float* dev_xyzw);
+int pyro_get_spins_device(pyro_ctx* ctx, int system, float* dev_xyzw);
+
+/* Plain method. One sweep = every colour class in order, each updated in
+ * one pass. Metropolis uses a cone proposal of half-angle acos(cosmax[t]) of
+ * the replica's temperature slot t. Replaces Mc / MCMultipleTemperaturesPerSystem
+ * (Pyrochlore.cu:74-133, 829-885) and OverRelaxationByPiStep (975-1007). */
+int pyro_metropolis_sweep(pyro_ctx* ctx, int n_sweeps);
+int pyro_overrelax_sweep(pyro_ctx* ctx, int n_sweeps);
+
+/* Cone widths (cos of the half-angle) per temperature slot of one system,
+ * and acceptance counts since the last reset. Replace CosThetaSolid and
+ * CalculateRatio (MonteCarlo.cu:346-367). */
+int pyro_set_cone(pyro_ctx* ctx, int system, const float* cosmax);
+int pyro_get_cone(pyro_ctx* ctx, int system, float* cosmax);
+int pyro_get_acceptance(pyro_ctx* ctx, int system, uint64_t* accepted, uint64_t* proposed);
+int pyro_reset_acceptance(pyro_ctx* ctx);
+/* Adapt each temperature's cone to `target` acceptance with `iterations`
+ * rounds of `sweeps_per_iteration` Metropolis sweeps (+ n_or over-relaxation
+ * sweeps each). Replaces CalculateSolidAngle (MonteCarlo.cu:371-426). */
+int pyro_tune_cone(pyro_ctx* ctx, double target, int iterations, int sweeps_per_iteration,
+                   int n_or);
+
+/* FP64 energy and magnetisation per replica of one system (replica order,
+ * i.e. configuration slots, not temperature order). Synchronous. Replaces
+ * TotalEnergyv2 (Math.cu:309-330) and Magnetization (Pyrochlore.cu:453-466). */
+int pyro_observables(pyro_ctx* ctx, int system, double* energy, double* magnetisation3);
+/* Stream-ordered variant into device buffers (n_replicas and 3 n_replicas). */
+int pyro_observables_device(pyro_ctx* ctx, int system, double* dev_energy,
+                            double* dev_magnetisation3);
+
+/* Temperatures. temperature_of_replica: T of each configuration slot (the
+ * reference's permuted `Temperatures` vector); replica_of_temperature: the
+ * inverse map. Global indices (all n_temperatures entries). */
+int pyro_get_temperatures(pyro_ctx* ctx, int system, double* temperature_of_replica);
+int pyro_get_permutation(pyro_ctx* ctx, int system, int* replica_of_temperature);
+
+/* Replica exchange between neighbouring temperatures (pairs (t, t+1) with
+ * t % 2 == parity), FP64 test, Philox(seed; pair, swap count). The temperature
+ * labels move, spins stay. Replaces TrySwapingTemperatures
+ * (MonteCarlo.cu:105-172). parity < 0 alternates automatically.
+ * n_accepted may be NULL (then the call does not synchronise). */
+int pyro_pt_swap(pyro_ctx* ctx, int parity, int* n_accepted);
+/* Sharded form: energies of ALL n_temperatures replicas of `system` (global
+ * replica order, device memory), gathered by the caller across GPUs. Every
+ * rank applies the identical decision. */
+int pyro_pt_swap_global(pyro_ctx* ctx, int system, const double* dev_energy_all, int parity);
+int pyro_get_swap_stats(pyro_ctx* ctx, int system, uint64_t* accepted, uint64_t* attempted);
+
+/* One or more cycles of n_metro Metropolis + n_or over-relaxation sweeps,
+ * energy, and (if do_swap) a replica exchange of alternating parity, replayed
+ * from a CUDA graph. Replaces ParallelTempering (MonteCarlo.cu:429-470).
+ * If a history buffer is enabled, each cycle appends the energy of every
+ * temperature slot. */
+int pyro_cycle(pyro_ctx* ctx, int n_metro, int n_or, int do_swap, int n_cycles);
+int pyro_enable_history(pyro_ctx* ctx, int capacity_cycles);
+/* Copies min(capacity, recorded) cycles of system `system`: out[c * n_temperatures + t]. */
+int pyro_get_history(pyro_ctx* ctx, int system, double* out, int* n_cycles);
+
+/* Counters: sweeps done so far (all systems advance together). */
+int pyro_get_sweep_count(pyro_ctx* ctx, uint64_t* sweeps);
+
+/* Check that every spin is finite with |S|^2 within tol of 1; returns
+ * PYRO_ERR_NAN and the first bad spin index otherwise. */
+int pyro_check_spins(pyro_ctx* ctx, float tol, long long* first_bad);
+
+/* Static structure factor S(q) = (1/N) sum_a |sum_i S_i^a e^{-i q.r_i}|^2,
+ * averaged over the replicas held, on a grid of G^3 wave vectors
+ * q = (2 pi / L) * stride * (h, k, l), h, k, l in [-G/2, G/2); out[(h' G + k') G + l'].
+ * One replica `replica` (>= 0) or all (-1). Replaces the cuFFT-based
+ * StructFactor path (Math.cu:721-741, Pyrochlore.cu:1303-1419). */
+int pyro_structure_factor(pyro_ctx* ctx, int system, int replica, int G, int stride, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PYRO_H */

@@ -1,0 +1,654 @@
+// ORACLE — test infrastructure only. Nothing in the engine links or calls
+// this file; tests/, the smoke check and the CPU-baseline leg of the
+// benchmark use it as the checker.
+//
+// A plain C++/OpenMP restatement of the pyrochlore Heisenberg Monte Carlo of
+// taillefu/cudacode with the engine's update order and Philox streams:
+//   energy convention and periodic neighbour arithmetic  Pyrochlore.cu:468-523 (TotalEnergy)
+//   site positions                                       Pyrochlore.cu:1339-1401
+//   sublattice colour classes                            Pyrochlore.cu:36-43
+//   sphere sampling                                      Math.cu:120-130
+//   cone proposal                                        Math.cu:244-281
+//   Metropolis rule                                      Math.cu:968-986
+//   over-relaxation S -> 2(S.h)h/|h|^2 - S               Math.cu:220-242
+//   replica exchange min(1, exp((b1-b2)(E1-E2)))         MonteCarlo.cu:105-172
+//   cone-width adaptation                                MonteCarlo.cu:371-426
+// Units: unit classical spins, H = J1 sum_<ij> S_i.S_j (+ J2, J3a, J3b shells).
+// The reference's TotalEnergy equals this energy times S^2 = 1/4 when its
+// J1 = J2 = J and J3 = J4 = 0 (couplings_const, Pyrochlore.cu:169-184).
+//
+// The reference itself cannot serve: its glue files (functions.h, reduce.cu,
+// Device.cu, Measure.hpp, StructFactor.hpp, Utils.hpp) are absent and it needs
+// MKL, GSL and popt, none of which exist here.
+//
+// Two precisions:
+//  * float: every update uses the functions of include/pyro_math.h, so the
+//    result is bit-identical to the CUDA kernels for any number of sweeps.
+//  * double: spins, fields and updates in FP64 with libm functions and the
+//    same Philox words; the "FP64 host run" for statistical comparisons.
+//
+// Geometry is derived independently of the engine's per-cell table: every
+// site gets real-space coordinates (units a/4) and its neighbours are found by
+// enumerating the displacement vectors of each distance shell and looking the
+// target up by coordinates; they are then put in the canonical order (shell,
+// target site of the cell, dx, dy, dz).
+#include <omp.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../include/pyro_math.h"
+
+namespace {
+
+const int kShellBegin[5] = {0, 6, 18, 24, 30};
+
+void pos4(int s, int p[3]) {
+  // FCC corners F and basis F/2 of the 16-site cubic cell (Pyrochlore.cu:1339-1401).
+  static const int F[4][3] = {{0, 0, 0}, {2, 2, 0}, {0, 2, 2}, {2, 0, 2}};
+  for (int k = 0; k < 3; ++k) p[k] = F[s / 4][k] + F[s % 4][k] / 2;
+}
+
+// site-in-cell id from coordinates mod 4 (units a/4), or -1.
+int site_at(int x, int y, int z) {
+  x &= 3;
+  y &= 3;
+  z &= 3;
+  for (int s = 0; s < 16; ++s) {
+    int p[3];
+    pos4(s, p);
+    if (p[0] == x && p[1] == y && p[2] == z) return s;
+  }
+  return -1;
+}
+
+struct Nbr {
+  int dx, dy, dz, t;
+};
+
+// nb[s][k], k in canonical order.
+std::array<std::array<Nbr, 30>, 16> build_geometry() {
+  std::array<std::array<Nbr, 30>, 16> nb;
+  for (int s = 0; s < 16; ++s) {
+    int p[3];
+    pos4(s, p);
+    struct C {
+      int shell, t, dx, dy, dz;
+    };
+    std::vector<C> c;
+    for (int vx = -3; vx <= 3; ++vx)
+      for (int vy = -3; vy <= 3; ++vy)
+        for (int vz = -3; vz <= 3; ++vz) {
+          const int r2 = vx * vx + vy * vy + vz * vz;
+          if (r2 != 2 && r2 != 6 && r2 != 8) continue;
+          const int q[3] = {p[0] + vx, p[1] + vy, p[2] + vz};
+          const int t = site_at(q[0], q[1], q[2]);
+          if (t < 0) continue;
+          int shell = r2 == 2 ? 0 : r2 == 6 ? 1 : 3;
+          if (r2 == 8 && (vx % 2 == 0) && (vy % 2 == 0) && (vz % 2 == 0)) {
+            // through a site: the midpoint is itself a site one J1 bond away
+            if (site_at(p[0] + vx / 2, p[1] + vy / 2, p[2] + vz / 2) >= 0) shell = 2;
+          }
+          auto fdiv = [](int a) { return a >= 0 ? a / 4 : -((-a + 3) / 4); };
+          c.push_back({shell, t, fdiv(q[0]), fdiv(q[1]), fdiv(q[2])});
+        }
+    std::sort(c.begin(), c.end(), [](const C& a, const C& b) {
+      if (a.shell != b.shell) return a.shell < b.shell;
+      if (a.t != b.t) return a.t < b.t;
+      if (a.dx != b.dx) return a.dx < b.dx;
+      if (a.dy != b.dy) return a.dy < b.dy;
+      return a.dz < b.dz;
+    });
+    if (c.size() != 30) {
+      fprintf(stderr, "oracle geometry: site %d has %zu neighbours\n", s, c.size());
+      std::abort();
+    }
+    for (int k = 0; k < 30; ++k) nb[s][k] = {c[k].dx, c[k].dy, c[k].dz, c[k].t};
+  }
+  return nb;
+}
+
+struct Sys {
+  int L, L3, R, off, nT, n_colours, temp_base, rep_key, shells;
+  double J[4];
+  std::vector<double> T;
+  size_t spin_off;  // in spins
+};
+
+struct Oracle {
+  bool fp64 = false;
+  uint64_t seed = 0;
+  int renorm_every = 0;
+  std::array<std::array<Nbr, 30>, 16> nb;
+  std::vector<Sys> sys;
+  std::vector<float> s32;   // 4 per spin
+  std::vector<double> s64;  // 4 per spin
+  std::vector<int> temp_of_rep, rep_of_temp;  // [temp_base + g], [temp_base + t]
+  std::vector<float> cosmax;
+  std::vector<uint64_t> accepted, swap_acc, swap_try;
+  std::vector<uint64_t> swap_count;
+  uint64_t sweep = 0;
+  uint64_t metro_since_reset = 0;
+  int total_temps = 0;
+};
+
+inline int wrap(int v, int L) { return v < 0 ? v + L : (v >= L ? v - L : v); }
+
+inline size_t nbr_index(const Sys& S, const Nbr& e, int x, int y, int z) {
+  return (size_t)e.t * S.L3 +
+         (size_t)((wrap(z + e.dz, S.L) * S.L + wrap(y + e.dy, S.L)) * S.L + wrap(x + e.dx, S.L));
+}
+
+// FP32 local field, summed in canonical order; identical arithmetic to the kernel.
+pyro_vec3 field32(const Oracle& o, const Sys& S, const float* rep, int s, int x, int y, int z) {
+  // The J1 shell is always summed (h = J1 * a1); further shells only when
+  // their coupling is non-zero, each folded in with one fused multiply-add.
+  const float Jf[4] = {(float)S.J[0], (float)S.J[1], (float)S.J[2], (float)S.J[3]};
+  pyro_vec3 h = {0.f, 0.f, 0.f};
+  for (int sh = 0; sh < 4; ++sh) {
+    if (sh > 0 && !(S.shells & (1 << sh))) continue;
+    const int k0 = kShellBegin[sh];
+    const float* v0 = rep + 4 * nbr_index(S, o.nb[s][k0], x, y, z);
+    float ax = v0[0], ay = v0[1], az = v0[2];
+    for (int k = k0 + 1; k < kShellBegin[sh + 1]; ++k) {
+      const float* v = rep + 4 * nbr_index(S, o.nb[s][k], x, y, z);
+      ax = ax + v[0];
+      ay = ay + v[1];
+      az = az + v[2];
+    }
+    if (sh == 0) {
+      h.x = Jf[0] * ax;
+      h.y = Jf[0] * ay;
+      h.z = Jf[0] * az;
+    } else {
+      h.x = fmaf(Jf[sh], ax, h.x);
+      h.y = fmaf(Jf[sh], ay, h.y);
+      h.z = fmaf(Jf[sh], az, h.z);
+    }
+  }
+  return h;
+}
+
+struct V3d {
+  double x, y, z;
+};
+
+V3d field64(const Oracle& o, const Sys& S, const double* rep, int s, int x, int y, int z) {
+  V3d h = {0, 0, 0};
+  for (int sh = 0; sh < 4; ++sh) {
+    if (!(S.shells & (1 << sh))) continue;
+    double ax = 0, ay = 0, az = 0;
+    for (int k = kShellBegin[sh]; k < kShellBegin[sh + 1]; ++k) {
+      const double* v = rep + 4 * nbr_index(S, o.nb[s][k], x, y, z);
+      ax += v[0];
+      ay += v[1];
+      az += v[2];
+    }
+    h.x += S.J[sh] * ax;
+    h.y += S.J[sh] * ay;
+    h.z += S.J[sh] * az;
+  }
+  return h;
+}
+
+// FP64 field from FP32 spins (observables of the FP32 chain).
+V3d field64f(const Oracle& o, const Sys& S, const float* rep, int s, int x, int y, int z) {
+  V3d h = {0, 0, 0};
+  for (int sh = 0; sh < 4; ++sh) {
+    if (!(S.shells & (1 << sh))) continue;
+    double ax = 0, ay = 0, az = 0;
+    for (int k = kShellBegin[sh]; k < kShellBegin[sh + 1]; ++k) {
+      const float* v = rep + 4 * nbr_index(S, o.nb[s][k], x, y, z);
+      ax += v[0];
+      ay += v[1];
+      az += v[2];
+    }
+    h.x += S.J[sh] * ax;
+    h.y += S.J[sh] * ay;
+    h.z += S.J[sh] * az;
+  }
+  return h;
+}
+
+int colour_site(int n_colours, int colour, int k) { return n_colours == 4 ? 4 * k + colour : colour; }
+
+void sweep_one(Oracle& o, bool metro) {
+  const uint64_t sweep = o.sweep;
+  const bool renorm = o.renorm_every > 0 && ((sweep + 1) % (uint64_t)o.renorm_every) == 0;
+  int max_col = 4;
+  for (auto& S : o.sys) max_col = std::max(max_col, S.n_colours);
+  for (int pass = 0; pass < max_col; ++pass) {
+    for (size_t si = 0; si < o.sys.size(); ++si) {
+      Sys& S = o.sys[si];
+      int colour = -1;
+      if (S.n_colours == max_col) colour = pass;
+      else if (pass % 4 == 0) colour = pass / 4;
+      if (colour < 0) continue;
+      const int per_col = 16 * S.L3 / S.n_colours;
+      const long long total = (long long)S.R * per_col;
+      std::vector<uint64_t> acc_rep(S.R, 0);
+#pragma omp parallel
+      {
+        std::vector<uint64_t> acc_local(S.R, 0);
+#pragma omp for schedule(static)
+        for (long long w = 0; w < total; ++w) {
+          const int r = (int)(w / per_col);
+          const int u = (int)(w - (long long)r * per_col);
+          const int k = u / S.L3, cell = u - k * S.L3;
+          const int s = colour_site(S.n_colours, colour, k);
+          const int x = cell % S.L, y = (cell / S.L) % S.L, z = cell / (S.L * S.L);
+          const size_t own = (size_t)s * S.L3 + cell;
+          const int g = S.off + r;
+          const int t = o.temp_of_rep[S.temp_base + g];
+          uint32_t rr[4] = {0, 0, 0, 0};
+          if (metro)
+            pyro_philox((uint32_t)own, (uint32_t)(S.rep_key + r), (uint32_t)sweep, PYRO_PURPOSE_METRO,
+                        (uint32_t)(o.seed & 0xffffffffu), (uint32_t)(o.seed >> 32), rr);
+          if (!o.fp64) {
+            float* rep = o.s32.data() + 4 * (S.spin_off + (size_t)r * 16 * S.L3);
+            const pyro_vec3 h = field32(o, S, rep, s, x, y, z);
+            pyro_vec3 sp = {rep[4 * own], rep[4 * own + 1], rep[4 * own + 2]};
+            pyro_vec3 out;
+            if (metro) {
+              const float beta = (float)(1.0 / S.T[t]);
+              const pyro_vec3 prop = pyro_cone_proposal(sp, o.cosmax[S.temp_base + t],
+                                                        pyro_uniform(rr[0]), pyro_uniform(rr[1]));
+              const float dE = pyro_delta_e(h, sp, prop);
+              const int a = pyro_metropolis_accept(dE, beta, pyro_uniform(rr[2]));
+              acc_local[r] += (uint64_t)a;
+              out = a ? prop : sp;
+            } else {
+              out = pyro_overrelax(sp, h);
+            }
+            if (renorm) out = pyro_renormalise(out);
+            rep[4 * own] = out.x;
+            rep[4 * own + 1] = out.y;
+            rep[4 * own + 2] = out.z;
+            rep[4 * own + 3] = 0.0f;
+          } else {
+            double* rep = o.s64.data() + 4 * (S.spin_off + (size_t)r * 16 * S.L3);
+            const V3d h = field64(o, S, rep, s, x, y, z);
+            V3d sp = {rep[4 * own], rep[4 * own + 1], rep[4 * own + 2]};
+            V3d out = sp;
+            if (metro) {
+              const double beta = 1.0 / S.T[t];
+              const double c0 = o.cosmax[S.temp_base + t];
+              const double u1 = pyro_uniform(rr[0]), u2 = pyro_uniform(rr[1]);
+              const double ct = 1.0 - (1.0 - c0) * u1;
+              const double st = std::sqrt(std::max(0.0, 1.0 - ct * ct));
+              const double ph = 2.0 * M_PI * u2;
+              const double cp = std::cos(ph), spp = std::sin(ph);
+              const double sgn = std::copysign(1.0, sp.z);
+              const double aa = -1.0 / (sgn + sp.z);
+              const double bb = sp.x * sp.y * aa;
+              const V3d e1 = {1.0 + sgn * sp.x * sp.x * aa, sgn * bb, -sgn * sp.x};
+              const V3d e2 = {bb, sgn + sp.y * sp.y * aa, -sp.y};
+              const V3d prop = {st * cp * e1.x + st * spp * e2.x + ct * sp.x,
+                                st * cp * e1.y + st * spp * e2.y + ct * sp.y,
+                                st * cp * e1.z + st * spp * e2.z + ct * sp.z};
+              const double dE =
+                  h.x * (prop.x - sp.x) + h.y * (prop.y - sp.y) + h.z * (prop.z - sp.z);
+              const int a = dE <= 0.0 || (double)pyro_uniform(rr[2]) < std::exp(-beta * dE);
+              acc_local[r] += (uint64_t)a;
+              out = a ? prop : sp;
+            } else {
+              const double hh = h.x * h.x + h.y * h.y + h.z * h.z;
+              if (hh > 0.0) {
+                const double k2 = 2.0 * (sp.x * h.x + sp.y * h.y + sp.z * h.z) / hh;
+                out = {k2 * h.x - sp.x, k2 * h.y - sp.y, k2 * h.z - sp.z};
+              }
+            }
+            if (renorm) {
+              const double n = std::sqrt(out.x * out.x + out.y * out.y + out.z * out.z);
+              out = {out.x / n, out.y / n, out.z / n};
+            }
+            rep[4 * own] = out.x;
+            rep[4 * own + 1] = out.y;
+            rep[4 * own + 2] = out.z;
+            rep[4 * own + 3] = 0.0;
+          }
+        }
+#pragma omp critical
+        for (int r = 0; r < S.R; ++r) acc_rep[r] += acc_local[r];
+      }
+      if (metro)
+        for (int r = 0; r < S.R; ++r)
+          o.accepted[S.temp_base + o.temp_of_rep[S.temp_base + S.off + r]] += acc_rep[r];
+    }
+  }
+  o.sweep += 1;
+  if (metro) o.metro_since_reset += 1;
+}
+
+void observables(const Oracle& o, int si, std::vector<double>* E, std::vector<double>* M) {
+  const Sys& S = o.sys[si];
+  E->assign(S.R, 0.0);
+  M->assign(3 * S.R, 0.0);
+  for (int r = 0; r < S.R; ++r) {
+    double e = 0, mx = 0, my = 0, mz = 0;
+    const size_t base = S.spin_off + (size_t)r * 16 * S.L3;
+#pragma omp parallel for reduction(+ : e, mx, my, mz) schedule(static)
+    for (long long i = 0; i < 16ll * S.L3; ++i) {
+      const int s = (int)(i / S.L3), cell = (int)(i % S.L3);
+      const int x = cell % S.L, y = (cell / S.L) % S.L, z = cell / (S.L * S.L);
+      double sx, sy, sz;
+      V3d h;
+      if (!o.fp64) {
+        const float* rep = o.s32.data() + 4 * base;
+        sx = rep[4 * i];
+        sy = rep[4 * i + 1];
+        sz = rep[4 * i + 2];
+        h = field64f(o, S, rep, s, x, y, z);
+      } else {
+        const double* rep = o.s64.data() + 4 * base;
+        sx = rep[4 * i];
+        sy = rep[4 * i + 1];
+        sz = rep[4 * i + 2];
+        h = field64(o, S, rep, s, x, y, z);
+      }
+      e += sx * h.x + sy * h.y + sz * h.z;
+      mx += sx;
+      my += sy;
+      mz += sz;
+    }
+    (*E)[r] = 0.5 * e;
+    (*M)[3 * r] = mx;
+    (*M)[3 * r + 1] = my;
+    (*M)[3 * r + 2] = mz;
+  }
+}
+
+// Replica exchange on one system given energies by global replica.
+int exchange(Oracle& o, int si, const double* E_global, int parity) {
+  Sys& S = o.sys[si];
+  const uint64_t count = o.swap_count[si];
+  if (parity < 0) parity = (int)(count & 1u);
+  int n_acc = 0;
+  for (int t = parity; t + 1 < S.nT; t += 2) {
+    const int ga = o.rep_of_temp[S.temp_base + t], gb = o.rep_of_temp[S.temp_base + t + 1];
+    uint32_t r[4];
+    pyro_philox((uint32_t)t, (uint32_t)count, (uint32_t)si, PYRO_PURPOSE_SWAP,
+                (uint32_t)(o.seed & 0xffffffffu), (uint32_t)(o.seed >> 32), r);
+    const double u = pyro_uniform53(r[0], r[1]);
+    const int acc = pyro_swap_accept(1.0 / S.T[t], 1.0 / S.T[t + 1], E_global[ga], E_global[gb], u);
+    o.swap_try[S.temp_base + t]++;
+    if (acc) {
+      o.rep_of_temp[S.temp_base + t] = gb;
+      o.rep_of_temp[S.temp_base + t + 1] = ga;
+      o.temp_of_rep[S.temp_base + ga] = t + 1;
+      o.temp_of_rep[S.temp_base + gb] = t;
+      o.swap_acc[S.temp_base + t]++;
+      ++n_acc;
+    }
+  }
+  o.swap_count[si] = count + 1;
+  return n_acc;
+}
+
+}  // namespace
+
+extern "C" {
+
+void* orc_create(int n_sys, const int* L, const int* n_rep, const int* rep_off, const int* n_temp,
+                 const double* temps_concat, const double* J4, uint64_t seed, int renorm_every,
+                 int fp64) {
+  Oracle* o = new Oracle();
+  o->fp64 = fp64 != 0;
+  o->seed = seed;
+  o->renorm_every = renorm_every;
+  o->nb = build_geometry();
+  size_t spin_off = 0;
+  int tb = 0;
+  for (int i = 0; i < n_sys; ++i) {
+    Sys S;
+    S.L = L[i];
+    S.L3 = L[i] * L[i] * L[i];
+    S.R = n_rep[i];
+    S.off = rep_off[i];
+    S.nT = n_temp[i];
+    for (int k = 0; k < 4; ++k) S.J[k] = J4[4 * i + k];
+    S.shells = 0;
+    for (int k = 0; k < 4; ++k)
+      if (S.J[k] != 0.0) S.shells |= 1 << k;
+    S.n_colours = (S.J[1] != 0.0 || S.J[2] != 0.0 || S.J[3] != 0.0) ? 16 : 4;
+    S.T.assign(temps_concat + tb, temps_concat + tb + S.nT);
+    S.temp_base = tb;
+    S.rep_key = tb + S.off;
+    S.spin_off = spin_off;
+    spin_off += (size_t)S.R * 16 * S.L3;
+    for (int t = 0; t < S.nT; ++t) {
+      o->temp_of_rep.push_back(t);
+      o->rep_of_temp.push_back(t);
+      o->cosmax.push_back(-1.0f);
+      o->accepted.push_back(0);
+      o->swap_acc.push_back(0);
+      o->swap_try.push_back(0);
+    }
+    o->swap_count.push_back(0);
+    tb += S.nT;
+    o->sys.push_back(S);
+  }
+  o->total_temps = tb;
+  if (o->fp64) o->s64.assign(4 * spin_off, 0.0);
+  else o->s32.assign(4 * spin_off, 0.0f);
+  return o;
+}
+
+void orc_destroy(void* p) { delete (Oracle*)p; }
+
+int orc_set_threads(int n) {
+  if (n > 0) omp_set_num_threads(n);
+  return omp_get_max_threads();
+}
+
+void orc_init_random(void* p) {
+  Oracle& o = *(Oracle*)p;
+  for (auto& S : o.sys) {
+    const long long n = (long long)S.R * 16 * S.L3;
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < n; ++i) {
+      const int r = (int)(i / (16ll * S.L3));
+      const int site = (int)(i % (16ll * S.L3));
+      uint32_t rr[4];
+      pyro_philox((uint32_t)site, (uint32_t)(S.rep_key + r), 0u, PYRO_PURPOSE_INIT,
+                  (uint32_t)(o.seed & 0xffffffffu), (uint32_t)(o.seed >> 32), rr);
+      const pyro_vec3 v = pyro_sphere_point(pyro_uniform(rr[0]), pyro_uniform(rr[1]));
+      const size_t j = 4 * (S.spin_off + (size_t)i);
+      if (o.fp64) {
+        o.s64[j] = v.x;
+        o.s64[j + 1] = v.y;
+        o.s64[j + 2] = v.z;
+        o.s64[j + 3] = 0.0;
+      } else {
+        o.s32[j] = v.x;
+        o.s32[j + 1] = v.y;
+        o.s32[j + 2] = v.z;
+        o.s32[j + 3] = 0.0f;
+      }
+    }
+  }
+}
+
+long long orc_n_spins(void* p, int si) {
+  Oracle& o = *(Oracle*)p;
+  const Sys& S = o.sys[si];
+  return (long long)S.R * 16 * S.L3;
+}
+
+void orc_set_spins(void* p, int si, const float* xyzw) {
+  Oracle& o = *(Oracle*)p;
+  const Sys& S = o.sys[si];
+  const size_t n = 4 * (size_t)S.R * 16 * S.L3;
+  for (size_t i = 0; i < n; ++i) {
+    if (o.fp64) o.s64[4 * S.spin_off + i] = xyzw[i];
+    else o.s32[4 * S.spin_off + i] = xyzw[i];
+  }
+}
+
+void orc_get_spins(void* p, int si, float* xyzw) {
+  Oracle& o = *(Oracle*)p;
+  const Sys& S = o.sys[si];
+  const size_t n = 4 * (size_t)S.R * 16 * S.L3;
+  for (size_t i = 0; i < n; ++i)
+    xyzw[i] = o.fp64 ? (float)o.s64[4 * S.spin_off + i] : o.s32[4 * S.spin_off + i];
+}
+
+void orc_get_spins64(void* p, int si, double* xyzw) {
+  Oracle& o = *(Oracle*)p;
+  const Sys& S = o.sys[si];
+  const size_t n = 4 * (size_t)S.R * 16 * S.L3;
+  for (size_t i = 0; i < n; ++i)
+    xyzw[i] = o.fp64 ? o.s64[4 * S.spin_off + i] : (double)o.s32[4 * S.spin_off + i];
+}
+
+void orc_metropolis_sweep(void* p, int n) {
+  for (int i = 0; i < n; ++i) sweep_one(*(Oracle*)p, true);
+}
+
+void orc_overrelax_sweep(void* p, int n) {
+  for (int i = 0; i < n; ++i) sweep_one(*(Oracle*)p, false);
+}
+
+void orc_set_cone(void* p, int si, const float* c) {
+  Oracle& o = *(Oracle*)p;
+  const Sys& S = o.sys[si];
+  for (int t = 0; t < S.nT; ++t) o.cosmax[S.temp_base + t] = c[t];
+}
+
+void orc_get_cone(void* p, int si, float* c) {
+  Oracle& o = *(Oracle*)p;
+  const Sys& S = o.sys[si];
+  for (int t = 0; t < S.nT; ++t) c[t] = o.cosmax[S.temp_base + t];
+}
+
+void orc_get_acceptance(void* p, int si, uint64_t* acc, uint64_t* prop) {
+  Oracle& o = *(Oracle*)p;
+  const Sys& S = o.sys[si];
+  for (int t = 0; t < S.nT; ++t) {
+    acc[t] = o.accepted[S.temp_base + t];
+    if (prop) prop[t] = (uint64_t)16 * S.L3 * o.metro_since_reset;
+  }
+}
+
+void orc_reset_acceptance(void* p) {
+  Oracle& o = *(Oracle*)p;
+  std::fill(o.accepted.begin(), o.accepted.end(), 0);
+  o.metro_since_reset = 0;
+}
+
+// Same adaptation rule as the engine's pyro_tune_cone.
+void orc_tune_cone(void* p, double target, int iterations, int sweeps_per_iteration, int n_or) {
+  Oracle& o = *(Oracle*)p;
+  for (int it = 0; it < iterations; ++it) {
+    orc_reset_acceptance(p);
+    for (int k = 0; k < sweeps_per_iteration; ++k) {
+      sweep_one(o, true);
+      for (int j = 0; j < n_or; ++j) sweep_one(o, false);
+    }
+    bool done = true;
+    for (auto& S : o.sys) {
+      for (int t = 0; t < S.nT; ++t) {
+        const double prop = (double)16 * S.L3 * o.metro_since_reset;
+        const double ratio = prop > 0 ? (double)o.accepted[S.temp_base + t] / prop : target;
+        if (std::fabs(ratio - target) > 0.02) done = false;
+        double theta =
+            std::acos(std::max(-1.0, std::min(1.0, (double)o.cosmax[S.temp_base + t])));
+        const double f = std::max(0.5, std::min(2.0, ratio / target));
+        theta = std::max(1e-4, std::min(M_PI, theta * f));
+        float c = (float)std::cos(theta);
+        if (c >= 1.0f) c = std::nextafter(1.0f, 0.0f);
+        if (c < -1.0f) c = -1.0f;
+        o.cosmax[S.temp_base + t] = c;
+      }
+    }
+    if (done) break;
+  }
+  orc_reset_acceptance(p);
+}
+
+void orc_observables(void* p, int si, double* E, double* M3) {
+  std::vector<double> e, m;
+  observables(*(Oracle*)p, si, &e, &m);
+  std::memcpy(E, e.data(), sizeof(double) * e.size());
+  if (M3) std::memcpy(M3, m.data(), sizeof(double) * m.size());
+}
+
+// Unsharded exchange on every system, energies computed here.
+int orc_pt_swap(void* p, int parity) {
+  Oracle& o = *(Oracle*)p;
+  int n = 0;
+  for (size_t si = 0; si < o.sys.size(); ++si) {
+    std::vector<double> e, m;
+    observables(o, (int)si, &e, &m);
+    n += exchange(o, (int)si, e.data(), parity);
+  }
+  return n;
+}
+
+int orc_pt_swap_global(void* p, int si, const double* E_all, int parity) {
+  return exchange(*(Oracle*)p, si, E_all, parity);
+}
+
+// n_cycles of (n_metro M + n_or OR sweeps, energies, optional exchange of
+// alternating parity). history (optional): [cycle][total_temps], E by slot.
+void orc_cycle(void* p, int n_metro, int n_or, int do_swap, int n_cycles, double* history) {
+  Oracle& o = *(Oracle*)p;
+  for (int c = 0; c < n_cycles; ++c) {
+    for (int i = 0; i < n_metro; ++i) sweep_one(o, true);
+    for (int i = 0; i < n_or; ++i) sweep_one(o, false);
+    for (size_t si = 0; si < o.sys.size(); ++si) {
+      Sys& S = o.sys[si];
+      std::vector<double> e, m;
+      observables(o, (int)si, &e, &m);
+      if (history)
+        for (int t = 0; t < S.nT; ++t)
+          history[(size_t)c * o.total_temps + S.temp_base + t] =
+              e[o.rep_of_temp[S.temp_base + t] - S.off];
+      if (do_swap) exchange(o, (int)si, e.data(), -1);
+    }
+  }
+}
+
+void orc_get_permutation(void* p, int si, int* rep_of_temp) {
+  Oracle& o = *(Oracle*)p;
+  const Sys& S = o.sys[si];
+  for (int t = 0; t < S.nT; ++t) rep_of_temp[t] = o.rep_of_temp[S.temp_base + t];
+}
+
+void orc_get_swap_stats(void* p, int si, uint64_t* acc, uint64_t* tried) {
+  Oracle& o = *(Oracle*)p;
+  const Sys& S = o.sys[si];
+  for (int t = 0; t < S.nT; ++t) {
+    acc[t] = o.swap_acc[S.temp_base + t];
+    tried[t] = o.swap_try[S.temp_base + t];
+  }
+}
+
+uint64_t orc_sweep_count(void* p) { return ((Oracle*)p)->sweep; }
+
+// Geometry export: out[k*4 + {0,1,2,3}] = dx, dy, dz, t for k < 30.
+void orc_neighbours(int s, int* out) {
+  static const auto nb = build_geometry();
+  for (int k = 0; k < 30; ++k) {
+    out[4 * k] = nb[s][k].dx;
+    out[4 * k + 1] = nb[s][k].dy;
+    out[4 * k + 2] = nb[s][k].dz;
+    out[4 * k + 3] = nb[s][k].t;
+  }
+}
+
+// Elementary functions of the update contract, for tests on the host.
+void orc_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
+  pyro_philox(ctr[0], ctr[1], ctr[2], ctr[3], key[0], key[1], out);
+}
+float orc_expf(float x) { return pyro_expf(x); }
+float orc_logf(float x) { return pyro_logf(x); }
+void orc_sincospif(float a, float* s, float* c) { pyro_sincospif(a, s, c); }
+double orc_exp64(double x) { return pyro_exp64(x); }
+
+}  // extern "C"

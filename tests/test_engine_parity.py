@@ -1,0 +1,231 @@
+"""GPU parity: the CUDA engine (through the C-ABI) against the host oracle on
+the same seeded inputs. The update arithmetic is specified bit-for-bit
+(include/pyro_math.h), so per-spin agreement is expected to be exact; the
+asserted bound is the 1e-5 per component over the first 100 sweeps that the
+engine promises. FP64 observables differ only by summation order: rel 1e-12."""
+import numpy as np
+import pytest
+
+from cudacode_b200.engine import Engine, PyroError, System, geometric_ladder
+from oracle.binding import Oracle
+
+pytestmark = pytest.mark.gpu
+
+SPIN_TOL = 1e-5
+
+
+def pair(systems, seed=2024, renorm_every=0):
+    e = Engine(systems, seed=seed, renorm_every=renorm_every)
+    o = Oracle(systems, seed=seed, renorm_every=renorm_every)
+    return e, o
+
+
+def assert_spins_equal(e, o, n_sys=1):
+    for k in range(n_sys):
+        a, b = e.get_spins(k), o.get_spins(k)
+        diff = np.abs(a - b).max()
+        assert diff <= SPIN_TOL, (k, diff)
+    return diff
+
+
+def test_init_random_bit_exact():
+    systems = [System(L=4, temperatures=[0.5, 1.0]), System(L=3, temperatures=[1.0], J2=0.1)]
+    e, o = pair(systems)
+    e.init_random()
+    o.init_random()
+    for k in range(2):
+        assert np.array_equal(e.get_spins(k), o.get_spins(k))
+    n = np.linalg.norm(e.get_spins(0)[..., :3], axis=-1)
+    assert np.abs(n - 1).max() < 1e-6
+
+
+@pytest.mark.parametrize("L,R", [(4, 1), (8, 3)])
+def test_plain_sweeps_100_per_spin(L, R):
+    temps = geometric_ladder(0.1, 2.0, R)
+    e, o = pair([System(L=L, temperatures=temps)], renorm_every=7)
+    e.init_random()
+    o.init_random()
+    cones = np.linspace(-0.5, 0.9, R).astype(np.float32)
+    e.set_cone(cones)
+    o.set_cone(cones)
+    for k in range(20):  # 20 x (1 M + 4 OR) = 100 sweeps
+        e.metropolis_sweep(1)
+        o.metropolis_sweep(1)
+        e.overrelax_sweep(4)
+        o.overrelax_sweep(4)
+    a, b = e.get_spins(), o.get_spins()
+    assert np.abs(a - b).max() <= SPIN_TOL
+    assert np.array_equal(a, b), "bit-exact contract"
+    acc_e, prop_e = e.acceptance()
+    acc_o, prop_o = o.acceptance()
+    assert np.array_equal(acc_e, acc_o) and np.array_equal(prop_e, prop_o)
+    assert e.sweep_count() == o.sweep_count() == 100
+
+
+def test_further_neighbour_sixteen_colours():
+    s = System(L=4, temperatures=[0.2, 0.7], J1=1.0, J2=-0.08, J3=0.06, J3b=0.03)
+    e, o = pair([s])
+    assert e.info()["n_colours"] == 16
+    e.init_random()
+    o.init_random()
+    c = np.array([0.3, -0.2], dtype=np.float32)
+    e.set_cone(c)
+    o.set_cone(c)
+    for _ in range(10):
+        e.metropolis_sweep(1)
+        o.metropolis_sweep(1)
+        e.overrelax_sweep(2)
+        o.overrelax_sweep(2)
+    assert np.array_equal(e.get_spins(), o.get_spins())
+
+
+def test_batched_uneven_systems():
+    rng = np.random.default_rng(5)
+    systems = []
+    for L in (3, 4, 5, 4):
+        nT = int(rng.integers(2, 5))
+        j2, j3 = rng.uniform(-0.1, 0.1, 2) if L != 5 else (0.0, 0.0)
+        systems.append(System(L=L, temperatures=geometric_ladder(0.05, 1.5, nT), J2=j2, J3=j3))
+    e, o = pair(systems, renorm_every=5)
+    e.init_random()
+    o.init_random()
+    for k, s in enumerate(systems):
+        c = np.linspace(0.0, 0.8, len(s.temperatures)).astype(np.float32)
+        e.set_cone(c, k)
+        o.set_cone(c, k)
+    for _ in range(6):
+        e.metropolis_sweep(1)
+        o.metropolis_sweep(1)
+        e.overrelax_sweep(2)
+        o.overrelax_sweep(2)
+    for k in range(len(systems)):
+        assert np.array_equal(e.get_spins(k), o.get_spins(k)), k
+
+
+def test_observables_fp64():
+    s = System(L=6, temperatures=[0.3, 0.9, 2.0], J2=0.05, J3=-0.04)
+    e, o = pair([s])
+    e.init_random()
+    o.init_random()
+    e.metropolis_sweep(3)
+    o.metropolis_sweep(3)
+    E1, M1 = e.observables()
+    E2, M2 = o.observables()
+    np.testing.assert_allclose(E1, E2, rtol=1e-12, atol=1e-9)
+    np.testing.assert_allclose(M1, M2, rtol=1e-12, atol=1e-9)
+
+
+def test_parallel_tempering_swaps_match():
+    temps = geometric_ladder(0.05, 2.0, 8)
+    e, o = pair([System(L=4, temperatures=temps)])
+    e.init_random()
+    o.init_random()
+    total = 0
+    for k in range(12):
+        e.metropolis_sweep(1)
+        o.metropolis_sweep(1)
+        e.overrelax_sweep(1)
+        o.overrelax_sweep(1)
+        n1 = e.pt_swap(-1)
+        n2 = o.pt_swap(-1)
+        assert n1 == n2
+        total += n1
+        assert np.array_equal(e.permutation(), o.permutation())
+    assert total > 0
+    assert np.array_equal(e.get_spins(), o.get_spins())
+    T = e.temperatures_of_replicas()
+    assert sorted(T) == pytest.approx(temps)
+
+
+def test_graph_cycle_matches_oracle():
+    temps = geometric_ladder(0.02, 2.0, 6)
+    e, o = pair([System(L=4, temperatures=temps)], renorm_every=10)
+    e.init_random()
+    o.init_random()
+    c = np.linspace(-1.0, 0.95, 6).astype(np.float32)
+    e.set_cone(c)
+    o.set_cone(c)
+    e.enable_history(64)
+    e.cycle(1, 4, True, 20)
+    h_o = o.cycle(1, 4, True, 20, record=True)
+    assert np.array_equal(e.get_spins(), o.get_spins())
+    assert np.array_equal(e.permutation(), o.permutation())
+    h_e = e.history()
+    assert h_e.shape == (20, 6)
+    np.testing.assert_allclose(h_e, h_o, rtol=1e-12, atol=1e-9)
+    assert e.sweep_count() == 100
+
+
+def test_tune_cone_matches_oracle():
+    temps = [0.1, 0.5, 3.0]
+    e, o = pair([System(L=4, temperatures=temps)])
+    e.init_random()
+    o.init_random()
+    e.tune_cone(0.5, 8, 3, 1)
+    o.tune_cone(0.5, 8, 3, 1)
+    assert np.array_equal(e.get_cone(), o.get_cone())
+    assert np.array_equal(e.get_spins(), o.get_spins())
+
+
+def test_sharded_contexts_equal_unsharded():
+    torch = pytest.importorskip("torch")
+    temps = geometric_ladder(0.05, 1.0, 6)
+    full = Engine([System(L=4, temperatures=temps)], seed=77)
+    halves = [Engine([System(L=4, temperatures=temps, n_replicas=3, replica_offset=3 * r)], seed=77)
+              for r in range(2)]
+    full.init_random()
+    for h in halves:
+        h.init_random()
+    e_all = torch.zeros(6, dtype=torch.float64, device="cuda")
+    for k in range(6):
+        full.cycle(1, 2, False, 1)
+        full.pt_swap(-1)
+        for r, h in enumerate(halves):
+            h.cycle(1, 2, False, 1)
+            h.observables_device(e_all.data_ptr() + 8 * 3 * r)
+            h.synchronize()
+        for h in halves:
+            h.pt_swap_global(e_all.data_ptr(), -1)
+        for h in halves:
+            assert np.array_equal(h.permutation(), full.permutation())
+    f = full.get_spins()
+    for r, h in enumerate(halves):
+        assert np.array_equal(h.get_spins(), f[3 * r:3 * r + 3])
+
+
+def test_determinism_two_runs():
+    def run():
+        e = Engine([System(L=5, temperatures=[0.2, 0.4])], seed=11)
+        e.init_random()
+        e.tune_cone(0.5, 3, 2)
+        e.cycle(1, 3, True, 5)
+        return e.get_spins(), e.observables()[0]
+    (a, ea), (b, eb) = run(), run()
+    assert np.array_equal(a, b) and np.array_equal(ea, eb)
+
+
+def test_errors_are_reported():
+    with pytest.raises(PyroError):
+        Engine([System(L=1, temperatures=[1.0])])
+    with pytest.raises(PyroError):
+        Engine([System(L=4, temperatures=[1.0, 0.5])])  # not increasing
+    e = Engine([System(L=4, temperatures=[1.0, 2.0])])
+    with pytest.raises(PyroError):
+        e.set_cone(np.array([2.0, 0.0], dtype=np.float32))
+    with pytest.raises(PyroError):
+        e.metropolis_sweep(-1)
+    sh = Engine([System(L=4, temperatures=[1.0, 2.0], n_replicas=1)])
+    with pytest.raises(PyroError):
+        sh.pt_swap()
+    with pytest.raises(PyroError):
+        sh.cycle(1, 1, True, 1)
+
+
+def test_check_spins_flags_planted_nan():
+    e = Engine([System(L=3, temperatures=[1.0])])
+    e.init_random()
+    assert e.check_spins() == -1
+    s = e.get_spins()
+    s[0, 5, 7, 1] = np.nan
+    e.set_spins(s)
+    assert e.check_spins() == 5 * 27 + 7
