@@ -41,6 +41,11 @@ FALLBACK_HBM_GBS = 6650.0
 BYTES_PER_UPDATE_PASS = 80  # float4 spins, J1 4-colour pass: 16 N/4 own + 48 N/4 nbr + 16 N/4 write
 
 
+def set_workload(l: int, replicas: int) -> None:
+    global L, R_PER_GPU
+    L, R_PER_GPU = l, replicas
+
+
 def hbm_peak():
     try:
         with open(PEAKS) as f:
@@ -155,22 +160,27 @@ def run_reference(args):
 
 
 def workload_config(n_gpus):
-    return {"workload": "pyrochlore Heisenberg AFM PT: L=32 (524,288 sites), J1=1, "
+    return {"workload": f"pyrochlore Heisenberg AFM PT: L={L} ({16 * L ** 3:,} sites), J1=1, "
                         f"{R_PER_GPU} replicas per GPU on a geometric ladder T in [0.02, 2.0], "
                         "1 Metropolis + 4 over-relaxation sweeps + FP64 energies + swap per step",
             "L": L, "replicas_per_gpu": R_PER_GPU, "global_replicas": R_PER_GPU * n_gpus,
             "sweeps_per_step": N_METRO + N_OR, "parallelism": f"replicas sharded over {n_gpus} GPU",
-            "l2": "inputs larger than L2 (537 MB of spins per GPU > 126 MB)"}
+            "l2": f"inputs larger than L2 ({R_PER_GPU * 16 * L ** 3 * 16 / 1e6:.0f} MB of spins "
+                  "per GPU > 126 MB)"}
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--L", type=int, default=L, help="lattice size (profiling cases)")
+    ap.add_argument("--replicas", type=int, default=R_PER_GPU, help="replicas per GPU")
     args = ap.parse_args()
+    set_workload(args.L, args.replicas)
     if args.impl == "reference":
         return run_reference(args)
 
@@ -248,7 +258,7 @@ def main():
     # End to end through the C-ABI with host buffers: each step uploads the cone
     # widths from pinned host memory, runs the cycle, and reads the FP64
     # energies and magnetisations back to host memory (synchronous).
-    e2e_steps = max(10, args.steps // 4)
+    e2e_steps = 0 if args.no_e2e else max(10, args.steps // 4)
     cones_h = torch.from_numpy(cones).pin_memory()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
@@ -256,8 +266,9 @@ def main():
         step()
         E, M = eng.observables()
     e2e_s = time.perf_counter() - t0
-    e2e_value = R_PER_GPU * n_gpus * 16 * L ** 3 * (N_METRO + N_OR) * e2e_steps / (e2e_s * 1e9)
-    if world > 1:
+    e2e_value = (R_PER_GPU * n_gpus * 16 * L ** 3 * (N_METRO + N_OR) * e2e_steps / (e2e_s * 1e9)
+                 if e2e_steps else None)
+    if world > 1 and e2e_value is not None:
         t = torch.tensor([e2e_value], device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MIN)
         e2e_value = float(t.item()) * 1.0

@@ -356,6 +356,10 @@ int pyro_create(const pyro_config* cfg, pyro_ctx** out) {
     s.J2 = (float)d.J2;
     s.J3a = (float)d.J3;
     s.J3b = (float)d.J3b;
+    s.J64[0] = d.J1;
+    s.J64[1] = d.J2;
+    s.J64[2] = d.J3;
+    s.J64[3] = d.J3b;
     s.shells = (d.J1 != 0.0 ? 1 : 0) | (d.J2 != 0.0 ? 2 : 0) | (d.J3 != 0.0 ? 4 : 0) |
                (d.J3b != 0.0 ? 8 : 0);
     ctx->sys.push_back(s);

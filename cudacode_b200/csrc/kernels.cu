@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(kObsThreads) observables_kernel(const ObsParam
   const int chunk = rel - rep * sg.blocks_per_rep;
   const int L = sd.L, L3 = sd.L3, n = 16 * L3;
   const float4* rep_base = p.spins + sd.spin_off + (long long)rep * n;
-  const double Js[4] = {sd.J1, sd.J2, sd.J3a, sd.J3b};
+  const double Js[4] = {sd.J64[0], sd.J64[1], sd.J64[2], sd.J64[3]};
   const int shell_begin[5] = {0, 6, 18, 24, 30};
 
   double e = 0.0, mx = 0.0, my = 0.0, mz = 0.0;

@@ -66,7 +66,8 @@ struct SysDev {
   int temp_base;       // offset of this system's temperature arrays
   int n_temp;          // ladder size
   long long spin_off;  // float4 offset of replica 0
-  float J1, J2, J3a, J3b;
+  float J1, J2, J3a, J3b;   // FP32 couplings of the update arithmetic
+  double J64[4];           // the same couplings in FP64 for the observables
   int shells;          // bitmask of non-zero shells: 1 J1, 2 J2, 4 J3a, 8 J3b
 };
 
