@@ -109,7 +109,7 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline_sample(threads: int | None = None, replicas: int = 4, cycles: int = 3):
+def cpu_baseline_sample(threads: int | None = None, replicas: int = 16, cycles: int = 25):
     """The reference algorithm's CPU path (oracle port) on a bounded sample."""
     from cudacode_b200.engine import System, geometric_ladder
     from oracle.binding import Oracle
@@ -138,9 +138,9 @@ def run_reference(args):
     vals = []
     n_threads = None
     for _ in range(args.warmup):
-        cpu_baseline_sample(cycles=1)
+        cpu_baseline_sample(replicas=4, cycles=1)
     for _ in range(args.steps):
-        v, n_threads, dt, sample = cpu_baseline_sample(cycles=1)
+        v, n_threads, dt, sample = cpu_baseline_sample(replicas=4, cycles=1)
         vals.append(v)
     value = statistics.median(vals)
     line = {
