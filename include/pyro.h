@@ -165,6 +165,35 @@ int pyro_check_spins(pyro_ctx* ctx, float tol, long long* first_bad);
  * StructFactor path (Math.cu:721-741, Pyrochlore.cu:1303-1419). */
 int pyro_structure_factor(pyro_ctx* ctx, int system, int replica, int G, int stride, double* out);
 
+/* Energy and magnetisation without any device allocation.
+ *
+ * This entry point has no counterpart in the reference. It is for callers
+ * that cannot call cudaMalloc: code that runs inside a memory pool or arena
+ * which owns all device memory, a framework that forbids allocation once its
+ * buffers are sized, or a process that cannot afford the allocations a
+ * pyro_ctx makes. It needs no context. The caller passes the spins of
+ * n_replicas replicas of one L lattice (the float4 layout above, device
+ * memory) and receives, like pyro_observables_device, the FP64 energy per
+ * replica in dev_energy[n_replicas] and, if dev_magnetisation3 is not NULL,
+ * the magnetisation in dev_magnetisation3[3 * n_replicas].
+ *
+ * Its working space is a fixed array inside the library of
+ * PYRO_NOALLOC_MAX_PARTIALS partial sums (32 B each, 2 MiB), present on every
+ * GPU that loads the library until the process exits. One partial covers
+ * 2048 sites, so a call handles at most 16 L^3 n_replicas <=
+ * 2048 * PYRO_NOALLOC_MAX_PARTIALS sites (e.g. 256 replicas at L = 32, 32 at
+ * L = 64); larger requests return PYRO_ERR_ARG with a message on stderr and
+ * launch nothing. The call runs on the current CUDA device, on `cuda_stream`
+ * (NULL = default stream), and returns without waiting. The first call on
+ * each device looks up the array's device address; make that first call
+ * before any stream capture. All calls share the one array, so calls that
+ * overlap on the GPU (other streams, other threads) race with each other:
+ * order them on one stream. */
+#define PYRO_NOALLOC_MAX_PARTIALS 65536
+int pyro_observables_noalloc(const float* dev_spins_xyzw, int L, int n_replicas, double J1,
+                             double J2, double J3, double J3b, double* dev_energy,
+                             double* dev_magnetisation3, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif
