@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/pyro.h"
+#include "j1_kernels.cuh"
 #include "kernels.cuh"
 #include "lattice.h"
 
@@ -30,7 +31,6 @@ struct pyro_ctx {
   uint64_t seed = 0;
   int renorm_every = 0;
   NbrTable tab;
-  bool j1_only = true;
 
   std::vector<SysDev> sys;
   std::vector<std::vector<double>> ladders;
@@ -57,13 +57,24 @@ struct pyro_ctx {
   int* d_rep_sys = nullptr;
   int* d_rep_local = nullptr;
 
-  std::vector<ObsSeg> obs_segs;
+  // Observables: obs_segs covers every system in the global partial
+  // numbering (read by the finalise kernel); obs_generic is the subset run by
+  // the generic kernel (launch-local block_begin, global partial_begin);
+  // J1-only systems on the specialised path are listed in obs_j1.
+  std::vector<ObsSeg> obs_segs, obs_generic;
+  std::vector<int> obs_j1;
   ObsSeg* d_obs_segs = nullptr;
-  int obs_blocks = 0;
+  ObsSeg* d_obs_generic = nullptr;
+  int obs_generic_blocks = 0;
+  int partials_cap = 0;
   double4* d_partials = nullptr;
 
+  // Colour passes: generic segments, plus (system, colour) launches of the
+  // specialised J1 kernel.
   int n_passes = 4;
+  bool use_j1_kernel = true;
   std::vector<std::vector<PassSeg>> pass_segs;
+  std::vector<std::vector<std::pair<int, int>>> pass_j1;
   std::vector<PassSeg*> d_pass_segs;
   std::vector<int> pass_blocks;
 
@@ -124,26 +135,71 @@ PassParams pass_params(pyro_ctx* ctx, int pass) {
 }
 
 // Queues one sweep (all colour passes) with the given offset from *d_sweep.
+J1PassParams j1_params(pyro_ctx* ctx, int si, unsigned long long off) {
+  const SysDev& s = ctx->sys[si];
+  J1PassParams p;
+  p.spins = ctx->d_spins + s.spin_off;
+  p.L = s.L;
+  p.L3 = s.L3;
+  p.n_rep = s.n_rep;
+  p.rcpL = 1.0f / (float)s.L;
+  p.rep_global = s.rep_global;
+  p.rep_key = s.rep_key;
+  p.temp_base = s.temp_base;
+  p.J1 = s.J1;
+  p.temp_of_rep = ctx->d_temp_of_rep;
+  p.beta = ctx->d_beta;
+  p.cosmax = ctx->d_cosmax;
+  p.accepted = ctx->d_accepted;
+  p.sweep_ctr = ctx->d_sweep;
+  p.sweep_off = off;
+  p.seed_lo = (uint32_t)(ctx->seed & 0xffffffffu);
+  p.seed_hi = (uint32_t)(ctx->seed >> 32);
+  p.renorm_every = ctx->renorm_every;
+  return p;
+}
+
 int queue_sweep(pyro_ctx* ctx, bool metro, unsigned long long off) {
   for (int pass = 0; pass < ctx->n_passes; ++pass) {
+    for (const auto& sc : ctx->pass_j1[pass]) {
+      launch_j1_pass(j1_params(ctx, sc.first, off), sc.second, metro, ctx->stream);
+      PYRO_CK_LAUNCH();
+    }
     if (ctx->pass_blocks[pass] == 0) continue;
     PassParams p = pass_params(ctx, pass);
     p.sweep_off = off;
-    launch_colour_pass(p, ctx->tab, ctx->pass_blocks[pass], metro, ctx->j1_only, ctx->stream);
+    launch_colour_pass(p, ctx->tab, ctx->pass_blocks[pass], metro, /*j1_only=*/false,
+                       ctx->stream);
     PYRO_CK_LAUNCH();
   }
   return PYRO_OK;
 }
 
 int queue_observables(pyro_ctx* ctx) {
-  ObsParams op;
-  op.segs = ctx->d_obs_segs;
-  op.nseg = (int)ctx->obs_segs.size();
-  op.sys = ctx->d_sys;
-  op.spins = ctx->d_spins;
-  op.partials = ctx->d_partials;
-  launch_observables(op, ctx->tab, ctx->obs_blocks, ctx->stream);
-  PYRO_CK_LAUNCH();
+  for (int si : ctx->obs_j1) {
+    const SysDev& s = ctx->sys[si];
+    J1ObsParams jp;
+    jp.spins = ctx->d_spins + s.spin_off;
+    jp.L = s.L;
+    jp.L3 = s.L3;
+    jp.n_rep = s.n_rep;
+    jp.rcpL = 1.0f / (float)s.L;
+    jp.J1 = s.J64[0];
+    jp.partials = ctx->d_partials;
+    jp.partial_begin = ctx->obs_segs[si].partial_begin;
+    launch_j1_observables(jp, ctx->stream);
+    PYRO_CK_LAUNCH();
+  }
+  if (ctx->obs_generic_blocks > 0) {
+    ObsParams op;
+    op.segs = ctx->d_obs_generic;
+    op.nseg = (int)ctx->obs_generic.size();
+    op.sys = ctx->d_sys;
+    op.spins = ctx->d_spins;
+    op.partials = ctx->d_partials;
+    launch_observables(op, ctx->tab, ctx->obs_generic_blocks, ctx->stream);
+    PYRO_CK_LAUNCH();
+  }
   launch_obs_finalise(ctx->d_partials, ctx->d_obs_segs, (int)ctx->obs_segs.size(), ctx->d_sys,
                       ctx->total_reps, ctx->d_rep_sys, ctx->d_rep_local, ctx->d_energy, ctx->d_mag,
                       ctx->stream);
@@ -199,7 +255,7 @@ void free_all(pyro_ctx* c) {
                   c->d_swap_acc,    c->d_swap_try,     c->d_swap_count,  c->d_last_accepted,
                   c->d_energy,      c->d_mag,          c->d_rep_sys,     c->d_rep_local,
                   c->d_obs_segs,    c->d_partials,     c->d_sweep,       c->d_scratch_u64,
-                  c->d_history,     c->d_history_count};
+                  c->d_history,     c->d_history_count, c->d_obs_generic};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto* p : c->d_pass_segs)
@@ -207,6 +263,87 @@ void free_all(pyro_ctx* c) {
   c->d_pass_segs.clear();
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   c->stream = nullptr;
+}
+
+// Pass p runs colour p of 16-colour systems, and colour p/4 of 4-colour
+// systems when p % 4 == 0 (every pass if all systems use 4 colours).
+// J1-only systems go to the specialised kernel unless use_j1_kernel is off.
+int build_schedule(pyro_ctx* ctx) {
+  for (auto* p : ctx->d_pass_segs)
+    if (p) cudaFree(p);
+  ctx->d_pass_segs.clear();
+  if (ctx->d_obs_segs) cudaFree(ctx->d_obs_segs);
+  if (ctx->d_obs_generic) cudaFree(ctx->d_obs_generic);
+  ctx->d_obs_segs = ctx->d_obs_generic = nullptr;
+  ctx->n_passes = 4;
+  for (const auto& s : ctx->sys) ctx->n_passes = std::max(ctx->n_passes, s.n_colours);
+  ctx->pass_segs.assign(ctx->n_passes, {});
+  ctx->pass_j1.assign(ctx->n_passes, {});
+  ctx->pass_blocks.assign(ctx->n_passes, 0);
+  auto j1_path = [&](const SysDev& s) { return ctx->use_j1_kernel && s.n_colours == 4 && s.shells == 1; };
+  for (int pass = 0; pass < ctx->n_passes; ++pass) {
+    int blocks = 0;
+    for (int i = 0; i < (int)ctx->sys.size(); ++i) {
+      const SysDev& s = ctx->sys[i];
+      int colour = -1;
+      if (s.n_colours == ctx->n_passes) colour = pass;
+      else if (pass % 4 == 0) colour = pass / 4;
+      if (colour < 0) continue;
+      if (j1_path(s)) {
+        ctx->pass_j1[pass].push_back({i, colour});
+        continue;
+      }
+      PassSeg g;
+      g.sys = i;
+      g.colour = colour;
+      g.blocks_per_rep = (s.units_per_colour + kPassThreads - 1) / kPassThreads;
+      g.block_begin = blocks;
+      blocks += g.blocks_per_rep * s.n_rep;
+      ctx->pass_segs[pass].push_back(g);
+    }
+    ctx->pass_blocks[pass] = blocks;
+  }
+  ctx->obs_segs.clear();
+  ctx->obs_generic.clear();
+  ctx->obs_j1.clear();
+  int partial = 0, gblocks = 0;
+  for (int i = 0; i < (int)ctx->sys.size(); ++i) {
+    const SysDev& s = ctx->sys[i];
+    ObsSeg g;
+    g.sys = i;
+    g.partial_begin = partial;
+    g.block_begin = partial;
+    if (j1_path(s)) {
+      g.blocks_per_rep = j1_blocks_per_replica(s.L3);
+      ctx->obs_j1.push_back(i);
+    } else {
+      g.blocks_per_rep = (16 * s.L3 + kObsThreads * kObsSitesPerThread - 1) /
+                         (kObsThreads * kObsSitesPerThread);
+      ObsSeg gg = g;
+      gg.block_begin = gblocks;
+      gblocks += g.blocks_per_rep * s.n_rep;
+      ctx->obs_generic.push_back(gg);
+    }
+    partial += g.blocks_per_rep * s.n_rep;
+    ctx->obs_segs.push_back(g);
+  }
+  ctx->obs_generic_blocks = gblocks;
+  if (partial > ctx->partials_cap) return fail(ctx, PYRO_ERR_STATE, "partials buffer too small");
+  ctx->d_pass_segs.assign(ctx->n_passes, nullptr);
+  PYRO_CK(alloc(&ctx->d_obs_segs, ctx->obs_segs.size()));
+  PYRO_CK(cudaMemcpy(ctx->d_obs_segs, ctx->obs_segs.data(), sizeof(ObsSeg) * ctx->obs_segs.size(),
+                     cudaMemcpyHostToDevice));
+  PYRO_CK(alloc(&ctx->d_obs_generic, ctx->obs_generic.size()));
+  if (!ctx->obs_generic.empty())
+    PYRO_CK(cudaMemcpy(ctx->d_obs_generic, ctx->obs_generic.data(),
+                       sizeof(ObsSeg) * ctx->obs_generic.size(), cudaMemcpyHostToDevice));
+  for (int pass = 0; pass < ctx->n_passes; ++pass) {
+    PYRO_CK(alloc(&ctx->d_pass_segs[pass], ctx->pass_segs[pass].size()));
+    if (!ctx->pass_segs[pass].empty())
+      PYRO_CK(cudaMemcpy(ctx->d_pass_segs[pass], ctx->pass_segs[pass].data(),
+                         sizeof(PassSeg) * ctx->pass_segs[pass].size(), cudaMemcpyHostToDevice));
+  }
+  return PYRO_OK;
 }
 
 int validate(const pyro_config* cfg, std::string* why) {
@@ -342,7 +479,6 @@ int pyro_create(const pyro_config* cfg, pyro_ctx** out) {
     s.L3 = d.L * d.L * d.L;
     const bool far = d.J2 != 0.0 || d.J3 != 0.0 || d.J3b != 0.0;
     s.n_colours = far ? 16 : 4;
-    if (far) ctx->j1_only = false;
     max_colours = std::max(max_colours, s.n_colours);
     s.units_per_colour = 16 * s.L3 / s.n_colours;
     s.n_rep = d.n_replicas;
@@ -384,45 +520,10 @@ int pyro_create(const pyro_config* cfg, pyro_ctx** out) {
   ctx->n_spins = spin_off;
   ctx->n_passes = max_colours;
 
-  // Pass schedules: pass p runs colour p of 16-colour systems, and colour p/4
-  // of 4-colour systems when p % 4 == 0 (or every pass if all use 4 colours).
-  ctx->pass_segs.assign(ctx->n_passes, {});
-  ctx->pass_blocks.assign(ctx->n_passes, 0);
-  for (int pass = 0; pass < ctx->n_passes; ++pass) {
-    int blocks = 0;
-    for (int i = 0; i < (int)ctx->sys.size(); ++i) {
-      const SysDev& s = ctx->sys[i];
-      int colour = -1;
-      if (s.n_colours == ctx->n_passes) colour = pass;
-      else if (pass % 4 == 0) colour = pass / 4;
-      if (colour < 0) continue;
-      PassSeg g;
-      g.sys = i;
-      g.colour = colour;
-      g.blocks_per_rep = (s.units_per_colour + kPassThreads - 1) / kPassThreads;
-      g.block_begin = blocks;
-      blocks += g.blocks_per_rep * s.n_rep;
-      ctx->pass_segs[pass].push_back(g);
-    }
-    ctx->pass_blocks[pass] = blocks;
-  }
-  // Observable segments.
-  {
-    int blocks = 0;
-    for (int i = 0; i < (int)ctx->sys.size(); ++i) {
-      const SysDev& s = ctx->sys[i];
-      ObsSeg g;
-      g.sys = i;
-      g.blocks_per_rep = (16 * s.L3 + kObsThreads * kObsSitesPerThread - 1) /
-                         (kObsThreads * kObsSitesPerThread);
-      g.block_begin = blocks;
-      g.partial_begin = blocks;
-      blocks += g.blocks_per_rep * s.n_rep;
-      ctx->obs_segs.push_back(g);
-    }
-    ctx->obs_blocks = blocks;
-  }
-
+  ctx->partials_cap = 0;
+  for (const auto& sd : ctx->sys)
+    ctx->partials_cap += sd.n_rep * ((16 * sd.L3 + kObsThreads * kObsSitesPerThread - 1) /
+                                     (kObsThreads * kObsSitesPerThread));
   const int nS = (int)ctx->sys.size(), nT = ctx->total_temps, nR = ctx->total_reps;
   CREATE_CK(alloc(&ctx->d_sys, nS));
   CREATE_CK(alloc(&ctx->d_spins, ctx->n_spins));
@@ -440,18 +541,10 @@ int pyro_create(const pyro_config* cfg, pyro_ctx** out) {
   CREATE_CK(alloc(&ctx->d_mag, 3 * nR));
   CREATE_CK(alloc(&ctx->d_rep_sys, nR));
   CREATE_CK(alloc(&ctx->d_rep_local, nR));
-  CREATE_CK(alloc(&ctx->d_obs_segs, ctx->obs_segs.size()));
-  CREATE_CK(alloc(&ctx->d_partials, ctx->obs_blocks));
+  CREATE_CK(alloc(&ctx->d_partials, ctx->partials_cap));
   CREATE_CK(alloc(&ctx->d_sweep, 1));
   CREATE_CK(alloc(&ctx->d_scratch_u64, 4));
   CREATE_CK(alloc(&ctx->d_history_count, 1));
-  ctx->d_pass_segs.assign(ctx->n_passes, nullptr);
-  for (int pass = 0; pass < ctx->n_passes; ++pass) {
-    CREATE_CK(alloc(&ctx->d_pass_segs[pass], ctx->pass_segs[pass].size()));
-    if (!ctx->pass_segs[pass].empty())
-      CREATE_CK(cudaMemcpy(ctx->d_pass_segs[pass], ctx->pass_segs[pass].data(),
-                           sizeof(PassSeg) * ctx->pass_segs[pass].size(), cudaMemcpyHostToDevice));
-  }
   CREATE_CK(cudaMemcpy(ctx->d_sys, ctx->sys.data(), sizeof(SysDev) * nS, cudaMemcpyHostToDevice));
   CREATE_CK(cudaMemcpy(ctx->d_temp_of_rep, h_temp_of_rep.data(), sizeof(int) * nT,
                        cudaMemcpyHostToDevice));
@@ -463,8 +556,6 @@ int pyro_create(const pyro_config* cfg, pyro_ctx** out) {
   CREATE_CK(cudaMemcpy(ctx->d_rep_sys, h_rep_sys.data(), sizeof(int) * nR, cudaMemcpyHostToDevice));
   CREATE_CK(cudaMemcpy(ctx->d_rep_local, h_rep_local.data(), sizeof(int) * nR,
                        cudaMemcpyHostToDevice));
-  CREATE_CK(cudaMemcpy(ctx->d_obs_segs, ctx->obs_segs.data(), sizeof(ObsSeg) * ctx->obs_segs.size(),
-                       cudaMemcpyHostToDevice));
   CREATE_CK(cudaMemset(ctx->d_accepted, 0, sizeof(unsigned long long) * nT));
   CREATE_CK(cudaMemset(ctx->d_swap_acc, 0, sizeof(unsigned long long) * nT));
   CREATE_CK(cudaMemset(ctx->d_swap_try, 0, sizeof(unsigned long long) * nT));
@@ -474,6 +565,8 @@ int pyro_create(const pyro_config* cfg, pyro_ctx** out) {
   CREATE_CK(cudaMemset(ctx->d_history_count, 0, sizeof(unsigned long long)));
   CREATE_CK(cudaMemset(ctx->d_spins, 0, sizeof(float4) * ctx->n_spins));
 #undef CREATE_CK
+  rc = build_schedule(ctx);
+  if (rc != PYRO_OK) return bail(rc);
   *out = ctx;
   return PYRO_OK;
 }
@@ -499,6 +592,21 @@ int pyro_set_stream(pyro_ctx* ctx, void* cuda_stream) {
   ctx->stream = (cudaStream_t)cuda_stream;
   ctx->own_stream = false;
   return PYRO_OK;
+}
+
+int pyro_set_option(pyro_ctx* ctx, int option, int value) {
+  if (!ctx) return PYRO_ERR_ARG;
+  PYRO_CK(cudaSetDevice(ctx->device));
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  if (option == PYRO_OPT_J1_KERNEL) {
+    if (value != 0 && value != 1) return fail(ctx, PYRO_ERR_ARG, "J1 kernel option is 0 or 1");
+    ctx->use_j1_kernel = value == 1;
+  } else {
+    return fail(ctx, PYRO_ERR_ARG, "unknown option");
+  }
+  for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+  ctx->graphs.clear();
+  return build_schedule(ctx);
 }
 
 void* pyro_get_stream(const pyro_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }

@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(kObsThreads) observables_kernel(const ObsParam
       o.z += red[2][q];
       o.w += red[3][q];
     }
-    p.partials[blockIdx.x] = o;
+    p.partials[sg.partial_begin + (blockIdx.x - sg.block_begin)] = o;
   }
 }
 

@@ -31,8 +31,8 @@ struct PassParams {
 struct ObsSeg {
   int sys;
   int blocks_per_rep;
-  int block_begin;
-  int partial_begin;  // index of this system's first partial
+  int block_begin;    // first CTA of the segment in its launch
+  int partial_begin;  // index of the segment's first partial in the shared buffer
 };
 
 struct ObsParams {

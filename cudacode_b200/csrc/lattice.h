@@ -32,6 +32,7 @@ struct NbrEntry {
   int8_t dx, dy, dz, t;  // neighbour cell offset and its site in the cell
 };
 
+
 struct NbrTable {
   NbrEntry e[kSitesPerCell][kMaxNbr];
 };
@@ -45,6 +46,44 @@ inline void site_pos4(int s, int p[3]) {
 
 // Builds the canonical table; returns false if a shell count is off.
 bool build_neighbour_table(NbrTable* tab);
+
+// Compile-time form of the J1 shell of the same table: the k-th (0..5)
+// nearest neighbour of cubic-cell site s, in the canonical order (target
+// site, dx, dy, dz). Enumerating the candidates in that order makes a sort
+// unnecessary. Used by kernels that need the offsets as constants.
+PYRO_HOSTDEV constexpr NbrEntry j1_neighbour(int s, int k) {
+  const int F[4][3] = {{0, 0, 0}, {2, 2, 0}, {0, 2, 2}, {2, 0, 2}};
+  int found = 0;
+  for (int t = 0; t < kSitesPerCell; ++t)
+    for (int dx = -1; dx <= 1; ++dx)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dz = -1; dz <= 1; ++dz) {
+          const int vx = 4 * dx + F[t >> 2][0] + F[t & 3][0] / 2 - F[s >> 2][0] - F[s & 3][0] / 2;
+          const int vy = 4 * dy + F[t >> 2][1] + F[t & 3][1] / 2 - F[s >> 2][1] - F[s & 3][1] / 2;
+          const int vz = 4 * dz + F[t >> 2][2] + F[t & 3][2] / 2 - F[s >> 2][2] - F[s & 3][2] / 2;
+          if (vx * vx + vy * vy + vz * vz == 2) {
+            if (found == k) return NbrEntry{(int8_t)dx, (int8_t)dy, (int8_t)dz, (int8_t)t};
+            ++found;
+          }
+        }
+  return NbrEntry{0, 0, 0, -1};
+}
+
+// Canonical index of the j-th (0..2) nearest neighbour of site s that is not
+// in s's own up-tetrahedron (same cell, same FCC corner): its down-tetrahedron
+// partners.
+PYRO_HOSTDEV constexpr int j1_down_index(int s, int j) {
+  int found = 0;
+  for (int k = 0; k < 6; ++k) {
+    const NbrEntry e = j1_neighbour(s, k);
+    const bool up = e.dx == 0 && e.dy == 0 && e.dz == 0 && (e.t >> 2) == (s >> 2);
+    if (!up) {
+      if (found == j) return k;
+      ++found;
+    }
+  }
+  return -1;
+}
 
 // Work description of one colour pass over one (system, colour) pair.
 struct PassSeg {

@@ -81,6 +81,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "pyro_last_error": (C.c_char_p, [P]),
         "pyro_version": (i, []),
         "pyro_neighbour_table": (i, [i, pi]),
+        "pyro_set_option": (i, [P, i, i]),
         "pyro_set_stream": (i, [P, P]),
         "pyro_get_stream": (P, [P]),
         "pyro_synchronize": (i, [P]),
@@ -211,6 +212,11 @@ class Engine:
 
     def __exit__(self, *exc):
         self.close()
+
+    OPT_J1_KERNEL = 1
+
+    def set_option(self, option: int, value: int) -> None:
+        self._ck(self.lib.pyro_set_option(self.ctx, option, value))
 
     def set_stream(self, stream_handle: int) -> None:
         self._ck(self.lib.pyro_set_stream(self.ctx, C.c_void_p(stream_handle)))

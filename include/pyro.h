@@ -71,6 +71,12 @@ int pyro_version(void);
  * (Pyrochlore.cu:152-167, 643-711). Needs no GPU. */
 int pyro_neighbour_table(int site, int* out120);
 
+/* Kernel choices (the autotuner's knobs). PYRO_OPT_J1_KERNEL: 1 (default)
+ * runs J1-only systems on the specialised one-thread-per-cell kernels, 0 on
+ * the generic colour-pass kernel; results are bit-identical either way. */
+#define PYRO_OPT_J1_KERNEL 1
+int pyro_set_option(pyro_ctx* ctx, int option, int value);
+
 /* Stream used by every call (default: a stream the context creates). */
 int pyro_set_stream(pyro_ctx* ctx, void* cuda_stream);
 void* pyro_get_stream(const pyro_ctx* ctx);

@@ -229,3 +229,43 @@ def test_check_spins_flags_planted_nan():
     s[0, 5, 7, 1] = np.nan
     e.set_spins(s)
     assert e.check_spins() == 5 * 27 + 7
+
+
+@pytest.mark.parametrize("specialised", [0, 1])
+def test_j1_kernel_variants_bit_exact(specialised):
+    temps = geometric_ladder(0.05, 1.0, 3)
+    e, o = pair([System(L=6, temperatures=temps)], renorm_every=3)
+    e.set_option(e.OPT_J1_KERNEL, specialised)
+    e.init_random()
+    o.init_random()
+    c = np.array([0.6, 0.1, -0.7], dtype=np.float32)
+    e.set_cone(c)
+    o.set_cone(c)
+    for _ in range(5):
+        e.metropolis_sweep(1)
+        o.metropolis_sweep(1)
+        e.overrelax_sweep(3)
+        o.overrelax_sweep(3)
+    assert np.array_equal(e.get_spins(), o.get_spins())
+    E1, M1 = e.observables()
+    E2, M2 = o.observables()
+    np.testing.assert_allclose(E1, E2, rtol=1e-12, atol=1e-9)
+    np.testing.assert_allclose(M1, M2, rtol=1e-12, atol=1e-9)
+    a1, _ = e.acceptance()
+    a2, _ = o.acceptance()
+    assert np.array_equal(a1, a2)
+
+
+def test_mixed_j1_and_further_neighbour_systems():
+    systems = [System(L=4, temperatures=[0.3, 0.8]),
+               System(L=3, temperatures=[0.5, 1.0, 2.0], J2=0.04, J3=-0.02),
+               System(L=5, temperatures=[1.0])]
+    e, o = pair(systems, renorm_every=4)
+    e.init_random()
+    o.init_random()
+    e.cycle(1, 3, True, 4)
+    o.cycle(1, 3, True, 4)
+    for k in range(3):
+        assert np.array_equal(e.get_spins(k), o.get_spins(k)), k
+        np.testing.assert_allclose(e.observables(k)[0], o.observables(k)[0], rtol=1e-12)
+        assert np.array_equal(e.permutation(k), o.permutation(k))
