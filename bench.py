@@ -179,6 +179,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--L", type=int, default=L, help="lattice size (profiling cases)")
     ap.add_argument("--replicas", type=int, default=R_PER_GPU, help="replicas per GPU")
+    ap.add_argument("--kernel", default="auto", choices=["auto", "pass", "cluster"],
+                    help="auto: autotuner picks; pass: one launch per colour pass; "
+                         "cluster: cluster-resident cycle kernel")
     args = ap.parse_args()
     set_workload(args.L, args.replicas)
     if args.impl == "reference":
@@ -206,6 +209,15 @@ def main():
     eng.init_random()
     cones = np.full(len(temps), 0.3, dtype=np.float32)
     eng.set_cone(cones)
+    variant = None
+    if args.kernel == "auto":
+        # the autotuner's cycles are untimed warm-up Monte Carlo steps
+        variant = eng.autotune(N_METRO, N_OR, 3) if world == 1 else None
+    else:
+        eng.set_option(eng.OPT_CYCLE_KERNEL, 1 if args.kernel == "cluster" else 0)
+    kernel_desc = {"cycle_kernel": eng.get_option(eng.OPT_CYCLE_KERNEL),
+                   "cluster_size": eng.get_option(eng.OPT_CLUSTER_SIZE),
+                   "j1_kernel": eng.get_option(eng.OPT_J1_KERNEL), "autotune_choice": variant}
     e_all = torch.zeros(R_PER_GPU * n_gpus, dtype=torch.float64, device=f"cuda:{local}")
     e_loc = torch.zeros(R_PER_GPU, dtype=torch.float64, device=f"cuda:{local}")
 
@@ -287,7 +299,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (random unit spins from Philox seed)",
-            "config": workload_config(n_gpus),
+            "config": dict(workload_config(n_gpus), kernels=kernel_desc),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "kernel": "colour_pass_kernel<J1, over-relaxation>",

@@ -73,6 +73,10 @@ struct pyro_ctx {
   // specialised J1 kernel.
   int n_passes = 4;
   bool use_j1_kernel = true;
+  // Cluster-resident cycle kernel for J1 systems (0 = per-pass launches).
+  int cycle_kernel = 0;
+  int cluster_size = 16;
+  bool cluster_checked = false;
   std::vector<std::vector<PassSeg>> pass_segs;
   std::vector<std::vector<std::pair<int, int>>> pass_j1;
   std::vector<PassSeg*> d_pass_segs;
@@ -159,9 +163,10 @@ J1PassParams j1_params(pyro_ctx* ctx, int si, unsigned long long off) {
   return p;
 }
 
-int queue_sweep(pyro_ctx* ctx, bool metro, unsigned long long off) {
+int queue_sweep(pyro_ctx* ctx, bool metro, unsigned long long off, bool skip_j1 = false) {
   for (int pass = 0; pass < ctx->n_passes; ++pass) {
     for (const auto& sc : ctx->pass_j1[pass]) {
+      if (skip_j1) break;
       launch_j1_pass(j1_params(ctx, sc.first, off), sc.second, metro, ctx->stream);
       PYRO_CK_LAUNCH();
     }
@@ -175,8 +180,9 @@ int queue_sweep(pyro_ctx* ctx, bool metro, unsigned long long off) {
   return PYRO_OK;
 }
 
-int queue_observables(pyro_ctx* ctx) {
+int queue_observables(pyro_ctx* ctx, bool skip_j1 = false) {
   for (int si : ctx->obs_j1) {
+    if (skip_j1) break;
     const SysDev& s = ctx->sys[si];
     J1ObsParams jp;
     jp.spins = ctx->d_spins + s.spin_off;
@@ -205,6 +211,55 @@ int queue_observables(pyro_ctx* ctx) {
                       ctx->stream);
   PYRO_CK_LAUNCH();
   return PYRO_OK;
+}
+
+// Checks once that the cluster size can be resident; falls back to smaller
+// clusters, then to per-pass launches.
+int check_cluster(pyro_ctx* ctx) {
+  if (ctx->cluster_checked) return PYRO_OK;
+  ctx->cluster_checked = true;
+  if (!ctx->cycle_kernel) return PYRO_OK;
+  for (int cs = ctx->cluster_size; cs >= 2; cs /= 2) {
+    int n = 0;
+    cudaError_t e = j1_cycle_prepare(cs, &n);
+    if (e == cudaSuccess && n > 0) {
+      ctx->cluster_size = cs;
+      return PYRO_OK;
+    }
+    cudaGetLastError();
+  }
+  ctx->cycle_kernel = 0;
+  return PYRO_OK;
+}
+
+bool use_cycle_kernel(const pyro_ctx* ctx) {
+  return ctx->cycle_kernel && ctx->use_j1_kernel && !ctx->obs_j1.empty();
+}
+
+// n_metro Metropolis + n_or over-relaxation sweeps of every system, and (if
+// with_obs) the observables partials and their per-replica sums.
+int queue_cycle_body(pyro_ctx* ctx, int n_metro, int n_or, bool with_obs) {
+  int rc = check_cluster(ctx);
+  if (rc) return rc;
+  const bool cyc = use_cycle_kernel(ctx);
+  if (cyc) {
+    for (int si : ctx->obs_j1) {
+      J1CycleParams cp;
+      cp.pass = j1_params(ctx, si, 0);
+      cp.n_metro = n_metro;
+      cp.n_or = n_or;
+      cp.cluster_size = ctx->cluster_size;
+      cp.J1_64 = ctx->sys[si].J64[0];
+      cp.partials = with_obs ? ctx->d_partials : nullptr;
+      cp.partial_begin = ctx->obs_segs[si].partial_begin;
+      PYRO_CK(launch_j1_cycle(cp, ctx->stream));
+    }
+  }
+  for (int i = 0; i < n_metro && rc == PYRO_OK; ++i) rc = queue_sweep(ctx, true, i, cyc);
+  for (int i = 0; i < n_or && rc == PYRO_OK; ++i) rc = queue_sweep(ctx, false, n_metro + i, cyc);
+  if (rc) return rc;
+  if (with_obs) rc = queue_observables(ctx, cyc);
+  return rc;
 }
 
 ExchangeParams exchange_params(pyro_ctx* ctx) {
@@ -601,12 +656,79 @@ int pyro_set_option(pyro_ctx* ctx, int option, int value) {
   if (option == PYRO_OPT_J1_KERNEL) {
     if (value != 0 && value != 1) return fail(ctx, PYRO_ERR_ARG, "J1 kernel option is 0 or 1");
     ctx->use_j1_kernel = value == 1;
+  } else if (option == PYRO_OPT_CYCLE_KERNEL) {
+    if (value != 0 && value != 1) return fail(ctx, PYRO_ERR_ARG, "cycle kernel option is 0 or 1");
+    ctx->cycle_kernel = value;
+    ctx->cluster_checked = false;
+  } else if (option == PYRO_OPT_CLUSTER_SIZE) {
+    if (value != 2 && value != 4 && value != 8 && value != 16)
+      return fail(ctx, PYRO_ERR_ARG, "cluster size is 2, 4, 8 or 16");
+    ctx->cluster_size = value;
+    ctx->cluster_checked = false;
   } else {
     return fail(ctx, PYRO_ERR_ARG, "unknown option");
   }
   for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
   ctx->graphs.clear();
   return build_schedule(ctx);
+}
+
+int pyro_get_option(pyro_ctx* ctx, int option, int* value) {
+  if (!ctx || !value) return PYRO_ERR_ARG;
+  int rc = check_cluster(ctx);
+  if (rc) return rc;
+  switch (option) {
+    case PYRO_OPT_J1_KERNEL: *value = ctx->use_j1_kernel ? 1 : 0; break;
+    case PYRO_OPT_CYCLE_KERNEL: *value = ctx->cycle_kernel; break;
+    case PYRO_OPT_CLUSTER_SIZE: *value = ctx->cluster_size; break;
+    default: return fail(ctx, PYRO_ERR_ARG, "unknown option");
+  }
+  return PYRO_OK;
+}
+
+// Times each kernel variant on `cycles` real cycles (they advance the chain:
+// every variant computes the same updates) and keeps the fastest.
+int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (cycles < 1 || n_metro < 0 || n_or < 0 || n_metro + n_or < 1)
+    return fail(ctx, PYRO_ERR_ARG, "autotune: need cycles >= 1 and at least one sweep");
+  struct Variant { int j1, cyc, cs; };
+  const Variant vs[] = {{0, 0, 16}, {1, 0, 16}, {1, 1, 16}, {1, 1, 8}, {1, 1, 4}};
+  const bool swap = !sharded(ctx);
+  cudaEvent_t a, b;
+  PYRO_CK(cudaEventCreate(&a));
+  PYRO_CK(cudaEventCreate(&b));
+  float best = 1e30f;
+  int best_i = -1;
+  const int n_var = (int)(sizeof(vs) / sizeof(vs[0]));
+  for (int i = 0; i < n_var; ++i) {
+    int rc = pyro_set_option(ctx, PYRO_OPT_J1_KERNEL, vs[i].j1);
+    if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_CYCLE_KERNEL, vs[i].cyc);
+    if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_CLUSTER_SIZE, vs[i].cs);
+    if (!rc) rc = check_cluster(ctx);
+    if (rc) continue;
+    if (vs[i].cyc && (ctx->cycle_kernel != 1 || ctx->cluster_size != vs[i].cs)) continue;
+    if ((rc = pyro_cycle(ctx, n_metro, n_or, swap, 1))) return rc;  // build the graph
+    PYRO_CK(cudaEventRecord(a, ctx->stream));
+    if ((rc = pyro_cycle(ctx, n_metro, n_or, swap, cycles))) return rc;
+    PYRO_CK(cudaEventRecord(b, ctx->stream));
+    PYRO_CK(cudaEventSynchronize(b));
+    float ms = 0.f;
+    PYRO_CK(cudaEventElapsedTime(&ms, a, b));
+    if (ms < best) {
+      best = ms;
+      best_i = i;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (best_i < 0) return fail(ctx, PYRO_ERR_STATE, "autotune: no variant ran");
+  const Variant& w = vs[best_i];
+  int rc = pyro_set_option(ctx, PYRO_OPT_J1_KERNEL, w.j1);
+  if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_CYCLE_KERNEL, w.cyc);
+  if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_CLUSTER_SIZE, w.cs);
+  if (chosen) *chosen = best_i;
+  return rc;
 }
 
 void* pyro_get_stream(const pyro_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
@@ -675,10 +797,8 @@ static int run_sweeps(pyro_ctx* ctx, int n, bool metro) {
   if (n < 0) return fail(ctx, PYRO_ERR_ARG, "n_sweeps must be >= 0");
   if (n == 0) return PYRO_OK;
   PYRO_CK(cudaSetDevice(ctx->device));
-  for (int i = 0; i < n; ++i) {
-    int rc = queue_sweep(ctx, metro, (unsigned long long)i);
-    if (rc != PYRO_OK) return rc;
-  }
+  int rc = queue_cycle_body(ctx, metro ? n : 0, metro ? 0 : n, false);
+  if (rc != PYRO_OK) return rc;
   launch_advance(ctx->d_sweep, (unsigned long long)n, ctx->stream);
   PYRO_CK_LAUNCH();
   ctx->h_sweep += (unsigned long long)n;
@@ -962,11 +1082,10 @@ int pyro_cycle(pyro_ctx* ctx, int n_metro, int n_or, int do_swap, int n_cycles) 
   auto it = ctx->graphs.find(key);
   if (it == ctx->graphs.end()) {
     cudaGraph_t g;
+    int rc = check_cluster(ctx);  // sets kernel attributes: not inside a capture
+    if (rc) return rc;
     PYRO_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = PYRO_OK;
-    for (int i = 0; i < n_metro && rc == PYRO_OK; ++i) rc = queue_sweep(ctx, true, i);
-    for (int i = 0; i < n_or && rc == PYRO_OK; ++i) rc = queue_sweep(ctx, false, n_metro + i);
-    if (rc == PYRO_OK) rc = queue_observables(ctx);
+    rc = queue_cycle_body(ctx, n_metro, n_or, true);
     if (rc == PYRO_OK) {
       ExchangeParams x = exchange_params(ctx);
       x.do_swap = do_swap ? 1 : 0;

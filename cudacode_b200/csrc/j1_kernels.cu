@@ -58,24 +58,35 @@ __device__ __forceinline__ CellFrame make_frame(int x, int y, int z, int L) {
   return f;
 }
 
-template <int S, int K>
+// Spin loads. Within one launch of a colour pass the neighbours read are
+// never written, so the read-only path (ld.global.nc) is safe. The
+// cluster-resident cycle kernel rewrites the lattice between passes of the
+// same launch, so it reads through L2 only (ld.global.cg): an SM's L1 may
+// still hold lines from an earlier pass.
+template <bool kL2Only>
+__device__ __forceinline__ float4 load_spin(const float4* p) {
+  if (kL2Only) return __ldcg(p);
+  return __ldg(p);
+}
+
+template <int S, int K, bool kL2Only = false>
 __device__ __forceinline__ float4 load_neighbour(const float4* __restrict__ rep, const CellFrame& f,
                                                  int L3) {
   constexpr NbrEntry e = j1_neighbour(S, K);
   static_assert(e.t >= 0, "neighbour table");
-  return __ldg(rep + f.zo[e.dz + 1] + f.yo[e.dy + 1] + f.xo[e.dx + 1] + e.t * L3);
+  return load_spin<kL2Only>(rep + f.zo[e.dz + 1] + f.yo[e.dy + 1] + f.xo[e.dx + 1] + e.t * L3);
 }
 
 // Sum of the 6 nearest neighbours of site S, in canonical order.
-template <int S>
+template <int S, bool kL2Only = false>
 __device__ __forceinline__ pyro_vec3 j1_sum(const float4* __restrict__ rep, const CellFrame& f,
                                             int L3) {
-  const float4 n0 = load_neighbour<S, 0>(rep, f, L3);
-  const float4 n1 = load_neighbour<S, 1>(rep, f, L3);
-  const float4 n2 = load_neighbour<S, 2>(rep, f, L3);
-  const float4 n3 = load_neighbour<S, 3>(rep, f, L3);
-  const float4 n4 = load_neighbour<S, 4>(rep, f, L3);
-  const float4 n5 = load_neighbour<S, 5>(rep, f, L3);
+  const float4 n0 = load_neighbour<S, 0, kL2Only>(rep, f, L3);
+  const float4 n1 = load_neighbour<S, 1, kL2Only>(rep, f, L3);
+  const float4 n2 = load_neighbour<S, 2, kL2Only>(rep, f, L3);
+  const float4 n3 = load_neighbour<S, 3, kL2Only>(rep, f, L3);
+  const float4 n4 = load_neighbour<S, 4, kL2Only>(rep, f, L3);
+  const float4 n5 = load_neighbour<S, 5, kL2Only>(rep, f, L3);
   pyro_vec3 a;
   a.x = ((((n0.x + n1.x) + n2.x) + n3.x) + n4.x) + n5.x;
   a.y = ((((n0.y + n1.y) + n2.y) + n3.y) + n4.y) + n5.y;
@@ -83,14 +94,14 @@ __device__ __forceinline__ pyro_vec3 j1_sum(const float4* __restrict__ rep, cons
   return a;
 }
 
-template <int S, bool kMetro>
+template <int S, bool kMetro, bool kL2Only = false>
 __device__ __forceinline__ int update_site(float4* __restrict__ rep, const CellFrame& f, int cell,
                                            int L3, float J1, float beta, float cosmax, uint32_t rkey,
                                            uint32_t sweep32, bool renorm, uint32_t seed_lo,
                                            uint32_t seed_hi) {
   const int own = S * L3 + cell;
-  const float4 sv = rep[own];
-  const pyro_vec3 a = j1_sum<S>(rep, f, L3);
+  const float4 sv = kL2Only ? __ldcg(rep + own) : rep[own];
+  const pyro_vec3 a = j1_sum<S, kL2Only>(rep, f, L3);
   pyro_vec3 h;
   h.x = J1 * a.x;
   h.y = J1 * a.y;
@@ -172,15 +183,15 @@ __device__ __forceinline__ double warp_sum_d(double v) {
 }
 
 // Down-tetrahedron partners of the sublattice-0 site 4F of a cell.
-template <int F>
+template <int F, bool kL2Only>
 __device__ __forceinline__ void down_partners(const float4* __restrict__ rep, const CellFrame& f,
                                               int L3, float4* d1, float4* d2, float4* d3) {
   constexpr int S0 = 4 * F;
   constexpr int k1 = j1_down_index(S0, 0), k2 = j1_down_index(S0, 1), k3 = j1_down_index(S0, 2);
   static_assert(k1 >= 0 && k2 >= 0 && k3 >= 0, "three down-tetrahedron partners");
-  *d1 = load_neighbour<S0, k1>(rep, f, L3);
-  *d2 = load_neighbour<S0, k2>(rep, f, L3);
-  *d3 = load_neighbour<S0, k3>(rep, f, L3);
+  *d1 = load_neighbour<S0, k1, kL2Only>(rep, f, L3);
+  *d2 = load_neighbour<S0, k2, kL2Only>(rep, f, L3);
+  *d3 = load_neighbour<S0, k3, kL2Only>(rep, f, L3);
 }
 
 // E_tet = J1 * sum_{i<j in tet} S_i.S_j = J1/2 (|sum S|^2 - sum |S|^2), FP64.
@@ -195,40 +206,41 @@ __device__ __forceinline__ double tet_energy(float4 a, float4 b, float4 c, float
   return 0.5 * (mx * mx + my * my + mz * mz - n2);
 }
 
-template <int F>
+template <int F, bool kL2Only = false>
 __device__ __forceinline__ void cell_corner(const float4* __restrict__ rep, const CellFrame& f,
                                             int cell, int L3, double* e, double* mx, double* my,
                                             double* mz) {
-  const float4 s0 = __ldg(rep + (4 * F + 0) * L3 + cell);
-  const float4 s1 = __ldg(rep + (4 * F + 1) * L3 + cell);
-  const float4 s2 = __ldg(rep + (4 * F + 2) * L3 + cell);
-  const float4 s3 = __ldg(rep + (4 * F + 3) * L3 + cell);
+  const float4 s0 = load_spin<kL2Only>(rep + (4 * F + 0) * L3 + cell);
+  const float4 s1 = load_spin<kL2Only>(rep + (4 * F + 1) * L3 + cell);
+  const float4 s2 = load_spin<kL2Only>(rep + (4 * F + 2) * L3 + cell);
+  const float4 s3 = load_spin<kL2Only>(rep + (4 * F + 3) * L3 + cell);
   float4 d1, d2, d3;
-  down_partners<F>(rep, f, L3, &d1, &d2, &d3);
+  down_partners<F, kL2Only>(rep, f, L3, &d1, &d2, &d3);
   *e += tet_energy(s0, s1, s2, s3) + tet_energy(s0, d1, d2, d3);
   *mx += (double)s0.x + s1.x + s2.x + s3.x;
   *my += (double)s0.y + s1.y + s2.y + s3.y;
   *mz += (double)s0.z + s1.z + s2.z + s3.z;
 }
 
-// Each cell owns its 4 up-tetrahedra and the 4 down-tetrahedra that contain
-// its sublattice-0 sites: every bond is counted exactly once.
-__global__ void __launch_bounds__(kJ1Threads) j1_observables_kernel(const J1ObsParams p) {
-  const int rep = blockIdx.y;
-  const int cell = blockIdx.x * kJ1Threads + threadIdx.x;
+// Energy (each bond once, by tetrahedra) and magnetisation of one chunk of
+// kJ1Threads cells, reduced over the CTA in a fixed order; thread 0 returns
+// (2 E, Mx, My, Mz) (the finalise step halves the site-sum convention of the
+// generic kernel, hence 2 E). Every thread of the CTA must call it.
+template <bool kL2Only>
+__device__ __forceinline__ double4 chunk_observables(const float4* __restrict__ rb, int cell,
+                                                     int L, int L3, float rcpL, double J1,
+                                                     double (*red)[kJ1Threads / 32]) {
   double e = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
-  if (cell < p.L3) {
+  if (cell < L3) {
     int x, y, z;
-    decode_cell(cell, p.L, p.rcpL, &x, &y, &z);
-    const CellFrame f = make_frame(x, y, z, p.L);
-    const float4* rb = p.spins + (long long)rep * 16 * p.L3;
-    cell_corner<0>(rb, f, cell, p.L3, &e, &mx, &my, &mz);
-    cell_corner<1>(rb, f, cell, p.L3, &e, &mx, &my, &mz);
-    cell_corner<2>(rb, f, cell, p.L3, &e, &mx, &my, &mz);
-    cell_corner<3>(rb, f, cell, p.L3, &e, &mx, &my, &mz);
-    e *= p.J1;
+    decode_cell(cell, L, rcpL, &x, &y, &z);
+    const CellFrame f = make_frame(x, y, z, L);
+    cell_corner<0, kL2Only>(rb, f, cell, L3, &e, &mx, &my, &mz);
+    cell_corner<1, kL2Only>(rb, f, cell, L3, &e, &mx, &my, &mz);
+    cell_corner<2, kL2Only>(rb, f, cell, L3, &e, &mx, &my, &mz);
+    cell_corner<3, kL2Only>(rb, f, cell, L3, &e, &mx, &my, &mz);
+    e *= J1;
   }
-  __shared__ double red[4][kJ1Threads / 32];
   e = warp_sum_d(e);
   mx = warp_sum_d(mx);
   my = warp_sum_d(my);
@@ -241,18 +253,182 @@ __global__ void __launch_bounds__(kJ1Threads) j1_observables_kernel(const J1ObsP
     red[3][w] = mz;
   }
   __syncthreads();
+  double4 o = make_double4(0.0, 0.0, 0.0, 0.0);
   if (threadIdx.x == 0) {
-    double4 o = make_double4(0.0, 0.0, 0.0, 0.0);
     for (int q = 0; q < kJ1Threads / 32; ++q) {
       o.x += red[0][q];
       o.y += red[1][q];
       o.z += red[2][q];
       o.w += red[3][q];
     }
-    // E is accumulated per tetrahedron (each bond once); the finalise step
-    // halves the site sum of the generic kernel, so store 2 E here.
     o.x *= 2.0;
-    p.partials[p.partial_begin + (long long)rep * gridDim.x + blockIdx.x] = o;
+  }
+  __syncthreads();
+  return o;
+}
+
+// Each cell owns its 4 up-tetrahedra and the 4 down-tetrahedra that contain
+// its sublattice-0 sites: every bond is counted exactly once.
+__global__ void __launch_bounds__(kJ1Threads) j1_observables_kernel(const J1ObsParams p) {
+  __shared__ double red[4][kJ1Threads / 32];
+  const int rep = blockIdx.y;
+  const int cell = blockIdx.x * kJ1Threads + threadIdx.x;
+  const float4* rb = p.spins + (long long)rep * 16 * p.L3;
+  const double4 o = chunk_observables<false>(rb, cell, p.L, p.L3, p.rcpL, p.J1, red);
+  if (threadIdx.x == 0) p.partials[p.partial_begin + (long long)rep * gridDim.x + blockIdx.x] = o;
+}
+
+// One site update of the cluster kernel: site S of `cell`, neighbours read
+// through L2. Returns 1 if a Metropolis move was accepted.
+template <int S, bool kMetro>
+__device__ __forceinline__ int cluster_site(float4* __restrict__ rb, int cell, int L, int L3,
+                                            float rcpL, float J1, float beta, float cosmax,
+                                            uint32_t rkey, uint32_t sw, bool renorm,
+                                            uint32_t seed_lo, uint32_t seed_hi) {
+  int x, y, z;
+  decode_cell(cell, L, rcpL, &x, &y, &z);
+  const CellFrame f = make_frame(x, y, z, L);
+  return update_site<S, kMetro, true>(rb, f, cell, L3, J1, beta, cosmax, rkey, sw, renorm,
+                                      seed_lo, seed_hi);
+}
+
+template <bool kMetro>
+__device__ __forceinline__ int cluster_dispatch(int s, float4* __restrict__ rb, int cell, int L,
+                                                int L3, float rcpL, float J1, float beta,
+                                                float cosmax, uint32_t rkey, uint32_t sw,
+                                                bool renorm, uint32_t seed_lo, uint32_t seed_hi) {
+  switch (s) {
+#define PYRO_SITE(S) \
+  case S:            \
+    return cluster_site<S, kMetro>(rb, cell, L, L3, rcpL, J1, beta, cosmax, rkey, sw, renorm, seed_lo, seed_hi);
+    PYRO_SITE(0) PYRO_SITE(1) PYRO_SITE(2) PYRO_SITE(3) PYRO_SITE(4) PYRO_SITE(5) PYRO_SITE(6)
+    PYRO_SITE(7) PYRO_SITE(8) PYRO_SITE(9) PYRO_SITE(10) PYRO_SITE(11) PYRO_SITE(12)
+    PYRO_SITE(13) PYRO_SITE(14) PYRO_SITE(15)
+#undef PYRO_SITE
+    default:
+      return 0;
+  }
+}
+
+__device__ __forceinline__ void cluster_barrier() {
+  // Release our spin stores to the cluster and acquire everyone else's.
+  asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+  asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+// A whole cycle for one replica per thread-block cluster: n_metro Metropolis
+// then n_or over-relaxation sweeps, each sweep 4 colour passes separated by a
+// cluster barrier, then (optionally) the observables partials of the final
+// state. In a pass the 4 L^3 sites of the colour are split in chunks of
+// kJ1CycleThreads over the CTAs of the cluster (chunk c to CTA c % cluster
+// size), one site per thread per chunk, so a CTA keeps 32 warps of
+// independent loads in flight. The replica's 16 L^3 float4 stay in L2 across
+// the passes; HBM sees about one read and one write of the lattice per call.
+// Results equal those of the per-pass kernels bit for bit.
+__global__ void __launch_bounds__(kJ1CycleThreads, 1)
+    j1_cycle_cluster_kernel(const J1CycleParams p) {
+  __shared__ double red[kJ1CycleThreads / kJ1Threads][4][kJ1Threads / 32];
+  __shared__ int warp_acc[kJ1CycleThreads / 32];
+  const int csize = p.cluster_size;
+  const int rep = blockIdx.x / csize;
+  const int rank = blockIdx.x - rep * csize;
+  const int g = p.pass.rep_global + rep;
+  const int t = p.pass.temp_of_rep[p.pass.temp_base + g];
+  const float beta = p.pass.beta[p.pass.temp_base + t];
+  const float cosmax = p.pass.cosmax[p.pass.temp_base + t];
+  const int L = p.pass.L, L3 = p.pass.L3;
+  const float rcpL = p.pass.rcpL;
+  float4* rb = p.pass.spins + (long long)rep * 16 * L3;
+  const uint32_t rkey = (uint32_t)(p.pass.rep_key + rep);
+  const unsigned long long base = (p.pass.sweep_ctr ? *p.pass.sweep_ctr : 0ull) + p.pass.sweep_off;
+  const int items = 4 * L3;
+  const int n_chunks = (items + kJ1CycleThreads - 1) / kJ1CycleThreads;
+  int acc = 0;
+  const int n_sweeps = p.n_metro + p.n_or;
+  for (int k = 0; k < n_sweeps; ++k) {
+    const unsigned long long sweep = base + (unsigned long long)k;
+    const bool renorm = p.pass.renorm_every > 0 &&
+                        ((sweep + 1) % (unsigned long long)p.pass.renorm_every) == 0;
+    const uint32_t sw = (uint32_t)sweep;
+    const bool metro = k < p.n_metro;
+#pragma unroll 1
+    for (int b = 0; b < 4; ++b) {
+#pragma unroll 1
+      for (int c = rank; c < n_chunks; c += csize) {
+        const int item = c * kJ1CycleThreads + threadIdx.x;
+        if (item < items) {
+          const int fc = item / L3;
+          const int cell = item - fc * L3;
+          const int s = 4 * fc + b;
+          if (metro)
+            acc += cluster_dispatch<true>(s, rb, cell, L, L3, rcpL, p.pass.J1, beta, cosmax, rkey,
+                                          sw, renorm, p.pass.seed_lo, p.pass.seed_hi);
+          else
+            cluster_dispatch<false>(s, rb, cell, L, L3, rcpL, p.pass.J1, beta, cosmax, rkey, sw,
+                                    renorm, p.pass.seed_lo, p.pass.seed_hi);
+        }
+      }
+      cluster_barrier();
+    }
+  }
+  if (p.n_metro > 0) {
+    int v = acc;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) warp_acc[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int s = 0;
+      for (int w = 0; w < kJ1CycleThreads / 32; ++w) s += warp_acc[w];
+      if (s > 0) atomicAdd(p.pass.accepted + p.pass.temp_base + t, (unsigned long long)s);
+    }
+  }
+  if (p.partials) {
+    // Same 256-cell chunks and reduction order as j1_observables_kernel:
+    // thread group q of the CTA handles observables chunk oc.
+    constexpr int kGroups = kJ1CycleThreads / kJ1Threads;
+    const int q = threadIdx.x / kJ1Threads;
+    const int lt = threadIdx.x - q * kJ1Threads;
+    const int n_obs = (L3 + kJ1Threads - 1) / kJ1Threads;
+    for (int base_c = rank * kGroups; base_c < n_obs; base_c += csize * kGroups) {
+      const int oc = base_c + q;
+      const int cell = oc * kJ1Threads + lt;
+      double e = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+      if (oc < n_obs && cell < L3) {
+        int x, y, z;
+        decode_cell(cell, L, rcpL, &x, &y, &z);
+        const CellFrame f = make_frame(x, y, z, L);
+        cell_corner<0, true>(rb, f, cell, L3, &e, &mx, &my, &mz);
+        cell_corner<1, true>(rb, f, cell, L3, &e, &mx, &my, &mz);
+        cell_corner<2, true>(rb, f, cell, L3, &e, &mx, &my, &mz);
+        cell_corner<3, true>(rb, f, cell, L3, &e, &mx, &my, &mz);
+        e *= p.J1_64;
+      }
+      e = warp_sum_d(e);
+      mx = warp_sum_d(mx);
+      my = warp_sum_d(my);
+      mz = warp_sum_d(mz);
+      const int w = lt >> 5, lane = lt & 31;
+      if (lane == 0) {
+        red[q][0][w] = e;
+        red[q][1][w] = mx;
+        red[q][2][w] = my;
+        red[q][3][w] = mz;
+      }
+      __syncthreads();
+      if (lt == 0 && oc < n_obs) {
+        double4 o = make_double4(0.0, 0.0, 0.0, 0.0);
+        for (int ww = 0; ww < kJ1Threads / 32; ++ww) {
+          o.x += red[q][0][ww];
+          o.y += red[q][1][ww];
+          o.z += red[q][2][ww];
+          o.w += red[q][3][ww];
+        }
+        o.x *= 2.0;
+        p.partials[p.partial_begin + (long long)rep * n_obs + oc] = o;
+      }
+      __syncthreads();
+    }
   }
 }
 
@@ -279,6 +455,40 @@ void launch_j1_pass(const J1PassParams& p, int colour, bool metro, cudaStream_t 
 void launch_j1_observables(const J1ObsParams& p, cudaStream_t st) {
   const dim3 grid((p.L3 + kJ1Threads - 1) / kJ1Threads, p.n_rep);
   j1_observables_kernel<<<grid, kJ1Threads, 0, st>>>(p);
+}
+
+cudaError_t j1_cycle_prepare(int cluster_size, int* max_active_clusters) {
+  *max_active_clusters = 0;
+  cudaError_t e = cudaFuncSetAttribute(j1_cycle_cluster_kernel,
+                                       cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cluster_size;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(cluster_size * 64, 1, 1);
+  cfg.blockDim = dim3(kJ1CycleThreads, 1, 1);
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaOccupancyMaxActiveClusters(max_active_clusters, j1_cycle_cluster_kernel, &cfg);
+}
+
+cudaError_t launch_j1_cycle(const J1CycleParams& p, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = p.cluster_size;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(p.cluster_size * p.pass.n_rep, 1, 1);
+  cfg.blockDim = dim3(kJ1CycleThreads, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, j1_cycle_cluster_kernel, p);
 }
 
 }  // namespace pyro

@@ -8,6 +8,7 @@
 namespace pyro {
 
 constexpr int kJ1Threads = 256;
+constexpr int kJ1CycleThreads = 1024;  // CTA size of the cluster-resident cycle kernel
 
 // One colour pass over all replicas of one J1-only system.
 struct J1PassParams {
@@ -37,7 +38,23 @@ struct J1ObsParams {
   int partial_begin;
 };
 
+// A whole cycle (n_metro + n_or sweeps, then observables partials if
+// partials != null) of every replica of one J1 system, one thread-block
+// cluster of cluster_size CTAs per replica.
+struct J1CycleParams {
+  J1PassParams pass;  // sweep_off = offset of the first sweep of the cycle
+  int n_metro, n_or;
+  int cluster_size;
+  double J1_64;
+  double4* partials;
+  int partial_begin;
+};
+
 void launch_j1_pass(const J1PassParams& p, int colour, bool metro, cudaStream_t st);
+cudaError_t launch_j1_cycle(const J1CycleParams& p, cudaStream_t st);
+// Sets the kernel's cluster attributes; reports how many clusters of this
+// size can be resident at once (0: size not supported).
+cudaError_t j1_cycle_prepare(int cluster_size, int* max_active_clusters);
 void launch_j1_observables(const J1ObsParams& p, cudaStream_t st);
 
 inline int j1_blocks_per_replica(int L3) { return (L3 + kJ1Threads - 1) / kJ1Threads; }

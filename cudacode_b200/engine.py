@@ -82,6 +82,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "pyro_version": (i, []),
         "pyro_neighbour_table": (i, [i, pi]),
         "pyro_set_option": (i, [P, i, i]),
+        "pyro_get_option": (i, [P, i, pi]),
+        "pyro_autotune": (i, [P, i, i, i, pi]),
         "pyro_set_stream": (i, [P, P]),
         "pyro_get_stream": (P, [P]),
         "pyro_synchronize": (i, [P]),
@@ -214,9 +216,22 @@ class Engine:
         self.close()
 
     OPT_J1_KERNEL = 1
+    OPT_CYCLE_KERNEL = 2
+    OPT_CLUSTER_SIZE = 3
 
     def set_option(self, option: int, value: int) -> None:
         self._ck(self.lib.pyro_set_option(self.ctx, option, value))
+
+    def get_option(self, option: int) -> int:
+        v = C.c_int()
+        self._ck(self.lib.pyro_get_option(self.ctx, option, C.byref(v)))
+        return v.value
+
+    def autotune(self, n_metro: int = 1, n_or: int = 4, cycles: int = 3) -> int:
+        """Times the kernel variants on real cycles and keeps the fastest."""
+        v = C.c_int()
+        self._ck(self.lib.pyro_autotune(self.ctx, n_metro, n_or, cycles, C.byref(v)))
+        return v.value
 
     def set_stream(self, stream_handle: int) -> None:
         self._ck(self.lib.pyro_set_stream(self.ctx, C.c_void_p(stream_handle)))

@@ -75,7 +75,21 @@ int pyro_neighbour_table(int site, int* out120);
  * runs J1-only systems on the specialised one-thread-per-cell kernels, 0 on
  * the generic colour-pass kernel; results are bit-identical either way. */
 #define PYRO_OPT_J1_KERNEL 1
+/* PYRO_OPT_CYCLE_KERNEL: 1 sweeps J1-only systems with the
+ * cluster-resident kernel (one thread-block cluster per replica runs every
+ * colour pass of a call, so the replica stays in L2), 0 (default) with one
+ * launch per colour pass. PYRO_OPT_CLUSTER_SIZE: CTAs per cluster (2, 4, 8, 16; the
+ * context falls back to the largest size that can be resident). */
+#define PYRO_OPT_CYCLE_KERNEL 2
+#define PYRO_OPT_CLUSTER_SIZE 3
 int pyro_set_option(pyro_ctx* ctx, int option, int value);
+int pyro_get_option(pyro_ctx* ctx, int option, int* value);
+/* Autotuner: times every kernel variant (per-pass generic, per-pass J1,
+ * cluster-resident J1 with cluster sizes 16/8/4) on
+ * `cycles` cycles of n_metro + n_or sweeps (+ exchange when the context holds
+ * the whole ladder) and keeps the fastest; *chosen = its index. The timed
+ * cycles are real Monte Carlo steps and advance the chain. */
+int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen);
 
 /* Stream used by every call (default: a stream the context creates). */
 int pyro_set_stream(pyro_ctx* ctx, void* cuda_stream);

@@ -269,3 +269,44 @@ def test_mixed_j1_and_further_neighbour_systems():
         assert np.array_equal(e.get_spins(k), o.get_spins(k)), k
         np.testing.assert_allclose(e.observables(k)[0], o.observables(k)[0], rtol=1e-12)
         assert np.array_equal(e.permutation(k), o.permutation(k))
+
+
+@pytest.mark.parametrize("cs", [16, 8, 4, 2])
+def test_cluster_cycle_kernel_bit_exact(cs):
+    temps = geometric_ladder(0.03, 1.5, 5)
+    e, o = pair([System(L=8, temperatures=temps)], renorm_every=6)
+    e.set_option(e.OPT_CYCLE_KERNEL, 1)
+    e.set_option(e.OPT_CLUSTER_SIZE, cs)
+    e.init_random()
+    o.init_random()
+    c = np.linspace(-0.9, 0.9, 5).astype(np.float32)
+    e.set_cone(c)
+    o.set_cone(c)
+    e.enable_history(16)
+    e.cycle(1, 4, True, 6)
+    h = o.cycle(1, 4, True, 6, record=True)
+    assert np.array_equal(e.get_spins(), o.get_spins())
+    assert np.array_equal(e.permutation(), o.permutation())
+    np.testing.assert_allclose(e.history(), h, rtol=1e-12, atol=1e-9)
+    e.metropolis_sweep(2)
+    o.metropolis_sweep(2)
+    e.overrelax_sweep(3)
+    o.overrelax_sweep(3)
+    assert np.array_equal(e.get_spins(), o.get_spins())
+    assert np.array_equal(e.acceptance()[0], o.acceptance()[0])
+    assert e.get_option(e.OPT_CYCLE_KERNEL) == 1
+    assert e.get_option(e.OPT_CLUSTER_SIZE) <= cs
+
+
+def test_autotune_keeps_results_exact():
+    temps = geometric_ladder(0.05, 1.0, 4)
+    e, o = pair([System(L=8, temperatures=temps)])
+    e.init_random()
+    o.init_random()
+    chosen = e.autotune(1, 2, 2)
+    assert chosen >= 0
+    # every variant ran 1 + 2 cycles of (1 M + 2 OR + swap); replay the same count on the oracle
+    n_cycles = e.sweep_count() // 3
+    o.cycle(1, 2, True, n_cycles)
+    assert np.array_equal(e.get_spins(), o.get_spins())
+    assert np.array_equal(e.permutation(), o.permutation())
