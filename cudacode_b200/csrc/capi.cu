@@ -73,6 +73,10 @@ struct pyro_ctx {
   // specialised J1 kernel.
   int n_passes = 4;
   bool use_j1_kernel = true;
+  // Per-pass J1 kernel form for Metropolis / over-relaxation passes:
+  // one site per thread (true) or the 4 sites of a cell per thread.
+  bool j1_metro_site_mode = true;
+  bool j1_or_site_mode = false;
   // Cluster-resident cycle kernel for J1 systems (0 = per-pass launches).
   int cycle_kernel = 0;
   int cluster_size = 16;
@@ -167,7 +171,8 @@ int queue_sweep(pyro_ctx* ctx, bool metro, unsigned long long off, bool skip_j1 
   for (int pass = 0; pass < ctx->n_passes; ++pass) {
     for (const auto& sc : ctx->pass_j1[pass]) {
       if (skip_j1) break;
-      launch_j1_pass(j1_params(ctx, sc.first, off), sc.second, metro, ctx->stream);
+      const bool site_mode = metro ? ctx->j1_metro_site_mode : ctx->j1_or_site_mode;
+      launch_j1_pass(j1_params(ctx, sc.first, off), sc.second, metro, site_mode, ctx->stream);
       PYRO_CK_LAUNCH();
     }
     if (ctx->pass_blocks[pass] == 0) continue;
@@ -219,7 +224,7 @@ int check_cluster(pyro_ctx* ctx) {
   if (ctx->cluster_checked) return PYRO_OK;
   ctx->cluster_checked = true;
   if (!ctx->cycle_kernel) return PYRO_OK;
-  for (int cs = ctx->cluster_size; cs >= 2; cs /= 2) {
+  for (int cs = ctx->cluster_size; cs >= 1; cs = cs > 8 ? 8 : cs / 2) {
     int n = 0;
     cudaError_t e = j1_cycle_prepare(cs, &n);
     if (e == cudaSuccess && n > 0) {
@@ -656,13 +661,16 @@ int pyro_set_option(pyro_ctx* ctx, int option, int value) {
   if (option == PYRO_OPT_J1_KERNEL) {
     if (value != 0 && value != 1) return fail(ctx, PYRO_ERR_ARG, "J1 kernel option is 0 or 1");
     ctx->use_j1_kernel = value == 1;
+  } else if (option == PYRO_OPT_J1_SITE_MODE) {
+    if (value < 0 || value > 3) return fail(ctx, PYRO_ERR_ARG, "J1 site mode is 0..3");
+    ctx->j1_metro_site_mode = (value & 1) != 0;
+    ctx->j1_or_site_mode = (value & 2) != 0;
   } else if (option == PYRO_OPT_CYCLE_KERNEL) {
     if (value != 0 && value != 1) return fail(ctx, PYRO_ERR_ARG, "cycle kernel option is 0 or 1");
     ctx->cycle_kernel = value;
     ctx->cluster_checked = false;
   } else if (option == PYRO_OPT_CLUSTER_SIZE) {
-    if (value != 2 && value != 4 && value != 8 && value != 16)
-      return fail(ctx, PYRO_ERR_ARG, "cluster size is 2, 4, 8 or 16");
+    if (value < 1 || value > 16) return fail(ctx, PYRO_ERR_ARG, "cluster size is 1..16");
     ctx->cluster_size = value;
     ctx->cluster_checked = false;
   } else {
@@ -681,6 +689,9 @@ int pyro_get_option(pyro_ctx* ctx, int option, int* value) {
     case PYRO_OPT_J1_KERNEL: *value = ctx->use_j1_kernel ? 1 : 0; break;
     case PYRO_OPT_CYCLE_KERNEL: *value = ctx->cycle_kernel; break;
     case PYRO_OPT_CLUSTER_SIZE: *value = ctx->cluster_size; break;
+    case PYRO_OPT_J1_SITE_MODE:
+      *value = (ctx->j1_metro_site_mode ? 1 : 0) | (ctx->j1_or_site_mode ? 2 : 0);
+      break;
     default: return fail(ctx, PYRO_ERR_ARG, "unknown option");
   }
   return PYRO_OK;
@@ -692,8 +703,9 @@ int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen)
   if (!ctx) return PYRO_ERR_ARG;
   if (cycles < 1 || n_metro < 0 || n_or < 0 || n_metro + n_or < 1)
     return fail(ctx, PYRO_ERR_ARG, "autotune: need cycles >= 1 and at least one sweep");
-  struct Variant { int j1, cyc, cs; };
-  const Variant vs[] = {{0, 0, 16}, {1, 0, 16}, {1, 1, 16}, {1, 1, 8}, {1, 1, 4}};
+  struct Variant { int j1, cyc, cs, site; };
+  const Variant vs[] = {{0, 0, 16, 1}, {1, 0, 16, 0}, {1, 0, 16, 1}, {1, 0, 16, 3},
+                        {1, 1, 16, 1}, {1, 1, 10, 1}, {1, 1, 9, 1},  {1, 1, 8, 1}};
   const bool swap = !sharded(ctx);
   cudaEvent_t a, b;
   PYRO_CK(cudaEventCreate(&a));
@@ -705,6 +717,7 @@ int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen)
     int rc = pyro_set_option(ctx, PYRO_OPT_J1_KERNEL, vs[i].j1);
     if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_CYCLE_KERNEL, vs[i].cyc);
     if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_CLUSTER_SIZE, vs[i].cs);
+    if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_J1_SITE_MODE, vs[i].site);
     if (!rc) rc = check_cluster(ctx);
     if (rc) continue;
     if (vs[i].cyc && (ctx->cycle_kernel != 1 || ctx->cluster_size != vs[i].cs)) continue;
@@ -727,6 +740,7 @@ int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen)
   int rc = pyro_set_option(ctx, PYRO_OPT_J1_KERNEL, w.j1);
   if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_CYCLE_KERNEL, w.cyc);
   if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_CLUSTER_SIZE, w.cs);
+  if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_J1_SITE_MODE, w.site);
   if (chosen) *chosen = best_i;
   return rc;
 }

@@ -176,6 +176,60 @@ __global__ void __launch_bounds__(kJ1Threads) j1_pass_kernel(const J1PassParams 
   }
 }
 
+// Same pass, one site per thread: blockIdx.y is the FCC corner f (so site
+// S = 4 f + B is uniform in a CTA), blockIdx.z the replica. Fewer live
+// registers than the cell-per-thread form, hence more warps in flight; the
+// Metropolis pass (Philox, cone, exp) is latency-bound without them.
+template <int B, bool kMetro>
+__global__ void __launch_bounds__(kJ1Threads) j1_site_pass_kernel(const J1PassParams p) {
+  const int f = blockIdx.y;
+  const int rep = blockIdx.z;
+  const int cell = blockIdx.x * kJ1Threads + threadIdx.x;
+  const int g = p.rep_global + rep;
+  float beta = 0.0f, cosmax = 0.0f;
+  int t = 0;
+  if (kMetro) {
+    t = p.temp_of_rep[p.temp_base + g];
+    beta = p.beta[p.temp_base + t];
+    cosmax = p.cosmax[p.temp_base + t];
+  }
+  int acc = 0;
+  if (cell < p.L3) {
+    int x, y, z;
+    decode_cell(cell, p.L, p.rcpL, &x, &y, &z);
+    const CellFrame fr = make_frame(x, y, z, p.L);
+    float4* rb = p.spins + (long long)rep * 16 * p.L3;
+    const unsigned long long sweep = (p.sweep_ctr ? *p.sweep_ctr : 0ull) + p.sweep_off;
+    const bool renorm =
+        p.renorm_every > 0 && ((sweep + 1) % (unsigned long long)p.renorm_every) == 0;
+    const uint32_t rkey = (uint32_t)(p.rep_key + rep);
+    const uint32_t sw = (uint32_t)sweep;
+    switch (f) {
+      case 0:
+        acc = update_site<B, kMetro>(rb, fr, cell, p.L3, p.J1, beta, cosmax, rkey, sw, renorm,
+                                     p.seed_lo, p.seed_hi);
+        break;
+      case 1:
+        acc = update_site<4 + B, kMetro>(rb, fr, cell, p.L3, p.J1, beta, cosmax, rkey, sw, renorm,
+                                         p.seed_lo, p.seed_hi);
+        break;
+      case 2:
+        acc = update_site<8 + B, kMetro>(rb, fr, cell, p.L3, p.J1, beta, cosmax, rkey, sw, renorm,
+                                         p.seed_lo, p.seed_hi);
+        break;
+      default:
+        acc = update_site<12 + B, kMetro>(rb, fr, cell, p.L3, p.J1, beta, cosmax, rkey, sw,
+                                          renorm, p.seed_lo, p.seed_hi);
+        break;
+    }
+  }
+  if (kMetro) {
+    const int n = __syncthreads_count(acc);
+    if (threadIdx.x == 0 && n > 0)
+      atomicAdd(p.accepted + p.temp_base + t, (unsigned long long)n);
+  }
+}
+
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -434,12 +488,19 @@ __global__ void __launch_bounds__(kJ1CycleThreads, 1)
 
 }  // namespace
 
-void launch_j1_pass(const J1PassParams& p, int colour, bool metro, cudaStream_t st) {
+void launch_j1_pass(const J1PassParams& p, int colour, bool metro, bool site_per_thread,
+                    cudaStream_t st) {
   const dim3 grid((p.L3 + kJ1Threads - 1) / kJ1Threads, p.n_rep);
+  const dim3 sgrid((p.L3 + kJ1Threads - 1) / kJ1Threads, 4, p.n_rep);
 #define PYRO_J1_CASE(B)                                                          \
   case B:                                                                        \
-    if (metro) j1_pass_kernel<B, true><<<grid, kJ1Threads, 0, st>>>(p);          \
-    else j1_pass_kernel<B, false><<<grid, kJ1Threads, 0, st>>>(p);               \
+    if (site_per_thread) {                                                       \
+      if (metro) j1_site_pass_kernel<B, true><<<sgrid, kJ1Threads, 0, st>>>(p);  \
+      else j1_site_pass_kernel<B, false><<<sgrid, kJ1Threads, 0, st>>>(p);       \
+    } else {                                                                     \
+      if (metro) j1_pass_kernel<B, true><<<grid, kJ1Threads, 0, st>>>(p);        \
+      else j1_pass_kernel<B, false><<<grid, kJ1Threads, 0, st>>>(p);             \
+    }                                                                            \
     break;
   switch (colour) {
     PYRO_J1_CASE(0)

@@ -50,7 +50,10 @@ struct J1CycleParams {
   int partial_begin;
 };
 
-void launch_j1_pass(const J1PassParams& p, int colour, bool metro, cudaStream_t st);
+// site_per_thread: one site per thread (more warps in flight) instead of the
+// 4 sites of a cell per thread; identical results.
+void launch_j1_pass(const J1PassParams& p, int colour, bool metro, bool site_per_thread,
+                    cudaStream_t st);
 cudaError_t launch_j1_cycle(const J1CycleParams& p, cudaStream_t st);
 // Sets the kernel's cluster attributes; reports how many clusters of this
 // size can be resident at once (0: size not supported).

@@ -82,10 +82,15 @@ int pyro_neighbour_table(int site, int* out120);
  * context falls back to the largest size that can be resident). */
 #define PYRO_OPT_CYCLE_KERNEL 2
 #define PYRO_OPT_CLUSTER_SIZE 3
+/* PYRO_OPT_J1_SITE_MODE: bit 0 = Metropolis passes, bit 1 = over-relaxation
+ * passes of the per-pass J1 kernel run one site per thread (set) or the four
+ * sites of a cell per thread (clear). Default 1. */
+#define PYRO_OPT_J1_SITE_MODE 4
 int pyro_set_option(pyro_ctx* ctx, int option, int value);
 int pyro_get_option(pyro_ctx* ctx, int option, int* value);
 /* Autotuner: times every kernel variant (per-pass generic, per-pass J1,
- * cluster-resident J1 with cluster sizes 16/8/4) on
+ * per-pass J1 in its site/cell forms, cluster-resident J1 with cluster sizes
+ * 16, 10, 9, 8) on
  * `cycles` cycles of n_metro + n_or sweeps (+ exchange when the context holds
  * the whole ladder) and keeps the fastest; *chosen = its index. The timed
  * cycles are real Monte Carlo steps and advance the chain. */

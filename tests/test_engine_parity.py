@@ -231,11 +231,12 @@ def test_check_spins_flags_planted_nan():
     assert e.check_spins() == 5 * 27 + 7
 
 
-@pytest.mark.parametrize("specialised", [0, 1])
-def test_j1_kernel_variants_bit_exact(specialised):
+@pytest.mark.parametrize("specialised,site_mode", [(0, 0), (1, 0), (1, 1), (1, 2), (1, 3)])
+def test_j1_kernel_variants_bit_exact(specialised, site_mode):
     temps = geometric_ladder(0.05, 1.0, 3)
     e, o = pair([System(L=6, temperatures=temps)], renorm_every=3)
     e.set_option(e.OPT_J1_KERNEL, specialised)
+    e.set_option(e.OPT_J1_SITE_MODE, site_mode)
     e.init_random()
     o.init_random()
     c = np.array([0.6, 0.1, -0.7], dtype=np.float32)
