@@ -20,6 +20,7 @@
 #include "j1_kernels.cuh"
 #include "kernels.cuh"
 #include "lattice.h"
+#include "sq_kernels.cuh"
 
 using namespace pyro;
 
@@ -96,6 +97,14 @@ struct pyro_ctx {
   unsigned long long* d_history_count = nullptr;
 
   std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;
+
+  // Structure-factor scratch, grown on demand.
+  double2* d_sq_s1 = nullptr;
+  double2* d_sq_s2 = nullptr;
+  double2* d_sq_s3 = nullptr;
+  double2* d_sq_tw = nullptr;
+  double* d_sq_out = nullptr;
+  size_t sq_s1 = 0, sq_s2 = 0, sq_s3 = 0, sq_tw = 0, sq_out = 0;
 };
 
 namespace {
@@ -315,7 +324,9 @@ void free_all(pyro_ctx* c) {
                   c->d_swap_acc,    c->d_swap_try,     c->d_swap_count,  c->d_last_accepted,
                   c->d_energy,      c->d_mag,          c->d_rep_sys,     c->d_rep_local,
                   c->d_obs_segs,    c->d_partials,     c->d_sweep,       c->d_scratch_u64,
-                  c->d_history,     c->d_history_count, c->d_obs_generic};
+                  c->d_history,     c->d_history_count, c->d_obs_generic,
+                  c->d_sq_s1,       c->d_sq_s2,        c->d_sq_s3,       c->d_sq_tw,
+                  c->d_sq_out};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto* p : c->d_pass_segs)
@@ -1152,13 +1163,63 @@ int pyro_check_spins(pyro_ctx* ctx, float tol, long long* first_bad) {
   return PYRO_OK;
 }
 
+static int grow(pyro_ctx* ctx, double2** p, size_t* cap, size_t n) {
+  if (n <= *cap && *p) return PYRO_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  cudaError_t e = cudaMalloc((void**)p, sizeof(double2) * n);
+  if (e != cudaSuccess)
+    return fail(ctx, e == cudaErrorMemoryAllocation ? PYRO_ERR_NOMEM : PYRO_ERR_CUDA,
+                std::string("structure factor scratch: ") + cudaGetErrorString(e));
+  *cap = n;
+  return PYRO_OK;
+}
+
 int pyro_structure_factor(pyro_ctx* ctx, int system, int replica, int G, int stride, double* out) {
-  (void)system;
-  (void)replica;
-  (void)G;
-  (void)stride;
-  (void)out;
-  return fail(ctx, PYRO_ERR_STATE, "structure_factor: not available in this build");
+  if (!ctx) return PYRO_ERR_ARG;
+  if (system < 0 || system >= (int)ctx->sys.size() || !out)
+    return fail(ctx, PYRO_ERR_ARG, "structure_factor: bad system or null pointer");
+  const SysDev& sd = ctx->sys[system];
+  if (G < 2 || G > 256 || (G & 1) || stride < 1 || stride > 4 * sd.L)
+    return fail(ctx, PYRO_ERR_ARG, "structure_factor: need even 2 <= G <= 256, 1 <= stride <= 4L");
+  if (replica < -1 || replica >= sd.n_rep)
+    return fail(ctx, PYRO_ERR_ARG, "structure_factor: replica out of range");
+  PYRO_CK(cudaSetDevice(ctx->device));
+  const int L = sd.L;
+  const size_t G3 = (size_t)G * G * G;
+  int rc = grow(ctx, &ctx->d_sq_s1, &ctx->sq_s1, (size_t)48 * L * L * G);
+  if (!rc) rc = grow(ctx, &ctx->d_sq_s2, &ctx->sq_s2, (size_t)48 * L * G * G);
+  if (!rc) rc = grow(ctx, &ctx->d_sq_s3, &ctx->sq_s3, (size_t)48 * G3);
+  if (!rc) rc = grow(ctx, &ctx->d_sq_tw, &ctx->sq_tw, (size_t)4 * L);
+  if (!rc) rc = grow(ctx, (double2**)&ctx->d_sq_out, &ctx->sq_out, (G3 + 1) / 2);
+  if (rc) return rc;
+  std::vector<double2> tw(4 * L);
+  for (int j = 0; j < 4 * L; ++j) {
+    const double ang = -2.0 * M_PI * (double)j / (4.0 * L);
+    tw[j] = make_double2(std::cos(ang), std::sin(ang));
+  }
+  PYRO_CK(cudaMemcpyAsync(ctx->d_sq_tw, tw.data(), sizeof(double2) * tw.size(),
+                          cudaMemcpyHostToDevice, ctx->stream));
+  PYRO_CK(cudaMemsetAsync(ctx->d_sq_out, 0, sizeof(double) * G3, ctx->stream));
+  SqParams p;
+  p.L = L;
+  p.G = G;
+  p.stride = stride;
+  p.tw = ctx->d_sq_tw;
+  for (int s = 0; s < 16; ++s) site_pos4(s, &p.pos4[3 * s]);
+  const int r0 = replica < 0 ? 0 : replica, r1 = replica < 0 ? sd.n_rep : replica + 1;
+  p.inv_n_norm = 1.0 / ((double)16 * sd.L3 * (double)(r1 - r0));
+  for (int r = r0; r < r1; ++r) {
+    launch_structure_factor_replica(ctx->d_spins + sd.spin_off + (long long)r * 16 * sd.L3, p,
+                                    ctx->d_sq_s1, ctx->d_sq_s2, ctx->d_sq_s3, ctx->d_sq_out,
+                                    ctx->stream);
+    PYRO_CK_LAUNCH();
+  }
+  PYRO_CK(cudaMemcpyAsync(out, ctx->d_sq_out, sizeof(double) * G3, cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  return PYRO_OK;
 }
 
 }  // extern "C"

@@ -48,6 +48,7 @@ def load() -> C.CDLL:
         "orc_get_permutation": (None, [P, i, pi]),
         "orc_get_swap_stats": (None, [P, i, pu64, pu64]),
         "orc_sweep_count": (C.c_uint64, [P]),
+        "orc_structure_factor": (None, [P, i, i, i, i, pd]),
         "orc_neighbours": (None, [i, pi]),
         "orc_philox": (None, [pu32, pu32, pu32]),
         "orc_expf": (f, [f]),
@@ -181,6 +182,11 @@ class Oracle:
         t = np.zeros(n, dtype=np.uint64)
         self.lib.orc_get_swap_stats(self.h, system, _p(a, C.c_uint64), _p(t, C.c_uint64))
         return a, t
+
+    def structure_factor(self, G, stride=1, replica=-1, system=0):
+        out = np.empty((G, G, G))
+        self.lib.orc_structure_factor(self.h, system, replica, G, stride, _p(out, C.c_double))
+        return out
 
     def sweep_count(self):
         return int(self.lib.orc_sweep_count(self.h))

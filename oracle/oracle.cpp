@@ -631,6 +631,44 @@ void orc_get_swap_stats(void* p, int si, uint64_t* acc, uint64_t* tried) {
 
 uint64_t orc_sweep_count(void* p) { return ((Oracle*)p)->sweep; }
 
+// Static structure factor by the direct sum over sites (Math.cu:721-741 sums
+// |m_q|^2 over components after the FFT; positions Pyrochlore.cu:1339-1401):
+// S(q) = (1/N) sum_a |sum_i S_i^a exp(-i q.r_i)|^2, q = (2 pi/L) stride (h,k,l),
+// averaged over the chosen replicas; out[((h+G/2) G + (k+G/2)) G + (l+G/2)].
+void orc_structure_factor(void* p, int si, int replica, int G, int stride, double* out) {
+  Oracle& o = *(Oracle*)p;
+  const Sys& S = o.sys[si];
+  const int r0 = replica < 0 ? 0 : replica, r1 = replica < 0 ? S.R : replica + 1;
+  const long long N = 16ll * S.L3;
+  const long long G3 = (long long)G * G * G;
+#pragma omp parallel for schedule(dynamic)
+  for (long long q = 0; q < G3; ++q) {
+    const int hi = (int)(q / (G * G)), ki = (int)((q / G) % G), li = (int)(q % G);
+    const double th = 2.0 * M_PI * stride / S.L;
+    const double qx = th * (hi - G / 2), qy = th * (ki - G / 2), qz = th * (li - G / 2);
+    double acc = 0.0;
+    for (int r = r0; r < r1; ++r) {
+      double re[3] = {0, 0, 0}, im[3] = {0, 0, 0};
+      for (long long i = 0; i < N; ++i) {
+        const int s = (int)(i / S.L3), cell = (int)(i % S.L3);
+        const int x = cell % S.L, y = (cell / S.L) % S.L, z = cell / (S.L * S.L);
+        int p4[3];
+        pos4(s, p4);
+        const double ang = -(qx * (x + p4[0] / 4.0) + qy * (y + p4[1] / 4.0) + qz * (z + p4[2] / 4.0));
+        const double c = std::cos(ang), sn = std::sin(ang);
+        const size_t j = 4 * (S.spin_off + (size_t)r * N + (size_t)i);
+        for (int a = 0; a < 3; ++a) {
+          const double v = o.fp64 ? o.s64[j + a] : (double)o.s32[j + a];
+          re[a] += v * c;
+          im[a] += v * sn;
+        }
+      }
+      for (int a = 0; a < 3; ++a) acc += re[a] * re[a] + im[a] * im[a];
+    }
+    out[q] = acc / ((double)N * (r1 - r0));
+  }
+}
+
 // Geometry export: out[k*4 + {0,1,2,3}] = dx, dy, dz, t for k < 30.
 void orc_neighbours(int s, int* out) {
   static const auto nb = build_geometry();

@@ -311,3 +311,22 @@ def test_autotune_keeps_results_exact():
     o.cycle(1, 2, True, n_cycles)
     assert np.array_equal(e.get_spins(), o.get_spins())
     assert np.array_equal(e.permutation(), o.permutation())
+
+
+@pytest.mark.parametrize("L,G,stride,replica", [(4, 8, 1, -1), (4, 16, 1, 0), (6, 6, 4, 1),
+                                               (3, 12, 1, -1)])
+def test_structure_factor_matches_direct_sum(L, G, stride, replica):
+    s = System(L=L, temperatures=[0.2, 0.6, 1.4], J2=0.05 if L == 3 else 0.0)
+    e, o = pair([s])
+    e.init_random()
+    o.init_random()
+    e.cycle(1, 2, True, 3)
+    o.cycle(1, 2, True, 3)
+    a = e.structure_factor(G, stride, replica)
+    b = o.structure_factor(G, stride, replica)
+    np.testing.assert_allclose(a, b, rtol=1e-9, atol=1e-9)
+    if stride == 1 and G == 4 * L:
+        spins = e.get_spins()[..., :3].astype(np.float64)
+        sel = spins if replica < 0 else spins[replica:replica + 1]
+        assert a.sum() == pytest.approx((4 * L) ** 3 * (sel ** 2).sum() / (16 * L ** 3) /
+                                        sel.shape[0], rel=1e-9)

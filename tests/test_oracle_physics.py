@@ -95,3 +95,32 @@ def test_fp32_oracle_deterministic():
         return o.get_spins()
     a, b = run(), run()
     assert np.array_equal(a, b)
+
+
+def test_structure_factor_ferromagnet_and_sum_rule():
+    L = 2
+    o = Oracle([System(L=L, temperatures=[1.0])], fp64=True)
+    set_spins(o, L, lambda s: (0.0, 1.0, 0.0))
+    sq = o.structure_factor(G=4, stride=1)
+    N = 16 * L ** 3
+    # q = 0 carries |M|^2 / N = N; other q of the cubic grid with all four
+    # FCC corners in phase vanish unless a reciprocal-lattice vector of the FCC
+    assert sq[2, 2, 2] == pytest.approx(N)
+    assert (sq >= -1e-9).all()
+
+
+def test_structure_factor_sum_rule_over_full_zone():
+    """sum over the L^3 wave vectors of one cubic zone, times the 64 basis
+    translations of the extended zone (stride 1, G = 4L covers 4 zones per
+    axis), equals sum_i |S_i|^2 * (4L)^3 / N-normalisation: the Parseval
+    identity for a lattice with basis on the 4L grid."""
+    L = 2
+    o = Oracle([System(L=L, temperatures=[1.0])], fp64=True, seed=3)
+    o.init_random()
+    G = 4 * L
+    sq = o.structure_factor(G=G, stride=1)
+    # positions are multiples of a/4: on the (4L)^3 grid the DFT is unitary,
+    # sum_q |F(q)|^2 = (4L)^3 sum_i |S_i|^2, and S = |F|^2 / N.
+    N = 16 * L ** 3
+    s = o.get_spins64()[..., :3]
+    assert sq.sum() == pytest.approx((4 * L) ** 3 * (s ** 2).sum() / N, rel=1e-9)
