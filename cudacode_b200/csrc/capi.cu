@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/pyro.h"
+#include "ctx.h"
 #include "j1_kernels.cuh"
 #include "kernels.cuh"
 #include "lattice.h"
@@ -24,109 +25,7 @@
 
 using namespace pyro;
 
-struct pyro_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  std::string err;
-  uint64_t seed = 0;
-  int renorm_every = 0;
-  NbrTable tab;
-
-  std::vector<SysDev> sys;
-  std::vector<std::vector<double>> ladders;
-  SysDev* d_sys = nullptr;
-  int total_temps = 0;
-  int total_reps = 0;  // replicas held
-
-  float4* d_spins = nullptr;
-  long long n_spins = 0;
-
-  int* d_temp_of_rep = nullptr;
-  int* d_rep_of_temp = nullptr;
-  float* d_beta = nullptr;
-  double* d_beta64 = nullptr;
-  float* d_cosmax = nullptr;
-  unsigned long long* d_accepted = nullptr;
-  unsigned long long* d_swap_acc = nullptr;
-  unsigned long long* d_swap_try = nullptr;
-  unsigned long long* d_swap_count = nullptr;
-  int* d_last_accepted = nullptr;
-
-  double* d_energy = nullptr;
-  double* d_mag = nullptr;
-  int* d_rep_sys = nullptr;
-  int* d_rep_local = nullptr;
-
-  // Observables: obs_segs covers every system in the global partial
-  // numbering (read by the finalise kernel); obs_generic is the subset run by
-  // the generic kernel (launch-local block_begin, global partial_begin);
-  // J1-only systems on the specialised path are listed in obs_j1.
-  std::vector<ObsSeg> obs_segs, obs_generic;
-  std::vector<int> obs_j1;
-  ObsSeg* d_obs_segs = nullptr;
-  ObsSeg* d_obs_generic = nullptr;
-  int obs_generic_blocks = 0;
-  int partials_cap = 0;
-  double4* d_partials = nullptr;
-
-  // Colour passes: generic segments, plus (system, colour) launches of the
-  // specialised J1 kernel.
-  int n_passes = 4;
-  bool use_j1_kernel = true;
-  // Per-pass J1 kernel form for Metropolis / over-relaxation passes:
-  // one site per thread (true) or the 4 sites of a cell per thread.
-  bool j1_metro_site_mode = true;
-  bool j1_or_site_mode = false;
-  // Cluster-resident cycle kernel for J1 systems (0 = per-pass launches).
-  int cycle_kernel = 0;
-  int cluster_size = 16;
-  bool cluster_checked = false;
-  std::vector<std::vector<PassSeg>> pass_segs;
-  std::vector<std::vector<std::pair<int, int>>> pass_j1;
-  std::vector<PassSeg*> d_pass_segs;
-  std::vector<int> pass_blocks;
-
-  unsigned long long* d_sweep = nullptr;
-  unsigned long long h_sweep = 0;
-  unsigned long long metro_sweeps_since_reset = 0;
-  unsigned long long* d_scratch_u64 = nullptr;
-
-  double* d_history = nullptr;
-  int history_cap = 0;
-  unsigned long long* d_history_count = nullptr;
-
-  std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;
-
-  // Structure-factor scratch, grown on demand.
-  double2* d_sq_s1 = nullptr;
-  double2* d_sq_s2 = nullptr;
-  double2* d_sq_s3 = nullptr;
-  double2* d_sq_tw = nullptr;
-  double* d_sq_out = nullptr;
-  size_t sq_s1 = 0, sq_s2 = 0, sq_s3 = 0, sq_tw = 0, sq_out = 0;
-};
-
 namespace {
-
-int fail(pyro_ctx* c, int code, const std::string& msg) {
-  if (c) c->err = msg;
-  return code;
-}
-
-#define PYRO_CK(call)                                                                   \
-  do {                                                                                  \
-    cudaError_t e_ = (call);                                                            \
-    if (e_ != cudaSuccess)                                                              \
-      return fail(ctx, PYRO_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-  } while (0)
-
-#define PYRO_CK_LAUNCH()                                                                \
-  do {                                                                                  \
-    cudaError_t e_ = cudaGetLastError();                                                \
-    if (e_ != cudaSuccess)                                                              \
-      return fail(ctx, PYRO_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
-  } while (0)
 
 template <typename T>
 cudaError_t alloc(T** p, size_t n) {
@@ -317,6 +216,7 @@ bool sharded(const pyro_ctx* ctx) {
 }
 
 void free_all(pyro_ctx* c) {
+  tet_free(c);
   for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
   c->graphs.clear();
   void* ptrs[] = {c->d_sys,         c->d_spins,        c->d_temp_of_rep, c->d_rep_of_temp,
@@ -1094,23 +994,29 @@ int pyro_get_history(pyro_ctx* ctx, int system, double* out, int* n_cycles) {
   return PYRO_OK;
 }
 
-int pyro_cycle(pyro_ctx* ctx, int n_metro, int n_or, int do_swap, int n_cycles) {
+static int run_cycles(pyro_ctx* ctx, int n_metro, int n_or, int n_tet, int do_swap, int n_cycles) {
   if (!ctx) return PYRO_ERR_ARG;
-  if (n_metro < 0 || n_or < 0 || n_cycles < 0)
+  if (n_metro < 0 || n_or < 0 || n_tet < 0 || n_cycles < 0)
     return fail(ctx, PYRO_ERR_ARG, "cycle: counts must be >= 0");
   if (do_swap && sharded(ctx))
     return fail(ctx, PYRO_ERR_STATE,
                 "cycle: a sharded context exchanges through pyro_pt_swap_global");
+  if (n_tet > 0 && !ctx->tet)
+    return fail(ctx, PYRO_ERR_STATE, "cycle: learned moves need pyro_tet_init first");
   if (n_cycles == 0) return PYRO_OK;
   PYRO_CK(cudaSetDevice(ctx->device));
-  const auto key = std::make_tuple(n_metro, n_or, do_swap ? 1 : 0);
+  const auto key = std::make_tuple(n_metro, n_or, n_tet, do_swap ? 1 : 0);
   auto it = ctx->graphs.find(key);
   if (it == ctx->graphs.end()) {
     cudaGraph_t g;
     int rc = check_cluster(ctx);  // sets kernel attributes: not inside a capture
     if (rc) return rc;
     PYRO_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    rc = queue_cycle_body(ctx, n_metro, n_or, true);
+    rc = queue_cycle_body(ctx, n_metro, n_or, n_tet == 0);
+    if (rc == PYRO_OK && n_tet > 0) {
+      rc = queue_tet_sweeps(ctx, n_tet);
+      if (rc == PYRO_OK) rc = queue_observables(ctx);
+    }
     if (rc == PYRO_OK) {
       ExchangeParams x = exchange_params(ctx);
       x.do_swap = do_swap ? 1 : 0;
@@ -1135,7 +1041,16 @@ int pyro_cycle(pyro_ctx* ctx, int n_metro, int n_or, int do_swap, int n_cycles) 
   for (int c = 0; c < n_cycles; ++c) PYRO_CK(cudaGraphLaunch(it->second, ctx->stream));
   ctx->h_sweep += (unsigned long long)(n_metro + n_or) * n_cycles;
   ctx->metro_sweeps_since_reset += (unsigned long long)n_metro * n_cycles;
+  if (n_tet > 0) tet_count_sweeps(ctx, (unsigned long long)n_tet * n_cycles);
   return PYRO_OK;
+}
+
+int pyro_cycle(pyro_ctx* ctx, int n_metro, int n_or, int do_swap, int n_cycles) {
+  return run_cycles(ctx, n_metro, n_or, 0, do_swap, n_cycles);
+}
+
+int pyro_cycle_tet(pyro_ctx* ctx, int n_metro, int n_or, int n_tet, int do_swap, int n_cycles) {
+  return run_cycles(ctx, n_metro, n_or, n_tet, do_swap, n_cycles);
 }
 
 int pyro_get_sweep_count(pyro_ctx* ctx, uint64_t* sweeps) {

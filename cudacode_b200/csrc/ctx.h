@@ -1,0 +1,132 @@
+// The engine context (one per GPU) shared by the C-ABI translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <tuple>
+#include <utility>
+#include <vector>
+
+#include "../../include/pyro.h"
+#include "kernels.cuh"
+#include "lattice.h"
+
+namespace pyro {
+struct TetState;  // learned tetrahedron move (tet_capi.cu)
+}
+
+struct pyro_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+  uint64_t seed = 0;
+  int renorm_every = 0;
+  pyro::NbrTable tab;
+
+  std::vector<pyro::SysDev> sys;
+  std::vector<std::vector<double>> ladders;
+  pyro::SysDev* d_sys = nullptr;
+  int total_temps = 0;
+  int total_reps = 0;  // replicas held
+
+  float4* d_spins = nullptr;
+  long long n_spins = 0;
+
+  int* d_temp_of_rep = nullptr;
+  int* d_rep_of_temp = nullptr;
+  float* d_beta = nullptr;
+  double* d_beta64 = nullptr;
+  float* d_cosmax = nullptr;
+  unsigned long long* d_accepted = nullptr;
+  unsigned long long* d_swap_acc = nullptr;
+  unsigned long long* d_swap_try = nullptr;
+  unsigned long long* d_swap_count = nullptr;
+  int* d_last_accepted = nullptr;
+
+  double* d_energy = nullptr;
+  double* d_mag = nullptr;
+  int* d_rep_sys = nullptr;
+  int* d_rep_local = nullptr;
+
+  // Observables: obs_segs covers every system in the global partial
+  // numbering (read by the finalise kernel); obs_generic is the subset run by
+  // the generic kernel (launch-local block_begin, global partial_begin);
+  // J1-only systems on the specialised path are listed in obs_j1.
+  std::vector<pyro::ObsSeg> obs_segs, obs_generic;
+  std::vector<int> obs_j1;
+  pyro::ObsSeg* d_obs_segs = nullptr;
+  pyro::ObsSeg* d_obs_generic = nullptr;
+  int obs_generic_blocks = 0;
+  int partials_cap = 0;
+  double4* d_partials = nullptr;
+
+  // Colour passes: generic segments, plus (system, colour) launches of the
+  // specialised J1 kernel.
+  int n_passes = 4;
+  bool use_j1_kernel = true;
+  // Per-pass J1 kernel form for Metropolis / over-relaxation passes:
+  // one site per thread (true) or the 4 sites of a cell per thread.
+  bool j1_metro_site_mode = true;
+  bool j1_or_site_mode = false;
+  // Cluster-resident cycle kernel for J1 systems (0 = per-pass launches).
+  int cycle_kernel = 0;
+  int cluster_size = 16;
+  bool cluster_checked = false;
+  std::vector<std::vector<pyro::PassSeg>> pass_segs;
+  std::vector<std::vector<std::pair<int, int>>> pass_j1;
+  std::vector<pyro::PassSeg*> d_pass_segs;
+  std::vector<int> pass_blocks;
+
+  unsigned long long* d_sweep = nullptr;
+  unsigned long long h_sweep = 0;
+  unsigned long long metro_sweeps_since_reset = 0;
+  unsigned long long* d_scratch_u64 = nullptr;
+
+  double* d_history = nullptr;
+  int history_cap = 0;
+  unsigned long long* d_history_count = nullptr;
+
+  std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs;
+
+  // Structure-factor scratch, grown on demand.
+  double2* d_sq_s1 = nullptr;
+  double2* d_sq_s2 = nullptr;
+  double2* d_sq_s3 = nullptr;
+  double2* d_sq_tw = nullptr;
+  double* d_sq_out = nullptr;
+  size_t sq_s1 = 0, sq_s2 = 0, sq_s3 = 0, sq_tw = 0, sq_out = 0;
+
+  pyro::TetState* tet = nullptr;
+};
+
+namespace pyro {
+
+inline int fail(pyro_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+// Frees the learned-move state (tet_capi.cu).
+void tet_free(pyro_ctx* ctx);
+// Queues n learned tetrahedron sweeps of every J1-only system (tet_capi.cu).
+int queue_tet_sweeps(pyro_ctx* ctx, int n);
+// Adds n to the learned-move proposal count (acceptance statistics).
+void tet_count_sweeps(pyro_ctx* ctx, unsigned long long n);
+
+}  // namespace pyro
+
+#define PYRO_CK(call)                                                                   \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return ::pyro::fail(ctx, PYRO_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define PYRO_CK_LAUNCH()                                                                \
+  do {                                                                                  \
+    cudaError_t e_ = cudaGetLastError();                                                \
+    if (e_ != cudaSuccess)                                                              \
+      return ::pyro::fail(ctx, PYRO_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+  } while (0)

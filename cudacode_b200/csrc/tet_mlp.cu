@@ -1,0 +1,844 @@
+// Learned tetrahedron proposal for the J1 pyrochlore antiferromagnet, sm_100a.
+//
+// The up-tetrahedron at FCC corner f of a cubic cell holds the sites
+// 4f..4f+3 of that cell; every other bond of those sites goes to a
+// down-tetrahedron, i.e. to up-tetrahedra of the other three corners. So the
+// tetrahedra of one corner share no bond and are moved together in one pass
+// (4 passes = one sweep over all up-tetrahedra).
+//
+// For each tetrahedron the external field of site k is h_k = J1 * (sum of its
+// three down-tetrahedron neighbours). A 16 -> 64 -> 64 -> 16 MLP (SiLU, BF16
+// weights and activations, FP32 accumulation with mma.sync m16n8k16 on the
+// tensor cores) maps (h_0..h_3 / 3, log(beta) / 3) to a von Mises-Fisher
+// distribution vMF(mu_k, kappa_k) per site. The joint proposal of the four
+// spins is independent of their current values, so the Metropolis-Hastings
+// ratio is
+//   exp(-beta (E(S') - E(S))) * q(S) / q(S'),
+//   log q(S) - log q(S') = sum_k kappa_k mu_k . (S_k - S'_k),
+// with E the exact FP32 energy of the tetrahedron (its 6 internal bonds and
+// the external fields). Detailed balance holds whatever the network outputs.
+// vMF sampling on the sphere follows Wood (1994): w = 1 + log(u + (1 - u)
+// e^{-2 kappa}) / kappa, azimuth uniform, frame of Duff et al. (2017).
+//
+// The network is trained by maximum likelihood on tetrahedron configurations
+// collected from the plain chains; the gradient kernel runs the same forward
+// pass and its backward pass on the tensor cores, one warp per 32 samples.
+// This move has no counterpart in taillefu/cudacode.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "../../include/pyro_math.h"
+#include "lattice.h"
+#include "tet_mlp.cuh"
+
+namespace pyro {
+namespace {
+
+constexpr int kTetThreads = 128;  // 4 warps x 32 tetrahedra
+constexpr int kLdIn = 24;         // padded row of 16 bf16 (48 B): conflict-free fragments
+constexpr int kLdH = 72;          // padded row of 64 bf16 (144 B)
+constexpr int kLdB = 40;          // padded row of 32 batch entries (bf16)
+constexpr int kLdOut = 17;        // padded row of 16 floats
+
+__device__ __forceinline__ uint32_t ld32(const __nv_bfloat16* p) {
+  return *reinterpret_cast<const uint32_t*>(p);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+
+// D = A * B + D, m16n8k16, BF16 inputs, FP32 accumulators.
+__device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2,
+                                         uint32_t a3, uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ float silu(float x) { return x / (1.0f + expf(-x)); }
+__device__ __forceinline__ float silu_grad(float x) {
+  const float s = 1.0f / (1.0f + expf(-x));
+  return s * (1.0f + x * (1.0f - s));
+}
+
+// Weights staged in shared memory (padded rows).
+struct MlpSmem {
+  __nv_bfloat16* w1t;  // [64][kLdIn]
+  __nv_bfloat16* w2t;  // [64][kLdH]
+  __nv_bfloat16* w3t;  // [16][kLdH]
+  __nv_bfloat16* w2;   // [64][kLdH]  (backward)
+  __nv_bfloat16* w3;   // [64][kLdIn] (backward)
+  float* b1;           // [64]
+  float* b2;           // [64]
+  float* b3;           // [16]
+};
+
+constexpr int kSmemWeightsFwd =
+    (64 * kLdIn + 64 * kLdH + 16 * kLdH) * 2 + (64 + 64 + 16) * 4;
+constexpr int kSmemWeightsAll = kSmemWeightsFwd + (64 * kLdH + 64 * kLdIn) * 2;
+
+__device__ MlpSmem carve_weights(unsigned char* base, bool backward) {
+  MlpSmem w;
+  __nv_bfloat16* b = reinterpret_cast<__nv_bfloat16*>(base);
+  w.w1t = b;
+  w.w2t = w.w1t + 64 * kLdIn;
+  w.w3t = w.w2t + 64 * kLdH;
+  __nv_bfloat16* end = w.w3t + 16 * kLdH;
+  if (backward) {
+    w.w2 = end;
+    w.w3 = w.w2 + 64 * kLdH;
+    end = w.w3 + 64 * kLdIn;
+  } else {
+    w.w2 = w.w3 = nullptr;
+  }
+  float* f = reinterpret_cast<float*>(end);
+  w.b1 = f;
+  w.b2 = f + 64;
+  w.b3 = f + 128;
+  return w;
+}
+
+__device__ void stage_weights(const MlpSmem& w, const __nv_bfloat16* __restrict__ packed,
+                              const float* __restrict__ master, bool backward) {
+  for (int i = threadIdx.x; i < 64 * 16; i += blockDim.x)
+    w.w1t[(i / 16) * kLdIn + i % 16] = packed[kPackW1t + i];
+  for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x)
+    w.w2t[(i / 64) * kLdH + i % 64] = packed[kPackW2t + i];
+  for (int i = threadIdx.x; i < 16 * 64; i += blockDim.x)
+    w.w3t[(i / 64) * kLdH + i % 64] = packed[kPackW3t + i];
+  if (backward) {
+    for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x)
+      w.w2[(i / 64) * kLdH + i % 64] = packed[kPackW2 + i];
+    for (int i = threadIdx.x; i < 64 * 16; i += blockDim.x)
+      w.w3[(i / 16) * kLdIn + i % 16] = packed[kPackW3 + i];
+  }
+  for (int i = threadIdx.x; i < 64; i += blockDim.x) {
+    w.b1[i] = master[kOffB1 + i];
+    w.b2[i] = master[kOffB2 + i];
+  }
+  for (int i = threadIdx.x; i < 16; i += blockDim.x) w.b3[i] = master[kOffB3 + i];
+}
+
+// Forward pass of one 16-row m-tile of a warp. feat: [rows][kLdIn] bf16 row
+// major (the tile starts at row r_base). Returns outputs in C-fragment
+// layout; optionally keeps pre-activations and writes activations
+// feature-major (bf16, [feature][kLdB]) for the weight-gradient GEMMs.
+struct TileFwd {
+  float o[2][4];
+  float pre1[8][4];
+  float pre2[8][4];
+};
+
+template <bool kKeep>
+__device__ __forceinline__ void tile_forward(const __nv_bfloat16* feat, int r_base, const MlpSmem& w,
+                                             TileFwd& f, __nv_bfloat16* h1t,
+                                             __nv_bfloat16* h2t) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int r0 = r_base + g, r1 = r0 + 8;
+  // layer 1: [16 x 16] x [16 x 64]
+  const uint32_t a0 = ld32(feat + r0 * kLdIn + 2 * t), a1 = ld32(feat + r1 * kLdIn + 2 * t);
+  const uint32_t a2 = ld32(feat + r0 * kLdIn + 8 + 2 * t), a3 = ld32(feat + r1 * kLdIn + 8 + 2 * t);
+  float h1[8][4];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    h1[j][0] = h1[j][2] = w.b1[8 * j + 2 * t];
+    h1[j][1] = h1[j][3] = w.b1[8 * j + 2 * t + 1];
+    const __nv_bfloat16* bw = w.w1t + (8 * j + g) * kLdIn + 2 * t;
+    mma_bf16(h1[j], a0, a1, a2, a3, ld32(bw), ld32(bw + 8));
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      if (kKeep) f.pre1[j][e] = h1[j][e];
+      h1[j][e] = silu(h1[j][e]);
+    }
+  if (kKeep) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int c = 8 * j + 2 * t;
+      h1t[c * kLdB + r0] = __float2bfloat16_rn(h1[j][0]);
+      h1t[(c + 1) * kLdB + r0] = __float2bfloat16_rn(h1[j][1]);
+      h1t[c * kLdB + r1] = __float2bfloat16_rn(h1[j][2]);
+      h1t[(c + 1) * kLdB + r1] = __float2bfloat16_rn(h1[j][3]);
+    }
+  }
+  // layer 2: [16 x 64] x [64 x 64]
+  float h2[8][4];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    h2[j][0] = h2[j][2] = w.b2[8 * j + 2 * t];
+    h2[j][1] = h2[j][3] = w.b2[8 * j + 2 * t + 1];
+  }
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk) {
+    const uint32_t x0 = pack_bf16(h1[2 * kk][0], h1[2 * kk][1]);
+    const uint32_t x1 = pack_bf16(h1[2 * kk][2], h1[2 * kk][3]);
+    const uint32_t x2 = pack_bf16(h1[2 * kk + 1][0], h1[2 * kk + 1][1]);
+    const uint32_t x3 = pack_bf16(h1[2 * kk + 1][2], h1[2 * kk + 1][3]);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const __nv_bfloat16* bw = w.w2t + (8 * j + g) * kLdH + 16 * kk + 2 * t;
+      mma_bf16(h2[j], x0, x1, x2, x3, ld32(bw), ld32(bw + 8));
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      if (kKeep) f.pre2[j][e] = h2[j][e];
+      h2[j][e] = silu(h2[j][e]);
+    }
+  if (kKeep) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int c = 8 * j + 2 * t;
+      h2t[c * kLdB + r0] = __float2bfloat16_rn(h2[j][0]);
+      h2t[(c + 1) * kLdB + r0] = __float2bfloat16_rn(h2[j][1]);
+      h2t[c * kLdB + r1] = __float2bfloat16_rn(h2[j][2]);
+      h2t[(c + 1) * kLdB + r1] = __float2bfloat16_rn(h2[j][3]);
+    }
+  }
+  // layer 3: [16 x 64] x [64 x 16]
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    f.o[j][0] = f.o[j][2] = w.b3[8 * j + 2 * t];
+    f.o[j][1] = f.o[j][3] = w.b3[8 * j + 2 * t + 1];
+  }
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk) {
+    const uint32_t x0 = pack_bf16(h2[2 * kk][0], h2[2 * kk][1]);
+    const uint32_t x1 = pack_bf16(h2[2 * kk][2], h2[2 * kk][3]);
+    const uint32_t x2 = pack_bf16(h2[2 * kk + 1][0], h2[2 * kk + 1][1]);
+    const uint32_t x3 = pack_bf16(h2[2 * kk + 1][2], h2[2 * kk + 1][3]);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const __nv_bfloat16* bw = w.w3t + (8 * j + g) * kLdH + 16 * kk + 2 * t;
+      mma_bf16(f.o[j], x0, x1, x2, x3, ld32(bw), ld32(bw + 8));
+    }
+  }
+}
+
+__device__ __forceinline__ void store_out(const TileFwd& f, int r_base, float* out) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int r0 = r_base + g, r1 = r0 + 8;
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    out[r0 * kLdOut + 8 * j + 2 * t] = f.o[j][0];
+    out[r0 * kLdOut + 8 * j + 2 * t + 1] = f.o[j][1];
+    out[r1 * kLdOut + 8 * j + 2 * t] = f.o[j][2];
+    out[r1 * kLdOut + 8 * j + 2 * t + 1] = f.o[j][3];
+  }
+}
+
+// Network outputs -> (mu_k, kappa_k) for the four sites.
+struct VmfParams {
+  pyro_vec3 mu[4];
+  float kappa[4];
+  float z[4];      // clamped log kappa
+  bool z_in[4];    // log kappa strictly inside the clamp range
+  float onorm[4];  // |o_k| before normalisation
+};
+
+__device__ __forceinline__ VmfParams vmf_params(const float* o) {
+  VmfParams v;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float x = o[4 * k], y = o[4 * k + 1], z = o[4 * k + 2];
+    float n = sqrtf(x * x + y * y + z * z);
+    pyro_vec3 m;
+    if (n > 1e-20f) {
+      m.x = x / n;
+      m.y = y / n;
+      m.z = z / n;
+    } else {
+      m.x = 0.0f;
+      m.y = 0.0f;
+      m.z = 1.0f;
+      n = 1e-20f;
+    }
+    v.mu[k] = m;
+    v.onorm[k] = n;
+    const float lz = o[4 * k + 3];
+    v.z[k] = fminf(fmaxf(lz, kLogKappaMin), kLogKappaMax);
+    v.z_in[k] = lz > kLogKappaMin && lz < kLogKappaMax;
+    v.kappa[k] = expf(v.z[k]);
+  }
+  return v;
+}
+
+// Cell frame (periodic neighbour rows), as in the J1 kernels.
+struct Frame {
+  int zo[3], yo[3], xo[3];
+};
+
+__device__ __forceinline__ Frame cell_frame(int cell, int L, float rcpL) {
+  int q = (int)((float)cell * rcpL);
+  int r = cell - q * L;
+  if (r < 0) { --q; r += L; } else if (r >= L) { ++q; r -= L; }
+  int q2 = (int)((float)q * rcpL);
+  int r2 = q - q2 * L;
+  if (r2 < 0) { --q2; r2 += L; } else if (r2 >= L) { ++q2; r2 -= L; }
+  const int x = r, y = r2, z = q2, L2 = L * L;
+  Frame f;
+  f.xo[0] = x == 0 ? L - 1 : x - 1;
+  f.xo[1] = x;
+  f.xo[2] = x == L - 1 ? 0 : x + 1;
+  f.yo[0] = (y == 0 ? L - 1 : y - 1) * L;
+  f.yo[1] = y * L;
+  f.yo[2] = (y == L - 1 ? 0 : y + 1) * L;
+  f.zo[0] = (z == 0 ? L - 1 : z - 1) * L2;
+  f.zo[1] = z * L2;
+  f.zo[2] = (z == L - 1 ? 0 : z + 1) * L2;
+  return f;
+}
+
+template <int S, int K>
+__device__ __forceinline__ float4 nbr(const float4* __restrict__ rep, const Frame& f, int L3) {
+  constexpr NbrEntry e = j1_neighbour(S, K);
+  return __ldg(rep + f.zo[e.dz + 1] + f.yo[e.dy + 1] + f.xo[e.dx + 1] + e.t * L3);
+}
+
+// External field of site S (sum of its three down-tetrahedron neighbours).
+template <int S>
+__device__ __forceinline__ pyro_vec3 ext_field(const float4* __restrict__ rep, const Frame& f,
+                                               int L3, float J1) {
+  constexpr int k0 = j1_down_index(S, 0), k1 = j1_down_index(S, 1), k2 = j1_down_index(S, 2);
+  const float4 a = nbr<S, k0>(rep, f, L3), b = nbr<S, k1>(rep, f, L3), c = nbr<S, k2>(rep, f, L3);
+  pyro_vec3 h;
+  h.x = J1 * ((a.x + b.x) + c.x);
+  h.y = J1 * ((a.y + b.y) + c.y);
+  h.z = J1 * ((a.z + b.z) + c.z);
+  return h;
+}
+
+template <int F>
+__device__ __forceinline__ void tet_fields(const float4* __restrict__ rep, const Frame& fr, int L3,
+                                           float J1, pyro_vec3 h[4]) {
+  h[0] = ext_field<4 * F + 0>(rep, fr, L3, J1);
+  h[1] = ext_field<4 * F + 1>(rep, fr, L3, J1);
+  h[2] = ext_field<4 * F + 2>(rep, fr, L3, J1);
+  h[3] = ext_field<4 * F + 3>(rep, fr, L3, J1);
+}
+
+__device__ __forceinline__ float dot3(pyro_vec3 a, pyro_vec3 b) {
+  return a.x * b.x + a.y * b.y + a.z * b.z;
+}
+
+__device__ __forceinline__ float tet_energy(const pyro_vec3 s[4], const pyro_vec3 h[4], float J1) {
+  const float bonds = dot3(s[0], s[1]) + dot3(s[0], s[2]) + dot3(s[0], s[3]) + dot3(s[1], s[2]) +
+                      dot3(s[1], s[3]) + dot3(s[2], s[3]);
+  return J1 * bonds + dot3(s[0], h[0]) + dot3(s[1], h[1]) + dot3(s[2], h[2]) + dot3(s[3], h[3]);
+}
+
+__device__ __forceinline__ void write_features(__nv_bfloat16* row, const pyro_vec3 h[4], float beta) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    row[3 * k] = __float2bfloat16_rn(h[k].x * (1.0f / 3.0f));
+    row[3 * k + 1] = __float2bfloat16_rn(h[k].y * (1.0f / 3.0f));
+    row[3 * k + 2] = __float2bfloat16_rn(h[k].z * (1.0f / 3.0f));
+  }
+  row[12] = __float2bfloat16_rn(logf(beta) * (1.0f / 3.0f));
+  row[13] = row[14] = row[15] = __float2bfloat16_rn(0.0f);
+}
+
+// vMF(mu, kappa) sample on the sphere (Wood 1994).
+__device__ __forceinline__ pyro_vec3 vmf_sample(pyro_vec3 mu, float kappa, float u, float v) {
+  float w = 1.0f + logf(u + (1.0f - u) * expf(-2.0f * kappa)) / kappa;
+  w = fminf(1.0f, fmaxf(-1.0f, w));
+  const float st = sqrtf(fmaxf(0.0f, 1.0f - w * w));
+  float sp, cp;
+  pyro_sincospif(2.0f * v, &sp, &cp);
+  return pyro_about_axis(mu, w, st, cp, sp);
+}
+
+template <int F>
+__global__ void __launch_bounds__(kTetThreads) tet_move_kernel(const TetMoveParams p) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  MlpSmem w = carve_weights(smem, false);
+  __nv_bfloat16* feat_all = reinterpret_cast<__nv_bfloat16*>(smem + kSmemWeightsFwd);
+  float* out_all = reinterpret_cast<float*>(smem + kSmemWeightsFwd + kTetThreads * kLdIn * 2);
+  stage_weights(w, p.packed, p.master, false);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __nv_bfloat16* feat = feat_all + warp * 32 * kLdIn;
+  float* out = out_all + warp * 32 * kLdOut;
+  const long long tet = (long long)blockIdx.x * kTetThreads + threadIdx.x;  // rep * L3 + cell
+  const bool active = tet < (long long)p.n_rep * p.L3;
+  const int rep = active ? (int)(tet / p.L3) : 0;
+  const int cell = active ? (int)(tet - (long long)rep * p.L3) : 0;
+  const float4* rb = p.spins + (long long)rep * 16 * p.L3;
+  const int g = p.rep_global + rep;
+  const int tslot = p.temp_of_rep[p.temp_base + g];
+  const float beta = p.beta[p.temp_base + tslot];
+  pyro_vec3 h[4], s[4];
+  if (active) {
+    const Frame fr = cell_frame(cell, p.L, p.rcpL);
+    tet_fields<F>(rb, fr, p.L3, p.J1, h);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float4 v = rb[(4 * F + k) * p.L3 + cell];
+      s[k].x = v.x;
+      s[k].y = v.y;
+      s[k].z = v.z;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      h[k].x = h[k].y = h[k].z = 0.0f;
+      s[k].x = s[k].y = 0.0f;
+      s[k].z = 1.0f;
+    }
+  }
+  write_features(feat + lane * kLdIn, h, active ? beta : 1.0f);
+  __syncthreads();  // weights staged, features written
+
+  TileFwd fw;
+  tile_forward<false>(feat, 0, w, fw, nullptr, nullptr);
+  store_out(fw, 0, out);
+  tile_forward<false>(feat, 16, w, fw, nullptr, nullptr);
+  store_out(fw, 16, out);
+  __syncwarp();
+
+  int accepted = 0;
+  if (active) {
+    float o[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) o[i] = out[lane * kLdOut + i];
+    const VmfParams vm = vmf_params(o);
+    const unsigned long long sweep = (p.tet_ctr ? *p.tet_ctr : 0ull) + p.tet_off;
+    const uint32_t key_tet = (uint32_t)(F * p.L3 + cell);
+    uint32_t r0[4], r1[4], r2[4];
+    pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + 0,
+                p.seed_lo, p.seed_hi, r0);
+    pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + 1,
+                p.seed_lo, p.seed_hi, r1);
+    pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + 2,
+                p.seed_lo, p.seed_hi, r2);
+    pyro_vec3 sn[4];
+    sn[0] = vmf_sample(vm.mu[0], vm.kappa[0], pyro_uniform(r0[0]), pyro_uniform(r0[1]));
+    sn[1] = vmf_sample(vm.mu[1], vm.kappa[1], pyro_uniform(r0[2]), pyro_uniform(r0[3]));
+    sn[2] = vmf_sample(vm.mu[2], vm.kappa[2], pyro_uniform(r1[0]), pyro_uniform(r1[1]));
+    sn[3] = vmf_sample(vm.mu[3], vm.kappa[3], pyro_uniform(r1[2]), pyro_uniform(r1[3]));
+    const float dE = tet_energy(sn, h, p.J1) - tet_energy(s, h, p.J1);
+    float log_q = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) log_q += vm.kappa[k] * (dot3(vm.mu[k], s[k]) - dot3(vm.mu[k], sn[k]));
+    const float log_r = -beta * dE + log_q;
+    accepted = log_r >= 0.0f || pyro_uniform(r2[0]) < expf(log_r);
+    if (accepted) {
+      float4* wb = p.spins + (long long)rep * 16 * p.L3;
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        wb[(4 * F + k) * p.L3 + cell] = make_float4(sn[k].x, sn[k].y, sn[k].z, 0.0f);
+    }
+  }
+  // Per-replica acceptance: a CTA may span replicas, so count per thread.
+  if (accepted) atomicAdd(p.accepted + p.temp_base + tslot, 1ull);
+}
+
+template <int F>
+__device__ __forceinline__ void collect_one(const TetCollectParams& p, int rep, int cell, float* feat,
+                                            float* targ) {
+  const float4* rb = p.spins + (long long)rep * 16 * p.L3;
+  const Frame fr = cell_frame(cell, p.L, p.rcpL);
+  pyro_vec3 h[4];
+  tet_fields<F>(rb, fr, p.L3, p.J1, h);
+  const int g = p.rep_global + rep;
+  const float beta = p.beta[p.temp_base + p.temp_of_rep[p.temp_base + g]];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    feat[3 * k] = h[k].x * (1.0f / 3.0f);
+    feat[3 * k + 1] = h[k].y * (1.0f / 3.0f);
+    feat[3 * k + 2] = h[k].z * (1.0f / 3.0f);
+    const float4 v = __ldg(rb + (4 * F + k) * p.L3 + cell);
+    targ[3 * k] = v.x;
+    targ[3 * k + 1] = v.y;
+    targ[3 * k + 2] = v.z;
+  }
+  feat[12] = logf(beta) * (1.0f / 3.0f);
+  feat[13] = feat[14] = feat[15] = 0.0f;
+}
+
+__global__ void tet_collect_kernel(const TetCollectParams p) {
+  const long long per_class_rep = (p.L3 + p.stride - 1) / p.stride;
+  const long long total = 4ll * p.n_rep * per_class_rep;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int f = (int)(i / ((long long)p.n_rep * per_class_rep));
+    const long long rest = i - (long long)f * p.n_rep * per_class_rep;
+    const int rep = (int)(rest / per_class_rep);
+    const int cell = (int)(rest - (long long)rep * per_class_rep) * p.stride;
+    const long long slot = (p.head + i) % p.cap;
+    float* feat = p.features + slot * 16;
+    float* targ = p.targets + slot * 12;
+    switch (f) {
+      case 0: collect_one<0>(p, rep, cell, feat, targ); break;
+      case 1: collect_one<1>(p, rep, cell, feat, targ); break;
+      case 2: collect_one<2>(p, rep, cell, feat, targ); break;
+      default: collect_one<3>(p, rep, cell, feat, targ); break;
+    }
+  }
+}
+
+__global__ void mlp_pack_kernel(const float* __restrict__ m, __nv_bfloat16* packed) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kPackSize; i += gridDim.x * blockDim.x) {
+    float v;
+    if (i < kPackW2t) {  // w1t[o][i] = W1[i][o]
+      const int o = i / 16, in = i % 16;
+      v = m[kOffW1 + in * 64 + o];
+    } else if (i < kPackW3t) {
+      const int j = i - kPackW2t, o = j / 64, in = j % 64;
+      v = m[kOffW2 + in * 64 + o];
+    } else if (i < kPackW2) {
+      const int j = i - kPackW3t, o = j / 64, in = j % 64;
+      v = m[kOffW3 + in * 16 + o];
+    } else if (i < kPackW3) {
+      v = m[kOffW2 + (i - kPackW2)];
+    } else {
+      v = m[kOffW3 + (i - kPackW3)];
+    }
+    packed[i] = __float2bfloat16_rn(v);
+  }
+}
+
+__global__ void __launch_bounds__(kTetThreads) mlp_forward_kernel(const float* __restrict__ features,
+                                                                  int n,
+                                                                  const __nv_bfloat16* packed,
+                                                                  const float* master, float* out) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  MlpSmem w = carve_weights(smem, false);
+  __nv_bfloat16* feat_all = reinterpret_cast<__nv_bfloat16*>(smem + kSmemWeightsFwd);
+  float* out_all = reinterpret_cast<float*>(smem + kSmemWeightsFwd + kTetThreads * kLdIn * 2);
+  stage_weights(w, packed, master, false);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __nv_bfloat16* feat = feat_all + warp * 32 * kLdIn;
+  float* o = out_all + warp * 32 * kLdOut;
+  const long long row = (long long)blockIdx.x * kTetThreads + threadIdx.x;
+  for (int i = 0; i < 16; ++i)
+    feat[lane * kLdIn + i] = __float2bfloat16_rn(row < n ? features[row * 16 + i] : 0.0f);
+  __syncthreads();
+  TileFwd fw;
+  tile_forward<false>(feat, 0, w, fw, nullptr, nullptr);
+  store_out(fw, 0, o);
+  tile_forward<false>(feat, 16, w, fw, nullptr, nullptr);
+  store_out(fw, 16, o);
+  __syncwarp();
+  if (row < n)
+    for (int i = 0; i < 16; ++i) out[row * 16 + i] = o[lane * kLdOut + i];
+}
+
+// Per-warp shared buffers of the gradient kernel.
+struct GradWarpSmem {
+  __nv_bfloat16* feat;  // [32][kLdIn] row major
+  __nv_bfloat16* xt;    // [16][kLdB]  feature major
+  __nv_bfloat16* h1t;   // [64][kLdB]
+  __nv_bfloat16* h2t;   // [64][kLdB]
+  __nv_bfloat16* dorow;  // [32][kLdIn] dL/do row major
+  __nv_bfloat16* dot;   // [16][kLdB]
+  __nv_bfloat16* da2t;  // [64][kLdB]
+  __nv_bfloat16* da1t;  // [64][kLdB]
+  float* out;           // [32][kLdOut]
+};
+constexpr int kGradWarpBytes =
+    (32 * kLdIn + 16 * kLdB + 64 * kLdB * 2 + 32 * kLdIn + 16 * kLdB + 64 * kLdB * 2) * 2 +
+    32 * kLdOut * 4;
+constexpr int kGradSmem = kSmemWeightsAll + 4 * kGradWarpBytes + kMlpParams * 4;
+
+__device__ GradWarpSmem carve_warp(unsigned char* base) {
+  GradWarpSmem s;
+  __nv_bfloat16* b = reinterpret_cast<__nv_bfloat16*>(base);
+  s.feat = b;
+  s.xt = s.feat + 32 * kLdIn;
+  s.h1t = s.xt + 16 * kLdB;
+  s.h2t = s.h1t + 64 * kLdB;
+  s.dorow = s.h2t + 64 * kLdB;
+  s.dot = s.dorow + 32 * kLdIn;
+  s.da2t = s.dot + 16 * kLdB;
+  s.da1t = s.da2t + 64 * kLdB;
+  s.out = reinterpret_cast<float*>(s.da1t + 64 * kLdB);
+  return s;
+}
+
+// sum over the 8 row groups (lanes with equal lane % 4)
+__device__ __forceinline__ float group_sum(float v) {
+  v += __shfl_xor_sync(0xffffffffu, v, 4);
+  v += __shfl_xor_sync(0xffffffffu, v, 8);
+  v += __shfl_xor_sync(0xffffffffu, v, 16);
+  return v;
+}
+
+// Weight-gradient GEMM of one warp: G[m][n] += sum_b AT[m][b] * BT[n][b],
+// AT: [M][kLdB], BT: [N][kLdB] (feature major, 32 batch entries), added to
+// the shared FP32 gradient block at `grad` with row stride n_total.
+template <int M, int N>
+__device__ __forceinline__ void weight_grad(const __nv_bfloat16* at, const __nv_bfloat16* bt,
+                                            float* grad, int n_total) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int mt = 0; mt < M / 16; ++mt) {
+    float c[N / 8][4];
+#pragma unroll
+    for (int j = 0; j < N / 8; ++j) c[j][0] = c[j][1] = c[j][2] = c[j][3] = 0.0f;
+#pragma unroll
+    for (int ks = 0; ks < 2; ++ks) {
+      const __nv_bfloat16* ar = at + (16 * mt + g) * kLdB + 16 * ks + 2 * t;
+      const uint32_t a0 = ld32(ar), a1 = ld32(ar + 8 * kLdB), a2 = ld32(ar + 8),
+                     a3 = ld32(ar + 8 * kLdB + 8);
+#pragma unroll
+      for (int j = 0; j < N / 8; ++j) {
+        const __nv_bfloat16* br = bt + (8 * j + g) * kLdB + 16 * ks + 2 * t;
+        mma_bf16(c[j], a0, a1, a2, a3, ld32(br), ld32(br + 8));
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < N / 8; ++j) {
+      const int r0 = 16 * mt + g, col = 8 * j + 2 * t;
+      atomicAdd(grad + r0 * n_total + col, c[j][0]);
+      atomicAdd(grad + r0 * n_total + col + 1, c[j][1]);
+      atomicAdd(grad + (r0 + 8) * n_total + col, c[j][2]);
+      atomicAdd(grad + (r0 + 8) * n_total + col + 1, c[j][3]);
+    }
+  }
+}
+
+// Negative log-likelihood of the targets under the vMF mixture of one sample
+// and its gradient with respect to the 16 network outputs.
+__device__ __forceinline__ float nll_and_grad(const float* o, const float* s, float* d) {
+  const VmfParams v = vmf_params(o);
+  float loss = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float kap = v.kappa[k];
+    pyro_vec3 sk;
+    sk.x = s[3 * k];
+    sk.y = s[3 * k + 1];
+    sk.z = s[3 * k + 2];
+    const float m = dot3(v.mu[k], sk);
+    const float em = -expm1f(-2.0f * kap);  // 1 - e^{-2 kappa}
+    // log f = z - log(2 pi) - log(1 - e^{-2 kappa}) + kappa (m - 1)
+    loss -= v.z[k] - 1.8378770664093453f - logf(em) + kap * (m - 1.0f);
+    const float r = 2.0f * kap / expm1f(2.0f * kap);
+    d[4 * k + 3] = v.z_in[k] ? -(1.0f - r + kap * (m - 1.0f)) : 0.0f;
+    // d/d mu = -kappa s; through mu = o / |o|
+    const float inv = 1.0f / v.onorm[k];
+    d[4 * k + 0] = -kap * (sk.x - m * v.mu[k].x) * inv;
+    d[4 * k + 1] = -kap * (sk.y - m * v.mu[k].y) * inv;
+    d[4 * k + 2] = -kap * (sk.z - m * v.mu[k].z) * inv;
+  }
+  return loss;
+}
+
+__global__ void __launch_bounds__(kTetThreads) mlp_gradient_kernel(
+    const float* __restrict__ features, const float* __restrict__ targets, const int* idx, int n,
+    const __nv_bfloat16* packed, const float* master, float* grad, double* loss_sum) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  MlpSmem w = carve_weights(smem, true);
+  unsigned char* wbase = smem + kSmemWeightsAll;
+  float* g_acc = reinterpret_cast<float*>(wbase + 4 * kGradWarpBytes);
+  stage_weights(w, packed, master, true);
+  for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) g_acc[i] = 0.0f;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  GradWarpSmem ws = carve_warp(wbase + warp * kGradWarpBytes);
+  __syncthreads();
+  float loss_local = 0.0f;
+  for (long long base = (long long)blockIdx.x * kTetThreads; base < n;
+       base += (long long)gridDim.x * kTetThreads) {
+    const long long row = base + threadIdx.x;
+    const bool valid = row < n;
+    const long long src = valid ? (idx ? (long long)idx[row] : row) : 0;
+    float tg[12];
+    for (int i = 0; i < 16; ++i) {
+      const float x = valid ? features[src * 16 + i] : 0.0f;
+      const __nv_bfloat16 xb = __float2bfloat16_rn(x);
+      ws.feat[lane * kLdIn + i] = xb;
+      ws.xt[i * kLdB + lane] = xb;
+    }
+    for (int i = 0; i < 12; ++i) tg[i] = valid ? targets[src * 12 + i] : 0.0f;
+    __syncwarp();
+    // forward + output gradient, tile by tile
+    TileFwd fw[2];
+    tile_forward<true>(ws.feat, 0, w, fw[0], ws.h1t, ws.h2t);
+    store_out(fw[0], 0, ws.out);
+    tile_forward<true>(ws.feat, 16, w, fw[1], ws.h1t, ws.h2t);
+    store_out(fw[1], 16, ws.out);
+    __syncwarp();
+    {
+      float o[16], d[16];
+      for (int i = 0; i < 16; ++i) o[i] = ws.out[lane * kLdOut + i];
+      const float l = nll_and_grad(o, tg, d);
+      if (valid) loss_local += l;
+      for (int i = 0; i < 16; ++i) {
+        const __nv_bfloat16 db = __float2bfloat16_rn(valid ? d[i] : 0.0f);
+        ws.dorow[lane * kLdIn + i] = db;
+        ws.dot[i * kLdB + lane] = db;
+        if (valid) atomicAdd(&g_acc[kOffB3 + i], d[i]);  // bias b3, FP32
+      }
+    }
+    __syncwarp();
+    // backward through layers 3 and 2, tile by tile
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+      const int r0 = 16 * mt + g, r1 = r0 + 8;
+      const uint32_t a0 = ld32(ws.dorow + r0 * kLdIn + 2 * t), a1 = ld32(ws.dorow + r1 * kLdIn + 2 * t);
+      const uint32_t a2 = ld32(ws.dorow + r0 * kLdIn + 8 + 2 * t),
+                     a3 = ld32(ws.dorow + r1 * kLdIn + 8 + 2 * t);
+      float da2[8][4];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        da2[j][0] = da2[j][1] = da2[j][2] = da2[j][3] = 0.0f;
+        const __nv_bfloat16* bw = w.w3 + (8 * j + g) * kLdIn + 2 * t;
+        mma_bf16(da2[j], a0, a1, a2, a3, ld32(bw), ld32(bw + 8));
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) da2[j][e] *= silu_grad(fw[mt].pre2[j][e]);
+        const int c = 8 * j + 2 * t;
+        ws.da2t[c * kLdB + r0] = __float2bfloat16_rn(da2[j][0]);
+        ws.da2t[(c + 1) * kLdB + r0] = __float2bfloat16_rn(da2[j][1]);
+        ws.da2t[c * kLdB + r1] = __float2bfloat16_rn(da2[j][2]);
+        ws.da2t[(c + 1) * kLdB + r1] = __float2bfloat16_rn(da2[j][3]);
+        const float s0 = group_sum(da2[j][0] + da2[j][2]), s1 = group_sum(da2[j][1] + da2[j][3]);
+        if (g == 0) {
+          atomicAdd(&g_acc[kOffB2 + c], s0);
+          atomicAdd(&g_acc[kOffB2 + c + 1], s1);
+        }
+      }
+      float da1[8][4];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) da1[j][0] = da1[j][1] = da1[j][2] = da1[j][3] = 0.0f;
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) {
+        const uint32_t x0 = pack_bf16(da2[2 * kk][0], da2[2 * kk][1]);
+        const uint32_t x1 = pack_bf16(da2[2 * kk][2], da2[2 * kk][3]);
+        const uint32_t x2 = pack_bf16(da2[2 * kk + 1][0], da2[2 * kk + 1][1]);
+        const uint32_t x3 = pack_bf16(da2[2 * kk + 1][2], da2[2 * kk + 1][3]);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const __nv_bfloat16* bw = w.w2 + (8 * j + g) * kLdH + 16 * kk + 2 * t;
+          mma_bf16(da1[j], x0, x1, x2, x3, ld32(bw), ld32(bw + 8));
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) da1[j][e] *= silu_grad(fw[mt].pre1[j][e]);
+        const int c = 8 * j + 2 * t;
+        ws.da1t[c * kLdB + r0] = __float2bfloat16_rn(da1[j][0]);
+        ws.da1t[(c + 1) * kLdB + r0] = __float2bfloat16_rn(da1[j][1]);
+        ws.da1t[c * kLdB + r1] = __float2bfloat16_rn(da1[j][2]);
+        ws.da1t[(c + 1) * kLdB + r1] = __float2bfloat16_rn(da1[j][3]);
+        const float s0 = group_sum(da1[j][0] + da1[j][2]), s1 = group_sum(da1[j][1] + da1[j][3]);
+        if (g == 0) {
+          atomicAdd(&g_acc[kOffB1 + c], s0);
+          atomicAdd(&g_acc[kOffB1 + c + 1], s1);
+        }
+      }
+    }
+    __syncwarp();
+    // weight gradients: dW1 = X^T dA1, dW2 = H1^T dA2, dW3 = H2^T dO
+    weight_grad<16, 64>(ws.xt, ws.da1t, g_acc + kOffW1, 64);
+    weight_grad<64, 64>(ws.h1t, ws.da2t, g_acc + kOffW2, 64);
+    weight_grad<64, 16>(ws.h2t, ws.dot, g_acc + kOffW3, 16);
+    __syncwarp();
+  }
+  // loss: warp sum, one atomic per warp
+  for (int o = 16; o > 0; o >>= 1) loss_local += __shfl_down_sync(0xffffffffu, loss_local, o);
+  if (lane == 0) atomicAdd(loss_sum, (double)loss_local);
+  __syncthreads();
+  for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x)
+    if (g_acc[i] != 0.0f) atomicAdd(grad + i, g_acc[i]);
+}
+
+__global__ void adam_kernel(float* w, float* m, float* v, const float* g, int n, float lr,
+                            float b1, float b2, float eps, float scale, float c1, float c2) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float gi = g[i] * scale;
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  }
+}
+
+__global__ void draw_batch_kernel(int* idx, int n, long long n_avail, uint32_t seed_lo,
+                                  uint32_t seed_hi, uint32_t step) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t r[4];
+    pyro_philox((uint32_t)i, step, 0u, PYRO_PURPOSE_TET + 8, seed_lo, seed_hi, r);
+    const unsigned long long x = ((unsigned long long)r[0] << 32) | r[1];
+    idx[i] = (int)(x % (unsigned long long)n_avail);
+  }
+}
+
+constexpr int kTetSmem = kSmemWeightsFwd + kTetThreads * kLdIn * 2 + kTetThreads * kLdOut * 4;
+
+}  // namespace
+
+void launch_mlp_pack(const float* master, __nv_bfloat16* packed, cudaStream_t st) {
+  mlp_pack_kernel<<<(kPackSize + 255) / 256, 256, 0, st>>>(master, packed);
+}
+
+void launch_tet_move(const TetMoveParams& p, int f, cudaStream_t st) {
+  const long long n = (long long)p.n_rep * p.L3;
+  const int blocks = (int)((n + kTetThreads - 1) / kTetThreads);
+  switch (f) {
+    case 0: tet_move_kernel<0><<<blocks, kTetThreads, kTetSmem, st>>>(p); break;
+    case 1: tet_move_kernel<1><<<blocks, kTetThreads, kTetSmem, st>>>(p); break;
+    case 2: tet_move_kernel<2><<<blocks, kTetThreads, kTetSmem, st>>>(p); break;
+    default: tet_move_kernel<3><<<blocks, kTetThreads, kTetSmem, st>>>(p); break;
+  }
+}
+
+long long tet_collect_count(int L3, int n_rep, int stride) {
+  return 4ll * n_rep * ((L3 + stride - 1) / stride);
+}
+
+void launch_tet_collect(const TetCollectParams& p, cudaStream_t st) {
+  const long long n = tet_collect_count(p.L3, p.n_rep, p.stride);
+  long long blocks = (n + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  tet_collect_kernel<<<(int)blocks, 256, 0, st>>>(p);
+}
+
+void launch_mlp_forward(const float* features, int n, const __nv_bfloat16* packed,
+                        const float* master, float* out, cudaStream_t st) {
+  const int blocks = (n + kTetThreads - 1) / kTetThreads;
+  mlp_forward_kernel<<<blocks, kTetThreads, kTetSmem, st>>>(features, n, packed, master, out);
+}
+
+void launch_mlp_gradient(const float* features, const float* targets, const int* idx, int n,
+                         const __nv_bfloat16* packed, const float* master, float* grad,
+                         double* loss, cudaStream_t st) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(mlp_gradient_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kGradSmem);
+    attr_set = true;
+  }
+  int blocks = (n + kTetThreads - 1) / kTetThreads;
+  if (blocks > 148 * 2) blocks = 148 * 2;
+  if (blocks < 1) blocks = 1;
+  mlp_gradient_kernel<<<blocks, kTetThreads, kGradSmem, st>>>(features, targets, idx, n, packed,
+                                                               master, grad, loss);
+}
+
+void launch_adam(float* master, float* m, float* v, const float* grad, int n, float lr,
+                 float beta1, float beta2, float eps, float scale, int step, cudaStream_t st) {
+  const float c1 = 1.0f - powf(beta1, (float)step), c2 = 1.0f - powf(beta2, (float)step);
+  adam_kernel<<<(n + 255) / 256, 256, 0, st>>>(master, m, v, grad, n, lr, beta1, beta2, eps, scale,
+                                               c1, c2);
+}
+
+void launch_draw_batch(int* idx, int n, long long n_avail, uint32_t seed_lo, uint32_t seed_hi,
+                       uint32_t step, cudaStream_t st) {
+  draw_batch_kernel<<<(n + 255) / 256, 256, 0, st>>>(idx, n, n_avail, seed_lo, seed_hi, step);
+}
+
+}  // namespace pyro

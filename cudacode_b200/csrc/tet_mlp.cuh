@@ -1,0 +1,88 @@
+// Learned tetrahedron proposal: a 16 -> 64 -> 64 -> 16 MLP (BF16 weights,
+// FP32 accumulation on the tensor cores) that maps the external fields of the
+// four spins of an up-tetrahedron (and beta) to a von Mises-Fisher
+// distribution for each of them; a joint move of the four spins drawn from it
+// is accepted with the exact Metropolis-Hastings ratio.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pyro {
+
+constexpr int kMlpIn = 16;   // 12 field components / 3, log(beta) / 3, 3 zeros
+constexpr int kMlpHidden = 64;
+constexpr int kMlpOut = 16;  // per site k: mu direction (3, unnormalised), log kappa
+// FP32 master layout (row = input feature, contiguous = output feature):
+constexpr int kOffW1 = 0;                                  // [16][64]
+constexpr int kOffB1 = kOffW1 + kMlpIn * kMlpHidden;       // [64]
+constexpr int kOffW2 = kOffB1 + kMlpHidden;                // [64][64]
+constexpr int kOffB2 = kOffW2 + kMlpHidden * kMlpHidden;   // [64]
+constexpr int kOffW3 = kOffB2 + kMlpHidden;                // [64][16]
+constexpr int kOffB3 = kOffW3 + kMlpHidden * kMlpOut;      // [16]
+constexpr int kMlpParams = kOffB3 + kMlpOut;               // 6288
+constexpr float kLogKappaMin = -4.0f, kLogKappaMax = 6.0f;
+
+// BF16 operand copies of the weights: forward B operands are the transposed
+// matrices ([out][in], input contiguous), backward B operands the master
+// orientation ([in][out], output contiguous).
+constexpr int kPackW1t = 0;                                 // [64][16]
+constexpr int kPackW2t = kPackW1t + kMlpHidden * kMlpIn;    // [64][64]
+constexpr int kPackW3t = kPackW2t + kMlpHidden * kMlpHidden;  // [16][64]
+constexpr int kPackW2 = kPackW3t + kMlpOut * kMlpHidden;    // [64][64]
+constexpr int kPackW3 = kPackW2 + kMlpHidden * kMlpHidden;  // [64][16]
+constexpr int kPackSize = kPackW3 + kMlpHidden * kMlpOut;
+
+struct TetMoveParams {
+  float4* spins;  // replica 0 of the system
+  int L, L3, n_rep;
+  float rcpL;
+  int rep_global, rep_key, temp_base;
+  float J1;
+  const int* temp_of_rep;
+  const float* beta;
+  unsigned long long* accepted;  // [temp_base + t]
+  const unsigned long long* tet_ctr;
+  unsigned long long tet_off;
+  uint32_t seed_lo, seed_hi;
+  const __nv_bfloat16* packed;  // kPackSize
+  const float* master;          // biases read from here
+};
+
+struct TetCollectParams {
+  const float4* spins;
+  int L, L3, n_rep;
+  float rcpL;
+  int rep_global, temp_base;
+  float J1;
+  const int* temp_of_rep;
+  const float* beta;
+  int stride;          // every stride-th tetrahedron of a class
+  float* features;     // ring [cap][16]
+  float* targets;      // ring [cap][12]
+  int cap;
+  long long head;      // first slot written (mod cap)
+};
+
+void launch_mlp_pack(const float* master, __nv_bfloat16* packed, cudaStream_t st);
+// One pass of the learned move over up-tetrahedra of FCC corner f.
+void launch_tet_move(const TetMoveParams& p, int f, cudaStream_t st);
+// Number of samples one collect call writes: 4 classes x n_rep x ceil(L3 / stride).
+long long tet_collect_count(int L3, int n_rep, int stride);
+void launch_tet_collect(const TetCollectParams& p, cudaStream_t st);
+// Network outputs for n feature rows (host-visible test path).
+void launch_mlp_forward(const float* features, int n, const __nv_bfloat16* packed,
+                        const float* master, float* out, cudaStream_t st);
+// Adds d(sum of per-sample negative log-likelihood)/d(params) of rows
+// idx[0..n) (or 0..n if idx is null) to grad[kMlpParams] and the loss sum to
+// *loss.
+void launch_mlp_gradient(const float* features, const float* targets, const int* idx, int n,
+                         const __nv_bfloat16* packed, const float* master, float* grad,
+                         double* loss, cudaStream_t st);
+void launch_adam(float* master, float* m, float* v, const float* grad, int n, float lr,
+                 float beta1, float beta2, float eps, float scale, int step, cudaStream_t st);
+// idx[i] = Philox-drawn sample indices in [0, n_avail).
+void launch_draw_batch(int* idx, int n, long long n_avail, uint32_t seed_lo, uint32_t seed_hi,
+                       uint32_t step, cudaStream_t st);
+
+}  // namespace pyro

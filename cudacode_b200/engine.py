@@ -113,6 +113,18 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "pyro_get_sweep_count": (i, [P, pu64]),
         "pyro_check_spins": (i, [P, f, C.POINTER(C.c_longlong)]),
         "pyro_structure_factor": (i, [P, i, i, i, i, pd]),
+        "pyro_tet_init": (i, [P, C.c_uint64, C.c_longlong]),
+        "pyro_tet_set_weights": (i, [P, pf, i]),
+        "pyro_tet_get_weights": (i, [P, pf, i]),
+        "pyro_tet_sweep": (i, [P, i]),
+        "pyro_tet_acceptance": (i, [P, i, pu64, pu64]),
+        "pyro_tet_reset_acceptance": (i, [P]),
+        "pyro_tet_collect": (i, [P, i, i, C.POINTER(C.c_longlong)]),
+        "pyro_tet_samples": (i, [P, pf, pf, C.c_longlong, C.POINTER(C.c_longlong)]),
+        "pyro_tet_train": (i, [P, i, i, f, pd]),
+        "pyro_tet_forward": (i, [P, pf, i, pf]),
+        "pyro_tet_gradient": (i, [P, pf, pf, i, pf, pd]),
+        "pyro_cycle_tet": (i, [P, i, i, i, i, i]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -379,3 +391,71 @@ class Engine:
         self._ck(self.lib.pyro_structure_factor(self.ctx, system, replica, G, stride,
                                                 _ptr(out, C.c_double)))
         return out
+
+    # -- learned tetrahedron proposal -------------------------------------
+    N_MLP_PARAMS = 6288
+
+    def tet_init(self, seed: int = 1, sample_capacity: int = 0) -> None:
+        self._ck(self.lib.pyro_tet_init(self.ctx, seed, sample_capacity))
+
+    def tet_weights(self) -> np.ndarray:
+        w = np.empty(self.N_MLP_PARAMS, dtype=np.float32)
+        self._ck(self.lib.pyro_tet_get_weights(self.ctx, _ptr(w, C.c_float), w.size))
+        return w
+
+    def tet_set_weights(self, w) -> None:
+        a = np.ascontiguousarray(w, dtype=np.float32)
+        self._ck(self.lib.pyro_tet_set_weights(self.ctx, _ptr(a, C.c_float), a.size))
+
+    def tet_sweep(self, n: int = 1) -> None:
+        self._ck(self.lib.pyro_tet_sweep(self.ctx, n))
+
+    def tet_acceptance(self, system: int = 0):
+        n = len(self.systems[system].temperatures)
+        a = np.zeros(n, dtype=np.uint64)
+        p = np.zeros(n, dtype=np.uint64)
+        self._ck(self.lib.pyro_tet_acceptance(self.ctx, system, _ptr(a, C.c_uint64),
+                                              _ptr(p, C.c_uint64)))
+        return a, p
+
+    def tet_reset_acceptance(self) -> None:
+        self._ck(self.lib.pyro_tet_reset_acceptance(self.ctx))
+
+    def tet_collect(self, stride: int = 1, system: int = 0) -> int:
+        n = C.c_longlong()
+        self._ck(self.lib.pyro_tet_collect(self.ctx, system, stride, C.byref(n)))
+        return n.value
+
+    def tet_samples(self, max_n: int):
+        f = np.empty((max_n, 16), dtype=np.float32)
+        t = np.empty((max_n, 12), dtype=np.float32)
+        n = C.c_longlong()
+        self._ck(self.lib.pyro_tet_samples(self.ctx, _ptr(f, C.c_float), _ptr(t, C.c_float), max_n,
+                                           C.byref(n)))
+        return f[: n.value], t[: n.value]
+
+    def tet_train(self, steps: int, batch: int = 4096, lr: float = 1e-3) -> float:
+        loss = C.c_double()
+        self._ck(self.lib.pyro_tet_train(self.ctx, steps, batch, lr, C.byref(loss)))
+        return loss.value
+
+    def tet_forward(self, feats) -> np.ndarray:
+        x = np.ascontiguousarray(feats, dtype=np.float32)
+        out = np.empty((x.shape[0], 16), dtype=np.float32)
+        self._ck(self.lib.pyro_tet_forward(self.ctx, _ptr(x, C.c_float), x.shape[0],
+                                           _ptr(out, C.c_float)))
+        return out
+
+    def tet_gradient(self, feats, targets):
+        x = np.ascontiguousarray(feats, dtype=np.float32)
+        t = np.ascontiguousarray(targets, dtype=np.float32)
+        g = np.empty(self.N_MLP_PARAMS, dtype=np.float32)
+        loss = C.c_double()
+        self._ck(self.lib.pyro_tet_gradient(self.ctx, _ptr(x, C.c_float), _ptr(t, C.c_float),
+                                            x.shape[0], _ptr(g, C.c_float), C.byref(loss)))
+        return g, loss.value
+
+    def cycle_tet(self, n_metro: int, n_or: int, n_tet: int, do_swap: bool = True,
+                  n_cycles: int = 1) -> None:
+        self._ck(self.lib.pyro_cycle_tet(self.ctx, n_metro, n_or, n_tet, int(bool(do_swap)),
+                                         n_cycles))

@@ -190,6 +190,44 @@ int pyro_check_spins(pyro_ctx* ctx, float tol, long long* first_bad);
  * StructFactor path (Math.cu:721-741, Pyrochlore.cu:1303-1419). */
 int pyro_structure_factor(pyro_ctx* ctx, int system, int replica, int G, int stride, double* out);
 
+/* Learned tetrahedron proposal (no counterpart in the reference).
+ * Up-tetrahedra of one FCC corner share no bond, so the four corners are four
+ * colour classes; a tetrahedron sweep is one pass per class. For each
+ * up-tetrahedron a 16 -> 64 -> 64 -> 16 MLP (BF16 weights, FP32 tensor-core
+ * accumulation) maps the external fields of its four spins and beta to a
+ * von Mises-Fisher distribution per spin; a joint move drawn from it is
+ * accepted with the exact Metropolis-Hastings ratio (FP32 energy of the
+ * tetrahedron), so detailed balance holds for any weights. J1-only systems.
+ *
+ * pyro_tet_init: allocates the network (He-initialised from `seed`) and a ring
+ * of `sample_capacity` training samples. Weights: 6288 FP32 values, layout
+ * W1[16][64], b1[64], W2[64][64], b2[64], W3[64][16], b3[16] (row = input). */
+int pyro_tet_init(pyro_ctx* ctx, uint64_t seed, long long sample_capacity);
+int pyro_tet_set_weights(pyro_ctx* ctx, const float* weights, int n);
+int pyro_tet_get_weights(pyro_ctx* ctx, float* weights, int n);
+/* n learned tetrahedron sweeps of every J1-only system. */
+int pyro_tet_sweep(pyro_ctx* ctx, int n_sweeps);
+int pyro_tet_acceptance(pyro_ctx* ctx, int system, uint64_t* accepted, uint64_t* proposed);
+int pyro_tet_reset_acceptance(pyro_ctx* ctx);
+/* Appends (features[16], spins[12]) of every stride-th up-tetrahedron of each
+ * class and replica of `system` to the sample ring (oldest overwritten). */
+int pyro_tet_collect(pyro_ctx* ctx, int system, int stride, long long* n_written);
+int pyro_tet_samples(pyro_ctx* ctx, float* features, float* targets, long long max_n,
+                     long long* n_out);
+/* `steps` Adam steps (lr, beta 0.9/0.999) of maximum likelihood on random
+ * batches of `batch` samples; *mean_loss = last batch's mean negative
+ * log-likelihood. */
+int pyro_tet_train(pyro_ctx* ctx, int steps, int batch, float lr, double* mean_loss);
+/* Host-buffer test paths: network outputs for n feature rows, and the
+ * gradient (6288 values) and loss sum of the negative log-likelihood. */
+int pyro_tet_forward(pyro_ctx* ctx, const float* features, int n, float* out16);
+int pyro_tet_gradient(pyro_ctx* ctx, const float* features, const float* targets, int n,
+                      float* grad, double* loss_sum);
+/* Cycles with learned moves: n_metro Metropolis + n_or over-relaxation
+ * sweeps, n_tet tetrahedron sweeps, energies and (if do_swap) an exchange,
+ * replayed from a CUDA graph. */
+int pyro_cycle_tet(pyro_ctx* ctx, int n_metro, int n_or, int n_tet, int do_swap, int n_cycles);
+
 /* Energy and magnetisation without any device allocation.
  *
  * This entry point has no counterpart in the reference. It is for callers

@@ -49,6 +49,11 @@ def load() -> C.CDLL:
         "orc_get_swap_stats": (None, [P, i, pu64, pu64]),
         "orc_sweep_count": (C.c_uint64, [P]),
         "orc_structure_factor": (None, [P, i, i, i, i, pd]),
+        "orc_mlp_param_count": (i, []),
+        "orc_mlp_set_bf16": (None, [i]),
+        "orc_mlp_forward": (None, [pf, pf, i, pd]),
+        "orc_mlp_gradient": (None, [pf, pf, pf, i, pd, pd]),
+        "orc_tet_features": (None, [P, i, i, i, pf, pf]),
         "orc_neighbours": (None, [i, pi]),
         "orc_philox": (None, [pu32, pu32, pu32]),
         "orc_expf": (f, [f]),
@@ -188,6 +193,13 @@ class Oracle:
         self.lib.orc_structure_factor(self.h, system, replica, G, stride, _p(out, C.c_double))
         return out
 
+    def tet_features(self, replica, corner, system=0):
+        L3 = self.systems[system].L ** 3
+        f = np.empty((L3, 16), dtype=np.float32)
+        s = np.empty((L3, 12), dtype=np.float32)
+        self.lib.orc_tet_features(self.h, system, replica, corner, _p(f, C.c_float), _p(s, C.c_float))
+        return f, s
+
     def sweep_count(self):
         return int(self.lib.orc_sweep_count(self.h))
 
@@ -222,3 +234,22 @@ def sincospif(a: float):
 
 def exp64(x: float) -> float:
     return load().orc_exp64(x)
+
+
+def mlp_forward(weights, feats):
+    w = np.ascontiguousarray(weights, dtype=np.float32)
+    x = np.ascontiguousarray(feats, dtype=np.float32)
+    out = np.empty((x.shape[0], 16))
+    load().orc_mlp_forward(_p(w, C.c_float), _p(x, C.c_float), x.shape[0], _p(out, C.c_double))
+    return out
+
+
+def mlp_gradient(weights, feats, targets):
+    w = np.ascontiguousarray(weights, dtype=np.float32)
+    x = np.ascontiguousarray(feats, dtype=np.float32)
+    t = np.ascontiguousarray(targets, dtype=np.float32)
+    g = np.empty(load().orc_mlp_param_count())
+    loss = C.c_double()
+    load().orc_mlp_gradient(_p(w, C.c_float), _p(x, C.c_float), _p(t, C.c_float), x.shape[0],
+                            _p(g, C.c_double), C.byref(loss))
+    return g, loss.value

@@ -690,3 +690,180 @@ void orc_sincospif(float a, float* s, float* c) { pyro_sincospif(a, s, c); }
 double orc_exp64(double x) { return pyro_exp64(x); }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Learned tetrahedron proposal (no counterpart in the reference): FP64 restatement of
+// the network, its negative log-likelihood gradient and the MH move, with the
+// engine's BF16 rounding points (inputs, weights, hidden activations and the
+// backward activations are rounded to BF16 where the engine feeds them to
+// the tensor cores; accumulation in FP64 here, FP32 there).
+namespace {
+
+const int kIn = 16, kH = 64, kOut = 16;
+const int oW1 = 0, oB1 = oW1 + kIn * kH, oW2 = oB1 + kH, oB2 = oW2 + kH * kH, oW3 = oB2 + kH,
+          oB3 = oW3 + kH * kOut, kParams = oB3 + kOut;
+
+bool g_bf16 = true;  // round where the engine rounds (tests may switch it off)
+
+double bf16(double x) {
+  if (!g_bf16) return x;
+  float f = (float)x;
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u) return f;  // inf / nan unchanged
+  const uint32_t lsb = (u >> 16) & 1u;
+  u += 0x7fffu + lsb;  // round to nearest even
+  u &= 0xffff0000u;
+  memcpy(&f, &u, 4);
+  return f;
+}
+
+double silu(double x) { return x / (1.0 + std::exp(-x)); }
+double silu_grad(double x) {
+  const double s = 1.0 / (1.0 + std::exp(-x));
+  return s * (1.0 + x * (1.0 - s));
+}
+
+struct Fwd {
+  double x[kIn], pre1[kH], h1[kH], pre2[kH], h2[kH], o[kOut];
+};
+
+void mlp_forward(const float* m, const float* feat, Fwd& f) {
+  for (int i = 0; i < kIn; ++i) f.x[i] = bf16(feat[i]);
+  for (int o = 0; o < kH; ++o) {
+    double a = m[oB1 + o];
+    for (int i = 0; i < kIn; ++i) a += f.x[i] * bf16(m[oW1 + i * kH + o]);
+    f.pre1[o] = a;
+    f.h1[o] = bf16(silu(a));
+  }
+  for (int o = 0; o < kH; ++o) {
+    double a = m[oB2 + o];
+    for (int i = 0; i < kH; ++i) a += f.h1[i] * bf16(m[oW2 + i * kH + o]);
+    f.pre2[o] = a;
+    f.h2[o] = bf16(silu(a));
+  }
+  for (int o = 0; o < kOut; ++o) {
+    double a = m[oB3 + o];
+    for (int i = 0; i < kH; ++i) a += f.h2[i] * bf16(m[oW3 + i * kOut + o]);
+    f.o[o] = a;
+  }
+}
+
+const double kZmin = -4.0, kZmax = 6.0;
+
+// loss and d loss / d o for one sample (outputs o, target spins s[12]).
+double nll(const double* o, const float* s, double* d) {
+  double loss = 0.0;
+  for (int k = 0; k < 4; ++k) {
+    double n = std::sqrt(o[4 * k] * o[4 * k] + o[4 * k + 1] * o[4 * k + 1] + o[4 * k + 2] * o[4 * k + 2]);
+    double mu[3] = {0, 0, 1};
+    if (n > 1e-20) {
+      mu[0] = o[4 * k] / n;
+      mu[1] = o[4 * k + 1] / n;
+      mu[2] = o[4 * k + 2] / n;
+    } else {
+      n = 1e-20;
+    }
+    const double lz = o[4 * k + 3];
+    const double z = std::min(std::max(lz, kZmin), kZmax);
+    const bool zin = lz > kZmin && lz < kZmax;
+    const double kap = std::exp(z);
+    const double m = mu[0] * s[3 * k] + mu[1] * s[3 * k + 1] + mu[2] * s[3 * k + 2];
+    loss -= z - std::log(2.0 * M_PI) - std::log(-std::expm1(-2.0 * kap)) + kap * (m - 1.0);
+    const double r = 2.0 * kap / std::expm1(2.0 * kap);
+    d[4 * k + 3] = zin ? -(1.0 - r + kap * (m - 1.0)) : 0.0;
+    for (int a = 0; a < 3; ++a) d[4 * k + a] = -kap * (s[3 * k + a] - m * mu[a]) / n;
+  }
+  return loss;
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_mlp_param_count() { return kParams; }
+void orc_mlp_set_bf16(int on) { g_bf16 = on != 0; }
+
+void orc_mlp_forward(const float* master, const float* feats, int n, double* out) {
+#pragma omp parallel for schedule(static)
+  for (int r = 0; r < n; ++r) {
+    Fwd f;
+    mlp_forward(master, feats + 16 * r, f);
+    for (int o = 0; o < kOut; ++o) out[16 * r + o] = f.o[o];
+  }
+}
+
+// Sum over samples of d NLL / d params (same layout as the weights) and the
+// loss sum, with the engine's BF16 rounding points.
+void orc_mlp_gradient(const float* master, const float* feats, const float* targets, int n,
+                      double* grad, double* loss_sum) {
+  std::vector<double> G(kParams, 0.0);
+  double L = 0.0;
+  for (int r = 0; r < n; ++r) {
+    Fwd f;
+    mlp_forward(master, feats + 16 * r, f);
+    double d[kOut];
+    L += nll(f.o, targets + 12 * r, d);
+    double db[kOut];
+    for (int o = 0; o < kOut; ++o) {
+      G[oB3 + o] += d[o];
+      db[o] = bf16(d[o]);
+    }
+    double da2[kH], da2b[kH];
+    for (int i = 0; i < kH; ++i) {
+      double a = 0.0;
+      for (int o = 0; o < kOut; ++o) a += db[o] * bf16(master[oW3 + i * kOut + o]);
+      da2[i] = a * silu_grad(f.pre2[i]);
+      G[oB2 + i] += da2[i];
+      da2b[i] = bf16(da2[i]);
+    }
+    double da1b[kH];
+    for (int i = 0; i < kH; ++i) {
+      double a = 0.0;
+      for (int o = 0; o < kH; ++o) a += da2b[o] * bf16(master[oW2 + i * kH + o]);
+      const double v = a * silu_grad(f.pre1[i]);
+      G[oB1 + i] += v;
+      da1b[i] = bf16(v);
+    }
+    for (int i = 0; i < kIn; ++i)
+      for (int o = 0; o < kH; ++o) G[oW1 + i * kH + o] += f.x[i] * da1b[o];
+    for (int i = 0; i < kH; ++i)
+      for (int o = 0; o < kH; ++o) G[oW2 + i * kH + o] += f.h1[i] * da2b[o];
+    for (int i = 0; i < kH; ++i)
+      for (int o = 0; o < kOut; ++o) G[oW3 + i * kOut + o] += f.h2[i] * db[o];
+  }
+  memcpy(grad, G.data(), sizeof(double) * kParams);
+  *loss_sum = L;
+}
+
+// Features of every up-tetrahedron of corner f of replica r (rows = cells):
+// h_k / 3 (k = 0..3), log(beta) / 3, three zeros; and its four spins.
+void orc_tet_features(void* p, int si, int r, int f, float* feats, float* spins) {
+  Oracle& o = *(Oracle*)p;
+  const Sys& S = o.sys[si];
+  const size_t base = S.spin_off + (size_t)r * 16 * S.L3;
+  const int t = o.temp_of_rep[S.temp_base + S.off + r];
+  const double beta = 1.0 / S.T[t];
+  for (int cell = 0; cell < S.L3; ++cell) {
+    const int x = cell % S.L, y = (cell / S.L) % S.L, z = cell / (S.L * S.L);
+    for (int k = 0; k < 4; ++k) {
+      const int s = 4 * f + k;
+      double h[3] = {0, 0, 0};
+      for (int q = 0; q < 6; ++q) {
+        const Nbr& e = o.nb[s][q];
+        const bool up = e.dx == 0 && e.dy == 0 && e.dz == 0 && e.t / 4 == f;
+        if (up) continue;
+        const size_t j = base + nbr_index(S, e, x, y, z);
+        for (int a = 0; a < 3; ++a) h[a] += o.fp64 ? o.s64[4 * j + a] : o.s32[4 * j + a];
+      }
+      for (int a = 0; a < 3; ++a) feats[16 * cell + 3 * k + a] = (float)(S.J[0] * h[a] / 3.0);
+      const size_t own = base + (size_t)s * S.L3 + cell;
+      for (int a = 0; a < 3; ++a)
+        spins[12 * cell + 3 * k + a] = o.fp64 ? (float)o.s64[4 * own + a] : o.s32[4 * own + a];
+    }
+    feats[16 * cell + 12] = (float)(std::log(beta) / 3.0);
+    feats[16 * cell + 13] = feats[16 * cell + 14] = feats[16 * cell + 15] = 0.0f;
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,149 @@
+"""GPU checks of the learned tetrahedron proposal: the tensor-core forward
+pass and the training gradient against the oracle's FP64 restatement (same
+BF16 rounding points), detailed balance of the MH-corrected move against the
+plain chain, and maximum-likelihood training lowering the loss."""
+import numpy as np
+import pytest
+
+from cudacode_b200.engine import Engine, PyroError, System, geometric_ladder
+from oracle import binding as orc
+from oracle.binding import Oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def test_forward_matches_oracle():
+    e = Engine([System(L=4, temperatures=[0.2, 0.5])], seed=3)
+    e.tet_init(seed=11)
+    w = e.tet_weights()
+    rng = np.random.default_rng(0)
+    x = rng.normal(size=(300, 16)).astype(np.float32)
+    x[:, 13:] = 0.0
+    got = e.tet_forward(x)
+    want = orc.mlp_forward(w, x)
+    err = np.abs(got - want).max() / np.abs(want).max()
+    assert err < 2e-3, err
+
+
+def test_gradient_matches_oracle():
+    e = Engine([System(L=4, temperatures=[0.2, 0.5])], seed=3)
+    e.tet_init(seed=12)
+    rng = np.random.default_rng(1)
+    w = (rng.normal(size=6288) * 0.15).astype(np.float32)
+    w[13 * 64:16 * 64] = 0.0
+    e.tet_set_weights(w)
+    n = 517  # not a multiple of the 128-sample CTA tile
+    x = rng.normal(size=(n, 16)).astype(np.float32)
+    x[:, 13:] = 0.0
+    s = rng.normal(size=(n, 4, 3))
+    s /= np.linalg.norm(s, axis=-1, keepdims=True)
+    s = s.reshape(n, 12).astype(np.float32)
+    g, loss = e.tet_gradient(x, s)
+    g_ref, loss_ref = orc.mlp_gradient(w, x, s)
+    assert loss == pytest.approx(loss_ref, rel=1e-3)
+    rel = np.linalg.norm(g - g_ref) / np.linalg.norm(g_ref)
+    cos = float(g @ g_ref / (np.linalg.norm(g) * np.linalg.norm(g_ref)))
+    assert rel < 1e-2 and cos > 0.9999, (rel, cos)
+
+
+def test_collected_features_match_oracle():
+    s = System(L=4, temperatures=[0.3, 0.9])
+    e = Engine([s], seed=5)
+    o = Oracle([s], seed=5)
+    e.init_random()
+    o.init_random()
+    e.tet_init(seed=1, sample_capacity=4 * 2 * 64)
+    assert e.tet_collect(stride=1) == 4 * 2 * 64
+    f, t = e.tet_samples(4 * 2 * 64)
+    f = f.reshape(4, 2, 64, 16)
+    t = t.reshape(4, 2, 64, 12)
+    for corner in range(4):
+        for r in range(2):
+            fo, so = o.tet_features(r, corner)
+            np.testing.assert_allclose(f[corner, r], fo, rtol=1e-6, atol=1e-6)
+            assert np.array_equal(t[corner, r], so)
+
+
+def chain_energy(e, n_burn, n_meas, step):
+    for _ in range(n_burn):
+        step()
+    es = []
+    for _ in range(n_meas):
+        step()
+        es.append(e.observables()[0])
+    return np.array(es)
+
+
+def mean_and_error(x):
+    """Mean and its standard error from batch means (20 batches)."""
+    b = x[: len(x) // 20 * 20].reshape(20, -1).mean(axis=1)
+    return b.mean(), b.std(ddof=1) / np.sqrt(20)
+
+
+def test_learned_move_preserves_the_boltzmann_distribution():
+    """Tetrahedron moves alone (untrained network) and the plain method,
+    both started from the same equilibrated spins, sample the same energy
+    distribution: detailed balance of the MH test."""
+    temps = [0.4, 1.2]
+    s = System(L=4, temperatures=temps)
+    plain = Engine([s], seed=21)
+    plain.init_random()
+    plain.tune_cone(0.5, 10, 5)
+    for _ in range(300):
+        plain.metropolis_sweep(1)
+        plain.overrelax_sweep(1)
+    start = plain.get_spins()
+    e_plain = chain_energy(plain, 0, 2000, lambda: plain.metropolis_sweep(1))
+    tet = Engine([s], seed=22)
+    tet.set_spins(start)
+    tet.tet_init(seed=5)
+    e_tet = chain_energy(tet, 100, 2000, lambda: tet.tet_sweep(1))
+    acc, prop = tet.tet_acceptance()
+    assert (acc > 0).all()
+    for k in range(2):
+        m1, s1 = mean_and_error(e_plain[:, k])
+        m2, s2 = mean_and_error(e_tet[:, k])
+        assert abs(m1 - m2) < 4.0 * np.hypot(s1, s2) + 1e-9, (k, m1, s1, m2, s2)
+
+
+def test_training_lowers_the_loss_and_raises_acceptance():
+    s = System(L=6, temperatures=geometric_ladder(0.05, 0.5, 4))
+    e = Engine([s], seed=8)
+    e.init_random()
+    e.tune_cone(0.5, 10, 5, 2)
+    e.tet_init(seed=3, sample_capacity=200_000)
+    for _ in range(20):
+        e.cycle(1, 4, True, 5)
+        e.tet_collect(stride=1)
+    first = e.tet_train(1, batch=4096, lr=2e-3)
+    e.tet_reset_acceptance()
+    e.tet_sweep(5)
+    a0, p0 = e.tet_acceptance()
+    last = e.tet_train(600, batch=4096, lr=2e-3)
+    assert last < first - 1.0, (first, last)
+    e.tet_reset_acceptance()
+    e.tet_sweep(5)
+    a1, p1 = e.tet_acceptance()
+    assert (a1 / p1).mean() > (a0 / p0).mean(), (a0 / p0, a1 / p1)
+    # the trained move alone still samples the plain chain's distribution:
+    # replica perm[t] holds temperature slot t in `e`; the plain chain gets
+    # the same configurations with replica t at slot t.
+    start = e.get_spins()
+    perm = e.permutation()
+    plain = Engine([s], seed=9)
+    plain.set_spins(start[perm])
+    plain.set_cone(e.get_cone())
+    plain_E = chain_energy(plain, 50, 1500, lambda: (plain.metropolis_sweep(1),
+                                                     plain.overrelax_sweep(2)))
+    tet_E = chain_energy(e, 50, 1500, lambda: e.tet_sweep(1))
+    assert np.array_equal(perm, e.permutation())  # no exchanges in either chain
+    for t in range(4):
+        m1, s1 = mean_and_error(plain_E[:, t])
+        m2, s2 = mean_and_error(tet_E[:, perm[t]])
+        assert abs(m1 - m2) < 4.0 * np.hypot(s1, s2) + 1e-6, (t, m1, s1, m2, s2)
+
+
+def test_learned_move_requires_j1_only():
+    e = Engine([System(L=3, temperatures=[1.0], J2=0.1)])
+    with pytest.raises(PyroError):
+        e.tet_init()
