@@ -169,6 +169,89 @@ def workload_config(n_gpus):
                   "per GPU > 126 MB)"}
 
 
+def run_learned(args):
+    """Energy ESS/s of plain PT cycles (1 Metropolis + 4 over-relaxation
+    sweeps + exchange) against the same cycles with one learned tetrahedron
+    sweep added, at L=16, 8 temperatures on a geometric ladder in [0.05, 0.5].
+    The network is trained on the GPU on ~10^6 tetrahedra from the plain
+    chains first. Device time by CUDA events; tau_int by Sokal windowing."""
+    import torch
+
+    from cudacode_b200 import stats
+    from cudacode_b200.engine import Engine, System, geometric_ladder
+
+    Ll, nT = 16, 8
+    temps = geometric_ladder(0.05, 0.5, nT)
+    cycles = args.steps if args.steps != 300 else 20000
+    eng = Engine([System(L=Ll, temperatures=temps)], seed=SEED + 3)
+    stream = torch.cuda.Stream()
+    eng.set_stream(stream.cuda_stream)
+    eng.init_random()
+    eng.tune_cone(0.5, 20, 5, 4)
+    eng.cycle(1, 4, True, 2000)
+    eng.tet_init(seed=7, sample_capacity=1 << 20)
+    n_samples = 0
+    while n_samples < (1 << 20):
+        eng.cycle(1, 4, True, 25)
+        n_samples += eng.tet_collect(1)
+    t0 = time.perf_counter()
+    loss0 = eng.tet_train(1, 4096, 2e-3)
+    loss = eng.tet_train(1500, 4096, 2e-3)
+    loss = eng.tet_train(1500, 4096, 5e-4)
+    train_s = time.perf_counter() - t0
+    choice = eng.autotune(1, 4, 5)
+
+    def measure(n_tet, n_metro=1, n_or=4):
+        eng.enable_history(cycles)
+        eng.tet_reset_acceptance()
+        run = (lambda k: eng.cycle(n_metro, n_or, True, k)) if n_tet == 0 else \
+            (lambda k: eng.cycle_tet(n_metro, n_or, n_tet, True, k))
+        run(args.warmup)
+        eng.enable_history(cycles)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        run(cycles)
+        b.record(stream)
+        torch.cuda.synchronize()
+        sec = a.elapsed_time(b) / 1e3
+        h = eng.history()
+        taus = [stats.tau_int(h[:, t]) for t in range(nT)]
+        ess_s = [len(h) / (2 * tau) / sec for tau in taus]
+        means = [stats.mean_error(h[:, t]) for t in range(nT)]
+        acc, prop = eng.tet_acceptance()
+        return {"schedule": {"metropolis": n_metro, "overrelax": n_or, "tetrahedron": n_tet},
+                "seconds": sec, "us_per_cycle": 1e6 * sec / cycles, "tau_int": taus,
+                "ess_per_s": ess_s,
+                "E_per_site": [(m / (16 * Ll ** 3), e / (16 * Ll ** 3)) for m, e in means],
+                "tet_acceptance": (acc / np.maximum(prop, 1)).tolist() if n_tet else None}
+
+    plain = measure(0)
+    schedules = [measure(1, 1, 4), measure(1, 1, 1), measure(1, 0, 1), measure(2, 0, 1)]
+    learned = max(schedules, key=lambda r: r["ess_per_s"][0])
+    ratio = learned["ess_per_s"][0] / plain["ess_per_s"][0]
+    agree = [abs(p[0] - q[0]) / max(np.hypot(p[1], q[1]), 1e-30)
+             for p, q in zip(plain["E_per_site"], learned["E_per_site"])]
+    line = {"metric": "energy ESS/s learned-proposal vs plain at T=0.05", "value": ratio,
+            "unit": "x", "higher_is_better": True, "n_gpus": 1, "steps": cycles,
+            "warmup": args.warmup, "dtype": "f32 spins, bf16 MLP",
+            "data": "synthetic (random unit spins from Philox seed)",
+            "config": {"workload": "learned tetrahedron proposal: L=16 (65,536 sites), J1=1 AFM, "
+                                   "8 temperatures geometric in [0.05, 0.5], cycle = 1 Metropolis "
+                                   "+ 4 over-relaxation sweeps (+ 1 learned tetrahedron sweep) + "
+                                   "exchange", "training_samples": n_samples,
+                       "train_seconds": train_s, "loss_first": loss0, "loss_last": loss},
+            "kernels_autotune_choice": choice,
+            "plain": plain, "learned": learned,
+            "learned_schedules": [{"schedule": r["schedule"], "us_per_cycle": r["us_per_cycle"],
+                                   "tau_int_T0.05": r["tau_int"][0],
+                                   "ratio_T0.05": r["ess_per_s"][0] / plain["ess_per_s"][0]}
+                                  for r in schedules],
+            "energy_agreement_sigma": agree}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -179,10 +262,15 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--L", type=int, default=L, help="lattice size (profiling cases)")
     ap.add_argument("--replicas", type=int, default=R_PER_GPU, help="replicas per GPU")
+    ap.add_argument("--workload", default="pt", choices=["pt", "learned"],
+                    help="pt: the parallel-tempering benchmark (default); learned: energy "
+                         "ESS/s of the learned tetrahedron proposal vs the plain method")
     ap.add_argument("--kernel", default="auto", choices=["auto", "pass", "cluster"],
                     help="auto: autotuner picks; pass: one launch per colour pass; "
                          "cluster: cluster-resident cycle kernel")
     args = ap.parse_args()
+    if args.workload == "learned":
+        return run_learned(args)
     set_workload(args.L, args.replicas)
     if args.impl == "reference":
         return run_reference(args)

@@ -34,7 +34,8 @@
 namespace pyro {
 namespace {
 
-constexpr int kTetThreads = 128;  // 4 warps x 32 tetrahedra
+constexpr int kTetThreads = 128;      // training / test kernels: 4 warps x 32 rows
+constexpr int kTetMoveThreads = 256;  // move kernel: 8 warps x 32 tetrahedra
 constexpr int kLdIn = 24;         // padded row of 16 bf16 (48 B): conflict-free fragments
 constexpr int kLdH = 72;          // padded row of 64 bf16 (144 B)
 constexpr int kLdB = 40;          // padded row of 32 batch entries (bf16)
@@ -59,9 +60,12 @@ __device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1
       : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-__device__ __forceinline__ float silu(float x) { return x / (1.0f + expf(-x)); }
+// SiLU with the hardware exponential: the network only parameterises the
+// proposal, whose exact density enters the MH test, so its last bits do not
+// matter for correctness.
+__device__ __forceinline__ float silu(float x) { return __fdividef(x, 1.0f + __expf(-x)); }
 __device__ __forceinline__ float silu_grad(float x) {
-  const float s = 1.0f / (1.0f + expf(-x));
+  const float s = __fdividef(1.0f, 1.0f + __expf(-x));
   return s * (1.0f + x * (1.0f - s));
 }
 
@@ -346,9 +350,10 @@ __device__ __forceinline__ void write_features(__nv_bfloat16* row, const pyro_ve
   row[13] = row[14] = row[15] = __float2bfloat16_rn(0.0f);
 }
 
-// vMF(mu, kappa) sample on the sphere (Wood 1994).
+// vMF(mu, kappa) sample on the sphere (Wood 1994). Any rounding of the
+// sampler is harmless: the MH ratio uses the density of the value drawn.
 __device__ __forceinline__ pyro_vec3 vmf_sample(pyro_vec3 mu, float kappa, float u, float v) {
-  float w = 1.0f + logf(u + (1.0f - u) * expf(-2.0f * kappa)) / kappa;
+  float w = 1.0f + __fdividef(__logf(u + (1.0f - u) * __expf(-2.0f * kappa)), kappa);
   w = fminf(1.0f, fmaxf(-1.0f, w));
   const float st = sqrtf(fmaxf(0.0f, 1.0f - w * w));
   float sp, cp;
@@ -357,17 +362,17 @@ __device__ __forceinline__ pyro_vec3 vmf_sample(pyro_vec3 mu, float kappa, float
 }
 
 template <int F>
-__global__ void __launch_bounds__(kTetThreads) tet_move_kernel(const TetMoveParams p) {
+__global__ void __launch_bounds__(kTetMoveThreads) tet_move_kernel(const TetMoveParams p) {
   extern __shared__ __align__(16) unsigned char smem[];
   MlpSmem w = carve_weights(smem, false);
   __nv_bfloat16* feat_all = reinterpret_cast<__nv_bfloat16*>(smem + kSmemWeightsFwd);
-  float* out_all = reinterpret_cast<float*>(smem + kSmemWeightsFwd + kTetThreads * kLdIn * 2);
+  float* out_all = reinterpret_cast<float*>(smem + kSmemWeightsFwd + kTetMoveThreads * kLdIn * 2);
   stage_weights(w, p.packed, p.master, false);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   __nv_bfloat16* feat = feat_all + warp * 32 * kLdIn;
   float* out = out_all + warp * 32 * kLdOut;
-  const long long tet = (long long)blockIdx.x * kTetThreads + threadIdx.x;  // rep * L3 + cell
+  const long long tet = (long long)blockIdx.x * kTetMoveThreads + threadIdx.x;  // rep * L3 + cell
   const bool active = tet < (long long)p.n_rep * p.L3;
   const int rep = active ? (int)(tet / p.L3) : 0;
   const int cell = active ? (int)(tet - (long long)rep * p.L3) : 0;
@@ -429,7 +434,7 @@ __global__ void __launch_bounds__(kTetThreads) tet_move_kernel(const TetMovePara
 #pragma unroll
     for (int k = 0; k < 4; ++k) log_q += vm.kappa[k] * (dot3(vm.mu[k], s[k]) - dot3(vm.mu[k], sn[k]));
     const float log_r = -beta * dE + log_q;
-    accepted = log_r >= 0.0f || pyro_uniform(r2[0]) < expf(log_r);
+    accepted = log_r >= 0.0f || pyro_uniform(r2[0]) < __expf(log_r);
     if (accepted) {
       float4* wb = p.spins + (long long)rep * 16 * p.L3;
 #pragma unroll
@@ -437,8 +442,12 @@ __global__ void __launch_bounds__(kTetThreads) tet_move_kernel(const TetMovePara
         wb[(4 * F + k) * p.L3 + cell] = make_float4(sn[k].x, sn[k].y, sn[k].z, 0.0f);
     }
   }
-  // Per-replica acceptance: a CTA may span replicas, so count per thread.
-  if (accepted) atomicAdd(p.accepted + p.temp_base + tslot, 1ull);
+  // Acceptance per temperature slot: lanes of a warp that share a slot add
+  // once (a warp may straddle two replicas).
+  const unsigned peers = __match_any_sync(0xffffffffu, tslot);
+  const unsigned acc_mask = __ballot_sync(0xffffffffu, accepted) & peers;
+  if (lane == __ffs(peers) - 1 && acc_mask)
+    atomicAdd(p.accepted + p.temp_base + tslot, (unsigned long long)__popc(acc_mask));
 }
 
 template <int F>
@@ -778,6 +787,8 @@ __global__ void draw_batch_kernel(int* idx, int n, long long n_avail, uint32_t s
 }
 
 constexpr int kTetSmem = kSmemWeightsFwd + kTetThreads * kLdIn * 2 + kTetThreads * kLdOut * 4;
+constexpr int kTetMoveSmem =
+    kSmemWeightsFwd + kTetMoveThreads * kLdIn * 2 + kTetMoveThreads * kLdOut * 4;
 
 }  // namespace
 
@@ -787,12 +798,12 @@ void launch_mlp_pack(const float* master, __nv_bfloat16* packed, cudaStream_t st
 
 void launch_tet_move(const TetMoveParams& p, int f, cudaStream_t st) {
   const long long n = (long long)p.n_rep * p.L3;
-  const int blocks = (int)((n + kTetThreads - 1) / kTetThreads);
+  const int blocks = (int)((n + kTetMoveThreads - 1) / kTetMoveThreads);
   switch (f) {
-    case 0: tet_move_kernel<0><<<blocks, kTetThreads, kTetSmem, st>>>(p); break;
-    case 1: tet_move_kernel<1><<<blocks, kTetThreads, kTetSmem, st>>>(p); break;
-    case 2: tet_move_kernel<2><<<blocks, kTetThreads, kTetSmem, st>>>(p); break;
-    default: tet_move_kernel<3><<<blocks, kTetThreads, kTetSmem, st>>>(p); break;
+    case 0: tet_move_kernel<0><<<blocks, kTetMoveThreads, kTetMoveSmem, st>>>(p); break;
+    case 1: tet_move_kernel<1><<<blocks, kTetMoveThreads, kTetMoveSmem, st>>>(p); break;
+    case 2: tet_move_kernel<2><<<blocks, kTetMoveThreads, kTetMoveSmem, st>>>(p); break;
+    default: tet_move_kernel<3><<<blocks, kTetMoveThreads, kTetMoveSmem, st>>>(p); break;
   }
 }
 
