@@ -306,18 +306,16 @@ def main():
     kernel_desc = {"cycle_kernel": eng.get_option(eng.OPT_CYCLE_KERNEL),
                    "cluster_size": eng.get_option(eng.OPT_CLUSTER_SIZE),
                    "j1_kernel": eng.get_option(eng.OPT_J1_KERNEL), "autotune_choice": variant}
-    e_all = torch.zeros(R_PER_GPU * n_gpus, dtype=torch.float64, device=f"cuda:{local}")
-    e_loc = torch.zeros(R_PER_GPU, dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        from cudacode_b200.distributed import EngineBackend, ShardedPT
+        pt = ShardedPT(EngineBackend(eng, torch.device(f"cuda:{local}")), R_PER_GPU * n_gpus)
 
     def step():
         if world == 1:
             eng.cycle(N_METRO, N_OR, True, 1)
         else:
-            eng.cycle(N_METRO, N_OR, False, 1)
-            eng.observables_device(e_loc.data_ptr())
             with torch.cuda.stream(stream):
-                dist.all_gather_into_tensor(e_all, e_loc)
-            eng.pt_swap_global(e_all.data_ptr(), -1)
+                pt.cycle(N_METRO, N_OR)
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):

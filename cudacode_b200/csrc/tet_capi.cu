@@ -5,6 +5,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -35,6 +36,9 @@ struct TetState {
   long long written = 0;  // samples ever written
   int adam_step = 0;
   uint64_t seed = 0;
+  int sweep_kernel = 1;   // 1: cluster kernel (one launch per call) when it fits
+  int cluster_max = 8;    // largest cluster size tried
+  int cluster_ok = -1;    // -1 unknown, else the usable size (0: none)
 };
 
 void tet_free(pyro_ctx* ctx) {
@@ -122,6 +126,30 @@ void tet_count_sweeps(pyro_ctx* ctx, unsigned long long n) {
 // Queues n tetrahedron sweeps (4 passes each) over every J1-only system;
 // offsets from the device counter, which this call advances.
 int queue_tet_sweeps(pyro_ctx* ctx, int n) {
+  TetState* t = ctx->tet;
+  if (t->sweep_kernel == 1 && t->cluster_ok != 0) {
+    if (t->cluster_ok < 0) {
+      t->cluster_ok = 0;
+      for (int cs = t->cluster_max; cs >= 1; --cs) {
+        int n_active = 0;
+        if (tet_cluster_prepare(cs, &n_active) == cudaSuccess && n_active > 0) {
+          t->cluster_ok = cs;
+          break;
+        }
+        cudaGetLastError();
+      }
+    }
+    if (t->cluster_ok > 0) {
+      for (int si = 0; si < (int)ctx->sys.size(); ++si) {
+        if (!j1_only_system(ctx->sys[si])) continue;
+        const int cs = std::min(t->cluster_ok, tet_chunks(ctx->sys[si].L3));
+        PYRO_CK(launch_tet_sweep_cluster(move_params(ctx, si, 0), n, cs, ctx->stream));
+      }
+      launch_advance(t->d_ctr, (unsigned long long)n, ctx->stream);
+      PYRO_CK_LAUNCH();
+      return PYRO_OK;
+    }
+  }
   for (int k = 0; k < n; ++k)
     for (int f = 0; f < 4; ++f)
       for (int si = 0; si < (int)ctx->sys.size(); ++si) {
@@ -198,6 +226,18 @@ int pyro_tet_get_weights(pyro_ctx* ctx, float* w, int n) {
   PYRO_CK(cudaMemcpyAsync(w, ctx->tet->d_master, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost,
                           ctx->stream));
   PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  return PYRO_OK;
+}
+
+int pyro_tet_set_kernel(pyro_ctx* ctx, int cluster) {
+  int rc = need_tet(ctx);
+  if (rc) return rc;
+  if (cluster != 0 && cluster != 1) return fail(ctx, PYRO_ERR_ARG, "tet kernel option is 0 or 1");
+  PYRO_CK(cudaSetDevice(ctx->device));
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  ctx->tet->sweep_kernel = cluster;
+  for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+  ctx->graphs.clear();
   return PYRO_OK;
 }
 

@@ -301,18 +301,27 @@ __device__ __forceinline__ Frame cell_frame(int cell, int L, float rcpL) {
   return f;
 }
 
-template <int S, int K>
+// kL2: read through L2 only (the cluster kernel rewrites the lattice between
+// passes of one launch, so an SM's L1 may hold stale lines).
+template <bool kL2>
+__device__ __forceinline__ float4 ld_spin(const float4* p) {
+  if (kL2) return __ldcg(p);
+  return __ldg(p);
+}
+
+template <int S, int K, bool kL2 = false>
 __device__ __forceinline__ float4 nbr(const float4* __restrict__ rep, const Frame& f, int L3) {
   constexpr NbrEntry e = j1_neighbour(S, K);
-  return __ldg(rep + f.zo[e.dz + 1] + f.yo[e.dy + 1] + f.xo[e.dx + 1] + e.t * L3);
+  return ld_spin<kL2>(rep + f.zo[e.dz + 1] + f.yo[e.dy + 1] + f.xo[e.dx + 1] + e.t * L3);
 }
 
 // External field of site S (sum of its three down-tetrahedron neighbours).
-template <int S>
+template <int S, bool kL2 = false>
 __device__ __forceinline__ pyro_vec3 ext_field(const float4* __restrict__ rep, const Frame& f,
                                                int L3, float J1) {
   constexpr int k0 = j1_down_index(S, 0), k1 = j1_down_index(S, 1), k2 = j1_down_index(S, 2);
-  const float4 a = nbr<S, k0>(rep, f, L3), b = nbr<S, k1>(rep, f, L3), c = nbr<S, k2>(rep, f, L3);
+  const float4 a = nbr<S, k0, kL2>(rep, f, L3), b = nbr<S, k1, kL2>(rep, f, L3),
+               c = nbr<S, k2, kL2>(rep, f, L3);
   pyro_vec3 h;
   h.x = J1 * ((a.x + b.x) + c.x);
   h.y = J1 * ((a.y + b.y) + c.y);
@@ -320,13 +329,13 @@ __device__ __forceinline__ pyro_vec3 ext_field(const float4* __restrict__ rep, c
   return h;
 }
 
-template <int F>
+template <int F, bool kL2 = false>
 __device__ __forceinline__ void tet_fields(const float4* __restrict__ rep, const Frame& fr, int L3,
                                            float J1, pyro_vec3 h[4]) {
-  h[0] = ext_field<4 * F + 0>(rep, fr, L3, J1);
-  h[1] = ext_field<4 * F + 1>(rep, fr, L3, J1);
-  h[2] = ext_field<4 * F + 2>(rep, fr, L3, J1);
-  h[3] = ext_field<4 * F + 3>(rep, fr, L3, J1);
+  h[0] = ext_field<4 * F + 0, kL2>(rep, fr, L3, J1);
+  h[1] = ext_field<4 * F + 1, kL2>(rep, fr, L3, J1);
+  h[2] = ext_field<4 * F + 2, kL2>(rep, fr, L3, J1);
+  h[3] = ext_field<4 * F + 3, kL2>(rep, fr, L3, J1);
 }
 
 __device__ __forceinline__ float dot3(pyro_vec3 a, pyro_vec3 b) {
@@ -361,32 +370,23 @@ __device__ __forceinline__ pyro_vec3 vmf_sample(pyro_vec3 mu, float kappa, float
   return pyro_about_axis(mu, w, st, cp, sp);
 }
 
-template <int F>
-__global__ void __launch_bounds__(kTetMoveThreads) tet_move_kernel(const TetMoveParams p) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  MlpSmem w = carve_weights(smem, false);
-  __nv_bfloat16* feat_all = reinterpret_cast<__nv_bfloat16*>(smem + kSmemWeightsFwd);
-  float* out_all = reinterpret_cast<float*>(smem + kSmemWeightsFwd + kTetMoveThreads * kLdIn * 2);
-  stage_weights(w, p.packed, p.master, false);
-
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  __nv_bfloat16* feat = feat_all + warp * 32 * kLdIn;
-  float* out = out_all + warp * 32 * kLdOut;
-  const long long tet = (long long)blockIdx.x * kTetMoveThreads + threadIdx.x;  // rep * L3 + cell
-  const bool active = tet < (long long)p.n_rep * p.L3;
-  const int rep = active ? (int)(tet / p.L3) : 0;
-  const int cell = active ? (int)(tet - (long long)rep * p.L3) : 0;
+// One warp's 32 tetrahedra of corner F (one per lane; lanes with
+// active == false only feed the warp-wide MMAs): features, network, vMF
+// proposals, MH test, write-back. Returns 1 if this lane's move was accepted.
+template <int F, bool kL2>
+__device__ __forceinline__ int tet_warp_step(const TetMoveParams& p, const MlpSmem& w, bool active,
+                                             int rep, int cell, float beta,
+                                             unsigned long long sweep, __nv_bfloat16* feat,
+                                             float* out) {
+  const int lane = threadIdx.x & 31;
   const float4* rb = p.spins + (long long)rep * 16 * p.L3;
-  const int g = p.rep_global + rep;
-  const int tslot = p.temp_of_rep[p.temp_base + g];
-  const float beta = p.beta[p.temp_base + tslot];
   pyro_vec3 h[4], s[4];
   if (active) {
     const Frame fr = cell_frame(cell, p.L, p.rcpL);
-    tet_fields<F>(rb, fr, p.L3, p.J1, h);
+    tet_fields<F, kL2>(rb, fr, p.L3, p.J1, h);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      const float4 v = rb[(4 * F + k) * p.L3 + cell];
+      const float4 v = ld_spin<kL2>(rb + (4 * F + k) * p.L3 + cell);
       s[k].x = v.x;
       s[k].y = v.y;
       s[k].z = v.z;
@@ -400,22 +400,19 @@ __global__ void __launch_bounds__(kTetMoveThreads) tet_move_kernel(const TetMove
     }
   }
   write_features(feat + lane * kLdIn, h, active ? beta : 1.0f);
-  __syncthreads();  // weights staged, features written
-
+  __syncwarp();
   TileFwd fw;
   tile_forward<false>(feat, 0, w, fw, nullptr, nullptr);
   store_out(fw, 0, out);
   tile_forward<false>(feat, 16, w, fw, nullptr, nullptr);
   store_out(fw, 16, out);
   __syncwarp();
-
   int accepted = 0;
   if (active) {
     float o[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) o[i] = out[lane * kLdOut + i];
     const VmfParams vm = vmf_params(o);
-    const unsigned long long sweep = (p.tet_ctr ? *p.tet_ctr : 0ull) + p.tet_off;
     const uint32_t key_tet = (uint32_t)(F * p.L3 + cell);
     uint32_t r0[4], r1[4], r2[4];
     pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + 0,
@@ -442,12 +439,92 @@ __global__ void __launch_bounds__(kTetMoveThreads) tet_move_kernel(const TetMove
         wb[(4 * F + k) * p.L3 + cell] = make_float4(sn[k].x, sn[k].y, sn[k].z, 0.0f);
     }
   }
-  // Acceptance per temperature slot: lanes of a warp that share a slot add
-  // once (a warp may straddle two replicas).
+  return accepted;
+}
+
+// Acceptance per temperature slot: lanes of a warp that share a slot add
+// once (a warp may straddle two replicas).
+__device__ __forceinline__ void count_accepted(const TetMoveParams& p, int tslot, int accepted) {
+  const int lane = threadIdx.x & 31;
   const unsigned peers = __match_any_sync(0xffffffffu, tslot);
   const unsigned acc_mask = __ballot_sync(0xffffffffu, accepted) & peers;
   if (lane == __ffs(peers) - 1 && acc_mask)
     atomicAdd(p.accepted + p.temp_base + tslot, (unsigned long long)__popc(acc_mask));
+}
+
+template <int F>
+__global__ void __launch_bounds__(kTetMoveThreads) tet_move_kernel(const TetMoveParams p) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  MlpSmem w = carve_weights(smem, false);
+  __nv_bfloat16* feat_all = reinterpret_cast<__nv_bfloat16*>(smem + kSmemWeightsFwd);
+  float* out_all = reinterpret_cast<float*>(smem + kSmemWeightsFwd + kTetMoveThreads * kLdIn * 2);
+  stage_weights(w, p.packed, p.master, false);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5;
+  const long long tet = (long long)blockIdx.x * kTetMoveThreads + threadIdx.x;  // rep * L3 + cell
+  const bool active = tet < (long long)p.n_rep * p.L3;
+  const int rep = active ? (int)(tet / p.L3) : 0;
+  const int cell = active ? (int)(tet - (long long)rep * p.L3) : 0;
+  const int tslot = p.temp_of_rep[p.temp_base + p.rep_global + rep];
+  const float beta = p.beta[p.temp_base + tslot];
+  const unsigned long long sweep = (p.tet_ctr ? *p.tet_ctr : 0ull) + p.tet_off;
+  const int acc = tet_warp_step<F, false>(p, w, active, rep, cell, beta, sweep,
+                                          feat_all + warp * 32 * kLdIn,
+                                          out_all + warp * 32 * kLdOut);
+  count_accepted(p, tslot, acc);
+}
+
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+  asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+// n_sweeps tetrahedron sweeps of one replica per thread-block cluster: the
+// four corner passes of a sweep are separated by cluster barriers, the
+// weights are staged once, and the CTAs of the cluster split the replica's
+// L^3 tetrahedra of a corner in chunks of kTetMoveThreads. Same proposals and
+// decisions as the per-pass kernel.
+__global__ void __launch_bounds__(kTetMoveThreads) tet_sweep_cluster_kernel(const TetMoveParams p,
+                                                                            int n_sweeps,
+                                                                            int csize) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  MlpSmem w = carve_weights(smem, false);
+  __nv_bfloat16* feat_all = reinterpret_cast<__nv_bfloat16*>(smem + kSmemWeightsFwd);
+  float* out_all = reinterpret_cast<float*>(smem + kSmemWeightsFwd + kTetMoveThreads * kLdIn * 2);
+  stage_weights(w, p.packed, p.master, false);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5;
+  __nv_bfloat16* feat = feat_all + warp * 32 * kLdIn;
+  float* out = out_all + warp * 32 * kLdOut;
+  const int rep = blockIdx.x / csize, rank = blockIdx.x - rep * csize;
+  const int tslot = p.temp_of_rep[p.temp_base + p.rep_global + rep];
+  const float beta = p.beta[p.temp_base + tslot];
+  const unsigned long long base = (p.tet_ctr ? *p.tet_ctr : 0ull) + p.tet_off;
+  const int n_chunks = (p.L3 + kTetMoveThreads - 1) / kTetMoveThreads;
+  int acc = 0;
+  for (int k = 0; k < n_sweeps; ++k) {
+    const unsigned long long sweep = base + (unsigned long long)k;
+#pragma unroll 1
+    for (int f = 0; f < 4; ++f) {
+      for (int c = rank; c < n_chunks; c += csize) {
+        const int cell = c * kTetMoveThreads + threadIdx.x;
+        const bool active = cell < p.L3;
+        const int cl = active ? cell : 0;
+        switch (f) {
+          case 0: acc += tet_warp_step<0, true>(p, w, active, rep, cl, beta, sweep, feat, out); break;
+          case 1: acc += tet_warp_step<1, true>(p, w, active, rep, cl, beta, sweep, feat, out); break;
+          case 2: acc += tet_warp_step<2, true>(p, w, active, rep, cl, beta, sweep, feat, out); break;
+          default: acc += tet_warp_step<3, true>(p, w, active, rep, cl, beta, sweep, feat, out); break;
+        }
+      }
+      cluster_sync_all();
+    }
+  }
+  // every lane of this CTA belongs to one replica: plain warp sum
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0 && acc > 0)
+    atomicAdd(p.accepted + p.temp_base + tslot, (unsigned long long)acc);
 }
 
 template <int F>
@@ -806,6 +883,44 @@ void launch_tet_move(const TetMoveParams& p, int f, cudaStream_t st) {
     default: tet_move_kernel<3><<<blocks, kTetMoveThreads, kTetMoveSmem, st>>>(p); break;
   }
 }
+
+cudaError_t tet_cluster_prepare(int csize, int* max_active) {
+  *max_active = 0;
+  cudaError_t e = cudaFuncSetAttribute(tet_sweep_cluster_kernel,
+                                       cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = csize;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(csize * 8, 1, 1);
+  cfg.blockDim = dim3(kTetMoveThreads, 1, 1);
+  cfg.dynamicSmemBytes = kTetMoveSmem;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaOccupancyMaxActiveClusters(max_active, tet_sweep_cluster_kernel, &cfg);
+}
+
+cudaError_t launch_tet_sweep_cluster(const TetMoveParams& p, int n_sweeps, int csize,
+                                     cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = csize;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(csize * p.n_rep, 1, 1);
+  cfg.blockDim = dim3(kTetMoveThreads, 1, 1);
+  cfg.dynamicSmemBytes = kTetMoveSmem;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, tet_sweep_cluster_kernel, p, n_sweeps, csize);
+}
+
+int tet_chunks(int L3) { return (L3 + kTetMoveThreads - 1) / kTetMoveThreads; }
 
 long long tet_collect_count(int L3, int n_rep, int stride) {
   return 4ll * n_rep * ((L3 + stride - 1) / stride);

@@ -67,6 +67,12 @@ struct TetCollectParams {
 void launch_mlp_pack(const float* master, __nv_bfloat16* packed, cudaStream_t st);
 // One pass of the learned move over up-tetrahedra of FCC corner f.
 void launch_tet_move(const TetMoveParams& p, int f, cudaStream_t st);
+// n sweeps (4 corner passes each) of every replica in one launch, one
+// thread-block cluster of csize CTAs per replica.
+cudaError_t launch_tet_sweep_cluster(const TetMoveParams& p, int n_sweeps, int csize,
+                                     cudaStream_t st);
+cudaError_t tet_cluster_prepare(int csize, int* max_active);
+int tet_chunks(int L3);  // chunks of tetrahedra per corner and replica
 // Number of samples one collect call writes: 4 classes x n_rep x ceil(L3 / stride).
 long long tet_collect_count(int L3, int n_rep, int stride);
 void launch_tet_collect(const TetCollectParams& p, cudaStream_t st);

@@ -1,0 +1,93 @@
+"""Parallel tempering across GPUs: one process per GPU, replicas sharded.
+
+Each rank holds a contiguous block of the configurations of one global
+temperature ladder (``System(n_replicas=R, replica_offset=rank * R)``). A
+cycle is: the local sweeps (no exchange), the FP64 energies of the local
+replicas, an ``all_gather`` of those energies (8 bytes per replica, over
+NCCL on GPUs), and the exchange step applied identically on every rank from
+the gathered vector (``pyro_pt_swap_global``: Philox-driven, so no decision
+has to be broadcast). Spins never leave their GPU; only temperature labels
+move. Because Philox keys use the global replica index, a sharded run
+reproduces the single-GPU run of the same ladder.
+
+Replaces the reference's multi-GPU layer: one pthread per GPU with
+host-staged energy reductions and a host-side swap (MonteCarlo.cu:15-245,
+TrySwapingTemperatures MonteCarlo.cu:105-172).
+
+The driver only needs an object with ``sweeps(n_metro, n_or)``,
+``local_energies() -> tensor`` and ``swap_global(all_energies, parity)``;
+:class:`EngineBackend` binds it to the CUDA engine.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import torch
+import torch.distributed as dist
+
+from .engine import Engine, System
+
+
+def shard(n_total: int, world: int, rank: int) -> tuple[int, int]:
+    """(offset, count) of the replicas held by `rank`; blocks differ by <= 1."""
+    if n_total < world:
+        raise ValueError(f"{n_total} replicas cannot be spread over {world} ranks")
+    base, extra = divmod(n_total, world)
+    count = base + (1 if rank < extra else 0)
+    offset = rank * base + min(rank, extra)
+    return offset, count
+
+
+class EngineBackend:
+    """The CUDA engine as a sharded-PT backend (energies stay on the GPU)."""
+
+    def __init__(self, engine: Engine, device: torch.device):
+        self.engine = engine
+        self.device = device
+        self.n_local = engine.systems[0].replicas()
+        self._e = torch.zeros(self.n_local, dtype=torch.float64, device=device)
+
+    def sweeps(self, n_metro: int, n_or: int) -> None:
+        self.engine.cycle(n_metro, n_or, False, 1)
+
+    def local_energies(self) -> torch.Tensor:
+        self.engine.observables_device(self._e.data_ptr())
+        return self._e
+
+    def swap_global(self, all_energies: torch.Tensor, parity: int) -> None:
+        self.engine.pt_swap_global(all_energies.data_ptr(), parity)
+
+
+@dataclass
+class ShardedPT:
+    backend: object
+    n_total: int
+    group: object = None
+
+    def __post_init__(self):
+        self.world = dist.get_world_size(self.group) if dist.is_initialized() else 1
+        self.rank = dist.get_rank(self.group) if dist.is_initialized() else 0
+        self.offset, self.count = shard(self.n_total, self.world, self.rank)
+        counts = [shard(self.n_total, self.world, r)[1] for r in range(self.world)]
+        if len(set(counts)) != 1:
+            raise ValueError("all_gather needs equal shards: choose replicas divisible by ranks")
+
+    def cycle(self, n_metro: int, n_or: int, parity: int = -1) -> torch.Tensor:
+        """One cycle; returns the gathered energies (global replica order)."""
+        self.backend.sweeps(n_metro, n_or)
+        e_local = self.backend.local_energies()
+        if self.world > 1:
+            e_all = torch.empty(self.n_total, dtype=e_local.dtype, device=e_local.device)
+            dist.all_gather_into_tensor(e_all, e_local.contiguous(), group=self.group)
+        else:
+            e_all = e_local
+        self.backend.swap_global(e_all, parity)
+        return e_all
+
+
+def make_engine_shard(L: int, temperatures, world: int, rank: int, seed: int, device: int,
+                      **couplings) -> Engine:
+    """Engine holding this rank's block of the global ladder."""
+    offset, count = shard(len(temperatures), world, rank)
+    return Engine([System(L=L, temperatures=list(temperatures), n_replicas=count,
+                          replica_offset=offset, **couplings)], seed=seed, device=device)

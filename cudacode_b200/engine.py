@@ -117,6 +117,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "pyro_tet_set_weights": (i, [P, pf, i]),
         "pyro_tet_get_weights": (i, [P, pf, i]),
         "pyro_tet_sweep": (i, [P, i]),
+        "pyro_tet_set_kernel": (i, [P, i]),
         "pyro_tet_acceptance": (i, [P, i, pu64, pu64]),
         "pyro_tet_reset_acceptance": (i, [P]),
         "pyro_tet_collect": (i, [P, i, i, C.POINTER(C.c_longlong)]),
@@ -406,6 +407,9 @@ class Engine:
     def tet_set_weights(self, w) -> None:
         a = np.ascontiguousarray(w, dtype=np.float32)
         self._ck(self.lib.pyro_tet_set_weights(self.ctx, _ptr(a, C.c_float), a.size))
+
+    def tet_set_kernel(self, cluster: int) -> None:
+        self._ck(self.lib.pyro_tet_set_kernel(self.ctx, cluster))
 
     def tet_sweep(self, n: int = 1) -> None:
         self._ck(self.lib.pyro_tet_sweep(self.ctx, n))

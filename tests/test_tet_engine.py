@@ -147,3 +147,20 @@ def test_learned_move_requires_j1_only():
     e = Engine([System(L=3, temperatures=[1.0], J2=0.1)])
     with pytest.raises(PyroError):
         e.tet_init()
+
+
+@pytest.mark.parametrize("L", [4, 7, 16])
+def test_cluster_and_per_pass_tet_kernels_agree(L):
+    s = System(L=L, temperatures=[0.1, 0.3, 0.9])
+    runs = []
+    for cluster in (0, 1):
+        e = Engine([s], seed=41)
+        e.init_random()
+        e.tet_init(seed=2)
+        e.tet_set_kernel(cluster)
+        e.tet_sweep(3)
+        e.cycle_tet(1, 1, 2, True, 2)
+        runs.append((e.get_spins(), e.tet_acceptance()[0], e.permutation()))
+    assert np.array_equal(runs[0][0], runs[1][0])
+    assert np.array_equal(runs[0][1], runs[1][1])
+    assert np.array_equal(runs[0][2], runs[1][2])
