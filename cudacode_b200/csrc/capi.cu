@@ -21,6 +21,7 @@
 #include "j1_kernels.cuh"
 #include "kernels.cuh"
 #include "lattice.h"
+#include "smem_kernels.cuh"
 #include "sq_kernels.cuh"
 
 using namespace pyro;
@@ -572,6 +573,9 @@ int pyro_set_option(pyro_ctx* ctx, int option, int value) {
   if (option == PYRO_OPT_J1_KERNEL) {
     if (value != 0 && value != 1) return fail(ctx, PYRO_ERR_ARG, "J1 kernel option is 0 or 1");
     ctx->use_j1_kernel = value == 1;
+  } else if (option == PYRO_OPT_SMEM_KERNEL) {
+    if (value != 0 && value != 1) return fail(ctx, PYRO_ERR_ARG, "smem kernel option is 0 or 1");
+    ctx->smem_kernel = value;
   } else if (option == PYRO_OPT_J1_SITE_MODE) {
     if (value < 0 || value > 3) return fail(ctx, PYRO_ERR_ARG, "J1 site mode is 0..3");
     ctx->j1_metro_site_mode = (value & 1) != 0;
@@ -600,6 +604,7 @@ int pyro_get_option(pyro_ctx* ctx, int option, int* value) {
     case PYRO_OPT_J1_KERNEL: *value = ctx->use_j1_kernel ? 1 : 0; break;
     case PYRO_OPT_CYCLE_KERNEL: *value = ctx->cycle_kernel; break;
     case PYRO_OPT_CLUSTER_SIZE: *value = ctx->cluster_size; break;
+    case PYRO_OPT_SMEM_KERNEL: *value = ctx->smem_kernel; break;
     case PYRO_OPT_J1_SITE_MODE:
       *value = (ctx->j1_metro_site_mode ? 1 : 0) | (ctx->j1_or_site_mode ? 2 : 0);
       break;
@@ -994,6 +999,50 @@ int pyro_get_history(pyro_ctx* ctx, int system, double* out, int* n_cycles) {
   return PYRO_OK;
 }
 
+// Small lattices: every system fits one CTA's shared memory.
+static bool use_smem_path(const pyro_ctx* ctx) {
+  if (!ctx->smem_kernel) return false;
+  for (const auto& s : ctx->sys)
+    if (s.L > kSmemMaxL) return false;
+  return true;
+}
+
+// Cycles without exchange on the shared-memory kernel: one launch per system
+// for all cycles; the energy of every cycle goes to the history ring.
+static int run_smem_cycles(pyro_ctx* ctx, int n_metro, int n_or, int n_cycles) {
+  for (int si = 0; si < (int)ctx->sys.size(); ++si) {
+    const SysDev& s = ctx->sys[si];
+    SmemCycleParams p;
+    p.sys = s;
+    p.spins = ctx->d_spins + s.spin_off;
+    p.temp_of_rep = ctx->d_temp_of_rep;
+    p.beta = ctx->d_beta;
+    p.cosmax = ctx->d_cosmax;
+    p.accepted = ctx->d_accepted;
+    p.sweep_ctr = ctx->d_sweep;
+    p.n_metro = n_metro;
+    p.n_or = n_or;
+    p.n_cycles = n_cycles;
+    p.renorm_every = ctx->renorm_every;
+    p.seed_lo = (uint32_t)(ctx->seed & 0xffffffffu);
+    p.seed_hi = (uint32_t)(ctx->seed >> 32);
+    p.history = ctx->d_history;
+    p.history_count = ctx->d_history_count;
+    p.history_cap = ctx->history_cap;
+    p.total_temps = ctx->total_temps;
+    PYRO_CK(launch_smem_cycles(p, ctx->tab, ctx->stream));
+  }
+  launch_advance(ctx->d_sweep, (unsigned long long)(n_metro + n_or) * n_cycles, ctx->stream);
+  PYRO_CK_LAUNCH();
+  if (ctx->d_history) {
+    launch_advance(ctx->d_history_count, (unsigned long long)n_cycles, ctx->stream);
+    PYRO_CK_LAUNCH();
+  }
+  ctx->h_sweep += (unsigned long long)(n_metro + n_or) * n_cycles;
+  ctx->metro_sweeps_since_reset += (unsigned long long)n_metro * n_cycles;
+  return PYRO_OK;
+}
+
 static int run_cycles(pyro_ctx* ctx, int n_metro, int n_or, int n_tet, int do_swap, int n_cycles) {
   if (!ctx) return PYRO_ERR_ARG;
   if (n_metro < 0 || n_or < 0 || n_tet < 0 || n_cycles < 0)
@@ -1005,6 +1054,7 @@ static int run_cycles(pyro_ctx* ctx, int n_metro, int n_or, int n_tet, int do_sw
     return fail(ctx, PYRO_ERR_STATE, "cycle: learned moves need pyro_tet_init first");
   if (n_cycles == 0) return PYRO_OK;
   PYRO_CK(cudaSetDevice(ctx->device));
+  if (!do_swap && n_tet == 0 && use_smem_path(ctx)) return run_smem_cycles(ctx, n_metro, n_or, n_cycles);
   const auto key = std::make_tuple(n_metro, n_or, n_tet, do_swap ? 1 : 0);
   auto it = ctx->graphs.find(key);
   if (it == ctx->graphs.end()) {

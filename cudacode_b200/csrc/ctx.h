@@ -72,6 +72,7 @@ struct pyro_ctx {
   bool j1_or_site_mode = false;
   // Cluster-resident cycle kernel for J1 systems (0 = per-pass launches).
   int cycle_kernel = 0;
+  int smem_kernel = 1;  // cycles without exchange of L <= 8 systems in shared memory
   int cluster_size = 16;
   bool cluster_checked = false;
   std::vector<std::vector<pyro::PassSeg>> pass_segs;

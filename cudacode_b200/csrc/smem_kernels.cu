@@ -1,0 +1,188 @@
+// Small lattices resident in shared memory, for sm_100a.
+//
+// For L <= 8 a replica (16 L^3 float4, at most 128 KiB) fits in one CTA's
+// shared memory. One CTA per replica then runs many whole cycles (Metropolis
+// and over-relaxation sweeps, every colour pass separated by __syncthreads,
+// and the FP64 energy after each cycle) in a single launch: no kernel launch
+// and no HBM round trip per pass, which is what bounds the per-pass kernels
+// at these sizes. The updates are exactly those of the other kernels (same
+// neighbour order, same pyro_math.h arithmetic, same Philox counters), so the
+// results are bit-identical.
+//
+// Replaces the reference's special 4x4x4 shared-memory kernel MCKernel4x4x4
+// (Pyrochlore.cu:713-827), which loaded the wrong cells across blocks.
+#include <cuda_runtime.h>
+
+#include "../../include/pyro_math.h"
+#include "smem_kernels.cuh"
+
+namespace pyro {
+namespace {
+
+__device__ __forceinline__ int wrap_s(int v, int L) {
+  v = v < 0 ? v + L : v;
+  return v >= L ? v - L : v;
+}
+
+__device__ __forceinline__ float3 shell_sum_smem(const float4* lat, const NbrTable& tab, int s,
+                                                 int first, int last, int x, int y, int z, int L,
+                                                 int L3) {
+  float3 a;
+  {
+    const NbrEntry e = tab.e[s][first];
+    const float4 v =
+        lat[(wrap_s(z + e.dz, L) * L + wrap_s(y + e.dy, L)) * L + wrap_s(x + e.dx, L) + e.t * L3];
+    a = make_float3(v.x, v.y, v.z);
+  }
+  for (int k = first + 1; k < last; ++k) {
+    const NbrEntry e = tab.e[s][k];
+    const float4 v =
+        lat[(wrap_s(z + e.dz, L) * L + wrap_s(y + e.dy, L)) * L + wrap_s(x + e.dx, L) + e.t * L3];
+    a.x = a.x + v.x;
+    a.y = a.y + v.y;
+    a.z = a.z + v.z;
+  }
+  return a;
+}
+
+__device__ __forceinline__ double block_sum(double v, double* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += red[i];
+  __syncthreads();
+  return s;
+}
+
+__global__ void __launch_bounds__(kSmemThreads) smem_cycles_kernel(const SmemCycleParams p,
+                                                                   const NbrTable tab) {
+  extern __shared__ float4 lat[];
+  __shared__ double red[kSmemThreads / 32];
+  const SysDev sd = p.sys;
+  const int L = sd.L, L3 = sd.L3, n = 16 * L3;
+  const int rep = blockIdx.x;
+  float4* g = p.spins + (long long)rep * n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) lat[i] = g[i];
+  const int slot = p.temp_of_rep[sd.temp_base + sd.rep_global + rep];
+  const float beta = p.beta[sd.temp_base + slot];
+  const float cosmax = p.cosmax[sd.temp_base + slot];
+  const uint32_t rkey = (uint32_t)(sd.rep_key + rep);
+  const unsigned long long base = *p.sweep_ctr;
+  const unsigned long long hist0 = p.history ? *p.history_count : 0ull;
+  const int per_cycle = p.n_metro + p.n_or;
+  __syncthreads();
+  unsigned long long acc = 0;
+  for (int c = 0; c < p.n_cycles; ++c) {
+    for (int k = 0; k < per_cycle; ++k) {
+      const unsigned long long sweep = base + (unsigned long long)c * per_cycle + k;
+      const bool metro = k < p.n_metro;
+      const bool renorm =
+          p.renorm_every > 0 && ((sweep + 1) % (unsigned long long)p.renorm_every) == 0;
+      for (int colour = 0; colour < sd.n_colours; ++colour) {
+        for (int u = threadIdx.x; u < sd.units_per_colour; u += blockDim.x) {
+          const int kk = u / L3, cell = u - kk * L3;
+          const int s = colour_site(sd.n_colours, colour, kk);
+          const int x = cell % L, yz = cell / L, y = yz % L, z = yz / L;
+          const int own = s * L3 + cell;
+          const float3 a1 = shell_sum_smem(lat, tab, s, 0, 6, x, y, z, L, L3);
+          pyro_vec3 h;
+          h.x = sd.J1 * a1.x;
+          h.y = sd.J1 * a1.y;
+          h.z = sd.J1 * a1.z;
+          if (sd.shells & 2) {
+            const float3 a = shell_sum_smem(lat, tab, s, 6, 18, x, y, z, L, L3);
+            h.x = fmaf(sd.J2, a.x, h.x);
+            h.y = fmaf(sd.J2, a.y, h.y);
+            h.z = fmaf(sd.J2, a.z, h.z);
+          }
+          if (sd.shells & 4) {
+            const float3 a = shell_sum_smem(lat, tab, s, 18, 24, x, y, z, L, L3);
+            h.x = fmaf(sd.J3a, a.x, h.x);
+            h.y = fmaf(sd.J3a, a.y, h.y);
+            h.z = fmaf(sd.J3a, a.z, h.z);
+          }
+          if (sd.shells & 8) {
+            const float3 a = shell_sum_smem(lat, tab, s, 24, 30, x, y, z, L, L3);
+            h.x = fmaf(sd.J3b, a.x, h.x);
+            h.y = fmaf(sd.J3b, a.y, h.y);
+            h.z = fmaf(sd.J3b, a.z, h.z);
+          }
+          const float4 sv = lat[own];
+          pyro_vec3 sp;
+          sp.x = sv.x;
+          sp.y = sv.y;
+          sp.z = sv.z;
+          pyro_vec3 out;
+          if (metro) {
+            uint32_t r[4];
+            pyro_philox((uint32_t)own, rkey, (uint32_t)sweep, PYRO_PURPOSE_METRO, p.seed_lo,
+                        p.seed_hi, r);
+            const pyro_vec3 prop =
+                pyro_cone_proposal(sp, cosmax, pyro_uniform(r[0]), pyro_uniform(r[1]));
+            const int a = pyro_metropolis_accept(pyro_delta_e(h, sp, prop), beta, pyro_uniform(r[2]));
+            acc += (unsigned long long)a;
+            out = a ? prop : sp;
+          } else {
+            out = pyro_overrelax(sp, h);
+          }
+          if (renorm) out = pyro_renormalise(out);
+          lat[own] = make_float4(out.x, out.y, out.z, 0.0f);
+        }
+        __syncthreads();
+      }
+    }
+    if (p.history) {
+      // FP64 energy of the cycle's final state: E = 1/2 sum_i S_i . h_i
+      double e = 0.0;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int s = i / L3, cell = i - s * L3;
+        const int x = cell % L, yz = cell / L, y = yz % L, z = yz / L;
+        const float4 sv = lat[i];
+        const int sb[5] = {0, 6, 18, 24, 30};
+        for (int sh = 0; sh < 4; ++sh) {
+          if (!(sd.shells & (1 << sh))) continue;
+          double ax = 0.0, ay = 0.0, az = 0.0;
+          for (int q = sb[sh]; q < sb[sh + 1]; ++q) {
+            const NbrEntry en = tab.e[s][q];
+            const float4 v = lat[(wrap_s(z + en.dz, L) * L + wrap_s(y + en.dy, L)) * L +
+                                 wrap_s(x + en.dx, L) + en.t * L3];
+            ax += v.x;
+            ay += v.y;
+            az += v.z;
+          }
+          e += sd.J64[sh] * ((double)sv.x * ax + (double)sv.y * ay + (double)sv.z * az);
+        }
+      }
+      const double tot = block_sum(e, red);
+      if (threadIdx.x == 0) {
+        const unsigned long long row = (hist0 + c) % (unsigned long long)p.history_cap;
+        p.history[row * p.total_temps + sd.temp_base + slot] = 0.5 * tot;
+      }
+    }
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) g[i] = lat[i];
+  if (p.n_metro > 0) {
+    const double a = block_sum((double)acc, red);
+    if (threadIdx.x == 0 && a > 0.0)
+      atomicAdd(p.accepted + sd.temp_base + slot, (unsigned long long)(a + 0.5));
+  }
+}
+
+}  // namespace
+
+size_t smem_cycle_bytes(int L) { return sizeof(float4) * 16 * (size_t)L * L * L; }
+
+cudaError_t launch_smem_cycles(const SmemCycleParams& p, const NbrTable& tab, cudaStream_t st) {
+  const size_t bytes = smem_cycle_bytes(p.sys.L);
+  cudaError_t e = cudaFuncSetAttribute(smem_cycles_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e != cudaSuccess) return e;
+  smem_cycles_kernel<<<p.sys.n_rep, kSmemThreads, bytes, st>>>(p, tab);
+  return cudaGetLastError();
+}
+
+}  // namespace pyro

@@ -36,7 +36,7 @@ struct TetState {
   long long written = 0;  // samples ever written
   int adam_step = 0;
   uint64_t seed = 0;
-  int sweep_kernel = 1;   // 1: cluster kernel (one launch per call) when it fits
+  int sweep_kernel = 0;   // 1: cluster kernel (one launch per call) when it fits
   int cluster_max = 8;    // largest cluster size tried
   int cluster_ok = -1;    // -1 unknown, else the usable size (0: none)
 };

@@ -232,6 +232,7 @@ class Engine:
     OPT_CYCLE_KERNEL = 2
     OPT_CLUSTER_SIZE = 3
     OPT_J1_SITE_MODE = 4
+    OPT_SMEM_KERNEL = 5
 
     def set_option(self, option: int, value: int) -> None:
         self._ck(self.lib.pyro_set_option(self.ctx, option, value))

@@ -86,6 +86,11 @@ int pyro_neighbour_table(int site, int* out120);
  * passes of the per-pass J1 kernel run one site per thread (set) or the four
  * sites of a cell per thread (clear). Default 1. */
 #define PYRO_OPT_J1_SITE_MODE 4
+/* PYRO_OPT_SMEM_KERNEL: 1 (default) runs pyro_cycle without exchange, when
+ * every system has L <= 8, as one launch per system with each replica held
+ * in one CTA's shared memory for all cycles; 0 uses the other kernels.
+ * Identical results. */
+#define PYRO_OPT_SMEM_KERNEL 5
 int pyro_set_option(pyro_ctx* ctx, int option, int value);
 int pyro_get_option(pyro_ctx* ctx, int option, int* value);
 /* Autotuner: times every kernel variant (per-pass generic, per-pass J1,
@@ -207,8 +212,8 @@ int pyro_tet_set_weights(pyro_ctx* ctx, const float* weights, int n);
 int pyro_tet_get_weights(pyro_ctx* ctx, float* weights, int n);
 /* n learned tetrahedron sweeps of every J1-only system. */
 int pyro_tet_sweep(pyro_ctx* ctx, int n_sweeps);
-/* 1 (default): all passes of a call in one launch, one thread-block cluster
- * per replica; 0: one launch per corner pass. Identical results. */
+/* 1: all passes of a call in one launch, one thread-block cluster per
+ * replica; 0 (default): one launch per corner pass. Identical results. */
 int pyro_tet_set_kernel(pyro_ctx* ctx, int cluster);
 int pyro_tet_acceptance(pyro_ctx* ctx, int system, uint64_t* accepted, uint64_t* proposed);
 int pyro_tet_reset_acceptance(pyro_ctx* ctx);

@@ -330,3 +330,27 @@ def test_structure_factor_matches_direct_sum(L, G, stride, replica):
         sel = spins if replica < 0 else spins[replica:replica + 1]
         assert a.sum() == pytest.approx((4 * L) ** 3 * (sel ** 2).sum() / (16 * L ** 3) /
                                         sel.shape[0], rel=1e-9)
+
+
+@pytest.mark.parametrize("L,J2,J3", [(4, 0.0, 0.0), (8, 0.0, 0.0), (5, 0.06, -0.04)])
+def test_shared_memory_cycles_bit_exact(L, J2, J3):
+    temps = geometric_ladder(0.1, 1.0, 3)
+    e, o = pair([System(L=L, temperatures=temps, J2=J2, J3=J3)], renorm_every=4)
+    assert e.get_option(e.OPT_SMEM_KERNEL) == 1
+    e.init_random()
+    o.init_random()
+    c = np.array([0.7, 0.2, -0.6], dtype=np.float32)
+    e.set_cone(c)
+    o.set_cone(c)
+    e.enable_history(32)
+    e.cycle(1, 5, False, 7)
+    h = o.cycle(1, 5, False, 7, record=True)
+    assert np.array_equal(e.get_spins(), o.get_spins())
+    assert np.array_equal(e.acceptance()[0], o.acceptance()[0])
+    np.testing.assert_allclose(e.history(), h, rtol=1e-12, atol=1e-9)
+    assert e.sweep_count() == 42
+    # the next call continues the same chain on the other kernels
+    e.set_option(e.OPT_SMEM_KERNEL, 0)
+    e.cycle(1, 5, False, 2)
+    o.cycle(1, 5, False, 2)
+    assert np.array_equal(e.get_spins(), o.get_spins())
