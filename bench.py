@@ -169,6 +169,170 @@ def workload_config(n_gpus):
                   "per GPU > 126 MB)"}
 
 
+def _timed(stream, fn):
+    import torch
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / 1e3
+
+
+def run_small(args):
+    """L=4 (1,024 sites), J1=1, T=0.5, one replica, cone tuned to 50%
+    acceptance, cycle = 1 Metropolis + 5 over-relaxation sweeps, 10^4 cycles,
+    on the GPU (shared-memory kernel) and on the host (oracle port, all host
+    cores); energy per site compared within 2 sigma."""
+    import torch
+
+    from cudacode_b200 import stats
+    from cudacode_b200.engine import Engine, System
+    from oracle.binding import Oracle
+
+    cycles = 10_000
+    s = System(L=4, temperatures=[0.5])
+    eng = Engine([s], seed=SEED + 1)
+    stream = torch.cuda.Stream()
+    eng.set_stream(stream.cuda_stream)
+    eng.init_random()
+    eng.tune_cone(0.5, 30, 20, 5)
+    eng.cycle(1, 5, False, 1000)
+    eng.enable_history(cycles)
+    sec = _timed(stream, lambda: eng.cycle(1, 5, False, cycles))
+    eng.reset_acceptance()
+    eng.metropolis_sweep(200)
+    acc, prop = eng.acceptance()
+    h = eng.history()[:, 0] / 1024
+    o = Oracle([s], seed=SEED + 1, threads=os.cpu_count())
+    o.init_random()
+    o.tune_cone(0.5, 30, 20, 5)
+    o.cycle(1, 5, False, 1000)
+    t0 = time.perf_counter()
+    ho = o.cycle(1, 5, False, cycles, record=True)[:, 0] / 1024
+    host_s = time.perf_counter() - t0
+    updates = 1024 * 6 * cycles
+    m1, e1 = stats.mean_error(h)
+    m2, e2 = stats.mean_error(ho)
+    print(json.dumps({
+        "metric": "spin-updates/ns", "workload": "small", "value": updates / (sec * 1e9),
+        "unit": "updates/ns", "host_value": updates / (host_s * 1e9), "host_cores": os.cpu_count(),
+        "gpu_seconds": sec, "host_seconds": host_s, "acceptance": float(acc[0] / prop[0]),
+        "E_per_site_gpu": [m1, e1], "E_per_site_host": [m2, e2],
+        "agreement_sigma": abs(m1 - m2) / np.hypot(e1, e2),
+        "config": {"workload": "L=4 (1,024 sites) J1=1 T=0.5, 1 replica, 1 Metropolis + 5 "
+                               "over-relaxation sweeps per cycle, 10^4 cycles",
+                   "kernel": "shared-memory-resident cycles (one launch)"}}), flush=True)
+    return 0
+
+
+def run_batched(args):
+    """256 systems, L uniform in {8,12,16,20,24}, 16-32 replicas each on its
+    own geometric ladder in [0.05, 1.5], J1=1 and J2, J3 uniform in
+    [-0.1, 0.1] (16-colour schedule); cycle = 1 Metropolis + 4 over-relaxation
+    sweeps + FP64 energies + exchange, one CUDA graph for all systems."""
+    import torch
+
+    from cudacode_b200.engine import Engine, System, geometric_ladder
+
+    rng = np.random.default_rng(12345 + 3)
+    systems = []
+    for _ in range(256):
+        Ls = int(rng.choice([8, 12, 16, 20, 24]))
+        nT = int(rng.integers(16, 33))
+        j2, j3 = rng.uniform(-0.1, 0.1, 2)
+        systems.append(System(L=Ls, temperatures=geometric_ladder(0.05, 1.5, nT), J2=float(j2),
+                              J3=float(j3)))
+    eng = Engine(systems, seed=SEED + 2)
+    stream = torch.cuda.Stream()
+    eng.set_stream(stream.cuda_stream)
+    eng.init_random()
+    for k, sy in enumerate(systems):
+        eng.set_cone(np.full(len(sy.temperatures), 0.3, dtype=np.float32), k)
+    choice = eng.autotune(1, 4, 2)
+    eng.cycle(1, 4, True, args.warmup)
+    steps = args.steps if args.steps != 300 else 20
+    sec = _timed(stream, lambda: eng.cycle(1, 4, True, steps))
+    spins = sum(len(sy.temperatures) * sy.n_sites for sy in systems)
+    updates = spins * 5 * steps
+    # dominant kernel: one over-relaxation sweep (16 colour passes)
+    or_s = _timed(stream, lambda: eng.overrelax_sweep(2)) / 2
+    pass_bytes = 272 * spins  # per sweep: 16 passes x (16 N + 16 N / 16) bytes per N/16 updates
+    peak, kind = hbm_peak()
+    print(json.dumps({
+        "metric": "spin-updates/ns", "workload": "batched", "value": updates / (sec * 1e9),
+        "unit": "updates/ns", "ms_per_step": 1e3 * sec / steps, "steps": steps,
+        "spins": spins, "systems": 256, "autotune_choice": choice,
+        "roofline": {"bound": "hbm", "kernel": "colour_pass_kernel<general, over-relaxation>",
+                     "bytes_per_update": 272, "achieved": pass_bytes / or_s / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": pass_bytes / or_s / 1e9 / peak, "peak_kind": kind},
+        "config": {"workload": "256 systems, L in {8,12,16,20,24}, 16-32 replicas each, ladders "
+                               "in [0.05, 1.5], J2, J3 in [-0.1, 0.1], 1 M + 4 OR + exchange"}}),
+          flush=True)
+    return 0
+
+
+def run_large(args):
+    """L=64 (4,194,304 sites), J1=1, J2=J3=0.05, 32 replicas on a geometric
+    ladder in [0.03, 1.0], renormalised every 100 sweeps; cycles of 1
+    Metropolis + 4 over-relaxation sweeps + FP64 energies + exchange; S(q) on
+    a 32^3 grid; FP64-oracle error of E, M and S(q) over the first 100 sweeps
+    of one replica."""
+    import torch
+
+    from cudacode_b200.engine import Engine, System, geometric_ladder
+    from oracle.binding import Oracle
+
+    temps = geometric_ladder(0.03, 1.0, 32)
+    s = System(L=64, temperatures=temps, J2=0.05, J3=0.05)
+    eng = Engine([s], seed=SEED + 4, renorm_every=100)
+    stream = torch.cuda.Stream()
+    eng.set_stream(stream.cuda_stream)
+    eng.init_random()
+    eng.set_cone(np.full(32, 0.3, dtype=np.float32))
+    choice = eng.autotune(1, 4, 1)
+    eng.cycle(1, 4, True, args.warmup)
+    steps = args.steps if args.steps != 300 else 10
+    sec = _timed(stream, lambda: eng.cycle(1, 4, True, steps))
+    updates = 32 * s.n_sites * 5 * steps
+    sq_s = _timed(stream, lambda: eng.structure_factor(32, 4))
+    # precision accounting: replica 0 of a 1-replica L=64 system, first 100
+    # sweeps, GPU FP32 vs the host FP64 oracle from the same initial spins
+    one = System(L=64, temperatures=[0.1], J2=0.05, J3=0.05)
+    g1 = Engine([one], seed=SEED + 5, renorm_every=100)
+    g1.init_random()
+    g1.set_cone(np.array([0.5], dtype=np.float32))
+    o64 = Oracle([one], seed=SEED + 5, renorm_every=100, fp64=True, threads=os.cpu_count())
+    o64.set_spins(g1.get_spins())
+    o64.set_cone(np.array([0.5], dtype=np.float32))
+    errs = []
+    for k in range(1, 101):
+        g1.metropolis_sweep(1) if k % 5 == 1 else g1.overrelax_sweep(1)
+        o64.metropolis_sweep(1) if k % 5 == 1 else o64.overrelax_sweep(1)
+        if k in (1, 5, 10, 25, 50, 100):
+            e_g, m_g = g1.observables()
+            e_o, m_o = o64.observables()
+            rec = {"sweep": k, "E_rel": float(abs(e_g[0] - e_o[0]) / abs(e_o[0])),
+                   "M_abs_per_site": float(np.abs(m_g - m_o).max() / one.n_sites)}
+            if k in (1, 100):
+                sg = g1.structure_factor(4, 32)
+                so = o64.structure_factor(4, 32)
+                rec["Sq_rel"] = float(np.abs(sg - so).max() / np.abs(so).max())
+            errs.append(dict(rec,
+                             max_spin_diff=float(np.abs(g1.get_spins() -
+                                                        o64.get_spins64().astype(np.float32)).max())))
+    print(json.dumps({
+        "metric": "spin-updates/ns", "workload": "large", "value": updates / (sec * 1e9),
+        "unit": "updates/ns", "ms_per_step": 1e3 * sec / steps, "steps": steps,
+        "structure_factor_32cubed_ms": 1e3 * sq_s, "autotune_choice": choice,
+        "fp64_error_first_100_sweeps": errs,
+        "config": {"workload": "L=64, J1=1, J2=J3=0.05, 32 replicas in [0.03, 1.0], renormalise "
+                               "every 100 sweeps, 1 M + 4 OR + exchange; S(q) 32^3, stride 4"}}),
+          flush=True)
+    return 0
+
+
 def run_learned(args):
     """Energy ESS/s of plain PT cycles (1 Metropolis + 4 over-relaxation
     sweeps + exchange) against the same cycles with one learned tetrahedron
@@ -262,15 +426,24 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--L", type=int, default=L, help="lattice size (profiling cases)")
     ap.add_argument("--replicas", type=int, default=R_PER_GPU, help="replicas per GPU")
-    ap.add_argument("--workload", default="pt", choices=["pt", "learned"],
+    ap.add_argument("--workload", default="pt",
+                    choices=["pt", "learned", "small", "batched", "large"],
                     help="pt: the parallel-tempering benchmark (default); learned: energy "
-                         "ESS/s of the learned tetrahedron proposal vs the plain method")
+                         "ESS/s of the learned tetrahedron proposal vs the plain method; "
+                         "small: L=4 on the GPU and on the host; batched: 256 uneven "
+                         "systems; large: L=64 with J2/J3, S(q) and FP64 error accounting")
     ap.add_argument("--kernel", default="auto", choices=["auto", "pass", "cluster"],
                     help="auto: autotuner picks; pass: one launch per colour pass; "
                          "cluster: cluster-resident cycle kernel")
     args = ap.parse_args()
     if args.workload == "learned":
         return run_learned(args)
+    if args.workload == "small":
+        return run_small(args)
+    if args.workload == "batched":
+        return run_batched(args)
+    if args.workload == "large":
+        return run_large(args)
     set_workload(args.L, args.replicas)
     if args.impl == "reference":
         return run_reference(args)
