@@ -14,6 +14,7 @@
 
 namespace pyro {
 struct TetState;  // learned tetrahedron move (tet_capi.cu)
+constexpr int kMaxChains = 4;
 }
 
 struct pyro_ctx {
@@ -72,7 +73,12 @@ struct pyro_ctx {
   bool j1_or_site_mode = false;
   // Cluster-resident cycle kernel for J1 systems (0 = per-pass launches).
   int cycle_kernel = 0;
-  int smem_kernel = 1;  // cycles without exchange of L <= 8 systems in shared memory
+  int smem_kernel = 1;
+  int rep_group = 0;    // per-pass J1 kernels over groups of this many replicas (0: all)
+  int n_chains = 1;     // concurrent streams the replica groups are dealt to
+  cudaStream_t chain_stream[pyro::kMaxChains] = {};
+  cudaEvent_t chain_event[pyro::kMaxChains] = {};
+  cudaEvent_t fork_event = nullptr;  // cycles without exchange of L <= 8 systems in shared memory
   int cluster_size = 16;
   bool cluster_checked = false;
   std::vector<std::vector<pyro::PassSeg>> pass_segs;

@@ -233,6 +233,8 @@ class Engine:
     OPT_CLUSTER_SIZE = 3
     OPT_J1_SITE_MODE = 4
     OPT_SMEM_KERNEL = 5
+    OPT_REPLICA_GROUP = 6
+    OPT_CHAINS = 7
 
     def set_option(self, option: int, value: int) -> None:
         self._ck(self.lib.pyro_set_option(self.ctx, option, value))

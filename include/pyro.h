@@ -91,11 +91,18 @@ int pyro_neighbour_table(int site, int* out120);
  * in one CTA's shared memory for all cycles; 0 uses the other kernels.
  * Identical results. */
 #define PYRO_OPT_SMEM_KERNEL 5
+/* PYRO_OPT_REPLICA_GROUP: with the per-pass J1 kernels, run every sweep of
+ * one group of this many replicas before the next group (0, default: all
+ * replicas in every pass), keeping a group's spins in L2. Identical results. */
+#define PYRO_OPT_REPLICA_GROUP 6
+/* PYRO_OPT_CHAINS: 1..4 concurrent streams (parallel branches of the cycle
+ * graph) the replica groups are dealt to. Identical results. */
+#define PYRO_OPT_CHAINS 7
 int pyro_set_option(pyro_ctx* ctx, int option, int value);
 int pyro_get_option(pyro_ctx* ctx, int option, int* value);
 /* Autotuner: times every kernel variant (per-pass generic, per-pass J1,
- * per-pass J1 in its site/cell forms, cluster-resident J1 with cluster sizes
- * 16, 10, 9, 8) on
+ * per-pass J1 in its site/cell forms, replica groups of 2..8 on 1, 2 or 4
+ * concurrent chains, cluster-resident J1 with cluster sizes 16, 10) on
  * `cycles` cycles of n_metro + n_or sweeps (+ exchange when the context holds
  * the whole ladder) and keeps the fastest; *chosen = its index. The timed
  * cycles are real Monte Carlo steps and advance the chain. */

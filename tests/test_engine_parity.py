@@ -299,6 +299,20 @@ def test_cluster_cycle_kernel_bit_exact(cs):
     assert e.get_option(e.OPT_CLUSTER_SIZE) <= cs
 
 
+@pytest.mark.parametrize("group,chains", [(1, 1), (2, 1), (3, 1), (1, 2), (2, 4)])
+def test_replica_groups_bit_exact(group, chains):
+    temps = geometric_ladder(0.05, 1.0, 5)
+    e, o = pair([System(L=6, temperatures=temps)], renorm_every=3)
+    e.set_option(e.OPT_REPLICA_GROUP, group)
+    e.set_option(e.OPT_CHAINS, chains)
+    e.init_random()
+    o.init_random()
+    e.cycle(1, 3, True, 4)
+    o.cycle(1, 3, True, 4)
+    assert np.array_equal(e.get_spins(), o.get_spins())
+    assert np.array_equal(e.permutation(), o.permutation())
+
+
 def test_autotune_keeps_results_exact():
     temps = geometric_ladder(0.05, 1.0, 4)
     e, o = pair([System(L=8, temperatures=temps)])
