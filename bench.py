@@ -432,9 +432,12 @@ def main():
                          "ESS/s of the learned tetrahedron proposal vs the plain method; "
                          "small: L=4 on the GPU and on the host; batched: 256 uneven "
                          "systems; large: L=64 with J2/J3, S(q) and FP64 error accounting")
-    ap.add_argument("--kernel", default="auto", choices=["auto", "pass", "cluster"],
+    ap.add_argument("--kernel", default="auto", choices=["auto", "pass", "cluster", "grouped"],
                     help="auto: autotuner picks; pass: one launch per colour pass; "
-                         "cluster: cluster-resident cycle kernel")
+                         "cluster: cluster-resident cycle kernel; grouped: per-pass kernels "
+                         "over replica groups (--group) on concurrent chains (--chains)")
+    ap.add_argument("--group", type=int, default=4)
+    ap.add_argument("--chains", type=int, default=2)
     args = ap.parse_args()
     if args.workload == "learned":
         return run_learned(args)
@@ -476,9 +479,15 @@ def main():
         variant = eng.autotune(N_METRO, N_OR, 8) if world == 1 else None
     else:
         eng.set_option(eng.OPT_CYCLE_KERNEL, 1 if args.kernel == "cluster" else 0)
+        if args.kernel == "grouped":
+            eng.set_option(eng.OPT_REPLICA_GROUP, args.group)
+            eng.set_option(eng.OPT_CHAINS, args.chains)
     kernel_desc = {"cycle_kernel": eng.get_option(eng.OPT_CYCLE_KERNEL),
                    "cluster_size": eng.get_option(eng.OPT_CLUSTER_SIZE),
-                   "j1_kernel": eng.get_option(eng.OPT_J1_KERNEL), "autotune_choice": variant}
+                   "j1_kernel": eng.get_option(eng.OPT_J1_KERNEL),
+                   "replica_group": eng.get_option(eng.OPT_REPLICA_GROUP),
+                   "chains": eng.get_option(eng.OPT_CHAINS),
+                   "j1_site_mode": eng.get_option(eng.OPT_J1_SITE_MODE), "autotune_choice": variant}
     if world > 1:
         from cudacode_b200.distributed import EngineBackend, ShardedPT
         pt = ShardedPT(EngineBackend(eng, torch.device(f"cuda:{local}")), R_PER_GPU * n_gpus)
@@ -499,11 +508,13 @@ def main():
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with ClockSampler(local) as clk:
             torch.cuda.synchronize()
+            launches0 = eng.launch_count()
             start.record(stream)
             for _ in range(args.steps):
                 step()
             stop.record(stream)
             torch.cuda.synchronize()
+            launches_timed = eng.launch_count() - launches0
         ms = start.elapsed_time(stop)
     if world > 1:
         t = torch.tensor([ms], device=f"cuda:{local}")
@@ -553,8 +564,6 @@ def main():
         cpu = {"value": v, "unit": "updates/ns", "cores": nt, "kind": "port",
                "sample": sample + f" ({dt:.1f} s)"}
 
-    passes_per_step = 4 * (N_METRO + N_OR)
-    launches_per_step = passes_per_step + 3  # + observables, finalise, exchange
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "updates/ns", "n_gpus": n_gpus,
@@ -575,7 +584,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "updates/ns",
                     "h2d_bytes_per_step": 4 * len(temps),
                     "d2h_bytes_per_step": 8 * R_PER_GPU + 24 * R_PER_GPU},
-            "gpu_launches": launches_per_step * args.steps,
+            "gpu_launches": launches_timed,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)

@@ -285,6 +285,7 @@ void free_all(pyro_ctx* c) {
   c->fork_event = nullptr;
   for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
   c->graphs.clear();
+  c->graph_kernels.clear();
   void* ptrs[] = {c->d_sys,         c->d_spins,        c->d_temp_of_rep, c->d_rep_of_temp,
                   c->d_beta,        c->d_beta64,       c->d_cosmax,      c->d_accepted,
                   c->d_swap_acc,    c->d_swap_try,     c->d_swap_count,  c->d_last_accepted,
@@ -622,6 +623,7 @@ int pyro_set_stream(pyro_ctx* ctx, void* cuda_stream) {
   PYRO_CK(cudaSetDevice(ctx->device));
   for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
   ctx->graphs.clear();
+  ctx->graph_kernels.clear();
   if (ctx->own_stream && ctx->stream) {
     PYRO_CK(cudaStreamSynchronize(ctx->stream));
     cudaStreamDestroy(ctx->stream);
@@ -664,6 +666,7 @@ int pyro_set_option(pyro_ctx* ctx, int option, int value) {
   }
   for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
   ctx->graphs.clear();
+  ctx->graph_kernels.clear();
   return build_schedule(ctx);
 }
 
@@ -927,6 +930,7 @@ int pyro_observables_device(pyro_ctx* ctx, int system, double* dev_energy,
   PYRO_CK(cudaSetDevice(ctx->device));
   int rc = queue_observables(ctx);
   if (rc) return rc;
+  ctx->launches += ctx->obs_j1.size() + (ctx->obs_generic_blocks > 0 ? 1 : 0) + 1;
   const SysDev& s = ctx->sys[system];
   if (dev_energy)
     PYRO_CK(cudaMemcpyAsync(dev_energy, ctx->d_energy + s.rep_ctx_base, sizeof(double) * s.n_rep,
@@ -1020,6 +1024,7 @@ int pyro_pt_swap_global(pyro_ctx* ctx, int system, const double* dev_energy_all,
   x.history_count = nullptr;
   launch_exchange(x, 1, (ctx->sys[system].n_temp + 1) / 2, ctx->stream);
   PYRO_CK_LAUNCH();
+  ctx->launches += 1;
   return PYRO_OK;
 }
 
@@ -1046,6 +1051,7 @@ int pyro_enable_history(pyro_ctx* ctx, int capacity_cycles) {
   PYRO_CK(cudaStreamSynchronize(ctx->stream));
   for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
   ctx->graphs.clear();
+  ctx->graph_kernels.clear();
   if (ctx->d_history) cudaFree(ctx->d_history);
   ctx->d_history = nullptr;
   ctx->history_cap = capacity_cycles;
@@ -1114,6 +1120,7 @@ static int run_smem_cycles(pyro_ctx* ctx, int n_metro, int n_or, int n_cycles) {
     p.history_cap = ctx->history_cap;
     p.total_temps = ctx->total_temps;
     PYRO_CK(launch_smem_cycles(p, ctx->tab, ctx->stream));
+    ctx->launches += 1;
   }
   launch_advance(ctx->d_sweep, (unsigned long long)(n_metro + n_or) * n_cycles, ctx->stream);
   PYRO_CK_LAUNCH();
@@ -1164,14 +1171,28 @@ static int run_cycles(pyro_ctx* ctx, int n_metro, int n_or, int n_tet, int do_sw
     if (rc != PYRO_OK) return fail(ctx, rc, "cycle: capture failed: " + ctx->err);
     if (e != cudaSuccess)
       return fail(ctx, PYRO_ERR_CUDA, std::string("cycle: end capture: ") + cudaGetErrorString(e));
+    // kernels in the graph (for the launch count)
+    size_t n_nodes = 0;
+    unsigned long long n_kernels = 0;
+    if (cudaGraphGetNodes(g, nullptr, &n_nodes) == cudaSuccess && n_nodes > 0) {
+      std::vector<cudaGraphNode_t> nodes(n_nodes);
+      if (cudaGraphGetNodes(g, nodes.data(), &n_nodes) == cudaSuccess)
+        for (auto nd : nodes) {
+          cudaGraphNodeType ty;
+          if (cudaGraphNodeGetType(nd, &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel)
+            ++n_kernels;
+        }
+    }
     cudaGraphExec_t ge;
     e = cudaGraphInstantiate(&ge, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess)
       return fail(ctx, PYRO_ERR_CUDA, std::string("cycle: instantiate: ") + cudaGetErrorString(e));
     it = ctx->graphs.emplace(key, ge).first;
+    ctx->graph_kernels[key] = n_kernels;
   }
   for (int c = 0; c < n_cycles; ++c) PYRO_CK(cudaGraphLaunch(it->second, ctx->stream));
+  ctx->launches += ctx->graph_kernels[key] * (unsigned long long)n_cycles;
   ctx->h_sweep += (unsigned long long)(n_metro + n_or) * n_cycles;
   ctx->metro_sweeps_since_reset += (unsigned long long)n_metro * n_cycles;
   if (n_tet > 0) tet_count_sweeps(ctx, (unsigned long long)n_tet * n_cycles);
@@ -1184,6 +1205,12 @@ int pyro_cycle(pyro_ctx* ctx, int n_metro, int n_or, int do_swap, int n_cycles) 
 
 int pyro_cycle_tet(pyro_ctx* ctx, int n_metro, int n_or, int n_tet, int do_swap, int n_cycles) {
   return run_cycles(ctx, n_metro, n_or, n_tet, do_swap, n_cycles);
+}
+
+int pyro_get_launch_count(pyro_ctx* ctx, uint64_t* launches) {
+  if (!ctx || !launches) return PYRO_ERR_ARG;
+  *launches = ctx->launches;
+  return PYRO_OK;
 }
 
 int pyro_get_sweep_count(pyro_ctx* ctx, uint64_t* sweeps) {

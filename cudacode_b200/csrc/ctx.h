@@ -96,6 +96,8 @@ struct pyro_ctx {
   unsigned long long* d_history_count = nullptr;
 
   std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs;
+  std::map<std::tuple<int, int, int, int>, unsigned long long> graph_kernels;
+  unsigned long long launches = 0;  // kernels run by graph replays and direct calls
 
   // Structure-factor scratch, grown on demand.
   double2* d_sq_s1 = nullptr;

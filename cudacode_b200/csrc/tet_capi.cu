@@ -202,6 +202,7 @@ int pyro_tet_init(pyro_ctx* ctx, uint64_t seed, long long sample_capacity) {
   PYRO_CK(cudaStreamSynchronize(ctx->stream));
   for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
   ctx->graphs.clear();
+  ctx->graph_kernels.clear();
   return PYRO_OK;
 }
 
@@ -238,6 +239,7 @@ int pyro_tet_set_kernel(pyro_ctx* ctx, int cluster) {
   ctx->tet->sweep_kernel = cluster;
   for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
   ctx->graphs.clear();
+  ctx->graph_kernels.clear();
   return PYRO_OK;
 }
 

@@ -111,6 +111,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "pyro_enable_history": (i, [P, i]),
         "pyro_get_history": (i, [P, i, pd, pi]),
         "pyro_get_sweep_count": (i, [P, pu64]),
+        "pyro_get_launch_count": (i, [P, pu64]),
         "pyro_check_spins": (i, [P, f, C.POINTER(C.c_longlong)]),
         "pyro_structure_factor": (i, [P, i, i, i, i, pd]),
         "pyro_tet_init": (i, [P, C.c_uint64, C.c_longlong]),
@@ -304,6 +305,11 @@ class Engine:
 
     def cycle(self, n_metro: int, n_or: int, do_swap: bool = True, n_cycles: int = 1) -> None:
         self._ck(self.lib.pyro_cycle(self.ctx, n_metro, n_or, int(bool(do_swap)), n_cycles))
+
+    def launch_count(self) -> int:
+        v = C.c_uint64()
+        self._ck(self.lib.pyro_get_launch_count(self.ctx, C.byref(v)))
+        return v.value
 
     def sweep_count(self) -> int:
         v = C.c_uint64()

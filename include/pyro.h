@@ -188,8 +188,11 @@ int pyro_enable_history(pyro_ctx* ctx, int capacity_cycles);
 /* Copies min(capacity, recorded) cycles of system `system`: out[c * n_temperatures + t]. */
 int pyro_get_history(pyro_ctx* ctx, int system, double* out, int* n_cycles);
 
-/* Counters: sweeps done so far (all systems advance together). */
+/* Counters: sweeps done so far (all systems advance together), and kernels
+ * launched by pyro_cycle / pyro_cycle_tet (graph replays count the kernels
+ * of the captured graph). */
 int pyro_get_sweep_count(pyro_ctx* ctx, uint64_t* sweeps);
+int pyro_get_launch_count(pyro_ctx* ctx, uint64_t* launches);
 
 /* Check that every spin is finite with |S|^2 within tol of 1; returns
  * PYRO_ERR_NAN and the first bad spin index otherwise. */
