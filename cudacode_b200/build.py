@@ -75,6 +75,22 @@ def build_engine(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+CLI = os.path.join(PKG, "pyro_run")
+
+
+def build_cli(force: bool = False) -> str:
+    """The C++ command-line driver (host code only), linked to libpyro.so."""
+    src = os.path.join(PKG, "host", "pyro_run.cpp")
+    deps = [src, os.path.join(PKG, "host", "pyro_host.hpp"), os.path.join(ROOT, "include", "pyro.h"),
+            LIB]
+    if not force and _newer(CLI, deps):
+        return CLI
+    cxx = shutil.which("g++") or "/usr/bin/g++"
+    subprocess.run([cxx, "-O2", "-std=c++17", "-Wall", src, "-o", CLI, "-L", PKG, "-lpyro",
+                    "-Wl,-rpath,$ORIGIN", "-Wl,--enable-new-dtags"], check=True)
+    return CLI
+
+
 def build_oracle(force: bool = False) -> str:
     """Compiles the host oracle (test infrastructure) with make."""
     subprocess.run(["make", "-s", "-C", ORACLE_DIR] + (["-B"] if force else []), check=True)
@@ -84,6 +100,7 @@ def build_oracle(force: bool = False) -> str:
 def main(argv: list[str]) -> int:
     force = "--force" in argv
     build_engine(force=force, verbose="-v" in argv)
+    build_cli(force=force)
     if "--engine" not in argv:
         build_oracle(force=force)
     return 0
