@@ -123,6 +123,9 @@ void tet_free(pyro_ctx* ctx);
 int queue_tet_sweeps(pyro_ctx* ctx, int n);
 // Adds n to the learned-move proposal count (acceptance statistics).
 void tet_count_sweeps(pyro_ctx* ctx, unsigned long long n);
+// Learned-move sweep counter (device), read / set synchronously.
+unsigned long long tet_counter(pyro_ctx* ctx);
+void tet_set_counter(pyro_ctx* ctx, unsigned long long v);
 
 }  // namespace pyro
 

@@ -119,6 +119,16 @@ TetMoveParams move_params(pyro_ctx* ctx, int si, unsigned long long off) {
 
 namespace pyro {
 
+unsigned long long tet_counter(pyro_ctx* ctx) {
+  unsigned long long v = 0;
+  if (ctx->tet) cudaMemcpy(&v, ctx->tet->d_ctr, 8, cudaMemcpyDeviceToHost);
+  return v;
+}
+
+void tet_set_counter(pyro_ctx* ctx, unsigned long long v) {
+  if (ctx->tet) cudaMemcpy(ctx->tet->d_ctr, &v, 8, cudaMemcpyHostToDevice);
+}
+
 void tet_count_sweeps(pyro_ctx* ctx, unsigned long long n) {
   if (ctx->tet) ctx->tet->proposed_sweeps += n;
 }

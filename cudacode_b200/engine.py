@@ -127,6 +127,10 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "pyro_tet_forward": (i, [P, pf, i, pf]),
         "pyro_tet_gradient": (i, [P, pf, pf, i, pf, pd]),
         "pyro_cycle_tet": (i, [P, i, i, i, i, i]),
+        "pyro_save_checkpoint": (i, [P, C.c_char_p]),
+        "pyro_load_checkpoint": (i, [P, C.c_char_p]),
+        "pyro_save_configurations": (i, [P, i, C.c_char_p, i]),
+        "pyro_read_configurations": (i, [P, i, C.c_char_p, i]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -401,6 +405,21 @@ class Engine:
         self._ck(self.lib.pyro_structure_factor(self.ctx, system, replica, G, stride,
                                                 _ptr(out, C.c_double)))
         return out
+
+    # -- checkpoint / configuration files ---------------------------------
+    def save_checkpoint(self, path: str) -> None:
+        self._ck(self.lib.pyro_save_checkpoint(self.ctx, os.fsencode(path)))
+
+    def load_checkpoint(self, path: str) -> None:
+        self._ck(self.lib.pyro_load_checkpoint(self.ctx, os.fsencode(path)))
+
+    def save_configurations(self, prefix: str, append: bool = False, system: int = 0) -> None:
+        self._ck(self.lib.pyro_save_configurations(self.ctx, system, os.fsencode(prefix),
+                                                   int(append)))
+
+    def read_configurations(self, prefix: str, repetition: int = 0, system: int = 0) -> None:
+        self._ck(self.lib.pyro_read_configurations(self.ctx, system, os.fsencode(prefix),
+                                                   repetition))
 
     # -- learned tetrahedron proposal -------------------------------------
     N_MLP_PARAMS = 6288

@@ -198,6 +198,25 @@ int pyro_get_launch_count(pyro_ctx* ctx, uint64_t* launches);
  * PYRO_ERR_NAN and the first bad spin index otherwise. */
 int pyro_check_spins(pyro_ctx* ctx, float tol, long long* first_bad);
 
+/* Checkpoint / resume: the whole chain state (spins, temperature labels,
+ * cone widths, sweep and exchange counters, learned-move weights and
+ * counter) in one file with a checksum. Philox is counter-based, so this is
+ * all a resumed run needs to continue bit for bit. Loading into a context
+ * created with another configuration gives PYRO_ERR_ARG; a missing, short
+ * or corrupt file PYRO_ERR_IO (nothing is changed then). Replaces the
+ * InitialConf%d.dat / Conf%d.dat files and --ContinueMeasurement of the
+ * reference (Math.cu:618-701, Pyrochlore.cu:1190-1194, 1528-1531). */
+int pyro_save_checkpoint(pyro_ctx* ctx, const char* path);
+int pyro_load_checkpoint(pyro_ctx* ctx, const char* path);
+/* The reference's configuration files (SaveConfigurations /
+ * ReadConfigurations, Math.cu:618-701): "<prefix><k>.dat" per temperature,
+ * k = 0 the highest, each repetition the spins as consecutive (x, y, z)
+ * doubles in site-plane-then-cell order; save appends a repetition if
+ * `append`, read loads repetition `repetition` into the replica that holds
+ * each temperature. */
+int pyro_save_configurations(pyro_ctx* ctx, int system, const char* prefix, int append);
+int pyro_read_configurations(pyro_ctx* ctx, int system, const char* prefix, int repetition);
+
 /* Static structure factor S(q) = (1/N) sum_a |sum_i S_i^a e^{-i q.r_i}|^2,
  * averaged over the replicas held, on a grid of G^3 wave vectors
  * q = (2 pi / L) * stride * (h, k, l), h, k, l in [-G/2, G/2); out[(h' G + k') G + l'].
