@@ -155,10 +155,14 @@ bool use_cycle_kernel(const pyro_ctx* ctx) {
 // Per-pass J1 kernels in replica groups: every sweep of one group of
 // rep_group replicas before the next group, so that a group's spins stay in
 // L2 across its passes. Same updates, same order within each replica.
-int queue_j1_grouped(pyro_ctx* ctx, int n_metro, int n_or) {
-  // Groups are dealt round-robin to `chains` streams that fork from and
-  // join back into the context stream (parallel branches of a captured
-  // graph), so one chain's launch gaps are filled by another's kernels.
+// Grouped schedule: J1 systems in groups of rep_group replicas (per-pass J1
+// kernels) and the other systems in groups of about gen_group_mb MB (generic
+// kernel), each group running all its sweeps before the next group, the
+// groups dealt round-robin to `chains` streams that fork from and join back
+// into the context stream (parallel branches of a captured graph), so a
+// group's spins stay in L2 across its passes and one chain's launch gaps are
+// filled by another's kernels. Same updates, same order within each replica.
+int queue_grouped(pyro_ctx* ctx, int n_metro, int n_or, bool j1_grouped, bool gen_grouped) {
   const int chains = std::max(1, std::min(ctx->n_chains, kMaxChains));
   if (chains > 1) {
     for (int c = 0; c < chains; ++c) {
@@ -172,21 +176,41 @@ int queue_j1_grouped(pyro_ctx* ctx, int n_metro, int n_or) {
     for (int c = 0; c < chains; ++c) PYRO_CK(cudaStreamWaitEvent(ctx->chain_stream[c], ctx->fork_event, 0));
   }
   int gi = 0;
-  for (int si : ctx->obs_j1) {
-    const SysDev& s = ctx->sys[si];
-    for (int r0 = 0; r0 < s.n_rep; r0 += ctx->rep_group, ++gi) {
+  if (j1_grouped) {
+    for (int si : ctx->obs_j1) {
+      const SysDev& s = ctx->sys[si];
+      for (int r0 = 0; r0 < s.n_rep; r0 += ctx->rep_group, ++gi) {
+        cudaStream_t st = chains > 1 ? ctx->chain_stream[gi % chains] : ctx->stream;
+        const int cnt = std::min(ctx->rep_group, s.n_rep - r0);
+        for (int k = 0; k < n_metro + n_or; ++k) {
+          const bool metro = k < n_metro;
+          for (int colour = 0; colour < 4; ++colour) {
+            J1PassParams p = j1_params(ctx, si, (unsigned long long)k);
+            p.spins += (long long)r0 * 16 * s.L3;
+            p.n_rep = cnt;
+            p.rep_global += r0;
+            p.rep_key += r0;
+            launch_j1_pass(p, colour, metro,
+                           metro ? ctx->j1_metro_site_mode : ctx->j1_or_site_mode, st);
+            PYRO_CK_LAUNCH();
+          }
+        }
+      }
+    }
+  }
+  if (gen_grouped) {
+    for (const auto& G : ctx->gen_groups) {
       cudaStream_t st = chains > 1 ? ctx->chain_stream[gi % chains] : ctx->stream;
-      const int cnt = std::min(ctx->rep_group, s.n_rep - r0);
+      ++gi;
       for (int k = 0; k < n_metro + n_or; ++k) {
         const bool metro = k < n_metro;
-        for (int colour = 0; colour < 4; ++colour) {
-          J1PassParams p = j1_params(ctx, si, (unsigned long long)k);
-          p.spins += (long long)r0 * 16 * s.L3;
-          p.n_rep = cnt;
-          p.rep_global += r0;
-          p.rep_key += r0;
-          launch_j1_pass(p, colour, metro, metro ? ctx->j1_metro_site_mode : ctx->j1_or_site_mode,
-                         st);
+        for (int pass = 0; pass < ctx->n_passes; ++pass) {
+          if (G.pass_blocks[pass] == 0) continue;
+          PassParams p = pass_params(ctx, pass);
+          p.segs = G.d_pass_segs[pass];
+          p.nseg = (int)G.pass_segs[pass].size();
+          p.sweep_off = (unsigned long long)k;
+          launch_colour_pass(p, ctx->tab, G.pass_blocks[pass], metro, false, st);
           PYRO_CK_LAUNCH();
         }
       }
@@ -201,16 +225,50 @@ int queue_j1_grouped(pyro_ctx* ctx, int n_metro, int n_or) {
   return PYRO_OK;
 }
 
+// Generic (non-J1-path) sweeps of every system, ungrouped.
+int queue_generic_sweeps(pyro_ctx* ctx, int n_metro, int n_or) {
+  int rc = PYRO_OK;
+  for (int i = 0; i < n_metro && rc == PYRO_OK; ++i) rc = queue_sweep(ctx, true, i, true);
+  for (int i = 0; i < n_or && rc == PYRO_OK; ++i) rc = queue_sweep(ctx, false, n_metro + i, true);
+  return rc;
+}
+
 int queue_cycle_body(pyro_ctx* ctx, int n_metro, int n_or, bool with_obs) {
   int rc = check_cluster(ctx);
   if (rc) return rc;
   const bool cyc = use_cycle_kernel(ctx);
-  if (!cyc && ctx->rep_group > 0 && ctx->use_j1_kernel && !ctx->obs_j1.empty()) {
-    rc = queue_j1_grouped(ctx, n_metro, n_or);
-    for (int i = 0; i < n_metro && rc == PYRO_OK; ++i) rc = queue_sweep(ctx, true, i, true);
-    for (int i = 0; i < n_or && rc == PYRO_OK; ++i) rc = queue_sweep(ctx, false, n_metro + i, true);
+  const bool j1_grouped = !cyc && ctx->rep_group > 0 && ctx->use_j1_kernel && !ctx->obs_j1.empty();
+  const bool gen_grouped = !ctx->gen_groups.empty();
+  if (j1_grouped || gen_grouped) {
+    rc = queue_grouped(ctx, n_metro, n_or, j1_grouped, gen_grouped);
     if (rc) return rc;
-    if (with_obs) rc = queue_observables(ctx, false);
+    if (!gen_grouped) rc = queue_generic_sweeps(ctx, n_metro, n_or);
+    if (rc) return rc;
+    if (!j1_grouped) {  // J1 systems ungrouped: their per-pass kernels or the cluster kernel
+      if (cyc) {
+        for (int si : ctx->obs_j1) {
+          J1CycleParams cp;
+          cp.pass = j1_params(ctx, si, 0);
+          cp.n_metro = n_metro;
+          cp.n_or = n_or;
+          cp.cluster_size = ctx->cluster_size;
+          cp.J1_64 = ctx->sys[si].J64[0];
+          cp.partials = with_obs ? ctx->d_partials : nullptr;
+          cp.partial_begin = ctx->obs_segs[si].partial_begin;
+          PYRO_CK(launch_j1_cycle(cp, ctx->stream));
+        }
+      } else {
+        for (int k = 0; k < n_metro + n_or; ++k)
+          for (int pass = 0; pass < ctx->n_passes; ++pass)
+            for (const auto& sc : ctx->pass_j1[pass]) {
+              const bool metro = k < n_metro;
+              launch_j1_pass(j1_params(ctx, sc.first, (unsigned long long)k), sc.second, metro,
+                             metro ? ctx->j1_metro_site_mode : ctx->j1_or_site_mode, ctx->stream);
+              PYRO_CK_LAUNCH();
+            }
+      }
+    }
+    if (with_obs) rc = queue_observables(ctx, cyc && !j1_grouped);
     return rc;
   }
   if (cyc) {
@@ -275,6 +333,10 @@ bool sharded(const pyro_ctx* ctx) {
 
 void free_all(pyro_ctx* c) {
   tet_free(c);
+  for (auto& g : c->gen_groups)
+    for (auto* p : g.d_pass_segs)
+      if (p) cudaFree(p);
+  c->gen_groups.clear();
   for (int i = 0; i < kMaxChains; ++i) {
     if (c->chain_stream[i]) cudaStreamDestroy(c->chain_stream[i]);
     if (c->chain_event[i]) cudaEventDestroy(c->chain_event[i]);
@@ -336,6 +398,7 @@ int build_schedule(pyro_ctx* ctx) {
       g.colour = colour;
       g.blocks_per_rep = (s.units_per_colour + kPassThreads - 1) / kPassThreads;
       g.block_begin = blocks;
+      g.rep_begin = 0;
       blocks += g.blocks_per_rep * s.n_rep;
       ctx->pass_segs[pass].push_back(g);
     }
@@ -380,6 +443,65 @@ int build_schedule(pyro_ctx* ctx) {
     if (!ctx->pass_segs[pass].empty())
       PYRO_CK(cudaMemcpy(ctx->d_pass_segs[pass], ctx->pass_segs[pass].data(),
                          sizeof(PassSeg) * ctx->pass_segs[pass].size(), cudaMemcpyHostToDevice));
+  }
+  // Replica groups of the generic path: consecutive (system, replica) ranges
+  // of about gen_group_mb MB each; every group gets its own segment list per
+  // pass, so all its sweeps can run while its spins stay in L2.
+  for (auto& g : ctx->gen_groups)
+    for (auto* p : g.d_pass_segs)
+      if (p) cudaFree(p);
+  ctx->gen_groups.clear();
+  if (ctx->gen_group_mb > 0) {
+    const double budget = (double)ctx->gen_group_mb * 1048576.0;
+    struct Range { int sys, r0, n; };
+    std::vector<std::vector<Range>> groups(1);
+    double bytes = 0.0;
+    for (int i = 0; i < (int)ctx->sys.size(); ++i) {
+      const SysDev& s = ctx->sys[i];
+      if (j1_path(s)) continue;
+      const double per_rep = 16.0 * 16.0 * s.L3;
+      for (int r = 0; r < s.n_rep; ++r) {
+        if (bytes > 0.0 && bytes + per_rep > budget) {
+          groups.emplace_back();
+          bytes = 0.0;
+        }
+        auto& cur = groups.back();
+        if (!cur.empty() && cur.back().sys == i && cur.back().r0 + cur.back().n == r) ++cur.back().n;
+        else cur.push_back({i, r, 1});
+        bytes += per_rep;
+      }
+    }
+    if (groups.back().empty()) groups.pop_back();
+    for (const auto& gr : groups) {
+      pyro_ctx::GenGroup G;
+      G.pass_segs.assign(ctx->n_passes, {});
+      G.pass_blocks.assign(ctx->n_passes, 0);
+      G.d_pass_segs.assign(ctx->n_passes, nullptr);
+      for (int pass = 0; pass < ctx->n_passes; ++pass) {
+        int blocks = 0;
+        for (const Range& rg : gr) {
+          const SysDev& s = ctx->sys[rg.sys];
+          int colour = -1;
+          if (s.n_colours == ctx->n_passes) colour = pass;
+          else if (pass % 4 == 0) colour = pass / 4;
+          if (colour < 0) continue;
+          PassSeg g;
+          g.sys = rg.sys;
+          g.colour = colour;
+          g.blocks_per_rep = (s.units_per_colour + kPassThreads - 1) / kPassThreads;
+          g.block_begin = blocks;
+          g.rep_begin = rg.r0;
+          blocks += g.blocks_per_rep * rg.n;
+          G.pass_segs[pass].push_back(g);
+        }
+        G.pass_blocks[pass] = blocks;
+        PYRO_CK(alloc(&G.d_pass_segs[pass], G.pass_segs[pass].size()));
+        if (!G.pass_segs[pass].empty())
+          PYRO_CK(cudaMemcpy(G.d_pass_segs[pass], G.pass_segs[pass].data(),
+                             sizeof(PassSeg) * G.pass_segs[pass].size(), cudaMemcpyHostToDevice));
+      }
+      ctx->gen_groups.push_back(std::move(G));
+    }
   }
   return PYRO_OK;
 }
@@ -640,6 +762,9 @@ int pyro_set_option(pyro_ctx* ctx, int option, int value) {
   if (option == PYRO_OPT_J1_KERNEL) {
     if (value != 0 && value != 1) return fail(ctx, PYRO_ERR_ARG, "J1 kernel option is 0 or 1");
     ctx->use_j1_kernel = value == 1;
+  } else if (option == PYRO_OPT_GROUP_MB) {
+    if (value < 0) return fail(ctx, PYRO_ERR_ARG, "group size in MB must be >= 0");
+    ctx->gen_group_mb = value;
   } else if (option == PYRO_OPT_CHAINS) {
     if (value < 1 || value > kMaxChains) return fail(ctx, PYRO_ERR_ARG, "chains is 1..4");
     ctx->n_chains = value;
@@ -681,6 +806,7 @@ int pyro_get_option(pyro_ctx* ctx, int option, int* value) {
     case PYRO_OPT_SMEM_KERNEL: *value = ctx->smem_kernel; break;
     case PYRO_OPT_REPLICA_GROUP: *value = ctx->rep_group; break;
     case PYRO_OPT_CHAINS: *value = ctx->n_chains; break;
+    case PYRO_OPT_GROUP_MB: *value = ctx->gen_group_mb; break;
     case PYRO_OPT_J1_SITE_MODE:
       *value = (ctx->j1_metro_site_mode ? 1 : 0) | (ctx->j1_or_site_mode ? 2 : 0);
       break;
@@ -695,28 +821,63 @@ int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen)
   if (!ctx) return PYRO_ERR_ARG;
   if (cycles < 1 || n_metro < 0 || n_or < 0 || n_metro + n_or < 1)
     return fail(ctx, PYRO_ERR_ARG, "autotune: need cycles >= 1 and at least one sweep");
-  struct Variant { int j1, cyc, cs, site, group, chains; };
-  const Variant vs[] = {{0, 0, 16, 1, 0, 1}, {1, 0, 16, 1, 0, 1}, {1, 0, 16, 1, 8, 1},
-                        {1, 0, 16, 1, 4, 2}, {1, 0, 16, 3, 4, 2}, {1, 0, 16, 1, 3, 2},
-                        {1, 0, 16, 1, 2, 2}, {1, 0, 16, 1, 2, 3}, {1, 0, 16, 1, 3, 3},
-                        {1, 0, 16, 1, 2, 4}, {1, 0, 16, 1, 1, 4}, {1, 1, 10, 1, 0, 1}};
+  struct Variant { int j1, cyc, cs, site, group, chains, gen_mb; };
+  bool any_j1 = false, any_gen = false;
+  for (const auto& s : ctx->sys) {
+    if (s.n_colours == 4 && s.shells == 1) any_j1 = true;
+    else any_gen = true;
+  }
+  std::vector<Variant> vs;
+  if (any_j1) {
+    const Variant j1v[] = {{0, 0, 16, 1, 0, 1, 0}, {1, 0, 16, 1, 0, 1, 0}, {1, 0, 16, 3, 0, 1, 0},
+                           {1, 0, 16, 1, 8, 1, 0}, {1, 0, 16, 1, 4, 2, 0}, {1, 0, 16, 3, 4, 2, 0},
+                           {1, 0, 16, 1, 3, 2, 0}, {1, 0, 16, 1, 2, 2, 0}, {1, 0, 16, 1, 2, 3, 0},
+                           {1, 0, 16, 1, 3, 3, 0}, {1, 0, 16, 1, 2, 4, 0}, {1, 0, 16, 1, 1, 4, 0},
+                           {1, 1, 16, 1, 0, 1, 0}, {1, 1, 10, 1, 0, 1, 0}};
+    vs.insert(vs.end(), std::begin(j1v), std::end(j1v));
+  }
+  if (any_gen) {
+    const int base = vs.size();  // filled with the best J1 knobs after stage 1
+    const Variant gv[] = {{1, 0, 16, 1, 0, 1, 0},  {1, 0, 16, 1, 0, 1, 24}, {1, 0, 16, 1, 0, 1, 40},
+                          {1, 0, 16, 1, 0, 1, 64}, {1, 0, 16, 1, 0, 2, 24}, {1, 0, 16, 1, 0, 2, 40},
+                          {1, 0, 16, 1, 0, 3, 24}};
+    vs.insert(vs.end(), std::begin(gv), std::end(gv));
+    (void)base;
+  }
   const bool swap = !sharded(ctx);
   cudaEvent_t a, b;
   PYRO_CK(cudaEventCreate(&a));
   PYRO_CK(cudaEventCreate(&b));
+  auto apply = [&](const Variant& v) {
+    int rc = pyro_set_option(ctx, PYRO_OPT_J1_KERNEL, v.j1);
+    if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_CYCLE_KERNEL, v.cyc);
+    if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_CLUSTER_SIZE, v.cs);
+    if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_J1_SITE_MODE, v.site);
+    if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_REPLICA_GROUP, v.group);
+    if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_CHAINS, v.chains);
+    if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_GROUP_MB, v.gen_mb);
+    if (!rc) rc = check_cluster(ctx);
+    return rc;
+  };
   float best = 1e30f;
   int best_i = -1;
-  const int n_var = (int)(sizeof(vs) / sizeof(vs[0]));
-  for (int i = 0; i < n_var; ++i) {
-    int rc = pyro_set_option(ctx, PYRO_OPT_J1_KERNEL, vs[i].j1);
-    if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_CYCLE_KERNEL, vs[i].cyc);
-    if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_CLUSTER_SIZE, vs[i].cs);
-    if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_J1_SITE_MODE, vs[i].site);
-    if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_REPLICA_GROUP, vs[i].group);
-    if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_CHAINS, vs[i].chains);
-    if (!rc) rc = check_cluster(ctx);
+  const int n_j1 = any_j1 ? 14 : 0;
+  for (int i = 0; i < (int)vs.size(); ++i) {
+    Variant v = vs[i];
+    if (i >= n_j1 && best_i >= 0 && best_i < n_j1) {
+      // stage 2 (generic groups) keeps the J1 knobs of stage 1's winner
+      const Variant& w = vs[best_i];
+      v.j1 = w.j1;
+      v.cyc = w.cyc;
+      v.cs = w.cs;
+      v.site = w.site;
+      v.group = w.group;
+      if (v.chains == 1) v.chains = w.chains;
+      vs[i] = v;
+    }
+    int rc = apply(v);
     if (rc) continue;
-    if (vs[i].cyc && (ctx->cycle_kernel != 1 || ctx->cluster_size != vs[i].cs)) continue;
+    if (v.cyc && (ctx->cycle_kernel != 1 || ctx->cluster_size != v.cs)) continue;
     if ((rc = pyro_cycle(ctx, n_metro, n_or, swap, 1))) return rc;  // build the graph
     float ms = 1e30f;
     for (int rep = 0; rep < 2; ++rep) {  // best of two timings
@@ -736,13 +897,7 @@ int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen)
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   if (best_i < 0) return fail(ctx, PYRO_ERR_STATE, "autotune: no variant ran");
-  const Variant& w = vs[best_i];
-  int rc = pyro_set_option(ctx, PYRO_OPT_J1_KERNEL, w.j1);
-  if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_CYCLE_KERNEL, w.cyc);
-  if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_CLUSTER_SIZE, w.cs);
-  if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_J1_SITE_MODE, w.site);
-  if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_REPLICA_GROUP, w.group);
-  if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_CHAINS, w.chains);
+  int rc = apply(vs[best_i]);
   if (chosen) *chosen = best_i;
   return rc;
 }

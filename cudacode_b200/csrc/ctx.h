@@ -75,6 +75,13 @@ struct pyro_ctx {
   int cycle_kernel = 0;
   int smem_kernel = 1;
   int rep_group = 0;    // per-pass J1 kernels over groups of this many replicas (0: all)
+  int gen_group_mb = 0; // generic kernels over groups of replicas of about this many MB (0: off)
+  struct GenGroup {
+    std::vector<std::vector<pyro::PassSeg>> pass_segs;  // per pass
+    std::vector<int> pass_blocks;
+    std::vector<pyro::PassSeg*> d_pass_segs;
+  };
+  std::vector<GenGroup> gen_groups;
   int n_chains = 1;     // concurrent streams the replica groups are dealt to
   cudaStream_t chain_stream[pyro::kMaxChains] = {};
   cudaEvent_t chain_event[pyro::kMaxChains] = {};

@@ -78,8 +78,9 @@ __global__ void __launch_bounds__(kPassThreads) colour_pass_kernel(const PassPar
   const PassSeg sg = p.segs[seg_i];
   const SysDev& sd = p.sys[sg.sys];
   const int rel = blockIdx.x - sg.block_begin;
-  const int rep = rel / sg.blocks_per_rep;
-  const int u = (rel - rep * sg.blocks_per_rep) * kPassThreads + threadIdx.x;
+  const int rep_in_seg = rel / sg.blocks_per_rep;
+  const int rep = sg.rep_begin + rep_in_seg;
+  const int u = (rel - rep_in_seg * sg.blocks_per_rep) * kPassThreads + threadIdx.x;
   const bool active = u < sd.units_per_colour;
   const int L = sd.L, L3 = sd.L3;
 

@@ -91,6 +91,7 @@ struct PassSeg {
   int colour;          // colour class
   int blocks_per_rep;  // CTAs per replica
   int block_begin;     // first CTA of the segment in the launch
+  int rep_begin;       // first replica of the system covered by the segment
 };
 
 // Per-system constants in device memory.

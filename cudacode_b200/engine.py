@@ -240,6 +240,7 @@ class Engine:
     OPT_SMEM_KERNEL = 5
     OPT_REPLICA_GROUP = 6
     OPT_CHAINS = 7
+    OPT_GROUP_MB = 8
 
     def set_option(self, option: int, value: int) -> None:
         self._ck(self.lib.pyro_set_option(self.ctx, option, value))

@@ -98,6 +98,11 @@ int pyro_neighbour_table(int site, int* out120);
 /* PYRO_OPT_CHAINS: 1..4 concurrent streams (parallel branches of the cycle
  * graph) the replica groups are dealt to. Identical results. */
 #define PYRO_OPT_CHAINS 7
+/* PYRO_OPT_GROUP_MB: run the generic (J2/J3) colour passes over groups of
+ * replicas of about this many MB, all sweeps of a group before the next,
+ * groups dealt to the PYRO_OPT_CHAINS streams (0, default: off).
+ * Identical results. */
+#define PYRO_OPT_GROUP_MB 8
 int pyro_set_option(pyro_ctx* ctx, int option, int value);
 int pyro_get_option(pyro_ctx* ctx, int option, int* value);
 /* Autotuner: times every kernel variant (per-pass generic, per-pass J1,

@@ -313,6 +313,26 @@ def test_replica_groups_bit_exact(group, chains):
     assert np.array_equal(e.permutation(), o.permutation())
 
 
+@pytest.mark.parametrize("mb,chains", [(1, 1), (1, 2), (3, 3)])
+def test_generic_groups_bit_exact(mb, chains):
+    rng = np.random.default_rng(3)
+    systems = [System(L=L, temperatures=geometric_ladder(0.05, 1.5, nt), J2=float(j2), J3=float(j3))
+               for L, nt, (j2, j3) in [(4, 5, rng.uniform(-0.1, 0.1, 2)), (5, 3, (0.05, 0.02)),
+                                       (3, 4, (-0.03, 0.06))]]
+    systems.append(System(L=4, temperatures=[0.2, 0.5, 1.0]))  # J1 system in the same context
+    e, o = pair(systems, renorm_every=4)
+    e.set_option(e.OPT_GROUP_MB, mb)
+    e.set_option(e.OPT_CHAINS, chains)
+    e.set_option(e.OPT_REPLICA_GROUP, 2)
+    e.init_random()
+    o.init_random()
+    e.cycle(1, 3, True, 3)
+    o.cycle(1, 3, True, 3)
+    for k in range(len(systems)):
+        assert np.array_equal(e.get_spins(k), o.get_spins(k)), k
+        assert np.array_equal(e.permutation(k), o.permutation(k)), k
+
+
 def test_autotune_keeps_results_exact():
     temps = geometric_ladder(0.05, 1.0, 4)
     e, o = pair([System(L=8, temperatures=temps)])
