@@ -21,6 +21,7 @@
 #include "j1_kernels.cuh"
 #include "kernels.cuh"
 #include "lattice.h"
+#include "far_kernels.cuh"
 #include "smem_kernels.cuh"
 #include "sq_kernels.cuh"
 
@@ -87,8 +88,11 @@ int queue_sweep(pyro_ctx* ctx, bool metro, unsigned long long off, bool skip_j1 
     if (ctx->pass_blocks[pass] == 0) continue;
     PassParams p = pass_params(ctx, pass);
     p.sweep_off = off;
-    launch_colour_pass(p, ctx->tab, ctx->pass_blocks[pass], metro, /*j1_only=*/false,
-                       ctx->stream);
+    if (ctx->far_kernel && ctx->pass_all16[pass])
+      launch_far_pass(p, pass, ctx->pass_blocks[pass], metro, ctx->stream);
+    else
+      launch_colour_pass(p, ctx->tab, ctx->pass_blocks[pass], metro, /*j1_only=*/false,
+                         ctx->stream);
     PYRO_CK_LAUNCH();
   }
   return PYRO_OK;
@@ -210,7 +214,10 @@ int queue_grouped(pyro_ctx* ctx, int n_metro, int n_or, bool j1_grouped, bool ge
           p.segs = G.d_pass_segs[pass];
           p.nseg = (int)G.pass_segs[pass].size();
           p.sweep_off = (unsigned long long)k;
-          launch_colour_pass(p, ctx->tab, G.pass_blocks[pass], metro, false, st);
+          if (ctx->far_kernel && G.all16[pass])
+            launch_far_pass(p, pass, G.pass_blocks[pass], metro, st);
+          else
+            launch_colour_pass(p, ctx->tab, G.pass_blocks[pass], metro, false, st);
           PYRO_CK_LAUNCH();
         }
       }
@@ -404,6 +411,10 @@ int build_schedule(pyro_ctx* ctx) {
     }
     ctx->pass_blocks[pass] = blocks;
   }
+  ctx->pass_all16.assign(ctx->n_passes, 1);
+  for (int pass = 0; pass < ctx->n_passes; ++pass)
+    for (const PassSeg& g : ctx->pass_segs[pass])
+      if (ctx->sys[g.sys].n_colours != 16) ctx->pass_all16[pass] = 0;
   ctx->obs_segs.clear();
   ctx->obs_generic.clear();
   ctx->obs_j1.clear();
@@ -477,6 +488,7 @@ int build_schedule(pyro_ctx* ctx) {
       G.pass_segs.assign(ctx->n_passes, {});
       G.pass_blocks.assign(ctx->n_passes, 0);
       G.d_pass_segs.assign(ctx->n_passes, nullptr);
+      G.all16.assign(ctx->n_passes, 1);
       for (int pass = 0; pass < ctx->n_passes; ++pass) {
         int blocks = 0;
         for (const Range& rg : gr) {
@@ -493,6 +505,7 @@ int build_schedule(pyro_ctx* ctx) {
           g.rep_begin = rg.r0;
           blocks += g.blocks_per_rep * rg.n;
           G.pass_segs[pass].push_back(g);
+          if (s.n_colours != 16) G.all16[pass] = 0;
         }
         G.pass_blocks[pass] = blocks;
         PYRO_CK(alloc(&G.d_pass_segs[pass], G.pass_segs[pass].size()));
@@ -648,6 +661,7 @@ int pyro_create(const pyro_config* cfg, pyro_ctx** out) {
     s.temp_base = temp_base;
     s.n_temp = d.n_temperatures;
     s.spin_off = spin_off;
+    s.rcpL = 1.0f / (float)d.L;
     s.J1 = (float)d.J1;
     s.J2 = (float)d.J2;
     s.J3a = (float)d.J3;
@@ -762,6 +776,9 @@ int pyro_set_option(pyro_ctx* ctx, int option, int value) {
   if (option == PYRO_OPT_J1_KERNEL) {
     if (value != 0 && value != 1) return fail(ctx, PYRO_ERR_ARG, "J1 kernel option is 0 or 1");
     ctx->use_j1_kernel = value == 1;
+  } else if (option == PYRO_OPT_FAR_KERNEL) {
+    if (value != 0 && value != 1) return fail(ctx, PYRO_ERR_ARG, "far kernel option is 0 or 1");
+    ctx->far_kernel = value;
   } else if (option == PYRO_OPT_GROUP_MB) {
     if (value < 0) return fail(ctx, PYRO_ERR_ARG, "group size in MB must be >= 0");
     ctx->gen_group_mb = value;
@@ -807,6 +824,7 @@ int pyro_get_option(pyro_ctx* ctx, int option, int* value) {
     case PYRO_OPT_REPLICA_GROUP: *value = ctx->rep_group; break;
     case PYRO_OPT_CHAINS: *value = ctx->n_chains; break;
     case PYRO_OPT_GROUP_MB: *value = ctx->gen_group_mb; break;
+    case PYRO_OPT_FAR_KERNEL: *value = ctx->far_kernel; break;
     case PYRO_OPT_J1_SITE_MODE:
       *value = (ctx->j1_metro_site_mode ? 1 : 0) | (ctx->j1_or_site_mode ? 2 : 0);
       break;

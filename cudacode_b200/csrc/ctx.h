@@ -80,7 +80,10 @@ struct pyro_ctx {
     std::vector<std::vector<pyro::PassSeg>> pass_segs;  // per pass
     std::vector<int> pass_blocks;
     std::vector<pyro::PassSeg*> d_pass_segs;
+    std::vector<char> all16;  // every segment of the pass is a 16-colour system
   };
+  std::vector<char> pass_all16;  // same, for the ungrouped generic lists
+  int far_kernel = 1;  // compile-time-offset kernel for 16-colour passes
   std::vector<GenGroup> gen_groups;
   int n_chains = 1;     // concurrent streams the replica groups are dealt to
   cudaStream_t chain_stream[pyro::kMaxChains] = {};

@@ -69,6 +69,49 @@ PYRO_HOSTDEV constexpr NbrEntry j1_neighbour(int s, int k) {
   return NbrEntry{0, 0, 0, -1};
 }
 
+// Compile-time form of the full canonical table (all four shells): entry k
+// (0..29) of site s, enumerated in the order (shell, target site, dx, dy, dz)
+// exactly as build_neighbour_table sorts it.
+PYRO_HOSTDEV constexpr int site_at4(int x, int y, int z) {
+  const int F[4][3] = {{0, 0, 0}, {2, 2, 0}, {0, 2, 2}, {2, 0, 2}};
+  x &= 3;
+  y &= 3;
+  z &= 3;
+  for (int t = 0; t < kSitesPerCell; ++t)
+    if (F[t >> 2][0] + F[t & 3][0] / 2 == x && F[t >> 2][1] + F[t & 3][1] / 2 == y &&
+        F[t >> 2][2] + F[t & 3][2] / 2 == z)
+      return t;
+  return -1;
+}
+
+PYRO_HOSTDEV constexpr NbrEntry far_neighbour(int s, int k) {
+  const int F[4][3] = {{0, 0, 0}, {2, 2, 0}, {0, 2, 2}, {2, 0, 2}};
+  const int px = F[s >> 2][0] + F[s & 3][0] / 2, py = F[s >> 2][1] + F[s & 3][1] / 2,
+            pz = F[s >> 2][2] + F[s & 3][2] / 2;
+  int found = 0;
+  for (int shell = 0; shell < 4; ++shell)
+    for (int t = 0; t < kSitesPerCell; ++t)
+      for (int dx = -1; dx <= 1; ++dx)
+        for (int dy = -1; dy <= 1; ++dy)
+          for (int dz = -1; dz <= 1; ++dz) {
+            const int vx = 4 * dx + F[t >> 2][0] + F[t & 3][0] / 2 - px;
+            const int vy = 4 * dy + F[t >> 2][1] + F[t & 3][1] / 2 - py;
+            const int vz = 4 * dz + F[t >> 2][2] + F[t & 3][2] / 2 - pz;
+            const int r2 = vx * vx + vy * vy + vz * vz;
+            int sh = -1;
+            if (r2 == 2) sh = 0;
+            else if (r2 == 6) sh = 1;
+            else if (r2 == 8) {
+              const bool even = vx % 2 == 0 && vy % 2 == 0 && vz % 2 == 0;
+              sh = even && site_at4(px + vx / 2, py + vy / 2, pz + vz / 2) >= 0 ? 2 : 3;
+            }
+            if (sh != shell) continue;
+            if (found == k) return NbrEntry{(int8_t)dx, (int8_t)dy, (int8_t)dz, (int8_t)t};
+            ++found;
+          }
+  return NbrEntry{0, 0, 0, -1};
+}
+
 // Canonical index of the j-th (0..2) nearest neighbour of site s that is not
 // in s's own up-tetrahedron (same cell, same FCC corner): its down-tetrahedron
 // partners.
@@ -106,6 +149,7 @@ struct SysDev {
   int temp_base;       // offset of this system's temperature arrays
   int n_temp;          // ladder size
   long long spin_off;  // float4 offset of replica 0
+  float rcpL;              // 1 / L (cell decode)
   float J1, J2, J3a, J3b;   // FP32 couplings of the update arithmetic
   double J64[4];           // the same couplings in FP64 for the observables
   int shells;          // bitmask of non-zero shells: 1 J1, 2 J2, 4 J3a, 8 J3b

@@ -103,6 +103,10 @@ int pyro_neighbour_table(int site, int* out120);
  * groups dealt to the PYRO_OPT_CHAINS streams (0, default: off).
  * Identical results. */
 #define PYRO_OPT_GROUP_MB 8
+/* PYRO_OPT_FAR_KERNEL: 1 (default) runs 16-colour passes (J2/J3 systems) on
+ * the kernel with compile-time neighbour offsets, 0 on the generic kernel.
+ * Identical results. */
+#define PYRO_OPT_FAR_KERNEL 9
 int pyro_set_option(pyro_ctx* ctx, int option, int value);
 int pyro_get_option(pyro_ctx* ctx, int option, int* value);
 /* Autotuner: times every kernel variant (per-pass generic, per-pass J1,

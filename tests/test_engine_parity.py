@@ -62,9 +62,11 @@ def test_plain_sweeps_100_per_spin(L, R):
     assert e.sweep_count() == o.sweep_count() == 100
 
 
-def test_further_neighbour_sixteen_colours():
+@pytest.mark.parametrize("far", [0, 1])
+def test_further_neighbour_sixteen_colours(far):
     s = System(L=4, temperatures=[0.2, 0.7], J1=1.0, J2=-0.08, J3=0.06, J3b=0.03)
     e, o = pair([s])
+    e.set_option(e.OPT_FAR_KERNEL, far)
     assert e.info()["n_colours"] == 16
     e.init_random()
     o.init_random()
