@@ -36,7 +36,7 @@ struct TetState {
   long long written = 0;  // samples ever written
   int adam_step = 0;
   uint64_t seed = 0;
-  int sweep_kernel = 0;   // 1: cluster kernel (one launch per call) when it fits
+  int sweep_kernel = 2;   // 0 per pass, 1 cluster (one launch per call), 2 per pass, lane pairs
   int cluster_max = 8;    // largest cluster size tried
   int cluster_ok = -1;    // -1 unknown, else the usable size (0: none)
 };
@@ -136,7 +136,7 @@ void tet_count_sweeps(pyro_ctx* ctx, unsigned long long n) {
 // Queues n tetrahedron sweeps (4 passes each) over every J1-only system;
 // offsets from the device counter, which this call advances.
 int queue_tet_sweeps(pyro_ctx* ctx, int n) {
-  TetState* t = ctx->tet;
+  TetState* t = ctx->tet;  // sweep_kernel: 0 per pass, 1 cluster, 2 per pass with lane pairs
   if (t->sweep_kernel == 1 && t->cluster_ok != 0) {
     if (t->cluster_ok < 0) {
       t->cluster_ok = 0;
@@ -164,7 +164,8 @@ int queue_tet_sweeps(pyro_ctx* ctx, int n) {
     for (int f = 0; f < 4; ++f)
       for (int si = 0; si < (int)ctx->sys.size(); ++si) {
         if (!j1_only_system(ctx->sys[si])) continue;
-        launch_tet_move(move_params(ctx, si, (unsigned long long)k), f, ctx->stream);
+        launch_tet_move(move_params(ctx, si, (unsigned long long)k), f, t->sweep_kernel == 2,
+                        ctx->stream);
         PYRO_CK_LAUNCH();
       }
   launch_advance(ctx->tet->d_ctr, (unsigned long long)n, ctx->stream);
@@ -243,7 +244,7 @@ int pyro_tet_get_weights(pyro_ctx* ctx, float* w, int n) {
 int pyro_tet_set_kernel(pyro_ctx* ctx, int cluster) {
   int rc = need_tet(ctx);
   if (rc) return rc;
-  if (cluster != 0 && cluster != 1) return fail(ctx, PYRO_ERR_ARG, "tet kernel option is 0 or 1");
+  if (cluster < 0 || cluster > 2) return fail(ctx, PYRO_ERR_ARG, "tet kernel option is 0, 1 or 2");
   PYRO_CK(cudaSetDevice(ctx->device));
   PYRO_CK(cudaStreamSynchronize(ctx->stream));
   ctx->tet->sweep_kernel = cluster;

@@ -442,6 +442,119 @@ __device__ __forceinline__ int tet_warp_step(const TetMoveParams& p, const MlpSm
   return accepted;
 }
 
+// Same move with two lanes per tetrahedron (16 per warp, one MMA m-tile):
+// lane l < 16 handles sites 0 and 1 of tetrahedron l, lane l + 16 sites 2
+// and 3 (their fields, proposals and stores), which halves the serial work
+// of a warp. Lane l then gathers the partner's values and evaluates the
+// energy change and the proposal ratio with exactly the single-lane
+// expressions, so the decisions are identical. Returns 1 on the lower lane
+// of an accepted move.
+template <int F, bool kL2>
+__device__ __forceinline__ int tet_pair_step(const TetMoveParams& p, const MlpSmem& w, bool active,
+                                             int rep, int cell, float beta,
+                                             unsigned long long sweep, __nv_bfloat16* feat,
+                                             float* out) {
+  const int lane = threadIdx.x & 31;
+  const int half = lane >> 4;  // 0: sites 0, 1; 1: sites 2, 3
+  const int row = lane & 15;
+  const float4* rb = p.spins + (long long)rep * 16 * p.L3;
+  pyro_vec3 h[2], s[2];
+  if (active) {
+    const Frame fr = cell_frame(cell, p.L, p.rcpL);
+    if (half == 0) {
+      h[0] = ext_field<4 * F + 0, kL2>(rb, fr, p.L3, p.J1);
+      h[1] = ext_field<4 * F + 1, kL2>(rb, fr, p.L3, p.J1);
+    } else {
+      h[0] = ext_field<4 * F + 2, kL2>(rb, fr, p.L3, p.J1);
+      h[1] = ext_field<4 * F + 3, kL2>(rb, fr, p.L3, p.J1);
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const float4 v = ld_spin<kL2>(rb + (4 * F + 2 * half + k) * p.L3 + cell);
+      s[k].x = v.x;
+      s[k].y = v.y;
+      s[k].z = v.z;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      h[k].x = h[k].y = h[k].z = 0.0f;
+      s[k].x = s[k].y = 0.0f;
+      s[k].z = 1.0f;
+    }
+  }
+  __nv_bfloat16* frow = feat + row * kLdIn;
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const int c = 3 * (2 * half + k);
+    frow[c] = __float2bfloat16_rn(h[k].x * (1.0f / 3.0f));
+    frow[c + 1] = __float2bfloat16_rn(h[k].y * (1.0f / 3.0f));
+    frow[c + 2] = __float2bfloat16_rn(h[k].z * (1.0f / 3.0f));
+  }
+  if (half == 0) {
+    frow[12] = __float2bfloat16_rn(logf(active ? beta : 1.0f) * (1.0f / 3.0f));
+    frow[13] = frow[14] = frow[15] = __float2bfloat16_rn(0.0f);
+  }
+  __syncwarp();
+  TileFwd fw;
+  tile_forward<false>(feat, 0, w, fw, nullptr, nullptr);
+  store_out(fw, 0, out);
+  __syncwarp();
+  // this lane's two sites: network outputs 8 * half .. 8 * half + 7
+  float o[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) o[i] = out[row * kLdOut + i];
+  const VmfParams vm = vmf_params(o);
+  const uint32_t key_tet = (uint32_t)(F * p.L3 + cell);
+  uint32_t r[4];
+  pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + half,
+              p.seed_lo, p.seed_hi, r);
+  pyro_vec3 sn[2];
+  sn[0] = vmf_sample(vm.mu[2 * half], vm.kappa[2 * half], pyro_uniform(r[0]), pyro_uniform(r[1]));
+  sn[1] = vmf_sample(vm.mu[2 * half + 1], vm.kappa[2 * half + 1], pyro_uniform(r[2]),
+                     pyro_uniform(r[3]));
+  // gather sites 2, 3 on the lower lane
+  pyro_vec3 S[4], SN[4], H[4];
+  S[0] = s[0];
+  S[1] = s[1];
+  SN[0] = sn[0];
+  SN[1] = sn[1];
+  H[0] = h[0];
+  H[1] = h[1];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    S[2 + k].x = __shfl_down_sync(0xffffffffu, s[k].x, 16);
+    S[2 + k].y = __shfl_down_sync(0xffffffffu, s[k].y, 16);
+    S[2 + k].z = __shfl_down_sync(0xffffffffu, s[k].z, 16);
+    SN[2 + k].x = __shfl_down_sync(0xffffffffu, sn[k].x, 16);
+    SN[2 + k].y = __shfl_down_sync(0xffffffffu, sn[k].y, 16);
+    SN[2 + k].z = __shfl_down_sync(0xffffffffu, sn[k].z, 16);
+    H[2 + k].x = __shfl_down_sync(0xffffffffu, h[k].x, 16);
+    H[2 + k].y = __shfl_down_sync(0xffffffffu, h[k].y, 16);
+    H[2 + k].z = __shfl_down_sync(0xffffffffu, h[k].z, 16);
+  }
+  uint32_t acc_word = 0;
+  if (half == 0 && active) {
+    const float dE = tet_energy(SN, H, p.J1) - tet_energy(S, H, p.J1);
+    float log_q = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) log_q += vm.kappa[k] * (dot3(vm.mu[k], S[k]) - dot3(vm.mu[k], SN[k]));
+    const float log_r = -beta * dE + log_q;
+    uint32_t r2[4];
+    pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + 2,
+                p.seed_lo, p.seed_hi, r2);
+    acc_word = (log_r >= 0.0f || pyro_uniform(r2[0]) < __expf(log_r)) ? 1u : 0u;
+  }
+  const uint32_t accepted = __shfl_sync(0xffffffffu, acc_word, row);
+  if (accepted && active) {
+    float4* wb = p.spins + (long long)rep * 16 * p.L3;
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+      wb[(4 * F + 2 * half + k) * p.L3 + cell] = make_float4(sn[k].x, sn[k].y, sn[k].z, 0.0f);
+  }
+  return half == 0 ? (int)accepted : 0;
+}
+
 // Acceptance per temperature slot: lanes of a warp that share a slot add
 // once (a warp may straddle two replicas).
 __device__ __forceinline__ void count_accepted(const TetMoveParams& p, int tslot, int accepted) {
@@ -469,6 +582,29 @@ __global__ void __launch_bounds__(kTetMoveThreads) tet_move_kernel(const TetMove
   const float beta = p.beta[p.temp_base + tslot];
   const unsigned long long sweep = (p.tet_ctr ? *p.tet_ctr : 0ull) + p.tet_off;
   const int acc = tet_warp_step<F, false>(p, w, active, rep, cell, beta, sweep,
+                                          feat_all + warp * 32 * kLdIn,
+                                          out_all + warp * 32 * kLdOut);
+  count_accepted(p, tslot, acc);
+}
+
+// Per-pass kernel, two lanes per tetrahedron (256 threads = 128 tetrahedra).
+template <int F>
+__global__ void __launch_bounds__(kTetMoveThreads) tet_move_pair_kernel(const TetMoveParams p) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  MlpSmem w = carve_weights(smem, false);
+  __nv_bfloat16* feat_all = reinterpret_cast<__nv_bfloat16*>(smem + kSmemWeightsFwd);
+  float* out_all = reinterpret_cast<float*>(smem + kSmemWeightsFwd + kTetMoveThreads * kLdIn * 2);
+  stage_weights(w, p.packed, p.master, false);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long tet = (long long)blockIdx.x * (kTetMoveThreads / 2) + warp * 16 + (lane & 15);
+  const bool active = tet < (long long)p.n_rep * p.L3;
+  const int rep = active ? (int)(tet / p.L3) : 0;
+  const int cell = active ? (int)(tet - (long long)rep * p.L3) : 0;
+  const int tslot = p.temp_of_rep[p.temp_base + p.rep_global + rep];
+  const float beta = p.beta[p.temp_base + tslot];
+  const unsigned long long sweep = (p.tet_ctr ? *p.tet_ctr : 0ull) + p.tet_off;
+  const int acc = tet_pair_step<F, false>(p, w, active, rep, cell, beta, sweep,
                                           feat_all + warp * 32 * kLdIn,
                                           out_all + warp * 32 * kLdOut);
   count_accepted(p, tslot, acc);
@@ -873,8 +1009,19 @@ void launch_mlp_pack(const float* master, __nv_bfloat16* packed, cudaStream_t st
   mlp_pack_kernel<<<(kPackSize + 255) / 256, 256, 0, st>>>(master, packed);
 }
 
-void launch_tet_move(const TetMoveParams& p, int f, cudaStream_t st) {
+void launch_tet_move(const TetMoveParams& p, int f, bool pair_mode, cudaStream_t st) {
   const long long n = (long long)p.n_rep * p.L3;
+  if (pair_mode) {
+    const int half = kTetMoveThreads / 2;
+    const int blocks = (int)((n + half - 1) / half);
+    switch (f) {
+      case 0: tet_move_pair_kernel<0><<<blocks, kTetMoveThreads, kTetMoveSmem, st>>>(p); break;
+      case 1: tet_move_pair_kernel<1><<<blocks, kTetMoveThreads, kTetMoveSmem, st>>>(p); break;
+      case 2: tet_move_pair_kernel<2><<<blocks, kTetMoveThreads, kTetMoveSmem, st>>>(p); break;
+      default: tet_move_pair_kernel<3><<<blocks, kTetMoveThreads, kTetMoveSmem, st>>>(p); break;
+    }
+    return;
+  }
   const int blocks = (int)((n + kTetMoveThreads - 1) / kTetMoveThreads);
   switch (f) {
     case 0: tet_move_kernel<0><<<blocks, kTetMoveThreads, kTetMoveSmem, st>>>(p); break;

@@ -65,8 +65,9 @@ struct TetCollectParams {
 };
 
 void launch_mlp_pack(const float* master, __nv_bfloat16* packed, cudaStream_t st);
-// One pass of the learned move over up-tetrahedra of FCC corner f.
-void launch_tet_move(const TetMoveParams& p, int f, cudaStream_t st);
+// One pass of the learned move over up-tetrahedra of FCC corner f; pair_mode:
+// two lanes per tetrahedron (same decisions).
+void launch_tet_move(const TetMoveParams& p, int f, bool pair_mode, cudaStream_t st);
 // n sweeps (4 corner passes each) of every replica in one launch, one
 // thread-block cluster of csize CTAs per replica.
 cudaError_t launch_tet_sweep_cluster(const TetMoveParams& p, int n_sweeps, int csize,

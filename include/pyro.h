@@ -250,9 +250,10 @@ int pyro_tet_set_weights(pyro_ctx* ctx, const float* weights, int n);
 int pyro_tet_get_weights(pyro_ctx* ctx, float* weights, int n);
 /* n learned tetrahedron sweeps of every J1-only system. */
 int pyro_tet_sweep(pyro_ctx* ctx, int n_sweeps);
-/* 1: all passes of a call in one launch, one thread-block cluster per
- * replica; 0 (default): one launch per corner pass. Identical results. */
-int pyro_tet_set_kernel(pyro_ctx* ctx, int cluster);
+/* 0: one launch per corner pass, one lane per tetrahedron; 1: all passes of
+ * a call in one launch, one thread-block cluster per replica; 2 (default):
+ * one launch per corner pass, two lanes per tetrahedron. Identical results. */
+int pyro_tet_set_kernel(pyro_ctx* ctx, int mode);
 int pyro_tet_acceptance(pyro_ctx* ctx, int system, uint64_t* accepted, uint64_t* proposed);
 int pyro_tet_reset_acceptance(pyro_ctx* ctx);
 /* Appends (features[16], spins[12]) of every stride-th up-tetrahedron of each
