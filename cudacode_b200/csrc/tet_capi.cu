@@ -23,7 +23,7 @@ struct TetState {
   float* d_m = nullptr;       // Adam moments
   float* d_v = nullptr;
   float* d_grad = nullptr;
-  __nv_bfloat16* d_packed = nullptr;
+  unsigned char* d_image = nullptr;  // kImgBytes weight image
   unsigned long long* d_ctr = nullptr;       // tetrahedron sweeps done
   unsigned long long* d_accepted = nullptr;  // per temperature slot
   unsigned long long proposed_sweeps = 0;    // since the last reset
@@ -44,7 +44,7 @@ struct TetState {
 void tet_free(pyro_ctx* ctx) {
   if (!ctx || !ctx->tet) return;
   TetState* t = ctx->tet;
-  void* ptrs[] = {t->d_master, t->d_m,     t->d_v,    t->d_grad, t->d_packed, t->d_ctr,
+  void* ptrs[] = {t->d_master, t->d_m,     t->d_v,    t->d_grad, t->d_image, t->d_ctr,
                   t->d_accepted, t->d_loss, t->d_idx, t->d_feat, t->d_targ};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -110,8 +110,7 @@ TetMoveParams move_params(pyro_ctx* ctx, int si, unsigned long long off) {
   p.tet_off = off;
   p.seed_lo = (uint32_t)(ctx->seed & 0xffffffffu);
   p.seed_hi = (uint32_t)(ctx->seed >> 32);
-  p.packed = ctx->tet->d_packed;
-  p.master = ctx->tet->d_master;
+  p.image = ctx->tet->d_image;
   return p;
 }
 
@@ -193,7 +192,7 @@ int pyro_tet_init(pyro_ctx* ctx, uint64_t seed, long long sample_capacity) {
   PYRO_CK(cudaMalloc((void**)&t->d_m, sizeof(float) * kMlpParams));
   PYRO_CK(cudaMalloc((void**)&t->d_v, sizeof(float) * kMlpParams));
   PYRO_CK(cudaMalloc((void**)&t->d_grad, sizeof(float) * kMlpParams));
-  PYRO_CK(cudaMalloc((void**)&t->d_packed, sizeof(__nv_bfloat16) * kPackSize));
+  PYRO_CK(cudaMalloc((void**)&t->d_image, kImgBytes));
   PYRO_CK(cudaMalloc((void**)&t->d_ctr, sizeof(unsigned long long)));
   PYRO_CK(cudaMalloc((void**)&t->d_accepted, sizeof(unsigned long long) * ctx->total_temps));
   PYRO_CK(cudaMalloc((void**)&t->d_loss, sizeof(double)));
@@ -208,7 +207,7 @@ int pyro_tet_init(pyro_ctx* ctx, uint64_t seed, long long sample_capacity) {
   PYRO_CK(cudaMemset(t->d_v, 0, sizeof(float) * kMlpParams));
   PYRO_CK(cudaMemset(t->d_ctr, 0, sizeof(unsigned long long)));
   PYRO_CK(cudaMemset(t->d_accepted, 0, sizeof(unsigned long long) * ctx->total_temps));
-  launch_mlp_pack(t->d_master, t->d_packed, ctx->stream);
+  launch_mlp_pack(t->d_master, t->d_image, ctx->stream);
   PYRO_CK_LAUNCH();
   PYRO_CK(cudaStreamSynchronize(ctx->stream));
   for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
@@ -224,7 +223,7 @@ int pyro_tet_set_weights(pyro_ctx* ctx, const float* w, int n) {
   PYRO_CK(cudaSetDevice(ctx->device));
   PYRO_CK(cudaMemcpyAsync(ctx->tet->d_master, w, sizeof(float) * kMlpParams, cudaMemcpyHostToDevice,
                           ctx->stream));
-  launch_mlp_pack(ctx->tet->d_master, ctx->tet->d_packed, ctx->stream);
+  launch_mlp_pack(ctx->tet->d_master, ctx->tet->d_image, ctx->stream);
   PYRO_CK_LAUNCH();
   PYRO_CK(cudaStreamSynchronize(ctx->stream));
   return PYRO_OK;
@@ -364,13 +363,13 @@ int pyro_tet_train(pyro_ctx* ctx, int steps, int batch, float lr, double* mean_l
                       (uint32_t)(t->seed >> 32), (uint32_t)t->adam_step, ctx->stream);
     PYRO_CK(cudaMemsetAsync(t->d_grad, 0, sizeof(float) * kMlpParams, ctx->stream));
     PYRO_CK(cudaMemsetAsync(t->d_loss, 0, sizeof(double), ctx->stream));
-    launch_mlp_gradient(t->d_feat, t->d_targ, t->d_idx, batch, t->d_packed, t->d_master,
-                        t->d_grad, t->d_loss, ctx->stream);
+    launch_mlp_gradient(t->d_feat, t->d_targ, t->d_idx, batch, t->d_image, t->d_grad, t->d_loss,
+                        ctx->stream);
     PYRO_CK_LAUNCH();
     launch_adam(t->d_master, t->d_m, t->d_v, t->d_grad, kMlpParams, lr, 0.9f, 0.999f, 1e-8f,
                 1.0f / (float)batch, t->adam_step, ctx->stream);
     PYRO_CK_LAUNCH();
-    launch_mlp_pack(t->d_master, t->d_packed, ctx->stream);
+    launch_mlp_pack(t->d_master, t->d_image, ctx->stream);
     PYRO_CK_LAUNCH();
   }
   if (mean_loss) {
@@ -393,7 +392,7 @@ int pyro_tet_forward(pyro_ctx* ctx, const float* features, int n, float* out) {
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(d_in, features, sizeof(float) * 16 * n, cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess) {
-    launch_mlp_forward(d_in, n, ctx->tet->d_packed, ctx->tet->d_master, d_out, ctx->stream);
+    launch_mlp_forward(d_in, n, ctx->tet->d_image, d_out, ctx->stream);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess)
@@ -421,8 +420,8 @@ int pyro_tet_gradient(pyro_ctx* ctx, const float* features, const float* targets
   if (e == cudaSuccess) e = cudaMemsetAsync(ctx->tet->d_grad, 0, sizeof(float) * kMlpParams, ctx->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(ctx->tet->d_loss, 0, sizeof(double), ctx->stream);
   if (e == cudaSuccess) {
-    launch_mlp_gradient(d_f, d_t, nullptr, n, ctx->tet->d_packed, ctx->tet->d_master,
-                        ctx->tet->d_grad, ctx->tet->d_loss, ctx->stream);
+    launch_mlp_gradient(d_f, d_t, nullptr, n, ctx->tet->d_image, ctx->tet->d_grad,
+                        ctx->tet->d_loss, ctx->stream);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess)

@@ -7,7 +7,7 @@
 // (4 passes = one sweep over all up-tetrahedra).
 //
 // For each tetrahedron the external field of site k is h_k = J1 * (sum of its
-// three down-tetrahedron neighbours). A 16 -> 64 -> 64 -> 16 MLP (SiLU, BF16
+// three down-tetrahedron neighbours). A 16 -> 64 -> 64 -> 16 MLP (hard-swish, BF16
 // weights and activations, FP32 accumulation with mma.sync m16n8k16 on the
 // tensor cores) maps (h_0..h_3 / 3, log(beta) / 3) to a von Mises-Fisher
 // distribution vMF(mu_k, kappa_k) per site. The joint proposal of the four
@@ -36,8 +36,6 @@ namespace {
 
 constexpr int kTetThreads = 128;      // training / test kernels: 4 warps x 32 rows
 constexpr int kTetMoveThreads = 256;  // move kernel: 8 warps x 32 tetrahedra
-constexpr int kLdIn = 24;         // padded row of 16 bf16 (48 B): conflict-free fragments
-constexpr int kLdH = 72;          // padded row of 64 bf16 (144 B)
 constexpr int kLdB = 40;          // padded row of 32 batch entries (bf16)
 constexpr int kLdOut = 17;        // padded row of 16 floats
 
@@ -60,71 +58,62 @@ __device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1
       : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-// SiLU with the hardware exponential: the network only parameterises the
-// proposal, whose exact density enters the MH test, so its last bits do not
-// matter for correctness.
-__device__ __forceinline__ float silu(float x) { return __fdividef(x, 1.0f + __expf(-x)); }
-__device__ __forceinline__ float silu_grad(float x) {
-  const float s = __fdividef(1.0f, 1.0f + __expf(-x));
-  return s * (1.0f + x * (1.0f - s));
+// Hard-swish, x * clamp(x + 3, 0, 6) / 6 (Howard et al. 2019): smooth
+// enough for a proposal network, and plain FMA-pipe arithmetic. With SiLU the
+// special-function unit (two operations per activation) bounded the move's
+// per-pass latency.
+__device__ __forceinline__ float hswish(float x) {
+  return x * fminf(fmaxf(x + 3.0f, 0.0f), 6.0f) * (1.0f / 6.0f);
+}
+__device__ __forceinline__ float hswish_grad(float x) {
+  return x <= -3.0f ? 0.0f : (x >= 3.0f ? 1.0f : x * (1.0f / 3.0f) + 0.5f);
 }
 
-// Weights staged in shared memory (padded rows).
+// Weights staged in shared memory: the weight image, copied verbatim.
 struct MlpSmem {
-  __nv_bfloat16* w1t;  // [64][kLdIn]
-  __nv_bfloat16* w2t;  // [64][kLdH]
-  __nv_bfloat16* w3t;  // [16][kLdH]
-  __nv_bfloat16* w2;   // [64][kLdH]  (backward)
-  __nv_bfloat16* w3;   // [64][kLdIn] (backward)
-  float* b1;           // [64]
-  float* b2;           // [64]
-  float* b3;           // [16]
+  const __nv_bfloat16* w1t;  // [64][kLdIn]
+  const __nv_bfloat16* w2t;  // [64][kLdH]
+  const __nv_bfloat16* w3t;  // [16][kLdH]
+  const __nv_bfloat16* w2;   // [64][kLdH]  (backward)
+  const __nv_bfloat16* w3;   // [64][kLdIn] (backward)
+  const float* b1;           // [64]
+  const float* b2;           // [64]
+  const float* b3;           // [16]
 };
 
-constexpr int kSmemWeightsFwd =
-    (64 * kLdIn + 64 * kLdH + 16 * kLdH) * 2 + (64 + 64 + 16) * 4;
-constexpr int kSmemWeightsAll = kSmemWeightsFwd + (64 * kLdH + 64 * kLdIn) * 2;
+constexpr int kSmemWeightsFwd = kImgFwdBytes;
+constexpr int kSmemWeightsAll = kImgBytes;
 
-__device__ MlpSmem carve_weights(unsigned char* base, bool backward) {
+__device__ MlpSmem carve_weights(const unsigned char* base) {
   MlpSmem w;
-  __nv_bfloat16* b = reinterpret_cast<__nv_bfloat16*>(base);
-  w.w1t = b;
-  w.w2t = w.w1t + 64 * kLdIn;
-  w.w3t = w.w2t + 64 * kLdH;
-  __nv_bfloat16* end = w.w3t + 16 * kLdH;
-  if (backward) {
-    w.w2 = end;
-    w.w3 = w.w2 + 64 * kLdH;
-    end = w.w3 + 64 * kLdIn;
-  } else {
-    w.w2 = w.w3 = nullptr;
-  }
-  float* f = reinterpret_cast<float*>(end);
-  w.b1 = f;
-  w.b2 = f + 64;
-  w.b3 = f + 128;
+  w.w1t = reinterpret_cast<const __nv_bfloat16*>(base + kImgW1t);
+  w.w2t = reinterpret_cast<const __nv_bfloat16*>(base + kImgW2t);
+  w.w3t = reinterpret_cast<const __nv_bfloat16*>(base + kImgW3t);
+  w.w2 = reinterpret_cast<const __nv_bfloat16*>(base + kImgW2);
+  w.w3 = reinterpret_cast<const __nv_bfloat16*>(base + kImgW3);
+  w.b1 = reinterpret_cast<const float*>(base + kImgB1);
+  w.b2 = reinterpret_cast<const float*>(base + kImgB2);
+  w.b3 = reinterpret_cast<const float*>(base + kImgB3);
   return w;
 }
 
-__device__ void stage_weights(const MlpSmem& w, const __nv_bfloat16* __restrict__ packed,
-                              const float* __restrict__ master, bool backward) {
-  for (int i = threadIdx.x; i < 64 * 16; i += blockDim.x)
-    w.w1t[(i / 16) * kLdIn + i % 16] = packed[kPackW1t + i];
-  for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x)
-    w.w2t[(i / 64) * kLdH + i % 64] = packed[kPackW2t + i];
-  for (int i = threadIdx.x; i < 16 * 64; i += blockDim.x)
-    w.w3t[(i / 64) * kLdH + i % 64] = packed[kPackW3t + i];
-  if (backward) {
-    for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x)
-      w.w2[(i / 64) * kLdH + i % 64] = packed[kPackW2 + i];
-    for (int i = threadIdx.x; i < 64 * 16; i += blockDim.x)
-      w.w3[(i / 16) * kLdIn + i % 16] = packed[kPackW3 + i];
+// Starts the copy of the first `bytes` of the weight image into shared
+// memory (16-byte cp.async granules, L2 only); stage_wait() completes it for
+// the whole CTA. Between the two a kernel issues its spin loads, so the two
+// memory latencies overlap.
+__device__ __forceinline__ void stage_weights(unsigned char* smem, const unsigned char* image,
+                                              int bytes) {
+  for (int i = threadIdx.x * 16; i < bytes; i += blockDim.x * 16) {
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(smem + i);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(image + i)
+                 : "memory");
   }
-  for (int i = threadIdx.x; i < 64; i += blockDim.x) {
-    w.b1[i] = master[kOffB1 + i];
-    w.b2[i] = master[kOffB2 + i];
-  }
-  for (int i = threadIdx.x; i < 16; i += blockDim.x) w.b3[i] = master[kOffB3 + i];
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+__device__ __forceinline__ void stage_wait() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncthreads();
 }
 
 // Forward pass of one 16-row m-tile of a warp. feat: [rows][kLdIn] bf16 row
@@ -159,7 +148,7 @@ __device__ __forceinline__ void tile_forward(const __nv_bfloat16* feat, int r_ba
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       if (kKeep) f.pre1[j][e] = h1[j][e];
-      h1[j][e] = silu(h1[j][e]);
+      h1[j][e] = hswish(h1[j][e]);
     }
   if (kKeep) {
 #pragma unroll
@@ -195,7 +184,7 @@ __device__ __forceinline__ void tile_forward(const __nv_bfloat16* feat, int r_ba
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       if (kKeep) f.pre2[j][e] = h2[j][e];
-      h2[j][e] = silu(h2[j][e]);
+      h2[j][e] = hswish(h2[j][e]);
     }
   if (kKeep) {
 #pragma unroll
@@ -359,21 +348,78 @@ __device__ __forceinline__ void write_features(__nv_bfloat16* row, const pyro_ve
   row[13] = row[14] = row[15] = __float2bfloat16_rn(0.0f);
 }
 
-// vMF(mu, kappa) sample on the sphere (Wood 1994). Any rounding of the
-// sampler is harmless: the MH ratio uses the density of the value drawn.
+// Uniform in (0, 1] from the top 23 bits of a Philox word (mantissa fill,
+// integer pipe only).
+__device__ __forceinline__ float tet_uniform(uint32_t r) {
+  return 2.0f - __uint_as_float(0x3f800000u | (r >> 9));
+}
+
+// Rotation of (sin t cos p, sin t sin p, cos t) onto the axis n, in the
+// frame of Duff et al. (2017), with the approximate reciprocal (|sgn + n.z|
+// >= 1).
+__device__ __forceinline__ pyro_vec3 about_axis_fast(pyro_vec3 n, float ct, float st, float cp,
+                                                     float sp) {
+  const float sgn = copysignf(1.0f, n.z);
+  const float a = __fdividef(-1.0f, sgn + n.z);
+  const float b = n.x * n.y * a;
+  const float c1 = st * cp, c2 = st * sp;
+  pyro_vec3 o;
+  o.x = ct * n.x + c2 * b + c1 * (sgn * n.x * n.x * a + 1.0f);
+  o.y = ct * n.y + c2 * (n.y * n.y * a + sgn) + c1 * (sgn * b);
+  o.z = ct * n.z - c2 * n.y - c1 * (sgn * n.x);
+  return o;
+}
+
+// vMF(mu, kappa) sample on the sphere (Wood 1994): w = 1 + log(u + (1 - u)
+// e^{-2 kappa}) / kappa, azimuth 2 pi v. The sampler runs on the hardware
+// approximations; the MH ratio is evaluated with the vMF density at the
+// value drawn.
 __device__ __forceinline__ pyro_vec3 vmf_sample(pyro_vec3 mu, float kappa, float u, float v) {
   float w = 1.0f + __fdividef(__logf(u + (1.0f - u) * __expf(-2.0f * kappa)), kappa);
   w = fminf(1.0f, fmaxf(-1.0f, w));
-  const float st = sqrtf(fmaxf(0.0f, 1.0f - w * w));
+  const float q = 1.0f - w * w;
+  const float st = q > 0.0f ? q * rsqrtf(q) : 0.0f;
   float sp, cp;
   pyro_sincospif(2.0f * v, &sp, &cp);
-  return pyro_about_axis(mu, w, st, cp, sp);
+  return about_axis_fast(mu, w, st, cp, sp);
+}
+
+// Proposal for one site from its four network outputs o[0..3]: mu = o_xyz /
+// |o_xyz|, kappa = exp(clamp(o_w)); returns the sample and the site's term
+// kappa mu . (s - s') of log q(S) - log q(S').
+struct SiteMove {
+  pyro_vec3 sn;
+  float lq;
+};
+
+__device__ __forceinline__ SiteMove site_move(const float* o, pyro_vec3 s, uint32_t ru,
+                                              uint32_t rv) {
+  const float x = o[0], y = o[1], z = o[2];
+  const float n2 = x * x + y * y + z * z;
+  pyro_vec3 mu;
+  if (n2 > 1e-30f) {
+    const float inv = rsqrtf(n2);
+    mu.x = x * inv;
+    mu.y = y * inv;
+    mu.z = z * inv;
+  } else {
+    mu.x = 0.0f;
+    mu.y = 0.0f;
+    mu.z = 1.0f;
+  }
+  const float kappa = __expf(fminf(fmaxf(o[3], kLogKappaMin), kLogKappaMax));
+  SiteMove m;
+  m.sn = vmf_sample(mu, kappa, tet_uniform(ru), tet_uniform(rv));
+  m.lq = kappa * (dot3(mu, s) - dot3(mu, m.sn));
+  return m;
 }
 
 // One warp's 32 tetrahedra of corner F (one per lane; lanes with
 // active == false only feed the warp-wide MMAs): features, network, vMF
 // proposals, MH test, write-back. Returns 1 if this lane's move was accepted.
-template <int F, bool kL2>
+// kWait: the weight copy of this CTA is still in flight (stage_weights) and
+// is completed after the spin loads, a CTA-wide barrier.
+template <int F, bool kL2, bool kWait>
 __device__ __forceinline__ int tet_warp_step(const TetMoveParams& p, const MlpSmem& w, bool active,
                                              int rep, int cell, float beta,
                                              unsigned long long sweep, __nv_bfloat16* feat,
@@ -400,7 +446,8 @@ __device__ __forceinline__ int tet_warp_step(const TetMoveParams& p, const MlpSm
     }
   }
   write_features(feat + lane * kLdIn, h, active ? beta : 1.0f);
-  __syncwarp();
+  if (kWait) stage_wait();
+  else __syncwarp();
   TileFwd fw;
   tile_forward<false>(feat, 0, w, fw, nullptr, nullptr);
   store_out(fw, 0, out);
@@ -412,7 +459,6 @@ __device__ __forceinline__ int tet_warp_step(const TetMoveParams& p, const MlpSm
     float o[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) o[i] = out[lane * kLdOut + i];
-    const VmfParams vm = vmf_params(o);
     const uint32_t key_tet = (uint32_t)(F * p.L3 + cell);
     uint32_t r0[4], r1[4], r2[4];
     pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + 0,
@@ -421,17 +467,15 @@ __device__ __forceinline__ int tet_warp_step(const TetMoveParams& p, const MlpSm
                 p.seed_lo, p.seed_hi, r1);
     pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + 2,
                 p.seed_lo, p.seed_hi, r2);
-    pyro_vec3 sn[4];
-    sn[0] = vmf_sample(vm.mu[0], vm.kappa[0], pyro_uniform(r0[0]), pyro_uniform(r0[1]));
-    sn[1] = vmf_sample(vm.mu[1], vm.kappa[1], pyro_uniform(r0[2]), pyro_uniform(r0[3]));
-    sn[2] = vmf_sample(vm.mu[2], vm.kappa[2], pyro_uniform(r1[0]), pyro_uniform(r1[1]));
-    sn[3] = vmf_sample(vm.mu[3], vm.kappa[3], pyro_uniform(r1[2]), pyro_uniform(r1[3]));
+    const SiteMove m0 = site_move(o + 0, s[0], r0[0], r0[1]);
+    const SiteMove m1 = site_move(o + 4, s[1], r0[2], r0[3]);
+    const SiteMove m2 = site_move(o + 8, s[2], r1[0], r1[1]);
+    const SiteMove m3 = site_move(o + 12, s[3], r1[2], r1[3]);
+    const pyro_vec3 sn[4] = {m0.sn, m1.sn, m2.sn, m3.sn};
     const float dE = tet_energy(sn, h, p.J1) - tet_energy(s, h, p.J1);
-    float log_q = 0.0f;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) log_q += vm.kappa[k] * (dot3(vm.mu[k], s[k]) - dot3(vm.mu[k], sn[k]));
+    const float log_q = (m0.lq + m1.lq) + (m2.lq + m3.lq);
     const float log_r = -beta * dE + log_q;
-    accepted = log_r >= 0.0f || pyro_uniform(r2[0]) < __expf(log_r);
+    accepted = log_r >= 0.0f || tet_uniform(r2[0]) < __expf(log_r);
     if (accepted) {
       float4* wb = p.spins + (long long)rep * 16 * p.L3;
 #pragma unroll
@@ -448,8 +492,8 @@ __device__ __forceinline__ int tet_warp_step(const TetMoveParams& p, const MlpSm
 // of a warp. Lane l then gathers the partner's values and evaluates the
 // energy change and the proposal ratio with exactly the single-lane
 // expressions, so the decisions are identical. Returns 1 on the lower lane
-// of an accepted move.
-template <int F, bool kL2>
+// of an accepted move. kWait as in tet_warp_step.
+template <int F, bool kL2, bool kWait>
 __device__ __forceinline__ int tet_pair_step(const TetMoveParams& p, const MlpSmem& w, bool active,
                                              int rep, int cell, float beta,
                                              unsigned long long sweep, __nv_bfloat16* feat,
@@ -495,24 +539,24 @@ __device__ __forceinline__ int tet_pair_step(const TetMoveParams& p, const MlpSm
     frow[12] = __float2bfloat16_rn(logf(active ? beta : 1.0f) * (1.0f / 3.0f));
     frow[13] = frow[14] = frow[15] = __float2bfloat16_rn(0.0f);
   }
-  __syncwarp();
+  if (kWait) stage_wait();
+  else __syncwarp();
   TileFwd fw;
   tile_forward<false>(feat, 0, w, fw, nullptr, nullptr);
   store_out(fw, 0, out);
   __syncwarp();
   // this lane's two sites: network outputs 8 * half .. 8 * half + 7
-  float o[16];
+  float o[8];
 #pragma unroll
-  for (int i = 0; i < 16; ++i) o[i] = out[row * kLdOut + i];
-  const VmfParams vm = vmf_params(o);
+  for (int i = 0; i < 8; ++i) o[i] = out[row * kLdOut + 8 * half + i];
   const uint32_t key_tet = (uint32_t)(F * p.L3 + cell);
   uint32_t r[4];
   pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + half,
               p.seed_lo, p.seed_hi, r);
-  pyro_vec3 sn[2];
-  sn[0] = vmf_sample(vm.mu[2 * half], vm.kappa[2 * half], pyro_uniform(r[0]), pyro_uniform(r[1]));
-  sn[1] = vmf_sample(vm.mu[2 * half + 1], vm.kappa[2 * half + 1], pyro_uniform(r[2]),
-                     pyro_uniform(r[3]));
+  const SiteMove ma = site_move(o + 0, s[0], r[0], r[1]);
+  const SiteMove mb = site_move(o + 4, s[1], r[2], r[3]);
+  const pyro_vec3 sn[2] = {ma.sn, mb.sn};
+  const float lq_half = ma.lq + mb.lq;
   // gather sites 2, 3 on the lower lane
   pyro_vec3 S[4], SN[4], H[4];
   S[0] = s[0];
@@ -533,17 +577,16 @@ __device__ __forceinline__ int tet_pair_step(const TetMoveParams& p, const MlpSm
     H[2 + k].y = __shfl_down_sync(0xffffffffu, h[k].y, 16);
     H[2 + k].z = __shfl_down_sync(0xffffffffu, h[k].z, 16);
   }
+  const float lq_hi = __shfl_down_sync(0xffffffffu, lq_half, 16);
   uint32_t acc_word = 0;
   if (half == 0 && active) {
     const float dE = tet_energy(SN, H, p.J1) - tet_energy(S, H, p.J1);
-    float log_q = 0.0f;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) log_q += vm.kappa[k] * (dot3(vm.mu[k], S[k]) - dot3(vm.mu[k], SN[k]));
+    const float log_q = lq_half + lq_hi;
     const float log_r = -beta * dE + log_q;
     uint32_t r2[4];
     pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + 2,
                 p.seed_lo, p.seed_hi, r2);
-    acc_word = (log_r >= 0.0f || pyro_uniform(r2[0]) < __expf(log_r)) ? 1u : 0u;
+    acc_word = (log_r >= 0.0f || tet_uniform(r2[0]) < __expf(log_r)) ? 1u : 0u;
   }
   const uint32_t accepted = __shfl_sync(0xffffffffu, acc_word, row);
   if (accepted && active) {
@@ -568,11 +611,10 @@ __device__ __forceinline__ void count_accepted(const TetMoveParams& p, int tslot
 template <int F>
 __global__ void __launch_bounds__(kTetMoveThreads) tet_move_kernel(const TetMoveParams p) {
   extern __shared__ __align__(16) unsigned char smem[];
-  MlpSmem w = carve_weights(smem, false);
+  const MlpSmem w = carve_weights(smem);
   __nv_bfloat16* feat_all = reinterpret_cast<__nv_bfloat16*>(smem + kSmemWeightsFwd);
   float* out_all = reinterpret_cast<float*>(smem + kSmemWeightsFwd + kTetMoveThreads * kLdIn * 2);
-  stage_weights(w, p.packed, p.master, false);
-  __syncthreads();
+  stage_weights(smem, p.image, kImgFwdBytes);
   const int warp = threadIdx.x >> 5;
   const long long tet = (long long)blockIdx.x * kTetMoveThreads + threadIdx.x;  // rep * L3 + cell
   const bool active = tet < (long long)p.n_rep * p.L3;
@@ -581,7 +623,7 @@ __global__ void __launch_bounds__(kTetMoveThreads) tet_move_kernel(const TetMove
   const int tslot = p.temp_of_rep[p.temp_base + p.rep_global + rep];
   const float beta = p.beta[p.temp_base + tslot];
   const unsigned long long sweep = (p.tet_ctr ? *p.tet_ctr : 0ull) + p.tet_off;
-  const int acc = tet_warp_step<F, false>(p, w, active, rep, cell, beta, sweep,
+  const int acc = tet_warp_step<F, false, true>(p, w, active, rep, cell, beta, sweep,
                                           feat_all + warp * 32 * kLdIn,
                                           out_all + warp * 32 * kLdOut);
   count_accepted(p, tslot, acc);
@@ -591,11 +633,10 @@ __global__ void __launch_bounds__(kTetMoveThreads) tet_move_kernel(const TetMove
 template <int F>
 __global__ void __launch_bounds__(kTetMoveThreads) tet_move_pair_kernel(const TetMoveParams p) {
   extern __shared__ __align__(16) unsigned char smem[];
-  MlpSmem w = carve_weights(smem, false);
+  const MlpSmem w = carve_weights(smem);
   __nv_bfloat16* feat_all = reinterpret_cast<__nv_bfloat16*>(smem + kSmemWeightsFwd);
   float* out_all = reinterpret_cast<float*>(smem + kSmemWeightsFwd + kTetMoveThreads * kLdIn * 2);
-  stage_weights(w, p.packed, p.master, false);
-  __syncthreads();
+  stage_weights(smem, p.image, kImgFwdBytes);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long tet = (long long)blockIdx.x * (kTetMoveThreads / 2) + warp * 16 + (lane & 15);
   const bool active = tet < (long long)p.n_rep * p.L3;
@@ -604,7 +645,7 @@ __global__ void __launch_bounds__(kTetMoveThreads) tet_move_pair_kernel(const Te
   const int tslot = p.temp_of_rep[p.temp_base + p.rep_global + rep];
   const float beta = p.beta[p.temp_base + tslot];
   const unsigned long long sweep = (p.tet_ctr ? *p.tet_ctr : 0ull) + p.tet_off;
-  const int acc = tet_pair_step<F, false>(p, w, active, rep, cell, beta, sweep,
+  const int acc = tet_pair_step<F, false, true>(p, w, active, rep, cell, beta, sweep,
                                           feat_all + warp * 32 * kLdIn,
                                           out_all + warp * 32 * kLdOut);
   count_accepted(p, tslot, acc);
@@ -624,11 +665,11 @@ __global__ void __launch_bounds__(kTetMoveThreads) tet_sweep_cluster_kernel(cons
                                                                             int n_sweeps,
                                                                             int csize) {
   extern __shared__ __align__(16) unsigned char smem[];
-  MlpSmem w = carve_weights(smem, false);
+  const MlpSmem w = carve_weights(smem);
   __nv_bfloat16* feat_all = reinterpret_cast<__nv_bfloat16*>(smem + kSmemWeightsFwd);
   float* out_all = reinterpret_cast<float*>(smem + kSmemWeightsFwd + kTetMoveThreads * kLdIn * 2);
-  stage_weights(w, p.packed, p.master, false);
-  __syncthreads();
+  stage_weights(smem, p.image, kImgFwdBytes);
+  stage_wait();
   const int warp = threadIdx.x >> 5;
   __nv_bfloat16* feat = feat_all + warp * 32 * kLdIn;
   float* out = out_all + warp * 32 * kLdOut;
@@ -647,10 +688,10 @@ __global__ void __launch_bounds__(kTetMoveThreads) tet_sweep_cluster_kernel(cons
         const bool active = cell < p.L3;
         const int cl = active ? cell : 0;
         switch (f) {
-          case 0: acc += tet_warp_step<0, true>(p, w, active, rep, cl, beta, sweep, feat, out); break;
-          case 1: acc += tet_warp_step<1, true>(p, w, active, rep, cl, beta, sweep, feat, out); break;
-          case 2: acc += tet_warp_step<2, true>(p, w, active, rep, cl, beta, sweep, feat, out); break;
-          default: acc += tet_warp_step<3, true>(p, w, active, rep, cl, beta, sweep, feat, out); break;
+          case 0: acc += tet_warp_step<0, true, false>(p, w, active, rep, cl, beta, sweep, feat, out); break;
+          case 1: acc += tet_warp_step<1, true, false>(p, w, active, rep, cl, beta, sweep, feat, out); break;
+          case 2: acc += tet_warp_step<2, true, false>(p, w, active, rep, cl, beta, sweep, feat, out); break;
+          default: acc += tet_warp_step<3, true, false>(p, w, active, rep, cl, beta, sweep, feat, out); break;
         }
       }
       cluster_sync_all();
@@ -707,43 +748,51 @@ __global__ void tet_collect_kernel(const TetCollectParams p) {
   }
 }
 
-__global__ void mlp_pack_kernel(const float* __restrict__ m, __nv_bfloat16* packed) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kPackSize; i += gridDim.x * blockDim.x) {
-    float v;
-    if (i < kPackW2t) {  // w1t[o][i] = W1[i][o]
-      const int o = i / 16, in = i % 16;
-      v = m[kOffW1 + in * 64 + o];
-    } else if (i < kPackW3t) {
-      const int j = i - kPackW2t, o = j / 64, in = j % 64;
-      v = m[kOffW2 + in * 64 + o];
-    } else if (i < kPackW2) {
-      const int j = i - kPackW3t, o = j / 64, in = j % 64;
-      v = m[kOffW3 + in * 16 + o];
-    } else if (i < kPackW3) {
-      v = m[kOffW2 + (i - kPackW2)];
-    } else {
-      v = m[kOffW3 + (i - kPackW3)];
-    }
-    packed[i] = __float2bfloat16_rn(v);
+// One BF16 matrix region of the weight image: rows x ld entries, the first
+// `cols` of a row taken from the master array (element (r, c) at
+// m[off + r * rs + c * cs]), the padding zero.
+__device__ __forceinline__ void pack_region(const float* __restrict__ m, unsigned char* image,
+                                            int region, int rows, int ld, int cols, int off,
+                                            int rs, int cs, int tid, int nthreads) {
+  __nv_bfloat16* dst = reinterpret_cast<__nv_bfloat16*>(image + region);
+  for (int i = tid; i < rows * ld; i += nthreads) {
+    const int r = i / ld, c = i - r * ld;
+    dst[i] = __float2bfloat16_rn(c < cols ? m[off + r * rs + c * cs] : 0.0f);
   }
+}
+
+__global__ void mlp_pack_kernel(const float* __restrict__ m, unsigned char* image) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+  // forward operands, [out][in]: element (o, i) = W[i][o]
+  pack_region(m, image, kImgW1t, kMlpHidden, kLdIn, kMlpIn, kOffW1, 1, kMlpHidden, tid, nt);
+  pack_region(m, image, kImgW2t, kMlpHidden, kLdH, kMlpHidden, kOffW2, 1, kMlpHidden, tid, nt);
+  pack_region(m, image, kImgW3t, kMlpOut, kLdH, kMlpHidden, kOffW3, 1, kMlpOut, tid, nt);
+  // backward operands, [in][out]
+  pack_region(m, image, kImgW2, kMlpHidden, kLdH, kMlpHidden, kOffW2, kMlpHidden, 1, tid, nt);
+  pack_region(m, image, kImgW3, kMlpHidden, kLdIn, kMlpOut, kOffW3, kMlpOut, 1, tid, nt);
+  float* b = reinterpret_cast<float*>(image + kImgB1);  // b1, b2, b3 contiguous
+  for (int i = tid; i < 2 * kMlpHidden + kMlpOut; i += nt)
+    b[i] = i < kMlpHidden ? m[kOffB1 + i]
+                          : (i < 2 * kMlpHidden ? m[kOffB2 + i - kMlpHidden]
+                                                : m[kOffB3 + i - 2 * kMlpHidden]);
 }
 
 __global__ void __launch_bounds__(kTetThreads) mlp_forward_kernel(const float* __restrict__ features,
                                                                   int n,
-                                                                  const __nv_bfloat16* packed,
-                                                                  const float* master, float* out) {
+                                                                  const unsigned char* image,
+                                                                  float* out) {
   extern __shared__ __align__(16) unsigned char smem[];
-  MlpSmem w = carve_weights(smem, false);
+  const MlpSmem w = carve_weights(smem);
   __nv_bfloat16* feat_all = reinterpret_cast<__nv_bfloat16*>(smem + kSmemWeightsFwd);
   float* out_all = reinterpret_cast<float*>(smem + kSmemWeightsFwd + kTetThreads * kLdIn * 2);
-  stage_weights(w, packed, master, false);
+  stage_weights(smem, image, kImgFwdBytes);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   __nv_bfloat16* feat = feat_all + warp * 32 * kLdIn;
   float* o = out_all + warp * 32 * kLdOut;
   const long long row = (long long)blockIdx.x * kTetThreads + threadIdx.x;
   for (int i = 0; i < 16; ++i)
     feat[lane * kLdIn + i] = __float2bfloat16_rn(row < n ? features[row * 16 + i] : 0.0f);
-  __syncthreads();
+  stage_wait();
   TileFwd fw;
   tile_forward<false>(feat, 0, w, fw, nullptr, nullptr);
   store_out(fw, 0, o);
@@ -857,16 +906,16 @@ __device__ __forceinline__ float nll_and_grad(const float* o, const float* s, fl
 
 __global__ void __launch_bounds__(kTetThreads) mlp_gradient_kernel(
     const float* __restrict__ features, const float* __restrict__ targets, const int* idx, int n,
-    const __nv_bfloat16* packed, const float* master, float* grad, double* loss_sum) {
+    const unsigned char* image, float* grad, double* loss_sum) {
   extern __shared__ __align__(16) unsigned char smem[];
-  MlpSmem w = carve_weights(smem, true);
+  const MlpSmem w = carve_weights(smem);
   unsigned char* wbase = smem + kSmemWeightsAll;
   float* g_acc = reinterpret_cast<float*>(wbase + 4 * kGradWarpBytes);
-  stage_weights(w, packed, master, true);
+  stage_weights(smem, image, kImgBytes);
   for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) g_acc[i] = 0.0f;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   GradWarpSmem ws = carve_warp(wbase + warp * kGradWarpBytes);
-  __syncthreads();
+  stage_wait();
   float loss_local = 0.0f;
   for (long long base = (long long)blockIdx.x * kTetThreads; base < n;
        base += (long long)gridDim.x * kTetThreads) {
@@ -919,7 +968,7 @@ __global__ void __launch_bounds__(kTetThreads) mlp_gradient_kernel(
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
 #pragma unroll
-        for (int e = 0; e < 4; ++e) da2[j][e] *= silu_grad(fw[mt].pre2[j][e]);
+        for (int e = 0; e < 4; ++e) da2[j][e] *= hswish_grad(fw[mt].pre2[j][e]);
         const int c = 8 * j + 2 * t;
         ws.da2t[c * kLdB + r0] = __float2bfloat16_rn(da2[j][0]);
         ws.da2t[(c + 1) * kLdB + r0] = __float2bfloat16_rn(da2[j][1]);
@@ -949,7 +998,7 @@ __global__ void __launch_bounds__(kTetThreads) mlp_gradient_kernel(
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
 #pragma unroll
-        for (int e = 0; e < 4; ++e) da1[j][e] *= silu_grad(fw[mt].pre1[j][e]);
+        for (int e = 0; e < 4; ++e) da1[j][e] *= hswish_grad(fw[mt].pre1[j][e]);
         const int c = 8 * j + 2 * t;
         ws.da1t[c * kLdB + r0] = __float2bfloat16_rn(da1[j][0]);
         ws.da1t[(c + 1) * kLdB + r0] = __float2bfloat16_rn(da1[j][1]);
@@ -1005,8 +1054,8 @@ constexpr int kTetMoveSmem =
 
 }  // namespace
 
-void launch_mlp_pack(const float* master, __nv_bfloat16* packed, cudaStream_t st) {
-  mlp_pack_kernel<<<(kPackSize + 255) / 256, 256, 0, st>>>(master, packed);
+void launch_mlp_pack(const float* master, unsigned char* image, cudaStream_t st) {
+  mlp_pack_kernel<<<(kImgBytes / 2 + 255) / 256, 256, 0, st>>>(master, image);
 }
 
 void launch_tet_move(const TetMoveParams& p, int f, bool pair_mode, cudaStream_t st) {
@@ -1080,15 +1129,15 @@ void launch_tet_collect(const TetCollectParams& p, cudaStream_t st) {
   tet_collect_kernel<<<(int)blocks, 256, 0, st>>>(p);
 }
 
-void launch_mlp_forward(const float* features, int n, const __nv_bfloat16* packed,
-                        const float* master, float* out, cudaStream_t st) {
+void launch_mlp_forward(const float* features, int n, const unsigned char* image, float* out,
+                        cudaStream_t st) {
   const int blocks = (n + kTetThreads - 1) / kTetThreads;
-  mlp_forward_kernel<<<blocks, kTetThreads, kTetSmem, st>>>(features, n, packed, master, out);
+  mlp_forward_kernel<<<blocks, kTetThreads, kTetSmem, st>>>(features, n, image, out);
 }
 
 void launch_mlp_gradient(const float* features, const float* targets, const int* idx, int n,
-                         const __nv_bfloat16* packed, const float* master, float* grad,
-                         double* loss, cudaStream_t st) {
+                         const unsigned char* image, float* grad, double* loss,
+                         cudaStream_t st) {
   static bool attr_set = false;
   if (!attr_set) {
     cudaFuncSetAttribute(mlp_gradient_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1098,8 +1147,8 @@ void launch_mlp_gradient(const float* features, const float* targets, const int*
   int blocks = (n + kTetThreads - 1) / kTetThreads;
   if (blocks > 148 * 2) blocks = 148 * 2;
   if (blocks < 1) blocks = 1;
-  mlp_gradient_kernel<<<blocks, kTetThreads, kGradSmem, st>>>(features, targets, idx, n, packed,
-                                                               master, grad, loss);
+  mlp_gradient_kernel<<<blocks, kTetThreads, kGradSmem, st>>>(features, targets, idx, n, image,
+                                                               grad, loss);
 }
 
 void launch_adam(float* master, float* m, float* v, const float* grad, int n, float lr,

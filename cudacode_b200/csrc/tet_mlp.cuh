@@ -23,15 +23,28 @@ constexpr int kOffB3 = kOffW3 + kMlpHidden * kMlpOut;      // [16]
 constexpr int kMlpParams = kOffB3 + kMlpOut;               // 6288
 constexpr float kLogKappaMin = -4.0f, kLogKappaMax = 6.0f;
 
-// BF16 operand copies of the weights: forward B operands are the transposed
-// matrices ([out][in], input contiguous), backward B operands the master
-// orientation ([in][out], output contiguous).
-constexpr int kPackW1t = 0;                                 // [64][16]
-constexpr int kPackW2t = kPackW1t + kMlpHidden * kMlpIn;    // [64][64]
-constexpr int kPackW3t = kPackW2t + kMlpHidden * kMlpHidden;  // [16][64]
-constexpr int kPackW2 = kPackW3t + kMlpOut * kMlpHidden;    // [64][64]
-constexpr int kPackW3 = kPackW2 + kMlpHidden * kMlpHidden;  // [64][16]
-constexpr int kPackSize = kPackW3 + kMlpHidden * kMlpOut;
+// The weights as the byte image of the kernels' shared-memory copy: BF16
+// operand matrices in padded rows (conflict-free fragment loads), FP32
+// biases. Forward operands are the transposed matrices ([out][in], input
+// contiguous), backward operands the master orientation ([in][out]). The
+// forward part comes first, so forward-only kernels copy a prefix; every
+// offset is a multiple of 16 bytes, so a CTA stages the image with 16-byte
+// asynchronous copies.
+constexpr int kLdIn = 24;  // padded row of 16 bf16 (48 B)
+constexpr int kLdH = 72;   // padded row of 64 bf16 (144 B)
+constexpr int kImgW1t = 0;                                   // bf16 [64][kLdIn]
+constexpr int kImgW2t = kImgW1t + kMlpHidden * kLdIn * 2;    // bf16 [64][kLdH]
+constexpr int kImgW3t = kImgW2t + kMlpHidden * kLdH * 2;     // bf16 [16][kLdH]
+constexpr int kImgB1 = kImgW3t + kMlpOut * kLdH * 2;         // f32 [64]
+constexpr int kImgB2 = kImgB1 + kMlpHidden * 4;              // f32 [64]
+constexpr int kImgB3 = kImgB2 + kMlpHidden * 4;              // f32 [16]
+constexpr int kImgFwdBytes = kImgB3 + kMlpOut * 4;
+constexpr int kImgW2 = kImgFwdBytes;                         // bf16 [64][kLdH]
+constexpr int kImgW3 = kImgW2 + kMlpHidden * kLdH * 2;       // bf16 [64][kLdIn]
+constexpr int kImgBytes = kImgW3 + kMlpHidden * kLdIn * 2;
+static_assert(kImgW2t % 16 == 0 && kImgW3t % 16 == 0 && kImgB1 % 16 == 0 &&
+                  kImgFwdBytes % 16 == 0 && kImgW3 % 16 == 0 && kImgBytes % 16 == 0,
+              "16-byte staging granules");
 
 struct TetMoveParams {
   float4* spins;  // replica 0 of the system
@@ -45,8 +58,7 @@ struct TetMoveParams {
   const unsigned long long* tet_ctr;
   unsigned long long tet_off;
   uint32_t seed_lo, seed_hi;
-  const __nv_bfloat16* packed;  // kPackSize
-  const float* master;          // biases read from here
+  const unsigned char* image;  // kImgBytes weight image
 };
 
 struct TetCollectParams {
@@ -64,7 +76,8 @@ struct TetCollectParams {
   long long head;      // first slot written (mod cap)
 };
 
-void launch_mlp_pack(const float* master, __nv_bfloat16* packed, cudaStream_t st);
+// Writes the weight image (kImgBytes) of the FP32 master weights.
+void launch_mlp_pack(const float* master, unsigned char* image, cudaStream_t st);
 // One pass of the learned move over up-tetrahedra of FCC corner f; pair_mode:
 // two lanes per tetrahedron (same decisions).
 void launch_tet_move(const TetMoveParams& p, int f, bool pair_mode, cudaStream_t st);
@@ -78,14 +91,13 @@ int tet_chunks(int L3);  // chunks of tetrahedra per corner and replica
 long long tet_collect_count(int L3, int n_rep, int stride);
 void launch_tet_collect(const TetCollectParams& p, cudaStream_t st);
 // Network outputs for n feature rows (host-visible test path).
-void launch_mlp_forward(const float* features, int n, const __nv_bfloat16* packed,
-                        const float* master, float* out, cudaStream_t st);
+void launch_mlp_forward(const float* features, int n, const unsigned char* image, float* out,
+                        cudaStream_t st);
 // Adds d(sum of per-sample negative log-likelihood)/d(params) of rows
 // idx[0..n) (or 0..n if idx is null) to grad[kMlpParams] and the loss sum to
 // *loss.
 void launch_mlp_gradient(const float* features, const float* targets, const int* idx, int n,
-                         const __nv_bfloat16* packed, const float* master, float* grad,
-                         double* loss, cudaStream_t st);
+                         const unsigned char* image, float* grad, double* loss, cudaStream_t st);
 void launch_adam(float* master, float* m, float* v, const float* grad, int n, float lr,
                  float beta1, float beta2, float eps, float scale, int step, cudaStream_t st);
 // idx[i] = Philox-drawn sample indices in [0, n_avail).

@@ -718,11 +718,9 @@ double bf16(double x) {
   return f;
 }
 
-double silu(double x) { return x / (1.0 + std::exp(-x)); }
-double silu_grad(double x) {
-  const double s = 1.0 / (1.0 + std::exp(-x));
-  return s * (1.0 + x * (1.0 - s));
-}
+// hard-swish x * clamp(x + 3, 0, 6) / 6 and its derivative
+double hswish(double x) { return x * std::min(std::max(x + 3.0, 0.0), 6.0) / 6.0; }
+double hswish_grad(double x) { return x <= -3.0 ? 0.0 : (x >= 3.0 ? 1.0 : x / 3.0 + 0.5); }
 
 struct Fwd {
   double x[kIn], pre1[kH], h1[kH], pre2[kH], h2[kH], o[kOut];
@@ -734,13 +732,13 @@ void mlp_forward(const float* m, const float* feat, Fwd& f) {
     double a = m[oB1 + o];
     for (int i = 0; i < kIn; ++i) a += f.x[i] * bf16(m[oW1 + i * kH + o]);
     f.pre1[o] = a;
-    f.h1[o] = bf16(silu(a));
+    f.h1[o] = bf16(hswish(a));
   }
   for (int o = 0; o < kH; ++o) {
     double a = m[oB2 + o];
     for (int i = 0; i < kH; ++i) a += f.h1[i] * bf16(m[oW2 + i * kH + o]);
     f.pre2[o] = a;
-    f.h2[o] = bf16(silu(a));
+    f.h2[o] = bf16(hswish(a));
   }
   for (int o = 0; o < kOut; ++o) {
     double a = m[oB3 + o];
@@ -813,7 +811,7 @@ void orc_mlp_gradient(const float* master, const float* feats, const float* targ
     for (int i = 0; i < kH; ++i) {
       double a = 0.0;
       for (int o = 0; o < kOut; ++o) a += db[o] * bf16(master[oW3 + i * kOut + o]);
-      da2[i] = a * silu_grad(f.pre2[i]);
+      da2[i] = a * hswish_grad(f.pre2[i]);
       G[oB2 + i] += da2[i];
       da2b[i] = bf16(da2[i]);
     }
@@ -821,7 +819,7 @@ void orc_mlp_gradient(const float* master, const float* feats, const float* targ
     for (int i = 0; i < kH; ++i) {
       double a = 0.0;
       for (int o = 0; o < kH; ++o) a += da2b[o] * bf16(master[oW2 + i * kH + o]);
-      const double v = a * silu_grad(f.pre1[i]);
+      const double v = a * hswish_grad(f.pre1[i]);
       G[oB1 + i] += v;
       da1b[i] = bf16(v);
     }
