@@ -49,6 +49,7 @@ PassParams pass_params(pyro_ctx* ctx, int pass) {
   p.seed_lo = (uint32_t)(ctx->seed & 0xffffffffu);
   p.seed_hi = (uint32_t)(ctx->seed >> 32);
   p.renorm_every = ctx->renorm_every;
+  p.exch = ctx->d_exch;
   return p;
 }
 
@@ -121,6 +122,7 @@ int queue_observables(pyro_ctx* ctx, bool skip_j1 = false) {
     op.sys = ctx->d_sys;
     op.spins = ctx->d_spins;
     op.partials = ctx->d_partials;
+    op.exch = ctx->d_exch;
     launch_observables(op, ctx->tab, ctx->obs_generic_blocks, ctx->stream);
     PYRO_CK_LAUNCH();
   }
@@ -362,7 +364,7 @@ void free_all(pyro_ctx* c) {
                   c->d_obs_segs,    c->d_partials,     c->d_sweep,       c->d_scratch_u64,
                   c->d_history,     c->d_history_count, c->d_obs_generic,
                   c->d_sq_s1,       c->d_sq_s2,        c->d_sq_s3,       c->d_sq_tw,
-                  c->d_sq_out};
+                  c->d_sq_out,      c->d_exch};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto* p : c->d_pass_segs)
@@ -387,7 +389,7 @@ int build_schedule(pyro_ctx* ctx) {
   ctx->pass_segs.assign(ctx->n_passes, {});
   ctx->pass_j1.assign(ctx->n_passes, {});
   ctx->pass_blocks.assign(ctx->n_passes, 0);
-  auto j1_path = [&](const SysDev& s) { return ctx->use_j1_kernel && s.n_colours == 4 && s.shells == 1; };
+  auto j1_path = [&](const SysDev& s) { return ctx->use_j1_kernel && j1_only(s); };
   for (int pass = 0; pass < ctx->n_passes; ++pass) {
     int blocks = 0;
     for (int i = 0; i < (int)ctx->sys.size(); ++i) {
@@ -414,7 +416,7 @@ int build_schedule(pyro_ctx* ctx) {
   ctx->pass_all16.assign(ctx->n_passes, 1);
   for (int pass = 0; pass < ctx->n_passes; ++pass)
     for (const PassSeg& g : ctx->pass_segs[pass])
-      if (ctx->sys[g.sys].n_colours != 16) ctx->pass_all16[pass] = 0;
+      if (ctx->sys[g.sys].n_colours != 16 || ctx->sys[g.sys].exch >= 0) ctx->pass_all16[pass] = 0;
   ctx->obs_segs.clear();
   ctx->obs_generic.clear();
   ctx->obs_j1.clear();
@@ -505,7 +507,7 @@ int build_schedule(pyro_ctx* ctx) {
           g.rep_begin = rg.r0;
           blocks += g.blocks_per_rep * rg.n;
           G.pass_segs[pass].push_back(g);
-          if (s.n_colours != 16) G.all16[pass] = 0;
+          if (s.n_colours != 16 || s.exch >= 0) G.all16[pass] = 0;
         }
         G.pass_blocks[pass] = blocks;
         PYRO_CK(alloc(&G.d_pass_segs[pass], G.pass_segs[pass].size()));
@@ -575,6 +577,15 @@ int validate(const pyro_config* cfg, std::string* why) {
 }
 
 }  // namespace
+
+namespace pyro {
+int rebuild_schedule(pyro_ctx* ctx) {
+  for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+  ctx->graphs.clear();
+  ctx->graph_kernels.clear();
+  return build_schedule(ctx);
+}
+}  // namespace pyro
 
 extern "C" {
 
@@ -672,6 +683,7 @@ int pyro_create(const pyro_config* cfg, pyro_ctx** out) {
     s.J64[3] = d.J3b;
     s.shells = (d.J1 != 0.0 ? 1 : 0) | (d.J2 != 0.0 ? 2 : 0) | (d.J3 != 0.0 ? 4 : 0) |
                (d.J3b != 0.0 ? 8 : 0);
+    s.exch = -1;
     ctx->sys.push_back(s);
     ctx->ladders.emplace_back(d.temperatures, d.temperatures + d.n_temperatures);
     for (int t = 0; t < d.n_temperatures; ++t) {
@@ -842,7 +854,7 @@ int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen)
   struct Variant { int j1, cyc, cs, site, group, chains, gen_mb; };
   bool any_j1 = false, any_gen = false;
   for (const auto& s : ctx->sys) {
-    if (s.n_colours == 4 && s.shells == 1) any_j1 = true;
+    if (j1_only(s)) any_j1 = true;
     else any_gen = true;
   }
   std::vector<Variant> vs;
@@ -1292,6 +1304,7 @@ static int run_smem_cycles(pyro_ctx* ctx, int n_metro, int n_or, int n_cycles) {
     p.history_count = ctx->d_history_count;
     p.history_cap = ctx->history_cap;
     p.total_temps = ctx->total_temps;
+    p.exch = ctx->d_exch;
     PYRO_CK(launch_smem_cycles(p, ctx->tab, ctx->stream));
     ctx->launches += 1;
   }

@@ -7,7 +7,9 @@
 //   "PYROCKP1", u32 version, u32 n_systems, u64 seed, i32 renorm_every,
 //   u32 has_tet, u64 sweeps, u64 tet_sweeps,
 //   per system: i32 L, n_replicas, replica_offset, n_temperatures,
-//               f64 J1, J2, J3, J3b, f64 T[n_temperatures],
+//               f64 J1, J2, J3, J3b,
+//               u32 has_exchange, [f64 A[144], f64 f[12] if has_exchange],
+//               f64 T[n_temperatures],
 //               i32 temperature_of_replica[n_temperatures],
 //               i32 replica_of_temperature[n_temperatures],
 //               f32 cosmax[n_temperatures], u64 swap_count,
@@ -39,7 +41,7 @@ using namespace pyro;
 namespace {
 
 const char kMagic[8] = {'P', 'Y', 'R', 'O', 'C', 'K', 'P', '1'};
-const uint32_t kVersion = 1;
+const uint32_t kVersion = 2;  // 1: no exchange block (isotropic systems only)
 
 struct Fnv {
   uint64_t h = 1469598103934665603ull;
@@ -116,6 +118,14 @@ int pyro_save_checkpoint(pyro_ctx* ctx, const char* path) {
     w.put((int32_t)s.rep_global);
     w.put((int32_t)s.n_temp);
     for (int k = 0; k < 4; ++k) w.put(s.J64[k]);
+    w.put((uint32_t)(s.exch >= 0 ? 1 : 0));
+    if (s.exch >= 0) {
+      const ExchangeDev& X = ctx->exch[s.exch];
+      for (int p = 0; p < 16; ++p)
+        for (int q = 0; q < 9; ++q) w.put(X.A64[p][q]);
+      for (int b = 0; b < 4; ++b)
+        for (int q = 0; q < 3; ++q) w.put(X.f64[b][q]);
+    }
     for (double T : ctx->ladders[si]) w.put(T);
     std::vector<int> tor(s.n_temp), rot(s.n_temp);
     std::vector<float> cone(s.n_temp);
@@ -180,7 +190,8 @@ int pyro_load_checkpoint(pyro_ctx* ctx, const char* path) {
   const uint32_t has_tet = r.get<uint32_t>();
   const uint64_t sweeps = r.get<uint64_t>();
   const uint64_t tet_sweeps = r.get<uint64_t>();
-  if (!r.ok || version != kVersion) return fail(ctx, PYRO_ERR_IO, "load_checkpoint: bad header");
+  if (!r.ok || (version != kVersion && version != 1))
+    return fail(ctx, PYRO_ERR_IO, "load_checkpoint: bad header");
   if (n_sys != ctx->sys.size() || seed != ctx->seed || renorm != ctx->renorm_every)
     return fail(ctx, PYRO_ERR_ARG, "load_checkpoint: written for another configuration");
   struct SysState {
@@ -200,6 +211,20 @@ int pyro_load_checkpoint(pyro_ctx* ctx, const char* path) {
       return fail(ctx, PYRO_ERR_ARG, "load_checkpoint: lattice or replicas differ");
     for (int k = 0; k < 4; ++k)
       if (J[k] != s.J64[k]) return fail(ctx, PYRO_ERR_ARG, "load_checkpoint: couplings differ");
+    const uint32_t has_x = version >= 2 ? r.get<uint32_t>() : 0u;
+    if (!r.ok) return fail(ctx, PYRO_ERR_IO, "load_checkpoint: truncated");
+    if ((has_x != 0) != (s.exch >= 0))
+      return fail(ctx, PYRO_ERR_ARG, "load_checkpoint: exchange matrices differ");
+    if (has_x) {
+      const ExchangeDev& X = ctx->exch[s.exch];
+      bool same = true;
+      for (int p = 0; p < 16; ++p)
+        for (int q = 0; q < 9; ++q) same = (r.get<double>() == X.A64[p][q]) && same;
+      for (int b = 0; b < 4; ++b)
+        for (int q = 0; q < 3; ++q) same = (r.get<double>() == X.f64[b][q]) && same;
+      if (!r.ok) return fail(ctx, PYRO_ERR_IO, "load_checkpoint: truncated");
+      if (!same) return fail(ctx, PYRO_ERR_ARG, "load_checkpoint: exchange matrices differ");
+    }
     for (int t = 0; t < nT; ++t)
       if (r.get<double>() != ctx->ladders[si][t])
         return fail(ctx, PYRO_ERR_ARG, "load_checkpoint: temperature ladder differs");

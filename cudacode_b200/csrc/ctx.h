@@ -27,6 +27,8 @@ struct pyro_ctx {
   pyro::NbrTable tab;
 
   std::vector<pyro::SysDev> sys;
+  std::vector<pyro::ExchangeDev> exch;  // bond matrices of the anisotropic systems (SysDev::exch)
+  pyro::ExchangeDev* d_exch = nullptr;
   std::vector<std::vector<double>> ladders;
   pyro::SysDev* d_sys = nullptr;
   int total_temps = 0;
@@ -122,10 +124,18 @@ struct pyro_ctx {
 
 namespace pyro {
 
+// Systems on the isotropic nearest-neighbour-only paths (specialised J1
+// kernels, learned tetrahedron move).
+inline bool j1_only(const SysDev& s) { return s.n_colours == 4 && s.shells == 1 && s.exch < 0; }
+
 inline int fail(pyro_ctx* c, int code, const std::string& msg) {
   if (c) c->err = msg;
   return code;
 }
+
+// Drops the captured cycle graphs and rebuilds the pass schedules (after a
+// change of kernel options or of a system's Hamiltonian).
+int rebuild_schedule(pyro_ctx* ctx);
 
 // Frees the learned-move state (tet_capi.cu).
 void tet_free(pyro_ctx* ctx);

@@ -71,6 +71,28 @@ __device__ __forceinline__ Acc3 shell_sum(const float4* __restrict__ rep, const 
   return a;
 }
 
+// Nearest-neighbour field of site s with bond matrices (anisotropic
+// exchange), minus the site's Zeeman field: sum over the six neighbours in
+// table order of A[b][b_k] S_k (pyro_matvec_add), then - f[b].
+__device__ __forceinline__ pyro_vec3 exch_field(const float4* __restrict__ rep, const NbrTable& tab,
+                                                const ExchangeDev& X, int s, int x, int y, int z,
+                                                int L, int L3) {
+  const int b = s & 3;
+  pyro_vec3 h;
+  h.x = h.y = h.z = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const NbrEntry e = tab.e[s][k];
+    const int idx = (wrap(z + e.dz, L) * L + wrap(y + e.dy, L)) * L + wrap(x + e.dx, L) + e.t * L3;
+    const float4 v = __ldg(rep + idx);
+    h = pyro_matvec_add(h, X.A[4 * b + (e.t & 3)], v.x, v.y, v.z);
+  }
+  h.x = h.x - X.f[b][0];
+  h.y = h.y - X.f[b][1];
+  h.z = h.z - X.f[b][2];
+  return h;
+}
+
 template <bool kJ1Only, bool kMetro>
 __global__ void __launch_bounds__(kPassThreads) colour_pass_kernel(const PassParams p,
                                                                    const NbrTable tab) {
@@ -97,11 +119,15 @@ __global__ void __launch_bounds__(kPassThreads) colour_pass_kernel(const PassPar
     const int own = s * L3 + cell;
     const float4 sv = rep_base[own];
 
-    const Acc3 a1 = shell_sum(rep_base, tab, s, 0, 6, x, y, z, L, L3);
     pyro_vec3 h;
-    h.x = sd.J1 * a1.x;
-    h.y = sd.J1 * a1.y;
-    h.z = sd.J1 * a1.z;
+    if (!kJ1Only && sd.exch >= 0) {
+      h = exch_field(rep_base, tab, p.exch[sd.exch], s, x, y, z, L, L3);
+    } else {
+      const Acc3 a1 = shell_sum(rep_base, tab, s, 0, 6, x, y, z, L, L3);
+      h.x = sd.J1 * a1.x;
+      h.y = sd.J1 * a1.y;
+      h.z = sd.J1 * a1.z;
+    }
     if (!kJ1Only) {
       if (sd.shells & 2) {
         const Acc3 a = shell_sum(rep_base, tab, s, 6, 18, x, y, z, L, L3);
@@ -183,7 +209,9 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// FP64 energy E = 1/2 sum_i S_i . h_i and magnetisation sum_i S_i.
+// FP64 energy E = 1/2 sum_i S_i . h_i and magnetisation sum_i S_i (with
+// bond matrices: E = 1/2 sum_i S_i . (sum_k A S_k) - sum_i f . S_i; the
+// partials hold twice the energy, halved by the finalise kernel).
 __global__ void __launch_bounds__(kObsThreads) observables_kernel(const ObsParams p,
                                                                   const NbrTable tab) {
   const int seg_i = find_segment(p.segs, p.nseg, blockIdx.x);
@@ -207,8 +235,26 @@ __global__ void __launch_bounds__(kObsThreads) observables_kernel(const ObsParam
     const int x = cell % L, yz = cell / L, y = yz % L, z = yz / L;
     const float4 sv = __ldg(rep_base + i);
     double hx = 0.0, hy = 0.0, hz = 0.0;
+    if (sd.exch >= 0) {
+      const ExchangeDev& X = p.exch[sd.exch];
+      const int b = s & 3;
+      for (int q = 0; q < 6; ++q) {
+        const NbrEntry en = tab.e[s][q];
+        const int idx =
+            (wrap(z + en.dz, L) * L + wrap(y + en.dy, L)) * L + wrap(x + en.dx, L) + en.t * L3;
+        const float4 v = __ldg(rep_base + idx);
+        const double* m = X.A64[4 * b + (en.t & 3)];
+        hx += m[0] * v.x + m[1] * v.y + m[2] * v.z;
+        hy += m[3] * v.x + m[4] * v.y + m[5] * v.z;
+        hz += m[6] * v.x + m[7] * v.y + m[8] * v.z;
+      }
+      hx -= 2.0 * X.f64[b][0];
+      hy -= 2.0 * X.f64[b][1];
+      hz -= 2.0 * X.f64[b][2];
+    }
     for (int sh = 0; sh < 4; ++sh) {
       if (!(sd.shells & (1 << sh))) continue;
+      if (sh == 0 && sd.exch >= 0) continue;
       double ax = 0.0, ay = 0.0, az = 0.0;
       for (int q = shell_begin[sh]; q < shell_begin[sh + 1]; ++q) {
         const NbrEntry en = tab.e[s][q];

@@ -25,6 +25,7 @@ struct PassParams {
   unsigned long long sweep_off; // added to *sweep_ctr (absolute if null)
   uint32_t seed_lo, seed_hi;
   int renorm_every;
+  const ExchangeDev* exch;      // bond matrices of anisotropic systems (SysDev::exch >= 0)
 };
 
 // Energy / magnetisation partial sums, one block per chunk of a replica.
@@ -41,6 +42,7 @@ struct ObsParams {
   const SysDev* sys;
   const float4* spins;
   double4* partials;  // one per block: (E, Mx, My, Mz)
+  const ExchangeDev* exch;
 };
 
 struct ExchangeParams {

@@ -153,6 +153,18 @@ struct SysDev {
   float J1, J2, J3a, J3b;   // FP32 couplings of the update arithmetic
   double J64[4];           // the same couplings in FP64 for the observables
   int shells;          // bitmask of non-zero shells: 1 J1, 2 J2, 4 J3a, 8 J3b
+  int exch;            // index of the system's bond matrices (ExchangeDev), -1: isotropic J1
+};
+
+// Bond-dependent nearest-neighbour exchange and Zeeman field of one system:
+// H = sum_<ij> S_i^T A[b_i][b_j] S_j - sum_i f[b_i] . S_i, b the pyrochlore
+// sublattice (site & 3). A[4 * bi + bj] is row-major; A[bj][bi] = A[bi][bj]^T.
+// Replaces the isotropic J1 shell (further shells stay isotropic).
+struct ExchangeDev {
+  float A[16][9];
+  float f[4][3];
+  double A64[16][9];
+  double f64[4][3];
 };
 
 // Sites of colour class c: for the 4-colour schedule colour b holds sites

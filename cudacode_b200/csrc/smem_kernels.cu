@@ -45,6 +45,26 @@ __device__ __forceinline__ float3 shell_sum_smem(const float4* lat, const NbrTab
   return a;
 }
 
+// Nearest-neighbour field with bond matrices minus the Zeeman field, in the
+// arithmetic of the per-pass kernels (pyro_matvec_add in table order).
+__device__ __forceinline__ pyro_vec3 exch_field_smem(const float4* lat, const NbrTable& tab,
+                                                     const ExchangeDev& X, int s, int x, int y,
+                                                     int z, int L, int L3) {
+  const int b = s & 3;
+  pyro_vec3 h;
+  h.x = h.y = h.z = 0.0f;
+  for (int k = 0; k < 6; ++k) {
+    const NbrEntry e = tab.e[s][k];
+    const float4 v =
+        lat[(wrap_s(z + e.dz, L) * L + wrap_s(y + e.dy, L)) * L + wrap_s(x + e.dx, L) + e.t * L3];
+    h = pyro_matvec_add(h, X.A[4 * b + (e.t & 3)], v.x, v.y, v.z);
+  }
+  h.x = h.x - X.f[b][0];
+  h.y = h.y - X.f[b][1];
+  h.z = h.z - X.f[b][2];
+  return h;
+}
+
 __device__ __forceinline__ double block_sum(double v, double* red) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -88,11 +108,15 @@ __global__ void __launch_bounds__(kSmemThreads) smem_cycles_kernel(const SmemCyc
           const int s = colour_site(sd.n_colours, colour, kk);
           const int x = cell % L, yz = cell / L, y = yz % L, z = yz / L;
           const int own = s * L3 + cell;
-          const float3 a1 = shell_sum_smem(lat, tab, s, 0, 6, x, y, z, L, L3);
           pyro_vec3 h;
-          h.x = sd.J1 * a1.x;
-          h.y = sd.J1 * a1.y;
-          h.z = sd.J1 * a1.z;
+          if (sd.exch >= 0) {
+            h = exch_field_smem(lat, tab, p.exch[sd.exch], s, x, y, z, L, L3);
+          } else {
+            const float3 a1 = shell_sum_smem(lat, tab, s, 0, 6, x, y, z, L, L3);
+            h.x = sd.J1 * a1.x;
+            h.y = sd.J1 * a1.y;
+            h.z = sd.J1 * a1.z;
+          }
           if (sd.shells & 2) {
             const float3 a = shell_sum_smem(lat, tab, s, 6, 18, x, y, z, L, L3);
             h.x = fmaf(sd.J2, a.x, h.x);
@@ -143,8 +167,24 @@ __global__ void __launch_bounds__(kSmemThreads) smem_cycles_kernel(const SmemCyc
         const int x = cell % L, yz = cell / L, y = yz % L, z = yz / L;
         const float4 sv = lat[i];
         const int sb[5] = {0, 6, 18, 24, 30};
+        if (sd.exch >= 0) {  // twice the bond energy of this site minus twice its Zeeman term
+          const ExchangeDev& X = p.exch[sd.exch];
+          const int b = s & 3;
+          double hx = -2.0 * X.f64[b][0], hy = -2.0 * X.f64[b][1], hz = -2.0 * X.f64[b][2];
+          for (int q = 0; q < 6; ++q) {
+            const NbrEntry en = tab.e[s][q];
+            const float4 v = lat[(wrap_s(z + en.dz, L) * L + wrap_s(y + en.dy, L)) * L +
+                                 wrap_s(x + en.dx, L) + en.t * L3];
+            const double* m = X.A64[4 * b + (en.t & 3)];
+            hx += m[0] * v.x + m[1] * v.y + m[2] * v.z;
+            hy += m[3] * v.x + m[4] * v.y + m[5] * v.z;
+            hz += m[6] * v.x + m[7] * v.y + m[8] * v.z;
+          }
+          e += (double)sv.x * hx + (double)sv.y * hy + (double)sv.z * hz;
+        }
         for (int sh = 0; sh < 4; ++sh) {
           if (!(sd.shells & (1 << sh))) continue;
+          if (sh == 0 && sd.exch >= 0) continue;
           double ax = 0.0, ay = 0.0, az = 0.0;
           for (int q = sb[sh]; q < sb[sh + 1]; ++q) {
             const NbrEntry en = tab.e[s][q];

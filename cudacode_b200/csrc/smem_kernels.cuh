@@ -26,6 +26,7 @@ struct SmemCycleParams {
   double* history;  // may be null
   const unsigned long long* history_count;
   int history_cap, total_temps;
+  const ExchangeDev* exch;  // bond matrices (sys.exch >= 0)
 };
 
 size_t smem_cycle_bytes(int L);

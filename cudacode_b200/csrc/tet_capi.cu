@@ -64,7 +64,7 @@ int need_tet(pyro_ctx* ctx) {
   return PYRO_OK;
 }
 
-bool j1_only_system(const SysDev& s) { return s.n_colours == 4 && s.shells == 1; }
+bool j1_only_system(const SysDev& s) { return j1_only(s); }
 
 // He-style initial weights from Philox (host), zero biases; the direction
 // outputs start as a random linear map, log kappa near 0.

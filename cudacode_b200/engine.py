@@ -131,6 +131,10 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "pyro_load_checkpoint": (i, [P, C.c_char_p]),
         "pyro_save_configurations": (i, [P, i, C.c_char_p, i]),
         "pyro_read_configurations": (i, [P, i, C.c_char_p, i]),
+        "pyro_set_exchange": (i, [P, i, pd, pd]),
+        "pyro_get_exchange": (i, [P, i, pd, pd, pi]),
+        "pyro_reference_exchange": (i, [d, d, d, d, pd]),
+        "pyro_reference_field": (i, [d, d, pd, pd]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -177,6 +181,26 @@ def neighbour_table(site: int) -> np.ndarray:
     if rc != PYRO_OK:
         raise PyroError(rc, "pyro_neighbour_table")
     return out.reshape(30, 4)
+
+
+def reference_exchange(J1: float, J2: float, J3: float, J4: float) -> np.ndarray:
+    """Bond matrices (4, 4, 3, 3) of the reference's J1..J4 model in this
+    engine's convention (energies and temperatures as the reference's)."""
+    out = np.empty(144, dtype=np.float64)
+    rc = load_library().pyro_reference_exchange(J1, J2, J3, J4, _ptr(out, C.c_double))
+    if rc != PYRO_OK:
+        raise PyroError(rc, "pyro_reference_exchange")
+    return out.reshape(4, 4, 3, 3)
+
+
+def reference_field(gxy: float, gz: float, B) -> np.ndarray:
+    """Site fields (4, 3) of a field B (tesla) with the reference's g-tensors."""
+    b = np.ascontiguousarray(B, dtype=np.float64).reshape(3)
+    out = np.empty(12, dtype=np.float64)
+    rc = load_library().pyro_reference_field(gxy, gz, _ptr(b, C.c_double), _ptr(out, C.c_double))
+    if rc != PYRO_OK:
+        raise PyroError(rc, "pyro_reference_field")
+    return out.reshape(4, 3)
 
 
 def geometric_ladder(t_min: float, t_max: float, n: int) -> list[float]:
@@ -321,6 +345,27 @@ class Engine:
         v = C.c_uint64()
         self._ck(self.lib.pyro_get_sweep_count(self.ctx, C.byref(v)))
         return v.value
+
+    # -- anisotropic exchange ----------------------------------------------
+    def set_exchange(self, exchange, field=None, system: int = 0) -> None:
+        """Bond matrices (4, 4, 3, 3) and site fields (4, 3) of a system;
+        exchange=None returns it to isotropic J1."""
+        if exchange is None:
+            self._ck(self.lib.pyro_set_exchange(self.ctx, system, None, None))
+            return
+        a = np.ascontiguousarray(exchange, dtype=np.float64).reshape(144)
+        f = None if field is None else np.ascontiguousarray(field, dtype=np.float64).reshape(12)
+        self._ck(self.lib.pyro_set_exchange(self.ctx, system, _ptr(a, C.c_double),
+                                            None if f is None else _ptr(f, C.c_double)))
+
+    def get_exchange(self, system: int = 0):
+        """(matrices, fields) as set, or None for an isotropic system."""
+        a = np.empty(144, dtype=np.float64)
+        f = np.empty(12, dtype=np.float64)
+        is_set = C.c_int()
+        self._ck(self.lib.pyro_get_exchange(self.ctx, system, _ptr(a, C.c_double),
+                                            _ptr(f, C.c_double), C.byref(is_set)))
+        return (a.reshape(4, 4, 3, 3), f.reshape(4, 3)) if is_set.value else None
 
     # -- cone -------------------------------------------------------------
     def set_cone(self, cosmax, system: int = 0) -> None:

@@ -226,6 +226,35 @@ int pyro_load_checkpoint(pyro_ctx* ctx, const char* path);
 int pyro_save_configurations(pyro_ctx* ctx, int system, const char* prefix, int append);
 int pyro_read_configurations(pyro_ctx* ctx, int system, const char* prefix, int repetition);
 
+/* Bond-dependent nearest-neighbour exchange and Zeeman field of one system
+ * (the reference's anisotropic model: bond matrices couplings_const,
+ * Pyrochlore.cu:169-184, used by CalculateLocalExchangeField 210-275 and
+ * TotalEnergy 468-523; site fields InitializeMagneticField 414-450):
+ *   H = sum_<ij> S_i^T A[b_i][b_j] S_j - sum_i f[b_i] . S_i + (J2, J3 shells),
+ * S unit vectors, b = site & 3 the pyrochlore sublattice.
+ * exchange144[(4 a + b) * 9 + 3 r + c] = A[a][b][r][c]; A[b][a] must be the
+ * transpose of A[a][b] (else PYRO_ERR_ARG); the diagonal blocks are ignored.
+ * field12[3 b + r] = f[b][r] (NULL: no field). The matrices replace the
+ * system's J1; its J2 / J3 shells stay. exchange144 = NULL returns the
+ * system to isotropic J1. Updates keep the bit-exact contract (each bond one
+ * pyro_matvec_add in canonical neighbour order, then minus f). Such a system
+ * runs on the generic and shared-memory kernels; the learned tetrahedron
+ * move skips it. Invalidates the captured cycle graphs. */
+int pyro_set_exchange(pyro_ctx* ctx, int system, const double* exchange144,
+                      const double* field12);
+/* The system's matrices and field as set (is_set = 0 for isotropic J1). */
+int pyro_get_exchange(pyro_ctx* ctx, int system, double* exchange144, double* field12,
+                      int* is_set);
+/* The reference's parameterisation in this convention, so that energies
+ * and temperatures equal the reference's (its spin-1/2 factor 1/4 folded
+ * in): A = -C / 4 with C the couplings_const matrices of J1..J4
+ * (Pyrochlore.cu:169-184), generated from the lattice symmetry; and
+ * f_b = (1/2) mu_B g_b B with g_b = gxy I + (gz - gxy) z_b z_b^T (z_b the
+ * local <111> axis of sublattice b), B in tesla, mu_B = 0.0578838261305
+ * meV/T (InitializeMagneticField, Pyrochlore.cu:414-450). */
+int pyro_reference_exchange(double J1, double J2, double J3, double J4, double* exchange144);
+int pyro_reference_field(double gxy, double gz, const double* B3, double* field12);
+
 /* Static structure factor S(q) = (1/N) sum_a |sum_i S_i^a e^{-i q.r_i}|^2,
  * averaged over the replicas held, on a grid of G^3 wave vectors
  * q = (2 pi / L) * stride * (h, k, l), h, k, l in [-G/2, G/2); out[(h' G + k') G + l'].

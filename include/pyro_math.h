@@ -228,6 +228,18 @@ PYRO_HD pyro_vec3 pyro_cone_proposal(pyro_vec3 s, float cosmax, float u1, float 
   return pyro_about_axis(s, ct, st, cp, sp);
 }
 
+/* h + M v for one bond of the anisotropic exchange, M the row-major 3x3
+ * bond matrix: each component one chain of fused multiply-adds over the
+ * columns in order. The local field of a site is the sum of these over its
+ * six nearest neighbours in canonical order, minus its Zeeman field. */
+PYRO_HD pyro_vec3 pyro_matvec_add(pyro_vec3 h, const float* m, float vx, float vy, float vz) {
+  pyro_vec3 o;
+  o.x = fmaf(m[2], vz, fmaf(m[1], vy, fmaf(m[0], vx, h.x)));
+  o.y = fmaf(m[5], vz, fmaf(m[4], vy, fmaf(m[3], vx, h.y)));
+  o.z = fmaf(m[8], vz, fmaf(m[7], vy, fmaf(m[6], vx, h.z)));
+  return o;
+}
+
 /* Energy change of replacing s by t in local field h (E_i = s . h). */
 PYRO_HD float pyro_delta_e(pyro_vec3 h, pyro_vec3 s, pyro_vec3 t) {
   const float dx = t.x - s.x, dy = t.y - s.y, dz = t.z - s.z;

@@ -37,6 +37,7 @@ def load() -> C.CDLL:
         "orc_metropolis_sweep": (None, [P, i]),
         "orc_overrelax_sweep": (None, [P, i]),
         "orc_set_cone": (None, [P, i, pf]),
+        "orc_set_exchange": (None, [P, i, pd, pd]),
         "orc_get_cone": (None, [P, i, pf]),
         "orc_get_acceptance": (None, [P, i, pu64, pu64]),
         "orc_reset_acceptance": (None, [P]),
@@ -133,6 +134,16 @@ class Oracle:
 
     def overrelax_sweep(self, n=1):
         self.lib.orc_overrelax_sweep(self.h, n)
+
+    def set_exchange(self, exchange, field=None, system=0):
+        """Bond matrices (4 x 4 x 3 x 3) and site fields (4 x 3) of a system."""
+        if exchange is None:
+            self.lib.orc_set_exchange(self.h, system, None, None)
+            return
+        a = np.ascontiguousarray(exchange, dtype=np.float64).reshape(144)
+        f = None if field is None else np.ascontiguousarray(field, dtype=np.float64).reshape(12)
+        self.lib.orc_set_exchange(self.h, system, _p(a, C.c_double),
+                                  None if f is None else _p(f, C.c_double))
 
     def set_cone(self, c, system=0):
         a = np.ascontiguousarray(c, dtype=np.float32)

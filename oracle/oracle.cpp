@@ -13,7 +13,12 @@
 //   over-relaxation S -> 2(S.h)h/|h|^2 - S               Math.cu:220-242
 //   replica exchange min(1, exp((b1-b2)(E1-E2)))         MonteCarlo.cu:105-172
 //   cone-width adaptation                                MonteCarlo.cu:371-426
-// Units: unit classical spins, H = J1 sum_<ij> S_i.S_j (+ J2, J3a, J3b shells).
+// Units: unit classical spins, H = J1 sum_<ij> S_i.S_j (+ J2, J3a, J3b shells),
+// or, for the anisotropic model, H = sum_<ij> S_i^T A[b_i][b_j] S_j -
+// sum_i f[b_i] . S_i (b the sublattice; CalculateLocalExchangeField
+// Pyrochlore.cu:210-275 and TotalEnergy 468-523 with the bond matrices of
+// couplings_const 169-184 and the site fields of InitializeMagneticField
+// 414-450, their spin-1/2 factor folded into A and f).
 // The reference's TotalEnergy equals this energy times S^2 = 1/4 when its
 // J1 = J2 = J and J3 = J4 = 0 (couplings_const, Pyrochlore.cu:169-184).
 //
@@ -116,6 +121,9 @@ std::array<std::array<Nbr, 30>, 16> build_geometry() {
 struct Sys {
   int L, L3, R, off, nT, n_colours, temp_base, rep_key, shells;
   double J[4];
+  bool exch = false;  // bond matrices replace the isotropic J1 shell
+  float A[16][9] = {}, f[4][3] = {};
+  double A64[16][9] = {}, f64[4][3] = {};
   std::vector<double> T;
   size_t spin_off;  // in spins
 };
@@ -151,6 +159,19 @@ pyro_vec3 field32(const Oracle& o, const Sys& S, const float* rep, int s, int x,
   const float Jf[4] = {(float)S.J[0], (float)S.J[1], (float)S.J[2], (float)S.J[3]};
   pyro_vec3 h = {0.f, 0.f, 0.f};
   for (int sh = 0; sh < 4; ++sh) {
+    if (sh == 0 && S.exch) {
+      // bond matrices: h = sum_k A[b][b_k] S_k (pyro_matvec_add), then - f[b]
+      const int b = s & 3;
+      for (int k = 0; k < 6; ++k) {
+        const Nbr& e = o.nb[s][k];
+        const float* v = rep + 4 * nbr_index(S, e, x, y, z);
+        h = pyro_matvec_add(h, S.A[4 * b + (e.t & 3)], v[0], v[1], v[2]);
+      }
+      h.x = h.x - S.f[b][0];
+      h.y = h.y - S.f[b][1];
+      h.z = h.z - S.f[b][2];
+      continue;
+    }
     if (sh > 0 && !(S.shells & (1 << sh))) continue;
     const int k0 = kShellBegin[sh];
     const float* v0 = rep + 4 * nbr_index(S, o.nb[s][k0], x, y, z);
@@ -178,10 +199,28 @@ struct V3d {
   double x, y, z;
 };
 
+// FP64 bond-matrix field minus the site field (anisotropic systems).
+template <typename T>
+V3d exch_field64(const Oracle& o, const Sys& S, const T* rep, int s, int x, int y, int z) {
+  const int b = s & 3;
+  V3d h = {-S.f64[b][0], -S.f64[b][1], -S.f64[b][2]};
+  for (int k = 0; k < 6; ++k) {
+    const Nbr& e = o.nb[s][k];
+    const T* v = rep + 4 * nbr_index(S, e, x, y, z);
+    const double* m = S.A64[4 * b + (e.t & 3)];
+    h.x += m[0] * v[0] + m[1] * v[1] + m[2] * v[2];
+    h.y += m[3] * v[0] + m[4] * v[1] + m[5] * v[2];
+    h.z += m[6] * v[0] + m[7] * v[1] + m[8] * v[2];
+  }
+  return h;
+}
+
 V3d field64(const Oracle& o, const Sys& S, const double* rep, int s, int x, int y, int z) {
   V3d h = {0, 0, 0};
+  if (S.exch) h = exch_field64(o, S, rep, s, x, y, z);
   for (int sh = 0; sh < 4; ++sh) {
     if (!(S.shells & (1 << sh))) continue;
+    if (sh == 0 && S.exch) continue;
     double ax = 0, ay = 0, az = 0;
     for (int k = kShellBegin[sh]; k < kShellBegin[sh + 1]; ++k) {
       const double* v = rep + 4 * nbr_index(S, o.nb[s][k], x, y, z);
@@ -199,8 +238,10 @@ V3d field64(const Oracle& o, const Sys& S, const double* rep, int s, int x, int 
 // FP64 field from FP32 spins (observables of the FP32 chain).
 V3d field64f(const Oracle& o, const Sys& S, const float* rep, int s, int x, int y, int z) {
   V3d h = {0, 0, 0};
+  if (S.exch) h = exch_field64(o, S, rep, s, x, y, z);
   for (int sh = 0; sh < 4; ++sh) {
     if (!(S.shells & (1 << sh))) continue;
+    if (sh == 0 && S.exch) continue;
     double ax = 0, ay = 0, az = 0;
     for (int k = kShellBegin[sh]; k < kShellBegin[sh + 1]; ++k) {
       const float* v = rep + 4 * nbr_index(S, o.nb[s][k], x, y, z);
@@ -352,6 +393,10 @@ void observables(const Oracle& o, int si, std::vector<double>* E, std::vector<do
         h = field64(o, S, rep, s, x, y, z);
       }
       e += sx * h.x + sy * h.y + sz * h.z;
+      if (S.exch) {  // the site field enters E once, not halved like the bonds
+        const int b = s & 3;
+        e -= S.f64[b][0] * sx + S.f64[b][1] * sy + S.f64[b][2] * sz;
+      }
       mx += sx;
       my += sy;
       mz += sz;
@@ -512,6 +557,23 @@ void orc_metropolis_sweep(void* p, int n) {
 
 void orc_overrelax_sweep(void* p, int n) {
   for (int i = 0; i < n; ++i) sweep_one(*(Oracle*)p, false);
+}
+
+// Bond matrices A[16][9] (row-major per sublattice pair) and site fields
+// f[4][3] (null: none) of one system; A = null returns it to isotropic J1.
+void orc_set_exchange(void* p, int si, const double* A144, const double* f12) {
+  Oracle& o = *(Oracle*)p;
+  Sys& S = o.sys[si];
+  S.exch = A144 != nullptr;
+  for (int q = 0; q < 144; ++q) {
+    const int a = (q / 9) / 4, b = (q / 9) % 4;
+    S.A64[q / 9][q % 9] = (A144 && a != b) ? A144[q] : 0.0;
+    S.A[q / 9][q % 9] = (float)S.A64[q / 9][q % 9];
+  }
+  for (int q = 0; q < 12; ++q) {
+    S.f64[q / 3][q % 3] = (A144 && f12) ? f12[q] : 0.0;
+    S.f[q / 3][q % 3] = (float)S.f64[q / 3][q % 3];
+  }
 }
 
 void orc_set_cone(void* p, int si, const float* c) {
