@@ -333,6 +333,59 @@ def run_large(args):
     return 0
 
 
+def run_aniso(args):
+    """The reference's anisotropic model (bond matrices of J1..J4 at the
+    reference's default couplings, g-tensor Zeeman field of B = 1 T along
+    [001], gxy = 2.4, gz = 0.3): L=32, 64 replicas on a geometric ladder in
+    [0.02, 2.0], cycles of 1 Metropolis + 4 over-relaxation sweeps + FP64
+    energies + exchange; host baseline: the oracle port on 4 replicas."""
+    import time
+
+    import torch
+
+    from cudacode_b200.engine import (Engine, System, geometric_ladder, reference_exchange,
+                                      reference_field)
+    from oracle.binding import Oracle
+
+    J = (-0.09 / 0.29, -0.22 / 0.29, -1.00, 0.0)
+    A = reference_exchange(*J)
+    f = reference_field(2.4, 0.3, [0.0, 0.0, 1.0])
+    temps = geometric_ladder(0.02, 2.0, 64)
+    s = System(L=32, temperatures=temps, J1=0.0)
+    eng = Engine([s], seed=SEED + 6)
+    stream = torch.cuda.Stream()
+    eng.set_stream(stream.cuda_stream)
+    eng.set_exchange(A, f)
+    eng.init_random()
+    eng.set_cone(np.full(64, 0.3, dtype=np.float32))
+    choice = eng.autotune(1, 4, 1)
+    eng.cycle(1, 4, True, max(3, args.warmup))
+    steps = args.steps if args.steps != 300 else 100
+    sec = _timed(stream, lambda: eng.cycle(1, 4, True, steps))
+    updates = 64 * s.n_sites * 5 * steps
+    # host: the oracle port on 4 of the replicas, all cores
+    host = System(L=32, temperatures=temps[:4], J1=0.0)
+    o = Oracle([host], seed=SEED + 6, threads=os.cpu_count())
+    o.set_exchange(A, f)
+    o.init_random()
+    o.set_cone(np.full(4, 0.3, dtype=np.float32))
+    t0 = time.perf_counter()
+    o.cycle(1, 4, True, 3)
+    host_s = time.perf_counter() - t0
+    host_rate = 4 * host.n_sites * 5 * 3 / (host_s * 1e9)
+    print(json.dumps({
+        "metric": "spin-updates/ns", "workload": "aniso", "value": updates / (sec * 1e9),
+        "unit": "updates/ns", "ms_per_step": 1e3 * sec / steps, "steps": steps,
+        "autotune_choice": choice,
+        "cpu_baseline": {"value": host_rate, "unit": "updates/ns", "cores": os.cpu_count(),
+                         "kind": "port", "sample": "4 replicas x 3 cycles"},
+        "config": {"workload": "anisotropic J1-J4 model at the reference's default couplings "
+                               "(-0.09/0.29, -0.22/0.29, -1, 0) with a 1 T [001] field (gxy 2.4, "
+                               "gz 0.3): L=32, 64 replicas in [0.02, 2.0], 1 M + 4 OR + "
+                               "exchange"}}), flush=True)
+    return 0
+
+
 def run_learned(args):
     """Energy ESS/s of plain PT cycles (1 Metropolis + 4 over-relaxation
     sweeps + exchange) against the same cycles with one learned tetrahedron
@@ -427,11 +480,12 @@ def main():
     ap.add_argument("--L", type=int, default=L, help="lattice size (profiling cases)")
     ap.add_argument("--replicas", type=int, default=R_PER_GPU, help="replicas per GPU")
     ap.add_argument("--workload", default="pt",
-                    choices=["pt", "learned", "small", "batched", "large"],
+                    choices=["pt", "learned", "small", "batched", "large", "aniso"],
                     help="pt: the parallel-tempering benchmark (default); learned: energy "
                          "ESS/s of the learned tetrahedron proposal vs the plain method; "
                          "small: L=4 on the GPU and on the host; batched: 256 uneven "
-                         "systems; large: L=64 with J2/J3, S(q) and FP64 error accounting")
+                         "systems; large: L=64 with J2/J3, S(q) and FP64 error accounting; "
+                         "aniso: the reference's anisotropic J1-J4 model with a field")
     ap.add_argument("--kernel", default="auto", choices=["auto", "pass", "cluster", "grouped"],
                     help="auto: autotuner picks; pass: one launch per colour pass; "
                          "cluster: cluster-resident cycle kernel; grouped: per-pass kernels "
@@ -447,6 +501,8 @@ def main():
         return run_batched(args)
     if args.workload == "large":
         return run_large(args)
+    if args.workload == "aniso":
+        return run_aniso(args)
     set_workload(args.L, args.replicas)
     if args.impl == "reference":
         return run_reference(args)

@@ -75,6 +75,20 @@ J1PassParams j1_params(pyro_ctx* ctx, int si, unsigned long long off) {
   p.seed_lo = (uint32_t)(ctx->seed & 0xffffffffu);
   p.seed_hi = (uint32_t)(ctx->seed >> 32);
   p.renorm_every = ctx->renorm_every;
+  p.exch = s.exch >= 0 ? 1 : 0;
+  std::memset(p.xa, 0, sizeof p.xa);
+  std::memset(p.xf, 0, sizeof p.xf);
+  if (s.exch >= 0) {
+    const ExchangeDev& X = ctx->exch[s.exch];
+    for (int b = 0; b < 4; ++b) {
+      for (int t = 0, slot = 0; t < 4; ++t) {
+        if (t == b) continue;
+        for (int q = 0; q < 9; ++q) p.xa[b][slot][q] = X.A[4 * b + t][q];
+        ++slot;
+      }
+      for (int q = 0; q < 3; ++q) p.xf[b][q] = X.f[b][q];
+    }
+  }
   return p;
 }
 
@@ -152,8 +166,11 @@ int check_cluster(pyro_ctx* ctx) {
   return PYRO_OK;
 }
 
+// The cluster-resident cycle kernel runs isotropic J1 systems only; with a
+// bond-matrix system on the J1 path every J1 system takes per-pass kernels.
 bool use_cycle_kernel(const pyro_ctx* ctx) {
-  return ctx->cycle_kernel && ctx->use_j1_kernel && !ctx->obs_j1.empty();
+  return ctx->cycle_kernel && ctx->use_j1_kernel && !ctx->obs_j1.empty() &&
+         ctx->j1_sys.size() == ctx->obs_j1.size();
 }
 
 // n_metro Metropolis + n_or over-relaxation sweeps of every system, and (if
@@ -183,7 +200,7 @@ int queue_grouped(pyro_ctx* ctx, int n_metro, int n_or, bool j1_grouped, bool ge
   }
   int gi = 0;
   if (j1_grouped) {
-    for (int si : ctx->obs_j1) {
+    for (int si : ctx->j1_sys) {
       const SysDev& s = ctx->sys[si];
       for (int r0 = 0; r0 < s.n_rep; r0 += ctx->rep_group, ++gi) {
         cudaStream_t st = chains > 1 ? ctx->chain_stream[gi % chains] : ctx->stream;
@@ -246,7 +263,7 @@ int queue_cycle_body(pyro_ctx* ctx, int n_metro, int n_or, bool with_obs) {
   int rc = check_cluster(ctx);
   if (rc) return rc;
   const bool cyc = use_cycle_kernel(ctx);
-  const bool j1_grouped = !cyc && ctx->rep_group > 0 && ctx->use_j1_kernel && !ctx->obs_j1.empty();
+  const bool j1_grouped = !cyc && ctx->rep_group > 0 && ctx->use_j1_kernel && !ctx->j1_sys.empty();
   const bool gen_grouped = !ctx->gen_groups.empty();
   if (j1_grouped || gen_grouped) {
     rc = queue_grouped(ctx, n_metro, n_or, j1_grouped, gen_grouped);
@@ -389,7 +406,7 @@ int build_schedule(pyro_ctx* ctx) {
   ctx->pass_segs.assign(ctx->n_passes, {});
   ctx->pass_j1.assign(ctx->n_passes, {});
   ctx->pass_blocks.assign(ctx->n_passes, 0);
-  auto j1_path = [&](const SysDev& s) { return ctx->use_j1_kernel && j1_only(s); };
+  auto j1_path = [&](const SysDev& s) { return ctx->use_j1_kernel && j1_sweepable(s); };
   for (int pass = 0; pass < ctx->n_passes; ++pass) {
     int blocks = 0;
     for (int i = 0; i < (int)ctx->sys.size(); ++i) {
@@ -420,6 +437,7 @@ int build_schedule(pyro_ctx* ctx) {
   ctx->obs_segs.clear();
   ctx->obs_generic.clear();
   ctx->obs_j1.clear();
+  ctx->j1_sys.clear();
   int partial = 0, gblocks = 0;
   for (int i = 0; i < (int)ctx->sys.size(); ++i) {
     const SysDev& s = ctx->sys[i];
@@ -427,7 +445,8 @@ int build_schedule(pyro_ctx* ctx) {
     g.sys = i;
     g.partial_begin = partial;
     g.block_begin = partial;
-    if (j1_path(s)) {
+    if (j1_path(s)) ctx->j1_sys.push_back(i);
+    if (j1_path(s) && s.exch < 0) {
       g.blocks_per_rep = j1_blocks_per_replica(s.L3);
       ctx->obs_j1.push_back(i);
     } else {
@@ -854,7 +873,7 @@ int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen)
   struct Variant { int j1, cyc, cs, site, group, chains, gen_mb; };
   bool any_j1 = false, any_gen = false;
   for (const auto& s : ctx->sys) {
-    if (j1_only(s)) any_j1 = true;
+    if (j1_sweepable(s)) any_j1 = true;
     else any_gen = true;
   }
   std::vector<Variant> vs;

@@ -59,6 +59,9 @@ struct pyro_ctx {
   // J1-only systems on the specialised path are listed in obs_j1.
   std::vector<pyro::ObsSeg> obs_segs, obs_generic;
   std::vector<int> obs_j1;
+  // Systems swept by the specialised J1 kernels: obs_j1 (isotropic) plus the
+  // 4-colour systems with bond matrices (their observables run generic).
+  std::vector<int> j1_sys;
   pyro::ObsSeg* d_obs_segs = nullptr;
   pyro::ObsSeg* d_obs_generic = nullptr;
   int obs_generic_blocks = 0;
@@ -127,6 +130,11 @@ namespace pyro {
 // Systems on the isotropic nearest-neighbour-only paths (specialised J1
 // kernels, learned tetrahedron move).
 inline bool j1_only(const SysDev& s) { return s.n_colours == 4 && s.shells == 1 && s.exch < 0; }
+// Systems the specialised nearest-neighbour sweep kernels can run: J1-only,
+// or bond matrices with no further shells.
+inline bool j1_sweepable(const SysDev& s) {
+  return s.n_colours == 4 && (j1_only(s) || (s.exch >= 0 && (s.shells & ~1) == 0));
+}
 
 inline int fail(pyro_ctx* c, int code, const std::string& msg) {
   if (c) c->err = msg;

@@ -1,6 +1,10 @@
 // Nearest-neighbour (J1-only) kernels: the 4-colour schedule of the
 // pyrochlore Heisenberg model, specialised for sm_100a.
 //
+// Systems with bond matrices (anisotropic exchange and a Zeeman field) run
+// the same per-pass kernels with the field of ExchangeDev: six
+// pyro_matvec_add in canonical order, minus f, as the generic kernel.
+//
 // One thread owns one cubic cell of one replica and, in the pass of colour b,
 // updates the four sites {b, 4+b, 8+b, 12+b} of that cell (one per FCC
 // corner; none of them are neighbours). The 24 neighbour offsets are
@@ -94,18 +98,43 @@ __device__ __forceinline__ pyro_vec3 j1_sum(const float4* __restrict__ rep, cons
   return a;
 }
 
-template <int S, bool kMetro, bool kL2Only = false>
+// h + A[b][b_K] S_K for neighbour K of site S (b = S & 3): the matrix of
+// the neighbour's sublattice among the three kept for b.
+template <int S, int K, bool kL2Only>
+__device__ __forceinline__ pyro_vec3 exch_add(pyro_vec3 h, const float4* __restrict__ rep,
+                                              const CellFrame& f, int L3, const J1PassParams& p) {
+  constexpr NbrEntry e = j1_neighbour(S, K);
+  constexpr int b = S & 3, t = e.t & 3, slot = t < b ? t : t - 1;
+  static_assert(t != b, "nearest neighbours are on other sublattices");
+  const float4 v = load_neighbour<S, K, kL2Only>(rep, f, L3);
+  return pyro_matvec_add(h, p.xa[b][slot], v.x, v.y, v.z);
+}
+
+template <int S, bool kMetro, bool kL2Only = false, bool kExch = false>
 __device__ __forceinline__ int update_site(float4* __restrict__ rep, const CellFrame& f, int cell,
                                            int L3, float J1, float beta, float cosmax, uint32_t rkey,
                                            uint32_t sweep32, bool renorm, uint32_t seed_lo,
-                                           uint32_t seed_hi) {
+                                           uint32_t seed_hi, const J1PassParams& p) {
   const int own = S * L3 + cell;
   const float4 sv = kL2Only ? __ldcg(rep + own) : rep[own];
-  const pyro_vec3 a = j1_sum<S, kL2Only>(rep, f, L3);
   pyro_vec3 h;
-  h.x = J1 * a.x;
-  h.y = J1 * a.y;
-  h.z = J1 * a.z;
+  if (kExch) {
+    h.x = h.y = h.z = 0.0f;
+    h = exch_add<S, 0, kL2Only>(h, rep, f, L3, p);
+    h = exch_add<S, 1, kL2Only>(h, rep, f, L3, p);
+    h = exch_add<S, 2, kL2Only>(h, rep, f, L3, p);
+    h = exch_add<S, 3, kL2Only>(h, rep, f, L3, p);
+    h = exch_add<S, 4, kL2Only>(h, rep, f, L3, p);
+    h = exch_add<S, 5, kL2Only>(h, rep, f, L3, p);
+    h.x = h.x - p.xf[S & 3][0];
+    h.y = h.y - p.xf[S & 3][1];
+    h.z = h.z - p.xf[S & 3][2];
+  } else {
+    const pyro_vec3 a = j1_sum<S, kL2Only>(rep, f, L3);
+    h.x = J1 * a.x;
+    h.y = J1 * a.y;
+    h.z = J1 * a.z;
+  }
   pyro_vec3 sp;
   sp.x = sv.x;
   sp.y = sv.y;
@@ -127,7 +156,7 @@ __device__ __forceinline__ int update_site(float4* __restrict__ rep, const CellF
   return acc;
 }
 
-template <int B, bool kMetro>
+template <int B, bool kMetro, bool kExch>
 __global__ void __launch_bounds__(kJ1Threads) j1_pass_kernel(const J1PassParams p) {
   const int rep = blockIdx.y;
   const int cell = blockIdx.x * kJ1Threads + threadIdx.x;
@@ -150,14 +179,14 @@ __global__ void __launch_bounds__(kJ1Threads) j1_pass_kernel(const J1PassParams 
         p.renorm_every > 0 && ((sweep + 1) % (unsigned long long)p.renorm_every) == 0;
     const uint32_t rkey = (uint32_t)(p.rep_key + rep);
     const uint32_t sw = (uint32_t)sweep;
-    acc += update_site<B, kMetro>(rb, f, cell, p.L3, p.J1, beta, cosmax, rkey, sw, renorm,
-                                  p.seed_lo, p.seed_hi);
-    acc += update_site<4 + B, kMetro>(rb, f, cell, p.L3, p.J1, beta, cosmax, rkey, sw, renorm,
-                                      p.seed_lo, p.seed_hi);
-    acc += update_site<8 + B, kMetro>(rb, f, cell, p.L3, p.J1, beta, cosmax, rkey, sw, renorm,
-                                      p.seed_lo, p.seed_hi);
-    acc += update_site<12 + B, kMetro>(rb, f, cell, p.L3, p.J1, beta, cosmax, rkey, sw, renorm,
-                                       p.seed_lo, p.seed_hi);
+    acc += update_site<B, kMetro, false, kExch>(rb, f, cell, p.L3, p.J1, beta, cosmax, rkey, sw,
+                                                renorm, p.seed_lo, p.seed_hi, p);
+    acc += update_site<4 + B, kMetro, false, kExch>(rb, f, cell, p.L3, p.J1, beta, cosmax, rkey,
+                                                    sw, renorm, p.seed_lo, p.seed_hi, p);
+    acc += update_site<8 + B, kMetro, false, kExch>(rb, f, cell, p.L3, p.J1, beta, cosmax, rkey,
+                                                    sw, renorm, p.seed_lo, p.seed_hi, p);
+    acc += update_site<12 + B, kMetro, false, kExch>(rb, f, cell, p.L3, p.J1, beta, cosmax, rkey,
+                                                     sw, renorm, p.seed_lo, p.seed_hi, p);
   }
   if (kMetro) {
     // Block-wide count of accepted moves: one atomic per CTA.
@@ -180,7 +209,7 @@ __global__ void __launch_bounds__(kJ1Threads) j1_pass_kernel(const J1PassParams 
 // S = 4 f + B is uniform in a CTA), blockIdx.z the replica. Fewer live
 // registers than the cell-per-thread form, hence more warps in flight; the
 // Metropolis pass (Philox, cone, exp) is latency-bound without them.
-template <int B, bool kMetro>
+template <int B, bool kMetro, bool kExch>
 __global__ void __launch_bounds__(kJ1Threads) j1_site_pass_kernel(const J1PassParams p) {
   const int f = blockIdx.y;
   const int rep = blockIdx.z;
@@ -206,20 +235,20 @@ __global__ void __launch_bounds__(kJ1Threads) j1_site_pass_kernel(const J1PassPa
     const uint32_t sw = (uint32_t)sweep;
     switch (f) {
       case 0:
-        acc = update_site<B, kMetro>(rb, fr, cell, p.L3, p.J1, beta, cosmax, rkey, sw, renorm,
-                                     p.seed_lo, p.seed_hi);
+        acc = update_site<B, kMetro, false, kExch>(rb, fr, cell, p.L3, p.J1, beta, cosmax, rkey,
+                                                   sw, renorm, p.seed_lo, p.seed_hi, p);
         break;
       case 1:
-        acc = update_site<4 + B, kMetro>(rb, fr, cell, p.L3, p.J1, beta, cosmax, rkey, sw, renorm,
-                                         p.seed_lo, p.seed_hi);
+        acc = update_site<4 + B, kMetro, false, kExch>(rb, fr, cell, p.L3, p.J1, beta, cosmax,
+                                                       rkey, sw, renorm, p.seed_lo, p.seed_hi, p);
         break;
       case 2:
-        acc = update_site<8 + B, kMetro>(rb, fr, cell, p.L3, p.J1, beta, cosmax, rkey, sw, renorm,
-                                         p.seed_lo, p.seed_hi);
+        acc = update_site<8 + B, kMetro, false, kExch>(rb, fr, cell, p.L3, p.J1, beta, cosmax,
+                                                       rkey, sw, renorm, p.seed_lo, p.seed_hi, p);
         break;
       default:
-        acc = update_site<12 + B, kMetro>(rb, fr, cell, p.L3, p.J1, beta, cosmax, rkey, sw,
-                                          renorm, p.seed_lo, p.seed_hi);
+        acc = update_site<12 + B, kMetro, false, kExch>(rb, fr, cell, p.L3, p.J1, beta, cosmax,
+                                                        rkey, sw, renorm, p.seed_lo, p.seed_hi, p);
         break;
     }
   }
@@ -338,23 +367,26 @@ template <int S, bool kMetro>
 __device__ __forceinline__ int cluster_site(float4* __restrict__ rb, int cell, int L, int L3,
                                             float rcpL, float J1, float beta, float cosmax,
                                             uint32_t rkey, uint32_t sw, bool renorm,
-                                            uint32_t seed_lo, uint32_t seed_hi) {
+                                            uint32_t seed_lo, uint32_t seed_hi,
+                                            const J1PassParams& pp) {
   int x, y, z;
   decode_cell(cell, L, rcpL, &x, &y, &z);
   const CellFrame f = make_frame(x, y, z, L);
   return update_site<S, kMetro, true>(rb, f, cell, L3, J1, beta, cosmax, rkey, sw, renorm,
-                                      seed_lo, seed_hi);
+                                      seed_lo, seed_hi, pp);
 }
 
 template <bool kMetro>
 __device__ __forceinline__ int cluster_dispatch(int s, float4* __restrict__ rb, int cell, int L,
                                                 int L3, float rcpL, float J1, float beta,
                                                 float cosmax, uint32_t rkey, uint32_t sw,
-                                                bool renorm, uint32_t seed_lo, uint32_t seed_hi) {
+                                                bool renorm, uint32_t seed_lo, uint32_t seed_hi,
+                                                const J1PassParams& pp) {
   switch (s) {
 #define PYRO_SITE(S) \
   case S:            \
-    return cluster_site<S, kMetro>(rb, cell, L, L3, rcpL, J1, beta, cosmax, rkey, sw, renorm, seed_lo, seed_hi);
+    return cluster_site<S, kMetro>(rb, cell, L, L3, rcpL, J1, beta, cosmax, rkey, sw, renorm, \
+                                   seed_lo, seed_hi, pp);
     PYRO_SITE(0) PYRO_SITE(1) PYRO_SITE(2) PYRO_SITE(3) PYRO_SITE(4) PYRO_SITE(5) PYRO_SITE(6)
     PYRO_SITE(7) PYRO_SITE(8) PYRO_SITE(9) PYRO_SITE(10) PYRO_SITE(11) PYRO_SITE(12)
     PYRO_SITE(13) PYRO_SITE(14) PYRO_SITE(15)
@@ -416,10 +448,10 @@ __global__ void __launch_bounds__(kJ1CycleThreads, 1)
           const int s = 4 * fc + b;
           if (metro)
             acc += cluster_dispatch<true>(s, rb, cell, L, L3, rcpL, p.pass.J1, beta, cosmax, rkey,
-                                          sw, renorm, p.pass.seed_lo, p.pass.seed_hi);
+                                          sw, renorm, p.pass.seed_lo, p.pass.seed_hi, p.pass);
           else
             cluster_dispatch<false>(s, rb, cell, L, L3, rcpL, p.pass.J1, beta, cosmax, rkey, sw,
-                                    renorm, p.pass.seed_lo, p.pass.seed_hi);
+                                    renorm, p.pass.seed_lo, p.pass.seed_hi, p.pass);
         }
       }
       cluster_barrier();
@@ -492,23 +524,34 @@ void launch_j1_pass(const J1PassParams& p, int colour, bool metro, bool site_per
                     cudaStream_t st) {
   const dim3 grid((p.L3 + kJ1Threads - 1) / kJ1Threads, p.n_rep);
   const dim3 sgrid((p.L3 + kJ1Threads - 1) / kJ1Threads, 4, p.n_rep);
-#define PYRO_J1_CASE(B)                                                          \
-  case B:                                                                        \
-    if (site_per_thread) {                                                       \
-      if (metro) j1_site_pass_kernel<B, true><<<sgrid, kJ1Threads, 0, st>>>(p);  \
-      else j1_site_pass_kernel<B, false><<<sgrid, kJ1Threads, 0, st>>>(p);       \
-    } else {                                                                     \
-      if (metro) j1_pass_kernel<B, true><<<grid, kJ1Threads, 0, st>>>(p);        \
-      else j1_pass_kernel<B, false><<<grid, kJ1Threads, 0, st>>>(p);             \
-    }                                                                            \
+#define PYRO_J1_CASE(B, X)                                                            \
+  case B:                                                                             \
+    if (site_per_thread) {                                                            \
+      if (metro) j1_site_pass_kernel<B, true, X><<<sgrid, kJ1Threads, 0, st>>>(p);    \
+      else j1_site_pass_kernel<B, false, X><<<sgrid, kJ1Threads, 0, st>>>(p);         \
+    } else {                                                                          \
+      if (metro) j1_pass_kernel<B, true, X><<<grid, kJ1Threads, 0, st>>>(p);          \
+      else j1_pass_kernel<B, false, X><<<grid, kJ1Threads, 0, st>>>(p);               \
+    }                                                                                 \
     break;
-  switch (colour) {
-    PYRO_J1_CASE(0)
-    PYRO_J1_CASE(1)
-    PYRO_J1_CASE(2)
-    PYRO_J1_CASE(3)
-    default:
-      break;
+  if (p.exch) {
+    switch (colour) {
+      PYRO_J1_CASE(0, true)
+      PYRO_J1_CASE(1, true)
+      PYRO_J1_CASE(2, true)
+      PYRO_J1_CASE(3, true)
+      default:
+        break;
+    }
+  } else {
+    switch (colour) {
+      PYRO_J1_CASE(0, false)
+      PYRO_J1_CASE(1, false)
+      PYRO_J1_CASE(2, false)
+      PYRO_J1_CASE(3, false)
+      default:
+        break;
+    }
   }
 #undef PYRO_J1_CASE
 }

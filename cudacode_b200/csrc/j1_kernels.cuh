@@ -25,6 +25,13 @@ struct J1PassParams {
   unsigned long long sweep_off;
   uint32_t seed_lo, seed_hi;
   int renorm_every;
+  // Bond matrices and Zeeman field of an anisotropic system (exch != 0):
+  // xa[b][slot] = A[b][b'] for the three other sublattices b' in increasing
+  // order, xf[b] = f[b]. Kernel parameters, so the update's multiply-adds
+  // read them from the constant bank.
+  int exch;
+  float xa[4][3][9];
+  float xf[4][3];
 };
 
 // FP64 energy (by tetrahedra) and magnetisation partials of one J1 system;

@@ -232,3 +232,51 @@ def test_exchange_arguments_and_state(tmp_path):
     e3 = Engine([sysd], seed=1)  # isotropic: the checkpoint does not fit
     with pytest.raises(PyroError):
         e3.load_checkpoint(path)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("options", [
+    {"J1_KERNEL": 0},                       # generic colour-pass kernel
+    {"J1_SITE_MODE": 0},                    # cell per thread, both sweeps
+    {"J1_SITE_MODE": 3},                    # site per thread, both sweeps
+    {"REPLICA_GROUP": 2, "CHAINS": 2},      # L2-resident groups on two graph branches
+    {"CYCLE_KERNEL": 1},                    # isotropic-only kernel: falls back to per-pass
+])
+def test_kernel_variants_agree_with_the_oracle(options):
+    temps = geometric_ladder(0.1, 1.2, 6)
+    systems = [System(L=10, temperatures=temps, J1=0.0), System(L=9, temperatures=temps, J1=1.0)]
+    e, o = pair(systems, seed=21)
+    set_both(e, o, reference_exchange(0.4, -0.3, 0.2, 0.35),
+             10.0 * reference_field(2.4, 0.3, [0.0, 0.0, 1.0]), 0)
+    for name, value in options.items():
+        e.set_option(getattr(Engine, "OPT_" + name), value)
+    e.init_random()
+    o.init_random()
+    e.cycle(1, 3, True, 3)
+    o.cycle(1, 3, True, 3)
+    for s in (0, 1):
+        np.testing.assert_array_equal(e.get_spins(s), o.get_spins(s))
+    np.testing.assert_allclose(e.observables(0)[0], o.observables(0)[0], rtol=1e-12)
+
+
+@pytest.mark.gpu
+def test_autotuned_schedule_agrees_with_the_oracle():
+    temps = geometric_ladder(0.1, 1.2, 8)
+    sysd = System(L=12, temperatures=temps, J1=0.0)
+    A, f = reference_exchange(*DEFAULTS), reference_field(1.0, 1.0, [0.0, 0.0, 2.0])
+    tuner = Engine([sysd], seed=4)
+    tuner.set_exchange(A, f)
+    tuner.init_random()
+    tuner.autotune(1, 4, 1)
+    names = ["J1_KERNEL", "CYCLE_KERNEL", "CLUSTER_SIZE", "J1_SITE_MODE", "REPLICA_GROUP",
+             "CHAINS", "GROUP_MB", "FAR_KERNEL"]
+    chosen = {n: tuner.get_option(getattr(Engine, "OPT_" + n)) for n in names}
+    e, o = pair([sysd], seed=4)
+    set_both(e, o, A, f)
+    for n, v in chosen.items():
+        e.set_option(getattr(Engine, "OPT_" + n), v)
+    e.init_random()
+    o.init_random()
+    e.cycle(1, 4, True, 4)
+    o.cycle(1, 4, True, 4)
+    np.testing.assert_array_equal(e.get_spins(), o.get_spins())
