@@ -123,6 +123,10 @@ struct pyro_ctx {
   size_t sq_s1 = 0, sq_s2 = 0, sq_s3 = 0, sq_tw = 0, sq_out = 0;
 
   pyro::TetState* tet = nullptr;
+
+  // Per-sublattice magnetisation partials, grown on demand (exchange.cu).
+  double* d_submag = nullptr;
+  size_t submag_cap = 0;
 };
 
 namespace pyro {

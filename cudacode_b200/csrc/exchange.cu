@@ -64,6 +64,69 @@ void bond_matrix(int a, int b, double J1, double J2, double J3, double J4, doubl
   C[0][2] -= D[1];
 }
 
+constexpr int kMagThreads = 256;
+constexpr int kMagSitesPerThread = 8;
+
+// FP64 sum of the spins of one site plane (one cubic-cell site s, so one
+// sublattice s & 3) of one replica over a chunk of cells: block (chunk, s,
+// replica) -> partials[((rep * 16 + s) * chunks + chunk) * 3 + k].
+__global__ void __launch_bounds__(kMagThreads) plane_sum_kernel(const float4* __restrict__ spins,
+                                                                int L3, int chunks,
+                                                                double* partials) {
+  const int chunk = blockIdx.x, s = blockIdx.y, rep = blockIdx.z;
+  const float4* plane = spins + ((long long)rep * 16 + s) * L3;
+  double x = 0.0, y = 0.0, z = 0.0;
+  for (int k = 0; k < kMagSitesPerThread; ++k) {
+    const int c = (chunk * kMagSitesPerThread + k) * kMagThreads + threadIdx.x;
+    if (c < L3) {
+      const float4 v = __ldg(plane + c);
+      x += v.x;
+      y += v.y;
+      z += v.z;
+    }
+  }
+  __shared__ double red[3][kMagThreads / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    x += __shfl_down_sync(0xffffffffu, x, o);
+    y += __shfl_down_sync(0xffffffffu, y, o);
+    z += __shfl_down_sync(0xffffffffu, z, o);
+  }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    red[0][w] = x;
+    red[1][w] = y;
+    red[2][w] = z;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int q = 0; q < kMagThreads / 32; ++q) {
+      sx += red[0][q];
+      sy += red[1][q];
+      sz += red[2][q];
+    }
+    double* o = partials + (((long long)rep * 16 + s) * chunks + chunk) * 3;
+    o[0] = sx;
+    o[1] = sy;
+    o[2] = sz;
+  }
+}
+
+// out[(rep * 4 + b) * 3 + k]: planes b, 4 + b, 8 + b, 12 + b and their chunks
+// in a fixed order (deterministic).
+__global__ void sublattice_finalise_kernel(const double* __restrict__ partials, int n_rep,
+                                           int chunks, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;  // (rep, b, k)
+  if (i >= n_rep * 12) return;
+  const int rep = i / 12, b = (i / 3) % 4, k = i % 3;
+  double v = 0.0;
+  for (int f = 0; f < 4; ++f)
+    for (int c = 0; c < chunks; ++c)
+      v += partials[(((long long)rep * 16 + 4 * f + b) * chunks + c) * 3 + k];
+  out[i] = v;
+}
+
 bool finite_all(const double* v, int n) {
   for (int q = 0; q < n; ++q)
     if (!std::isfinite(v[q])) return false;
@@ -165,6 +228,51 @@ int pyro_set_exchange(pyro_ctx* ctx, int system, const double* exchange144,
   PYRO_CK(cudaMemcpy(ctx->d_sys, ctx->sys.data(), sizeof(SysDev) * ctx->sys.size(),
                      cudaMemcpyHostToDevice));
   return rebuild_schedule(ctx);
+}
+
+int pyro_reference_gtensor(double gxy, double gz, double* g36) {
+  if (!g36) return PYRO_ERR_ARG;
+  for (int b = 0; b < 4; ++b) {
+    double z[3];
+    for (int q = 0; q < 3; ++q) z[q] = (kBasis[b][q] - 0.5) / std::sqrt(0.75);
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c)
+        g36[9 * b + 3 * r + c] = (r == c ? gxy : 0.0) + (gz - gxy) * z[r] * z[c];
+  }
+  return PYRO_OK;
+}
+
+int pyro_sublattice_magnetisation(pyro_ctx* ctx, int system, double* out) {
+  if (!ctx || !out) return PYRO_ERR_ARG;
+  if (system < 0 || system >= (int)ctx->sys.size())
+    return fail(ctx, PYRO_ERR_ARG, "sublattice_magnetisation: no such system");
+  const SysDev& s = ctx->sys[system];
+  const int chunks = (s.L3 + kMagThreads * kMagSitesPerThread - 1) / (kMagThreads * kMagSitesPerThread);
+  const size_t need = (size_t)s.n_rep * 16 * chunks * 3 + (size_t)s.n_rep * 12;
+  PYRO_CK(cudaSetDevice(ctx->device));
+  if (need > ctx->submag_cap || !ctx->d_submag) {
+    if (ctx->d_submag) PYRO_CK(cudaFree(ctx->d_submag));
+    ctx->d_submag = nullptr;
+    ctx->submag_cap = 0;
+    const cudaError_t e = cudaMalloc((void**)&ctx->d_submag, sizeof(double) * need);
+    if (e != cudaSuccess)
+      return fail(ctx, e == cudaErrorMemoryAllocation ? PYRO_ERR_NOMEM : PYRO_ERR_CUDA,
+                  std::string("sublattice_magnetisation scratch: ") + cudaGetErrorString(e));
+    ctx->submag_cap = need;
+  }
+  double* partials = ctx->d_submag;
+  double* d_out = ctx->d_submag + (size_t)s.n_rep * 16 * chunks * 3;
+  plane_sum_kernel<<<dim3(chunks, 16, s.n_rep), kMagThreads, 0, ctx->stream>>>(
+      ctx->d_spins + s.spin_off, s.L3, chunks, partials);
+  PYRO_CK_LAUNCH();
+  sublattice_finalise_kernel<<<(s.n_rep * 12 + 127) / 128, 128, 0, ctx->stream>>>(partials, s.n_rep,
+                                                                                chunks, d_out);
+  PYRO_CK_LAUNCH();
+  ctx->launches += 2;
+  PYRO_CK(cudaMemcpyAsync(out, d_out, sizeof(double) * 12 * s.n_rep, cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  return PYRO_OK;
 }
 
 int pyro_get_exchange(pyro_ctx* ctx, int system, double* exchange144, double* field12,

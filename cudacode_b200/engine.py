@@ -135,6 +135,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "pyro_get_exchange": (i, [P, i, pd, pd, pi]),
         "pyro_reference_exchange": (i, [d, d, d, d, pd]),
         "pyro_reference_field": (i, [d, d, pd, pd]),
+        "pyro_reference_gtensor": (i, [d, d, pd]),
+        "pyro_sublattice_magnetisation": (i, [P, i, pd]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -201,6 +203,15 @@ def reference_field(gxy: float, gz: float, B) -> np.ndarray:
     if rc != PYRO_OK:
         raise PyroError(rc, "pyro_reference_field")
     return out.reshape(4, 3)
+
+
+def reference_gtensor(gxy: float, gz: float) -> np.ndarray:
+    """g-tensors (4, 3, 3) of the four sublattices."""
+    out = np.empty(36, dtype=np.float64)
+    rc = load_library().pyro_reference_gtensor(gxy, gz, _ptr(out, C.c_double))
+    if rc != PYRO_OK:
+        raise PyroError(rc, "pyro_reference_gtensor")
+    return out.reshape(4, 3, 3)
 
 
 def geometric_ladder(t_min: float, t_max: float, n: int) -> list[float]:
@@ -366,6 +377,12 @@ class Engine:
         self._ck(self.lib.pyro_get_exchange(self.ctx, system, _ptr(a, C.c_double),
                                             _ptr(f, C.c_double), C.byref(is_set)))
         return (a.reshape(4, 4, 3, 3), f.reshape(4, 3)) if is_set.value else None
+
+    def sublattice_magnetisation(self, system: int = 0) -> np.ndarray:
+        """(replicas, 4, 3) FP64 magnetisation of each sublattice, replica order."""
+        out = np.empty(self.systems[system].replicas() * 12, dtype=np.float64)
+        self._ck(self.lib.pyro_sublattice_magnetisation(self.ctx, system, _ptr(out, C.c_double)))
+        return out.reshape(-1, 4, 3)
 
     # -- cone -------------------------------------------------------------
     def set_cone(self, cosmax, system: int = 0) -> None:

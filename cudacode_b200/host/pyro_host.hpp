@@ -123,6 +123,33 @@ inline void CalculateSolidAngle(Device& d, int OverRelaxation, double ratio,
   d.check(pyro_get_cone(d.ctx(), 0, CosThetaSolid.data()));
 }
 
+// InitializeCouplings3D(nt, nspc, ..., MagneticField, B, device)
+// (Pyrochlore.cu:643-711) for the reference's anisotropic model: the bond
+// matrices of J1..J4 (couplings_const, Pyrochlore.cu:169-184) and, with
+// MagneticField, the site fields of B (tesla) through the g-tensors of gxy,
+// gz (InitializeMagneticField, Pyrochlore.cu:414-450). Energies and
+// temperatures are then in the reference's units.
+inline void InitializeCouplings3D(Device& d, double J1, double J2, double J3, double J4,
+                                  int MagneticField, const double* B, double gxy, double gz) {
+  std::vector<double> A(144), f(12, 0.0);
+  d.check(pyro_reference_exchange(J1, J2, J3, J4, A.data()));
+  if (MagneticField) d.check(pyro_reference_field(gxy, gz, B, f.data()));
+  d.check(pyro_set_exchange(d.ctx(), 0, A.data(), MagneticField ? f.data() : nullptr));
+}
+
+// Magnetization with the g-tensor (MagnetizationGPU, Pyrochlore.cu:277-342):
+// sum_b g_b m_b of every configuration slot, 3 per replica.
+inline void MagnetizationG(Device& d, double gxy, double gz, std::vector<double>& M) {
+  std::vector<double> g(36), m(12 * d.replicas());
+  d.check(pyro_reference_gtensor(gxy, gz, g.data()));
+  d.check(pyro_sublattice_magnetisation(d.ctx(), 0, m.data()));
+  M.assign(3 * d.replicas(), 0.0);
+  for (int r = 0; r < d.replicas(); ++r)
+    for (int b = 0; b < 4; ++b)
+      for (int i = 0; i < 3; ++i)
+        for (int k = 0; k < 3; ++k) M[3 * r + i] += g[9 * b + 3 * i + k] * m[(4 * r + b) * 3 + k];
+}
+
 // Geometric ("log scale") or linear ladder between tmin and tmax
 // (the reference's SetupLog/LinearTemperatures, whose source is absent).
 inline std::vector<double> Ladder(double tmin, double tmax, int n, bool log_scale) {

@@ -254,6 +254,15 @@ int pyro_get_exchange(pyro_ctx* ctx, int system, double* exchange144, double* fi
  * meV/T (InitializeMagneticField, Pyrochlore.cu:414-450). */
 int pyro_reference_exchange(double J1, double J2, double J3, double J4, double* exchange144);
 int pyro_reference_field(double gxy, double gz, const double* B3, double* field12);
+/* The reference's g-tensors g_b = gxy I + (gz - gxy) z_b z_b^T of the four
+ * sublattices, g36[9 b + 3 r + c] (MagnetizationGPU, Pyrochlore.cu:277-342,
+ * InitializeMagneticField 414-450). */
+int pyro_reference_gtensor(double gxy, double gz, double* g36);
+/* FP64 magnetisation of each sublattice of every replica held (replica
+ * order), out[(r * 4 + b) * 3 + k] = sum of S^k over the sites of
+ * sublattice b; the reference's g-weighted moment of MagnetizationGPU
+ * (Pyrochlore.cu:277-342) is sum_b g_b m_b. Synchronous. */
+int pyro_sublattice_magnetisation(pyro_ctx* ctx, int system, double* out);
 
 /* Static structure factor S(q) = (1/N) sum_a |sum_i S_i^a e^{-i q.r_i}|^2,
  * averaged over the replicas held, on a grid of G^3 wave vectors

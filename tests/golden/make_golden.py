@@ -52,6 +52,17 @@ def parse_couplings(text):
     return C
 
 
+def magnetization_gtensors(gxy, gz):
+    """The g1..g4 matrices of MagnetizationGPU (Pyrochlore.cu:283-286), with
+    _g1, _g2 set as in InitializeCouplings3D (Pyrochlore.cu:697-701)."""
+    g1 = (2.0 * gxy + gz) / 3.0
+    g2 = (gz - gxy) / 3.0
+    return [[[g1, g2, g2], [g2, g1, g2], [g2, g2, g1]],
+            [[g1, g2, -g2], [g2, g1, -g2], [-g2, -g2, g1]],
+            [[g1, -g2, -g2], [-g2, g1, g2], [-g2, g2, g1]],
+            [[g1, -g2, g2], [-g2, g1, -g2], [g2, -g2, g1]]]
+
+
 def initialize_magnetic_field(B, gxy, gz):
     """Pyrochlore.cu:414-450 (without its printf)."""
     g1 = (2.0 * gxy + gz) / 3.0
@@ -128,7 +139,8 @@ def main():
     for gxy, gz, B in ((1.0, 1.0, (0.0, 0.0, 1.0)), (2.4, 0.3, (0.7, -0.2, 1.5)),
                        (0.5, 3.0, (-1.0, 2.0, 0.25))):
         fields.append({"gxy": gxy, "gz": gz, "B": list(B),
-                       "field_on_site": initialize_magnetic_field(B, gxy, gz)})
+                       "field_on_site": initialize_magnetic_field(B, gxy, gz),
+                       "magnetization_g": magnetization_gtensors(gxy, gz)})
     acases = []
     rng = np.random.default_rng(20240612)
     defaults = (-0.09 / 0.29, -0.22 / 0.29, -1.00, 0.0)  # Pyrochlore.cu:138-141

@@ -280,3 +280,26 @@ def test_autotuned_schedule_agrees_with_the_oracle():
     e.cycle(1, 4, True, 4)
     o.cycle(1, 4, True, 4)
     np.testing.assert_array_equal(e.get_spins(), o.get_spins())
+
+
+def test_reference_gtensor_matches_magnetization_gpu():
+    from cudacode_b200.engine import reference_gtensor
+    for c in GOLDEN["fields"]:
+        np.testing.assert_allclose(reference_gtensor(c["gxy"], c["gz"]),
+                                   np.array(c["magnetization_g"]), rtol=1e-14, atol=1e-15)
+
+
+@pytest.mark.gpu
+def test_sublattice_magnetisation_matches_the_spins():
+    temps = geometric_ladder(0.2, 1.0, 3)
+    e = Engine([System(L=5, temperatures=temps), System(L=4, temperatures=temps, J1=0.0)], seed=3)
+    e.set_exchange(reference_exchange(*DEFAULTS), system=1)
+    e.init_random()
+    e.cycle(1, 1, True, 2)
+    for s in (0, 1):
+        got = e.sublattice_magnetisation(s)
+        sp = e.get_spins(s)[..., :3].astype(np.float64)  # (R, 16, L^3, 3)
+        want = np.stack([sp[:, b::4].sum(axis=(1, 2)) for b in range(4)], axis=1)
+        np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-9)
+        _, M = e.observables(s)
+        np.testing.assert_allclose(got.sum(axis=1), M.reshape(-1, 3), rtol=1e-12, atol=1e-9)

@@ -25,7 +25,7 @@ def test_cli_matches_python_engine(tmp_path):
     args = ["--nx", "4", "--NumberOfTemperatures", "6", "--TMin", "0.1", "--TMax", "1.5",
             "--LogScale", "--OverRelaxation", "3", "--McStepsParallelTempering", "1",
             "--ThermalizationSteps", "20", "--NumberOfMeasures", "15", "--Rng", "777",
-            "--Output", str(out)]
+            "--Heisenberg", "1", "--Output", str(out)]
     r = subprocess.run([CLI] + args, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     got = np.loadtxt(out)[:, 1:]
@@ -42,3 +42,40 @@ def test_cli_matches_python_engine(tmp_path):
         perm = e.permutation()
         want.append(E[perm] / (16 * 64))
     np.testing.assert_allclose(got, np.array(want), rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.gpu
+def test_cli_anisotropic_model_matches_python_engine(tmp_path):
+    from cudacode_b200.engine import (Engine, System, geometric_ladder, reference_exchange,
+                                      reference_field, reference_gtensor)
+
+    out = tmp_path / "E.dat"
+    J = (-0.09 / 0.29, -0.22 / 0.29, -1.00, 0.0)  # the reference's defaults
+    args = ["--nx", "3", "--NumberOfTemperatures", "4", "--TMin", "0.1", "--TMax", "2.0",
+            "--LogScale", "--OverRelaxation", "2", "--ThermalizationSteps", "10",
+            "--NumberOfMeasures", "8", "--Rng", "99", "--MagneticField", "--Bx", "0",
+            "--Bz", "2", "--gxy", "2.4", "--gz", "0.3", "--Magnetization", "--Output", str(out)]
+    r = subprocess.run([CLI] + args, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    got_e = np.loadtxt(out)[:, 1:]
+    got_m = np.loadtxt(str(out) + ".magnetization")[:, 1:]
+    temps = geometric_ladder(0.1, 2.0, 4)
+    e = Engine([System(L=3, temperatures=temps, J1=0.0)], seed=99, renorm_every=100)
+    e.set_exchange(reference_exchange(*J), reference_field(2.4, 0.3, [0.0, 0.0, 2.0]))
+    e.init_random()
+    e.tune_cone(0.5, 50, 10, 2)
+    for _ in range(10):
+        e.cycle(1, 2, True, 1)
+    g = reference_gtensor(2.4, 0.3)
+    N = 16 * 27
+    want_e, want_m = [], []
+    for _ in range(8):
+        e.cycle(1, 2, True, 1)
+        E, _ = e.observables()
+        perm = e.permutation()
+        sub = e.sublattice_magnetisation()  # (R, 4, 3)
+        Mg = np.einsum("bik,rbk->ri", g, sub)
+        want_e.append(E[perm] / N)
+        want_m.append((Mg[perm] / N).ravel())
+    np.testing.assert_allclose(got_e, np.array(want_e), rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(got_m, np.array(want_m), rtol=1e-9, atol=1e-12)
