@@ -381,7 +381,7 @@ void free_all(pyro_ctx* c) {
                   c->d_obs_segs,    c->d_partials,     c->d_sweep,       c->d_scratch_u64,
                   c->d_history,     c->d_history_count, c->d_obs_generic,
                   c->d_sq_s1,       c->d_sq_s2,        c->d_sq_s3,       c->d_sq_tw,
-                  c->d_sq_out,      c->d_exch,         c->d_submag};
+                  c->d_sq_out,      c->d_exch,         c->d_submag,      c->d_order};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto* p : c->d_pass_segs)

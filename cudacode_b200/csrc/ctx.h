@@ -127,6 +127,9 @@ struct pyro_ctx {
   // Per-sublattice magnetisation partials, grown on demand (exchange.cu).
   double* d_submag = nullptr;
   size_t submag_cap = 0;
+  // Order-parameter scratch, grown on demand (order.cu), bytes.
+  void* d_order = nullptr;
+  size_t order_cap = 0;
 };
 
 namespace pyro {

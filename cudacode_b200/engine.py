@@ -137,6 +137,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "pyro_reference_field": (i, [d, d, pd, pd]),
         "pyro_reference_gtensor": (i, [d, d, pd]),
         "pyro_sublattice_magnetisation": (i, [P, i, pd]),
+        "pyro_order_parameters": (i, [P, i, pd]),
+        "pyro_ising_configuration": (i, [P, i, i, pi]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -383,6 +385,20 @@ class Engine:
         out = np.empty(self.systems[system].replicas() * 12, dtype=np.float64)
         self._ck(self.lib.pyro_sublattice_magnetisation(self.ctx, system, _ptr(out, C.c_double)))
         return out.reshape(-1, 4, 3)
+
+    def order_parameters(self, system: int = 0) -> np.ndarray:
+        """(replicas, 20) FP64 order parameters, replica order: 12 irrep
+        components, 6 quadrupole sums, monopole density, |Sz| sum."""
+        out = np.empty(self.systems[system].replicas() * 20, dtype=np.float64)
+        self._ck(self.lib.pyro_order_parameters(self.ctx, system, _ptr(out, C.c_double)))
+        return out.reshape(-1, 20)
+
+    def ising_configuration(self, replica: int, system: int = 0) -> np.ndarray:
+        """(L^3,) int32 masks: bit 4 t + b set where a_b . S < 0."""
+        out = np.empty(self.systems[system].L ** 3, dtype=np.int32)
+        self._ck(self.lib.pyro_ising_configuration(self.ctx, system, replica,
+                                                   _ptr(out, C.c_int)))
+        return out
 
     # -- cone -------------------------------------------------------------
     def set_cone(self, cosmax, system: int = 0) -> None:

@@ -264,6 +264,23 @@ int pyro_reference_gtensor(double gxy, double gz, double* g36);
  * (Pyrochlore.cu:277-342) is sum_b g_b m_b. Synchronous. */
 int pyro_sublattice_magnetisation(pyro_ctx* ctx, int system, double* out);
 
+/* Order parameters of every replica held (replica order), FP64 sums over
+ * the lattice, out[r * 20 + q]:
+ *   q = 0..11  irrep components of Measurement (Pyrochlore.cu:526-641):
+ *              A2, E (2), T (3), uniform magnetisation (3), T' (3);
+ *   q = 12..17 quadrupole sum (S^a S^b - delta_ab/3), ab = xx xy xz yy yz zz
+ *              (_CudaQuadrupolarOrder, Math.cu:335-372);
+ *   q = 18     monopole density, sum over cells of 1/4 sum over its four
+ *              up-tetrahedra of |sum_b a_b . S| (CudaCalculateMonopoleSquare,
+ *              Math.cu:386-476);
+ *   q = 19     sum |a_b . S| / sqrt 3 (CudaCalculateAbsSz, Math.cu:478-510);
+ * a_b = (1,1,1), (-1,-1,1), (1,-1,-1), (-1,1,-1). Synchronous. */
+int pyro_order_parameters(pyro_ctx* ctx, int system, double* out);
+/* Ising projection of one replica (CudaCalculateIsingConf, Math.cu:513-541):
+ * out[cell] (L^3 ints) has bit 4 t + b set where a_b . S < 0 for the site
+ * 4 t + b of the cell. Synchronous. */
+int pyro_ising_configuration(pyro_ctx* ctx, int system, int replica, int* out);
+
 /* Static structure factor S(q) = (1/N) sum_a |sum_i S_i^a e^{-i q.r_i}|^2,
  * averaged over the replicas held, on a grid of G^3 wave vectors
  * q = (2 pi / L) * stride * (h, k, l), h, k, l in [-G/2, G/2); out[(h' G + k') G + l'].

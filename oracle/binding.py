@@ -38,6 +38,8 @@ def load() -> C.CDLL:
         "orc_overrelax_sweep": (None, [P, i]),
         "orc_set_cone": (None, [P, i, pf]),
         "orc_set_exchange": (None, [P, i, pd, pd]),
+        "orc_order_parameters": (None, [P, i, pd]),
+        "orc_ising_configuration": (None, [P, i, i, pi]),
         "orc_get_cone": (None, [P, i, pf]),
         "orc_get_acceptance": (None, [P, i, pu64, pu64]),
         "orc_reset_acceptance": (None, [P]),
@@ -144,6 +146,16 @@ class Oracle:
         f = None if field is None else np.ascontiguousarray(field, dtype=np.float64).reshape(12)
         self.lib.orc_set_exchange(self.h, system, _p(a, C.c_double),
                                   None if f is None else _p(f, C.c_double))
+
+    def order_parameters(self, system=0):
+        out = np.zeros((self.systems[system].replicas(), 20))
+        self.lib.orc_order_parameters(self.h, system, _p(out, C.c_double))
+        return out
+
+    def ising_configuration(self, replica, system=0):
+        out = np.zeros(self.systems[system].L ** 3, dtype=np.int32)
+        self.lib.orc_ising_configuration(self.h, system, replica, _p(out, C.c_int))
+        return out
 
     def set_cone(self, c, system=0):
         a = np.ascontiguousarray(c, dtype=np.float32)

@@ -559,6 +559,95 @@ void orc_overrelax_sweep(void* p, int n) {
   for (int i = 0; i < n; ++i) sweep_one(*(Oracle*)p, false);
 }
 
+// Order parameters of every replica of one system (FP64 sums over the
+// lattice, 20 per replica): the irrep components of Measurement
+// (Pyrochlore.cu:526-641) from the sublattice magnetisations, the quadrupole
+// sums (_CudaQuadrupolarOrder, Math.cu:335-372), the monopole density
+// (CudaCalculateMonopoleSquare, Math.cu:386-476) and sum |a_b . S| / sqrt 3
+// (CudaCalculateAbsSz, Math.cu:478-510), a_b the reference's sublattice axes.
+void orc_order_parameters(void* p, int si, double* out) {
+  const Oracle& o = *(Oracle*)p;
+  const Sys& S = o.sys[si];
+  static const int ax[4][3] = {{1, 1, 1}, {-1, -1, 1}, {1, -1, -1}, {-1, 1, -1}};
+  // irrep rows as coefficient vectors per sublattice, and their normalisation
+  static const int irrep[12][4][3] = {
+      {{1, 1, 1}, {-1, -1, 1}, {1, -1, -1}, {-1, 1, -1}},
+      {{-2, 1, 1}, {2, -1, 1}, {-2, -1, -1}, {2, 1, -1}},
+      {{0, -1, 1}, {0, 1, 1}, {0, 1, -1}, {0, -1, -1}},
+      {{0, -1, 1}, {0, -1, -1}, {0, 1, -1}, {0, 1, 1}},
+      {{1, 0, -1}, {1, 0, 1}, {-1, 0, -1}, {-1, 0, 1}},
+      {{-1, 1, 0}, {1, -1, 0}, {1, 1, 0}, {-1, -1, 0}},
+      {{1, 0, 0}, {1, 0, 0}, {1, 0, 0}, {1, 0, 0}},
+      {{0, 1, 0}, {0, 1, 0}, {0, 1, 0}, {0, 1, 0}},
+      {{0, 0, 1}, {0, 0, 1}, {0, 0, 1}, {0, 0, 1}},
+      {{0, -1, -1}, {0, -1, 1}, {0, 1, 1}, {0, 1, -1}},
+      {{-1, 0, -1}, {-1, 0, 1}, {1, 0, -1}, {1, 0, 1}},
+      {{-1, -1, 0}, {1, 1, 0}, {1, -1, 0}, {-1, 1, 0}}};
+  for (int r = 0; r < S.R; ++r) {
+    const size_t base = S.spin_off + (size_t)r * 16 * S.L3;
+    double M[4][3] = {}, Q[6] = {}, mono = 0.0, absz = 0.0;
+    for (int cell = 0; cell < S.L3; ++cell) {
+      double cell_mono = 0.0;
+      for (int t = 0; t < 4; ++t) {
+        double charge = 0.0;
+        for (int b = 0; b < 4; ++b) {
+          const size_t i = base + (size_t)(4 * t + b) * S.L3 + cell;
+          const double x = o.fp64 ? o.s64[4 * i] : o.s32[4 * i];
+          const double y = o.fp64 ? o.s64[4 * i + 1] : o.s32[4 * i + 1];
+          const double z = o.fp64 ? o.s64[4 * i + 2] : o.s32[4 * i + 2];
+          M[b][0] += x;
+          M[b][1] += y;
+          M[b][2] += z;
+          Q[0] += x * x - 1.0 / 3.0;
+          Q[1] += x * y;
+          Q[2] += x * z;
+          Q[3] += y * y - 1.0 / 3.0;
+          Q[4] += y * z;
+          Q[5] += z * z - 1.0 / 3.0;
+          const double pr = x * ax[b][0] + y * ax[b][1] + z * ax[b][2];
+          charge += pr;
+          absz += std::fabs(pr);
+        }
+        cell_mono += std::fabs(charge);
+      }
+      mono += 0.25 * cell_mono;
+    }
+    double* q = out + 20 * (size_t)r;
+    for (int m = 0; m < 12; ++m) {
+      const double norm = m == 0 ? 1.0 / std::sqrt(3.0)
+                          : m == 1 ? 1.0 / std::sqrt(6.0)
+                          : (m >= 6 && m <= 8) ? 1.0 : 1.0 / std::sqrt(2.0);
+      double v = 0.0;
+      for (int b = 0; b < 4; ++b)
+        for (int k = 0; k < 3; ++k) v += irrep[m][b][k] * M[b][k];
+      q[m] = norm * v;
+    }
+    for (int k = 0; k < 6; ++k) q[12 + k] = Q[k];
+    q[18] = mono;
+    q[19] = absz / std::sqrt(3.0);
+  }
+}
+
+// Ising projection (CudaCalculateIsingConf, Math.cu:513-541): per cell, bit
+// 4 t + b set where a_b . S < 0.
+void orc_ising_configuration(void* p, int si, int r, int* out) {
+  const Oracle& o = *(Oracle*)p;
+  const Sys& S = o.sys[si];
+  static const int ax[4][3] = {{1, 1, 1}, {-1, -1, 1}, {1, -1, -1}, {-1, 1, -1}};
+  const size_t base = S.spin_off + (size_t)r * 16 * S.L3;
+  for (int cell = 0; cell < S.L3; ++cell) {
+    int mask = 0;
+    for (int s = 0; s < 16; ++s) {
+      const size_t i = base + (size_t)s * S.L3 + cell;
+      const double x = o.fp64 ? o.s64[4 * i] : o.s32[4 * i];
+      const double y = o.fp64 ? o.s64[4 * i + 1] : o.s32[4 * i + 1];
+      const double z = o.fp64 ? o.s64[4 * i + 2] : o.s32[4 * i + 2];
+      if (x * ax[s & 3][0] + y * ax[s & 3][1] + z * ax[s & 3][2] < 0.0) mask |= 1 << s;
+    }
+    out[cell] = mask;
+  }
+}
+
 // Bond matrices A[16][9] (row-major per sublattice pair) and site fields
 // f[4][3] (null: none) of one system; A = null returns it to isotropic J1.
 void orc_set_exchange(void* p, int si, const double* A144, const double* f12) {

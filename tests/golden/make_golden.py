@@ -19,6 +19,13 @@ and its one CPU routine:
   (gxy, gz, B); and ``TotalEnergy`` of seeded configurations with the
   reference's default couplings (Pyrochlore.cu:138-141), a J4 case and a field
   (FieldOnSite = the fields above).
+* ``reference_order.json``: order parameters of seeded configurations, summed
+  over cells as the reference's reductions do: the irrep components of
+  ``Measurement`` (Pyrochlore.cu:526-641, its expressions evaluated from the
+  source text), the quadrupole of ``_CudaQuadrupolarOrder`` (Math.cu:335-372),
+  the monopole density of ``CudaCalculateMonopoleSquare`` (Math.cu:386-476),
+  ``CudaCalculateAbsSz`` (Math.cu:478-510) and the per-cell masks of
+  ``CudaCalculateIsingConf`` (Math.cu:513-541).
 
 Run from the repository root, in a checkout that has the reference at
 /root/reference:  python tests/golden/make_golden.py
@@ -61,6 +68,68 @@ def magnetization_gtensors(gxy, gz):
             [[g1, g2, -g2], [g2, g1, -g2], [-g2, -g2, g1]],
             [[g1, -g2, -g2], [-g2, g1, g2], [-g2, g2, g1]],
             [[g1, -g2, g2], [-g2, g1, -g2], [g2, -g2, g1]]]
+
+
+def parse_measurement(text):
+    """The per-cell irrep expressions of Measurement (Pyrochlore.cu:526-641),
+    taken from the source text; returns f(s0, s1, s2, s3) -> 12 values in the
+    order the kernel stores them."""
+    from types import SimpleNamespace as NS
+    body = text[text.index("GLOBAL void Measurement"):]
+    body = body[body.index("mm1="):body.index("TYPE *Order =")]
+    stmts = [" ".join(st.split()) for st in body.split(";") if st.strip()]
+
+    def f(s0, s1, s2, s3):
+        env = {"s0": s0, "s1": s1, "s2": s2, "s3": s3, "mm1": 0.0,
+               "mm2": NS(x=0.0, y=0.0), "mm3": NS(x=0.0, y=0.0, z=0.0),
+               "mm4": NS(x=0.0, y=0.0, z=0.0), "mm5": NS(x=0.0, y=0.0, z=0.0)}
+        for st in stmts:
+            exec(st, {}, env)
+        m2, m3, m4, m5 = env["mm2"], env["mm3"], env["mm4"], env["mm5"]
+        return [env["mm1"], m2.x, m2.y, m3.x, m3.y, m3.z, m4.x, m4.y, m4.z, m5.x, m5.y, m5.z]
+
+    return f
+
+
+def order_parameters(v, n, measurement):
+    """Sums over cells of Measurement, the quadrupole, monopole and |Sz|
+    kernels (Math.cu:335-510), and the Ising masks (Math.cu:513-541), of one
+    configuration v (plane-major, 16 n^3 x 3)."""
+    from types import SimpleNamespace as NS
+    sz = [[1, 1, 1], [-1, -1, 1], [1, -1, -1], [-1, 1, -1]]
+    nc = n ** 3
+    tot = np.zeros(20)
+    ising = []
+    for cell in range(nc):
+        sub = []
+        for b in range(4):
+            s = v[[cell + (4 * k + b) * nc for k in range(4)]].sum(axis=0)
+            sub.append(NS(x=s[0], y=s[1], z=s[2]))
+        tot[:12] += measurement(*sub)
+        q = [0.0] * 6
+        for s in range(16):
+            x, y, z = v[cell + s * nc]
+            q[0] += x * x - 0.333333333333333333333
+            q[1] += x * y
+            q[2] += x * z
+            q[3] += y * y - 0.333333333333333333333
+            q[4] += y * z
+            q[5] += z * z - 0.333333333333333333333
+        tot[12:18] += q
+        charge = [0.0] * 4
+        A = 0.0
+        cs = 0
+        for te in range(4):
+            for si in range(4):
+                scal = float(np.dot(v[cell + (4 * te + si) * nc], sz[si]))
+                charge[te] += scal
+                A += abs(scal)
+                cs |= (1 if scal < 0 else 0) << (4 * te + si)
+            charge[te] = abs(np.sqrt(charge[te] * charge[te]))
+        tot[18] += sum(charge) / 4.0
+        tot[19] += A / np.sqrt(3.0)
+        ising.append(cs)
+    return tot.tolist(), ising
 
 
 def initialize_magnetic_field(B, gxy, gz):
@@ -153,6 +222,27 @@ def main():
         e = total_energy(v[:, 0], v[:, 1], v[:, 2], n, links, couplings(*Js), F)
         acases.append({"L": n, "J": list(Js), "field_case": fi, "spins": v.tolist(),
                        "energy_reference_units": e})
+    measurement = parse_measurement(text)
+    ocases = []
+    rng = np.random.default_rng(20240613)
+    axes = np.array([[1, 1, 1], [-1, -1, 1], [1, -1, -1], [-1, 1, -1]], dtype=np.float64) / np.sqrt(3)
+    for n, kind in ((2, "random"), (3, "random"), (2, "tilted all-in-all-out")):
+        N = 16 * n ** 3
+        if kind == "random":
+            v = rng.normal(size=(N, 3))
+        else:  # sites along +-a_b with a random tilt, so every irrep is non-zero
+            b = np.arange(N) // n ** 3 % 4
+            v = axes[b] * np.where(rng.random(N) < 0.8, 1.0, -1.0)[:, None] + 0.3 * rng.normal(size=(N, 3))
+        v /= np.linalg.norm(v, axis=1, keepdims=True)
+        v = v.astype(np.float32).astype(np.float64)
+        tot, ising = order_parameters(v, n, measurement)
+        ocases.append({"L": n, "kind": kind, "spins": v.tolist(), "order": tot, "ising": ising})
+    with open(os.path.join(OUT, "reference_order.json"), "w") as f:
+        json.dump({"source": "Measurement Pyrochlore.cu:526-641; Math.cu:335-541",
+                   "spin_layout": "plane-major: index = site * L^3 + (z L + y) L + x",
+                   "order_layout": "12 irrep components (Order[] order), quadrupole xx xy xz "
+                                   "yy yz zz, monopole, |Sz|; sums over cells",
+                   "cases": ocases}, f)
     with open(os.path.join(OUT, "reference_anisotropic.json"), "w") as f:
         json.dump({"source": "couplings_const Pyrochlore.cu:169-184; InitializeMagneticField "
                              "414-450; TotalEnergy 468-523; defaults 138-141",
