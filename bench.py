@@ -273,21 +273,44 @@ def run_batched(args):
     sec = _timed(stream, lambda: eng.cycle(1, 4, True, steps))
     spins = sum(len(sy.temperatures) * sy.n_sites for sy in systems)
     updates = spins * 5 * steps
-    # dominant kernel: one over-relaxation sweep (16 colour passes)
-    or_s = _timed(stream, lambda: eng.overrelax_sweep(2)) / 2
-    pass_bytes = 272 * spins  # per sweep: 16 passes x (16 N + 16 N / 16) bytes per N/16 updates
-    peak, kind = hbm_peak()
+    roofline = far_roofline(eng, stream, spins, choice_schedule(eng), updates / (sec * 1e9))
     print(json.dumps({
         "metric": "spin-updates/ns", "workload": "batched", "value": updates / (sec * 1e9),
         "unit": "updates/ns", "ms_per_step": 1e3 * sec / steps, "steps": steps,
         "spins": spins, "systems": 256, "autotune_choice": choice,
-        "roofline": {"bound": "hbm", "kernel": "colour_pass_kernel<general, over-relaxation>",
-                     "bytes_per_update": 272, "achieved": pass_bytes / or_s / 1e9, "peak": peak,
-                     "unit": "GB/s", "frac": pass_bytes / or_s / 1e9 / peak, "peak_kind": kind},
+        "roofline": roofline,
         "config": {"workload": "256 systems, L in {8,12,16,20,24}, 16-32 replicas each, ladders "
                                "in [0.05, 1.5], J2, J3 in [-0.1, 0.1], 1 M + 4 OR + exchange"}}),
           flush=True)
     return 0
+
+
+def choice_schedule(eng):
+    """True when the chosen schedule keeps replica groups in L2 across a cycle."""
+    return eng.get_option(eng.OPT_GROUP_MB) > 0 or eng.get_option(eng.OPT_REPLICA_GROUP) > 0
+
+
+def far_roofline(eng, stream, spins, l2_resident, value):
+    """Roofline of the 16-colour over-relaxation pass (compile-time-offset
+    kernel) streaming from HBM: 272 algorithmic bytes per update (the replica
+    read once, one site plane written, per pass of 1/16 of the sites), timed
+    over whole sweeps with replica groups switched off; plus the HBM bytes of
+    the schedule that was timed."""
+    eng.set_option(eng.OPT_GROUP_MB, 0)
+    eng.set_option(eng.OPT_REPLICA_GROUP, 0)
+    eng.set_option(eng.OPT_CHAINS, 1)
+    eng.overrelax_sweep(1)
+    or_s = _timed(stream, lambda: eng.overrelax_sweep(2)) / 2
+    achieved = 272 * spins / or_s / 1e9  # per sweep: 16 passes x 272 B x N/16 updates
+    peak, kind = hbm_peak()
+    sched_bytes = 32.0 / 5 if l2_resident else 272.0
+    return {"bound": "hbm", "kernel": "far_pass_kernel<site, over-relaxation>, one launch per "
+                                      "colour pass over all replicas, streaming from HBM",
+            "bytes_per_update": 272, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": kind, "ms_per_launch": 1e3 * or_s / 16,
+            "traffic": None,
+            "schedule": {"l2_resident_groups": l2_resident, "hbm_bytes_per_update": sched_bytes,
+                         "achieved": value * sched_bytes, "frac": value * sched_bytes / peak}}
 
 
 def run_large(args):
@@ -313,6 +336,7 @@ def run_large(args):
     steps = args.steps if args.steps != 300 else 10
     sec = _timed(stream, lambda: eng.cycle(1, 4, True, steps))
     updates = 32 * s.n_sites * 5 * steps
+    roofline = far_roofline(eng, stream, 32 * s.n_sites, choice_schedule(eng), updates / (sec * 1e9))
     sq_s = _timed(stream, lambda: eng.structure_factor(32, 4))
     # precision accounting: replica 0 of a 1-replica L=64 system, first 100
     # sweeps, GPU FP32 vs the host FP64 oracle from the same initial spins
@@ -343,6 +367,7 @@ def run_large(args):
         "metric": "spin-updates/ns", "workload": "large", "value": updates / (sec * 1e9),
         "unit": "updates/ns", "ms_per_step": 1e3 * sec / steps, "steps": steps,
         "structure_factor_32cubed_ms": 1e3 * sq_s, "autotune_choice": choice,
+        "roofline": roofline,
         "fp64_error_first_100_sweeps": errs,
         "config": {"workload": "L=64, J1=1, J2=J3=0.05, 32 replicas in [0.03, 1.0], renormalise "
                                "every 100 sweeps, 1 M + 4 OR + exchange; S(q) 32^3, stride 4"}}),
