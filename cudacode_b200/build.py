@@ -81,8 +81,8 @@ CLI = os.path.join(PKG, "pyro_run")
 def build_cli(force: bool = False) -> str:
     """The C++ command-line driver (host code only), linked to libpyro.so."""
     src = os.path.join(PKG, "host", "pyro_run.cpp")
-    deps = [src, os.path.join(PKG, "host", "pyro_host.hpp"), os.path.join(ROOT, "include", "pyro.h"),
-            LIB]
+    deps = [src, os.path.join(PKG, "host", "pyro_host.hpp"), os.path.join(PKG, "host", "measure.hpp"),
+            os.path.join(ROOT, "include", "pyro.h"), LIB]
     if not force and _newer(CLI, deps):
         return CLI
     cxx = shutil.which("g++") or "/usr/bin/g++"

@@ -150,6 +150,14 @@ inline void MagnetizationG(Device& d, double gxy, double gz, std::vector<double>
         for (int k = 0; k < 3; ++k) M[3 * r + i] += g[9 * b + 3 * i + k] * m[(4 * r + b) * 3 + k];
 }
 
+// DoMeasurement / CalculateQuadrupole / CalculateAbsSz / CalculateAbsSumSz
+// (Pyrochlore.cu:1047-1100, Math.cu:335-510): the 20 order parameters of
+// every configuration slot (pyro_order_parameters layout).
+inline void OrderParameters(Device& d, std::vector<double>& out) {
+  out.resize(20 * d.replicas());
+  d.check(pyro_order_parameters(d.ctx(), 0, out.data()));
+}
+
 // Geometric ("log scale") or linear ladder between tmin and tmax
 // (the reference's SetupLog/LinearTemperatures, whose source is absent).
 inline std::vector<double> Ladder(double tmin, double tmax, int n, bool log_scale) {
