@@ -110,35 +110,45 @@ __device__ __forceinline__ pyro_vec3 exch_add(pyro_vec3 h, const float4* __restr
   return pyro_matvec_add(h, p.xa[b][slot], v.x, v.y, v.z);
 }
 
-template <int S, bool kMetro, bool kL2Only = false, bool kExch = false>
-__device__ __forceinline__ int update_site(float4* __restrict__ rep, const CellFrame& f, int cell,
-                                           int L3, float J1, float beta, float cosmax, uint32_t rkey,
-                                           uint32_t sweep32, bool renorm, uint32_t seed_lo,
-                                           uint32_t seed_hi, const J1PassParams& p) {
+// Own spin and local field of site S of `cell` (loads and field arithmetic).
+template <int S, bool kL2Only = false, bool kExch = false>
+__device__ __forceinline__ void site_field(const float4* __restrict__ rep, const CellFrame& f,
+                                           int cell, int L3, float J1, const J1PassParams& p,
+                                           pyro_vec3* sp, pyro_vec3* h) {
   const int own = S * L3 + cell;
-  const float4 sv = kL2Only ? __ldcg(rep + own) : rep[own];
-  pyro_vec3 h;
+  const float4 sv = kL2Only ? __ldcg(rep + own) : __ldg(rep + own);
   if (kExch) {
-    h.x = h.y = h.z = 0.0f;
-    h = exch_add<S, 0, kL2Only>(h, rep, f, L3, p);
-    h = exch_add<S, 1, kL2Only>(h, rep, f, L3, p);
-    h = exch_add<S, 2, kL2Only>(h, rep, f, L3, p);
-    h = exch_add<S, 3, kL2Only>(h, rep, f, L3, p);
-    h = exch_add<S, 4, kL2Only>(h, rep, f, L3, p);
-    h = exch_add<S, 5, kL2Only>(h, rep, f, L3, p);
-    h.x = h.x - p.xf[S & 3][0];
-    h.y = h.y - p.xf[S & 3][1];
-    h.z = h.z - p.xf[S & 3][2];
+    pyro_vec3 a;
+    a.x = a.y = a.z = 0.0f;
+    a = exch_add<S, 0, kL2Only>(a, rep, f, L3, p);
+    a = exch_add<S, 1, kL2Only>(a, rep, f, L3, p);
+    a = exch_add<S, 2, kL2Only>(a, rep, f, L3, p);
+    a = exch_add<S, 3, kL2Only>(a, rep, f, L3, p);
+    a = exch_add<S, 4, kL2Only>(a, rep, f, L3, p);
+    a = exch_add<S, 5, kL2Only>(a, rep, f, L3, p);
+    h->x = a.x - p.xf[S & 3][0];
+    h->y = a.y - p.xf[S & 3][1];
+    h->z = a.z - p.xf[S & 3][2];
   } else {
     const pyro_vec3 a = j1_sum<S, kL2Only>(rep, f, L3);
-    h.x = J1 * a.x;
-    h.y = J1 * a.y;
-    h.z = J1 * a.z;
+    h->x = J1 * a.x;
+    h->y = J1 * a.y;
+    h->z = J1 * a.z;
   }
-  pyro_vec3 sp;
-  sp.x = sv.x;
-  sp.y = sv.y;
-  sp.z = sv.z;
+  sp->x = sv.x;
+  sp->y = sv.y;
+  sp->z = sv.z;
+}
+
+// The update of site S given its spin and field: Metropolis (Philox, cone,
+// exp) or over-relaxation, optional renormalisation, store. Returns 1 if a
+// Metropolis move was accepted.
+template <int S, bool kMetro>
+__device__ __forceinline__ int site_update(float4* __restrict__ rep, int cell, int L3,
+                                           pyro_vec3 sp, pyro_vec3 h, float beta, float cosmax,
+                                           uint32_t rkey, uint32_t sweep32, bool renorm,
+                                           uint32_t seed_lo, uint32_t seed_hi) {
+  const int own = S * L3 + cell;
   pyro_vec3 out;
   int acc = 0;
   if (kMetro) {
@@ -154,6 +164,17 @@ __device__ __forceinline__ int update_site(float4* __restrict__ rep, const CellF
   if (renorm) out = pyro_renormalise(out);
   rep[own] = make_float4(out.x, out.y, out.z, 0.0f);
   return acc;
+}
+
+template <int S, bool kMetro, bool kL2Only = false, bool kExch = false>
+__device__ __forceinline__ int update_site(float4* __restrict__ rep, const CellFrame& f, int cell,
+                                           int L3, float J1, float beta, float cosmax, uint32_t rkey,
+                                           uint32_t sweep32, bool renorm, uint32_t seed_lo,
+                                           uint32_t seed_hi, const J1PassParams& p) {
+  pyro_vec3 sp, h;
+  site_field<S, kL2Only, kExch>(rep, f, cell, L3, J1, p, &sp, &h);
+  return site_update<S, kMetro>(rep, cell, L3, sp, h, beta, cosmax, rkey, sweep32, renorm, seed_lo,
+                                seed_hi);
 }
 
 template <int B, bool kMetro, bool kExch>
@@ -179,14 +200,22 @@ __global__ void __launch_bounds__(kJ1Threads) j1_pass_kernel(const J1PassParams 
         p.renorm_every > 0 && ((sweep + 1) % (unsigned long long)p.renorm_every) == 0;
     const uint32_t rkey = (uint32_t)(p.rep_key + rep);
     const uint32_t sw = (uint32_t)sweep;
-    acc += update_site<B, kMetro, false, kExch>(rb, f, cell, p.L3, p.J1, beta, cosmax, rkey, sw,
-                                                renorm, p.seed_lo, p.seed_hi, p);
-    acc += update_site<4 + B, kMetro, false, kExch>(rb, f, cell, p.L3, p.J1, beta, cosmax, rkey,
-                                                    sw, renorm, p.seed_lo, p.seed_hi, p);
-    acc += update_site<8 + B, kMetro, false, kExch>(rb, f, cell, p.L3, p.J1, beta, cosmax, rkey,
-                                                    sw, renorm, p.seed_lo, p.seed_hi, p);
-    acc += update_site<12 + B, kMetro, false, kExch>(rb, f, cell, p.L3, p.J1, beta, cosmax, rkey,
-                                                     sw, renorm, p.seed_lo, p.seed_hi, p);
+    // The four sites of the colour in this cell are not neighbours of each
+    // other (nor of any site written in this pass), so all their loads are
+    // issued before the first store: one memory round trip, not four.
+    pyro_vec3 s0, h0, s1, h1, s2, h2, s3, h3;
+    site_field<B, false, kExch>(rb, f, cell, p.L3, p.J1, p, &s0, &h0);
+    site_field<4 + B, false, kExch>(rb, f, cell, p.L3, p.J1, p, &s1, &h1);
+    site_field<8 + B, false, kExch>(rb, f, cell, p.L3, p.J1, p, &s2, &h2);
+    site_field<12 + B, false, kExch>(rb, f, cell, p.L3, p.J1, p, &s3, &h3);
+    acc += site_update<B, kMetro>(rb, cell, p.L3, s0, h0, beta, cosmax, rkey, sw, renorm,
+                                  p.seed_lo, p.seed_hi);
+    acc += site_update<4 + B, kMetro>(rb, cell, p.L3, s1, h1, beta, cosmax, rkey, sw, renorm,
+                                      p.seed_lo, p.seed_hi);
+    acc += site_update<8 + B, kMetro>(rb, cell, p.L3, s2, h2, beta, cosmax, rkey, sw, renorm,
+                                      p.seed_lo, p.seed_hi);
+    acc += site_update<12 + B, kMetro>(rb, cell, p.L3, s3, h3, beta, cosmax, rkey, sw, renorm,
+                                       p.seed_lo, p.seed_hi);
   }
   if (kMetro) {
     // Block-wide count of accepted moves: one atomic per CTA.
