@@ -76,6 +76,7 @@ J1PassParams j1_params(pyro_ctx* ctx, int si, unsigned long long off) {
   p.seed_hi = (uint32_t)(ctx->seed >> 32);
   p.renorm_every = ctx->renorm_every;
   p.exch = s.exch >= 0 ? 1 : 0;
+  p.pdl = ctx->pdl;
   std::memset(p.xa, 0, sizeof p.xa);
   std::memset(p.xf, 0, sizeof p.xf);
   if (s.exch >= 0) {
@@ -810,6 +811,9 @@ int pyro_set_option(pyro_ctx* ctx, int option, int value) {
   } else if (option == PYRO_OPT_FAR_KERNEL) {
     if (value != 0 && value != 1) return fail(ctx, PYRO_ERR_ARG, "far kernel option is 0 or 1");
     ctx->far_kernel = value;
+  } else if (option == PYRO_OPT_PDL) {
+    if (value != 0 && value != 1) return fail(ctx, PYRO_ERR_ARG, "PDL option is 0 or 1");
+    ctx->pdl = value;
   } else if (option == PYRO_OPT_GROUP_MB) {
     if (value < 0) return fail(ctx, PYRO_ERR_ARG, "group size in MB must be >= 0");
     ctx->gen_group_mb = value;
@@ -856,6 +860,7 @@ int pyro_get_option(pyro_ctx* ctx, int option, int* value) {
     case PYRO_OPT_CHAINS: *value = ctx->n_chains; break;
     case PYRO_OPT_GROUP_MB: *value = ctx->gen_group_mb; break;
     case PYRO_OPT_FAR_KERNEL: *value = ctx->far_kernel; break;
+    case PYRO_OPT_PDL: *value = ctx->pdl; break;
     case PYRO_OPT_J1_SITE_MODE:
       *value = (ctx->j1_metro_site_mode ? 1 : 0) | (ctx->j1_or_site_mode ? 2 : 0);
       break;

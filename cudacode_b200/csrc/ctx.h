@@ -89,6 +89,7 @@ struct pyro_ctx {
   };
   std::vector<char> pass_all16;  // same, for the ungrouped generic lists
   int far_kernel = 1;  // compile-time-offset kernel for 16-colour passes
+  int pdl = 1;         // programmatic dependent launch of the per-pass J1 kernels
   std::vector<GenGroup> gen_groups;
   int n_chains = 1;     // concurrent streams the replica groups are dealt to
   cudaStream_t chain_stream[pyro::kMaxChains] = {};

@@ -177,8 +177,17 @@ __device__ __forceinline__ int update_site(float4* __restrict__ rep, const CellF
                                 seed_hi);
 }
 
+// Start of a per-pass kernel: the grid this launch may overlap (programmatic
+// dependent launch) must have completed and its writes be visible before any
+// global load; then the next pass may begin launching.
+__device__ __forceinline__ void pass_prologue() {
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
 template <int B, bool kMetro, bool kExch>
 __global__ void __launch_bounds__(kJ1Threads) j1_pass_kernel(const J1PassParams p) {
+  pass_prologue();
   const int rep = blockIdx.y;
   const int cell = blockIdx.x * kJ1Threads + threadIdx.x;
   const int g = p.rep_global + rep;
@@ -240,6 +249,7 @@ __global__ void __launch_bounds__(kJ1Threads) j1_pass_kernel(const J1PassParams 
 // Metropolis pass (Philox, cone, exp) is latency-bound without them.
 template <int B, bool kMetro, bool kExch>
 __global__ void __launch_bounds__(kJ1Threads) j1_site_pass_kernel(const J1PassParams p) {
+  pass_prologue();
   const int f = blockIdx.y;
   const int rep = blockIdx.z;
   const int cell = blockIdx.x * kJ1Threads + threadIdx.x;
@@ -549,6 +559,23 @@ __global__ void __launch_bounds__(kJ1CycleThreads, 1)
 
 }  // namespace
 
+namespace {
+template <typename Kernel>
+void launch_pass(Kernel k, dim3 grid, const J1PassParams& p, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(kJ1Threads, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = p.pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k, p);  // errors are read back with cudaGetLastError
+}
+}  // namespace
+
 void launch_j1_pass(const J1PassParams& p, int colour, bool metro, bool site_per_thread,
                     cudaStream_t st) {
   const dim3 grid((p.L3 + kJ1Threads - 1) / kJ1Threads, p.n_rep);
@@ -556,11 +583,11 @@ void launch_j1_pass(const J1PassParams& p, int colour, bool metro, bool site_per
 #define PYRO_J1_CASE(B, X)                                                            \
   case B:                                                                             \
     if (site_per_thread) {                                                            \
-      if (metro) j1_site_pass_kernel<B, true, X><<<sgrid, kJ1Threads, 0, st>>>(p);    \
-      else j1_site_pass_kernel<B, false, X><<<sgrid, kJ1Threads, 0, st>>>(p);         \
+      if (metro) launch_pass(j1_site_pass_kernel<B, true, X>, sgrid, p, st);          \
+      else launch_pass(j1_site_pass_kernel<B, false, X>, sgrid, p, st);               \
     } else {                                                                          \
-      if (metro) j1_pass_kernel<B, true, X><<<grid, kJ1Threads, 0, st>>>(p);          \
-      else j1_pass_kernel<B, false, X><<<grid, kJ1Threads, 0, st>>>(p);               \
+      if (metro) launch_pass(j1_pass_kernel<B, true, X>, grid, p, st);                \
+      else launch_pass(j1_pass_kernel<B, false, X>, grid, p, st);                     \
     }                                                                                 \
     break;
   if (p.exch) {

@@ -32,6 +32,10 @@ struct J1PassParams {
   int exch;
   float xa[4][3][9];
   float xf[4][3];
+  // Programmatic dependent launch: the pass may be launched while the
+  // previous kernel of its stream drains; it waits (griddepcontrol.wait)
+  // before its first global memory access.
+  int pdl;
 };
 
 // FP64 energy (by tetrahedra) and magnetisation partials of one J1 system;

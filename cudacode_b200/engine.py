@@ -279,6 +279,7 @@ class Engine:
     OPT_CHAINS = 7
     OPT_GROUP_MB = 8
     OPT_FAR_KERNEL = 9
+    OPT_PDL = 10
 
     def set_option(self, option: int, value: int) -> None:
         self._ck(self.lib.pyro_set_option(self.ctx, option, value))

@@ -390,3 +390,21 @@ def test_shared_memory_cycles_bit_exact(L, J2, J3):
     e.cycle(1, 5, False, 2)
     o.cycle(1, 5, False, 2)
     assert np.array_equal(e.get_spins(), o.get_spins())
+
+
+@pytest.mark.parametrize("pdl, site_mode", [(0, 1), (1, 1), (1, 0), (1, 3)])
+def test_programmatic_dependent_launch_keeps_the_chain(pdl, site_mode):
+    temps = geometric_ladder(0.1, 1.5, 8)
+    s = System(L=9, temperatures=temps)
+    e, o = pair([s])
+    e.set_option(e.OPT_PDL, pdl)
+    e.set_option(e.OPT_J1_SITE_MODE, site_mode)
+    e.set_option(e.OPT_REPLICA_GROUP, 2)
+    e.set_option(e.OPT_CHAINS, 3)
+    assert e.get_option(e.OPT_PDL) == pdl
+    e.init_random()
+    o.init_random()
+    e.cycle(1, 4, True, 6)
+    o.cycle(1, 4, True, 6)
+    assert np.array_equal(e.get_spins(), o.get_spins())
+    assert np.array_equal(e.permutation(), o.permutation())
