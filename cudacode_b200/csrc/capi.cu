@@ -50,6 +50,7 @@ PassParams pass_params(pyro_ctx* ctx, int pass) {
   p.seed_hi = (uint32_t)(ctx->seed >> 32);
   p.renorm_every = ctx->renorm_every;
   p.exch = ctx->d_exch;
+  p.pdl = ctx->pdl;
   return p;
 }
 

@@ -89,6 +89,10 @@ __device__ __forceinline__ int find_seg(const Seg* segs, int nseg, int block) {
 
 template <int S, bool kMetro>
 __global__ void __launch_bounds__(kFarThreads) far_pass_kernel(const PassParams p) {
+  // may overlap the drain of the previous kernel (programmatic dependent
+  // launch): wait for it before any global access
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
   const int seg_i = find_seg(p.segs, p.nseg, blockIdx.x);
   const PassSeg sg = p.segs[seg_i];
   const SysDev& sd = p.sys[sg.sys];
@@ -156,12 +160,26 @@ __global__ void __launch_bounds__(kFarThreads) far_pass_kernel(const PassParams 
   }
 }
 
+template <typename Kernel>
+void launch_far_kernel(Kernel k, int n_blocks, const PassParams& p, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(n_blocks, 1, 1);
+  cfg.blockDim = dim3(kFarThreads, 1, 1);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = p.pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k, p);  // errors are read back with cudaGetLastError
+}
+
 template <bool kMetro>
 void launch_far(const PassParams& p, int site, int n_blocks, cudaStream_t st) {
   switch (site) {
 #define PYRO_FAR(S) \
   case S:           \
-    far_pass_kernel<S, kMetro><<<n_blocks, kFarThreads, 0, st>>>(p); \
+    launch_far_kernel(far_pass_kernel<S, kMetro>, n_blocks, p, st); \
     break;
     PYRO_FAR(0) PYRO_FAR(1) PYRO_FAR(2) PYRO_FAR(3) PYRO_FAR(4) PYRO_FAR(5) PYRO_FAR(6)
     PYRO_FAR(7) PYRO_FAR(8) PYRO_FAR(9) PYRO_FAR(10) PYRO_FAR(11) PYRO_FAR(12) PYRO_FAR(13)

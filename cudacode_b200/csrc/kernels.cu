@@ -96,6 +96,10 @@ __device__ __forceinline__ pyro_vec3 exch_field(const float4* __restrict__ rep, 
 template <bool kJ1Only, bool kMetro>
 __global__ void __launch_bounds__(kPassThreads) colour_pass_kernel(const PassParams p,
                                                                    const NbrTable tab) {
+  // may overlap the drain of the previous kernel (programmatic dependent
+  // launch): wait for it before any global access
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
   const int seg_i = find_segment(p.segs, p.nseg, blockIdx.x);
   const PassSeg sg = p.segs[seg_i];
   const SysDev& sd = p.sys[sg.sys];
@@ -404,15 +408,32 @@ __global__ void check_spins_kernel(const float4* spins, long long n, float tol,
 
 }  // namespace
 
+namespace {
+template <typename Kernel>
+void launch_pass_kernel(Kernel k, int n_blocks, const PassParams& p, const NbrTable& tab,
+                        cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(n_blocks, 1, 1);
+  cfg.blockDim = dim3(kPassThreads, 1, 1);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = p.pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k, p, tab);  // errors are read back with cudaGetLastError
+}
+}  // namespace
+
 void launch_colour_pass(const PassParams& p, const NbrTable& tab, int n_blocks, bool metro,
                         bool j1_only, cudaStream_t st) {
   if (n_blocks <= 0) return;
   if (metro) {
-    if (j1_only) colour_pass_kernel<true, true><<<n_blocks, kPassThreads, 0, st>>>(p, tab);
-    else colour_pass_kernel<false, true><<<n_blocks, kPassThreads, 0, st>>>(p, tab);
+    if (j1_only) launch_pass_kernel(colour_pass_kernel<true, true>, n_blocks, p, tab, st);
+    else launch_pass_kernel(colour_pass_kernel<false, true>, n_blocks, p, tab, st);
   } else {
-    if (j1_only) colour_pass_kernel<true, false><<<n_blocks, kPassThreads, 0, st>>>(p, tab);
-    else colour_pass_kernel<false, false><<<n_blocks, kPassThreads, 0, st>>>(p, tab);
+    if (j1_only) launch_pass_kernel(colour_pass_kernel<true, false>, n_blocks, p, tab, st);
+    else launch_pass_kernel(colour_pass_kernel<false, false>, n_blocks, p, tab, st);
   }
 }
 

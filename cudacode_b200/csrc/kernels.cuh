@@ -26,6 +26,7 @@ struct PassParams {
   uint32_t seed_lo, seed_hi;
   int renorm_every;
   const ExchangeDev* exch;      // bond matrices of anisotropic systems (SysDev::exch >= 0)
+  int pdl;                      // programmatic dependent launch (griddepcontrol.wait first)
 };
 
 // Energy / magnetisation partial sums, one block per chunk of a replica.

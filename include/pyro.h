@@ -107,7 +107,8 @@ int pyro_neighbour_table(int site, int* out120);
  * the kernel with compile-time neighbour offsets, 0 on the generic kernel.
  * Identical results. */
 #define PYRO_OPT_FAR_KERNEL 9
-/* PYRO_OPT_PDL: 1 (default) launches the per-pass nearest-neighbour kernels
+/* PYRO_OPT_PDL: 1 (default) launches the per-pass kernels (nearest-neighbour,
+ * 16-colour and generic)
  * with programmatic dependent launch, so a pass's launch overlaps the drain
  * of the previous kernel in its stream (each pass waits for that kernel's
  * completion before touching memory: results are unchanged); 0 plain
