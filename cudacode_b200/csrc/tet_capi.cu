@@ -111,6 +111,7 @@ TetMoveParams move_params(pyro_ctx* ctx, int si, unsigned long long off) {
   p.seed_lo = (uint32_t)(ctx->seed & 0xffffffffu);
   p.seed_hi = (uint32_t)(ctx->seed >> 32);
   p.image = ctx->tet->d_image;
+  p.pdl = ctx->pdl;
   return p;
 }
 

@@ -608,8 +608,17 @@ __device__ __forceinline__ void count_accepted(const TetMoveParams& p, int tslot
     atomicAdd(p.accepted + p.temp_base + tslot, (unsigned long long)__popc(acc_mask));
 }
 
+// Start of a per-pass kernel that may overlap the drain of the previous
+// kernel of its stream (programmatic dependent launch): that kernel must be
+// complete, its writes visible, before the first global access.
+__device__ __forceinline__ void pass_prologue() {
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
 template <int F>
 __global__ void __launch_bounds__(kTetMoveThreads) tet_move_kernel(const TetMoveParams p) {
+  pass_prologue();
   extern __shared__ __align__(16) unsigned char smem[];
   const MlpSmem w = carve_weights(smem);
   __nv_bfloat16* feat_all = reinterpret_cast<__nv_bfloat16*>(smem + kSmemWeightsFwd);
@@ -632,6 +641,7 @@ __global__ void __launch_bounds__(kTetMoveThreads) tet_move_kernel(const TetMove
 // Per-pass kernel, two lanes per tetrahedron (256 threads = 128 tetrahedra).
 template <int F>
 __global__ void __launch_bounds__(kTetMoveThreads) tet_move_pair_kernel(const TetMoveParams p) {
+  pass_prologue();
   extern __shared__ __align__(16) unsigned char smem[];
   const MlpSmem w = carve_weights(smem);
   __nv_bfloat16* feat_all = reinterpret_cast<__nv_bfloat16*>(smem + kSmemWeightsFwd);
@@ -1058,25 +1068,42 @@ void launch_mlp_pack(const float* master, unsigned char* image, cudaStream_t st)
   mlp_pack_kernel<<<(kImgBytes / 2 + 255) / 256, 256, 0, st>>>(master, image);
 }
 
+namespace {
+template <typename Kernel>
+void launch_move(Kernel k, int blocks, const TetMoveParams& p, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks, 1, 1);
+  cfg.blockDim = dim3(kTetMoveThreads, 1, 1);
+  cfg.dynamicSmemBytes = kTetMoveSmem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = p.pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k, p);  // errors are read back with cudaGetLastError
+}
+}  // namespace
+
 void launch_tet_move(const TetMoveParams& p, int f, bool pair_mode, cudaStream_t st) {
   const long long n = (long long)p.n_rep * p.L3;
   if (pair_mode) {
     const int half = kTetMoveThreads / 2;
     const int blocks = (int)((n + half - 1) / half);
     switch (f) {
-      case 0: tet_move_pair_kernel<0><<<blocks, kTetMoveThreads, kTetMoveSmem, st>>>(p); break;
-      case 1: tet_move_pair_kernel<1><<<blocks, kTetMoveThreads, kTetMoveSmem, st>>>(p); break;
-      case 2: tet_move_pair_kernel<2><<<blocks, kTetMoveThreads, kTetMoveSmem, st>>>(p); break;
-      default: tet_move_pair_kernel<3><<<blocks, kTetMoveThreads, kTetMoveSmem, st>>>(p); break;
+      case 0: launch_move(tet_move_pair_kernel<0>, blocks, p, st); break;
+      case 1: launch_move(tet_move_pair_kernel<1>, blocks, p, st); break;
+      case 2: launch_move(tet_move_pair_kernel<2>, blocks, p, st); break;
+      default: launch_move(tet_move_pair_kernel<3>, blocks, p, st); break;
     }
     return;
   }
   const int blocks = (int)((n + kTetMoveThreads - 1) / kTetMoveThreads);
   switch (f) {
-    case 0: tet_move_kernel<0><<<blocks, kTetMoveThreads, kTetMoveSmem, st>>>(p); break;
-    case 1: tet_move_kernel<1><<<blocks, kTetMoveThreads, kTetMoveSmem, st>>>(p); break;
-    case 2: tet_move_kernel<2><<<blocks, kTetMoveThreads, kTetMoveSmem, st>>>(p); break;
-    default: tet_move_kernel<3><<<blocks, kTetMoveThreads, kTetMoveSmem, st>>>(p); break;
+    case 0: launch_move(tet_move_kernel<0>, blocks, p, st); break;
+    case 1: launch_move(tet_move_kernel<1>, blocks, p, st); break;
+    case 2: launch_move(tet_move_kernel<2>, blocks, p, st); break;
+    default: launch_move(tet_move_kernel<3>, blocks, p, st); break;
   }
 }
 

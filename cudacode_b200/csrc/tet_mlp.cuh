@@ -59,6 +59,7 @@ struct TetMoveParams {
   unsigned long long tet_off;
   uint32_t seed_lo, seed_hi;
   const unsigned char* image;  // kImgBytes weight image
+  int pdl;                     // programmatic dependent launch of the per-pass kernels
 };
 
 struct TetCollectParams {
