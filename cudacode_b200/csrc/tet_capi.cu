@@ -37,6 +37,8 @@ struct TetState {
   int adam_step = 0;
   uint64_t seed = 0;
   int sweep_kernel = 2;   // 0 per pass, 1 cluster (one launch per call), 2 per pass, lane pairs
+  int forward_umma = 1;   // batched forward on tcgen05 (1) or mma.sync (0)
+  int* d_err = nullptr;   // set by the tcgen05 forward if a wait ran out
   int cluster_max = 8;    // largest cluster size tried
   int cluster_ok = -1;    // -1 unknown, else the usable size (0: none)
 };
@@ -44,7 +46,7 @@ struct TetState {
 void tet_free(pyro_ctx* ctx) {
   if (!ctx || !ctx->tet) return;
   TetState* t = ctx->tet;
-  void* ptrs[] = {t->d_master, t->d_m,     t->d_v,    t->d_grad, t->d_image, t->d_ctr,
+  void* ptrs[] = {t->d_err,    t->d_master, t->d_m,     t->d_v,    t->d_grad, t->d_image, t->d_ctr,
                   t->d_accepted, t->d_loss, t->d_idx, t->d_feat, t->d_targ};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -193,7 +195,7 @@ int pyro_tet_init(pyro_ctx* ctx, uint64_t seed, long long sample_capacity) {
   PYRO_CK(cudaMalloc((void**)&t->d_m, sizeof(float) * kMlpParams));
   PYRO_CK(cudaMalloc((void**)&t->d_v, sizeof(float) * kMlpParams));
   PYRO_CK(cudaMalloc((void**)&t->d_grad, sizeof(float) * kMlpParams));
-  PYRO_CK(cudaMalloc((void**)&t->d_image, kImgBytes));
+  PYRO_CK(cudaMalloc((void**)&t->d_image, kImgTotal));
   PYRO_CK(cudaMalloc((void**)&t->d_ctr, sizeof(unsigned long long)));
   PYRO_CK(cudaMalloc((void**)&t->d_accepted, sizeof(unsigned long long) * ctx->total_temps));
   PYRO_CK(cudaMalloc((void**)&t->d_loss, sizeof(double)));
@@ -381,6 +383,52 @@ int pyro_tet_train(pyro_ctx* ctx, int steps, int batch, float lr, double* mean_l
   return PYRO_OK;
 }
 
+int pyro_tet_set_forward(pyro_ctx* ctx, int tensor_memory) {
+  int rc = need_tet(ctx);
+  if (rc) return rc;
+  if (tensor_memory != 0 && tensor_memory != 1)
+    return fail(ctx, PYRO_ERR_ARG, "tet_set_forward: 0 (mma.sync) or 1 (tcgen05)");
+  ctx->tet->forward_umma = tensor_memory;
+  return PYRO_OK;
+}
+
+// Network outputs of n device-resident feature rows on the chosen kernel.
+static int tet_forward_queue(pyro_ctx* ctx, const float* d_in, int n, float* d_out) {
+  TetState* t = ctx->tet;
+  if (t->forward_umma) {
+    if (!t->d_err) {
+      PYRO_CK(cudaMalloc((void**)&t->d_err, sizeof(int)));
+      PYRO_CK(cudaMemset(t->d_err, 0, sizeof(int)));
+    }
+    PYRO_CK(launch_umma_forward(d_in, n, t->d_image, d_out, t->d_err, ctx->stream));
+  } else {
+    launch_mlp_forward(d_in, n, t->d_image, d_out, ctx->stream);
+    PYRO_CK_LAUNCH();
+  }
+  ctx->launches += 1;
+  return PYRO_OK;
+}
+
+static int tet_forward_check(pyro_ctx* ctx) {
+  TetState* t = ctx->tet;
+  if (!t->forward_umma || !t->d_err) return PYRO_OK;
+  int err = 0;
+  PYRO_CK(cudaMemcpy(&err, t->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) {
+    cudaMemset(t->d_err, 0, sizeof(int));
+    return fail(ctx, PYRO_ERR_TIMEOUT, "tet_forward: a tensor-core MMA did not complete in time");
+  }
+  return PYRO_OK;
+}
+
+int pyro_tet_forward_device(pyro_ctx* ctx, const float* dev_features, int n, float* dev_out16) {
+  int rc = need_tet(ctx);
+  if (rc) return rc;
+  if (!dev_features || !dev_out16 || n < 1) return fail(ctx, PYRO_ERR_ARG, "tet_forward: bad args");
+  PYRO_CK(cudaSetDevice(ctx->device));
+  return tet_forward_queue(ctx, dev_features, n, dev_out16);
+}
+
 // Test paths: host features in, host outputs / gradients out.
 int pyro_tet_forward(pyro_ctx* ctx, const float* features, int n, float* out) {
   int rc = need_tet(ctx);
@@ -393,8 +441,12 @@ int pyro_tet_forward(pyro_ctx* ctx, const float* features, int n, float* out) {
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(d_in, features, sizeof(float) * 16 * n, cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess) {
-    launch_mlp_forward(d_in, n, ctx->tet->d_image, d_out, ctx->stream);
-    e = cudaGetLastError();
+    rc = tet_forward_queue(ctx, d_in, n, d_out);
+    if (rc) {
+      cudaFree(d_in);
+      cudaFree(d_out);
+      return rc;
+    }
   }
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(out, d_out, sizeof(float) * 16 * n, cudaMemcpyDeviceToHost, ctx->stream);
@@ -402,7 +454,7 @@ int pyro_tet_forward(pyro_ctx* ctx, const float* features, int n, float* out) {
   cudaFree(d_in);
   if (d_out) cudaFree(d_out);
   if (e != cudaSuccess) return fail(ctx, PYRO_ERR_CUDA, std::string("tet_forward: ") + cudaGetErrorString(e));
-  return PYRO_OK;
+  return tet_forward_check(ctx);
 }
 
 int pyro_tet_gradient(pyro_ctx* ctx, const float* features, const float* targets, int n,

@@ -771,6 +771,18 @@ __device__ __forceinline__ void pack_region(const float* __restrict__ m, unsigne
   }
 }
 
+// An N x K operand W^T (element (n, k) = m[off + k * N + n]) in the
+// canonical K-major core-matrix layout of the tensor-memory MMA.
+__device__ __forceinline__ void pack_core(const float* __restrict__ m, unsigned char* image,
+                                          int region, int N, int K, int off, int tid, int nthreads) {
+  __nv_bfloat16* dst = reinterpret_cast<__nv_bfloat16*>(image + region);
+  for (int i = tid; i < N * K; i += nthreads) {
+    const int n = i / K, k = i - n * K;
+    const int byte = (n / 8) * (K / 8) * 128 + (k / 8) * 128 + (n % 8) * 16 + (k % 8) * 2;
+    dst[byte / 2] = __float2bfloat16_rn(m[off + k * N + n]);
+  }
+}
+
 __global__ void mlp_pack_kernel(const float* __restrict__ m, unsigned char* image) {
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
   // forward operands, [out][in]: element (o, i) = W[i][o]
@@ -780,6 +792,10 @@ __global__ void mlp_pack_kernel(const float* __restrict__ m, unsigned char* imag
   // backward operands, [in][out]
   pack_region(m, image, kImgW2, kMlpHidden, kLdH, kMlpHidden, kOffW2, kMlpHidden, 1, tid, nt);
   pack_region(m, image, kImgW3, kMlpHidden, kLdIn, kMlpOut, kOffW3, kMlpOut, 1, tid, nt);
+  // forward operands in the tcgen05 core-matrix layout, element (n, k) = W[k][n]
+  pack_core(m, image, kImgU1, kMlpHidden, kMlpIn, kOffW1, tid, nt);
+  pack_core(m, image, kImgU2, kMlpHidden, kMlpHidden, kOffW2, tid, nt);
+  pack_core(m, image, kImgU3, kMlpOut, kMlpHidden, kOffW3, tid, nt);
   float* b = reinterpret_cast<float*>(image + kImgB1);  // b1, b2, b3 contiguous
   for (int i = tid; i < 2 * kMlpHidden + kMlpOut; i += nt)
     b[i] = i < kMlpHidden ? m[kOffB1 + i]

@@ -42,9 +42,18 @@ constexpr int kImgFwdBytes = kImgB3 + kMlpOut * 4;
 constexpr int kImgW2 = kImgFwdBytes;                         // bf16 [64][kLdH]
 constexpr int kImgW3 = kImgW2 + kMlpHidden * kLdH * 2;       // bf16 [64][kLdIn]
 constexpr int kImgBytes = kImgW3 + kMlpHidden * kLdIn * 2;
+// The forward operands again in the tensor-memory MMA's canonical K-major
+// layout (8-row x 16-byte core matrices, no swizzle): element (n, k) of an
+// N x K operand at (n / 8) * (K / 8) * 128 + (k / 8) * 128 + (n % 8) * 16 +
+// (k % 8) * 2 bytes.
+constexpr int kImgU1 = kImgBytes;                            // W1^T, N=64, K=16
+constexpr int kImgU2 = kImgU1 + kMlpHidden * kMlpIn * 2;     // W2^T, N=64, K=64
+constexpr int kImgU3 = kImgU2 + kMlpHidden * kMlpHidden * 2; // W3^T, N=16, K=64
+constexpr int kImgTotal = kImgU3 + kMlpOut * kMlpHidden * 2;
 static_assert(kImgW2t % 16 == 0 && kImgW3t % 16 == 0 && kImgB1 % 16 == 0 &&
                   kImgFwdBytes % 16 == 0 && kImgW3 % 16 == 0 && kImgBytes % 16 == 0,
               "16-byte staging granules");
+static_assert(kImgU2 % 16 == 0 && kImgU3 % 16 == 0 && kImgTotal % 16 == 0, "core matrices");
 
 struct TetMoveParams {
   float4* spins;  // replica 0 of the system
@@ -91,6 +100,11 @@ int tet_chunks(int L3);  // chunks of tetrahedra per corner and replica
 // Number of samples one collect call writes: 4 classes x n_rep x ceil(L3 / stride).
 long long tet_collect_count(int L3, int n_rep, int stride);
 void launch_tet_collect(const TetCollectParams& p, cudaStream_t st);
+// Network outputs for n feature rows on the 5th-generation tensor cores
+// (tcgen05.mma, accumulators in tensor memory), 128 rows per CTA; *err is set
+// to 1 if a wait for an MMA ran out (the outputs are then not written).
+cudaError_t launch_umma_forward(const float* features, int n, const unsigned char* image,
+                               float* out, int* err, cudaStream_t st);
 // Network outputs for n feature rows (host-visible test path).
 void launch_mlp_forward(const float* features, int n, const unsigned char* image, float* out,
                         cudaStream_t st);

@@ -125,6 +125,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "pyro_tet_samples": (i, [P, pf, pf, C.c_longlong, C.POINTER(C.c_longlong)]),
         "pyro_tet_train": (i, [P, i, i, f, pd]),
         "pyro_tet_forward": (i, [P, pf, i, pf]),
+        "pyro_tet_forward_device": (i, [P, C.c_void_p, i, C.c_void_p]),
+        "pyro_tet_set_forward": (i, [P, i]),
         "pyro_tet_gradient": (i, [P, pf, pf, i, pf, pd]),
         "pyro_cycle_tet": (i, [P, i, i, i, i, i]),
         "pyro_save_checkpoint": (i, [P, C.c_char_p]),
@@ -558,6 +560,13 @@ class Engine:
         self._ck(self.lib.pyro_tet_forward(self.ctx, _ptr(x, C.c_float), x.shape[0],
                                            _ptr(out, C.c_float)))
         return out
+
+    def tet_set_forward(self, tensor_memory: int) -> None:
+        """Batched forward kernel: 1 tcgen05 (default), 0 mma.sync."""
+        self._ck(self.lib.pyro_tet_set_forward(self.ctx, tensor_memory))
+
+    def tet_forward_device(self, feats_ptr: int, n: int, out_ptr: int) -> None:
+        self._ck(self.lib.pyro_tet_forward_device(self.ctx, feats_ptr, n, out_ptr))
 
     def tet_gradient(self, feats, targets):
         x = np.ascontiguousarray(feats, dtype=np.float32)

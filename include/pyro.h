@@ -330,6 +330,14 @@ int pyro_tet_train(pyro_ctx* ctx, int steps, int batch, float lr, double* mean_l
 /* Host-buffer test paths: network outputs for n feature rows, and the
  * gradient (6288 values) and loss sum of the negative log-likelihood. */
 int pyro_tet_forward(pyro_ctx* ctx, const float* features, int n, float* out16);
+/* The same on device buffers, stream-ordered, no allocation after the first
+ * tcgen05 call (which allocates a 4-byte error flag). */
+int pyro_tet_forward_device(pyro_ctx* ctx, const float* dev_features, int n, float* dev_out16);
+/* Kernel of the batched forward: 1 (default) the 5th-generation tensor cores
+ * (tcgen05.mma, accumulators in tensor memory, 128 rows per CTA), 0 the
+ * mma.sync m16n8k16 kernel of the move and the training. A tcgen05 wait that
+ * runs out returns PYRO_ERR_TIMEOUT. */
+int pyro_tet_set_forward(pyro_ctx* ctx, int tensor_memory);
 int pyro_tet_gradient(pyro_ctx* ctx, const float* features, const float* targets, int n,
                       float* grad, double* loss_sum);
 /* Cycles with learned moves: n_metro Metropolis + n_or over-relaxation

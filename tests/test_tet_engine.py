@@ -12,17 +12,40 @@ from oracle.binding import Oracle
 pytestmark = pytest.mark.gpu
 
 
-def test_forward_matches_oracle():
+@pytest.mark.parametrize("tensor_memory", [1, 0])
+@pytest.mark.parametrize("n", [1, 128, 300, 5000])
+def test_forward_matches_oracle(tensor_memory, n):
+    """Both forward kernels (tcgen05 with tensor-memory accumulators, and
+    mma.sync) against the FP64 restatement with the same BF16 rounding
+    points; ragged row counts included."""
     e = Engine([System(L=4, temperatures=[0.2, 0.5])], seed=3)
     e.tet_init(seed=11)
-    w = e.tet_weights()
+    e.tet_set_forward(tensor_memory)
     rng = np.random.default_rng(0)
-    x = rng.normal(size=(300, 16)).astype(np.float32)
+    w = (rng.normal(size=6288) * 0.2).astype(np.float32)
+    w[13 * 64:16 * 64] = 0.0
+    e.tet_set_weights(w)
+    x = rng.normal(size=(n, 16)).astype(np.float32)
     x[:, 13:] = 0.0
     got = e.tet_forward(x)
     want = orc.mlp_forward(w, x)
     err = np.abs(got - want).max() / np.abs(want).max()
     assert err < 2e-3, err
+
+
+def test_tensor_memory_forward_agrees_with_mma_sync():
+    e = Engine([System(L=4, temperatures=[0.2, 0.5])], seed=3)
+    e.tet_init(seed=5)
+    rng = np.random.default_rng(2)
+    x = rng.normal(size=(4096, 16)).astype(np.float32)
+    x[:, 13:] = 0.0
+    e.tet_set_forward(1)
+    a = e.tet_forward(x)
+    b = e.tet_forward(x)
+    e.tet_set_forward(0)
+    c = e.tet_forward(x)
+    np.testing.assert_array_equal(a, b)  # deterministic
+    assert np.abs(a - c).max() / np.abs(c).max() < 2e-3
 
 
 def test_gradient_matches_oracle():
