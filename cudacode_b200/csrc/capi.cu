@@ -187,7 +187,11 @@ bool use_cycle_kernel(const pyro_ctx* ctx) {
 // into the context stream (parallel branches of a captured graph), so a
 // group's spins stay in L2 across its passes and one chain's launch gaps are
 // filled by another's kernels. Same updates, same order within each replica.
-int queue_grouped(pyro_ctx* ctx, int n_metro, int n_or, bool j1_grouped, bool gen_grouped) {
+// With with_obs, the FP64 energy partials of an isotropic J1 group are
+// computed on its chain right after its last pass, while its spins are still
+// in L2 (instead of one lattice-wide read from HBM after all groups).
+int queue_grouped(pyro_ctx* ctx, int n_metro, int n_or, bool j1_grouped, bool gen_grouped,
+                  bool with_obs) {
   const int chains = std::max(1, std::min(ctx->n_chains, kMaxChains));
   if (chains > 1) {
     for (int c = 0; c < chains; ++c) {
@@ -219,6 +223,19 @@ int queue_grouped(pyro_ctx* ctx, int n_metro, int n_or, bool j1_grouped, bool ge
                            metro ? ctx->j1_metro_site_mode : ctx->j1_or_site_mode, st);
             PYRO_CK_LAUNCH();
           }
+        }
+        if (with_obs && s.exch < 0) {
+          J1ObsParams jp;
+          jp.spins = ctx->d_spins + s.spin_off + (long long)r0 * 16 * s.L3;
+          jp.L = s.L;
+          jp.L3 = s.L3;
+          jp.n_rep = cnt;
+          jp.rcpL = 1.0f / (float)s.L;
+          jp.J1 = s.J64[0];
+          jp.partials = ctx->d_partials;
+          jp.partial_begin = ctx->obs_segs[si].partial_begin + r0 * j1_blocks_per_replica(s.L3);
+          launch_j1_observables(jp, st);
+          PYRO_CK_LAUNCH();
         }
       }
     }
@@ -268,7 +285,7 @@ int queue_cycle_body(pyro_ctx* ctx, int n_metro, int n_or, bool with_obs) {
   const bool j1_grouped = !cyc && ctx->rep_group > 0 && ctx->use_j1_kernel && !ctx->j1_sys.empty();
   const bool gen_grouped = !ctx->gen_groups.empty();
   if (j1_grouped || gen_grouped) {
-    rc = queue_grouped(ctx, n_metro, n_or, j1_grouped, gen_grouped);
+    rc = queue_grouped(ctx, n_metro, n_or, j1_grouped, gen_grouped, with_obs);
     if (rc) return rc;
     if (!gen_grouped) rc = queue_generic_sweeps(ctx, n_metro, n_or);
     if (rc) return rc;
@@ -296,7 +313,8 @@ int queue_cycle_body(pyro_ctx* ctx, int n_metro, int n_or, bool with_obs) {
             }
       }
     }
-    if (with_obs) rc = queue_observables(ctx, cyc && !j1_grouped);
+    // J1 observables were queued per group when grouped
+    if (with_obs) rc = queue_observables(ctx, (cyc && !j1_grouped) || j1_grouped);
     return rc;
   }
   if (cyc) {
