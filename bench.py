@@ -574,7 +574,7 @@ def main():
     variant = None
     if args.kernel == "auto":
         # the autotuner's cycles are untimed warm-up Monte Carlo steps
-        variant = eng.autotune(N_METRO, N_OR, 8) if world == 1 else None
+        variant = eng.autotune(N_METRO, N_OR, 16) if world == 1 else None
     else:
         eng.set_option(eng.OPT_CYCLE_KERNEL, 1 if args.kernel == "cluster" else 0)
         if args.kernel == "grouped":
@@ -696,8 +696,9 @@ def main():
                              "hbm_bytes_per_update": sched_bytes, "achieved": sched_gbs,
                              "frac": sched_gbs / peak,
                              "note": ("one read + one write of the lattice per cycle; the "
-                                      "schedule is bound by L2 bandwidth and launch latency, "
-                                      "not HBM" if l2_resident else
+                                      "schedule is bound by latency, occupancy and the "
+                                      "Metropolis update's instruction issue, not HBM"
+                                      if l2_resident else
                                       "every pass streams the lattice from HBM")}},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "updates/ns",
