@@ -573,8 +573,11 @@ def main():
     eng.set_cone(cones)
     variant = None
     if args.kernel == "auto":
-        # the autotuner's cycles are untimed warm-up Monte Carlo steps
-        variant = eng.autotune(N_METRO, N_OR, 16) if world == 1 else None
+        # the autotuner's cycles are untimed warm-up Monte Carlo steps; on a
+        # shard (one of several ranks) it runs them without the local
+        # exchange, and each rank keeps its own fastest variant (every
+        # variant gives the same chain)
+        variant = eng.autotune(N_METRO, N_OR, 16)
     else:
         eng.set_option(eng.OPT_CYCLE_KERNEL, 1 if args.kernel == "cluster" else 0)
         if args.kernel == "grouped":
