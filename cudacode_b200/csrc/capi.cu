@@ -1169,6 +1169,22 @@ int pyro_observables_device(pyro_ctx* ctx, int system, double* dev_energy,
   return PYRO_OK;
 }
 
+int pyro_last_observables_device(pyro_ctx* ctx, int system, double* dev_energy,
+                                 double* dev_magnetisation3) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (system < 0 || system >= (int)ctx->sys.size())
+    return fail(ctx, PYRO_ERR_ARG, "last_observables: bad system");
+  PYRO_CK(cudaSetDevice(ctx->device));
+  const SysDev& s = ctx->sys[system];
+  if (dev_energy)
+    PYRO_CK(cudaMemcpyAsync(dev_energy, ctx->d_energy + s.rep_ctx_base, sizeof(double) * s.n_rep,
+                            cudaMemcpyDeviceToDevice, ctx->stream));
+  if (dev_magnetisation3)
+    PYRO_CK(cudaMemcpyAsync(dev_magnetisation3, ctx->d_mag + 3 * s.rep_ctx_base,
+                            sizeof(double) * 3 * s.n_rep, cudaMemcpyDeviceToDevice, ctx->stream));
+  return PYRO_OK;
+}
+
 int pyro_observables(pyro_ctx* ctx, int system, double* energy, double* magnetisation3) {
   if (!ctx) return PYRO_ERR_ARG;
   if (system < 0 || system >= (int)ctx->sys.size())
@@ -1348,6 +1364,8 @@ static int run_smem_cycles(pyro_ctx* ctx, int n_metro, int n_or, int n_cycles) {
     p.history_cap = ctx->history_cap;
     p.total_temps = ctx->total_temps;
     p.exch = ctx->d_exch;
+    p.energy = ctx->d_energy;
+    p.mag = ctx->d_mag;
     PYRO_CK(launch_smem_cycles(p, ctx->tab, ctx->stream));
     ctx->launches += 1;
   }

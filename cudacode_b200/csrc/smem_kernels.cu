@@ -78,6 +78,50 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   return s;
 }
 
+// This thread's share of twice the FP64 energy of the replica in shared
+// memory: sum over its sites of S_i . h_i (bonds counted from both ends;
+// with bond matrices, minus twice the Zeeman term).
+__device__ double energy2_share(const float4* lat, const NbrTable& tab, const SysDev& sd,
+                                const ExchangeDev* exch, int L, int L3, int n) {
+  double e = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int s = i / L3, cell = i - s * L3;
+    const int x = cell % L, yz = cell / L, y = yz % L, z = yz / L;
+    const float4 sv = lat[i];
+    const int sb[5] = {0, 6, 18, 24, 30};
+    if (sd.exch >= 0) {  // twice the bond energy of this site minus twice its Zeeman term
+      const ExchangeDev& X = exch[sd.exch];
+      const int b = s & 3;
+      double hx = -2.0 * X.f64[b][0], hy = -2.0 * X.f64[b][1], hz = -2.0 * X.f64[b][2];
+      for (int q = 0; q < 6; ++q) {
+        const NbrEntry en = tab.e[s][q];
+        const float4 v = lat[(wrap_s(z + en.dz, L) * L + wrap_s(y + en.dy, L)) * L +
+                             wrap_s(x + en.dx, L) + en.t * L3];
+        const double* m = X.A64[4 * b + (en.t & 3)];
+        hx += m[0] * v.x + m[1] * v.y + m[2] * v.z;
+        hy += m[3] * v.x + m[4] * v.y + m[5] * v.z;
+        hz += m[6] * v.x + m[7] * v.y + m[8] * v.z;
+      }
+      e += (double)sv.x * hx + (double)sv.y * hy + (double)sv.z * hz;
+    }
+    for (int sh = 0; sh < 4; ++sh) {
+      if (!(sd.shells & (1 << sh))) continue;
+      if (sh == 0 && sd.exch >= 0) continue;
+      double ax = 0.0, ay = 0.0, az = 0.0;
+      for (int q = sb[sh]; q < sb[sh + 1]; ++q) {
+        const NbrEntry en = tab.e[s][q];
+        const float4 v = lat[(wrap_s(z + en.dz, L) * L + wrap_s(y + en.dy, L)) * L +
+                             wrap_s(x + en.dx, L) + en.t * L3];
+        ax += v.x;
+        ay += v.y;
+        az += v.z;
+      }
+      e += sd.J64[sh] * ((double)sv.x * ax + (double)sv.y * ay + (double)sv.z * az);
+    }
+  }
+  return e;
+}
+
 __global__ void __launch_bounds__(kSmemThreads) smem_cycles_kernel(const SmemCycleParams p,
                                                                    const NbrTable tab) {
   extern __shared__ float4 lat[];
@@ -161,42 +205,7 @@ __global__ void __launch_bounds__(kSmemThreads) smem_cycles_kernel(const SmemCyc
     }
     if (p.history) {
       // FP64 energy of the cycle's final state: E = 1/2 sum_i S_i . h_i
-      double e = 0.0;
-      for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const int s = i / L3, cell = i - s * L3;
-        const int x = cell % L, yz = cell / L, y = yz % L, z = yz / L;
-        const float4 sv = lat[i];
-        const int sb[5] = {0, 6, 18, 24, 30};
-        if (sd.exch >= 0) {  // twice the bond energy of this site minus twice its Zeeman term
-          const ExchangeDev& X = p.exch[sd.exch];
-          const int b = s & 3;
-          double hx = -2.0 * X.f64[b][0], hy = -2.0 * X.f64[b][1], hz = -2.0 * X.f64[b][2];
-          for (int q = 0; q < 6; ++q) {
-            const NbrEntry en = tab.e[s][q];
-            const float4 v = lat[(wrap_s(z + en.dz, L) * L + wrap_s(y + en.dy, L)) * L +
-                                 wrap_s(x + en.dx, L) + en.t * L3];
-            const double* m = X.A64[4 * b + (en.t & 3)];
-            hx += m[0] * v.x + m[1] * v.y + m[2] * v.z;
-            hy += m[3] * v.x + m[4] * v.y + m[5] * v.z;
-            hz += m[6] * v.x + m[7] * v.y + m[8] * v.z;
-          }
-          e += (double)sv.x * hx + (double)sv.y * hy + (double)sv.z * hz;
-        }
-        for (int sh = 0; sh < 4; ++sh) {
-          if (!(sd.shells & (1 << sh))) continue;
-          if (sh == 0 && sd.exch >= 0) continue;
-          double ax = 0.0, ay = 0.0, az = 0.0;
-          for (int q = sb[sh]; q < sb[sh + 1]; ++q) {
-            const NbrEntry en = tab.e[s][q];
-            const float4 v = lat[(wrap_s(z + en.dz, L) * L + wrap_s(y + en.dy, L)) * L +
-                                 wrap_s(x + en.dx, L) + en.t * L3];
-            ax += v.x;
-            ay += v.y;
-            az += v.z;
-          }
-          e += sd.J64[sh] * ((double)sv.x * ax + (double)sv.y * ay + (double)sv.z * az);
-        }
-      }
+      const double e = energy2_share(lat, tab, sd, p.exch, L, L3, n);
       const double tot = block_sum(e, red);
       if (threadIdx.x == 0) {
         const unsigned long long row = (hist0 + c) % (unsigned long long)p.history_cap;
@@ -205,6 +214,25 @@ __global__ void __launch_bounds__(kSmemThreads) smem_cycles_kernel(const SmemCyc
     }
   }
   for (int i = threadIdx.x; i < n; i += blockDim.x) g[i] = lat[i];
+  if (p.energy) {  // observables of the final state, as the per-pass path leaves them
+    const double e = block_sum(energy2_share(lat, tab, sd, p.exch, L, L3, n), red);
+    double mx = 0.0, my = 0.0, mz = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      mx += lat[i].x;
+      my += lat[i].y;
+      mz += lat[i].z;
+    }
+    mx = block_sum(mx, red);
+    my = block_sum(my, red);
+    mz = block_sum(mz, red);
+    if (threadIdx.x == 0) {
+      const int gi = sd.rep_ctx_base + rep;
+      p.energy[gi] = 0.5 * e;
+      p.mag[3 * gi] = mx;
+      p.mag[3 * gi + 1] = my;
+      p.mag[3 * gi + 2] = mz;
+    }
+  }
   if (p.n_metro > 0) {
     const double a = block_sum((double)acc, red);
     if (threadIdx.x == 0 && a > 0.0)

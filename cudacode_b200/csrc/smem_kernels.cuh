@@ -27,6 +27,8 @@ struct SmemCycleParams {
   const unsigned long long* history_count;
   int history_cap, total_temps;
   const ExchangeDev* exch;  // bond matrices (sys.exch >= 0)
+  double* energy;           // final-state energy / magnetisation per context replica (or null)
+  double* mag;
 };
 
 size_t smem_cycle_bytes(int L);

@@ -39,7 +39,11 @@ def shard(n_total: int, world: int, rank: int) -> tuple[int, int]:
 
 
 class EngineBackend:
-    """The CUDA engine as a sharded-PT backend (energies stay on the GPU)."""
+    """The CUDA engine as a sharded-PT backend (energies stay on the GPU).
+
+    The engine queues on its own stream and the collective on torch's
+    current stream; each hand-over makes the receiving stream wait for the
+    other (no host synchronisation)."""
 
     def __init__(self, engine: Engine, device: torch.device):
         self.engine = engine
@@ -47,14 +51,23 @@ class EngineBackend:
         self.n_local = engine.systems[0].replicas()
         self._e = torch.zeros(self.n_local, dtype=torch.float64, device=device)
 
+    def _engine_stream(self) -> torch.cuda.Stream:
+        h = self.engine.stream_handle()
+        if h == 0:
+            return torch.cuda.default_stream(self.device)
+        return torch.cuda.ExternalStream(h, device=self.device)
+
     def sweeps(self, n_metro: int, n_or: int) -> None:
         self.engine.cycle(n_metro, n_or, False, 1)
 
     def local_energies(self) -> torch.Tensor:
-        self.engine.observables_device(self._e.data_ptr())
+        # the cycle computed them at its end: copy, do not recompute
+        self.engine.last_observables_device(self._e.data_ptr())
+        torch.cuda.current_stream(self.device).wait_stream(self._engine_stream())
         return self._e
 
     def swap_global(self, all_energies: torch.Tensor, parity: int) -> None:
+        self._engine_stream().wait_stream(torch.cuda.current_stream(self.device))
         self.engine.pt_swap_global(all_energies.data_ptr(), parity)
 
 

@@ -126,6 +126,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "pyro_tet_train": (i, [P, i, i, f, pd]),
         "pyro_tet_forward": (i, [P, pf, i, pf]),
         "pyro_tet_forward_device": (i, [P, C.c_void_p, i, C.c_void_p]),
+        "pyro_last_observables_device": (i, [P, i, C.c_void_p, C.c_void_p]),
         "pyro_tet_set_forward": (i, [P, i]),
         "pyro_tet_gradient": (i, [P, pf, pf, i, pf, pd]),
         "pyro_cycle_tet": (i, [P, i, i, i, i, i]),
@@ -300,6 +301,10 @@ class Engine:
     def set_stream(self, stream_handle: int) -> None:
         self._ck(self.lib.pyro_set_stream(self.ctx, C.c_void_p(stream_handle)))
 
+    def stream_handle(self) -> int:
+        """The cudaStream_t the context queues its work on (as an integer)."""
+        return int(self.lib.pyro_get_stream(self.ctx) or 0)
+
     def synchronize(self) -> None:
         self._ck(self.lib.pyro_synchronize(self.ctx))
 
@@ -436,6 +441,11 @@ class Engine:
         self._ck(self.lib.pyro_observables(self.ctx, system, _ptr(e, C.c_double),
                                            _ptr(m, C.c_double)))
         return e, m
+
+    def last_observables_device(self, e_ptr: int, m_ptr: int = 0, system: int = 0) -> None:
+        """Energies (and magnetisations) of the last cycle, without recomputing."""
+        self._ck(self.lib.pyro_last_observables_device(self.ctx, system, e_ptr or None,
+                                                       m_ptr or None))
 
     def observables_device(self, e_ptr: int, m_ptr: int = 0, system: int = 0) -> None:
         self._ck(self.lib.pyro_observables_device(self.ctx, system, C.c_void_p(e_ptr),

@@ -175,6 +175,11 @@ int pyro_observables(pyro_ctx* ctx, int system, double* energy, double* magnetis
 /* Stream-ordered variant into device buffers (n_replicas and 3 n_replicas). */
 int pyro_observables_device(pyro_ctx* ctx, int system, double* dev_energy,
                             double* dev_magnetisation3);
+/* The energies / magnetisations of the last pyro_cycle (computed at the end
+ * of every cycle without learned moves) or pyro_observables* call, copied to
+ * device memory without recomputing them (replica order, stream-ordered). */
+int pyro_last_observables_device(pyro_ctx* ctx, int system, double* dev_energy,
+                                 double* dev_magnetisation3);
 
 /* Temperatures. temperature_of_replica: T of each configuration slot (the
  * reference's permuted `Temperatures` vector); replica_of_temperature: the
