@@ -122,6 +122,94 @@ __device__ double energy2_share(const float4* lat, const NbrTable& tab, const Sy
   return e;
 }
 
+// Isotropic J1-only systems: the colour pass with L and the neighbour
+// offsets as compile-time constants (periodic wraps by selects, cell decode
+// by constant division). Same arithmetic as the generic pass.
+template <int L, int S, int K>
+__device__ __forceinline__ int j1_nbr(int x, int y, int z) {
+  constexpr NbrEntry e = j1_neighbour(S, K);
+  static_assert(e.t >= 0, "neighbour table");
+  const int xx = e.dx == 0 ? x : (e.dx > 0 ? (x == L - 1 ? 0 : x + 1) : (x == 0 ? L - 1 : x - 1));
+  const int yy = e.dy == 0 ? y : (e.dy > 0 ? (y == L - 1 ? 0 : y + 1) : (y == 0 ? L - 1 : y - 1));
+  const int zz = e.dz == 0 ? z : (e.dz > 0 ? (z == L - 1 ? 0 : z + 1) : (z == 0 ? L - 1 : z - 1));
+  return (zz * L + yy) * L + xx + e.t * L * L * L;
+}
+
+template <int L, int S, bool kMetro>
+__device__ __forceinline__ int j1_site_smem(float4* lat, int cell, float J1, float beta,
+                                            float cosmax, uint32_t rkey, uint32_t sweep32,
+                                            bool renorm, uint32_t seed_lo, uint32_t seed_hi) {
+  constexpr int L3 = L * L * L;
+  const int x = cell % L, y = (cell / L) % L, z = cell / (L * L);
+  const float4 n0 = lat[j1_nbr<L, S, 0>(x, y, z)], n1 = lat[j1_nbr<L, S, 1>(x, y, z)],
+               n2 = lat[j1_nbr<L, S, 2>(x, y, z)], n3 = lat[j1_nbr<L, S, 3>(x, y, z)],
+               n4 = lat[j1_nbr<L, S, 4>(x, y, z)], n5 = lat[j1_nbr<L, S, 5>(x, y, z)];
+  pyro_vec3 h;
+  h.x = J1 * (((((n0.x + n1.x) + n2.x) + n3.x) + n4.x) + n5.x);
+  h.y = J1 * (((((n0.y + n1.y) + n2.y) + n3.y) + n4.y) + n5.y);
+  h.z = J1 * (((((n0.z + n1.z) + n2.z) + n3.z) + n4.z) + n5.z);
+  const int own = S * L3 + cell;
+  const float4 sv = lat[own];
+  pyro_vec3 sp;
+  sp.x = sv.x;
+  sp.y = sv.y;
+  sp.z = sv.z;
+  pyro_vec3 out;
+  int a = 0;
+  if (kMetro) {
+    uint32_t r[4];
+    pyro_philox((uint32_t)own, rkey, sweep32, PYRO_PURPOSE_METRO, seed_lo, seed_hi, r);
+    const pyro_vec3 prop = pyro_cone_proposal(sp, cosmax, pyro_uniform(r[0]), pyro_uniform(r[1]));
+    a = pyro_metropolis_accept(pyro_delta_e(h, sp, prop), beta, pyro_uniform(r[2]));
+    out = a ? prop : sp;
+  } else {
+    out = pyro_overrelax(sp, h);
+  }
+  if (renorm) out = pyro_renormalise(out);
+  lat[own] = make_float4(out.x, out.y, out.z, 0.0f);
+  return a;
+}
+
+// Colour B of the 4-colour schedule: sites B, 4+B, 8+B, 12+B of every cell.
+template <int L, int B, bool kMetro>
+__device__ __forceinline__ unsigned long long j1_pass_smem(float4* lat, float J1, float beta,
+                                                           float cosmax, uint32_t rkey,
+                                                           uint32_t sweep32, bool renorm,
+                                                           uint32_t seed_lo, uint32_t seed_hi) {
+  constexpr int L3 = L * L * L;
+  unsigned long long acc = 0;
+  for (int u = threadIdx.x; u < 4 * L3; u += blockDim.x) {
+    const int k = u / L3, cell = u - k * L3;
+    switch (k) {
+      case 0: acc += j1_site_smem<L, B, kMetro>(lat, cell, J1, beta, cosmax, rkey, sweep32, renorm, seed_lo, seed_hi); break;
+      case 1: acc += j1_site_smem<L, 4 + B, kMetro>(lat, cell, J1, beta, cosmax, rkey, sweep32, renorm, seed_lo, seed_hi); break;
+      case 2: acc += j1_site_smem<L, 8 + B, kMetro>(lat, cell, J1, beta, cosmax, rkey, sweep32, renorm, seed_lo, seed_hi); break;
+      default: acc += j1_site_smem<L, 12 + B, kMetro>(lat, cell, J1, beta, cosmax, rkey, sweep32, renorm, seed_lo, seed_hi); break;
+    }
+  }
+  return acc;
+}
+
+template <int L, bool kMetro>
+__device__ __forceinline__ unsigned long long j1_sweep_smem(float4* lat, float J1, float beta,
+                                                            float cosmax, uint32_t rkey,
+                                                            uint32_t sweep32, bool renorm,
+                                                            uint32_t seed_lo, uint32_t seed_hi) {
+  unsigned long long acc = 0;
+  acc += j1_pass_smem<L, 0, kMetro>(lat, J1, beta, cosmax, rkey, sweep32, renorm, seed_lo, seed_hi);
+  __syncthreads();
+  acc += j1_pass_smem<L, 1, kMetro>(lat, J1, beta, cosmax, rkey, sweep32, renorm, seed_lo, seed_hi);
+  __syncthreads();
+  acc += j1_pass_smem<L, 2, kMetro>(lat, J1, beta, cosmax, rkey, sweep32, renorm, seed_lo, seed_hi);
+  __syncthreads();
+  acc += j1_pass_smem<L, 3, kMetro>(lat, J1, beta, cosmax, rkey, sweep32, renorm, seed_lo, seed_hi);
+  __syncthreads();
+  return acc;
+}
+
+// kL = 0: any system (neighbour table at run time); kL > 0: an isotropic
+// J1-only system of that L (compile-time offsets).
+template <int kL>
 __global__ void __launch_bounds__(kSmemThreads) smem_cycles_kernel(const SmemCycleParams p,
                                                                    const NbrTable tab) {
   extern __shared__ float4 lat[];
@@ -146,6 +234,13 @@ __global__ void __launch_bounds__(kSmemThreads) smem_cycles_kernel(const SmemCyc
       const bool metro = k < p.n_metro;
       const bool renorm =
           p.renorm_every > 0 && ((sweep + 1) % (unsigned long long)p.renorm_every) == 0;
+      if constexpr (kL > 0) {
+        acc += metro ? j1_sweep_smem<kL, true>(lat, sd.J1, beta, cosmax, rkey, (uint32_t)sweep,
+                                               renorm, p.seed_lo, p.seed_hi)
+                     : j1_sweep_smem<kL, false>(lat, sd.J1, beta, cosmax, rkey, (uint32_t)sweep,
+                                                renorm, p.seed_lo, p.seed_hi);
+        continue;
+      }
       for (int colour = 0; colour < sd.n_colours; ++colour) {
         for (int u = threadIdx.x; u < sd.units_per_colour; u += blockDim.x) {
           const int kk = u / L3, cell = u - kk * L3;
@@ -244,13 +339,34 @@ __global__ void __launch_bounds__(kSmemThreads) smem_cycles_kernel(const SmemCyc
 
 size_t smem_cycle_bytes(int L) { return sizeof(float4) * 16 * (size_t)L * L * L; }
 
-cudaError_t launch_smem_cycles(const SmemCycleParams& p, const NbrTable& tab, cudaStream_t st) {
-  const size_t bytes = smem_cycle_bytes(p.sys.L);
-  cudaError_t e = cudaFuncSetAttribute(smem_cycles_kernel,
+namespace {
+template <int kL>
+cudaError_t launch_smem(const SmemCycleParams& p, const NbrTable& tab, size_t bytes,
+                        cudaStream_t st) {
+  cudaError_t e = cudaFuncSetAttribute(smem_cycles_kernel<kL>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   if (e != cudaSuccess) return e;
-  smem_cycles_kernel<<<p.sys.n_rep, kSmemThreads, bytes, st>>>(p, tab);
+  smem_cycles_kernel<kL><<<p.sys.n_rep, kSmemThreads, bytes, st>>>(p, tab);
   return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_smem_cycles(const SmemCycleParams& p, const NbrTable& tab, cudaStream_t st) {
+  const size_t bytes = smem_cycle_bytes(p.sys.L);
+  const SysDev& s = p.sys;
+  if (s.n_colours == 4 && s.shells == 1 && s.exch < 0) {
+    switch (s.L) {
+      case 2: return launch_smem<2>(p, tab, bytes, st);
+      case 3: return launch_smem<3>(p, tab, bytes, st);
+      case 4: return launch_smem<4>(p, tab, bytes, st);
+      case 5: return launch_smem<5>(p, tab, bytes, st);
+      case 6: return launch_smem<6>(p, tab, bytes, st);
+      case 7: return launch_smem<7>(p, tab, bytes, st);
+      case 8: return launch_smem<8>(p, tab, bytes, st);
+      default: break;
+    }
+  }
+  return launch_smem<0>(p, tab, bytes, st);
 }
 
 }  // namespace pyro
