@@ -76,3 +76,42 @@ def test_fp32_engine_matches_fp64_host_run():
             worst = max(worst, z)
             assert z < 3.0, ("S(q)", T, q, a, da, b, db)
     print(f"largest deviation: {worst:.2f} sigma")
+
+
+def test_anisotropic_model_matches_fp64_host_run():
+    """The reference's J1-J4 model with a field: energy and specific heat of
+    the FP32 engine against an independent FP64 host chain (the matrix and
+    field paths of both)."""
+    from cudacode_b200.engine import reference_exchange, reference_field
+    A = reference_exchange(0.4, -0.3, 0.2, 0.35)
+    f = 3.0 * reference_field(2.4, 0.3, [0.3, -0.2, 1.0])
+    temps = [0.08, 0.3]
+    s = System(L=L, temperatures=temps, J1=0.0)
+    n = s.n_sites
+
+    def chain(obj, is_engine):
+        obj.set_exchange(A, f)
+        obj.set_cone(np.array([0.5, -0.2], dtype=np.float32))
+        obj.init_random()
+        obj.cycle(1, 2, False, 2000)
+        if is_engine:
+            obj.enable_history(CYCLES)
+            obj.cycle(1, 2, False, CYCLES)
+            return obj.history()
+        return obj.cycle(1, 2, False, CYCLES, record=True)
+
+    e32 = chain(Engine([s], seed=303), True)
+    e64 = chain(Oracle([s], seed=404, fp64=True, threads=4), False)
+    worst = 0.0
+    for t, T in enumerate(temps):
+        m1, d1 = stats.mean_error(e32[:, t] / n)
+        m2, d2 = stats.mean_error(e64[:, t] / n)
+        z = abs(m1 - m2) / np.hypot(d1, d2)
+        worst = max(worst, z)
+        assert z < 3.0, ("E", T, m1, d1, m2, d2)
+        c1, dc1 = batch_heat(e32[:, t], T, n)
+        c2, dc2 = batch_heat(e64[:, t], T, n)
+        z = abs(c1 - c2) / np.hypot(dc1, dc2)
+        worst = max(worst, z)
+        assert z < 3.0, ("C", T, c1, dc1, c2, dc2)
+    print(f"largest deviation: {worst:.2f} sigma")
