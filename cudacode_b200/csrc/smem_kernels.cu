@@ -239,63 +239,63 @@ __global__ void __launch_bounds__(kSmemThreads) smem_cycles_kernel(const SmemCyc
                                                renorm, p.seed_lo, p.seed_hi)
                      : j1_sweep_smem<kL, false>(lat, sd.J1, beta, cosmax, rkey, (uint32_t)sweep,
                                                 renorm, p.seed_lo, p.seed_hi);
-        continue;
-      }
-      for (int colour = 0; colour < sd.n_colours; ++colour) {
-        for (int u = threadIdx.x; u < sd.units_per_colour; u += blockDim.x) {
-          const int kk = u / L3, cell = u - kk * L3;
-          const int s = colour_site(sd.n_colours, colour, kk);
-          const int x = cell % L, yz = cell / L, y = yz % L, z = yz / L;
-          const int own = s * L3 + cell;
-          pyro_vec3 h;
-          if (sd.exch >= 0) {
-            h = exch_field_smem(lat, tab, p.exch[sd.exch], s, x, y, z, L, L3);
-          } else {
-            const float3 a1 = shell_sum_smem(lat, tab, s, 0, 6, x, y, z, L, L3);
-            h.x = sd.J1 * a1.x;
-            h.y = sd.J1 * a1.y;
-            h.z = sd.J1 * a1.z;
+      } else {
+        for (int colour = 0; colour < sd.n_colours; ++colour) {
+          for (int u = threadIdx.x; u < sd.units_per_colour; u += blockDim.x) {
+            const int kk = u / L3, cell = u - kk * L3;
+            const int s = colour_site(sd.n_colours, colour, kk);
+            const int x = cell % L, yz = cell / L, y = yz % L, z = yz / L;
+            const int own = s * L3 + cell;
+            pyro_vec3 h;
+            if (sd.exch >= 0) {
+              h = exch_field_smem(lat, tab, p.exch[sd.exch], s, x, y, z, L, L3);
+            } else {
+              const float3 a1 = shell_sum_smem(lat, tab, s, 0, 6, x, y, z, L, L3);
+              h.x = sd.J1 * a1.x;
+              h.y = sd.J1 * a1.y;
+              h.z = sd.J1 * a1.z;
+            }
+            if (sd.shells & 2) {
+              const float3 a = shell_sum_smem(lat, tab, s, 6, 18, x, y, z, L, L3);
+              h.x = fmaf(sd.J2, a.x, h.x);
+              h.y = fmaf(sd.J2, a.y, h.y);
+              h.z = fmaf(sd.J2, a.z, h.z);
+            }
+            if (sd.shells & 4) {
+              const float3 a = shell_sum_smem(lat, tab, s, 18, 24, x, y, z, L, L3);
+              h.x = fmaf(sd.J3a, a.x, h.x);
+              h.y = fmaf(sd.J3a, a.y, h.y);
+              h.z = fmaf(sd.J3a, a.z, h.z);
+            }
+            if (sd.shells & 8) {
+              const float3 a = shell_sum_smem(lat, tab, s, 24, 30, x, y, z, L, L3);
+              h.x = fmaf(sd.J3b, a.x, h.x);
+              h.y = fmaf(sd.J3b, a.y, h.y);
+              h.z = fmaf(sd.J3b, a.z, h.z);
+            }
+            const float4 sv = lat[own];
+            pyro_vec3 sp;
+            sp.x = sv.x;
+            sp.y = sv.y;
+            sp.z = sv.z;
+            pyro_vec3 out;
+            if (metro) {
+              uint32_t r[4];
+              pyro_philox((uint32_t)own, rkey, (uint32_t)sweep, PYRO_PURPOSE_METRO, p.seed_lo,
+                          p.seed_hi, r);
+              const pyro_vec3 prop =
+                  pyro_cone_proposal(sp, cosmax, pyro_uniform(r[0]), pyro_uniform(r[1]));
+              const int a = pyro_metropolis_accept(pyro_delta_e(h, sp, prop), beta, pyro_uniform(r[2]));
+              acc += (unsigned long long)a;
+              out = a ? prop : sp;
+            } else {
+              out = pyro_overrelax(sp, h);
+            }
+            if (renorm) out = pyro_renormalise(out);
+            lat[own] = make_float4(out.x, out.y, out.z, 0.0f);
           }
-          if (sd.shells & 2) {
-            const float3 a = shell_sum_smem(lat, tab, s, 6, 18, x, y, z, L, L3);
-            h.x = fmaf(sd.J2, a.x, h.x);
-            h.y = fmaf(sd.J2, a.y, h.y);
-            h.z = fmaf(sd.J2, a.z, h.z);
-          }
-          if (sd.shells & 4) {
-            const float3 a = shell_sum_smem(lat, tab, s, 18, 24, x, y, z, L, L3);
-            h.x = fmaf(sd.J3a, a.x, h.x);
-            h.y = fmaf(sd.J3a, a.y, h.y);
-            h.z = fmaf(sd.J3a, a.z, h.z);
-          }
-          if (sd.shells & 8) {
-            const float3 a = shell_sum_smem(lat, tab, s, 24, 30, x, y, z, L, L3);
-            h.x = fmaf(sd.J3b, a.x, h.x);
-            h.y = fmaf(sd.J3b, a.y, h.y);
-            h.z = fmaf(sd.J3b, a.z, h.z);
-          }
-          const float4 sv = lat[own];
-          pyro_vec3 sp;
-          sp.x = sv.x;
-          sp.y = sv.y;
-          sp.z = sv.z;
-          pyro_vec3 out;
-          if (metro) {
-            uint32_t r[4];
-            pyro_philox((uint32_t)own, rkey, (uint32_t)sweep, PYRO_PURPOSE_METRO, p.seed_lo,
-                        p.seed_hi, r);
-            const pyro_vec3 prop =
-                pyro_cone_proposal(sp, cosmax, pyro_uniform(r[0]), pyro_uniform(r[1]));
-            const int a = pyro_metropolis_accept(pyro_delta_e(h, sp, prop), beta, pyro_uniform(r[2]));
-            acc += (unsigned long long)a;
-            out = a ? prop : sp;
-          } else {
-            out = pyro_overrelax(sp, h);
-          }
-          if (renorm) out = pyro_renormalise(out);
-          lat[own] = make_float4(out.x, out.y, out.z, 0.0f);
+          __syncthreads();
         }
-        __syncthreads();
       }
     }
     if (p.history) {

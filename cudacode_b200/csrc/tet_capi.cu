@@ -114,6 +114,7 @@ TetMoveParams move_params(pyro_ctx* ctx, int si, unsigned long long off) {
   p.seed_hi = (uint32_t)(ctx->seed >> 32);
   p.image = ctx->tet->d_image;
   p.pdl = ctx->pdl;
+  p.err = ctx->tet->d_err;
   return p;
 }
 
@@ -166,7 +167,7 @@ int queue_tet_sweeps(pyro_ctx* ctx, int n) {
     for (int f = 0; f < 4; ++f)
       for (int si = 0; si < (int)ctx->sys.size(); ++si) {
         if (!j1_only_system(ctx->sys[si])) continue;
-        launch_tet_move(move_params(ctx, si, (unsigned long long)k), f, t->sweep_kernel == 2,
+        launch_tet_move(move_params(ctx, si, (unsigned long long)k), f, t->sweep_kernel,
                         ctx->stream);
         PYRO_CK_LAUNCH();
       }
@@ -196,6 +197,8 @@ int pyro_tet_init(pyro_ctx* ctx, uint64_t seed, long long sample_capacity) {
   PYRO_CK(cudaMalloc((void**)&t->d_v, sizeof(float) * kMlpParams));
   PYRO_CK(cudaMalloc((void**)&t->d_grad, sizeof(float) * kMlpParams));
   PYRO_CK(cudaMalloc((void**)&t->d_image, kImgTotal));
+  PYRO_CK(cudaMalloc((void**)&t->d_err, sizeof(int)));
+  PYRO_CK(cudaMemset(t->d_err, 0, sizeof(int)));
   PYRO_CK(cudaMalloc((void**)&t->d_ctr, sizeof(unsigned long long)));
   PYRO_CK(cudaMalloc((void**)&t->d_accepted, sizeof(unsigned long long) * ctx->total_temps));
   PYRO_CK(cudaMalloc((void**)&t->d_loss, sizeof(double)));
@@ -246,7 +249,7 @@ int pyro_tet_get_weights(pyro_ctx* ctx, float* w, int n) {
 int pyro_tet_set_kernel(pyro_ctx* ctx, int cluster) {
   int rc = need_tet(ctx);
   if (rc) return rc;
-  if (cluster < 0 || cluster > 2) return fail(ctx, PYRO_ERR_ARG, "tet kernel option is 0, 1 or 2");
+  if (cluster < 0 || cluster > 3) return fail(ctx, PYRO_ERR_ARG, "tet kernel option is 0..3");
   PYRO_CK(cudaSetDevice(ctx->device));
   PYRO_CK(cudaStreamSynchronize(ctx->stream));
   ctx->tet->sweep_kernel = cluster;
@@ -280,6 +283,13 @@ int pyro_tet_acceptance(pyro_ctx* ctx, int system, uint64_t* accepted, uint64_t*
   if (proposed)
     for (int t = 0; t < s.n_temp; ++t)
       proposed[t] = s.n_rep == s.n_temp ? (uint64_t)4 * s.L3 * ctx->tet->proposed_sweeps : 0;
+  int err = 0;
+  PYRO_CK(cudaMemcpy(&err, ctx->tet->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) {
+    cudaMemset(ctx->tet->d_err, 0, sizeof(int));
+    return fail(ctx, PYRO_ERR_TIMEOUT,
+                "tet: a tensor-core MMA of the learned move did not complete in time");
+  }
   return PYRO_OK;
 }
 
@@ -396,10 +406,6 @@ int pyro_tet_set_forward(pyro_ctx* ctx, int tensor_memory) {
 static int tet_forward_queue(pyro_ctx* ctx, const float* d_in, int n, float* d_out) {
   TetState* t = ctx->tet;
   if (t->forward_umma) {
-    if (!t->d_err) {
-      PYRO_CK(cudaMalloc((void**)&t->d_err, sizeof(int)));
-      PYRO_CK(cudaMemset(t->d_err, 0, sizeof(int)));
-    }
     PYRO_CK(launch_umma_forward(d_in, n, t->d_image, d_out, t->d_err, ctx->stream));
   } else {
     launch_mlp_forward(d_in, n, t->d_image, d_out, ctx->stream);

@@ -30,6 +30,7 @@
 #include "../../include/pyro_math.h"
 #include "lattice.h"
 #include "tet_mlp.cuh"
+#include "tet_umma.cuh"
 
 namespace pyro {
 namespace {
@@ -414,6 +415,38 @@ __device__ __forceinline__ SiteMove site_move(const float* o, pyro_vec3 s, uint3
   return m;
 }
 
+// Proposal, MH test and write-back of one tetrahedron of corner F from its
+// network outputs o[16], its fields h and spins s. Returns 1 if accepted.
+template <int F>
+__device__ __forceinline__ int tet_finish(const TetMoveParams& p, int rep, int cell, float beta,
+                                          unsigned long long sweep, const pyro_vec3 h[4],
+                                          const pyro_vec3 s[4], const float* o) {
+  const uint32_t key_tet = (uint32_t)(F * p.L3 + cell);
+  uint32_t r0[4], r1[4], r2[4];
+  pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + 0,
+              p.seed_lo, p.seed_hi, r0);
+  pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + 1,
+              p.seed_lo, p.seed_hi, r1);
+  pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + 2,
+              p.seed_lo, p.seed_hi, r2);
+  const SiteMove m0 = site_move(o + 0, s[0], r0[0], r0[1]);
+  const SiteMove m1 = site_move(o + 4, s[1], r0[2], r0[3]);
+  const SiteMove m2 = site_move(o + 8, s[2], r1[0], r1[1]);
+  const SiteMove m3 = site_move(o + 12, s[3], r1[2], r1[3]);
+  const pyro_vec3 sn[4] = {m0.sn, m1.sn, m2.sn, m3.sn};
+  const float dE = tet_energy(sn, h, p.J1) - tet_energy(s, h, p.J1);
+  const float log_q = (m0.lq + m1.lq) + (m2.lq + m3.lq);
+  const float log_r = -beta * dE + log_q;
+  const int accepted = log_r >= 0.0f || tet_uniform(r2[0]) < __expf(log_r);
+  if (accepted) {
+    float4* wb = p.spins + (long long)rep * 16 * p.L3;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      wb[(4 * F + k) * p.L3 + cell] = make_float4(sn[k].x, sn[k].y, sn[k].z, 0.0f);
+  }
+  return accepted;
+}
+
 // One warp's 32 tetrahedra of corner F (one per lane; lanes with
 // active == false only feed the warp-wide MMAs): features, network, vMF
 // proposals, MH test, write-back. Returns 1 if this lane's move was accepted.
@@ -459,29 +492,7 @@ __device__ __forceinline__ int tet_warp_step(const TetMoveParams& p, const MlpSm
     float o[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) o[i] = out[lane * kLdOut + i];
-    const uint32_t key_tet = (uint32_t)(F * p.L3 + cell);
-    uint32_t r0[4], r1[4], r2[4];
-    pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + 0,
-                p.seed_lo, p.seed_hi, r0);
-    pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + 1,
-                p.seed_lo, p.seed_hi, r1);
-    pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + 2,
-                p.seed_lo, p.seed_hi, r2);
-    const SiteMove m0 = site_move(o + 0, s[0], r0[0], r0[1]);
-    const SiteMove m1 = site_move(o + 4, s[1], r0[2], r0[3]);
-    const SiteMove m2 = site_move(o + 8, s[2], r1[0], r1[1]);
-    const SiteMove m3 = site_move(o + 12, s[3], r1[2], r1[3]);
-    const pyro_vec3 sn[4] = {m0.sn, m1.sn, m2.sn, m3.sn};
-    const float dE = tet_energy(sn, h, p.J1) - tet_energy(s, h, p.J1);
-    const float log_q = (m0.lq + m1.lq) + (m2.lq + m3.lq);
-    const float log_r = -beta * dE + log_q;
-    accepted = log_r >= 0.0f || tet_uniform(r2[0]) < __expf(log_r);
-    if (accepted) {
-      float4* wb = p.spins + (long long)rep * 16 * p.L3;
-#pragma unroll
-      for (int k = 0; k < 4; ++k)
-        wb[(4 * F + k) * p.L3 + cell] = make_float4(sn[k].x, sn[k].y, sn[k].z, 0.0f);
-    }
+    accepted = tet_finish<F>(p, rep, cell, beta, sweep, h, s, o);
   }
   return accepted;
 }
@@ -659,6 +670,66 @@ __global__ void __launch_bounds__(kTetMoveThreads) tet_move_pair_kernel(const Te
                                           feat_all + warp * 32 * kLdIn,
                                           out_all + warp * 32 * kLdOut);
   count_accepted(p, tslot, acc);
+}
+
+// The move with the network on the 5th-generation tensor cores: one thread
+// per tetrahedron, 128 per CTA (tensor-memory lane = thread = row); fields
+// and spins as tet_warp_step, the network of tet_umma.cuh, then the same
+// proposal and MH test. A wait that runs out sets *p.err and skips the moves
+// of the CTA.
+template <int F>
+__global__ void __launch_bounds__(umma::kURows) tet_move_umma_kernel(const TetMoveParams p) {
+  pass_prologue();
+  extern __shared__ __align__(16) unsigned char smem[];
+  umma::stage_network(smem, p.image);
+  umma::setup(smem);
+  const long long tet = (long long)blockIdx.x * umma::kURows + threadIdx.x;  // rep * L3 + cell
+  const bool active = tet < (long long)p.n_rep * p.L3;
+  const int rep = active ? (int)(tet / p.L3) : 0;
+  const int cell = active ? (int)(tet - (long long)rep * p.L3) : 0;
+  const int tslot = p.temp_of_rep[p.temp_base + p.rep_global + rep];
+  const float beta = p.beta[p.temp_base + tslot];
+  const unsigned long long sweep = (p.tet_ctr ? *p.tet_ctr : 0ull) + p.tet_off;
+  const float4* rb = p.spins + (long long)rep * 16 * p.L3;
+  pyro_vec3 h[4], s[4];
+  if (active) {
+    const Frame fr = cell_frame(cell, p.L, p.rcpL);
+    tet_fields<F, false>(rb, fr, p.L3, p.J1, h);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float4 v = __ldg(rb + (4 * F + k) * p.L3 + cell);
+      s[k].x = v.x;
+      s[k].y = v.y;
+      s[k].z = v.z;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      h[k].x = h[k].y = h[k].z = 0.0f;
+      s[k].x = s[k].y = 0.0f;
+      s[k].z = 1.0f;
+    }
+  }
+  // features, rounded to BF16 as write_features does
+  float x[kMlpIn];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    x[3 * k] = h[k].x * (1.0f / 3.0f);
+    x[3 * k + 1] = h[k].y * (1.0f / 3.0f);
+    x[3 * k + 2] = h[k].z * (1.0f / 3.0f);
+  }
+  x[12] = logf(active ? beta : 1.0f) * (1.0f / 3.0f);
+  x[13] = x[14] = x[15] = 0.0f;
+  umma::store_row(smem + umma::kUA0, threadIdx.x, kMlpIn, x);
+  const uint32_t tmem = umma::ready(smem);
+  uint32_t parity = 0;
+  float o[kMlpOut];
+  const bool ok = umma::network(smem, tmem, o, &parity);
+  int acc = 0;
+  if (ok && active) acc = tet_finish<F>(p, rep, cell, beta, sweep, h, s, o);
+  if (!ok && threadIdx.x == 0 && p.err) atomicExch(p.err, 1);
+  count_accepted(p, tslot, acc);
+  umma::teardown(smem, tmem, ok, parity);
 }
 
 __device__ __forceinline__ void cluster_sync_all() {
@@ -1101,9 +1172,29 @@ void launch_move(Kernel k, int blocks, const TetMoveParams& p, cudaStream_t st) 
 }
 }  // namespace
 
-void launch_tet_move(const TetMoveParams& p, int f, bool pair_mode, cudaStream_t st) {
+void launch_tet_move(const TetMoveParams& p, int f, int form, cudaStream_t st) {
   const long long n = (long long)p.n_rep * p.L3;
-  if (pair_mode) {
+  if (form == 3) {
+    const int blocks = (int)((n + umma::kURows - 1) / umma::kURows);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks, 1, 1);
+    cfg.blockDim = dim3(umma::kURows, 1, 1);
+    cfg.dynamicSmemBytes = umma::kUSmem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = p.pdl ? 1 : 0;
+    switch (f) {
+      case 0: cudaLaunchKernelEx(&cfg, tet_move_umma_kernel<0>, p); break;
+      case 1: cudaLaunchKernelEx(&cfg, tet_move_umma_kernel<1>, p); break;
+      case 2: cudaLaunchKernelEx(&cfg, tet_move_umma_kernel<2>, p); break;
+      default: cudaLaunchKernelEx(&cfg, tet_move_umma_kernel<3>, p); break;
+    }
+    return;  // errors are read back with cudaGetLastError
+  }
+  if (form == 2) {
     const int half = kTetMoveThreads / 2;
     const int blocks = (int)((n + half - 1) / half);
     switch (f) {

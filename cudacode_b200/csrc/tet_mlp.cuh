@@ -69,6 +69,7 @@ struct TetMoveParams {
   uint32_t seed_lo, seed_hi;
   const unsigned char* image;  // kImgBytes weight image
   int pdl;                     // programmatic dependent launch of the per-pass kernels
+  int* err;                    // set to 1 if a tensor-core wait of the tcgen05 form ran out
 };
 
 struct TetCollectParams {
@@ -88,9 +89,12 @@ struct TetCollectParams {
 
 // Writes the weight image (kImgBytes) of the FP32 master weights.
 void launch_mlp_pack(const float* master, unsigned char* image, cudaStream_t st);
-// One pass of the learned move over up-tetrahedra of FCC corner f; pair_mode:
-// two lanes per tetrahedron (same decisions).
-void launch_tet_move(const TetMoveParams& p, int f, bool pair_mode, cudaStream_t st);
+// One pass of the learned move over up-tetrahedra of FCC corner f. form 0:
+// one lane per tetrahedron (mma.sync network); 2: two lanes per tetrahedron
+// (same decisions as 0); 3: the network on tcgen05 (tensor memory), one
+// thread per tetrahedron, 128 per CTA (same move, its own rounding of the
+// network's accumulations).
+void launch_tet_move(const TetMoveParams& p, int f, int form, cudaStream_t st);
 // n sweeps (4 corner passes each) of every replica in one launch, one
 // thread-block cluster of csize CTAs per replica.
 cudaError_t launch_tet_sweep_cluster(const TetMoveParams& p, int n_sweeps, int csize,

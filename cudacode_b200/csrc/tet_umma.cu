@@ -1,270 +1,43 @@
-// The learned proposal's network on the 5th-generation tensor cores, sm_100a.
-//
-// One CTA of 128 threads evaluates 128 feature rows: row r is thread r and
-// tensor-memory lane r. The three layers are tcgen05.mma (kind::f16, BF16
-// operands from shared memory in the canonical K-major core-matrix layout,
-// FP32 accumulators in tensor memory): M = 128, N = 64 / 64 / 16, K = 16 /
-// 64 / 64 (one MMA per 16-wide K slice). Thread 0 issues the MMAs and commits
-// them to an mbarrier; every thread waits on it (bounded), reads its row's
-// accumulators with tcgen05.ld, adds the bias, applies hard-swish, rounds to
-// BF16 and writes the row back to shared memory as the next layer's A
-// operand. The arithmetic is the same network as the mma.sync kernels (BF16
-// rounding points of the inputs, weights and hidden activations; FP32
-// accumulation), so both agree with the oracle's FP64 restatement within the
-// same tolerance.
+// Batched forward of the learned proposal's network on the 5th-generation
+// tensor cores (tet_umma.cuh), 128 feature rows per CTA; the arithmetic is
+// the same network as the mma.sync kernels (BF16 rounding points of inputs,
+// weights and hidden activations; FP32 accumulation), so both agree with the
+// oracle's FP64 restatement within the same tolerance.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "tet_mlp.cuh"
+#include "tet_umma.cuh"
 
 namespace pyro {
 namespace {
 
-constexpr int kURows = 128;
-constexpr int kUBias = kImgTotal - kImgU1;             // 12,288 B of core-matrix weights
-constexpr int kUA0 = kUBias + (2 * kMlpHidden + kMlpOut) * 4;  // 576 B of biases
-constexpr int kUA1 = kUA0 + kURows * kMlpIn * 2;        // A0: 128 x 16 bf16
-constexpr int kUBar = kUA1 + kURows * kMlpHidden * 2;   // A1: 128 x 64 bf16
-constexpr int kUSmem = kUBar + 16;                      // mbarrier + tensor-memory address
-constexpr int kUCols = 128;                             // tensor-memory columns held
-static_assert(kUA0 % 16 == 0 && kUA1 % 16 == 0 && kUBar % 8 == 0, "alignment");
-static_assert((kImgB1 % 16) == 0 && ((2 * kMlpHidden + kMlpOut) * 4) % 16 == 0, "bias copy");
-constexpr long long kWaitLimit = 1ll << 22;
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-// Shared-memory matrix descriptor: K-major, no swizzle; lbo = byte distance
-// between the two 8-element K chunks of a 16-wide slice, sbo = between 8-row
-// groups; version 1 (tcgen05).
-__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
-         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
-}
-
-// Instruction descriptor, kind::f16: FP32 accumulator, BF16 A and B, both
-// K-major, M = 128.
-__host__ __device__ constexpr uint32_t umma_idesc(int n) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
-         ((uint32_t)(kURows >> 4) << 24);
-}
-
-__device__ __forceinline__ void umma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
-                                     uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
-      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
-      : "memory");
-}
-
-__device__ __forceinline__ void umma_commit(uint32_t bar) {
-  asm volatile(
-      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
-      : "memory");
-}
-
-// Bounded wait for the mbarrier phase `parity`; false if it ran out.
-__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {
-  for (long long i = 0; i < kWaitLimit; ++i) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (ok) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void fence_before_sync() {
-  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-}
-__device__ __forceinline__ void fence_after_sync() {
-  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-}
-// Generic-proxy shared-memory writes made visible to the tensor cores.
-__device__ __forceinline__ void fence_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-}
-
-// 16 consecutive FP32 columns of this warp's 32 lanes (one row per thread).
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
-      "%15}, [%16];\n"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-__device__ __forceinline__ float hswish_u(float x) {
-  return x * fminf(fmaxf(x + 3.0f, 0.0f), 6.0f) * (1.0f / 6.0f);
-}
-
-__device__ __forceinline__ uint32_t pack2(float lo, float hi) {
-  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
-  return *reinterpret_cast<uint32_t*>(&v);
-}
-
-// Row `r` of an M x K operand in the core-matrix layout: K/8 chunks of 16 B.
-__device__ __forceinline__ void store_row(unsigned char* base, int r, int K, const float* x) {
-  for (int c = 0; c < K / 8; ++c) {
-    uint4 q;
-    q.x = pack2(x[8 * c + 0], x[8 * c + 1]);
-    q.y = pack2(x[8 * c + 2], x[8 * c + 3]);
-    q.z = pack2(x[8 * c + 4], x[8 * c + 5]);
-    q.w = pack2(x[8 * c + 6], x[8 * c + 7]);
-    *reinterpret_cast<uint4*>(base + (r / 8) * (K / 8) * 128 + c * 128 + (r % 8) * 16) = q;
-  }
-}
+using namespace umma;
 
 __global__ void __launch_bounds__(kURows) umma_forward_kernel(const float* __restrict__ features,
                                                               int n,
                                                               const unsigned char* __restrict__ image,
                                                               float* __restrict__ out, int* err) {
   extern __shared__ __align__(128) unsigned char smem[];
-  unsigned char* w = smem;                                // W1t | W2t | W3t (core layout)
-  const float* bias = reinterpret_cast<const float*>(smem + kUBias);  // b1 | b2 | b3
-  unsigned char* a0 = smem + kUA0;
-  unsigned char* a1 = smem + kUA1;
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kUBar + 8);
-  const uint32_t bar = smem_addr(smem + kUBar);
-  const int tid = threadIdx.x, warp = tid >> 5;
-
-  // weights and biases: 16-byte asynchronous copies
-  for (int i = tid * 16; i < kUBias; i += kURows * 16)
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(w + i)),
-                 "l"(image + kImgU1 + i)
-                 : "memory");
-  for (int i = tid * 16; i < (2 * kMlpHidden + kMlpOut) * 4; i += kURows * 16)
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(smem + kUBias + i)),
-                 "l"(image + kImgB1 + i)
-                 : "memory");
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
-                     smem_addr(tslot)),
-                 "r"(kUCols)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
-  }
-  if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-  }
-  // this thread's feature row -> A0
+  stage_network(smem, image);
+  setup(smem);
+  const int tid = threadIdx.x;
   const long long row = (long long)blockIdx.x * kURows + tid;
-  float x[kMlpHidden];
+  float x[kMlpIn];
 #pragma unroll
   for (int i = 0; i < kMlpIn; ++i) x[i] = row < n ? features[row * kMlpIn + i] : 0.0f;
-  store_row(a0, tid, kMlpIn, x);
-  asm volatile("cp.async.wait_all;\n" ::: "memory");
-  fence_async_smem();
-  fence_before_sync();
-  __syncthreads();
-  fence_after_sync();
-  const uint32_t tmem = *tslot;
-  const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-  const uint32_t a0s = smem_addr(a0), a1s = smem_addr(a1), ws = smem_addr(w);
-  bool ok = true;
+  store_row(smem + kUA0, tid, kMlpIn, x);
+  const uint32_t tmem = ready(smem);
   uint32_t parity = 0;
-
-  // layer 1: columns [0, 64) = A0 (128 x 16) . W1
-  if (tid == 0) {
-    umma(tmem, umma_desc(a0s, 128, 256), umma_desc(ws, 128, 256), umma_idesc(kMlpHidden), 0u);
-    umma_commit(bar);
-  }
-  ok = bar_wait(bar, parity);
-  if (ok) parity ^= 1u;
-  ok = __syncthreads_and(ok);
-  if (ok) {
-    fence_after_sync();
+  float o[kMlpOut];
+  const bool ok = network(smem, tmem, o, &parity);
+  if (ok && row < n) {
+    float4* dst = reinterpret_cast<float4*>(out + row * kMlpOut);
 #pragma unroll
-    for (int c = 0; c < kMlpHidden / 16; ++c) tmem_ld16(lane_base + 16 * c, x + 16 * c);
-#pragma unroll
-    for (int j = 0; j < kMlpHidden; ++j) x[j] = hswish_u(x[j] + bias[j]);
-    store_row(a1, tid, kMlpHidden, x);
-    fence_async_smem();
+    for (int q = 0; q < 4; ++q) dst[q] = make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
   }
-  fence_before_sync();
-  __syncthreads();
-  fence_after_sync();
-
-  // layer 2: columns [64, 128) = A1 (128 x 64) . W2, four K slices
-  if (ok) {
-    if (tid == 0) {
-      for (int kk = 0; kk < 4; ++kk)
-        umma(tmem + 64, umma_desc(a1s + kk * 256, 128, 1024),
-             umma_desc(ws + (kImgU2 - kImgU1) + kk * 256, 128, 1024), umma_idesc(kMlpHidden),
-             kk > 0 ? 1u : 0u);
-      umma_commit(bar);
-    }
-    ok = bar_wait(bar, parity);
-    if (ok) parity ^= 1u;
-  }
-  ok = __syncthreads_and(ok);
-  if (ok) {
-    fence_after_sync();
-#pragma unroll
-    for (int c = 0; c < kMlpHidden / 16; ++c) tmem_ld16(lane_base + 64 + 16 * c, x + 16 * c);
-#pragma unroll
-    for (int j = 0; j < kMlpHidden; ++j) x[j] = hswish_u(x[j] + bias[kMlpHidden + j]);
-    store_row(a1, tid, kMlpHidden, x);  // layer 2's reads of A1 completed with its commit
-    fence_async_smem();
-  }
-  fence_before_sync();
-  __syncthreads();
-  fence_after_sync();
-
-  // layer 3: columns [0, 16) = A1 (128 x 64) . W3
-  if (ok) {
-    if (tid == 0) {
-      for (int kk = 0; kk < 4; ++kk)
-        umma(tmem, umma_desc(a1s + kk * 256, 128, 1024),
-             umma_desc(ws + (kImgU3 - kImgU1) + kk * 256, 128, 1024), umma_idesc(kMlpOut),
-             kk > 0 ? 1u : 0u);
-      umma_commit(bar);
-    }
-    ok = bar_wait(bar, parity);
-    if (ok) parity ^= 1u;
-  }
-  ok = __syncthreads_and(ok);
-  if (ok) {
-    fence_after_sync();
-    tmem_ld16(lane_base, x);
-    if (row < n) {
-      float4* o = reinterpret_cast<float4*>(out + row * kMlpOut);
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-        o[q] = make_float4(x[4 * q] + bias[2 * kMlpHidden + 4 * q],
-                           x[4 * q + 1] + bias[2 * kMlpHidden + 4 * q + 1],
-                           x[4 * q + 2] + bias[2 * kMlpHidden + 4 * q + 2],
-                           x[4 * q + 3] + bias[2 * kMlpHidden + 4 * q + 3]);
-    }
-  } else if (tid == 0) {
-    atomicExch(err, 1);
-    // an MMA may still be in flight: give it (bounded) time before the
-    // tensor memory is released
-    bar_wait(bar, parity);
-  }
-  fence_before_sync();
-  __syncthreads();
-  if (warp == 0) {
-    fence_after_sync();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
-                 "r"(kUCols)
-                 : "memory");
-  }
+  if (!ok && tid == 0) atomicExch(err, 1);
+  teardown(smem, tmem, ok, parity);
 }
 
 }  // namespace

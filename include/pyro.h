@@ -319,7 +319,13 @@ int pyro_tet_get_weights(pyro_ctx* ctx, float* weights, int n);
 int pyro_tet_sweep(pyro_ctx* ctx, int n_sweeps);
 /* 0: one launch per corner pass, one lane per tetrahedron; 1: all passes of
  * a call in one launch, one thread-block cluster per replica; 2 (default):
- * one launch per corner pass, two lanes per tetrahedron. Identical results. */
+ * one launch per corner pass, two lanes per tetrahedron (0, 1 and 2 give
+ * identical results); 3: one launch per corner pass with the network on the
+ * 5th-generation tensor cores (tcgen05.mma, accumulators in tensor memory),
+ * 128 tetrahedra per CTA: the same move, with its own rounding of the
+ * network's accumulations. A tensor-core wait that runs out in form 3 skips
+ * the moves of its CTA and makes pyro_tet_acceptance return
+ * PYRO_ERR_TIMEOUT. */
 int pyro_tet_set_kernel(pyro_ctx* ctx, int mode);
 int pyro_tet_acceptance(pyro_ctx* ctx, int system, uint64_t* accepted, uint64_t* proposed);
 int pyro_tet_reset_acceptance(pyro_ctx* ctx);

@@ -103,10 +103,12 @@ def mean_and_error(x):
     return b.mean(), b.std(ddof=1) / np.sqrt(20)
 
 
-def test_learned_move_preserves_the_boltzmann_distribution():
+@pytest.mark.parametrize("form", [2, 3])
+def test_learned_move_preserves_the_boltzmann_distribution(form):
     """Tetrahedron moves alone (untrained network) and the plain method,
     both started from the same equilibrated spins, sample the same energy
-    distribution: detailed balance of the MH test."""
+    distribution: detailed balance of the MH test (form 3: the network on
+    tcgen05)."""
     temps = [0.4, 1.2]
     s = System(L=4, temperatures=temps)
     plain = Engine([s], seed=21)
@@ -120,6 +122,7 @@ def test_learned_move_preserves_the_boltzmann_distribution():
     tet = Engine([s], seed=22)
     tet.set_spins(start)
     tet.tet_init(seed=5)
+    tet.tet_set_kernel(form)
     e_tet = chain_energy(tet, 100, 2000, lambda: tet.tet_sweep(1))
     acc, prop = tet.tet_acceptance()
     assert (acc > 0).all()
@@ -188,3 +191,27 @@ def test_cluster_and_per_pass_tet_kernels_agree(L):
         assert np.array_equal(runs[0][0], runs[k][0])
         assert np.array_equal(runs[0][1], runs[k][1])
         assert np.array_equal(runs[0][2], runs[k][2])
+
+
+@pytest.mark.parametrize("L", [4, 7])
+def test_tensor_memory_move_matches_the_mma_sync_move_closely(L):
+    """Form 3 evaluates the same network on tcgen05; its accumulations round
+    differently, so the chains are not bit-identical, but one sweep from the
+    same state accepts almost the same moves and all spins stay unit."""
+    s = System(L=L, temperatures=[0.1, 0.3, 0.9])
+    runs = []
+    for form in (0, 3):
+        e = Engine([s], seed=41)
+        e.init_random()
+        e.tet_init(seed=2)
+        e.tet_set_kernel(form)
+        e.tet_sweep(1)
+        acc, prop = e.tet_acceptance()
+        runs.append((e.get_spins(), acc, prop))
+    a, b = runs[0][0], runs[1][0]
+    same = np.all(a == b, axis=-1)
+    assert same.mean() > 0.99
+    n = np.linalg.norm(b[..., :3], axis=-1)
+    assert np.abs(n - 1).max() < 1e-4
+    assert np.abs(runs[0][1].astype(np.int64) - runs[1][1].astype(np.int64)).max() <= \
+        max(2, int(0.01 * runs[0][2][0]))
