@@ -429,9 +429,12 @@ def run_aniso(args):
 
 
 def run_learned(args):
-    """Energy ESS/s of plain PT cycles (1 Metropolis + 4 over-relaxation
-    sweeps + exchange) against the same cycles with one learned tetrahedron
-    sweep added, at L=16, 8 temperatures on a geometric ladder in [0.05, 0.5].
+    """Energy ESS/s at T=0.05 of the learned method (plain PT cycles with
+    learned tetrahedron sweeps, at its best schedule) against the plain PT
+    cycle of the benchmark (1 Metropolis + 4 over-relaxation sweeps per
+    exchange) and against the plain method at its own best schedule
+    (`ratio_vs_plain_best_schedule`), at L=16, 8 temperatures on a geometric
+    ladder in [0.05, 0.5].
     The network is trained on the GPU on ~10^6 tetrahedra from the plain
     chains first. Device time by CUDA events; tau_int by Sokal windowing."""
     import torch
@@ -485,10 +488,30 @@ def run_learned(args):
                 "E_per_site": [(m / (16 * Ll ** 3), e / (16 * Ll ** 3)) for m, e in means],
                 "tet_acceptance": (acc / np.maximum(prop, 1)).tolist() if n_tet else None}
 
-    plain = measure(0)
-    schedules = [measure(1, 1, 4), measure(1, 1, 1), measure(1, 0, 1), measure(2, 0, 1)]
-    learned = max(schedules, key=lambda r: r["ess_per_s"][0])
+    # Schedules are chosen on one set of chains and the ratio is measured on
+    # fresh, longer chains of the two winners (no selection bias); the plain
+    # method gets its own best schedule.
+    plain_runs = [measure(0, 1, 4), measure(0, 1, 1), measure(0, 1, 2), measure(0, 2, 4)]
+    schedules = [measure(1, 1, 4), measure(1, 1, 1), measure(1, 0, 1), measure(2, 0, 1),
+                 measure(1, 1, 2)]
+    best_plain = max(plain_runs, key=lambda r: r["ess_per_s"][0])["schedule"]
+    best_learned = max(schedules, key=lambda r: r["ess_per_s"][0])["schedule"]
+    final_cycles = 3 * cycles
+
+    def remeasure(sch):
+        nonlocal cycles
+        keep, cycles = cycles, final_cycles
+        try:
+            return measure(sch["tetrahedron"], sch["metropolis"], sch["overrelax"])
+        finally:
+            cycles = keep
+
+    standard = {"metropolis": 1, "overrelax": 4, "tetrahedron": 0}
+    plain = remeasure(standard)  # the plain PT cycle of the benchmark (1 M + 4 OR)
+    plain_best = plain if best_plain == standard else remeasure(best_plain)
+    learned = remeasure(best_learned)
     ratio = learned["ess_per_s"][0] / plain["ess_per_s"][0]
+    ratio_best = learned["ess_per_s"][0] / plain_best["ess_per_s"][0]
     agree = [abs(p[0] - q[0]) / max(np.hypot(p[1], q[1]), 1e-30)
              for p, q in zip(plain["E_per_site"], learned["E_per_site"])]
     line = {"metric": "energy ESS/s learned-proposal vs plain at T=0.05", "value": ratio,
@@ -496,16 +519,22 @@ def run_learned(args):
             "warmup": args.warmup, "dtype": "f32 spins, bf16 MLP",
             "data": "synthetic (random unit spins from Philox seed)",
             "config": {"workload": "learned tetrahedron proposal: L=16 (65,536 sites), J1=1 AFM, "
-                                   "8 temperatures geometric in [0.05, 0.5], cycle = 1 Metropolis "
-                                   "+ 4 over-relaxation sweeps (+ 1 learned tetrahedron sweep) + "
-                                   "exchange", "training_samples": n_samples,
+                                   "8 temperatures geometric in [0.05, 0.5]; learned method at its "
+                                   "best schedule (chosen on separate chains) vs the plain 1 M + "
+                                   "4 OR cycle; ratio_vs_plain_best_schedule: vs the plain "
+                                   "method's own best schedule",
+                       "training_samples": n_samples,
                        "train_seconds": train_s, "loss_first": loss0, "loss_last": loss},
             "kernels_autotune_choice": choice,
             "plain": plain, "learned": learned,
+            "ratio_vs_plain_best_schedule": ratio_best, "plain_best": plain_best,
+            "selection_cycles": cycles, "final_cycles": final_cycles,
+            "plain_schedules": [{"schedule": r["schedule"], "us_per_cycle": r["us_per_cycle"],
+                                 "tau_int_T0.05": r["tau_int"][0],
+                                 "ess_per_s_T0.05": r["ess_per_s"][0]} for r in plain_runs],
             "learned_schedules": [{"schedule": r["schedule"], "us_per_cycle": r["us_per_cycle"],
                                    "tau_int_T0.05": r["tau_int"][0],
-                                   "ratio_T0.05": r["ess_per_s"][0] / plain["ess_per_s"][0]}
-                                  for r in schedules],
+                                   "ess_per_s_T0.05": r["ess_per_s"][0]} for r in schedules],
             "energy_agreement_sigma": agree}
     print(json.dumps(line), flush=True)
     return 0
