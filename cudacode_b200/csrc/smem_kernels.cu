@@ -190,11 +190,97 @@ __device__ __forceinline__ unsigned long long j1_pass_smem(float4* lat, float J1
   return acc;
 }
 
+// Spin-independent part of a Metropolis update: the Philox words of the
+// site and the cone geometry they give (cos, sin of the polar angle, the
+// azimuth's cos and sin, the acceptance uniform), exactly as
+// pyro_cone_proposal / pyro_metropolis_accept compute them.
+struct MetroDraw {
+  float ct, st, cp, sp, u3;
+};
+
+__device__ __forceinline__ MetroDraw metro_draw(uint32_t own, uint32_t rkey, uint32_t sweep32,
+                                                float cosmax, uint32_t seed_lo,
+                                                uint32_t seed_hi) {
+  uint32_t r[4];
+  pyro_philox(own, rkey, sweep32, PYRO_PURPOSE_METRO, seed_lo, seed_hi, r);
+  MetroDraw d;
+  d.ct = fmaf(-(1.0f - cosmax), pyro_uniform(r[0]), 1.0f);
+  d.st = sqrtf(fmaxf(0.0f, fmaf(-d.ct, d.ct, 1.0f)));
+  pyro_sincospif(2.0f * pyro_uniform(r[1]), &d.sp, &d.cp);
+  d.u3 = pyro_uniform(r[2]);
+  return d;
+}
+
+// Site S's Metropolis update from its precomputed draw.
+template <int L, int S>
+__device__ __forceinline__ int j1_metro_drawn(float4* lat, int cell, float J1, float beta,
+                                              const MetroDraw& d, bool renorm) {
+  constexpr int L3 = L * L * L;
+  const int x = cell % L, y = (cell / L) % L, z = cell / (L * L);
+  const float4 n0 = lat[j1_nbr<L, S, 0>(x, y, z)], n1 = lat[j1_nbr<L, S, 1>(x, y, z)],
+               n2 = lat[j1_nbr<L, S, 2>(x, y, z)], n3 = lat[j1_nbr<L, S, 3>(x, y, z)],
+               n4 = lat[j1_nbr<L, S, 4>(x, y, z)], n5 = lat[j1_nbr<L, S, 5>(x, y, z)];
+  pyro_vec3 h;
+  h.x = J1 * (((((n0.x + n1.x) + n2.x) + n3.x) + n4.x) + n5.x);
+  h.y = J1 * (((((n0.y + n1.y) + n2.y) + n3.y) + n4.y) + n5.y);
+  h.z = J1 * (((((n0.z + n1.z) + n2.z) + n3.z) + n4.z) + n5.z);
+  const int own = S * L3 + cell;
+  const float4 sv = lat[own];
+  pyro_vec3 sp;
+  sp.x = sv.x;
+  sp.y = sv.y;
+  sp.z = sv.z;
+  const pyro_vec3 prop = pyro_about_axis(sp, d.ct, d.st, d.cp, d.sp);
+  const int a = pyro_metropolis_accept(pyro_delta_e(h, sp, prop), beta, d.u3);
+  pyro_vec3 out = a ? prop : sp;
+  if (renorm) out = pyro_renormalise(out);
+  lat[own] = make_float4(out.x, out.y, out.z, 0.0f);
+  return a;
+}
+
+template <int L, int B>
+__device__ __forceinline__ int j1_metro_pass_drawn(float4* lat, float J1, float beta,
+                                                   const MetroDraw& d, bool renorm) {
+  constexpr int L3 = L * L * L;
+  const int u = threadIdx.x;
+  if (u >= 4 * L3) return 0;
+  const int k = u / L3, cell = u - k * L3;
+  switch (k) {
+    case 0: return j1_metro_drawn<L, B>(lat, cell, J1, beta, d, renorm);
+    case 1: return j1_metro_drawn<L, 4 + B>(lat, cell, J1, beta, d, renorm);
+    case 2: return j1_metro_drawn<L, 8 + B>(lat, cell, J1, beta, d, renorm);
+    default: return j1_metro_drawn<L, 12 + B>(lat, cell, J1, beta, d, renorm);
+  }
+}
+
 template <int L, bool kMetro>
 __device__ __forceinline__ unsigned long long j1_sweep_smem(float4* lat, float J1, float beta,
                                                             float cosmax, uint32_t rkey,
                                                             uint32_t sweep32, bool renorm,
                                                             uint32_t seed_lo, uint32_t seed_hi) {
+  constexpr int L3 = L * L * L;
+  if constexpr (kMetro && 4 * L3 <= kSmemThreads) {
+    // one site per thread and colour: the four draws of the sweep do not
+    // depend on the spins, so they are computed up front as four
+    // independent chains, off the passes' critical path
+    MetroDraw d[4];
+    const int u = threadIdx.x < 4 * L3 ? threadIdx.x : 0;
+    const int k = u / L3, cell = u - k * L3;
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+      d[b] = metro_draw((uint32_t)((4 * k + b) * L3 + cell), rkey, sweep32, cosmax, seed_lo,
+                        seed_hi);
+    unsigned long long acc = 0;
+    acc += j1_metro_pass_drawn<L, 0>(lat, J1, beta, d[0], renorm);
+    __syncthreads();
+    acc += j1_metro_pass_drawn<L, 1>(lat, J1, beta, d[1], renorm);
+    __syncthreads();
+    acc += j1_metro_pass_drawn<L, 2>(lat, J1, beta, d[2], renorm);
+    __syncthreads();
+    acc += j1_metro_pass_drawn<L, 3>(lat, J1, beta, d[3], renorm);
+    __syncthreads();
+    return acc;
+  }
   unsigned long long acc = 0;
   acc += j1_pass_smem<L, 0, kMetro>(lat, J1, beta, cosmax, rkey, sweep32, renorm, seed_lo, seed_hi);
   __syncthreads();
