@@ -663,7 +663,7 @@ def main():
     for _ in range(e2e_steps):
         eng.set_cone(cones_h.numpy())
         step()
-        E, M = eng.observables()
+        E, M = eng.last_observables()  # the energies the step computed
     e2e_s = time.perf_counter() - t0
     e2e_value = (R_PER_GPU * n_gpus * 16 * L ** 3 * (N_METRO + N_OR) * e2e_steps / (e2e_s * 1e9)
                  if e2e_steps else None)

@@ -1185,6 +1185,22 @@ int pyro_last_observables_device(pyro_ctx* ctx, int system, double* dev_energy,
   return PYRO_OK;
 }
 
+int pyro_last_observables(pyro_ctx* ctx, int system, double* energy, double* magnetisation3) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (system < 0 || system >= (int)ctx->sys.size())
+    return fail(ctx, PYRO_ERR_ARG, "last_observables: bad system");
+  PYRO_CK(cudaSetDevice(ctx->device));
+  const SysDev& s = ctx->sys[system];
+  if (energy)
+    PYRO_CK(cudaMemcpyAsync(energy, ctx->d_energy + s.rep_ctx_base, sizeof(double) * s.n_rep,
+                            cudaMemcpyDeviceToHost, ctx->stream));
+  if (magnetisation3)
+    PYRO_CK(cudaMemcpyAsync(magnetisation3, ctx->d_mag + 3 * s.rep_ctx_base,
+                            sizeof(double) * 3 * s.n_rep, cudaMemcpyDeviceToHost, ctx->stream));
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  return PYRO_OK;
+}
+
 int pyro_observables(pyro_ctx* ctx, int system, double* energy, double* magnetisation3) {
   if (!ctx) return PYRO_ERR_ARG;
   if (system < 0 || system >= (int)ctx->sys.size())

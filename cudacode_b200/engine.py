@@ -127,6 +127,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "pyro_tet_forward": (i, [P, pf, i, pf]),
         "pyro_tet_forward_device": (i, [P, C.c_void_p, i, C.c_void_p]),
         "pyro_last_observables_device": (i, [P, i, C.c_void_p, C.c_void_p]),
+        "pyro_last_observables": (i, [P, i, pd, pd]),
         "pyro_tet_set_forward": (i, [P, i]),
         "pyro_tet_gradient": (i, [P, pf, pf, i, pf, pd]),
         "pyro_cycle_tet": (i, [P, i, i, i, i, i]),
@@ -440,6 +441,15 @@ class Engine:
         m = np.empty((r, 3), dtype=np.float64)
         self._ck(self.lib.pyro_observables(self.ctx, system, _ptr(e, C.c_double),
                                            _ptr(m, C.c_double)))
+        return e, m
+
+    def last_observables(self, system: int = 0) -> tuple[np.ndarray, np.ndarray]:
+        """FP64 energies and magnetisations the last cycle computed (no recompute)."""
+        n = self.systems[system].replicas()
+        e = np.empty(n, dtype=np.float64)
+        m = np.empty((n, 3), dtype=np.float64)
+        self._ck(self.lib.pyro_last_observables(self.ctx, system, _ptr(e, C.c_double),
+                                                _ptr(m, C.c_double)))
         return e, m
 
     def last_observables_device(self, e_ptr: int, m_ptr: int = 0, system: int = 0) -> None:

@@ -180,6 +180,8 @@ int pyro_observables_device(pyro_ctx* ctx, int system, double* dev_energy,
  * device memory without recomputing them (replica order, stream-ordered). */
 int pyro_last_observables_device(pyro_ctx* ctx, int system, double* dev_energy,
                                  double* dev_magnetisation3);
+/* The same to host memory (synchronous). */
+int pyro_last_observables(pyro_ctx* ctx, int system, double* energy, double* magnetisation3);
 
 /* Temperatures. temperature_of_replica: T of each configuration slot (the
  * reference's permuted `Temperatures` vector); replica_of_temperature: the

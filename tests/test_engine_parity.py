@@ -443,3 +443,16 @@ def test_sharded_backend_reuses_the_cycle_energies(L):
     f = full.get_spins()
     for r, s in enumerate(shards):
         assert np.array_equal(s.get_spins(), f[3 * r:3 * r + 3])
+
+
+@pytest.mark.parametrize("L, swap, group", [(9, True, 0), (9, True, 2), (6, False, 0)])
+def test_last_observables_are_the_cycle_energies(L, swap, group):
+    s = System(L=L, temperatures=geometric_ladder(0.1, 1.0, 4))
+    e = Engine([s], seed=5)
+    e.set_option(e.OPT_REPLICA_GROUP, group)
+    e.init_random()
+    e.cycle(1, 2, swap, 3)
+    E0, M0 = e.last_observables()
+    E1, M1 = e.observables()
+    np.testing.assert_allclose(E0, E1, rtol=1e-12, atol=1e-9)
+    np.testing.assert_allclose(M0, M1.reshape(-1, 3), rtol=1e-12, atol=1e-9)
