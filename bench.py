@@ -491,9 +491,12 @@ def run_learned(args):
     # Schedules are chosen on one set of chains and the ratio is measured on
     # fresh, longer chains of the two winners (no selection bias); the plain
     # method gets its own best schedule.
-    plain_runs = [measure(0, 1, 4), measure(0, 1, 1), measure(0, 1, 2), measure(0, 2, 4)]
-    schedules = [measure(1, 1, 4), measure(1, 1, 1), measure(1, 0, 1), measure(2, 0, 1),
-                 measure(1, 1, 2)]
+    plain_runs = [measure(0, m, o) for m, o in
+                  ((1, 4), (1, 0), (1, 1), (1, 2), (2, 0), (2, 1), (2, 4), (3, 0), (3, 1),
+                   (4, 0), (4, 1))]
+    schedules = [measure(t, m, o) for t, m, o in
+                 ((1, 1, 4), (1, 1, 1), (1, 1, 0), (1, 0, 0), (1, 0, 1), (2, 0, 0), (2, 0, 1),
+                  (1, 2, 0), (1, 1, 2), (1, 2, 1))]
     best_plain = max(plain_runs, key=lambda r: r["ess_per_s"][0])["schedule"]
     best_learned = max(schedules, key=lambda r: r["ess_per_s"][0])["schedule"]
     final_cycles = 3 * cycles
@@ -510,6 +513,10 @@ def run_learned(args):
     plain = remeasure(standard)  # the plain PT cycle of the benchmark (1 M + 4 OR)
     plain_best = plain if best_plain == standard else remeasure(best_plain)
     learned = remeasure(best_learned)
+    # the same schedule with all four sites from the network's vMFs
+    eng.tet_set_proposal(0)
+    learned_product = remeasure(best_learned)
+    eng.tet_set_proposal(1)
     ratio = learned["ess_per_s"][0] / plain["ess_per_s"][0]
     ratio_best = learned["ess_per_s"][0] / plain_best["ess_per_s"][0]
     agree = [abs(p[0] - q[0]) / max(np.hypot(p[1], q[1]), 1e-30)
@@ -527,6 +534,9 @@ def run_learned(args):
                        "train_seconds": train_s, "loss_first": loss0, "loss_last": loss},
             "kernels_autotune_choice": choice,
             "plain": plain, "learned": learned,
+            "learned_product_proposal": {k: learned_product[k] for k in
+                                         ("us_per_cycle", "tau_int", "ess_per_s",
+                                          "tet_acceptance")},
             "ratio_vs_plain_best_schedule": ratio_best, "plain_best": plain_best,
             "selection_cycles": cycles, "final_cycles": final_cycles,
             "plain_schedules": [{"schedule": r["schedule"], "us_per_cycle": r["us_per_cycle"],

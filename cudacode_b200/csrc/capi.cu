@@ -190,8 +190,10 @@ bool use_cycle_kernel(const pyro_ctx* ctx) {
 // With with_obs, the FP64 energy partials of an isotropic J1 group are
 // computed on its chain right after its last pass, while its spins are still
 // in L2 (instead of one lattice-wide read from HBM after all groups).
+// n_tet learned tetrahedron sweeps of a J1-only group follow its plain
+// sweeps on the same chain (before its energy partials).
 int queue_grouped(pyro_ctx* ctx, int n_metro, int n_or, bool j1_grouped, bool gen_grouped,
-                  bool with_obs) {
+                  bool with_obs, int n_tet) {
   const int chains = std::max(1, std::min(ctx->n_chains, kMaxChains));
   if (chains > 1) {
     for (int c = 0; c < chains; ++c) {
@@ -223,6 +225,10 @@ int queue_grouped(pyro_ctx* ctx, int n_metro, int n_or, bool j1_grouped, bool ge
                            metro ? ctx->j1_metro_site_mode : ctx->j1_or_site_mode, st);
             PYRO_CK_LAUNCH();
           }
+        }
+        if (n_tet > 0) {
+          const int rc = queue_tet_group(ctx, si, r0, cnt, n_tet, st);
+          if (rc) return rc;
         }
         if (with_obs && s.exch < 0) {
           J1ObsParams jp;
@@ -278,15 +284,28 @@ int queue_generic_sweeps(pyro_ctx* ctx, int n_metro, int n_or) {
   return rc;
 }
 
-int queue_cycle_body(pyro_ctx* ctx, int n_metro, int n_or, bool with_obs) {
+// The J1 systems run per-pass kernels in replica groups.
+bool j1_grouped_path(const pyro_ctx* ctx) {
+  return !use_cycle_kernel(ctx) && ctx->rep_group > 0 && ctx->use_j1_kernel &&
+         !ctx->j1_sys.empty();
+}
+
+// n_tet > 0 only on the J1 grouped path with every J1-only system on it
+// (tet_in_groups): each group's learned sweeps follow its plain sweeps.
+int queue_cycle_body(pyro_ctx* ctx, int n_metro, int n_or, bool with_obs, int n_tet = 0) {
   int rc = check_cluster(ctx);
   if (rc) return rc;
   const bool cyc = use_cycle_kernel(ctx);
-  const bool j1_grouped = !cyc && ctx->rep_group > 0 && ctx->use_j1_kernel && !ctx->j1_sys.empty();
+  const bool j1_grouped = j1_grouped_path(ctx);
   const bool gen_grouped = !ctx->gen_groups.empty();
+  if (n_tet > 0 && !j1_grouped) return fail(ctx, PYRO_ERR_STATE, "learned sweeps need replica groups");
   if (j1_grouped || gen_grouped) {
-    rc = queue_grouped(ctx, n_metro, n_or, j1_grouped, gen_grouped, with_obs);
+    rc = queue_grouped(ctx, n_metro, n_or, j1_grouped, gen_grouped, with_obs, n_tet);
     if (rc) return rc;
+    if (n_tet > 0) {
+      tet_advance(ctx, n_tet);
+      PYRO_CK_LAUNCH();
+    }
     if (!gen_grouped) rc = queue_generic_sweeps(ctx, n_metro, n_or);
     if (rc) return rc;
     if (!j1_grouped) {  // J1 systems ungrouped: their per-pass kernels or the cluster kernel
@@ -833,6 +852,9 @@ int pyro_set_option(pyro_ctx* ctx, int option, int value) {
   } else if (option == PYRO_OPT_PDL) {
     if (value != 0 && value != 1) return fail(ctx, PYRO_ERR_ARG, "PDL option is 0 or 1");
     ctx->pdl = value;
+  } else if (option == PYRO_OPT_TET_GROUPED) {
+    if (value != 0 && value != 1) return fail(ctx, PYRO_ERR_ARG, "tet grouped option is 0 or 1");
+    ctx->tet_grouped = value;
   } else if (option == PYRO_OPT_GROUP_MB) {
     if (value < 0) return fail(ctx, PYRO_ERR_ARG, "group size in MB must be >= 0");
     ctx->gen_group_mb = value;
@@ -880,6 +902,7 @@ int pyro_get_option(pyro_ctx* ctx, int option, int* value) {
     case PYRO_OPT_GROUP_MB: *value = ctx->gen_group_mb; break;
     case PYRO_OPT_FAR_KERNEL: *value = ctx->far_kernel; break;
     case PYRO_OPT_PDL: *value = ctx->pdl; break;
+    case PYRO_OPT_TET_GROUPED: *value = ctx->tet_grouped; break;
     case PYRO_OPT_J1_SITE_MODE:
       *value = (ctx->j1_metro_site_mode ? 1 : 0) | (ctx->j1_or_site_mode ? 2 : 0);
       break;
@@ -1396,6 +1419,17 @@ static int run_smem_cycles(pyro_ctx* ctx, int n_metro, int n_or, int n_cycles) {
   return PYRO_OK;
 }
 
+// Learned sweeps can run inside the replica groups: the J1 grouped path
+// covers every J1-only system.
+static bool tet_in_groups(const pyro_ctx* ctx) {
+  if (!ctx->tet_grouped || !j1_grouped_path(ctx)) return false;
+  for (int i = 0; i < (int)ctx->sys.size(); ++i)
+    if (j1_only(ctx->sys[i]) &&
+        std::find(ctx->j1_sys.begin(), ctx->j1_sys.end(), i) == ctx->j1_sys.end())
+      return false;
+  return true;
+}
+
 static int run_cycles(pyro_ctx* ctx, int n_metro, int n_or, int n_tet, int do_swap, int n_cycles) {
   if (!ctx) return PYRO_ERR_ARG;
   if (n_metro < 0 || n_or < 0 || n_tet < 0 || n_cycles < 0)
@@ -1415,9 +1449,14 @@ static int run_cycles(pyro_ctx* ctx, int n_metro, int n_or, int n_tet, int do_sw
     int rc = check_cluster(ctx);  // sets kernel attributes: not inside a capture
     if (rc) return rc;
     PYRO_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    rc = queue_cycle_body(ctx, n_metro, n_or, n_tet == 0);
-    if (rc == PYRO_OK && n_tet > 0) {
-      rc = queue_tet_sweeps(ctx, n_tet);
+    if (n_tet == 0) {
+      rc = queue_cycle_body(ctx, n_metro, n_or, true);
+    } else if (tet_in_groups(ctx)) {
+      // each replica group's learned sweeps on its own chain
+      rc = queue_cycle_body(ctx, n_metro, n_or, true, n_tet);
+    } else {
+      rc = queue_cycle_body(ctx, n_metro, n_or, false);
+      if (rc == PYRO_OK) rc = queue_tet_sweeps(ctx, n_tet);
       if (rc == PYRO_OK) rc = queue_observables(ctx);
     }
     if (rc == PYRO_OK) {

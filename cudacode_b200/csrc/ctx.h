@@ -90,6 +90,7 @@ struct pyro_ctx {
   std::vector<char> pass_all16;  // same, for the ungrouped generic lists
   int far_kernel = 1;  // compile-time-offset kernel for 16-colour passes
   int pdl = 1;         // programmatic dependent launch of the per-pass J1 kernels
+  int tet_grouped = 1;  // learned sweeps inside the replica groups
   std::vector<GenGroup> gen_groups;
   int n_chains = 1;     // concurrent streams the replica groups are dealt to
   cudaStream_t chain_stream[pyro::kMaxChains] = {};
@@ -157,6 +158,11 @@ int rebuild_schedule(pyro_ctx* ctx);
 void tet_free(pyro_ctx* ctx);
 // Queues n learned tetrahedron sweeps of every J1-only system (tet_capi.cu).
 int queue_tet_sweeps(pyro_ctx* ctx, int n);
+// Queues n learned sweeps of replicas [r0, r0 + cnt) of system si on stream
+// st (a replica group of the grouped cycle; a no-op for other systems), and
+// advances the learned-move sweep counter by n on the context stream.
+int queue_tet_group(pyro_ctx* ctx, int si, int r0, int cnt, int n, cudaStream_t st);
+void tet_advance(pyro_ctx* ctx, int n);
 // Adds n to the learned-move proposal count (acceptance statistics).
 void tet_count_sweeps(pyro_ctx* ctx, unsigned long long n);
 // Learned-move sweep counter (device), read / set synchronously.

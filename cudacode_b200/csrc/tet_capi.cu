@@ -37,6 +37,7 @@ struct TetState {
   int adam_step = 0;
   uint64_t seed = 0;
   int sweep_kernel = 2;   // 0 per pass, 1 cluster (one launch per call), 2 per pass, lane pairs
+  int closure = 1;        // site 3 from its exact conditional (1) or the network's vMF (0)
   int forward_umma = 1;   // batched forward on tcgen05 (1) or mma.sync (0)
   int* d_err = nullptr;   // set by the tcgen05 forward if a wait ran out
   int cluster_max = 8;    // largest cluster size tried
@@ -113,6 +114,7 @@ TetMoveParams move_params(pyro_ctx* ctx, int si, unsigned long long off) {
   p.seed_lo = (uint32_t)(ctx->seed & 0xffffffffu);
   p.seed_hi = (uint32_t)(ctx->seed >> 32);
   p.image = ctx->tet->d_image;
+  p.closure = ctx->tet->closure;
   p.pdl = ctx->pdl;
   p.err = ctx->tet->d_err;
   return p;
@@ -136,44 +138,81 @@ void tet_count_sweeps(pyro_ctx* ctx, unsigned long long n) {
   if (ctx->tet) ctx->tet->proposed_sweeps += n;
 }
 
+// Cluster size of the one-launch sweep kernel (form 1), 0 if no cluster
+// can be resident (the per-pass kernels run instead); checked once.
+static int tet_cluster_size(TetState* t) {
+  if (t->sweep_kernel != 1) return 0;
+  if (t->cluster_ok < 0) {
+    t->cluster_ok = 0;
+    for (int cs = t->cluster_max; cs >= 1; --cs) {
+      int n_active = 0;
+      if (tet_cluster_prepare(cs, &n_active) == cudaSuccess && n_active > 0) {
+        t->cluster_ok = cs;
+        break;
+      }
+      cudaGetLastError();
+    }
+  }
+  return t->cluster_ok;
+}
+
 // Queues n tetrahedron sweeps (4 passes each) over every J1-only system;
 // offsets from the device counter, which this call advances.
 int queue_tet_sweeps(pyro_ctx* ctx, int n) {
   TetState* t = ctx->tet;  // sweep_kernel: 0 per pass, 1 cluster, 2 per pass with lane pairs
-  if (t->sweep_kernel == 1 && t->cluster_ok != 0) {
-    if (t->cluster_ok < 0) {
-      t->cluster_ok = 0;
-      for (int cs = t->cluster_max; cs >= 1; --cs) {
-        int n_active = 0;
-        if (tet_cluster_prepare(cs, &n_active) == cudaSuccess && n_active > 0) {
-          t->cluster_ok = cs;
-          break;
+  const int cluster = tet_cluster_size(t);
+  if (cluster > 0) {
+    for (int si = 0; si < (int)ctx->sys.size(); ++si) {
+      if (!j1_only_system(ctx->sys[si])) continue;
+      const int cs = std::min(cluster, tet_chunks(ctx->sys[si].L3));
+      PYRO_CK(launch_tet_sweep_cluster(move_params(ctx, si, 0), n, cs, ctx->stream));
+    }
+  } else {
+    for (int k = 0; k < n; ++k)
+      for (int f = 0; f < 4; ++f)
+        for (int si = 0; si < (int)ctx->sys.size(); ++si) {
+          if (!j1_only_system(ctx->sys[si])) continue;
+          launch_tet_move(move_params(ctx, si, (unsigned long long)k), f, t->sweep_kernel,
+                          ctx->stream);
+          PYRO_CK_LAUNCH();
         }
-        cudaGetLastError();
-      }
-    }
-    if (t->cluster_ok > 0) {
-      for (int si = 0; si < (int)ctx->sys.size(); ++si) {
-        if (!j1_only_system(ctx->sys[si])) continue;
-        const int cs = std::min(t->cluster_ok, tet_chunks(ctx->sys[si].L3));
-        PYRO_CK(launch_tet_sweep_cluster(move_params(ctx, si, 0), n, cs, ctx->stream));
-      }
-      launch_advance(t->d_ctr, (unsigned long long)n, ctx->stream);
-      PYRO_CK_LAUNCH();
-      return PYRO_OK;
-    }
   }
-  for (int k = 0; k < n; ++k)
-    for (int f = 0; f < 4; ++f)
-      for (int si = 0; si < (int)ctx->sys.size(); ++si) {
-        if (!j1_only_system(ctx->sys[si])) continue;
-        launch_tet_move(move_params(ctx, si, (unsigned long long)k), f, t->sweep_kernel,
-                        ctx->stream);
-        PYRO_CK_LAUNCH();
-      }
-  launch_advance(ctx->tet->d_ctr, (unsigned long long)n, ctx->stream);
+  tet_advance(ctx, n);
   PYRO_CK_LAUNCH();
   return PYRO_OK;
+}
+
+// n sweeps of replicas [r0, r0 + cnt) of system si on stream st (one replica
+// group of the grouped cycle; the sweeps of a replica are the same updates
+// in the same order as in queue_tet_sweeps). The caller advances the
+// counter once for all groups (tet_advance).
+int queue_tet_group(pyro_ctx* ctx, int si, int r0, int cnt, int n, cudaStream_t st) {
+  const SysDev& s = ctx->sys[si];
+  if (!j1_only_system(s) || n <= 0) return PYRO_OK;
+  TetState* t = ctx->tet;
+  auto group = [&](unsigned long long k) {
+    TetMoveParams p = move_params(ctx, si, k);
+    p.spins += (long long)r0 * 16 * s.L3;
+    p.n_rep = cnt;
+    p.rep_global += r0;
+    p.rep_key += r0;
+    return p;
+  };
+  const int cluster = tet_cluster_size(t);
+  if (cluster > 0) {
+    PYRO_CK(launch_tet_sweep_cluster(group(0), n, std::min(cluster, tet_chunks(s.L3)), st));
+    return PYRO_OK;
+  }
+  for (int k = 0; k < n; ++k)
+    for (int f = 0; f < 4; ++f) {
+      launch_tet_move(group((unsigned long long)k), f, t->sweep_kernel, st);
+      PYRO_CK_LAUNCH();
+    }
+  return PYRO_OK;
+}
+
+void tet_advance(pyro_ctx* ctx, int n) {
+  launch_advance(ctx->tet->d_ctr, (unsigned long long)n, ctx->stream);
 }
 
 }  // namespace pyro
@@ -253,6 +292,19 @@ int pyro_tet_set_kernel(pyro_ctx* ctx, int cluster) {
   PYRO_CK(cudaSetDevice(ctx->device));
   PYRO_CK(cudaStreamSynchronize(ctx->stream));
   ctx->tet->sweep_kernel = cluster;
+  for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+  ctx->graphs.clear();
+  ctx->graph_kernels.clear();
+  return PYRO_OK;
+}
+
+int pyro_tet_set_proposal(pyro_ctx* ctx, int kind) {
+  int rc = need_tet(ctx);
+  if (rc) return rc;
+  if (kind != 0 && kind != 1) return fail(ctx, PYRO_ERR_ARG, "tet proposal kind is 0 or 1");
+  PYRO_CK(cudaSetDevice(ctx->device));
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  ctx->tet->closure = kind;
   for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
   ctx->graphs.clear();
   ctx->graph_kernels.clear();

@@ -415,8 +415,66 @@ __device__ __forceinline__ SiteMove site_move(const float* o, pyro_vec3 s, uint3
   return m;
 }
 
+// log(sinh k / k) up to a constant, k - log k + log(1 - e^{-2k}): the
+// normalisation of a vMF density of concentration k > 0.
+__device__ __forceinline__ float vmf_log_norm(float k) {
+  return (k - __logf(k)) + __logf(1.0f - __expf(-2.0f * k));
+}
+
+// Natural parameter f = -beta (J1 (s0 + s1 + s2) + h3) of site 3's exact
+// conditional distribution p(s3 | s0, s1, s2) ~ exp(f . s3), as an axis and a
+// concentration (at least exp(kLogKappaMin), the network's smallest).
+__device__ __forceinline__ pyro_vec3 closure_axis(pyro_vec3 s0, pyro_vec3 s1, pyro_vec3 s2,
+                                                  pyro_vec3 h3, float beta, float J1,
+                                                  float* kappa) {
+  pyro_vec3 f;
+  f.x = -beta * (J1 * ((s0.x + s1.x) + s2.x) + h3.x);
+  f.y = -beta * (J1 * ((s0.y + s1.y) + s2.y) + h3.y);
+  f.z = -beta * (J1 * ((s0.z + s1.z) + s2.z) + h3.z);
+  const float n2 = f.x * f.x + f.y * f.y + f.z * f.z;
+  pyro_vec3 mu;
+  float k = 0.0f;
+  if (n2 > 1e-30f) {
+    const float inv = rsqrtf(n2);
+    mu.x = f.x * inv;
+    mu.y = f.y * inv;
+    mu.z = f.z * inv;
+    k = n2 * inv;
+  } else {
+    mu.x = 0.0f;
+    mu.y = 0.0f;
+    mu.z = 1.0f;
+  }
+  *kappa = fmaxf(k, kKappaFloor);
+  return mu;
+}
+
+// Site 3 drawn from its exact conditional distribution given the proposed
+// sites 0-2 (a0..a2) and its external field: a vMF whose natural parameter
+// is closure_axis. Returns the sample and the site's term of log q(S) -
+// log q(S'): the density of the current s3 under the conditional of the
+// current sites 0-2 (b0..b2) minus the density of the sample. The joint
+// proposal q = (network vMFs of sites 0-2) x (this conditional) is exactly
+// computable in both directions, so the MH test stays exact; site 3 is
+// integrated out of the mismatch between q and the Boltzmann weight, which
+// raises the acceptance of the joint move.
+__device__ __forceinline__ SiteMove closure_move(pyro_vec3 a0, pyro_vec3 a1, pyro_vec3 a2,
+                                                 pyro_vec3 b0, pyro_vec3 b1, pyro_vec3 b2,
+                                                 pyro_vec3 s3, pyro_vec3 h3, float beta,
+                                                 float J1, uint32_t ru, uint32_t rv) {
+  float kn, ko;
+  const pyro_vec3 mn = closure_axis(a0, a1, a2, h3, beta, J1, &kn);
+  const pyro_vec3 mo = closure_axis(b0, b1, b2, h3, beta, J1, &ko);
+  SiteMove m;
+  m.sn = vmf_sample(mn, kn, tet_uniform(ru), tet_uniform(rv));
+  m.lq = (ko * dot3(mo, s3) - vmf_log_norm(ko)) - (kn * dot3(mn, m.sn) - vmf_log_norm(kn));
+  return m;
+}
+
 // Proposal, MH test and write-back of one tetrahedron of corner F from its
 // network outputs o[16], its fields h and spins s. Returns 1 if accepted.
+// p.closure: site 3 from its exact conditional (closure_move) instead of the
+// network's fourth vMF.
 template <int F>
 __device__ __forceinline__ int tet_finish(const TetMoveParams& p, int rep, int cell, float beta,
                                           unsigned long long sweep, const pyro_vec3 h[4],
@@ -432,7 +490,9 @@ __device__ __forceinline__ int tet_finish(const TetMoveParams& p, int rep, int c
   const SiteMove m0 = site_move(o + 0, s[0], r0[0], r0[1]);
   const SiteMove m1 = site_move(o + 4, s[1], r0[2], r0[3]);
   const SiteMove m2 = site_move(o + 8, s[2], r1[0], r1[1]);
-  const SiteMove m3 = site_move(o + 12, s[3], r1[2], r1[3]);
+  const SiteMove m3 = p.closure ? closure_move(m0.sn, m1.sn, m2.sn, s[0], s[1], s[2], s[3], h[3],
+                                               beta, p.J1, r1[2], r1[3])
+                                : site_move(o + 12, s[3], r1[2], r1[3]);
   const pyro_vec3 sn[4] = {m0.sn, m1.sn, m2.sn, m3.sn};
   const float dE = tet_energy(sn, h, p.J1) - tet_energy(s, h, p.J1);
   const float log_q = (m0.lq + m1.lq) + (m2.lq + m3.lq);
@@ -565,7 +625,27 @@ __device__ __forceinline__ int tet_pair_step(const TetMoveParams& p, const MlpSm
   pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + half,
               p.seed_lo, p.seed_hi, r);
   const SiteMove ma = site_move(o + 0, s[0], r[0], r[1]);
-  const SiteMove mb = site_move(o + 4, s[1], r[2], r[3]);
+  SiteMove mb{};
+  if (!p.closure || half == 0) mb = site_move(o + 4, s[1], r[2], r[3]);
+  if (p.closure) {
+    // site 3 (upper lane) is conditional on the lower lane's sites 0, 1:
+    // their proposals (a) and current spins (b)
+    pyro_vec3 a0, a1, b0, b1;
+    a0.x = __shfl_up_sync(0xffffffffu, ma.sn.x, 16);
+    a0.y = __shfl_up_sync(0xffffffffu, ma.sn.y, 16);
+    a0.z = __shfl_up_sync(0xffffffffu, ma.sn.z, 16);
+    a1.x = __shfl_up_sync(0xffffffffu, mb.sn.x, 16);
+    a1.y = __shfl_up_sync(0xffffffffu, mb.sn.y, 16);
+    a1.z = __shfl_up_sync(0xffffffffu, mb.sn.z, 16);
+    b0.x = __shfl_up_sync(0xffffffffu, s[0].x, 16);
+    b0.y = __shfl_up_sync(0xffffffffu, s[0].y, 16);
+    b0.z = __shfl_up_sync(0xffffffffu, s[0].z, 16);
+    b1.x = __shfl_up_sync(0xffffffffu, s[1].x, 16);
+    b1.y = __shfl_up_sync(0xffffffffu, s[1].y, 16);
+    b1.z = __shfl_up_sync(0xffffffffu, s[1].z, 16);
+    if (half == 1)
+      mb = closure_move(a0, a1, ma.sn, b0, b1, s[0], s[1], h[1], beta, p.J1, r[2], r[3]);
+  }
   const pyro_vec3 sn[2] = {ma.sn, mb.sn};
   const float lq_half = ma.lq + mb.lq;
   // gather sites 2, 3 on the lower lane

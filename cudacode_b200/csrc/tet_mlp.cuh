@@ -1,8 +1,10 @@
 // Learned tetrahedron proposal: a 16 -> 64 -> 64 -> 16 MLP (BF16 weights,
 // FP32 accumulation on the tensor cores) that maps the external fields of the
 // four spins of an up-tetrahedron (and beta) to a von Mises-Fisher
-// distribution for each of them; a joint move of the four spins drawn from it
-// is accepted with the exact Metropolis-Hastings ratio.
+// distribution for each of them. The joint move draws sites 0-2 from the
+// network's vMFs and site 3 either from the network's fourth vMF or from its
+// exact conditional distribution given the three new spins and its external
+// field (a vMF too); it is accepted with the exact Metropolis-Hastings ratio.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -22,6 +24,7 @@ constexpr int kOffW3 = kOffB2 + kMlpHidden;                // [64][16]
 constexpr int kOffB3 = kOffW3 + kMlpHidden * kMlpOut;      // [16]
 constexpr int kMlpParams = kOffB3 + kMlpOut;               // 6288
 constexpr float kLogKappaMin = -4.0f, kLogKappaMax = 6.0f;
+constexpr float kKappaFloor = 0.018315639f;  // exp(kLogKappaMin)
 
 // The weights as the byte image of the kernels' shared-memory copy: BF16
 // operand matrices in padded rows (conflict-free fragment loads), FP32
@@ -68,6 +71,7 @@ struct TetMoveParams {
   unsigned long long tet_off;
   uint32_t seed_lo, seed_hi;
   const unsigned char* image;  // kImgBytes weight image
+  int closure;                 // 1: site 3 from its exact conditional, 0: the network's vMF
   int pdl;                     // programmatic dependent launch of the per-pass kernels
   int* err;                    // set to 1 if a tensor-core wait of the tcgen05 form ran out
 };

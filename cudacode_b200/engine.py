@@ -119,6 +119,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "pyro_tet_get_weights": (i, [P, pf, i]),
         "pyro_tet_sweep": (i, [P, i]),
         "pyro_tet_set_kernel": (i, [P, i]),
+        "pyro_tet_set_proposal": (i, [P, i]),
         "pyro_tet_acceptance": (i, [P, i, pu64, pu64]),
         "pyro_tet_reset_acceptance": (i, [P]),
         "pyro_tet_collect": (i, [P, i, i, C.POINTER(C.c_longlong)]),
@@ -284,6 +285,7 @@ class Engine:
     OPT_GROUP_MB = 8
     OPT_FAR_KERNEL = 9
     OPT_PDL = 10
+    OPT_TET_GROUPED = 11
 
     def set_option(self, option: int, value: int) -> None:
         self._ck(self.lib.pyro_set_option(self.ctx, option, value))
@@ -541,6 +543,11 @@ class Engine:
 
     def tet_set_kernel(self, cluster: int) -> None:
         self._ck(self.lib.pyro_tet_set_kernel(self.ctx, cluster))
+
+    def tet_set_proposal(self, kind: int) -> None:
+        """1 (default): site 3 of each tetrahedron from its exact conditional
+        given the proposed sites 0-2; 0: all four from the network's vMFs."""
+        self._ck(self.lib.pyro_tet_set_proposal(self.ctx, kind))
 
     def tet_sweep(self, n: int = 1) -> None:
         self._ck(self.lib.pyro_tet_sweep(self.ctx, n))

@@ -114,6 +114,11 @@ int pyro_neighbour_table(int site, int* out120);
  * completion before touching memory: results are unchanged); 0 plain
  * launches. */
 #define PYRO_OPT_PDL 10
+/* PYRO_OPT_TET_GROUPED: 1 (default) runs the learned tetrahedron sweeps of
+ * pyro_cycle_tet inside the replica groups of PYRO_OPT_REPLICA_GROUP, each
+ * group's right after its plain sweeps on the same chain; 0 runs them over
+ * all replicas after every group's plain sweeps. Identical results. */
+#define PYRO_OPT_TET_GROUPED 11
 int pyro_set_option(pyro_ctx* ctx, int option, int value);
 int pyro_get_option(pyro_ctx* ctx, int option, int* value);
 /* Autotuner: times every kernel variant (per-pass generic, per-pass J1,
@@ -329,6 +334,12 @@ int pyro_tet_sweep(pyro_ctx* ctx, int n_sweeps);
  * the moves of its CTA and makes pyro_tet_acceptance return
  * PYRO_ERR_TIMEOUT. */
 int pyro_tet_set_kernel(pyro_ctx* ctx, int mode);
+/* Proposal of the learned move. 1 (default): sites 0-2 of the tetrahedron
+ * from the network's vMFs, site 3 from its exact conditional distribution
+ * given the three proposed spins and its external field, a vMF of natural
+ * parameter -beta (J1 (s0' + s1' + s2') + h3); 0: all four sites from the
+ * network's vMFs. Both are exact MH moves. */
+int pyro_tet_set_proposal(pyro_ctx* ctx, int kind);
 int pyro_tet_acceptance(pyro_ctx* ctx, int system, uint64_t* accepted, uint64_t* proposed);
 int pyro_tet_reset_acceptance(pyro_ctx* ctx);
 /* Appends (features[16], spins[12]) of every stride-th up-tetrahedron of each

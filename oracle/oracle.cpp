@@ -844,7 +844,8 @@ double orc_exp64(double x) { return pyro_exp64(x); }
 
 // ---------------------------------------------------------------------------
 // Learned tetrahedron proposal (no counterpart in the reference): FP64 restatement of
-// the network, its negative log-likelihood gradient and the MH move, with the
+// the network, its negative log-likelihood gradient and the tetrahedron features
+// (the MH move itself is checked statistically, against the plain chain), with the
 // engine's BF16 rounding points (inputs, weights, hidden activations and the
 // backward activations are rounded to BF16 where the engine feeds them to
 // the tensor cores; accumulation in FP64 here, FP32 there).

@@ -103,12 +103,13 @@ def mean_and_error(x):
     return b.mean(), b.std(ddof=1) / np.sqrt(20)
 
 
-@pytest.mark.parametrize("form", [2, 3])
-def test_learned_move_preserves_the_boltzmann_distribution(form):
+@pytest.mark.parametrize("form,proposal", [(2, 1), (3, 1), (2, 0), (0, 1)])
+def test_learned_move_preserves_the_boltzmann_distribution(form, proposal):
     """Tetrahedron moves alone (untrained network) and the plain method,
     both started from the same equilibrated spins, sample the same energy
     distribution: detailed balance of the MH test (form 3: the network on
-    tcgen05)."""
+    tcgen05; proposal 1: site 3 from its exact conditional, 0: four network
+    vMFs)."""
     temps = [0.4, 1.2]
     s = System(L=4, temperatures=temps)
     plain = Engine([s], seed=21)
@@ -123,6 +124,7 @@ def test_learned_move_preserves_the_boltzmann_distribution(form):
     tet.set_spins(start)
     tet.tet_init(seed=5)
     tet.tet_set_kernel(form)
+    tet.tet_set_proposal(proposal)
     e_tet = chain_energy(tet, 100, 2000, lambda: tet.tet_sweep(1))
     acc, prop = tet.tet_acceptance()
     assert (acc > 0).all()
@@ -151,6 +153,16 @@ def test_training_lowers_the_loss_and_raises_acceptance():
     e.tet_sweep(5)
     a1, p1 = e.tet_acceptance()
     assert (a1 / p1).mean() > (a0 / p0).mean(), (a0 / p0, a1 / p1)
+    # drawing site 3 from its exact conditional accepts more often than the
+    # network's fourth vMF (same network, same states)
+    saved = e.get_spins()
+    e.tet_set_proposal(0)
+    e.tet_reset_acceptance()
+    e.tet_sweep(5)
+    a2, p2 = e.tet_acceptance()
+    e.set_spins(saved)
+    e.tet_set_proposal(1)
+    assert (a1 / p1).mean() > (a2 / p2).mean(), (a1 / p1, a2 / p2)
     # the trained move alone still samples the plain chain's distribution:
     # replica perm[t] holds temperature slot t in `e`; the plain chain gets
     # the same configurations with replica t at slot t.
@@ -175,8 +187,8 @@ def test_learned_move_requires_j1_only():
         e.tet_init()
 
 
-@pytest.mark.parametrize("L", [4, 7, 16])
-def test_cluster_and_per_pass_tet_kernels_agree(L):
+@pytest.mark.parametrize("L,proposal", [(4, 1), (7, 1), (16, 1), (7, 0)])
+def test_cluster_and_per_pass_tet_kernels_agree(L, proposal):
     s = System(L=L, temperatures=[0.1, 0.3, 0.9])
     runs = []
     for cluster in (0, 1, 2):
@@ -184,6 +196,7 @@ def test_cluster_and_per_pass_tet_kernels_agree(L):
         e.init_random()
         e.tet_init(seed=2)
         e.tet_set_kernel(cluster)
+        e.tet_set_proposal(proposal)
         e.tet_sweep(3)
         e.cycle_tet(1, 1, 2, True, 2)
         runs.append((e.get_spins(), e.tet_acceptance()[0], e.permutation()))
@@ -215,3 +228,32 @@ def test_tensor_memory_move_matches_the_mma_sync_move_closely(L):
     assert np.abs(n - 1).max() < 1e-4
     assert np.abs(runs[0][1].astype(np.int64) - runs[1][1].astype(np.int64)).max() <= \
         max(2, int(0.01 * runs[0][2][0]))
+
+
+@pytest.mark.parametrize("form,group,chains", [(2, 2, 3), (2, 3, 2), (0, 1, 4), (1, 2, 2),
+                                               (3, 4, 2)])
+def test_learned_sweeps_in_replica_groups_match_ungrouped(form, group, chains):
+    """Learned sweeps run inside the replica groups (each group's after its
+    plain sweeps, on its chain) give the same chain, bit for bit, as the
+    learned sweeps over all replicas after every group's plain sweeps."""
+    systems = [System(L=5, temperatures=geometric_ladder(0.05, 0.5, 7)),
+               System(L=4, temperatures=[0.1, 0.3, 0.9], J2=0.05),
+               System(L=6, temperatures=[0.08, 0.2])]
+    runs = []
+    for grouped in (0, 1):
+        e = Engine(systems, seed=43)
+        e.init_random()
+        e.tet_init(seed=4)
+        e.tet_set_kernel(form)
+        e.set_option(e.OPT_REPLICA_GROUP, group)
+        e.set_option(e.OPT_CHAINS, chains)
+        e.set_option(e.OPT_TET_GROUPED, grouped)
+        assert e.get_option(e.OPT_TET_GROUPED) == grouped
+        e.cycle_tet(1, 1, 1, True, 3)
+        e.cycle_tet(0, 1, 2, True, 2)
+        e.cycle(1, 2, True, 1)
+        runs.append([(e.get_spins(k), e.tet_acceptance(k)[0], e.permutation(k),
+                      *e.last_observables(k)) for k in range(len(systems))])
+    for k in range(len(systems)):
+        for a, b in zip(runs[0][k], runs[1][k]):
+            assert np.array_equal(a, b), k
