@@ -437,11 +437,12 @@ int pyro_tet_train(pyro_ctx* ctx, int steps, int batch, float lr, double* mean_l
     launch_mlp_pack(t->d_master, t->d_image, ctx->stream);
     PYRO_CK_LAUNCH();
   }
-  if (mean_loss) {
+  if (mean_loss)
     PYRO_CK(cudaMemcpyAsync(&last, t->d_loss, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    PYRO_CK(cudaStreamSynchronize(ctx->stream));
-    *mean_loss = last / (double)batch;
-  }
+  // the move kernels start copying the weight image before their dependency
+  // wait: no move may be queued behind the pack kernel
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  if (mean_loss) *mean_loss = last / (double)batch;
   return PYRO_OK;
 }
 

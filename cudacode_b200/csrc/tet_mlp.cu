@@ -452,22 +452,28 @@ __device__ __forceinline__ pyro_vec3 closure_axis(pyro_vec3 s0, pyro_vec3 s1, py
 // Site 3 drawn from its exact conditional distribution given the proposed
 // sites 0-2 (a0..a2) and its external field: a vMF whose natural parameter
 // is closure_axis. Returns the sample and the site's term of log q(S) -
-// log q(S'): the density of the current s3 under the conditional of the
-// current sites 0-2 (b0..b2) minus the density of the sample. The joint
-// proposal q = (network vMFs of sites 0-2) x (this conditional) is exactly
-// computable in both directions, so the MH test stays exact; site 3 is
-// integrated out of the mismatch between q and the Boltzmann weight, which
-// raises the acceptance of the joint move.
-__device__ __forceinline__ SiteMove closure_move(pyro_vec3 a0, pyro_vec3 a1, pyro_vec3 a2,
-                                                 pyro_vec3 b0, pyro_vec3 b1, pyro_vec3 b2,
+// log q(S'): `rev` (closure_reverse: the density of the current s3 under the
+// conditional of the current sites 0-2) minus the density of the sample. The
+// joint proposal q = (network vMFs of sites 0-2) x (this conditional) is
+// exactly computable in both directions, so the MH test stays exact; site 3
+// is integrated out of the mismatch between q and the Boltzmann weight,
+// which raises the acceptance of the joint move.
+__device__ __forceinline__ float closure_reverse(pyro_vec3 b0, pyro_vec3 b1, pyro_vec3 b2,
                                                  pyro_vec3 s3, pyro_vec3 h3, float beta,
-                                                 float J1, uint32_t ru, uint32_t rv) {
-  float kn, ko;
-  const pyro_vec3 mn = closure_axis(a0, a1, a2, h3, beta, J1, &kn);
+                                                 float J1) {
+  float ko;
   const pyro_vec3 mo = closure_axis(b0, b1, b2, h3, beta, J1, &ko);
+  return ko * dot3(mo, s3) - vmf_log_norm(ko);
+}
+
+__device__ __forceinline__ SiteMove closure_move(pyro_vec3 a0, pyro_vec3 a1, pyro_vec3 a2,
+                                                 float rev, pyro_vec3 h3, float beta, float J1,
+                                                 uint32_t ru, uint32_t rv) {
+  float kn;
+  const pyro_vec3 mn = closure_axis(a0, a1, a2, h3, beta, J1, &kn);
   SiteMove m;
   m.sn = vmf_sample(mn, kn, tet_uniform(ru), tet_uniform(rv));
-  m.lq = (ko * dot3(mo, s3) - vmf_log_norm(ko)) - (kn * dot3(mn, m.sn) - vmf_log_norm(kn));
+  m.lq = rev - (kn * dot3(mn, m.sn) - vmf_log_norm(kn));
   return m;
 }
 
@@ -490,9 +496,11 @@ __device__ __forceinline__ int tet_finish(const TetMoveParams& p, int rep, int c
   const SiteMove m0 = site_move(o + 0, s[0], r0[0], r0[1]);
   const SiteMove m1 = site_move(o + 4, s[1], r0[2], r0[3]);
   const SiteMove m2 = site_move(o + 8, s[2], r1[0], r1[1]);
-  const SiteMove m3 = p.closure ? closure_move(m0.sn, m1.sn, m2.sn, s[0], s[1], s[2], s[3], h[3],
-                                               beta, p.J1, r1[2], r1[3])
-                                : site_move(o + 12, s[3], r1[2], r1[3]);
+  const SiteMove m3 =
+      p.closure ? closure_move(m0.sn, m1.sn, m2.sn,
+                               closure_reverse(s[0], s[1], s[2], s[3], h[3], beta, p.J1), h[3],
+                               beta, p.J1, r1[2], r1[3])
+                : site_move(o + 12, s[3], r1[2], r1[3]);
   const pyro_vec3 sn[4] = {m0.sn, m1.sn, m2.sn, m3.sn};
   const float dE = tet_energy(sn, h, p.J1) - tet_energy(s, h, p.J1);
   const float log_q = (m0.lq + m1.lq) + (m2.lq + m3.lq);
@@ -564,6 +572,21 @@ __device__ __forceinline__ int tet_warp_step(const TetMoveParams& p, const MlpSm
 // energy change and the proposal ratio with exactly the single-lane
 // expressions, so the decisions are identical. Returns 1 on the lower lane
 // of an accepted move. kWait as in tet_warp_step.
+// Offset of down-tetrahedron neighbour M of site S from replica start.
+template <int S, int M>
+__device__ __forceinline__ int down_off(const Frame& f, int L3) {
+  constexpr NbrEntry e = j1_neighbour(S, j1_down_index(S, M));
+  return f.zo[e.dz + 1] + f.yo[e.dy + 1] + f.xo[e.dx + 1] + e.t * L3;
+}
+
+// Down neighbour M of site 4F + 2 half + K, the site chosen per lane by a
+// select instead of a branch, so that all loads of a lane issue together.
+template <int F, int K, int M>
+__device__ __forceinline__ int pair_down_off(const Frame& f, int L3, int half) {
+  const int lo = down_off<4 * F + K, M>(f, L3), hi = down_off<4 * F + 2 + K, M>(f, L3);
+  return half ? hi : lo;
+}
+
 template <int F, bool kL2, bool kWait>
 __device__ __forceinline__ int tet_pair_step(const TetMoveParams& p, const MlpSmem& w, bool active,
                                              int rep, int cell, float beta,
@@ -572,31 +595,50 @@ __device__ __forceinline__ int tet_pair_step(const TetMoveParams& p, const MlpSm
   const int lane = threadIdx.x & 31;
   const int half = lane >> 4;  // 0: sites 0, 1; 1: sites 2, 3
   const int row = lane & 15;
+  // rep and cell are valid on inactive lanes too (their loads are in bounds;
+  // they write nothing)
   const float4* rb = p.spins + (long long)rep * 16 * p.L3;
+  const Frame fr = cell_frame(cell, p.L, p.rcpL);
+  float4 nb[2][3], own[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) own[k] = ld_spin<kL2>(rb + (4 * F + 2 * half + k) * p.L3 + cell);
+  nb[0][0] = ld_spin<kL2>(rb + pair_down_off<F, 0, 0>(fr, p.L3, half));
+  nb[0][1] = ld_spin<kL2>(rb + pair_down_off<F, 0, 1>(fr, p.L3, half));
+  nb[0][2] = ld_spin<kL2>(rb + pair_down_off<F, 0, 2>(fr, p.L3, half));
+  nb[1][0] = ld_spin<kL2>(rb + pair_down_off<F, 1, 0>(fr, p.L3, half));
+  nb[1][1] = ld_spin<kL2>(rb + pair_down_off<F, 1, 1>(fr, p.L3, half));
+  nb[1][2] = ld_spin<kL2>(rb + pair_down_off<F, 1, 2>(fr, p.L3, half));
+  // random words (no dependence on the spins) while the loads are in flight:
+  // this lane's two proposals, and the lower lane's acceptance test
+  const uint32_t key_tet = (uint32_t)(F * p.L3 + cell);
+  uint32_t r[4], r2[4];
+  pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + half,
+              p.seed_lo, p.seed_hi, r);
+  pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + 2,
+              p.seed_lo, p.seed_hi, r2);
+  // external fields in ext_field's order
   pyro_vec3 h[2], s[2];
-  if (active) {
-    const Frame fr = cell_frame(cell, p.L, p.rcpL);
-    if (half == 0) {
-      h[0] = ext_field<4 * F + 0, kL2>(rb, fr, p.L3, p.J1);
-      h[1] = ext_field<4 * F + 1, kL2>(rb, fr, p.L3, p.J1);
-    } else {
-      h[0] = ext_field<4 * F + 2, kL2>(rb, fr, p.L3, p.J1);
-      h[1] = ext_field<4 * F + 3, kL2>(rb, fr, p.L3, p.J1);
-    }
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      const float4 v = ld_spin<kL2>(rb + (4 * F + 2 * half + k) * p.L3 + cell);
-      s[k].x = v.x;
-      s[k].y = v.y;
-      s[k].z = v.z;
-    }
-  } else {
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      h[k].x = h[k].y = h[k].z = 0.0f;
-      s[k].x = s[k].y = 0.0f;
-      s[k].z = 1.0f;
-    }
+  for (int k = 0; k < 2; ++k) {
+    h[k].x = p.J1 * ((nb[k][0].x + nb[k][1].x) + nb[k][2].x);
+    h[k].y = p.J1 * ((nb[k][0].y + nb[k][1].y) + nb[k][2].y);
+    h[k].z = p.J1 * ((nb[k][0].z + nb[k][1].z) + nb[k][2].z);
+    s[k].x = own[k].x;
+    s[k].y = own[k].y;
+    s[k].z = own[k].z;
+  }
+  // the reverse term of site 3's conditional (upper lane) needs only the
+  // current spins: evaluated before the network
+  float rev3 = 0.0f;
+  if (p.closure) {
+    pyro_vec3 b0, b1;
+    b0.x = __shfl_up_sync(0xffffffffu, s[0].x, 16);
+    b0.y = __shfl_up_sync(0xffffffffu, s[0].y, 16);
+    b0.z = __shfl_up_sync(0xffffffffu, s[0].z, 16);
+    b1.x = __shfl_up_sync(0xffffffffu, s[1].x, 16);
+    b1.y = __shfl_up_sync(0xffffffffu, s[1].y, 16);
+    b1.z = __shfl_up_sync(0xffffffffu, s[1].z, 16);
+    rev3 = closure_reverse(b0, b1, s[0], s[1], h[1], beta, p.J1);
   }
   __nv_bfloat16* frow = feat + row * kLdIn;
 #pragma unroll
@@ -620,31 +662,19 @@ __device__ __forceinline__ int tet_pair_step(const TetMoveParams& p, const MlpSm
   float o[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) o[i] = out[row * kLdOut + 8 * half + i];
-  const uint32_t key_tet = (uint32_t)(F * p.L3 + cell);
-  uint32_t r[4];
-  pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + half,
-              p.seed_lo, p.seed_hi, r);
   const SiteMove ma = site_move(o + 0, s[0], r[0], r[1]);
   SiteMove mb{};
   if (!p.closure || half == 0) mb = site_move(o + 4, s[1], r[2], r[3]);
   if (p.closure) {
-    // site 3 (upper lane) is conditional on the lower lane's sites 0, 1:
-    // their proposals (a) and current spins (b)
-    pyro_vec3 a0, a1, b0, b1;
+    // site 3 (upper lane) is conditional on the lower lane's proposed sites 0, 1
+    pyro_vec3 a0, a1;
     a0.x = __shfl_up_sync(0xffffffffu, ma.sn.x, 16);
     a0.y = __shfl_up_sync(0xffffffffu, ma.sn.y, 16);
     a0.z = __shfl_up_sync(0xffffffffu, ma.sn.z, 16);
     a1.x = __shfl_up_sync(0xffffffffu, mb.sn.x, 16);
     a1.y = __shfl_up_sync(0xffffffffu, mb.sn.y, 16);
     a1.z = __shfl_up_sync(0xffffffffu, mb.sn.z, 16);
-    b0.x = __shfl_up_sync(0xffffffffu, s[0].x, 16);
-    b0.y = __shfl_up_sync(0xffffffffu, s[0].y, 16);
-    b0.z = __shfl_up_sync(0xffffffffu, s[0].z, 16);
-    b1.x = __shfl_up_sync(0xffffffffu, s[1].x, 16);
-    b1.y = __shfl_up_sync(0xffffffffu, s[1].y, 16);
-    b1.z = __shfl_up_sync(0xffffffffu, s[1].z, 16);
-    if (half == 1)
-      mb = closure_move(a0, a1, ma.sn, b0, b1, s[0], s[1], h[1], beta, p.J1, r[2], r[3]);
+    if (half == 1) mb = closure_move(a0, a1, ma.sn, rev3, h[1], beta, p.J1, r[2], r[3]);
   }
   const pyro_vec3 sn[2] = {ma.sn, mb.sn};
   const float lq_half = ma.lq + mb.lq;
@@ -674,9 +704,6 @@ __device__ __forceinline__ int tet_pair_step(const TetMoveParams& p, const MlpSm
     const float dE = tet_energy(SN, H, p.J1) - tet_energy(S, H, p.J1);
     const float log_q = lq_half + lq_hi;
     const float log_r = -beta * dE + log_q;
-    uint32_t r2[4];
-    pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + 2,
-                p.seed_lo, p.seed_hi, r2);
     acc_word = (log_r >= 0.0f || tet_uniform(r2[0]) < __expf(log_r)) ? 1u : 0u;
   }
   const uint32_t accepted = __shfl_sync(0xffffffffu, acc_word, row);
@@ -732,12 +759,15 @@ __global__ void __launch_bounds__(kTetMoveThreads) tet_move_kernel(const TetMove
 // Per-pass kernel, two lanes per tetrahedron (256 threads = 128 tetrahedra).
 template <int F>
 __global__ void __launch_bounds__(kTetMoveThreads) tet_move_pair_kernel(const TetMoveParams p) {
-  pass_prologue();
   extern __shared__ __align__(16) unsigned char smem[];
+  // The weight image is written only by the pack kernel, and every call that
+  // packs synchronises its stream before returning, so no kernel that this
+  // one may overlap writes it: its copy starts before the dependency wait.
+  stage_weights(smem, p.image, kImgFwdBytes);
+  pass_prologue();
   const MlpSmem w = carve_weights(smem);
   __nv_bfloat16* feat_all = reinterpret_cast<__nv_bfloat16*>(smem + kSmemWeightsFwd);
   float* out_all = reinterpret_cast<float*>(smem + kSmemWeightsFwd + kTetMoveThreads * kLdIn * 2);
-  stage_weights(smem, p.image, kImgFwdBytes);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long tet = (long long)blockIdx.x * (kTetMoveThreads / 2) + warp * 16 + (lane & 15);
   const bool active = tet < (long long)p.n_rep * p.L3;

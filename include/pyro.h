@@ -348,8 +348,8 @@ int pyro_tet_collect(pyro_ctx* ctx, int system, int stride, long long* n_written
 int pyro_tet_samples(pyro_ctx* ctx, float* features, float* targets, long long max_n,
                      long long* n_out);
 /* `steps` Adam steps (lr, beta 0.9/0.999) of maximum likelihood on random
- * batches of `batch` samples; *mean_loss = last batch's mean negative
- * log-likelihood. */
+ * batches of `batch` samples; *mean_loss (may be null) = last batch's mean
+ * negative log-likelihood. Returns after the context stream has drained. */
 int pyro_tet_train(pyro_ctx* ctx, int steps, int batch, float lr, double* mean_loss);
 /* Host-buffer test paths: network outputs for n feature rows, and the
  * gradient (6288 values) and loss sum of the negative log-likelihood. */
