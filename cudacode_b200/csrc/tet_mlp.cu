@@ -217,6 +217,62 @@ __device__ __forceinline__ void tile_forward(const __nv_bfloat16* feat, int r_ba
   }
 }
 
+// The network of the learned move for one 16-row m-tile: tile_forward's
+// operands and accumulations, with the hidden activations rounded to BF16
+// first and evaluated by hswish_bf16x2 (tile_forward rounds after an FP32
+// activation). Used by every mma.sync form of the move, so they agree bit
+// for bit; the batched forward and the training keep tile_forward.
+__device__ __forceinline__ void tile_forward_move(const __nv_bfloat16* feat, int r_base,
+                                                  const MlpSmem& w, TileFwd& f) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int r0 = r_base + g, r1 = r0 + 8;
+  const uint32_t a0 = ld32(feat + r0 * kLdIn + 2 * t), a1 = ld32(feat + r1 * kLdIn + 2 * t);
+  const uint32_t a2 = ld32(feat + r0 * kLdIn + 8 + 2 * t), a3 = ld32(feat + r1 * kLdIn + 8 + 2 * t);
+  float h1[8][4];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    h1[j][0] = h1[j][2] = w.b1[8 * j + 2 * t];
+    h1[j][1] = h1[j][3] = w.b1[8 * j + 2 * t + 1];
+    const __nv_bfloat16* bw = w.w1t + (8 * j + g) * kLdIn + 2 * t;
+    mma_bf16(h1[j], a0, a1, a2, a3, ld32(bw), ld32(bw + 8));
+  }
+  float h2[8][4];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    h2[j][0] = h2[j][2] = w.b2[8 * j + 2 * t];
+    h2[j][1] = h2[j][3] = w.b2[8 * j + 2 * t + 1];
+  }
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk) {
+    const uint32_t x0 = hswish_bf16x2(pack_bf16(h1[2 * kk][0], h1[2 * kk][1]));
+    const uint32_t x1 = hswish_bf16x2(pack_bf16(h1[2 * kk][2], h1[2 * kk][3]));
+    const uint32_t x2 = hswish_bf16x2(pack_bf16(h1[2 * kk + 1][0], h1[2 * kk + 1][1]));
+    const uint32_t x3 = hswish_bf16x2(pack_bf16(h1[2 * kk + 1][2], h1[2 * kk + 1][3]));
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const __nv_bfloat16* bw = w.w2t + (8 * j + g) * kLdH + 16 * kk + 2 * t;
+      mma_bf16(h2[j], x0, x1, x2, x3, ld32(bw), ld32(bw + 8));
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    f.o[j][0] = f.o[j][2] = w.b3[8 * j + 2 * t];
+    f.o[j][1] = f.o[j][3] = w.b3[8 * j + 2 * t + 1];
+  }
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk) {
+    const uint32_t x0 = hswish_bf16x2(pack_bf16(h2[2 * kk][0], h2[2 * kk][1]));
+    const uint32_t x1 = hswish_bf16x2(pack_bf16(h2[2 * kk][2], h2[2 * kk][3]));
+    const uint32_t x2 = hswish_bf16x2(pack_bf16(h2[2 * kk + 1][0], h2[2 * kk + 1][1]));
+    const uint32_t x3 = hswish_bf16x2(pack_bf16(h2[2 * kk + 1][2], h2[2 * kk + 1][3]));
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const __nv_bfloat16* bw = w.w3t + (8 * j + g) * kLdH + 16 * kk + 2 * t;
+      mma_bf16(f.o[j], x0, x1, x2, x3, ld32(bw), ld32(bw + 8));
+    }
+  }
+}
+
 __device__ __forceinline__ void store_out(const TileFwd& f, int r_base, float* out) {
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   const int r0 = r_base + g, r1 = r0 + 8;
@@ -355,6 +411,14 @@ __device__ __forceinline__ float tet_uniform(uint32_t r) {
   return 2.0f - __uint_as_float(0x3f800000u | (r >> 9));
 }
 
+// Uniform in (0, 1] for the MH test from the low bits of the words whose top
+// 23 bits feed the proposals of sites 0 and 1 (9 + 9 + 5 bits of r[0..2]),
+// bits that no other draw of the move uses.
+__device__ __forceinline__ float tet_test_uniform(const uint32_t r[4]) {
+  const uint32_t m = ((r[0] & 0x1ffu) << 14) | ((r[1] & 0x1ffu) << 5) | (r[2] & 0x1fu);
+  return 2.0f - __uint_as_float(0x3f800000u | m);
+}
+
 // Rotation of (sin t cos p, sin t sin p, cos t) onto the axis n, in the
 // frame of Duff et al. (2017), with the approximate reciprocal (|sgn + n.z|
 // >= 1).
@@ -486,13 +550,11 @@ __device__ __forceinline__ int tet_finish(const TetMoveParams& p, int rep, int c
                                           unsigned long long sweep, const pyro_vec3 h[4],
                                           const pyro_vec3 s[4], const float* o) {
   const uint32_t key_tet = (uint32_t)(F * p.L3 + cell);
-  uint32_t r0[4], r1[4], r2[4];
+  uint32_t r0[4], r1[4];
   pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + 0,
               p.seed_lo, p.seed_hi, r0);
   pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + 1,
               p.seed_lo, p.seed_hi, r1);
-  pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + 2,
-              p.seed_lo, p.seed_hi, r2);
   const SiteMove m0 = site_move(o + 0, s[0], r0[0], r0[1]);
   const SiteMove m1 = site_move(o + 4, s[1], r0[2], r0[3]);
   const SiteMove m2 = site_move(o + 8, s[2], r1[0], r1[1]);
@@ -505,7 +567,7 @@ __device__ __forceinline__ int tet_finish(const TetMoveParams& p, int rep, int c
   const float dE = tet_energy(sn, h, p.J1) - tet_energy(s, h, p.J1);
   const float log_q = (m0.lq + m1.lq) + (m2.lq + m3.lq);
   const float log_r = -beta * dE + log_q;
-  const int accepted = log_r >= 0.0f || tet_uniform(r2[0]) < __expf(log_r);
+  const int accepted = log_r >= 0.0f || tet_test_uniform(r0) < __expf(log_r);
   if (accepted) {
     float4* wb = p.spins + (long long)rep * 16 * p.L3;
 #pragma unroll
@@ -550,9 +612,9 @@ __device__ __forceinline__ int tet_warp_step(const TetMoveParams& p, const MlpSm
   if (kWait) stage_wait();
   else __syncwarp();
   TileFwd fw;
-  tile_forward<false>(feat, 0, w, fw, nullptr, nullptr);
+  tile_forward_move(feat, 0, w, fw);
   store_out(fw, 0, out);
-  tile_forward<false>(feat, 16, w, fw, nullptr, nullptr);
+  tile_forward_move(feat, 16, w, fw);
   store_out(fw, 16, out);
   __syncwarp();
   int accepted = 0;
@@ -609,13 +671,11 @@ __device__ __forceinline__ int tet_pair_step(const TetMoveParams& p, const MlpSm
   nb[1][1] = ld_spin<kL2>(rb + pair_down_off<F, 1, 1>(fr, p.L3, half));
   nb[1][2] = ld_spin<kL2>(rb + pair_down_off<F, 1, 2>(fr, p.L3, half));
   // random words (no dependence on the spins) while the loads are in flight:
-  // this lane's two proposals, and the lower lane's acceptance test
+  // this lane's two proposals (and, on the lower lane, the acceptance test)
   const uint32_t key_tet = (uint32_t)(F * p.L3 + cell);
-  uint32_t r[4], r2[4];
+  uint32_t r[4];
   pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + half,
               p.seed_lo, p.seed_hi, r);
-  pyro_philox(key_tet, (uint32_t)(p.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_TET + 2,
-              p.seed_lo, p.seed_hi, r2);
   // external fields in ext_field's order
   pyro_vec3 h[2], s[2];
 #pragma unroll
@@ -655,7 +715,7 @@ __device__ __forceinline__ int tet_pair_step(const TetMoveParams& p, const MlpSm
   if (kWait) stage_wait();
   else __syncwarp();
   TileFwd fw;
-  tile_forward<false>(feat, 0, w, fw, nullptr, nullptr);
+  tile_forward_move(feat, 0, w, fw);
   store_out(fw, 0, out);
   __syncwarp();
   // this lane's two sites: network outputs 8 * half .. 8 * half + 7
@@ -704,7 +764,7 @@ __device__ __forceinline__ int tet_pair_step(const TetMoveParams& p, const MlpSm
     const float dE = tet_energy(SN, H, p.J1) - tet_energy(S, H, p.J1);
     const float log_q = lq_half + lq_hi;
     const float log_r = -beta * dE + log_q;
-    acc_word = (log_r >= 0.0f || tet_uniform(r2[0]) < __expf(log_r)) ? 1u : 0u;
+    acc_word = (log_r >= 0.0f || tet_test_uniform(r) < __expf(log_r)) ? 1u : 0u;
   }
   const uint32_t accepted = __shfl_sync(0xffffffffu, acc_word, row);
   if (accepted && active) {
@@ -834,7 +894,7 @@ __global__ void __launch_bounds__(umma::kURows) tet_move_umma_kernel(const TetMo
   const uint32_t tmem = umma::ready(smem);
   uint32_t parity = 0;
   float o[kMlpOut];
-  const bool ok = umma::network(smem, tmem, o, &parity);
+  const bool ok = umma::network<true>(smem, tmem, o, &parity);
   int acc = 0;
   if (ok && active) acc = tet_finish<F>(p, rep, cell, beta, sweep, h, s, o);
   if (!ok && threadIdx.x == 0 && p.err) atomicExch(p.err, 1);

@@ -15,6 +15,19 @@
 #include "tet_mlp.cuh"
 
 namespace pyro {
+// Hard-swish of a packed pair of BF16 values in BF16x2 arithmetic, for the
+// learned move's networks (their hidden activations are BF16 MMA operands
+// anyway): five paired operations per two activations instead of five per
+// one. The batched forward and the training keep the FP32 activation.
+__device__ __forceinline__ uint32_t hswish_bf16x2(uint32_t v) {
+  const __nv_bfloat162 x = *reinterpret_cast<const __nv_bfloat162*>(&v);
+  const __nv_bfloat162 three = __float2bfloat162_rn(3.0f), zero = __float2bfloat162_rn(0.0f),
+                       six = __float2bfloat162_rn(6.0f), sixth = __float2bfloat162_rn(1.0f / 6.0f);
+  const __nv_bfloat162 t = __hmin2(__hmax2(__hadd2(x, three), zero), six);
+  __nv_bfloat162 y = __hmul2(__hmul2(x, t), sixth);
+  return *reinterpret_cast<uint32_t*>(&y);
+}
+
 namespace umma {
 
 constexpr int kURows = 128;
@@ -113,6 +126,25 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
 }
 
 // Row `r` of an M x K operand in the core-matrix layout: K/8 chunks of 16 B.
+// kPacked: hidden activations x + bias, rounded to BF16 pairs and activated
+// by hswish_bf16x2 (the learned move's network); else x as given.
+template <bool kPacked>
+__device__ __forceinline__ void store_hidden(unsigned char* base, int r, const float* x,
+                                             const float* bias) {
+  constexpr int K = kMlpHidden;
+  for (int c = 0; c < K / 8; ++c) {
+    uint32_t w[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int j = 8 * c + 2 * q;
+      w[q] = kPacked ? hswish_bf16x2(pack2(x[j] + bias[j], x[j + 1] + bias[j + 1]))
+                     : pack2(hswish_u(x[j] + bias[j]), hswish_u(x[j + 1] + bias[j + 1]));
+    }
+    *reinterpret_cast<uint4*>(base + (r / 8) * (K / 8) * 128 + c * 128 + (r % 8) * 16) =
+        make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
 __device__ __forceinline__ void store_row(unsigned char* base, int r, int K, const float* x) {
   for (int c = 0; c < K / 8; ++c) {
     uint4 q;
@@ -171,6 +203,9 @@ __device__ __forceinline__ uint32_t ready(unsigned char* smem) {
 // The three layers for the CTA's 128 rows (A0 in place); on success o[16]
 // holds this thread's outputs (bias added). Returns false (for every thread)
 // if a wait ran out; *parity is the mbarrier phase still expected then.
+// kPacked: hidden activations in BF16x2 arithmetic (store_hidden), as the
+// mma.sync forms of the learned move evaluate them.
+template <bool kPacked = false>
 __device__ __forceinline__ bool network(unsigned char* smem, uint32_t tmem, float* o,
                                         uint32_t* parity_io) {
   const float* bias = reinterpret_cast<const float*>(smem + kUBias);
@@ -194,9 +229,7 @@ __device__ __forceinline__ bool network(unsigned char* smem, uint32_t tmem, floa
     fence_after_sync();
 #pragma unroll
     for (int c = 0; c < kMlpHidden / 16; ++c) tmem_ld16(lane_base + 16 * c, x + 16 * c);
-#pragma unroll
-    for (int j = 0; j < kMlpHidden; ++j) x[j] = hswish_u(x[j] + bias[j]);
-    store_row(a1, tid, kMlpHidden, x);
+    store_hidden<kPacked>(a1, tid, x, bias);
     fence_async_smem();
   }
   fence_before_sync();
@@ -219,9 +252,8 @@ __device__ __forceinline__ bool network(unsigned char* smem, uint32_t tmem, floa
     fence_after_sync();
 #pragma unroll
     for (int c = 0; c < kMlpHidden / 16; ++c) tmem_ld16(lane_base + 64 + 16 * c, x + 16 * c);
-#pragma unroll
-    for (int j = 0; j < kMlpHidden; ++j) x[j] = hswish_u(x[j] + bias[kMlpHidden + j]);
-    store_row(a1, tid, kMlpHidden, x);  // layer 2's reads of A1 completed with its commit
+    // layer 2's reads of A1 completed with its commit
+    store_hidden<kPacked>(a1, tid, x, bias + kMlpHidden);
     fence_async_smem();
   }
   fence_before_sync();
