@@ -924,13 +924,16 @@ int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen)
     else any_gen = true;
   }
   std::vector<Variant> vs;
+  int n_j1 = 0;  // stage 1: the J1 variants, first in vs
   if (any_j1) {
     const Variant j1v[] = {{0, 0, 16, 1, 0, 1, 0}, {1, 0, 16, 1, 0, 1, 0}, {1, 0, 16, 3, 0, 1, 0},
                            {1, 0, 16, 1, 8, 1, 0}, {1, 0, 16, 1, 4, 2, 0}, {1, 0, 16, 3, 4, 2, 0},
                            {1, 0, 16, 1, 3, 2, 0}, {1, 0, 16, 1, 2, 2, 0}, {1, 0, 16, 1, 2, 3, 0},
                            {1, 0, 16, 1, 3, 3, 0}, {1, 0, 16, 1, 2, 4, 0}, {1, 0, 16, 1, 1, 4, 0},
-                           {1, 1, 16, 1, 0, 1, 0}, {1, 1, 10, 1, 0, 1, 0}};
+                           {1, 1, 16, 1, 0, 1, 0}, {1, 1, 10, 1, 0, 1, 0}, {1, 0, 16, 1, 6, 2, 0},
+                           {1, 0, 16, 1, 4, 3, 0}, {1, 0, 16, 1, 5, 2, 0}};
     vs.insert(vs.end(), std::begin(j1v), std::end(j1v));
+    n_j1 = (int)vs.size();
   }
   if (any_gen) {
     const int base = vs.size();  // filled with the best J1 knobs after stage 1
@@ -957,7 +960,6 @@ int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen)
   };
   float best = 1e30f;
   int best_i = -1;
-  const int n_j1 = any_j1 ? 14 : 0;
   for (int i = 0; i < (int)vs.size(); ++i) {
     Variant v = vs[i];
     if (i >= n_j1 && best_i >= 0 && best_i < n_j1) {
