@@ -171,9 +171,9 @@ def test_training_lowers_the_loss_and_raises_acceptance():
     plain = Engine([s], seed=9)
     plain.set_spins(start[perm])
     plain.set_cone(e.get_cone())
-    plain_E = chain_energy(plain, 50, 1500, lambda: (plain.metropolis_sweep(1),
+    plain_E = chain_energy(plain, 50, 4000, lambda: (plain.metropolis_sweep(1),
                                                      plain.overrelax_sweep(2)))
-    tet_E = chain_energy(e, 50, 1500, lambda: e.tet_sweep(1))
+    tet_E = chain_energy(e, 50, 4000, lambda: e.tet_sweep(1))
     assert np.array_equal(perm, e.permutation())  # no exchanges in either chain
     for t in range(4):
         m1, s1 = mean_and_error(plain_E[:, t])
