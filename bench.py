@@ -496,7 +496,7 @@ def run_learned(args):
                    (4, 0), (4, 1))]
     schedules = [measure(t, m, o) for t, m, o in
                  ((1, 1, 4), (1, 1, 1), (1, 1, 0), (1, 0, 0), (1, 0, 1), (2, 0, 0), (2, 0, 1),
-                  (1, 2, 0), (1, 1, 2), (1, 2, 1))]
+                  (1, 2, 0), (1, 1, 2), (1, 2, 1), (3, 0, 0), (2, 1, 0), (3, 1, 0))]
     best_plain = max(plain_runs, key=lambda r: r["ess_per_s"][0])["schedule"]
     best_learned = max(schedules, key=lambda r: r["ess_per_s"][0])["schedule"]
     final_cycles = 3 * cycles

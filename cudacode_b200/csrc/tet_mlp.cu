@@ -49,6 +49,18 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   return *reinterpret_cast<uint32_t*>(&v);
 }
 
+// Four 8x8 BF16 matrices from shared memory (ldmatrix .x4): lane l gives the
+// 16-byte row address of matrix l / 8, row l % 8; register q receives this
+// lane's pair of matrix q (row lane / 4, columns 2 (lane % 4) and + 1), which
+// is the B fragment layout of mma m16n8k16 for a [n][k] (k-contiguous) matrix.
+__device__ __forceinline__ void ldsm_x4(const __nv_bfloat16* p, uint32_t (&r)[4]) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(a)
+               : "memory");
+}
+
 // D = A * B + D, m16n8k16, BF16 inputs, FP32 accumulators.
 __device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2,
                                          uint32_t a3, uint32_t b0, uint32_t b1) {
@@ -220,21 +232,30 @@ __device__ __forceinline__ void tile_forward(const __nv_bfloat16* feat, int r_ba
 // The network of the learned move for one 16-row m-tile: tile_forward's
 // operands and accumulations, with the hidden activations rounded to BF16
 // first and evaluated by hswish_bf16x2 (tile_forward rounds after an FP32
-// activation). Used by every mma.sync form of the move, so they agree bit
-// for bit; the batched forward and the training keep tile_forward.
+// activation), and the weight fragments fetched by ldmatrix (one
+// instruction per two n-tiles instead of four 32-bit loads). Used by every
+// mma.sync form of the move, so they agree bit for bit; the batched forward
+// and the training keep tile_forward.
 __device__ __forceinline__ void tile_forward_move(const __nv_bfloat16* feat, int r_base,
                                                   const MlpSmem& w, TileFwd& f) {
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   const int r0 = r_base + g, r1 = r0 + 8;
+  // ldmatrix row of this lane: matrix lane / 8 of an x4 load covers n-tile
+  // j + (lane / 16) and k half (lane / 8) % 2 of a 16-wide k step
+  const int bn = 8 * (lane >> 4) + (lane & 7), bk = 8 * ((lane >> 3) & 1);
   const uint32_t a0 = ld32(feat + r0 * kLdIn + 2 * t), a1 = ld32(feat + r1 * kLdIn + 2 * t);
   const uint32_t a2 = ld32(feat + r0 * kLdIn + 8 + 2 * t), a3 = ld32(feat + r1 * kLdIn + 8 + 2 * t);
   float h1[8][4];
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    h1[j][0] = h1[j][2] = w.b1[8 * j + 2 * t];
-    h1[j][1] = h1[j][3] = w.b1[8 * j + 2 * t + 1];
-    const __nv_bfloat16* bw = w.w1t + (8 * j + g) * kLdIn + 2 * t;
-    mma_bf16(h1[j], a0, a1, a2, a3, ld32(bw), ld32(bw + 8));
+  for (int j = 0; j < 8; j += 2) {
+    uint32_t b[4];
+    ldsm_x4(w.w1t + (8 * j + bn) * kLdIn + bk, b);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      h1[j + q][0] = h1[j + q][2] = w.b1[8 * (j + q) + 2 * t];
+      h1[j + q][1] = h1[j + q][3] = w.b1[8 * (j + q) + 2 * t + 1];
+      mma_bf16(h1[j + q], a0, a1, a2, a3, b[2 * q], b[2 * q + 1]);
+    }
   }
   float h2[8][4];
 #pragma unroll
@@ -249,9 +270,11 @@ __device__ __forceinline__ void tile_forward_move(const __nv_bfloat16* feat, int
     const uint32_t x2 = hswish_bf16x2(pack_bf16(h1[2 * kk + 1][0], h1[2 * kk + 1][1]));
     const uint32_t x3 = hswish_bf16x2(pack_bf16(h1[2 * kk + 1][2], h1[2 * kk + 1][3]));
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const __nv_bfloat16* bw = w.w2t + (8 * j + g) * kLdH + 16 * kk + 2 * t;
-      mma_bf16(h2[j], x0, x1, x2, x3, ld32(bw), ld32(bw + 8));
+    for (int j = 0; j < 8; j += 2) {
+      uint32_t b[4];
+      ldsm_x4(w.w2t + (8 * j + bn) * kLdH + 16 * kk + bk, b);
+      mma_bf16(h2[j], x0, x1, x2, x3, b[0], b[1]);
+      mma_bf16(h2[j + 1], x0, x1, x2, x3, b[2], b[3]);
     }
   }
 #pragma unroll
@@ -265,11 +288,10 @@ __device__ __forceinline__ void tile_forward_move(const __nv_bfloat16* feat, int
     const uint32_t x1 = hswish_bf16x2(pack_bf16(h2[2 * kk][2], h2[2 * kk][3]));
     const uint32_t x2 = hswish_bf16x2(pack_bf16(h2[2 * kk + 1][0], h2[2 * kk + 1][1]));
     const uint32_t x3 = hswish_bf16x2(pack_bf16(h2[2 * kk + 1][2], h2[2 * kk + 1][3]));
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      const __nv_bfloat16* bw = w.w3t + (8 * j + g) * kLdH + 16 * kk + 2 * t;
-      mma_bf16(f.o[j], x0, x1, x2, x3, ld32(bw), ld32(bw + 8));
-    }
+    uint32_t b[4];
+    ldsm_x4(w.w3t + bn * kLdH + 16 * kk + bk, b);
+    mma_bf16(f.o[0], x0, x1, x2, x3, b[0], b[1]);
+    mma_bf16(f.o[1], x0, x1, x2, x3, b[2], b[3]);
   }
 }
 
