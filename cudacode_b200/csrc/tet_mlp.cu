@@ -745,8 +745,10 @@ __device__ __forceinline__ int tet_pair_step(const TetMoveParams& p, const MlpSm
 #pragma unroll
   for (int i = 0; i < 8; ++i) o[i] = out[row * kLdOut + 8 * half + i];
   const SiteMove ma = site_move(o + 0, s[0], r[0], r[1]);
-  SiteMove mb{};
-  if (!p.closure || half == 0) mb = site_move(o + 4, s[1], r[2], r[3]);
+  // every lane draws its second network site (on the upper lane the draw for
+  // site 3 is discarded when site 3 comes from its conditional): no branch,
+  // so the two draws of a lane overlap
+  SiteMove mb = site_move(o + 4, s[1], r[2], r[3]);
   if (p.closure) {
     // site 3 (upper lane) is conditional on the lower lane's proposed sites 0, 1
     pyro_vec3 a0, a1;
