@@ -50,7 +50,8 @@
 #define PYRO_PURPOSE_INIT 0x1u       /* random initial spins            */
 #define PYRO_PURPOSE_METRO 0x2u      /* cone Metropolis proposal/accept */
 #define PYRO_PURPOSE_SWAP 0x3u       /* replica-exchange acceptance     */
-#define PYRO_PURPOSE_TET 0x10u       /* learned move: +0, +1 proposals and test, +8 training batches, +9 initial weights */
+/* learned move: +0, +1 proposals and test, +8 training batches, +9 initial weights */
+#define PYRO_PURPOSE_TET 0x10u
 
 typedef struct { float x, y, z; } pyro_vec3;
 
