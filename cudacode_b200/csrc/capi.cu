@@ -213,7 +213,22 @@ int queue_grouped(pyro_ctx* ctx, int n_metro, int n_or, bool j1_grouped, bool ge
       for (int r0 = 0; r0 < s.n_rep; r0 += ctx->rep_group, ++gi) {
         cudaStream_t st = chains > 1 ? ctx->chain_stream[gi % chains] : ctx->stream;
         const int cnt = std::min(ctx->rep_group, s.n_rep - r0);
-        for (int k = 0; k < n_metro + n_or; ++k) {
+        J1ObsParams jp;
+        jp.spins = ctx->d_spins + s.spin_off + (long long)r0 * 16 * s.L3;
+        jp.L = s.L;
+        jp.L3 = s.L3;
+        jp.n_rep = cnt;
+        jp.rcpL = 1.0f / (float)s.L;
+        jp.J1 = s.J64[0];
+        jp.partials = ctx->d_partials;
+        jp.partial_begin = ctx->obs_segs[si].partial_begin + r0 * j1_blocks_per_replica(s.L3);
+        // the group's energy partials from its last pass when that pass runs
+        // in the cell form (isotropic J1, no learned sweeps after it)
+        const int n_sw = n_metro + n_or;
+        const bool last_metro = n_or == 0;
+        const bool fuse = ctx->fused_obs && with_obs && s.exch < 0 && n_tet == 0 && n_sw > 0 &&
+                          !(last_metro ? ctx->j1_metro_site_mode : ctx->j1_or_site_mode);
+        for (int k = 0; k < n_sw; ++k) {
           const bool metro = k < n_metro;
           for (int colour = 0; colour < 4; ++colour) {
             J1PassParams p = j1_params(ctx, si, (unsigned long long)k);
@@ -221,8 +236,11 @@ int queue_grouped(pyro_ctx* ctx, int n_metro, int n_or, bool j1_grouped, bool ge
             p.n_rep = cnt;
             p.rep_global += r0;
             p.rep_key += r0;
-            launch_j1_pass(p, colour, metro,
-                           metro ? ctx->j1_metro_site_mode : ctx->j1_or_site_mode, st);
+            if (fuse && k == n_sw - 1 && colour == 3)
+              launch_j1_last_pass(p, jp, metro, st);
+            else
+              launch_j1_pass(p, colour, metro,
+                             metro ? ctx->j1_metro_site_mode : ctx->j1_or_site_mode, st);
             PYRO_CK_LAUNCH();
           }
         }
@@ -230,16 +248,7 @@ int queue_grouped(pyro_ctx* ctx, int n_metro, int n_or, bool j1_grouped, bool ge
           const int rc = queue_tet_group(ctx, si, r0, cnt, n_tet, st);
           if (rc) return rc;
         }
-        if (with_obs && s.exch < 0) {
-          J1ObsParams jp;
-          jp.spins = ctx->d_spins + s.spin_off + (long long)r0 * 16 * s.L3;
-          jp.L = s.L;
-          jp.L3 = s.L3;
-          jp.n_rep = cnt;
-          jp.rcpL = 1.0f / (float)s.L;
-          jp.J1 = s.J64[0];
-          jp.partials = ctx->d_partials;
-          jp.partial_begin = ctx->obs_segs[si].partial_begin + r0 * j1_blocks_per_replica(s.L3);
+        if (with_obs && s.exch < 0 && !fuse) {
           launch_j1_observables(jp, st);
           PYRO_CK_LAUNCH();
         }
@@ -852,6 +861,9 @@ int pyro_set_option(pyro_ctx* ctx, int option, int value) {
   } else if (option == PYRO_OPT_PDL) {
     if (value != 0 && value != 1) return fail(ctx, PYRO_ERR_ARG, "PDL option is 0 or 1");
     ctx->pdl = value;
+  } else if (option == PYRO_OPT_FUSED_OBS) {
+    if (value != 0 && value != 1) return fail(ctx, PYRO_ERR_ARG, "fused observables option is 0 or 1");
+    ctx->fused_obs = value;
   } else if (option == PYRO_OPT_TET_GROUPED) {
     if (value != 0 && value != 1) return fail(ctx, PYRO_ERR_ARG, "tet grouped option is 0 or 1");
     ctx->tet_grouped = value;
@@ -903,6 +915,7 @@ int pyro_get_option(pyro_ctx* ctx, int option, int* value) {
     case PYRO_OPT_FAR_KERNEL: *value = ctx->far_kernel; break;
     case PYRO_OPT_PDL: *value = ctx->pdl; break;
     case PYRO_OPT_TET_GROUPED: *value = ctx->tet_grouped; break;
+    case PYRO_OPT_FUSED_OBS: *value = ctx->fused_obs; break;
     case PYRO_OPT_J1_SITE_MODE:
       *value = (ctx->j1_metro_site_mode ? 1 : 0) | (ctx->j1_or_site_mode ? 2 : 0);
       break;

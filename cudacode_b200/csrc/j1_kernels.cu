@@ -185,6 +185,57 @@ __device__ __forceinline__ void pass_prologue() {
   asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
 }
 
+// The four sites of colour B in `cell` of replica `rep` (cell form of a
+// pass). Returns the number of accepted Metropolis moves.
+template <int B, bool kMetro, bool kExch>
+__device__ __forceinline__ int cell_pass(const J1PassParams& p, int rep, int cell, float beta,
+                                         float cosmax) {
+  int x, y, z;
+  decode_cell(cell, p.L, p.rcpL, &x, &y, &z);
+  const CellFrame f = make_frame(x, y, z, p.L);
+  float4* rb = p.spins + (long long)rep * 16 * p.L3;
+  const unsigned long long sweep = (p.sweep_ctr ? *p.sweep_ctr : 0ull) + p.sweep_off;
+  const bool renorm =
+      p.renorm_every > 0 && ((sweep + 1) % (unsigned long long)p.renorm_every) == 0;
+  const uint32_t rkey = (uint32_t)(p.rep_key + rep);
+  const uint32_t sw = (uint32_t)sweep;
+  // The four sites of the colour in this cell are not neighbours of each
+  // other (nor of any site written in this pass), so all their loads are
+  // issued before the first store: one memory round trip, not four.
+  pyro_vec3 s0, h0, s1, h1, s2, h2, s3, h3;
+  site_field<B, false, kExch>(rb, f, cell, p.L3, p.J1, p, &s0, &h0);
+  site_field<4 + B, false, kExch>(rb, f, cell, p.L3, p.J1, p, &s1, &h1);
+  site_field<8 + B, false, kExch>(rb, f, cell, p.L3, p.J1, p, &s2, &h2);
+  site_field<12 + B, false, kExch>(rb, f, cell, p.L3, p.J1, p, &s3, &h3);
+  int acc = 0;
+  acc += site_update<B, kMetro>(rb, cell, p.L3, s0, h0, beta, cosmax, rkey, sw, renorm,
+                                p.seed_lo, p.seed_hi);
+  acc += site_update<4 + B, kMetro>(rb, cell, p.L3, s1, h1, beta, cosmax, rkey, sw, renorm,
+                                    p.seed_lo, p.seed_hi);
+  acc += site_update<8 + B, kMetro>(rb, cell, p.L3, s2, h2, beta, cosmax, rkey, sw, renorm,
+                                    p.seed_lo, p.seed_hi);
+  acc += site_update<12 + B, kMetro>(rb, cell, p.L3, s3, h3, beta, cosmax, rkey, sw, renorm,
+                                     p.seed_lo, p.seed_hi);
+  return acc;
+}
+
+// Block-wide count of accepted moves: one atomic per CTA. Every thread of
+// the CTA calls it.
+__device__ __forceinline__ void block_accept(const J1PassParams& p, int t, int acc) {
+  __shared__ int warp_acc[kJ1Threads / 32];
+  int v = acc;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) warp_acc[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int s = 0;
+#pragma unroll
+    for (int w = 0; w < kJ1Threads / 32; ++w) s += warp_acc[w];
+    if (s > 0) atomicAdd(p.accepted + p.temp_base + t, (unsigned long long)s);
+  }
+}
+
 template <int B, bool kMetro, bool kExch>
 __global__ void __launch_bounds__(kJ1Threads) j1_pass_kernel(const J1PassParams p) {
   pass_prologue();
@@ -199,48 +250,8 @@ __global__ void __launch_bounds__(kJ1Threads) j1_pass_kernel(const J1PassParams 
     cosmax = p.cosmax[p.temp_base + t];
   }
   int acc = 0;
-  if (cell < p.L3) {
-    int x, y, z;
-    decode_cell(cell, p.L, p.rcpL, &x, &y, &z);
-    const CellFrame f = make_frame(x, y, z, p.L);
-    float4* rb = p.spins + (long long)rep * 16 * p.L3;
-    const unsigned long long sweep = (p.sweep_ctr ? *p.sweep_ctr : 0ull) + p.sweep_off;
-    const bool renorm =
-        p.renorm_every > 0 && ((sweep + 1) % (unsigned long long)p.renorm_every) == 0;
-    const uint32_t rkey = (uint32_t)(p.rep_key + rep);
-    const uint32_t sw = (uint32_t)sweep;
-    // The four sites of the colour in this cell are not neighbours of each
-    // other (nor of any site written in this pass), so all their loads are
-    // issued before the first store: one memory round trip, not four.
-    pyro_vec3 s0, h0, s1, h1, s2, h2, s3, h3;
-    site_field<B, false, kExch>(rb, f, cell, p.L3, p.J1, p, &s0, &h0);
-    site_field<4 + B, false, kExch>(rb, f, cell, p.L3, p.J1, p, &s1, &h1);
-    site_field<8 + B, false, kExch>(rb, f, cell, p.L3, p.J1, p, &s2, &h2);
-    site_field<12 + B, false, kExch>(rb, f, cell, p.L3, p.J1, p, &s3, &h3);
-    acc += site_update<B, kMetro>(rb, cell, p.L3, s0, h0, beta, cosmax, rkey, sw, renorm,
-                                  p.seed_lo, p.seed_hi);
-    acc += site_update<4 + B, kMetro>(rb, cell, p.L3, s1, h1, beta, cosmax, rkey, sw, renorm,
-                                      p.seed_lo, p.seed_hi);
-    acc += site_update<8 + B, kMetro>(rb, cell, p.L3, s2, h2, beta, cosmax, rkey, sw, renorm,
-                                      p.seed_lo, p.seed_hi);
-    acc += site_update<12 + B, kMetro>(rb, cell, p.L3, s3, h3, beta, cosmax, rkey, sw, renorm,
-                                       p.seed_lo, p.seed_hi);
-  }
-  if (kMetro) {
-    // Block-wide count of accepted moves: one atomic per CTA.
-    __shared__ int warp_acc[kJ1Threads / 32];
-    int v = acc;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0) warp_acc[threadIdx.x >> 5] = v;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int s = 0;
-#pragma unroll
-      for (int w = 0; w < kJ1Threads / 32; ++w) s += warp_acc[w];
-      if (s > 0) atomicAdd(p.accepted + p.temp_base + t, (unsigned long long)s);
-    }
-  }
+  if (cell < p.L3) acc = cell_pass<B, kMetro, kExch>(p, rep, cell, beta, cosmax);
+  if (kMetro) block_accept(p, t, acc);
 }
 
 // Same pass, one site per thread: blockIdx.y is the FCC corner f (so site
@@ -344,25 +355,10 @@ __device__ __forceinline__ void cell_corner(const float4* __restrict__ rep, cons
   *mz += (double)s0.z + s1.z + s2.z + s3.z;
 }
 
-// Energy (each bond once, by tetrahedra) and magnetisation of one chunk of
-// kJ1Threads cells, reduced over the CTA in a fixed order; thread 0 returns
-// (2 E, Mx, My, Mz) (the finalise step halves the site-sum convention of the
-// generic kernel, hence 2 E). Every thread of the CTA must call it.
-template <bool kL2Only>
-__device__ __forceinline__ double4 chunk_observables(const float4* __restrict__ rb, int cell,
-                                                     int L, int L3, float rcpL, double J1,
+// Fixed-order CTA reduction of per-thread (E, M) terms; thread 0 returns
+// (2 E, Mx, My, Mz). Every thread of the CTA calls it.
+__device__ __forceinline__ double4 block_observables(double e, double mx, double my, double mz,
                                                      double (*red)[kJ1Threads / 32]) {
-  double e = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
-  if (cell < L3) {
-    int x, y, z;
-    decode_cell(cell, L, rcpL, &x, &y, &z);
-    const CellFrame f = make_frame(x, y, z, L);
-    cell_corner<0, kL2Only>(rb, f, cell, L3, &e, &mx, &my, &mz);
-    cell_corner<1, kL2Only>(rb, f, cell, L3, &e, &mx, &my, &mz);
-    cell_corner<2, kL2Only>(rb, f, cell, L3, &e, &mx, &my, &mz);
-    cell_corner<3, kL2Only>(rb, f, cell, L3, &e, &mx, &my, &mz);
-    e *= J1;
-  }
   e = warp_sum_d(e);
   mx = warp_sum_d(mx);
   my = warp_sum_d(my);
@@ -389,6 +385,28 @@ __device__ __forceinline__ double4 chunk_observables(const float4* __restrict__ 
   return o;
 }
 
+// Energy (each bond once, by tetrahedra) and magnetisation of one chunk of
+// kJ1Threads cells, reduced over the CTA in a fixed order; thread 0 returns
+// (2 E, Mx, My, Mz) (the finalise step halves the site-sum convention of the
+// generic kernel, hence 2 E). Every thread of the CTA must call it.
+template <bool kL2Only>
+__device__ __forceinline__ double4 chunk_observables(const float4* __restrict__ rb, int cell,
+                                                     int L, int L3, float rcpL, double J1,
+                                                     double (*red)[kJ1Threads / 32]) {
+  double e = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+  if (cell < L3) {
+    int x, y, z;
+    decode_cell(cell, L, rcpL, &x, &y, &z);
+    const CellFrame f = make_frame(x, y, z, L);
+    cell_corner<0, kL2Only>(rb, f, cell, L3, &e, &mx, &my, &mz);
+    cell_corner<1, kL2Only>(rb, f, cell, L3, &e, &mx, &my, &mz);
+    cell_corner<2, kL2Only>(rb, f, cell, L3, &e, &mx, &my, &mz);
+    cell_corner<3, kL2Only>(rb, f, cell, L3, &e, &mx, &my, &mz);
+    e *= J1;
+  }
+  return block_observables(e, mx, my, mz, red);
+}
+
 // Each cell owns its 4 up-tetrahedra and the 4 down-tetrahedra that contain
 // its sublattice-0 sites: every bond is counted exactly once.
 __global__ void __launch_bounds__(kJ1Threads) j1_observables_kernel(const J1ObsParams p) {
@@ -398,6 +416,72 @@ __global__ void __launch_bounds__(kJ1Threads) j1_observables_kernel(const J1ObsP
   const float4* rb = p.spins + (long long)rep * 16 * p.L3;
   const double4 o = chunk_observables<false>(rb, cell, p.L, p.L3, p.rcpL, p.J1, red);
   if (threadIdx.x == 0) p.partials[p.partial_begin + (long long)rep * gridDim.x + blockIdx.x] = o;
+}
+
+// The two tetrahedra of the sublattice-3 site S = 4F + 3 of `cell` after a
+// colour-3 pass: the up-tetrahedron of corner F (sites 4F..4F + 3 of the
+// cell) and S's down-tetrahedron. Every tetrahedron holds exactly one
+// sublattice-3 site, so the cells' sums count each bond once; the up-
+// tetrahedra of a cell cover its 16 sites once (magnetisation). The
+// sublattice-3 spins are this thread's own stores of the pass, read back
+// through L2; the others were not written by the pass.
+template <int F>
+__device__ __forceinline__ void corner3_observables(const float4* __restrict__ rb,
+                                                    const CellFrame& f, int cell, int L3,
+                                                    double* e, double* mx, double* my,
+                                                    double* mz) {
+  constexpr int S = 4 * F + 3;
+  const float4 s0 = load_spin<false>(rb + (4 * F + 0) * L3 + cell);
+  const float4 s1 = load_spin<false>(rb + (4 * F + 1) * L3 + cell);
+  const float4 s2 = load_spin<false>(rb + (4 * F + 2) * L3 + cell);
+  const float4 s3 = load_spin<true>(rb + S * L3 + cell);
+  const float4 d1 = load_neighbour<S, j1_down_index(S, 0), false>(rb, f, L3);
+  const float4 d2 = load_neighbour<S, j1_down_index(S, 1), false>(rb, f, L3);
+  const float4 d3 = load_neighbour<S, j1_down_index(S, 2), false>(rb, f, L3);
+  *e += tet_energy(s0, s1, s2, s3) + tet_energy(s3, d1, d2, d3);
+  *mx += (double)s0.x + s1.x + s2.x + s3.x;
+  *my += (double)s0.y + s1.y + s2.y + s3.y;
+  *mz += (double)s0.z + s1.z + s2.z + s3.z;
+}
+
+// The last pass of a cycle (colour 3, cell form, isotropic J1) fused with
+// the FP64 energy and magnetisation partials of the state it leaves: the
+// same updates as j1_pass_kernel<3, kMetro, false>, then each cell's eight
+// tetrahedra from spins the pass just loaded (L1/L2), instead of a separate
+// observables kernel reading the lattice again. Partials in the layout of
+// j1_observables_kernel (one per CTA of kJ1Threads cells).
+template <bool kMetro>
+__global__ void __launch_bounds__(kJ1Threads) j1_last_pass_kernel(const J1PassParams p,
+                                                                  const J1ObsParams o) {
+  pass_prologue();
+  __shared__ double red[4][kJ1Threads / 32];
+  const int rep = blockIdx.y;
+  const int cell = blockIdx.x * kJ1Threads + threadIdx.x;
+  const int g = p.rep_global + rep;
+  float beta = 0.0f, cosmax = 0.0f;
+  int t = 0;
+  if (kMetro) {
+    t = p.temp_of_rep[p.temp_base + g];
+    beta = p.beta[p.temp_base + t];
+    cosmax = p.cosmax[p.temp_base + t];
+  }
+  int acc = 0;
+  double e = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+  if (cell < p.L3) {
+    acc = cell_pass<3, kMetro, false>(p, rep, cell, beta, cosmax);
+    int x, y, z;
+    decode_cell(cell, p.L, p.rcpL, &x, &y, &z);
+    const CellFrame f = make_frame(x, y, z, p.L);
+    const float4* rb = p.spins + (long long)rep * 16 * p.L3;
+    corner3_observables<0>(rb, f, cell, p.L3, &e, &mx, &my, &mz);
+    corner3_observables<1>(rb, f, cell, p.L3, &e, &mx, &my, &mz);
+    corner3_observables<2>(rb, f, cell, p.L3, &e, &mx, &my, &mz);
+    corner3_observables<3>(rb, f, cell, p.L3, &e, &mx, &my, &mz);
+    e *= o.J1;
+  }
+  if (kMetro) block_accept(p, t, acc);
+  const double4 r = block_observables(e, mx, my, mz, red);
+  if (threadIdx.x == 0) o.partials[o.partial_begin + (long long)rep * gridDim.x + blockIdx.x] = r;
 }
 
 // One site update of the cluster kernel: site S of `cell`, neighbours read
@@ -610,6 +694,22 @@ void launch_j1_pass(const J1PassParams& p, int colour, bool metro, bool site_per
     }
   }
 #undef PYRO_J1_CASE
+}
+
+void launch_j1_last_pass(const J1PassParams& p, const J1ObsParams& o, bool metro,
+                         cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((p.L3 + kJ1Threads - 1) / kJ1Threads, p.n_rep);
+  cfg.blockDim = dim3(kJ1Threads, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = p.pdl ? 1 : 0;
+  if (metro) cudaLaunchKernelEx(&cfg, j1_last_pass_kernel<true>, p, o);
+  else cudaLaunchKernelEx(&cfg, j1_last_pass_kernel<false>, p, o);
 }
 
 void launch_j1_observables(const J1ObsParams& p, cudaStream_t st) {

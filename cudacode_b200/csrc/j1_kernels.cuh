@@ -70,6 +70,10 @@ cudaError_t launch_j1_cycle(const J1CycleParams& p, cudaStream_t st);
 // size can be resident at once (0: size not supported).
 cudaError_t j1_cycle_prepare(int cluster_size, int* max_active_clusters);
 void launch_j1_observables(const J1ObsParams& p, cudaStream_t st);
+// The colour-3 pass (cell form, isotropic J1 only) with the observables
+// partials of the resulting state (as launch_j1_observables writes them).
+void launch_j1_last_pass(const J1PassParams& p, const J1ObsParams& o, bool metro,
+                         cudaStream_t st);
 
 inline int j1_blocks_per_replica(int L3) { return (L3 + kJ1Threads - 1) / kJ1Threads; }
 

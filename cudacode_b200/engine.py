@@ -286,6 +286,7 @@ class Engine:
     OPT_FAR_KERNEL = 9
     OPT_PDL = 10
     OPT_TET_GROUPED = 11
+    OPT_FUSED_OBS = 12
 
     def set_option(self, option: int, value: int) -> None:
         self._ck(self.lib.pyro_set_option(self.ctx, option, value))

@@ -119,6 +119,12 @@ int pyro_neighbour_table(int site, int* out120);
  * group's right after its plain sweeps on the same chain; 0 runs them over
  * all replicas after every group's plain sweeps. Identical results. */
 #define PYRO_OPT_TET_GROUPED 11
+/* PYRO_OPT_FUSED_OBS: 1 (default) computes the FP64 energy and magnetisation
+ * of an isotropic J1 replica group inside the group's last colour pass of a
+ * cycle (when that pass runs one cell per thread), from the spins the pass
+ * has just loaded; 0 runs a separate observables kernel after the pass.
+ * Same spins; energies equal up to FP64 summation order. */
+#define PYRO_OPT_FUSED_OBS 12
 int pyro_set_option(pyro_ctx* ctx, int option, int value);
 int pyro_get_option(pyro_ctx* ctx, int option, int* value);
 /* Autotuner: times every kernel variant (per-pass generic, per-pass J1,

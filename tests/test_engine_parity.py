@@ -456,3 +456,34 @@ def test_last_observables_are_the_cycle_energies(L, swap, group):
     E1, M1 = e.observables()
     np.testing.assert_allclose(E0, E1, rtol=1e-12, atol=1e-9)
     np.testing.assert_allclose(M0, M1.reshape(-1, 3), rtol=1e-12, atol=1e-9)
+
+
+@pytest.mark.parametrize("L,n_metro,n_or,site_mode,group,chains",
+                         [(6, 1, 3, 1, 2, 2), (5, 2, 0, 0, 3, 1), (8, 1, 1, 0, 4, 3)])
+def test_energies_from_the_last_pass(L, n_metro, n_or, site_mode, group, chains):
+    """The energies and magnetisations a replica group's last colour pass
+    computes (fused) equal a separate lattice-wide evaluation to FP64
+    rounding, and the chain (spins, exchange decisions) equals the one with
+    the separate observables kernel and the oracle's."""
+    temps = geometric_ladder(0.05, 1.0, 7)
+    runs = []
+    for fused in (1, 0):
+        e, o = pair([System(L=L, temperatures=temps)], renorm_every=3)
+        e.set_option(e.OPT_REPLICA_GROUP, group)
+        e.set_option(e.OPT_CHAINS, chains)
+        e.set_option(e.OPT_J1_SITE_MODE, site_mode)
+        e.set_option(e.OPT_FUSED_OBS, fused)
+        assert e.get_option(e.OPT_FUSED_OBS) == fused
+        e.init_random()
+        o.init_random()
+        e.cycle(n_metro, n_or, True, 4)
+        o.cycle(n_metro, n_or, True, 4)
+        assert np.array_equal(e.get_spins(), o.get_spins())
+        assert np.array_equal(e.permutation(), o.permutation())
+        E0, M0 = e.last_observables()
+        E1, M1 = e.observables()
+        np.testing.assert_allclose(E0, E1, rtol=1e-12, atol=1e-9)
+        np.testing.assert_allclose(M0, M1.reshape(-1, 3), rtol=1e-12, atol=1e-9)
+        runs.append((e.get_spins(), E0))
+    assert np.array_equal(runs[0][0], runs[1][0])
+    np.testing.assert_allclose(runs[0][1], runs[1][1], rtol=1e-12, atol=1e-9)
