@@ -654,6 +654,8 @@ def main():
                 step()
             stop.record(stream)
             torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
             launches_timed = eng.launch_count() - launches0
         ms = start.elapsed_time(stop)
     if world > 1:
