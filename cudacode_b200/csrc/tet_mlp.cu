@@ -649,13 +649,6 @@ __device__ __forceinline__ int tet_warp_step(const TetMoveParams& p, const MlpSm
   return accepted;
 }
 
-// Same move with two lanes per tetrahedron (16 per warp, one MMA m-tile):
-// lane l < 16 handles sites 0 and 1 of tetrahedron l, lane l + 16 sites 2
-// and 3 (their fields, proposals and stores), which halves the serial work
-// of a warp. Lane l then gathers the partner's values and evaluates the
-// energy change and the proposal ratio with exactly the single-lane
-// expressions, so the decisions are identical. Returns 1 on the lower lane
-// of an accepted move. kWait as in tet_warp_step.
 // Offset of down-tetrahedron neighbour M of site S from replica start.
 template <int S, int M>
 __device__ __forceinline__ int down_off(const Frame& f, int L3) {
@@ -671,6 +664,13 @@ __device__ __forceinline__ int pair_down_off(const Frame& f, int L3, int half) {
   return half ? hi : lo;
 }
 
+// Same move with two lanes per tetrahedron (16 per warp, one MMA m-tile):
+// lane l < 16 handles sites 0 and 1 of tetrahedron l, lane l + 16 sites 2
+// and 3 (their fields, proposals and stores), which halves the serial work
+// of a warp. Lane l then gathers the partner's values and evaluates the
+// energy change and the proposal ratio with exactly the single-lane
+// expressions, so the decisions are identical. Returns 1 on the lower lane
+// of an accepted move. kWait as in tet_warp_step.
 template <int F, bool kL2, bool kWait>
 __device__ __forceinline__ int tet_pair_step(const TetMoveParams& p, const MlpSmem& w, bool active,
                                              int rep, int cell, float beta,
