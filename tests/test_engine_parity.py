@@ -487,3 +487,22 @@ def test_energies_from_the_last_pass(L, n_metro, n_or, site_mode, group, chains)
         runs.append((e.get_spins(), E0))
     assert np.array_equal(runs[0][0], runs[1][0])
     np.testing.assert_allclose(runs[0][1], runs[1][1], rtol=1e-12, atol=1e-9)
+
+
+def test_option_and_proposal_values_are_checked():
+    e = Engine([System(L=4, temperatures=[0.5, 1.0])])
+    for opt in (e.OPT_TET_GROUPED, e.OPT_FUSED_OBS, e.OPT_PDL):
+        with pytest.raises(PyroError):
+            e.set_option(opt, 2)
+        with pytest.raises(PyroError):
+            e.set_option(opt, -1)
+    with pytest.raises(PyroError):  # the learned move is not initialised yet
+        e.tet_set_proposal(1)
+    with pytest.raises(PyroError):
+        e.cycle_tet(1, 1, 1, True, 1)
+    e.tet_init(seed=1)
+    for bad in (-1, 2):
+        with pytest.raises(PyroError):
+            e.tet_set_proposal(bad)
+    e.tet_set_proposal(0)
+    e.tet_set_proposal(1)
