@@ -142,6 +142,7 @@ int queue_observables(pyro_ctx* ctx, bool skip_j1 = false) {
     launch_observables(op, ctx->tab, ctx->obs_generic_blocks, ctx->stream);
     PYRO_CK_LAUNCH();
   }
+  if (ctx->defer_finalise) return PYRO_OK;  // the cycle's exchange kernel sums the partials
   launch_obs_finalise(ctx->d_partials, ctx->d_obs_segs, (int)ctx->obs_segs.size(), ctx->d_sys,
                       ctx->total_reps, ctx->d_rep_sys, ctx->d_rep_local, ctx->d_energy, ctx->d_mag,
                       ctx->stream);
@@ -1464,6 +1465,7 @@ static int run_cycles(pyro_ctx* ctx, int n_metro, int n_or, int n_tet, int do_sw
     int rc = check_cluster(ctx);  // sets kernel attributes: not inside a capture
     if (rc) return rc;
     PYRO_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    ctx->defer_finalise = true;  // the exchange kernel below finalises the observables
     if (n_tet == 0) {
       rc = queue_cycle_body(ctx, n_metro, n_or, true);
     } else if (tet_in_groups(ctx)) {
@@ -1474,8 +1476,13 @@ static int run_cycles(pyro_ctx* ctx, int n_metro, int n_or, int n_tet, int do_sw
       if (rc == PYRO_OK) rc = queue_tet_sweeps(ctx, n_tet);
       if (rc == PYRO_OK) rc = queue_observables(ctx);
     }
+    ctx->defer_finalise = false;
     if (rc == PYRO_OK) {
       ExchangeParams x = exchange_params(ctx);
+      x.partials = ctx->d_partials;
+      x.obs_segs = ctx->d_obs_segs;
+      x.energy_out = ctx->d_energy;
+      x.mag_out = ctx->d_mag;
       x.do_swap = do_swap ? 1 : 0;
       x.parity = -1;
       x.history = ctx->d_history;

@@ -92,6 +92,7 @@ struct pyro_ctx {
   int pdl = 1;         // programmatic dependent launch of the per-pass J1 kernels
   int tet_grouped = 1;  // learned sweeps inside the replica groups
   int fused_obs = 1;    // energy partials from a group's last pass (grouped J1 path)
+  bool defer_finalise = false;  // while a cycle is captured: its exchange kernel finalises
   std::vector<GenGroup> gen_groups;
   int n_chains = 1;     // concurrent streams the replica groups are dealt to
   cudaStream_t chain_stream[pyro::kMaxChains] = {};

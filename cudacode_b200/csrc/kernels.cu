@@ -304,15 +304,12 @@ __global__ void __launch_bounds__(kObsThreads) observables_kernel(const ObsParam
 }
 
 // One warp per replica: fixed-order sum of its partials.
-__global__ void obs_finalise_kernel(const double4* __restrict__ partials, const ObsSeg* segs,
-                                    const SysDev* sys, int total_reps, const int* rep_sys,
-                                    const int* rep_local, double* energy, double* mag) {
-  const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+// One warp sums the partials of replica r of system si in a fixed order and
+// writes its FP64 energy and magnetisation.
+__device__ __forceinline__ void finalise_replica(const double4* __restrict__ partials,
+                                                 const ObsSeg& sg, const SysDev& sd, int r,
+                                                 double* energy, double* mag) {
   const int lane = threadIdx.x & 31;
-  if (wid >= total_reps) return;
-  const int si = rep_sys[wid];
-  const int r = rep_local[wid];
-  const ObsSeg sg = segs[si];
   const double4* pp = partials + sg.block_begin + (long long)r * sg.blocks_per_rep;
   double e = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
   for (int b = lane; b < sg.blocks_per_rep; b += 32) {
@@ -327,12 +324,21 @@ __global__ void obs_finalise_kernel(const double4* __restrict__ partials, const 
   my = warp_sum(my);
   mz = warp_sum(mz);
   if (lane == 0) {
-    const int gi = sys[si].rep_ctx_base + r;
+    const int gi = sd.rep_ctx_base + r;
     energy[gi] = 0.5 * e;
     mag[3 * gi + 0] = mx;
     mag[3 * gi + 1] = my;
     mag[3 * gi + 2] = mz;
   }
+}
+
+__global__ void obs_finalise_kernel(const double4* __restrict__ partials, const ObsSeg* segs,
+                                    const SysDev* sys, int total_reps, const int* rep_sys,
+                                    const int* rep_local, double* energy, double* mag) {
+  const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (wid >= total_reps) return;
+  const int si = rep_sys[wid];
+  finalise_replica(partials, segs[si], sys[si], rep_local[wid], energy, mag);
 }
 
 // One block per system. Pairs (t, t+1) with t % 2 == parity exchange
@@ -344,6 +350,11 @@ __global__ void exchange_kernel(const ExchangeParams p) {
   const unsigned long long count = p.swap_count[si];
   __shared__ int n_acc;
   if (threadIdx.x == 0) n_acc = 0;
+  if (p.partials) {
+    const ObsSeg sg = p.obs_segs[si];
+    for (int r = threadIdx.x >> 5; r < sd.n_rep; r += blockDim.x >> 5)
+      finalise_replica(p.partials, sg, sd, r, p.energy_out, p.mag_out);
+  }
   __syncthreads();
   if (p.history) {
     const unsigned long long slot = *p.history_count % (unsigned long long)p.history_cap;
@@ -461,7 +472,7 @@ void launch_obs_finalise(const double4* partials, const ObsSeg* segs, int nseg, 
 }
 
 void launch_exchange(const ExchangeParams& p, int n_sys, int max_pairs, cudaStream_t st) {
-  int threads = 32;
+  int threads = p.partials ? 512 : 32;  // finalising: a warp per replica, 16 at a time
   while (threads < max_pairs && threads < 1024) threads *= 2;
   exchange_kernel<<<n_sys, threads, 0, st>>>(p);
 }

@@ -68,6 +68,13 @@ struct ExchangeParams {
   unsigned long long* sweep_ctr;   // advanced by sweep_advance (block 0) if non-null
   unsigned long long sweep_advance;
   int do_swap;
+  // Non-null: the block first sums its system's observables partials into
+  // energy and mag (as obs_finalise_kernel does, same order), so a cycle
+  // needs no separate finalise launch.
+  const double4* partials;
+  const ObsSeg* obs_segs;
+  double* energy_out;  // [rep_ctx_base + r]
+  double* mag_out;     // [3 (rep_ctx_base + r) + k]
 };
 
 void launch_colour_pass(const PassParams& p, const NbrTable& tab, int n_blocks, bool metro,
