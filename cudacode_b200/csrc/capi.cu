@@ -128,6 +128,7 @@ int queue_observables(pyro_ctx* ctx, bool skip_j1 = false) {
     jp.J1 = s.J64[0];
     jp.partials = ctx->d_partials;
     jp.partial_begin = ctx->obs_segs[si].partial_begin;
+    jp.pdl = ctx->pdl;
     launch_j1_observables(jp, ctx->stream);
     PYRO_CK_LAUNCH();
   }
@@ -223,6 +224,7 @@ int queue_grouped(pyro_ctx* ctx, int n_metro, int n_or, bool j1_grouped, bool ge
         jp.J1 = s.J64[0];
         jp.partials = ctx->d_partials;
         jp.partial_begin = ctx->obs_segs[si].partial_begin + r0 * j1_blocks_per_replica(s.L3);
+        jp.pdl = ctx->pdl;
         // the group's energy partials from its last pass when that pass runs
         // in the cell form (isotropic J1, no learned sweeps after it)
         const int n_sw = n_metro + n_or;

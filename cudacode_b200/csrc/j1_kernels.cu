@@ -410,6 +410,7 @@ __device__ __forceinline__ double4 chunk_observables(const float4* __restrict__ 
 // Each cell owns its 4 up-tetrahedra and the 4 down-tetrahedra that contain
 // its sublattice-0 sites: every bond is counted exactly once.
 __global__ void __launch_bounds__(kJ1Threads) j1_observables_kernel(const J1ObsParams p) {
+  pass_prologue();
   __shared__ double red[4][kJ1Threads / 32];
   const int rep = blockIdx.y;
   const int cell = blockIdx.x * kJ1Threads + threadIdx.x;
@@ -713,8 +714,17 @@ void launch_j1_last_pass(const J1PassParams& p, const J1ObsParams& o, bool metro
 }
 
 void launch_j1_observables(const J1ObsParams& p, cudaStream_t st) {
-  const dim3 grid((p.L3 + kJ1Threads - 1) / kJ1Threads, p.n_rep);
-  j1_observables_kernel<<<grid, kJ1Threads, 0, st>>>(p);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((p.L3 + kJ1Threads - 1) / kJ1Threads, p.n_rep);
+  cfg.blockDim = dim3(kJ1Threads, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = p.pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, j1_observables_kernel, p);  // errors are read back with cudaGetLastError
 }
 
 cudaError_t j1_cycle_prepare(int cluster_size, int* max_active_clusters) {

@@ -47,6 +47,7 @@ struct J1ObsParams {
   double J1;
   double4* partials;
   int partial_begin;
+  int pdl;  // programmatic dependent launch (waits for the previous kernel before reading)
 };
 
 // A whole cycle (n_metro + n_or sweeps, then observables partials if
