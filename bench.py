@@ -72,18 +72,51 @@ def hbm_peak():
 
 
 class ClockSampler:
-    """Samples SM clock and throttle reasons with nvidia-smi during a region."""
+    """Samples the SM clock and the clock-event (throttle) reasons during a
+    region: through NVML every 20 ms when the NVML binding is importable
+    (read-only queries), else through `nvidia-smi -lms 100`. The sampler is
+    running before the region starts."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, device_index: int):
         self.dev = device_index
         self.proc = None
+        self.nvml = None
+        self.stop = threading.Event()
         self.lines: list[str] = []
+        self.samples: list[tuple[float, float, set]] = []
 
     def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.dev)
+            self.nvml = (pynvml, h)
+            bits = {"hw_slowdown": pynvml.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": pynvml.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": pynvml.nvmlClocksEventReasonSwPowerCap}
+            mx = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+
+            def poll():
+                while True:
+                    sm = float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                    r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((sm, mx, {n for n, b in bits.items() if r & b}))
+                    if self.stop.wait(0.02):
+                        return
+
+            self.t = threading.Thread(target=poll, daemon=True)
+            self.t.start()
+            while not self.samples and self.t.is_alive():
+                time.sleep(0.001)
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
@@ -91,6 +124,9 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.perf_counter()
+            while not self.lines and time.perf_counter() - t0 < 3.0:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
         return self
@@ -100,6 +136,13 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *exc):
+        if self.nvml:
+            self.stop.set()
+            self.t.join(timeout=2)
+            try:
+                self.nvml[0].nvmlShutdown()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -109,7 +152,10 @@ class ClockSampler:
 
     def summary(self) -> dict:
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s_mhz, m_mhz, rs in self.samples:
+            sm.append(s_mhz)
+            mx = m_mhz
+            reasons |= rs
         for ln in self.lines:
             p = [x.strip() for x in ln.split(",")]
             if len(p) < 9:
@@ -119,11 +165,12 @@ class ClockSampler:
                 mx = float(p[2])
             except ValueError:
                 continue
-            for nm, v in zip(names, p[5:9]):
+            for nm, v in zip(self.NAMES, p[5:9]):
                 if v.lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvml" if self.samples else "nvidia-smi"}
 
 
 def cpu_baseline_sample(threads: int | None = None, replicas: int = 16, cycles: int = 25):
