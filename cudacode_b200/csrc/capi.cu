@@ -1068,6 +1068,51 @@ int pyro_get_spins(pyro_ctx* ctx, int system, float* host_xyzw) {
   if (!host_xyzw) return fail(ctx, PYRO_ERR_ARG, "get_spins: null pointer");
   return spin_copy(ctx, system, host_xyzw, nullptr, cudaMemcpyDeviceToHost, false, true);
 }
+// The reference's host layout: per replica three planes x, y, z of 16 L^3
+// values each (site index s L^3 + cell, as here), replicas one after another.
+int pyro_set_spins_planar(pyro_ctx* ctx, int system, const double* host_planes) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (!host_planes) return fail(ctx, PYRO_ERR_ARG, "set_spins_planar: null pointer");
+  if (system < 0 || system >= (int)ctx->sys.size())
+    return fail(ctx, PYRO_ERR_ARG, "set_spins_planar: bad system");
+  const SysDev& s = ctx->sys[system];
+  const size_t n = (size_t)16 * s.L3;
+  std::vector<float> buf(4 * n * (size_t)s.n_rep);
+  for (size_t r = 0; r < (size_t)s.n_rep; ++r) {
+    const double* x = host_planes + 3 * n * r;
+    for (size_t i = 0; i < n; ++i) {
+      float* o = buf.data() + 4 * (n * r + i);
+      o[0] = (float)x[i];
+      o[1] = (float)x[n + i];
+      o[2] = (float)x[2 * n + i];
+      o[3] = 0.0f;
+    }
+  }
+  return spin_copy(ctx, system, nullptr, buf.data(), cudaMemcpyHostToDevice, true, true);
+}
+
+int pyro_get_spins_planar(pyro_ctx* ctx, int system, double* host_planes) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (!host_planes) return fail(ctx, PYRO_ERR_ARG, "get_spins_planar: null pointer");
+  if (system < 0 || system >= (int)ctx->sys.size())
+    return fail(ctx, PYRO_ERR_ARG, "get_spins_planar: bad system");
+  const SysDev& s = ctx->sys[system];
+  const size_t n = (size_t)16 * s.L3;
+  std::vector<float> buf(4 * n * (size_t)s.n_rep);
+  const int rc = spin_copy(ctx, system, buf.data(), nullptr, cudaMemcpyDeviceToHost, false, true);
+  if (rc) return rc;
+  for (size_t r = 0; r < (size_t)s.n_rep; ++r) {
+    double* x = host_planes + 3 * n * r;
+    for (size_t i = 0; i < n; ++i) {
+      const float* v = buf.data() + 4 * (n * r + i);
+      x[i] = v[0];
+      x[n + i] = v[1];
+      x[2 * n + i] = v[2];
+    }
+  }
+  return PYRO_OK;
+}
+
 int pyro_set_spins_device(pyro_ctx* ctx, int system, const float* dev_xyzw) {
   if (!dev_xyzw) return fail(ctx, PYRO_ERR_ARG, "set_spins_device: null pointer");
   return spin_copy(ctx, system, nullptr, dev_xyzw, cudaMemcpyDeviceToDevice, true, false);

@@ -91,6 +91,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "pyro_init_random": (i, [P]),
         "pyro_set_spins": (i, [P, i, pf]),
         "pyro_get_spins": (i, [P, i, pf]),
+        "pyro_set_spins_planar": (i, [P, i, pd]),
+        "pyro_get_spins_planar": (i, [P, i, pd]),
         "pyro_set_spins_device": (i, [P, i, P]),
         "pyro_get_spins_device": (i, [P, i, P]),
         "pyro_metropolis_sweep": (i, [P, i]),
@@ -336,6 +338,20 @@ class Engine:
         if a.size != int(np.prod(self.spin_shape(system))):
             raise ValueError(f"expected {self.spin_shape(system)} spins, got {a.shape}")
         self._ck(self.lib.pyro_set_spins(self.ctx, system, _ptr(a, C.c_float)))
+
+    def get_spins_planar(self, system: int = 0) -> np.ndarray:
+        """Spins in the reference's layout: [replica][x, y, z][16 L^3], FP64."""
+        R, n = self.spin_shape(system)[0], int(np.prod(self.spin_shape(system)[1:-1]))
+        out = np.empty((R, 3, n), dtype=np.float64)
+        self._ck(self.lib.pyro_get_spins_planar(self.ctx, system, _ptr(out, C.c_double)))
+        return out
+
+    def set_spins_planar(self, planes: np.ndarray, system: int = 0) -> None:
+        R, n = self.spin_shape(system)[0], int(np.prod(self.spin_shape(system)[1:-1]))
+        a = np.ascontiguousarray(planes, dtype=np.float64)
+        if a.size != R * 3 * n:
+            raise ValueError(f"expected {(R, 3, n)} values, got {a.shape}")
+        self._ck(self.lib.pyro_set_spins_planar(self.ctx, system, _ptr(a, C.c_double)))
 
     def set_spins_device(self, ptr: int, system: int = 0) -> None:
         self._ck(self.lib.pyro_set_spins_device(self.ctx, system, C.c_void_p(ptr)))

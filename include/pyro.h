@@ -155,6 +155,13 @@ int pyro_system_info(const pyro_ctx* ctx, int system, int* L, int* n_sites,
 int pyro_init_random(pyro_ctx* ctx);
 int pyro_set_spins(pyro_ctx* ctx, int system, const float* host_xyzw);
 int pyro_get_spins(pyro_ctx* ctx, int system, float* host_xyzw);
+/* The same in the reference's spin layout (Sx = spin + 3 Offset, Sy = Sx +
+ * 16 L^3, Sz = Sy + 16 L^3, Pyrochlore.cu:288-290 with Offset = replica x
+ * 16 L^3, Math.cu:93): per replica three planes x, y, z of 16 L^3 doubles
+ * (site index s L^3 + cell), replicas consecutive; values are rounded to
+ * FP32 on the way in. Synchronous. */
+int pyro_set_spins_planar(pyro_ctx* ctx, int system, const double* host_planes);
+int pyro_get_spins_planar(pyro_ctx* ctx, int system, double* host_planes);
 /* Device-pointer variants (stream-ordered; the pointer must hold one system). */
 int pyro_set_spins_device(pyro_ctx* ctx, int system, const float* dev_xyzw);
 int pyro_get_spins_device(pyro_ctx* ctx, int system, float* dev_xyzw);

@@ -506,3 +506,26 @@ def test_option_and_proposal_values_are_checked():
             e.tet_set_proposal(bad)
     e.tet_set_proposal(0)
     e.tet_set_proposal(1)
+
+
+def test_spins_in_the_reference_layout():
+    """pyro_set/get_spins_planar use the reference's layout: per replica the
+    x, y and z planes of 16 L^3 values (site index s L^3 + cell)."""
+    s = System(L=3, temperatures=[0.5, 1.0, 2.0])
+    e = Engine([s], seed=4)
+    e.init_random()
+    f4 = e.get_spins()                        # [R][16][L^3][4]
+    planes = e.get_spins_planar()             # [R][3][16 L^3]
+    R = f4.shape[0]
+    expect = f4[..., :3].reshape(R, 16 * 27, 3).transpose(0, 2, 1)
+    assert np.array_equal(planes, expect.astype(np.float64))
+    rng = np.random.default_rng(2)
+    v = rng.normal(size=(R, 3, 16 * 27))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    e.set_spins_planar(v)
+    back = e.get_spins()
+    assert np.array_equal(back[..., :3].reshape(R, 16 * 27, 3),
+                          v.transpose(0, 2, 1).astype(np.float32))
+    assert np.all(back[..., 3] == 0.0)
+    with pytest.raises(ValueError):
+        e.set_spins_planar(v[:, :2])
