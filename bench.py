@@ -506,7 +506,8 @@ def run_learned(args):
     t0 = time.perf_counter()
     loss0 = eng.tet_train(1, 4096, 2e-3)
     loss = eng.tet_train(1500, 4096, 2e-3)
-    loss = eng.tet_train(1500, 4096, 5e-4)
+    loss = eng.tet_train(4500, 4096, 5e-4)
+    loss = eng.tet_train(3000, 4096, 2e-4)
     train_s = time.perf_counter() - t0
     choice = eng.autotune(1, 4, 5)
 
