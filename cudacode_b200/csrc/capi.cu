@@ -947,7 +947,8 @@ int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen)
                            {1, 0, 16, 1, 3, 2, 0}, {1, 0, 16, 1, 2, 2, 0}, {1, 0, 16, 1, 2, 3, 0},
                            {1, 0, 16, 1, 3, 3, 0}, {1, 0, 16, 1, 2, 4, 0}, {1, 0, 16, 1, 1, 4, 0},
                            {1, 1, 16, 1, 0, 1, 0}, {1, 1, 10, 1, 0, 1, 0}, {1, 0, 16, 1, 6, 2, 0},
-                           {1, 0, 16, 1, 4, 3, 0}, {1, 0, 16, 1, 5, 2, 0}};
+                           {1, 0, 16, 1, 4, 3, 0}, {1, 0, 16, 1, 5, 2, 0}, {1, 0, 16, 3, 2, 4, 0},
+                           {1, 0, 16, 3, 2, 2, 0}, {1, 0, 16, 3, 1, 4, 0}};
     vs.insert(vs.end(), std::begin(j1v), std::end(j1v));
     n_j1 = (int)vs.size();
   }
