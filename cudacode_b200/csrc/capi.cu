@@ -874,7 +874,7 @@ int pyro_set_option(pyro_ctx* ctx, int option, int value) {
     if (value < 0) return fail(ctx, PYRO_ERR_ARG, "group size in MB must be >= 0");
     ctx->gen_group_mb = value;
   } else if (option == PYRO_OPT_CHAINS) {
-    if (value < 1 || value > kMaxChains) return fail(ctx, PYRO_ERR_ARG, "chains is 1..4");
+    if (value < 1 || value > kMaxChains) return fail(ctx, PYRO_ERR_ARG, "chains is 1..8");
     ctx->n_chains = value;
   } else if (option == PYRO_OPT_REPLICA_GROUP) {
     if (value < 0) return fail(ctx, PYRO_ERR_ARG, "replica group must be >= 0");
@@ -948,7 +948,8 @@ int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen)
                            {1, 0, 16, 1, 3, 3, 0}, {1, 0, 16, 1, 2, 4, 0}, {1, 0, 16, 1, 1, 4, 0},
                            {1, 1, 16, 1, 0, 1, 0}, {1, 1, 10, 1, 0, 1, 0}, {1, 0, 16, 1, 6, 2, 0},
                            {1, 0, 16, 1, 4, 3, 0}, {1, 0, 16, 1, 5, 2, 0}, {1, 0, 16, 3, 2, 4, 0},
-                           {1, 0, 16, 3, 2, 2, 0}, {1, 0, 16, 3, 1, 4, 0}};
+                           {1, 0, 16, 3, 2, 2, 0}, {1, 0, 16, 3, 1, 4, 0}, {1, 0, 16, 1, 2, 6, 0},
+                           {1, 0, 16, 1, 1, 8, 0}, {1, 0, 16, 1, 1, 6, 0}};
     vs.insert(vs.end(), std::begin(j1v), std::end(j1v));
     n_j1 = (int)vs.size();
   }

@@ -14,7 +14,7 @@
 
 namespace pyro {
 struct TetState;  // learned tetrahedron move (tet_capi.cu)
-constexpr int kMaxChains = 4;
+constexpr int kMaxChains = 8;
 }
 
 struct pyro_ctx {

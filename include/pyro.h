@@ -95,7 +95,7 @@ int pyro_neighbour_table(int site, int* out120);
  * one group of this many replicas before the next group (0, default: all
  * replicas in every pass), keeping a group's spins in L2. Identical results. */
 #define PYRO_OPT_REPLICA_GROUP 6
-/* PYRO_OPT_CHAINS: 1..4 concurrent streams (parallel branches of the cycle
+/* PYRO_OPT_CHAINS: 1..8 concurrent streams (parallel branches of the cycle
  * graph) the replica groups are dealt to. Identical results. */
 #define PYRO_OPT_CHAINS 7
 /* PYRO_OPT_GROUP_MB: run the generic (J2/J3) colour passes over groups of
