@@ -173,6 +173,55 @@ class ClockSampler:
                 "source": "nvml" if self.samples else "nvidia-smi"}
 
 
+KERNEL_OPTIONS = ("J1_KERNEL", "CYCLE_KERNEL", "CLUSTER_SIZE", "J1_SITE_MODE", "REPLICA_GROUP",
+                  "CHAINS", "PDL", "FUSED_OBS")
+
+
+def cpu_baseline_and_parity(kernel_options: dict, cycles: int = 6):
+    """The cpu_baseline leg at the benchmark's own workload: the oracle port
+    runs `cycles` whole cycles (1 M + 4 OR sweeps, FP64 energies, exchange)
+    of all replicas of the L=32 ladder on every host core, timed; a fresh
+    engine context with the kernel schedule that was timed runs the same
+    cycles from the same seed, and its spins, permutation and energies are
+    checked against the oracle's (bit for bit; energies to FP64 rounding)."""
+    from cudacode_b200.engine import Engine, System, geometric_ladder
+    from oracle.binding import Oracle
+
+    temps = geometric_ladder(T_MIN, T_MAX, R_PER_GPU)
+    sysd = System(L=L, temperatures=temps)
+    cones = np.full(R_PER_GPU, 0.3, dtype=np.float32)
+    o = Oracle([sysd], seed=SEED, threads=os.cpu_count())
+    o.init_random()
+    o.set_cone(cones)
+    t0 = time.perf_counter()
+    o.cycle(N_METRO, N_OR, True, cycles)
+    dt = time.perf_counter() - t0
+    n_threads = o.lib.orc_set_threads(0)
+    updates = R_PER_GPU * 16 * L ** 3 * (N_METRO + N_OR) * cycles
+    cpu = {"value": updates / (dt * 1e9), "unit": "updates/ns", "cores": n_threads, "kind": "port",
+           "sample": f"all {R_PER_GPU} replicas, {cycles} cycles ({dt:.1f} s)"}
+    e = Engine([sysd], seed=SEED)
+    for name, value in kernel_options.items():
+        e.set_option(getattr(Engine, "OPT_" + name), value)
+    e.init_random()
+    e.set_cone(cones)
+    e.cycle(N_METRO, N_OR, True, cycles)
+    a, b = e.get_spins(), o.get_spins()
+    E0, _ = e.last_observables()
+    E1, _ = o.observables()
+    exact = bool(np.array_equal(a, b) and np.array_equal(e.permutation(), o.permutation()))
+    e_ok = bool(np.allclose(E0, E1, rtol=1e-12, atol=1e-9))
+    parity = {"check": "bit-exact" if exact and e_ok else "MISMATCH",
+              "what": f"the timed kernel schedule on a fresh context of the same workload and seed, "
+                      f"{cycles} cycles, all {R_PER_GPU} replicas, against the oracle: spins and "
+                      f"exchange permutation bit for bit, FP64 energies to rel 1e-12",
+              "max_spin_diff": float(np.abs(a - b).max()),
+              "max_energy_rel_diff": float(np.max(np.abs(E0 - E1) / np.maximum(np.abs(E1), 1.0)))}
+    e.close()
+    o.close()
+    return cpu, parity
+
+
 def cpu_baseline_sample(threads: int | None = None, replicas: int = 16, cycles: int = 25):
     """The reference algorithm's CPU path (oracle port) on a bounded sample."""
     from cudacode_b200.engine import System, geometric_ladder
@@ -598,6 +647,62 @@ def run_learned(args):
     return 0
 
 
+WAVE_PROFILE = os.path.join(ROOT, "profiles", "wave_kernel_L32_R64.md")
+
+
+def profiled_instructions():
+    """Warp instructions per spin update of the work-queue cycle kernel, from
+    its committed ncu summary (line 'warp_instructions_per_update: X')."""
+    try:
+        with open(WAVE_PROFILE) as f:
+            for line in f:
+                if line.startswith("warp_instructions_per_update:"):
+                    return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+def relaunch_under_torchrun(args) -> int | None:
+    """`--gpus N` (N > 1) outside torchrun runs this script again as N ranks
+    through torch.distributed.run (one process per GPU, 127.0.0.1
+    rendezvous); under torchrun, WORLD_SIZE must equal N."""
+    world = os.environ.get("WORLD_SIZE")
+    if world is None:
+        if args.gpus <= 1:
+            return None
+        import socket
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+               f"--nproc-per-node={args.gpus}", "--master-addr", "127.0.0.1",
+               "--master-port", str(port), os.path.abspath(__file__), *sys.argv[1:]]
+        return subprocess.call(cmd)
+    if int(world) != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}", file=sys.stderr)
+        return 2
+    return None
+
+
+def run_dry(args) -> int:
+    """Launcher check without a GPU: the ranks meet over gloo, and rank 0
+    prints the line's n_gpus (the world size)."""
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("gloo", timeout=timedelta(seconds=60))
+        t = __import__("torch").tensor([rank])
+        dist.all_reduce(t)
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({"dry_run": True, "n_gpus": world, "gpus_arg": args.gpus}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -606,6 +711,8 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--dry-run", action="store_true",
+                    help="check the launcher only: ranks meet over gloo, no GPU work")
     ap.add_argument("--L", type=int, default=L, help="lattice size (profiling cases)")
     ap.add_argument("--replicas", type=int, default=R_PER_GPU, help="replicas per GPU")
     ap.add_argument("--workload", default="pt",
@@ -615,13 +722,22 @@ def main():
                          "small: L=4 on the GPU and on the host; batched: 256 uneven "
                          "systems; large: L=64 with J2/J3, S(q) and FP64 error accounting; "
                          "aniso: the reference's anisotropic J1-J4 model with a field")
-    ap.add_argument("--kernel", default="auto", choices=["auto", "pass", "cluster", "grouped"],
+    ap.add_argument("--kernel", default="auto",
+                    choices=["auto", "pass", "cluster", "grouped", "wave"],
                     help="auto: autotuner picks; pass: one launch per colour pass; "
                          "cluster: cluster-resident cycle kernel; grouped: per-pass kernels "
-                         "over replica groups (--group) on concurrent chains (--chains)")
+                         "over replica groups (--group) on concurrent chains (--chains); "
+                         "wave: the work-queue cycle kernel over replica groups (--group), "
+                         "pass forms --site-mode")
     ap.add_argument("--group", type=int, default=4)
     ap.add_argument("--chains", type=int, default=2)
+    ap.add_argument("--site-mode", type=int, default=3)
     args = ap.parse_args()
+    rc = relaunch_under_torchrun(args)
+    if rc is not None:
+        return rc
+    if args.dry_run:
+        return run_dry(args)
     if args.workload == "learned":
         return run_learned(args)
     if args.workload == "small":
@@ -647,6 +763,9 @@ def main():
     torch.cuda.set_device(local)
     if world > 1:
         from datetime import timedelta
+        # the communicator's INIT lines name the ranks that joined
+        os.environ.setdefault("NCCL_DEBUG", "INFO")
+        os.environ.setdefault("NCCL_DEBUG_SUBSYS", "INIT")
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     n_gpus = world
 
@@ -666,16 +785,20 @@ def main():
         # variant gives the same chain)
         variant = eng.autotune(N_METRO, N_OR, 16)
     else:
-        eng.set_option(eng.OPT_CYCLE_KERNEL, 1 if args.kernel == "cluster" else 0)
-        if args.kernel == "grouped":
+        eng.set_option(eng.OPT_CYCLE_KERNEL, {"cluster": 1, "wave": 2}.get(args.kernel, 0))
+        if args.kernel in ("grouped", "wave"):
             eng.set_option(eng.OPT_REPLICA_GROUP, args.group)
+        if args.kernel == "grouped":
             eng.set_option(eng.OPT_CHAINS, args.chains)
-    kernel_desc = {"cycle_kernel": eng.get_option(eng.OPT_CYCLE_KERNEL),
-                   "cluster_size": eng.get_option(eng.OPT_CLUSTER_SIZE),
-                   "j1_kernel": eng.get_option(eng.OPT_J1_KERNEL),
-                   "replica_group": eng.get_option(eng.OPT_REPLICA_GROUP),
-                   "chains": eng.get_option(eng.OPT_CHAINS),
-                   "j1_site_mode": eng.get_option(eng.OPT_J1_SITE_MODE), "autotune_choice": variant}
+        if args.kernel == "wave":
+            eng.set_option(eng.OPT_J1_SITE_MODE, args.site_mode)
+    options = {n: eng.get_option(getattr(Engine, "OPT_" + n)) for n in KERNEL_OPTIONS}
+    kernel_desc = {"cycle_kernel": options["CYCLE_KERNEL"],
+                   "cluster_size": options["CLUSTER_SIZE"],
+                   "j1_kernel": options["J1_KERNEL"],
+                   "replica_group": options["REPLICA_GROUP"],
+                   "chains": options["CHAINS"],
+                   "j1_site_mode": options["J1_SITE_MODE"], "autotune_choice": variant}
     if world > 1:
         from cudacode_b200.distributed import EngineBackend, ShardedPT
         pt = ShardedPT(EngineBackend(eng, torch.device(f"cuda:{local}")), R_PER_GPU * n_gpus)
@@ -705,6 +828,7 @@ def main():
             if world > 1:
                 dist.barrier()
             launches_timed = eng.launch_count() - launches0
+        eng.synchronize()  # raises if a bounded device wait ran out
         ms = start.elapsed_time(stop)
     if world > 1:
         t = torch.tensor([ms], device=f"cuda:{local}")
@@ -712,6 +836,7 @@ def main():
         ms = float(t.item())
     updates = R_PER_GPU * n_gpus * 16 * L ** 3 * (N_METRO + N_OR) * args.steps
     value = updates / (ms * 1e6)
+    clocks = clk.summary()
 
     peak, peak_kind = hbm_peak()
     # End to end through the C-ABI with host buffers: each step uploads the cone
@@ -732,13 +857,31 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MIN)
         e2e_value = float(t.item()) * 1.0
 
-    # Dominant kernel: the over-relaxation colour pass (16 of the 20 passes of
-    # a step). Its roofline is taken as a kernel streaming the lattice from
-    # HBM: one launch per colour pass over all replicas (no replica groups),
-    # 80 algorithmic bytes per update, timed with CUDA events on the engine's
-    # stream. The timed schedule itself runs the same kernel on replica groups
-    # whose spins stay in L2 across their passes, so its HBM bytes are one
-    # read and one write of the lattice per cycle (32 B per 5 updates).
+    # Roofline of the timed step. With the work-queue kernel (or replica
+    # groups) a replica stays in L2 for all 20 passes of its cycle, so the
+    # step's algorithmic HBM bytes are one read and one write of every spin
+    # per cycle: 32 B per 5 updates. The binding resource is instruction
+    # issue: warp instructions per update (ncu, committed summary) times the
+    # updates, over 4 schedulers x the SMs x the sampled SM clock x the time.
+    l2_resident = (kernel_desc["replica_group"] > 0 or kernel_desc["cycle_kernel"] > 0)
+    sched_bytes = 32.0 / (N_METRO + N_OR) if l2_resident else float(BYTES_PER_UPDATE_PASS)
+    step_ms = ms / args.steps
+    step_updates = R_PER_GPU * 16 * L ** 3 * (N_METRO + N_OR)  # per GPU
+    achieved = step_updates * sched_bytes / (step_ms * 1e-3) / 1e9
+    wave = kernel_desc["cycle_kernel"] == 2
+    ipu = profiled_instructions() if (wave and (L, R_PER_GPU) == (32, 64)) else None
+    props = torch.cuda.get_device_properties(local)
+    issue = None
+    if ipu and clocks.get("sm_mhz"):
+        issue_slots = props.multi_processor_count * 4 * clocks["sm_mhz"] * 1e6 * step_ms * 1e-3
+        issue = {"resource": "warp-instruction issue (4 schedulers per SM)",
+                 "warp_instructions_per_update": ipu,
+                 "frac": ipu * step_updates / issue_slots,
+                 "sm_mhz": clocks["sm_mhz"], "sms": props.multi_processor_count,
+                 "source": "profiles/wave_kernel_L32_R64.md (ncu smsp__inst_executed.sum)"}
+
+    # The streaming form of the same passes, for comparison: one launch per
+    # colour pass over all replicas, 80 algorithmic bytes per update.
     pass_updates = R_PER_GPU * 16 * L ** 3 // 4
     or_ms = None
     if world == 1:
@@ -754,17 +897,12 @@ def main():
             b.record(stream)
             torch.cuda.synchronize()
             or_ms = a.elapsed_time(b) / (n_or_timed * 4)  # per colour pass
-    achieved = pass_updates * BYTES_PER_UPDATE_PASS / (or_ms * 1e-3) / 1e9 if or_ms else None
-    traffic = profiled_traffic() if (L, R_PER_GPU) == (32, 64) else None
-    l2_resident = kernel_desc["replica_group"] > 0 or kernel_desc["cycle_kernel"] > 0
-    sched_bytes = 32.0 / (N_METRO + N_OR) if l2_resident else float(BYTES_PER_UPDATE_PASS)
-    sched_gbs = value * sched_bytes  # updates/ns x bytes = GB/s
+    stream_gbs = pass_updates * BYTES_PER_UPDATE_PASS / (or_ms * 1e-3) / 1e9 if or_ms else None
+    eng.close()
 
-    cpu = None
+    cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, nt, dt, sample = cpu_baseline_sample()
-        cpu = {"value": v, "unit": "updates/ns", "cores": nt, "kind": "port",
-               "sample": sample + f" ({dt:.1f} s)"}
+        cpu, parity = cpu_baseline_and_parity(options)
 
     if rank == 0:
         line = {
@@ -773,34 +911,37 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (random unit spins from Philox seed)",
             "config": dict(workload_config(n_gpus), kernels=kernel_desc),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak if achieved else None, "peak_kind": peak_kind,
-                         "kernel": "j1_pass_kernel<colour, over-relaxation>: one launch per "
-                                   "colour pass over all replicas, streaming from HBM",
-                         "bytes_per_update": BYTES_PER_UPDATE_PASS,
-                         "updates_per_launch": pass_updates, "ms_per_launch": or_ms,
-                         "traffic": traffic,
-                         "schedule": {
-                             "what": ("the timed schedule: the same kernels on replica groups "
-                                      "whose spins stay in L2 across a cycle's 20 passes"
-                                      if l2_resident else
-                                      "the timed schedule: one launch per colour pass"),
-                             "hbm_bytes_per_update": sched_bytes, "achieved": sched_gbs,
-                             "frac": sched_gbs / peak,
-                             "note": ("one read + one write of the lattice per cycle; the "
-                                      "schedule is bound by latency, occupancy and the "
-                                      "Metropolis update's instruction issue, not HBM"
-                                      if l2_resident else
-                                      "every pass streams the lattice from HBM")}},
+            "roofline": {
+                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind,
+                "kernel": ("j1_wave_kernel: the step's sweeps and energies in one work-queue "
+                           "launch (plus a 33 KB memset and the exchange kernel)" if wave else
+                           "the step's per-pass J1 kernels over replica groups" if l2_resident
+                           else "j1_pass_kernel, one launch per colour pass"),
+                "bytes_per_update": sched_bytes, "updates_per_launch": step_updates,
+                "ms_per_launch": step_ms,
+                "traffic": None,
+                "binding": issue,
+                "note": ("HBM is not the bound of this schedule: each replica group stays in L2 "
+                         "for its cycle, so HBM sees one read and one write per spin per cycle; "
+                         "the binding resource is instruction issue (binding.frac)"
+                         if l2_resident else "every pass streams the lattice from HBM"),
+                "streaming_pass": {
+                    "what": "j1_pass_kernel<colour, over-relaxation> streaming from HBM, one "
+                            "launch per colour pass over all replicas (not the timed schedule)",
+                    "bytes_per_update": BYTES_PER_UPDATE_PASS, "updates_per_launch": pass_updates,
+                    "ms_per_launch": or_ms, "achieved": stream_gbs,
+                    "frac": stream_gbs / peak if stream_gbs else None,
+                    "traffic": profiled_traffic() if (L, R_PER_GPU) == (32, 64) else None}},
             "cpu_baseline": cpu,
+            "parity": parity,
             "e2e": {"value": e2e_value, "unit": "updates/ns",
                     "h2d_bytes_per_step": 4 * len(temps),
                     "d2h_bytes_per_step": 8 * R_PER_GPU + 24 * R_PER_GPU},
             "gpu_launches": launches_timed,
-            "clocks": clk.summary(),
+            "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
-    eng.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

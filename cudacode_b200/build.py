@@ -15,6 +15,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
@@ -60,6 +61,7 @@ def build_engine(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(build_dir, exist_ok=True)
     common = [nvcc(), *ARCH, "-lineinfo", "-O3", "--fmad=false", "-std=c++17",
               "-Xcompiler", "-fPIC,-O3,-ffp-contract=off", "-I", os.path.join(ROOT, "include")]
+    cmds = []
     for src in ENGINE_SOURCES:
         obj = os.path.join(build_dir, src.rsplit(".", 1)[0] + ".o")
         cmd = [*common, "-c", os.path.join(CSRC, src), "-o", obj]
@@ -67,8 +69,16 @@ def build_engine(force: bool = False, verbose: bool = False) -> str:
             cmd = [*common, "-x", "cu", "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(obj)
+    # Translation units compile independently: one nvcc per source, in parallel.
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as pool:
+        for res in pool.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds):
+            if res.returncode != 0:
+                sys.stderr.write(res.stdout + res.stderr)
+                raise subprocess.CalledProcessError(res.returncode, res.args)
+            if verbose and (res.stdout or res.stderr):
+                sys.stderr.write(res.stdout + res.stderr)
     tmp = LIB + ".tmp"
     subprocess.run([nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"], check=True)
     os.replace(tmp, LIB)

@@ -156,7 +156,7 @@ int queue_observables(pyro_ctx* ctx, bool skip_j1 = false) {
 int check_cluster(pyro_ctx* ctx) {
   if (ctx->cluster_checked) return PYRO_OK;
   ctx->cluster_checked = true;
-  if (!ctx->cycle_kernel) return PYRO_OK;
+  if (ctx->cycle_kernel != 1) return PYRO_OK;
   for (int cs = ctx->cluster_size; cs >= 1; cs = cs > 8 ? 8 : cs / 2) {
     int n = 0;
     cudaError_t e = j1_cycle_prepare(cs, &n);
@@ -173,8 +173,113 @@ int check_cluster(pyro_ctx* ctx) {
 // The cluster-resident cycle kernel runs isotropic J1 systems only; with a
 // bond-matrix system on the J1 path every J1 system takes per-pass kernels.
 bool use_cycle_kernel(const pyro_ctx* ctx) {
-  return ctx->cycle_kernel && ctx->use_j1_kernel && !ctx->obs_j1.empty() &&
+  return ctx->cycle_kernel == 1 && ctx->use_j1_kernel && !ctx->obs_j1.empty() &&
          ctx->j1_sys.size() == ctx->obs_j1.size();
+}
+
+// The work-queue cycle kernel runs the J1 systems of a cycle without
+// learned sweeps.
+bool use_wave_kernel(const pyro_ctx* ctx, int n_metro, int n_or, int n_tet) {
+  return ctx->cycle_kernel == 2 && ctx->use_j1_kernel && !ctx->j1_sys.empty() && n_tet == 0 &&
+         n_metro + n_or > 0;
+}
+
+constexpr size_t kWaveTicketWords = 32;  // a system's queue ticket, padded to 128 bytes
+
+// Work-queue buffers for the current systems (allocated outside any capture).
+int prepare_wave(pyro_ctx* ctx) {
+  size_t words = 0;
+  for (int si : ctx->j1_sys) {
+    const SysDev& s = ctx->sys[si];
+    words += kWaveTicketWords + (size_t)s.n_rep * j1_blocks_per_replica(s.L3);
+  }
+  if (words > ctx->wave_words) {
+    if (ctx->d_wave) cudaFree(ctx->d_wave);
+    ctx->d_wave = nullptr;
+    ctx->wave_words = 0;
+    PYRO_CK(alloc(&ctx->d_wave, words));
+    ctx->wave_words = words;
+  }
+  if (!ctx->d_wave_status) {
+    PYRO_CK(cudaHostAlloc((void**)&ctx->h_wave_status, sizeof(int), cudaHostAllocDefault));
+    *ctx->h_wave_status = 0;
+    PYRO_CK(alloc(&ctx->d_wave_status, 1));
+    PYRO_CK(cudaMemset(ctx->d_wave_status, 0, sizeof(int)));
+  }
+  return PYRO_OK;
+}
+
+// One work-queue launch per J1 system: n_metro + n_or sweeps and, with
+// with_obs, the energy partials of isotropic systems (the others' come from
+// the generic observables kernel).
+int queue_wave(pyro_ctx* ctx, int n_metro, int n_or, bool with_obs) {
+  if (!ctx->d_wave || !ctx->d_wave_status) return fail(ctx, PYRO_ERR_STATE, "work queue not prepared");
+  PYRO_CK(cudaMemsetAsync(ctx->d_wave, 0, ctx->wave_words * sizeof(unsigned int), ctx->stream));
+  const int forms = (ctx->j1_metro_site_mode ? 1 : 0) | (ctx->j1_or_site_mode ? 2 : 0);
+  size_t off = 0;
+  for (int si : ctx->j1_sys) {
+    const SysDev& s = ctx->sys[si];
+    J1WaveParams w;
+    std::memset(&w, 0, sizeof w);
+    w.pass = j1_params(ctx, si, 0);
+    w.pass.pdl = 0;
+    w.n_metro = n_metro;
+    w.n_or = n_or;
+    w.group = ctx->rep_group > 0 ? std::min(ctx->rep_group, s.n_rep) : s.n_rep;
+    w.n_chunks = j1_blocks_per_replica(s.L3);
+    w.dep = j1_wave_dep(s.L);
+    w.with_obs = with_obs && s.exch < 0 ? 1 : 0;
+    w.obs.spins = ctx->d_spins + s.spin_off;
+    w.obs.L = s.L;
+    w.obs.L3 = s.L3;
+    w.obs.n_rep = s.n_rep;
+    w.obs.rcpL = 1.0f / (float)s.L;
+    w.obs.J1 = s.J64[0];
+    w.obs.partials = ctx->d_partials;
+    w.obs.partial_begin = ctx->obs_segs[si].partial_begin;
+    w.sub_metro = (forms & 1) ? 4 : 1;
+    w.sub_or = (forms & 2) ? 4 : 1;
+    w.queue = ctx->d_wave + off;
+    w.progress = ctx->d_wave + off + kWaveTicketWords;
+    w.status = ctx->d_wave_status;
+    const long long items = (long long)s.n_rep * w.n_chunks *
+                            (4ll * n_metro * w.sub_metro + 4ll * n_or * w.sub_or + w.with_obs);
+    if (items > 0x7fffffffll) return fail(ctx, PYRO_ERR_ARG, "work-queue kernel: too many items");
+    w.n_items = (int)items;
+    w.spin_limit = ctx->wave_stall_item >= 0 ? 4096u : (1u << 20);
+    w.stall_item = ctx->wave_stall_item;
+    PYRO_CK(launch_j1_wave(w, forms, ctx->stream));
+    off += kWaveTicketWords + (size_t)s.n_rep * w.n_chunks;
+  }
+  return PYRO_OK;
+}
+
+// Queues the copy of the work-queue kernel's status word to pinned host
+// memory (read by wave_status_result after the stream synchronised).
+int queue_wave_status(pyro_ctx* ctx) {
+  if (!ctx->d_wave_status) return PYRO_OK;
+  PYRO_CK(cudaMemcpyAsync(ctx->h_wave_status, ctx->d_wave_status, sizeof(int),
+                          cudaMemcpyDeviceToHost, ctx->stream));
+  return PYRO_OK;
+}
+
+// After the stream synchronised: a dependency wait that gave up turns into
+// PYRO_ERR_TIMEOUT, and the status word is cleared.
+int wave_status_result(pyro_ctx* ctx) {
+  if (!ctx->d_wave_status || *ctx->h_wave_status == 0) return PYRO_OK;
+  *ctx->h_wave_status = 0;
+  PYRO_CK(cudaMemset(ctx->d_wave_status, 0, sizeof(int)));
+  return fail(ctx, PYRO_ERR_TIMEOUT,
+              "work-queue cycle kernel: a dependency wait ran out; the spins are partly updated");
+}
+
+// Synchronous check of the status word (for calls that synchronise anyway).
+int check_wave_status(pyro_ctx* ctx) {
+  if (!ctx->d_wave_status) return PYRO_OK;
+  int rc = queue_wave_status(ctx);
+  if (rc) return rc;
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  return wave_status_result(ctx);
 }
 
 // n_metro Metropolis + n_or over-relaxation sweeps of every system, and (if
@@ -307,6 +412,16 @@ bool j1_grouped_path(const pyro_ctx* ctx) {
 int queue_cycle_body(pyro_ctx* ctx, int n_metro, int n_or, bool with_obs, int n_tet = 0) {
   int rc = check_cluster(ctx);
   if (rc) return rc;
+  if (use_wave_kernel(ctx, n_metro, n_or, n_tet)) {
+    // other systems on their usual kernels, then one launch per J1 system
+    if (!ctx->gen_groups.empty())
+      rc = queue_grouped(ctx, n_metro, n_or, false, true, with_obs, 0);
+    else
+      rc = queue_generic_sweeps(ctx, n_metro, n_or);
+    if (rc == PYRO_OK) rc = queue_wave(ctx, n_metro, n_or, with_obs);
+    if (rc == PYRO_OK && with_obs) rc = queue_observables(ctx, /*skip_j1=*/true);
+    return rc;
+  }
   const bool cyc = use_cycle_kernel(ctx);
   const bool j1_grouped = j1_grouped_path(ctx);
   const bool gen_grouped = !ctx->gen_groups.empty();
@@ -432,9 +547,15 @@ void free_all(pyro_ctx* c) {
                   c->d_obs_segs,    c->d_partials,     c->d_sweep,       c->d_scratch_u64,
                   c->d_history,     c->d_history_count, c->d_obs_generic,
                   c->d_sq_s1,       c->d_sq_s2,        c->d_sq_s3,       c->d_sq_tw,
-                  c->d_sq_out,      c->d_exch,         c->d_submag,      c->d_order};
+                  c->d_sq_out,      c->d_exch,         c->d_submag,      c->d_order,
+                  c->d_wave,        c->d_wave_status};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  if (c->h_wave_status) cudaFreeHost(c->h_wave_status);
+  c->h_wave_status = nullptr;
+  c->d_wave = nullptr;
+  c->d_wave_status = nullptr;
+  c->wave_words = 0;
   for (auto* p : c->d_pass_segs)
     if (p) cudaFree(p);
   c->d_pass_segs.clear();
@@ -887,9 +1008,12 @@ int pyro_set_option(pyro_ctx* ctx, int option, int value) {
     ctx->j1_metro_site_mode = (value & 1) != 0;
     ctx->j1_or_site_mode = (value & 2) != 0;
   } else if (option == PYRO_OPT_CYCLE_KERNEL) {
-    if (value != 0 && value != 1) return fail(ctx, PYRO_ERR_ARG, "cycle kernel option is 0 or 1");
+    if (value < 0 || value > 2) return fail(ctx, PYRO_ERR_ARG, "cycle kernel option is 0, 1 or 2");
     ctx->cycle_kernel = value;
     ctx->cluster_checked = false;
+  } else if (option == PYRO_OPT_WAVE_STALL) {
+    if (value < -1) return fail(ctx, PYRO_ERR_ARG, "stall item is -1 (off) or an item index");
+    ctx->wave_stall_item = value;
   } else if (option == PYRO_OPT_CLUSTER_SIZE) {
     if (value < 1 || value > 16) return fail(ctx, PYRO_ERR_ARG, "cluster size is 1..16");
     ctx->cluster_size = value;
@@ -919,6 +1043,7 @@ int pyro_get_option(pyro_ctx* ctx, int option, int* value) {
     case PYRO_OPT_PDL: *value = ctx->pdl; break;
     case PYRO_OPT_TET_GROUPED: *value = ctx->tet_grouped; break;
     case PYRO_OPT_FUSED_OBS: *value = ctx->fused_obs; break;
+    case PYRO_OPT_WAVE_STALL: *value = ctx->wave_stall_item; break;
     case PYRO_OPT_J1_SITE_MODE:
       *value = (ctx->j1_metro_site_mode ? 1 : 0) | (ctx->j1_or_site_mode ? 2 : 0);
       break;
@@ -949,7 +1074,11 @@ int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen)
                            {1, 1, 16, 1, 0, 1, 0}, {1, 1, 10, 1, 0, 1, 0}, {1, 0, 16, 1, 6, 2, 0},
                            {1, 0, 16, 1, 4, 3, 0}, {1, 0, 16, 1, 5, 2, 0}, {1, 0, 16, 3, 2, 4, 0},
                            {1, 0, 16, 3, 2, 2, 0}, {1, 0, 16, 3, 1, 4, 0}, {1, 0, 16, 1, 2, 6, 0},
-                           {1, 0, 16, 1, 1, 8, 0}, {1, 0, 16, 1, 1, 6, 0}};
+                           {1, 0, 16, 1, 1, 8, 0}, {1, 0, 16, 1, 1, 6, 0},
+                           // the work-queue cycle kernel: forms, replica groups
+                           {1, 2, 16, 3, 2, 1, 0}, {1, 2, 16, 3, 4, 1, 0}, {1, 2, 16, 3, 8, 1, 0},
+                           {1, 2, 16, 3, 16, 1, 0}, {1, 2, 16, 3, 0, 1, 0}, {1, 2, 16, 1, 4, 1, 0},
+                           {1, 2, 16, 1, 8, 1, 0}, {1, 2, 16, 2, 8, 1, 0}};
     vs.insert(vs.end(), std::begin(j1v), std::end(j1v));
     n_j1 = (int)vs.size();
   }
@@ -993,7 +1122,8 @@ int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen)
     }
     int rc = apply(v);
     if (rc) continue;
-    if (v.cyc && (ctx->cycle_kernel != 1 || ctx->cluster_size != v.cs)) continue;
+    if (v.cyc == 1 && (ctx->cycle_kernel != 1 || ctx->cluster_size != v.cs)) continue;
+    if (v.cyc == 2 && ctx->cycle_kernel != 2) continue;
     if ((rc = pyro_cycle(ctx, n_metro, n_or, swap, 1))) return rc;  // build the graph
     float ms = 1e30f;
     for (int rep = 0; rep < 2; ++rep) {  // best of two timings
@@ -1024,7 +1154,7 @@ int pyro_synchronize(pyro_ctx* ctx) {
   if (!ctx) return PYRO_ERR_ARG;
   PYRO_CK(cudaSetDevice(ctx->device));
   PYRO_CK(cudaStreamSynchronize(ctx->stream));
-  return PYRO_OK;
+  return check_wave_status(ctx);
 }
 
 int pyro_system_info(const pyro_ctx* ctx, int system, int* L, int* n_sites, int* n_replicas,
@@ -1058,8 +1188,13 @@ static int spin_copy(pyro_ctx* ctx, int system, void* dst, const void* src, cuda
   float4* dev = ctx->d_spins + s.spin_off;
   if (to_device) PYRO_CK(cudaMemcpyAsync(dev, src, bytes, kind, ctx->stream));
   else PYRO_CK(cudaMemcpyAsync(dst, dev, bytes, kind, ctx->stream));
-  if (sync) PYRO_CK(cudaStreamSynchronize(ctx->stream));
-  return PYRO_OK;
+  if (!sync) return PYRO_OK;
+  if (!to_device) {
+    const int rc = queue_wave_status(ctx);
+    if (rc) return rc;
+  }
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  return to_device ? PYRO_OK : wave_status_result(ctx);
 }
 
 int pyro_set_spins(pyro_ctx* ctx, int system, const float* host_xyzw) {
@@ -1285,8 +1420,10 @@ int pyro_last_observables(pyro_ctx* ctx, int system, double* energy, double* mag
   if (magnetisation3)
     PYRO_CK(cudaMemcpyAsync(magnetisation3, ctx->d_mag + 3 * s.rep_ctx_base,
                             sizeof(double) * 3 * s.n_rep, cudaMemcpyDeviceToHost, ctx->stream));
+  const int rc = queue_wave_status(ctx);
+  if (rc) return rc;
   PYRO_CK(cudaStreamSynchronize(ctx->stream));
-  return PYRO_OK;
+  return wave_status_result(ctx);
 }
 
 int pyro_observables(pyro_ctx* ctx, int system, double* energy, double* magnetisation3) {
@@ -1303,8 +1440,10 @@ int pyro_observables(pyro_ctx* ctx, int system, double* energy, double* magnetis
   if (magnetisation3)
     PYRO_CK(cudaMemcpyAsync(magnetisation3, ctx->d_mag + 3 * s.rep_ctx_base,
                             sizeof(double) * 3 * s.n_rep, cudaMemcpyDeviceToHost, ctx->stream));
+  rc = queue_wave_status(ctx);
+  if (rc) return rc;
   PYRO_CK(cudaStreamSynchronize(ctx->stream));
-  return PYRO_OK;
+  return wave_status_result(ctx);
 }
 
 int pyro_get_temperatures(pyro_ctx* ctx, int system, double* temperature_of_replica) {
@@ -1513,6 +1652,7 @@ static int run_cycles(pyro_ctx* ctx, int n_metro, int n_or, int n_tet, int do_sw
     cudaGraph_t g;
     int rc = check_cluster(ctx);  // sets kernel attributes: not inside a capture
     if (rc) return rc;
+    if (use_wave_kernel(ctx, n_metro, n_or, n_tet) && (rc = prepare_wave(ctx))) return rc;
     PYRO_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     ctx->defer_finalise = true;  // the exchange kernel below finalises the observables
     if (n_tet == 0) {

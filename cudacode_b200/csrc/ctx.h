@@ -76,8 +76,17 @@ struct pyro_ctx {
   // one site per thread (true) or the 4 sites of a cell per thread.
   bool j1_metro_site_mode = true;
   bool j1_or_site_mode = false;
-  // Cluster-resident cycle kernel for J1 systems (0 = per-pass launches).
+  // Cycle kernel for J1 systems: 0 per-pass launches, 1 cluster-resident,
+  // 2 the work-queue kernel (one launch per system per cycle).
   int cycle_kernel = 0;
+  // Work-queue kernel: per J1 system, a queue ticket (padded to 128 bytes)
+  // and the per-(replica, chunk) progress counters; zeroed before each
+  // launch. wave_status is set by a dependency wait that gave up.
+  unsigned int* d_wave = nullptr;
+  size_t wave_words = 0;
+  int* d_wave_status = nullptr;
+  int* h_wave_status = nullptr;  // pinned copy, read after a synchronising call
+  int wave_stall_item = -1;
   int smem_kernel = 1;
   int rep_group = 0;    // per-pass J1 kernels over groups of this many replicas (0: all)
   int gen_group_mb = 0; // generic kernels over groups of replicas of about this many MB (0: off)

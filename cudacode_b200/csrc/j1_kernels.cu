@@ -63,34 +63,40 @@ __device__ __forceinline__ CellFrame make_frame(int x, int y, int z, int L) {
 }
 
 // Spin loads. Within one launch of a colour pass the neighbours read are
-// never written, so the read-only path (ld.global.nc) is safe. The
+// never written, so the read-only path (ld.global.nc, kLdNc) is safe. The
 // cluster-resident cycle kernel rewrites the lattice between passes of the
-// same launch, so it reads through L2 only (ld.global.cg): an SM's L1 may
-// still hold lines from an earlier pass.
-template <bool kL2Only>
+// same launch, so it reads through L2 only (ld.global.cg, kLdL2): an SM's L1
+// may still hold lines from an earlier pass. The work-queue cycle kernel
+// reads with ordinary coherent loads (ld.global.ca, kLdCoherent) after an
+// acquire of the progress counters that its producers released: the memory
+// model orders those loads after the producers' stores, so the SM's L1 can
+// serve the reuse within a work item without returning stale lines.
+constexpr int kLdNc = 0, kLdL2 = 1, kLdCoherent = 2;
+template <int kLd>
 __device__ __forceinline__ float4 load_spin(const float4* p) {
-  if (kL2Only) return __ldcg(p);
+  if (kLd == kLdL2) return __ldcg(p);
+  if (kLd == kLdCoherent) return __ldca(p);
   return __ldg(p);
 }
 
-template <int S, int K, bool kL2Only = false>
+template <int S, int K, int kLd = kLdNc>
 __device__ __forceinline__ float4 load_neighbour(const float4* __restrict__ rep, const CellFrame& f,
                                                  int L3) {
   constexpr NbrEntry e = j1_neighbour(S, K);
   static_assert(e.t >= 0, "neighbour table");
-  return load_spin<kL2Only>(rep + f.zo[e.dz + 1] + f.yo[e.dy + 1] + f.xo[e.dx + 1] + e.t * L3);
+  return load_spin<kLd>(rep + f.zo[e.dz + 1] + f.yo[e.dy + 1] + f.xo[e.dx + 1] + e.t * L3);
 }
 
 // Sum of the 6 nearest neighbours of site S, in canonical order.
-template <int S, bool kL2Only = false>
+template <int S, int kLd = kLdNc>
 __device__ __forceinline__ pyro_vec3 j1_sum(const float4* __restrict__ rep, const CellFrame& f,
                                             int L3) {
-  const float4 n0 = load_neighbour<S, 0, kL2Only>(rep, f, L3);
-  const float4 n1 = load_neighbour<S, 1, kL2Only>(rep, f, L3);
-  const float4 n2 = load_neighbour<S, 2, kL2Only>(rep, f, L3);
-  const float4 n3 = load_neighbour<S, 3, kL2Only>(rep, f, L3);
-  const float4 n4 = load_neighbour<S, 4, kL2Only>(rep, f, L3);
-  const float4 n5 = load_neighbour<S, 5, kL2Only>(rep, f, L3);
+  const float4 n0 = load_neighbour<S, 0, kLd>(rep, f, L3);
+  const float4 n1 = load_neighbour<S, 1, kLd>(rep, f, L3);
+  const float4 n2 = load_neighbour<S, 2, kLd>(rep, f, L3);
+  const float4 n3 = load_neighbour<S, 3, kLd>(rep, f, L3);
+  const float4 n4 = load_neighbour<S, 4, kLd>(rep, f, L3);
+  const float4 n5 = load_neighbour<S, 5, kLd>(rep, f, L3);
   pyro_vec3 a;
   a.x = ((((n0.x + n1.x) + n2.x) + n3.x) + n4.x) + n5.x;
   a.y = ((((n0.y + n1.y) + n2.y) + n3.y) + n4.y) + n5.y;
@@ -100,37 +106,37 @@ __device__ __forceinline__ pyro_vec3 j1_sum(const float4* __restrict__ rep, cons
 
 // h + A[b][b_K] S_K for neighbour K of site S (b = S & 3): the matrix of
 // the neighbour's sublattice among the three kept for b.
-template <int S, int K, bool kL2Only>
+template <int S, int K, int kLd>
 __device__ __forceinline__ pyro_vec3 exch_add(pyro_vec3 h, const float4* __restrict__ rep,
                                               const CellFrame& f, int L3, const J1PassParams& p) {
   constexpr NbrEntry e = j1_neighbour(S, K);
   constexpr int b = S & 3, t = e.t & 3, slot = t < b ? t : t - 1;
   static_assert(t != b, "nearest neighbours are on other sublattices");
-  const float4 v = load_neighbour<S, K, kL2Only>(rep, f, L3);
+  const float4 v = load_neighbour<S, K, kLd>(rep, f, L3);
   return pyro_matvec_add(h, p.xa[b][slot], v.x, v.y, v.z);
 }
 
 // Own spin and local field of site S of `cell` (loads and field arithmetic).
-template <int S, bool kL2Only = false, bool kExch = false>
+template <int S, int kLd = kLdNc, bool kExch = false>
 __device__ __forceinline__ void site_field(const float4* __restrict__ rep, const CellFrame& f,
                                            int cell, int L3, float J1, const J1PassParams& p,
                                            pyro_vec3* sp, pyro_vec3* h) {
   const int own = S * L3 + cell;
-  const float4 sv = kL2Only ? __ldcg(rep + own) : __ldg(rep + own);
+  const float4 sv = load_spin<kLd>(rep + own);
   if (kExch) {
     pyro_vec3 a;
     a.x = a.y = a.z = 0.0f;
-    a = exch_add<S, 0, kL2Only>(a, rep, f, L3, p);
-    a = exch_add<S, 1, kL2Only>(a, rep, f, L3, p);
-    a = exch_add<S, 2, kL2Only>(a, rep, f, L3, p);
-    a = exch_add<S, 3, kL2Only>(a, rep, f, L3, p);
-    a = exch_add<S, 4, kL2Only>(a, rep, f, L3, p);
-    a = exch_add<S, 5, kL2Only>(a, rep, f, L3, p);
+    a = exch_add<S, 0, kLd>(a, rep, f, L3, p);
+    a = exch_add<S, 1, kLd>(a, rep, f, L3, p);
+    a = exch_add<S, 2, kLd>(a, rep, f, L3, p);
+    a = exch_add<S, 3, kLd>(a, rep, f, L3, p);
+    a = exch_add<S, 4, kLd>(a, rep, f, L3, p);
+    a = exch_add<S, 5, kLd>(a, rep, f, L3, p);
     h->x = a.x - p.xf[S & 3][0];
     h->y = a.y - p.xf[S & 3][1];
     h->z = a.z - p.xf[S & 3][2];
   } else {
-    const pyro_vec3 a = j1_sum<S, kL2Only>(rep, f, L3);
+    const pyro_vec3 a = j1_sum<S, kLd>(rep, f, L3);
     h->x = J1 * a.x;
     h->y = J1 * a.y;
     h->z = J1 * a.z;
@@ -166,13 +172,13 @@ __device__ __forceinline__ int site_update(float4* __restrict__ rep, int cell, i
   return acc;
 }
 
-template <int S, bool kMetro, bool kL2Only = false, bool kExch = false>
+template <int S, bool kMetro, int kLd = kLdNc, bool kExch = false>
 __device__ __forceinline__ int update_site(float4* __restrict__ rep, const CellFrame& f, int cell,
                                            int L3, float J1, float beta, float cosmax, uint32_t rkey,
                                            uint32_t sweep32, bool renorm, uint32_t seed_lo,
                                            uint32_t seed_hi, const J1PassParams& p) {
   pyro_vec3 sp, h;
-  site_field<S, kL2Only, kExch>(rep, f, cell, L3, J1, p, &sp, &h);
+  site_field<S, kLd, kExch>(rep, f, cell, L3, J1, p, &sp, &h);
   return site_update<S, kMetro>(rep, cell, L3, sp, h, beta, cosmax, rkey, sweep32, renorm, seed_lo,
                                 seed_hi);
 }
@@ -187,14 +193,15 @@ __device__ __forceinline__ void pass_prologue() {
 
 // The four sites of colour B in `cell` of replica `rep` (cell form of a
 // pass). Returns the number of accepted Metropolis moves.
-template <int B, bool kMetro, bool kExch>
+template <int B, bool kMetro, bool kExch, int kLd = kLdNc>
 __device__ __forceinline__ int cell_pass(const J1PassParams& p, int rep, int cell, float beta,
-                                         float cosmax) {
+                                         float cosmax, unsigned long long sweep_add = 0) {
   int x, y, z;
   decode_cell(cell, p.L, p.rcpL, &x, &y, &z);
   const CellFrame f = make_frame(x, y, z, p.L);
   float4* rb = p.spins + (long long)rep * 16 * p.L3;
-  const unsigned long long sweep = (p.sweep_ctr ? *p.sweep_ctr : 0ull) + p.sweep_off;
+  const unsigned long long sweep =
+      (p.sweep_ctr ? *p.sweep_ctr : 0ull) + p.sweep_off + sweep_add;
   const bool renorm =
       p.renorm_every > 0 && ((sweep + 1) % (unsigned long long)p.renorm_every) == 0;
   const uint32_t rkey = (uint32_t)(p.rep_key + rep);
@@ -203,10 +210,10 @@ __device__ __forceinline__ int cell_pass(const J1PassParams& p, int rep, int cel
   // other (nor of any site written in this pass), so all their loads are
   // issued before the first store: one memory round trip, not four.
   pyro_vec3 s0, h0, s1, h1, s2, h2, s3, h3;
-  site_field<B, false, kExch>(rb, f, cell, p.L3, p.J1, p, &s0, &h0);
-  site_field<4 + B, false, kExch>(rb, f, cell, p.L3, p.J1, p, &s1, &h1);
-  site_field<8 + B, false, kExch>(rb, f, cell, p.L3, p.J1, p, &s2, &h2);
-  site_field<12 + B, false, kExch>(rb, f, cell, p.L3, p.J1, p, &s3, &h3);
+  site_field<B, kLd, kExch>(rb, f, cell, p.L3, p.J1, p, &s0, &h0);
+  site_field<4 + B, kLd, kExch>(rb, f, cell, p.L3, p.J1, p, &s1, &h1);
+  site_field<8 + B, kLd, kExch>(rb, f, cell, p.L3, p.J1, p, &s2, &h2);
+  site_field<12 + B, kLd, kExch>(rb, f, cell, p.L3, p.J1, p, &s3, &h3);
   int acc = 0;
   acc += site_update<B, kMetro>(rb, cell, p.L3, s0, h0, beta, cosmax, rkey, sw, renorm,
                                 p.seed_lo, p.seed_hi);
@@ -254,6 +261,38 @@ __global__ void __launch_bounds__(kJ1Threads) j1_pass_kernel(const J1PassParams 
   if (kMetro) block_accept(p, t, acc);
 }
 
+// Site 4 f + B of `cell` (site form of a pass). Returns 1 if a Metropolis
+// move was accepted.
+template <int B, bool kMetro, bool kExch, int kLd = kLdNc>
+__device__ __forceinline__ int site_item(const J1PassParams& p, int rep, int f, int cell,
+                                         float beta, float cosmax,
+                                         unsigned long long sweep_add = 0) {
+  int x, y, z;
+  decode_cell(cell, p.L, p.rcpL, &x, &y, &z);
+  const CellFrame fr = make_frame(x, y, z, p.L);
+  float4* rb = p.spins + (long long)rep * 16 * p.L3;
+  const unsigned long long sweep =
+      (p.sweep_ctr ? *p.sweep_ctr : 0ull) + p.sweep_off + sweep_add;
+  const bool renorm =
+      p.renorm_every > 0 && ((sweep + 1) % (unsigned long long)p.renorm_every) == 0;
+  const uint32_t rkey = (uint32_t)(p.rep_key + rep);
+  const uint32_t sw = (uint32_t)sweep;
+  switch (f) {
+    case 0:
+      return update_site<B, kMetro, kLd, kExch>(rb, fr, cell, p.L3, p.J1, beta, cosmax, rkey, sw,
+                                                renorm, p.seed_lo, p.seed_hi, p);
+    case 1:
+      return update_site<4 + B, kMetro, kLd, kExch>(rb, fr, cell, p.L3, p.J1, beta, cosmax, rkey,
+                                                    sw, renorm, p.seed_lo, p.seed_hi, p);
+    case 2:
+      return update_site<8 + B, kMetro, kLd, kExch>(rb, fr, cell, p.L3, p.J1, beta, cosmax, rkey,
+                                                    sw, renorm, p.seed_lo, p.seed_hi, p);
+    default:
+      return update_site<12 + B, kMetro, kLd, kExch>(rb, fr, cell, p.L3, p.J1, beta, cosmax, rkey,
+                                                     sw, renorm, p.seed_lo, p.seed_hi, p);
+  }
+}
+
 // Same pass, one site per thread: blockIdx.y is the FCC corner f (so site
 // S = 4 f + B is uniform in a CTA), blockIdx.z the replica. Fewer live
 // registers than the cell-per-thread form, hence more warps in flight; the
@@ -273,35 +312,7 @@ __global__ void __launch_bounds__(kJ1Threads) j1_site_pass_kernel(const J1PassPa
     cosmax = p.cosmax[p.temp_base + t];
   }
   int acc = 0;
-  if (cell < p.L3) {
-    int x, y, z;
-    decode_cell(cell, p.L, p.rcpL, &x, &y, &z);
-    const CellFrame fr = make_frame(x, y, z, p.L);
-    float4* rb = p.spins + (long long)rep * 16 * p.L3;
-    const unsigned long long sweep = (p.sweep_ctr ? *p.sweep_ctr : 0ull) + p.sweep_off;
-    const bool renorm =
-        p.renorm_every > 0 && ((sweep + 1) % (unsigned long long)p.renorm_every) == 0;
-    const uint32_t rkey = (uint32_t)(p.rep_key + rep);
-    const uint32_t sw = (uint32_t)sweep;
-    switch (f) {
-      case 0:
-        acc = update_site<B, kMetro, false, kExch>(rb, fr, cell, p.L3, p.J1, beta, cosmax, rkey,
-                                                   sw, renorm, p.seed_lo, p.seed_hi, p);
-        break;
-      case 1:
-        acc = update_site<4 + B, kMetro, false, kExch>(rb, fr, cell, p.L3, p.J1, beta, cosmax,
-                                                       rkey, sw, renorm, p.seed_lo, p.seed_hi, p);
-        break;
-      case 2:
-        acc = update_site<8 + B, kMetro, false, kExch>(rb, fr, cell, p.L3, p.J1, beta, cosmax,
-                                                       rkey, sw, renorm, p.seed_lo, p.seed_hi, p);
-        break;
-      default:
-        acc = update_site<12 + B, kMetro, false, kExch>(rb, fr, cell, p.L3, p.J1, beta, cosmax,
-                                                        rkey, sw, renorm, p.seed_lo, p.seed_hi, p);
-        break;
-    }
-  }
+  if (cell < p.L3) acc = site_item<B, kMetro, kExch>(p, rep, f, cell, beta, cosmax);
   if (kMetro) {
     const int n = __syncthreads_count(acc);
     if (threadIdx.x == 0 && n > 0)
@@ -316,15 +327,15 @@ __device__ __forceinline__ double warp_sum_d(double v) {
 }
 
 // Down-tetrahedron partners of the sublattice-0 site 4F of a cell.
-template <int F, bool kL2Only>
+template <int F, int kLd>
 __device__ __forceinline__ void down_partners(const float4* __restrict__ rep, const CellFrame& f,
                                               int L3, float4* d1, float4* d2, float4* d3) {
   constexpr int S0 = 4 * F;
   constexpr int k1 = j1_down_index(S0, 0), k2 = j1_down_index(S0, 1), k3 = j1_down_index(S0, 2);
   static_assert(k1 >= 0 && k2 >= 0 && k3 >= 0, "three down-tetrahedron partners");
-  *d1 = load_neighbour<S0, k1, kL2Only>(rep, f, L3);
-  *d2 = load_neighbour<S0, k2, kL2Only>(rep, f, L3);
-  *d3 = load_neighbour<S0, k3, kL2Only>(rep, f, L3);
+  *d1 = load_neighbour<S0, k1, kLd>(rep, f, L3);
+  *d2 = load_neighbour<S0, k2, kLd>(rep, f, L3);
+  *d3 = load_neighbour<S0, k3, kLd>(rep, f, L3);
 }
 
 // E_tet = J1 * sum_{i<j in tet} S_i.S_j = J1/2 (|sum S|^2 - sum |S|^2), FP64.
@@ -339,16 +350,16 @@ __device__ __forceinline__ double tet_energy(float4 a, float4 b, float4 c, float
   return 0.5 * (mx * mx + my * my + mz * mz - n2);
 }
 
-template <int F, bool kL2Only = false>
+template <int F, int kLd = kLdNc>
 __device__ __forceinline__ void cell_corner(const float4* __restrict__ rep, const CellFrame& f,
                                             int cell, int L3, double* e, double* mx, double* my,
                                             double* mz) {
-  const float4 s0 = load_spin<kL2Only>(rep + (4 * F + 0) * L3 + cell);
-  const float4 s1 = load_spin<kL2Only>(rep + (4 * F + 1) * L3 + cell);
-  const float4 s2 = load_spin<kL2Only>(rep + (4 * F + 2) * L3 + cell);
-  const float4 s3 = load_spin<kL2Only>(rep + (4 * F + 3) * L3 + cell);
+  const float4 s0 = load_spin<kLd>(rep + (4 * F + 0) * L3 + cell);
+  const float4 s1 = load_spin<kLd>(rep + (4 * F + 1) * L3 + cell);
+  const float4 s2 = load_spin<kLd>(rep + (4 * F + 2) * L3 + cell);
+  const float4 s3 = load_spin<kLd>(rep + (4 * F + 3) * L3 + cell);
   float4 d1, d2, d3;
-  down_partners<F, kL2Only>(rep, f, L3, &d1, &d2, &d3);
+  down_partners<F, kLd>(rep, f, L3, &d1, &d2, &d3);
   *e += tet_energy(s0, s1, s2, s3) + tet_energy(s0, d1, d2, d3);
   *mx += (double)s0.x + s1.x + s2.x + s3.x;
   *my += (double)s0.y + s1.y + s2.y + s3.y;
@@ -389,7 +400,7 @@ __device__ __forceinline__ double4 block_observables(double e, double mx, double
 // kJ1Threads cells, reduced over the CTA in a fixed order; thread 0 returns
 // (2 E, Mx, My, Mz) (the finalise step halves the site-sum convention of the
 // generic kernel, hence 2 E). Every thread of the CTA must call it.
-template <bool kL2Only>
+template <int kLd>
 __device__ __forceinline__ double4 chunk_observables(const float4* __restrict__ rb, int cell,
                                                      int L, int L3, float rcpL, double J1,
                                                      double (*red)[kJ1Threads / 32]) {
@@ -398,10 +409,17 @@ __device__ __forceinline__ double4 chunk_observables(const float4* __restrict__ 
     int x, y, z;
     decode_cell(cell, L, rcpL, &x, &y, &z);
     const CellFrame f = make_frame(x, y, z, L);
-    cell_corner<0, kL2Only>(rb, f, cell, L3, &e, &mx, &my, &mz);
-    cell_corner<1, kL2Only>(rb, f, cell, L3, &e, &mx, &my, &mz);
-    cell_corner<2, kL2Only>(rb, f, cell, L3, &e, &mx, &my, &mz);
-    cell_corner<3, kL2Only>(rb, f, cell, L3, &e, &mx, &my, &mz);
+    // In the work-queue kernel (kLd == kLdCoherent) the corners run one
+    // after another (a compiler barrier between them keeps 7 loads in
+    // flight instead of 28), which bounds its register count; the sums are
+    // the same in the same order.
+    cell_corner<0, kLd>(rb, f, cell, L3, &e, &mx, &my, &mz);
+    if (kLd == kLdCoherent) asm volatile("" ::: "memory");
+    cell_corner<1, kLd>(rb, f, cell, L3, &e, &mx, &my, &mz);
+    if (kLd == kLdCoherent) asm volatile("" ::: "memory");
+    cell_corner<2, kLd>(rb, f, cell, L3, &e, &mx, &my, &mz);
+    if (kLd == kLdCoherent) asm volatile("" ::: "memory");
+    cell_corner<3, kLd>(rb, f, cell, L3, &e, &mx, &my, &mz);
     e *= J1;
   }
   return block_observables(e, mx, my, mz, red);
@@ -426,23 +444,52 @@ __global__ void __launch_bounds__(kJ1Threads) j1_observables_kernel(const J1ObsP
 // tetrahedra of a cell cover its 16 sites once (magnetisation). The
 // sublattice-3 spins are this thread's own stores of the pass, read back
 // through L2; the others were not written by the pass.
-template <int F>
+template <int F, int kLd = kLdNc>
 __device__ __forceinline__ void corner3_observables(const float4* __restrict__ rb,
                                                     const CellFrame& f, int cell, int L3,
                                                     double* e, double* mx, double* my,
                                                     double* mz) {
   constexpr int S = 4 * F + 3;
-  const float4 s0 = load_spin<false>(rb + (4 * F + 0) * L3 + cell);
-  const float4 s1 = load_spin<false>(rb + (4 * F + 1) * L3 + cell);
-  const float4 s2 = load_spin<false>(rb + (4 * F + 2) * L3 + cell);
-  const float4 s3 = load_spin<true>(rb + S * L3 + cell);
-  const float4 d1 = load_neighbour<S, j1_down_index(S, 0), false>(rb, f, L3);
-  const float4 d2 = load_neighbour<S, j1_down_index(S, 1), false>(rb, f, L3);
-  const float4 d3 = load_neighbour<S, j1_down_index(S, 2), false>(rb, f, L3);
+  constexpr int kOwn = kLd == kLdNc ? kLdL2 : kLd;  // this thread's own stores
+  const float4 s0 = load_spin<kLd>(rb + (4 * F + 0) * L3 + cell);
+  const float4 s1 = load_spin<kLd>(rb + (4 * F + 1) * L3 + cell);
+  const float4 s2 = load_spin<kLd>(rb + (4 * F + 2) * L3 + cell);
+  const float4 s3 = load_spin<kOwn>(rb + S * L3 + cell);
+  const float4 d1 = load_neighbour<S, j1_down_index(S, 0), kLd>(rb, f, L3);
+  const float4 d2 = load_neighbour<S, j1_down_index(S, 1), kLd>(rb, f, L3);
+  const float4 d3 = load_neighbour<S, j1_down_index(S, 2), kLd>(rb, f, L3);
   *e += tet_energy(s0, s1, s2, s3) + tet_energy(s3, d1, d2, d3);
   *mx += (double)s0.x + s1.x + s2.x + s3.x;
   *my += (double)s0.y + s1.y + s2.y + s3.y;
   *mz += (double)s0.z + s1.z + s2.z + s3.z;
+}
+
+// Body of the fused last pass for one chunk of kJ1Threads cells: the colour-3
+// updates of `cell` (cell form), the chunk's acceptance count, and the
+// observables partial of the state it leaves, written to o.partials[slot].
+// Every thread of the CTA calls it.
+template <bool kMetro, int kLd>
+__device__ __forceinline__ void last_item(const J1PassParams& p, const J1ObsParams& o, int rep,
+                                          int cell, float beta, float cosmax, int t,
+                                          unsigned long long sweep_add,
+                                          double (*red)[kJ1Threads / 32], long long slot) {
+  int acc = 0;
+  double e = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+  if (cell < p.L3) {
+    acc = cell_pass<3, kMetro, false, kLd>(p, rep, cell, beta, cosmax, sweep_add);
+    int x, y, z;
+    decode_cell(cell, p.L, p.rcpL, &x, &y, &z);
+    const CellFrame f = make_frame(x, y, z, p.L);
+    const float4* rb = p.spins + (long long)rep * 16 * p.L3;
+    corner3_observables<0, kLd>(rb, f, cell, p.L3, &e, &mx, &my, &mz);
+    corner3_observables<1, kLd>(rb, f, cell, p.L3, &e, &mx, &my, &mz);
+    corner3_observables<2, kLd>(rb, f, cell, p.L3, &e, &mx, &my, &mz);
+    corner3_observables<3, kLd>(rb, f, cell, p.L3, &e, &mx, &my, &mz);
+    e *= o.J1;
+  }
+  if (kMetro) block_accept(p, t, acc);
+  const double4 r = block_observables(e, mx, my, mz, red);
+  if (threadIdx.x == 0) o.partials[slot] = r;
 }
 
 // The last pass of a cycle (colour 3, cell form, isotropic J1) fused with
@@ -466,23 +513,8 @@ __global__ void __launch_bounds__(kJ1Threads) j1_last_pass_kernel(const J1PassPa
     beta = p.beta[p.temp_base + t];
     cosmax = p.cosmax[p.temp_base + t];
   }
-  int acc = 0;
-  double e = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
-  if (cell < p.L3) {
-    acc = cell_pass<3, kMetro, false>(p, rep, cell, beta, cosmax);
-    int x, y, z;
-    decode_cell(cell, p.L, p.rcpL, &x, &y, &z);
-    const CellFrame f = make_frame(x, y, z, p.L);
-    const float4* rb = p.spins + (long long)rep * 16 * p.L3;
-    corner3_observables<0>(rb, f, cell, p.L3, &e, &mx, &my, &mz);
-    corner3_observables<1>(rb, f, cell, p.L3, &e, &mx, &my, &mz);
-    corner3_observables<2>(rb, f, cell, p.L3, &e, &mx, &my, &mz);
-    corner3_observables<3>(rb, f, cell, p.L3, &e, &mx, &my, &mz);
-    e *= o.J1;
-  }
-  if (kMetro) block_accept(p, t, acc);
-  const double4 r = block_observables(e, mx, my, mz, red);
-  if (threadIdx.x == 0) o.partials[o.partial_begin + (long long)rep * gridDim.x + blockIdx.x] = r;
+  last_item<kMetro, kLdNc>(p, o, rep, cell, beta, cosmax, t, 0ull, red,
+                          o.partial_begin + (long long)rep * gridDim.x + blockIdx.x);
 }
 
 // One site update of the cluster kernel: site S of `cell`, neighbours read
@@ -496,7 +528,7 @@ __device__ __forceinline__ int cluster_site(float4* __restrict__ rb, int cell, i
   int x, y, z;
   decode_cell(cell, L, rcpL, &x, &y, &z);
   const CellFrame f = make_frame(x, y, z, L);
-  return update_site<S, kMetro, true>(rb, f, cell, L3, J1, beta, cosmax, rkey, sw, renorm,
+  return update_site<S, kMetro, kLdL2>(rb, f, cell, L3, J1, beta, cosmax, rkey, sw, renorm,
                                       seed_lo, seed_hi, pp);
 }
 
@@ -642,6 +674,162 @@ __global__ void __launch_bounds__(kJ1CycleThreads, 1)
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Work-queue cycle kernel (see J1WaveParams in j1_kernels.cuh).
+
+__device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Publishes this CTA's completed item: the stores of every thread of the
+// CTA (ordered before this by the barrier that precedes the call) become
+// visible before the count does (a release fence, then the add).
+__device__ __forceinline__ void release_add_gpu(unsigned int* p, unsigned int v) {
+  asm volatile("fence.acq_rel.gpu;\n\tred.relaxed.gpu.global.add.u32 [%0], %1;\n" ::"l"(p), "r"(v)
+               : "memory");
+}
+
+// One work item: colour B of pass k on chunk q of replica rep, sub-item f
+// (FCC corner in the site form, unused in the cell form).
+template <int B, bool kExch, bool kMetroSite, bool kOrSite>
+__device__ __forceinline__ void wave_item(const J1WaveParams& w, int rep, int q, int f,
+                                          bool metro, unsigned long long sweep_add) {
+  const J1PassParams& p = w.pass;
+  const int cell = q * kJ1Threads + threadIdx.x;
+  float beta = 0.0f, cosmax = 0.0f;
+  int t = 0;
+  if (metro) {
+    t = p.temp_of_rep[p.temp_base + p.rep_global + rep];
+    beta = p.beta[p.temp_base + t];
+    cosmax = p.cosmax[p.temp_base + t];
+  }
+  int acc = 0;
+  if (cell < p.L3) {
+    if (metro) {
+      if (kMetroSite)
+        acc = site_item<B, true, kExch, kLdCoherent>(p, rep, f, cell, beta, cosmax, sweep_add);
+      else
+        acc = cell_pass<B, true, kExch, kLdCoherent>(p, rep, cell, beta, cosmax, sweep_add);
+    } else {
+      if (kOrSite)
+        site_item<B, false, kExch, kLdCoherent>(p, rep, f, cell, beta, cosmax, sweep_add);
+      else
+        cell_pass<B, false, kExch, kLdCoherent>(p, rep, cell, beta, cosmax, sweep_add);
+    }
+  }
+  if (metro) block_accept(p, t, acc);
+}
+
+// The observables item of the work-queue kernel, out of line: its FP64
+// sums get their own register allocation instead of raising the kernel's.
+__device__ __noinline__ void wave_observables(const float4* rb, int cell, int L, int L3,
+                                              float rcpL, double J1,
+                                              double (*red)[kJ1Threads / 32], double4* out) {
+  const double4 o = chunk_observables<kLdCoherent>(rb, cell, L, L3, rcpL, J1, red);
+  if (threadIdx.x == 0) *out = o;
+}
+
+// kForms: bit 0 the Metropolis passes in the site form, bit 1 the
+// over-relaxation passes in the site form (else the cell form); the item
+// numbering (J1WaveParams::sub_metro, sub_or) must match. Four resident
+// CTAs per SM with both passes in the site form (64 registers), two with a
+// cell-form pass (which needs more than 80 registers to run without
+// spilling). One item per CTA: the grid has
+// one CTA per item, and CTA c takes the c-th ticket of the queue, not item
+// blockIdx.x, so items are taken in order by CTAs that are already running
+// whatever order the hardware starts them in.
+template <bool kExch, int kForms>
+__global__ void __launch_bounds__(kJ1Threads, kForms == 3 ? 4 : 2)
+    j1_wave_kernel(const J1WaveParams w) {
+  constexpr bool kMetroSite = (kForms & 1) != 0, kOrSite = (kForms & 2) != 0;
+  __shared__ int s_item;
+  __shared__ double red[4][kJ1Threads / 32];
+  if (threadIdx.x == 0) s_item = (int)atomicAdd(w.queue, 1u);
+  __syncthreads();
+  const int item = s_item;
+  if (item >= w.n_items) return;
+  const int nq = w.n_chunks;
+  const int n_passes = 4 * (w.n_metro + w.n_or);  // colour passes; pass n_passes: observables
+  // Items per chunk before pass k (cum) and of pass k (sub): the Metropolis
+  // passes come first, then the over-relaxation passes, then (with_obs) one
+  // observables item per chunk.
+  const int m_items = 4 * w.n_metro * w.sub_metro;
+  const int c_items = m_items + 4 * w.n_or * w.sub_or;
+  // item -> (replica group g, pass k, position j, replica, sub-item f)
+  const int per_group = w.group * nq * (c_items + (w.with_obs ? 1 : 0));
+  const int g = item / per_group;
+  const int local = item - g * per_group;
+  const int r0 = g * w.group;
+  const int cnt = min(w.group, w.pass.n_rep - r0);
+  const int per_unit = cnt * nq;
+  const int u = local / per_unit;
+  int k, cum, sub;
+  if (u < m_items) {
+    sub = w.sub_metro;
+    k = u / sub;
+    cum = k * sub;
+  } else if (u < c_items) {
+    sub = w.sub_or;
+    k = 4 * w.n_metro + (u - m_items) / sub;
+    cum = m_items + (k - 4 * w.n_metro) * sub;
+  } else {
+    sub = 1;
+    k = n_passes;
+    cum = c_items;
+  }
+  const int wi = local - per_unit * cum;
+  const int f = wi % sub;  // FCC corner of a site-form pass
+  const int tt = wi / sub;
+  const int rep = r0 + tt % cnt;
+  const int j = tt / cnt;
+  const int q = (int)(((long long)j + (long long)w.dep * k) % nq);
+  // Wait until pass k - 1 is complete on every chunk holding a neighbour.
+  int failed = 0;
+  if (k > 0) {
+    const int n_dep = 2 * w.dep + 1 >= nq ? nq : 2 * w.dep + 1;
+    const unsigned int need = (unsigned int)cum;
+    const unsigned int* row = w.progress + (long long)rep * nq;
+    for (int d = threadIdx.x; d < n_dep; d += blockDim.x) {
+      int qq = n_dep == nq ? d : q - w.dep + d;
+      qq = qq < 0 ? qq + nq : (qq >= nq ? qq - nq : qq);
+      unsigned int polls = 0;
+      while (ld_acquire_gpu(row + qq) < need) {
+        if (++polls >= w.spin_limit || *(volatile int*)w.status) {
+          failed = 1;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+  }
+  if (__syncthreads_or(failed)) {
+    if (threadIdx.x == 0) atomicExch(w.status, 1);
+    return;
+  }
+  if (k == n_passes) {
+    // the observables pass: partials of the state the last pass left, in
+    // the layout and order of j1_observables_kernel
+    const float4* rb = w.pass.spins + (long long)rep * 16 * w.pass.L3;
+    wave_observables(rb, q * kJ1Threads + threadIdx.x, w.pass.L, w.pass.L3, w.pass.rcpL, w.obs.J1,
+                     red, w.obs.partials + w.obs.partial_begin + (long long)rep * nq + q);
+    return;  // nothing depends on it within the launch
+  }
+  const int sweep_idx = k >> 2;
+  const bool metro = sweep_idx < w.n_metro;
+  const unsigned long long sweep_add = (unsigned long long)sweep_idx;
+  switch (k & 3) {
+    case 0: wave_item<0, kExch, kMetroSite, kOrSite>(w, rep, q, f, metro, sweep_add); break;
+    case 1: wave_item<1, kExch, kMetroSite, kOrSite>(w, rep, q, f, metro, sweep_add); break;
+    case 2: wave_item<2, kExch, kMetroSite, kOrSite>(w, rep, q, f, metro, sweep_add); break;
+    default: wave_item<3, kExch, kMetroSite, kOrSite>(w, rep, q, f, metro, sweep_add); break;
+  }
+  __syncthreads();  // every store of the item is issued
+  if (threadIdx.x == 0 && item != w.stall_item)
+    release_add_gpu(w.progress + (long long)rep * nq + q, 1u);
+}
 }  // namespace
 
 namespace {
@@ -725,6 +913,30 @@ void launch_j1_observables(const J1ObsParams& p, cudaStream_t st) {
   cfg.attrs = attr;
   cfg.numAttrs = p.pdl ? 1 : 0;
   cudaLaunchKernelEx(&cfg, j1_observables_kernel, p);  // errors are read back with cudaGetLastError
+}
+
+int j1_wave_dep(int L) {
+  // A neighbour of a cell lies in the plane before or after it, at most
+  // 2 L^2 - 1 cells away (modulo L^3); one chunk of slack covers the
+  // partial last chunk when the distance wraps around.
+  return (2 * L * L + kJ1Threads - 1) / kJ1Threads + 1;
+}
+
+namespace {
+using WaveKernel = void (*)(const J1WaveParams);
+WaveKernel wave_kernel(bool exch, int forms) {
+  static const WaveKernel k[2][4] = {
+      {j1_wave_kernel<false, 0>, j1_wave_kernel<false, 1>, j1_wave_kernel<false, 2>,
+       j1_wave_kernel<false, 3>},
+      {j1_wave_kernel<true, 0>, j1_wave_kernel<true, 1>, j1_wave_kernel<true, 2>,
+       j1_wave_kernel<true, 3>}};
+  return k[exch ? 1 : 0][forms & 3];
+}
+}  // namespace
+
+cudaError_t launch_j1_wave(const J1WaveParams& p, int forms, cudaStream_t st) {
+  wave_kernel(p.pass.exch != 0, forms)<<<p.n_items, kJ1Threads, 0, st>>>(p);
+  return cudaGetLastError();
 }
 
 cudaError_t j1_cycle_prepare(int cluster_size, int* max_active_clusters) {

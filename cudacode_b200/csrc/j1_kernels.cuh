@@ -62,6 +62,50 @@ struct J1CycleParams {
   int partial_begin;
 };
 
+// A whole cycle of one J1 system as one launch over a work queue (the
+// work-queue cycle kernel). A work item is one colour pass of one
+// kJ1Threads-cell chunk of one replica: one CTA of the per-pass kernel
+// (cell form), or a quarter of it (site form, one FCC corner). Items are
+// numbered replica group by replica group, pass by pass, the chunks of pass
+// k starting at chunk dep * k so that an item's inputs were issued a whole
+// pass earlier. The grid has one CTA per item; each CTA takes the next
+// ticket of an atomic counter as its item. Before it starts, the item of
+// pass k on chunk q waits until pass k - 1 is complete on chunks
+// q - dep .. q + dep (every chunk holding a neighbour of its cells):
+// progress[rep][chunk] counts the items completed on that chunk, released
+// after the item's stores and acquired before the dependants' loads. An item
+// only waits on items with smaller tickets, all of them taken by CTAs that
+// are running, so the launch always makes progress; every wait is bounded
+// all the same (spin_limit polls), after which the kernel sets *status = 1
+// and the waiting CTAs return.
+struct J1WaveParams {
+  J1PassParams pass;  // whole system; sweep_off = offset of the cycle's first sweep
+  J1ObsParams obs;    // observables partials (with_obs), as launch_j1_observables writes them
+  int n_metro, n_or;
+  int group;       // replicas per group
+  int n_chunks;    // chunks of kJ1Threads cells per replica
+  int dep;         // dependency half-width, in chunks
+  // After the 4 (n_metro + n_or) colour passes, an observables pass (one
+  // cell-form item per chunk) writes the FP64 energy and magnetisation
+  // partials of the state the last pass left.
+  int with_obs;
+  // Items per chunk of a Metropolis / over-relaxation pass: 1 (cell form)
+  // or 4 (site form, one per FCC corner), as the kernel variant's forms.
+  int sub_metro, sub_or;
+  unsigned int* progress;  // [n_rep][n_chunks], zero at launch
+  unsigned int* queue;     // next ticket, zero at launch
+  int* status;             // set to 1 when a wait gave up
+  int n_items;             // = grid size
+  unsigned int spin_limit;
+  int stall_item;          // diagnostics: this item never reports completion (-1: none)
+};
+
+// forms: bit 0 Metropolis passes in the site form, bit 1 over-relaxation
+// passes in the site form.
+cudaError_t launch_j1_wave(const J1WaveParams& p, int forms, cudaStream_t st);
+// Dependency half-width in chunks for lattice size L.
+int j1_wave_dep(int L);
+
 // site_per_thread: one site per thread (more warps in flight) instead of the
 // 4 sites of a cell per thread; identical results.
 void launch_j1_pass(const J1PassParams& p, int colour, bool metro, bool site_per_thread,

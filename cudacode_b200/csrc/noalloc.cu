@@ -12,6 +12,7 @@
 // buffers; the function allocates nothing and calls no allocating routine.
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <cstdio>
 #include <mutex>
 
@@ -190,6 +191,15 @@ extern "C" int pyro_observables_noalloc(const float* dev_spins_xyzw, int L, int 
   if (!dev_spins_xyzw || !dev_energy || L < 2 || L > 256 || n_replicas < 1) {
     fprintf(stderr, "pyro_observables_noalloc: need spins and energy pointers, 2 <= L <= 256, "
                     "n_replicas >= 1\n");
+    return PYRO_ERR_ARG;
+  }
+  // The kernels read the spins as float4 and write doubles: a misaligned
+  // caller pointer would fault the GPU, so it is refused here, before any
+  // CUDA call.
+  if (((uintptr_t)dev_spins_xyzw & 15u) || ((uintptr_t)dev_energy & 7u) ||
+      ((uintptr_t)dev_magnetisation3 & 7u)) {
+    fprintf(stderr, "pyro_observables_noalloc: spins must be 16-byte aligned and the energy "
+                    "and magnetisation buffers 8-byte aligned\n");
     return PYRO_ERR_ARG;
   }
   const long long sites = 16ll * L * L * L;

@@ -289,6 +289,7 @@ class Engine:
     OPT_PDL = 10
     OPT_TET_GROUPED = 11
     OPT_FUSED_OBS = 12
+    OPT_WAVE_STALL = 13
 
     def set_option(self, option: int, value: int) -> None:
         self._ck(self.lib.pyro_set_option(self.ctx, option, value))

@@ -78,8 +78,18 @@ int pyro_neighbour_table(int site, int* out120);
 /* PYRO_OPT_CYCLE_KERNEL: 1 sweeps J1-only systems with the
  * cluster-resident kernel (one thread-block cluster per replica runs every
  * colour pass of a call, so the replica stays in L2), 0 (default) with one
- * launch per colour pass. PYRO_OPT_CLUSTER_SIZE: CTAs per cluster (2, 4, 8, 16; the
- * context falls back to the largest size that can be resident). */
+ * launch per colour pass. 2 runs the colour passes of a pyro_cycle (and its
+ * energies) of each J1 system as one launch over a work queue: an item is
+ * one pass of a 256-cell chunk of one replica, items are numbered replica
+ * group (PYRO_OPT_REPLICA_GROUP, 0 = all replicas) by replica group and pass
+ * by pass, and each item waits only until the previous pass is complete on
+ * the chunks that hold its neighbours (per-chunk counters, released and
+ * acquired at GPU scope, every wait bounded; a wait that runs out makes the
+ * next pyro_synchronize return PYRO_ERR_TIMEOUT). PYRO_OPT_J1_SITE_MODE
+ * chooses its pass forms. Calls other than pyro_cycle use the per-pass
+ * kernels. PYRO_OPT_CLUSTER_SIZE: CTAs per cluster (2, 4, 8, 16; the
+ * context falls back to the largest size that can be resident).
+ * Identical results in every mode. */
 #define PYRO_OPT_CYCLE_KERNEL 2
 #define PYRO_OPT_CLUSTER_SIZE 3
 /* PYRO_OPT_J1_SITE_MODE: bit 0 = Metropolis passes, bit 1 = over-relaxation
@@ -125,11 +135,20 @@ int pyro_neighbour_table(int site, int* out120);
  * has just loaded; 0 runs a separate observables kernel after the pass.
  * Same spins; energies equal up to FP64 summation order. */
 #define PYRO_OPT_FUSED_OBS 12
+/* PYRO_OPT_WAVE_STALL (diagnostics of the work-queue cycle kernel): when
+ * >= 0, item `value` of the kernel's launches never reports its completion
+ * and every dependency wait gives up after 4096 polls, so the cycle ends
+ * with its waits run out: the next pyro_synchronize returns
+ * PYRO_ERR_TIMEOUT (and clears the condition) and the spins are left
+ * partly updated. -1 (default) is normal operation. Used to test the
+ * bounded waits without a device fault. */
+#define PYRO_OPT_WAVE_STALL 13
 int pyro_set_option(pyro_ctx* ctx, int option, int value);
 int pyro_get_option(pyro_ctx* ctx, int option, int* value);
 /* Autotuner: times every kernel variant (per-pass generic, per-pass J1,
- * per-pass J1 in its site/cell forms, replica groups of 2..8 on 1, 2 or 4
- * concurrent chains, cluster-resident J1 with cluster sizes 16, 10) on
+ * per-pass J1 in its site/cell forms, replica groups of 1..8 on 1..8
+ * concurrent chains, cluster-resident J1 with cluster sizes 16, 10, the
+ * work-queue cycle kernel in its forms over replica groups of 2..16 or all) on
  * `cycles` cycles of n_metro + n_or sweeps (+ exchange when the context holds
  * the whole ladder) and keeps the fastest; *chosen = its index. The timed
  * cycles are real Monte Carlo steps and advance the chain. */
@@ -390,9 +409,14 @@ int pyro_cycle_tet(pyro_ctx* ctx, int n_metro, int n_or, int n_tet, int do_swap,
  * buffers are sized, or a process that cannot afford the allocations a
  * pyro_ctx makes. It needs no context. The caller passes the spins of
  * n_replicas replicas of one L lattice (the float4 layout above, device
- * memory) and receives, like pyro_observables_device, the FP64 energy per
- * replica in dev_energy[n_replicas] and, if dev_magnetisation3 is not NULL,
- * the magnetisation in dev_magnetisation3[3 * n_replicas].
+ * memory, 16-byte aligned) and receives the FP64 energy per replica in
+ * dev_energy[n_replicas] and, if dev_magnetisation3 is not NULL, the
+ * magnetisation in dev_magnetisation3[3 * n_replicas] (both 8-byte aligned;
+ * a misaligned pointer returns PYRO_ERR_ARG and launches nothing). The
+ * energy is that of the isotropic Heisenberg model with the four couplings
+ * J1, J2, J3 (through a site) and J3b (across a hexagon) only: it has no
+ * field and no bond matrices, so for a context built with either it differs
+ * from pyro_observables_device.
  *
  * Its working space is a fixed array inside the library of
  * PYRO_NOALLOC_MAX_PARTIALS partial sums (32 B each, 2 MiB), present on every
@@ -403,7 +427,9 @@ int pyro_cycle_tet(pyro_ctx* ctx, int n_metro, int n_or, int n_tet, int do_swap,
  * launch nothing. The call runs on the current CUDA device, on `cuda_stream`
  * (NULL = default stream), and returns without waiting. The first call on
  * each device looks up the array's device address; make that first call
- * before any stream capture. All calls share the one array, so calls that
+ * before any stream capture. That address is kept per device ordinal, so
+ * only the device's primary context (the one the CUDA runtime uses) is
+ * supported. All calls share the one array, so calls that
  * overlap on the GPU (other streams, other threads) race with each other:
  * order them on one stream. */
 #define PYRO_NOALLOC_MAX_PARTIALS 65536

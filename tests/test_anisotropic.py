@@ -241,6 +241,8 @@ def test_exchange_arguments_and_state(tmp_path):
     {"J1_SITE_MODE": 3},                    # site per thread, both sweeps
     {"REPLICA_GROUP": 2, "CHAINS": 2},      # L2-resident groups on two graph branches
     {"CYCLE_KERNEL": 1},                    # isotropic-only kernel: falls back to per-pass
+    {"CYCLE_KERNEL": 2, "J1_SITE_MODE": 3, "REPLICA_GROUP": 2},  # work-queue kernel, site form
+    {"CYCLE_KERNEL": 2, "J1_SITE_MODE": 1},                     # work queue, cell-form OR
 ])
 def test_kernel_variants_agree_with_the_oracle(options):
     temps = geometric_ladder(0.1, 1.2, 6)

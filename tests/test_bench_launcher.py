@@ -1,0 +1,43 @@
+"""bench.py's launcher (CPU, no GPU work): `--gpus N` outside torchrun runs N
+ranks through torch.distributed.run and the line reports n_gpus = N; under
+torchrun a WORLD_SIZE that differs from --gpus is refused."""
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BENCH = os.path.join(ROOT, "bench.py")
+
+
+def run(args, env_extra=None):
+    env = dict(os.environ)
+    for k in ("WORLD_SIZE", "RANK", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT"):
+        env.pop(k, None)
+    env.update(env_extra or {})
+    return subprocess.run([sys.executable, BENCH, *args], capture_output=True, text=True,
+                          timeout=240, env=env, cwd=ROOT)
+
+
+def last_json(out):
+    lines = [ln for ln in out.splitlines() if ln.startswith("{")]
+    return json.loads(lines[-1])
+
+
+def test_gpus_two_spawns_two_ranks():
+    r = run(["--gpus", "2", "--dry-run"])
+    assert r.returncode == 0, r.stderr
+    line = last_json(r.stdout)
+    assert line["n_gpus"] == 2 and line["gpus_arg"] == 2
+
+
+def test_single_rank_dry_run():
+    r = run(["--dry-run"])
+    assert r.returncode == 0, r.stderr
+    assert last_json(r.stdout)["n_gpus"] == 1
+
+
+def test_world_size_must_match_gpus():
+    r = run(["--gpus", "2", "--dry-run"], {"WORLD_SIZE": "3", "RANK": "0"})
+    assert r.returncode == 2
+    assert "WORLD_SIZE=3" in r.stderr
