@@ -117,6 +117,7 @@ TetMoveParams move_params(pyro_ctx* ctx, int si, unsigned long long off) {
   p.closure = ctx->tet->closure;
   p.pdl = ctx->pdl;
   p.err = ctx->tet->d_err;
+  p.trace = nullptr;
   return p;
 }
 
@@ -308,6 +309,39 @@ int pyro_tet_set_proposal(pyro_ctx* ctx, int kind) {
   for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
   ctx->graphs.clear();
   ctx->graph_kernels.clear();
+  return PYRO_OK;
+}
+
+int pyro_tet_trace_pass(pyro_ctx* ctx, int system, int corner, int form, float* records) {
+  int rc = need_tet(ctx);
+  if (rc) return rc;
+  if (system < 0 || system >= (int)ctx->sys.size() || !j1_only_system(ctx->sys[system]))
+    return fail(ctx, PYRO_ERR_ARG, "tet_trace_pass: not a J1-only system");
+  if (corner < 0 || corner > 3 || (form != 0 && form != 3) || !records)
+    return fail(ctx, PYRO_ERR_ARG, "tet_trace_pass: corner 0..3, form 0 or 3, records");
+  PYRO_CK(cudaSetDevice(ctx->device));
+  const SysDev& s = ctx->sys[system];
+  const size_t n = (size_t)s.n_rep * s.L3 * kTetTraceFloats;
+  float* d = nullptr;
+  PYRO_CK(cudaMalloc((void**)&d, sizeof(float) * n));
+  TetMoveParams p = move_params(ctx, system, 0);
+  p.trace = d;
+  p.pdl = 0;
+  launch_tet_move(p, corner, form, ctx->stream);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(records, d, sizeof(float) * n, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d);
+  if (e != cudaSuccess)
+    return fail(ctx, PYRO_ERR_CUDA, std::string("tet_trace_pass: ") + cudaGetErrorString(e));
+  int err = 0;
+  PYRO_CK(cudaMemcpy(&err, ctx->tet->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) {
+    cudaMemset(ctx->tet->d_err, 0, sizeof(int));
+    return fail(ctx, PYRO_ERR_TIMEOUT,
+                "tet: a tensor-core MMA of the learned move did not complete in time");
+  }
   return PYRO_OK;
 }
 

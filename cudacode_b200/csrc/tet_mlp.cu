@@ -590,6 +590,27 @@ __device__ __forceinline__ int tet_finish(const TetMoveParams& p, int rep, int c
   const float log_q = (m0.lq + m1.lq) + (m2.lq + m3.lq);
   const float log_r = -beta * dE + log_q;
   const int accepted = log_r >= 0.0f || tet_test_uniform(r0) < __expf(log_r);
+  if (p.trace) {
+    float* t = p.trace + ((long long)rep * p.L3 + cell) * kTetTraceFloats;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      t[3 * k] = s[k].x;
+      t[3 * k + 1] = s[k].y;
+      t[3 * k + 2] = s[k].z;
+      t[12 + 3 * k] = h[k].x;
+      t[12 + 3 * k + 1] = h[k].y;
+      t[12 + 3 * k + 2] = h[k].z;
+      t[40 + 3 * k] = sn[k].x;
+      t[40 + 3 * k + 1] = sn[k].y;
+      t[40 + 3 * k + 2] = sn[k].z;
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i) t[24 + i] = o[i];
+    t[52] = log_r;
+    t[53] = (float)accepted;
+    t[54] = tet_test_uniform(r0);
+    t[55] = beta;
+  }
   if (accepted) {
     float4* wb = p.spins + (long long)rep * 16 * p.L3;
 #pragma unroll

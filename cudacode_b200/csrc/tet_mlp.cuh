@@ -74,7 +74,15 @@ struct TetMoveParams {
   int closure;                 // 1: site 3 from its exact conditional, 0: the network's vMF
   int pdl;                     // programmatic dependent launch of the per-pass kernels
   int* err;                    // set to 1 if a tensor-core wait of the tcgen05 form ran out
+  // Diagnostics (null in the Monte Carlo): one record of kTetTraceFloats per
+  // tetrahedron at trace[(rep * L3 + cell) * kTetTraceFloats] (forms 0 and 3).
+  float* trace;
 };
+
+// Trace record of one learned move: spins before (12), external fields (12),
+// network outputs (16), proposal (12), log of the MH ratio as evaluated,
+// decision (0 / 1), the test uniform, beta.
+constexpr int kTetTraceFloats = 56;
 
 struct TetCollectParams {
   const float4* spins;

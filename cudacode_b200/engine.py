@@ -120,6 +120,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "pyro_tet_set_weights": (i, [P, pf, i]),
         "pyro_tet_get_weights": (i, [P, pf, i]),
         "pyro_tet_sweep": (i, [P, i]),
+        "pyro_tet_trace_pass": (i, [P, i, i, i, pf]),
         "pyro_tet_set_kernel": (i, [P, i]),
         "pyro_tet_set_proposal": (i, [P, i]),
         "pyro_tet_acceptance": (i, [P, i, pu64, pu64]),
@@ -569,6 +570,17 @@ class Engine:
 
     def tet_sweep(self, n: int = 1) -> None:
         self._ck(self.lib.pyro_tet_sweep(self.ctx, n))
+
+    TET_TRACE_FLOATS = 56
+
+    def tet_trace_pass(self, corner: int, form: int = 0, system: int = 0) -> np.ndarray:
+        """One learned pass over corner `corner` with per-tetrahedron records
+        [n_rep][L^3][56] (see pyro_tet_trace_pass)."""
+        s = self.systems[system]
+        out = np.empty((s.replicas(), s.L ** 3, self.TET_TRACE_FLOATS), dtype=np.float32)
+        self._ck(self.lib.pyro_tet_trace_pass(self.ctx, system, corner, form,
+                                              _ptr(out, C.c_float)))
+        return out
 
     def tet_acceptance(self, system: int = 0):
         n = len(self.systems[system].temperatures)

@@ -396,6 +396,17 @@ int pyro_tet_forward_device(pyro_ctx* ctx, const float* dev_features, int n, flo
 int pyro_tet_set_forward(pyro_ctx* ctx, int tensor_memory);
 int pyro_tet_gradient(pyro_ctx* ctx, const float* features, const float* targets, int n,
                       float* grad, double* loss_sum);
+/* Diagnostics of the learned move: one pass over the up-tetrahedra of FCC
+ * corner `corner` of every replica of J1-only system `system`, with the
+ * single-lane form (form 0, network on mma.sync) or the tcgen05 form
+ * (form 3), at the learned-move counter's current value (the counter is not
+ * advanced). The pass updates the spins like any other and writes, per
+ * tetrahedron (record index rep * L^3 + cell), 56 floats to `records`: the
+ * four spins before the move (12), their external fields (12), the network
+ * outputs (16), the proposal (12), the log of the Metropolis-Hastings ratio
+ * as evaluated, the decision (0 or 1), the test uniform and beta. A test
+ * compares them with an FP64 restatement of the move. Synchronous. */
+int pyro_tet_trace_pass(pyro_ctx* ctx, int system, int corner, int form, float* records);
 /* Cycles with learned moves: n_metro Metropolis + n_or over-relaxation
  * sweeps, n_tet tetrahedron sweeps, energies and (if do_swap) an exchange,
  * replayed from a CUDA graph. */

@@ -57,6 +57,7 @@ def load() -> C.CDLL:
         "orc_mlp_forward": (None, [pf, pf, i, pd]),
         "orc_mlp_gradient": (None, [pf, pf, pf, i, pd, pd]),
         "orc_tet_features": (None, [P, i, i, i, pf, pf]),
+        "orc_tet_move_check": (None, [pf, i, pi, pi, i, i, C.c_uint64, C.c_uint64, d, i, pd]),
         "orc_neighbours": (None, [i, pi]),
         "orc_philox": (None, [pu32, pu32, pu32]),
         "orc_expf": (f, [f]),
@@ -276,3 +277,17 @@ def mlp_gradient(weights, feats, targets):
     load().orc_mlp_gradient(_p(w, C.c_float), _p(x, C.c_float), _p(t, C.c_float), x.shape[0],
                             _p(g, C.c_double), C.byref(loss))
     return g, loss.value
+
+
+def tet_move_check(records, rep_key, cell, corner, L3, seed, sweep, J1, closure):
+    """FP64 restatement of the learned move for trace records (n, 56): per
+    record log r, test uniform, decision, log q ratio, dE and the FP64 vMF
+    draws (12) from the move's Philox words; array (n, 17)."""
+    rec = np.ascontiguousarray(records, dtype=np.float32).reshape(-1, 56)
+    n = rec.shape[0]
+    rk = np.ascontiguousarray(rep_key, dtype=np.int32).reshape(n)
+    ce = np.ascontiguousarray(cell, dtype=np.int32).reshape(n)
+    out = np.empty((n, 17))
+    load().orc_tet_move_check(_p(rec, C.c_float), n, _p(rk, C.c_int), _p(ce, C.c_int), corner, L3,
+                              seed, sweep, J1, int(closure), _p(out, C.c_double))
+    return out

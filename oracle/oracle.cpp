@@ -1016,4 +1016,163 @@ void orc_tet_features(void* p, int si, int r, int f, float* feats, float* spins)
   }
 }
 
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// FP64 restatement of one learned tetrahedron move (the engine's tet_finish
+// in cudacode_b200/csrc/tet_mlp.cu), checked against the engine's trace
+// records (pyro_tet_trace_pass). From the record's spins s, fields h,
+// network outputs o and proposal s', and the move's Philox words (recomputed
+// here from seed, tetrahedron, replica key and counter):
+//   * the vMF draws of sites 0-2 (mu = o_xyz / |o_xyz|, kappa = e^clamp(o_w))
+//     and of site 3 (the network's fourth vMF, or its exact conditional
+//     given the recorded s'_0..s'_2: natural parameter
+//     -beta (J1 (s'_0 + s'_1 + s'_2) + h_3)) by Wood's (1994) inverse CDF,
+//     w = 1 + log(u + (1 - u) e^{-2 kappa}) / kappa, azimuth 2 pi v, in the
+//     orthonormal frame of Duff et al. (2017);
+//   * log q(S | S') - log q(S' | S): the network sites' kappa mu.(s - s'),
+//     plus for the conditional site the difference of the two vMF log
+//     densities with their normalisations log(2 sinh k / k);
+//   * dE = E(S') - E(S) with E = J1 sum_{i<j} s_i.s_j + sum_k h_k.s_k;
+//   * log r = -beta dE + log q ratio and the decision u < min(1, e^log r).
+// The uniforms are formed from the Philox bits exactly as the engine forms
+// them (23-bit mantissa fill); everything else is FP64 with libm.
+namespace {
+
+double tet_u(uint32_t r) {
+  const uint32_t b = 0x3f800000u | (r >> 9);
+  float f;
+  memcpy(&f, &b, 4);
+  return 2.0 - (double)f;
+}
+
+double tet_test_u(const uint32_t r[4]) {
+  const uint32_t m = ((r[0] & 0x1ffu) << 14) | ((r[1] & 0x1ffu) << 5) | (r[2] & 0x1fu);
+  const uint32_t b = 0x3f800000u | m;
+  float f;
+  memcpy(&f, &b, 4);
+  return 2.0 - (double)f;
+}
+
+struct V3 {
+  double x, y, z;
+};
+double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+V3 vmf_draw64(V3 mu, double kappa, double u, double v) {
+  double w = 1.0 + std::log(u + (1.0 - u) * std::exp(-2.0 * kappa)) / kappa;
+  w = std::min(1.0, std::max(-1.0, w));
+  const double st = std::sqrt(std::max(0.0, 1.0 - w * w));
+  const double cp = std::cos(2.0 * M_PI * v), sp = std::sin(2.0 * M_PI * v);
+  const double sgn = std::copysign(1.0, mu.z);
+  const double a = -1.0 / (sgn + mu.z);
+  const double b = mu.x * mu.y * a;
+  const V3 e1 = {1.0 + sgn * mu.x * mu.x * a, sgn * b, -sgn * mu.x};
+  const V3 e2 = {b, sgn + mu.y * mu.y * a, -mu.y};
+  return {w * mu.x + st * (cp * e1.x + sp * e2.x), w * mu.y + st * (cp * e1.y + sp * e2.y),
+          w * mu.z + st * (cp * e1.z + sp * e2.z)};
+}
+
+// log(2 sinh k / k): the vMF normaliser up to the constant log(2 pi).
+double vmf_lognorm64(double k) { return k - std::log(k) + std::log1p(-std::exp(-2.0 * k)); }
+
+void net_vmf(const float* o, V3* mu, double* kappa) {
+  const double x = o[0], y = o[1], z = o[2];
+  const double n2 = x * x + y * y + z * z;
+  if (n2 > 1e-30) {
+    const double n = std::sqrt(n2);
+    *mu = {x / n, y / n, z / n};
+  } else {
+    *mu = {0.0, 0.0, 1.0};
+  }
+  *kappa = std::exp(std::min(std::max((double)o[3], -4.0), 6.0));
+}
+
+// Site 3's conditional given sites 0-2 (a0..a2) and its field h3.
+void closure64(V3 a0, V3 a1, V3 a2, V3 h3, double beta, double J1, V3* mu, double* kappa) {
+  const V3 f = {-beta * (J1 * (a0.x + a1.x + a2.x) + h3.x), -beta * (J1 * (a0.y + a1.y + a2.y) + h3.y),
+                -beta * (J1 * (a0.z + a1.z + a2.z) + h3.z)};
+  const double n2 = dot(f, f);
+  double k = 0.0;
+  if (n2 > 1e-30) {
+    k = std::sqrt(n2);
+    *mu = {f.x / k, f.y / k, f.z / k};
+  } else {
+    *mu = {0.0, 0.0, 1.0};
+  }
+  *kappa = std::max(k, (double)0.018315639f);  // the engine's floor, e^-4 in FP32
+}
+
+double tet_e64(const V3 s[4], const V3 h[4], double J1) {
+  double b = 0.0;
+  for (int i = 0; i < 4; ++i)
+    for (int j = i + 1; j < 4; ++j) b += dot(s[i], s[j]);
+  double e = J1 * b;
+  for (int k = 0; k < 4; ++k) e += dot(s[k], h[k]);
+  return e;
+}
+
+}  // namespace
+
+extern "C" {
+
+// rec: n trace records of 56 floats; rep_key[i], cell[i]: the replica's
+// Philox key and the cell of record i. out: n x 17 doubles per record:
+// log r, test uniform, decision, log q ratio, dE, the FP64 draws (12).
+void orc_tet_move_check(const float* rec, int n, const int* rep_key, const int* cell, int corner,
+                        int L3, uint64_t seed, uint64_t sweep, double J1, int closure,
+                        double* out) {
+  const uint32_t seed_lo = (uint32_t)(seed & 0xffffffffu), seed_hi = (uint32_t)(seed >> 32);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) {
+    const float* t = rec + (size_t)i * 56;
+    V3 s[4], h[4], sn[4];
+    for (int k = 0; k < 4; ++k) {
+      s[k] = {t[3 * k], t[3 * k + 1], t[3 * k + 2]};
+      h[k] = {t[12 + 3 * k], t[12 + 3 * k + 1], t[12 + 3 * k + 2]};
+      sn[k] = {t[40 + 3 * k], t[40 + 3 * k + 1], t[40 + 3 * k + 2]};
+    }
+    const double beta = t[55];
+    const uint32_t key_tet = (uint32_t)(corner * L3 + cell[i]);
+    uint32_t r0[4], r1[4];
+    pyro_philox(key_tet, (uint32_t)rep_key[i], (uint32_t)sweep, PYRO_PURPOSE_TET + 0, seed_lo,
+                seed_hi, r0);
+    pyro_philox(key_tet, (uint32_t)rep_key[i], (uint32_t)sweep, PYRO_PURPOSE_TET + 1, seed_lo,
+                seed_hi, r1);
+    const uint32_t ru[4] = {r0[0], r0[2], r1[0], r1[2]}, rv[4] = {r0[1], r0[3], r1[1], r1[3]};
+    double* o = out + (size_t)i * 17;
+    double log_q = 0.0;
+    for (int k = 0; k < 3 + (closure ? 0 : 1); ++k) {
+      V3 mu;
+      double kap;
+      net_vmf(t + 24 + 4 * k, &mu, &kap);
+      const V3 d = vmf_draw64(mu, kap, tet_u(ru[k]), tet_u(rv[k]));
+      o[5 + 3 * k] = d.x;
+      o[5 + 3 * k + 1] = d.y;
+      o[5 + 3 * k + 2] = d.z;
+      log_q += kap * (dot(mu, s[k]) - dot(mu, sn[k]));
+    }
+    if (closure) {
+      V3 mo, mn;
+      double ko, kn;
+      closure64(s[0], s[1], s[2], h[3], beta, J1, &mo, &ko);
+      closure64(sn[0], sn[1], sn[2], h[3], beta, J1, &mn, &kn);
+      const V3 d = vmf_draw64(mn, kn, tet_u(ru[3]), tet_u(rv[3]));
+      o[14] = d.x;
+      o[15] = d.y;
+      o[16] = d.z;
+      log_q += (ko * dot(mo, s[3]) - vmf_lognorm64(ko)) - (kn * dot(mn, sn[3]) - vmf_lognorm64(kn));
+    }
+    const double dE = tet_e64(sn, h, J1) - tet_e64(s, h, J1);
+    const double log_r = -beta * dE + log_q;
+    const double u = tet_test_u(r0);
+    o[0] = log_r;
+    o[1] = u;
+    o[2] = (log_r >= 0.0 || u < std::exp(log_r)) ? 1.0 : 0.0;
+    o[3] = log_q;
+    o[4] = dE;
+  }
+}
+
 }  // extern "C"

@@ -27,17 +27,27 @@ and its one CPU routine:
   ``CudaCalculateAbsSz`` (Math.cu:478-510) and the per-cell masks of
   ``CudaCalculateIsingConf`` (Math.cu:513-541).
 
-Run from the repository root, in a checkout that has the reference at
-/root/reference:  python tests/golden/make_golden.py
+Run from the repository root with the path of the reference's Pyrochlore.cu
+(or set PYRO_REFERENCE_SOURCE):
+
+    python tests/golden/make_golden.py <path>/Pyrochlore.cu
 """
 import json
 import os
 import re
+import sys
 
 import numpy as np
 
-REF = "/root/reference/Pyrochlore.cu"
 OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def reference_source() -> str:
+    path = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PYRO_REFERENCE_SOURCE")
+    if not path:
+        sys.exit("usage: make_golden.py <path to the reference's Pyrochlore.cu> "
+                 "(or set PYRO_REFERENCE_SOURCE)")
+    return path
 
 
 def parse_links16(text):
@@ -183,7 +193,7 @@ def total_energy(Sx, Sy, Sz, n, links, C, field=None):
 
 
 def main():
-    text = open(REF).read()
+    text = open(reference_source()).read()
     links = parse_links16(text)
     couplings = parse_couplings(text)
     with open(os.path.join(OUT, "links16.json"), "w") as f:

@@ -350,7 +350,11 @@ def test_autotune_keeps_results_exact():
 
 
 @pytest.mark.parametrize("L,G,stride,replica", [(4, 8, 1, -1), (4, 16, 1, 0), (6, 6, 4, 1),
-                                               (3, 12, 1, -1)])
+                                               (3, 12, 1, -1),
+                                               (8, 4, 1, -1),    # fold period 8 >= G: no residues
+                                               (5, 10, 3, -1),   # stride coprime with L, residues
+                                               (8, 6, 2, 0),     # fold period 4 < G
+                                               (12, 8, 3, 2)])   # fold period 4, one replica
 def test_structure_factor_matches_direct_sum(L, G, stride, replica):
     s = System(L=L, temperatures=[0.2, 0.6, 1.4], J2=0.05 if L == 3 else 0.0)
     e, o = pair([s])

@@ -257,3 +257,72 @@ def test_learned_sweeps_in_replica_groups_match_ungrouped(form, group, chains):
     for k in range(len(systems)):
         for a, b in zip(runs[0][k], runs[1][k]):
             assert np.array_equal(a, b), k
+
+
+OFF_B3 = 6288 - 16  # output biases: per site (mu_x, mu_y, mu_z, log kappa)
+
+
+@pytest.mark.parametrize("closure,form,T,corner", [(1, 0, 0.05, 0), (0, 0, 0.5, 2),
+                                                    (1, 3, 0.2, 3), (1, 0, 1.0, 1)])
+def test_learned_move_matches_the_fp64_restatement(closure, form, T, corner):
+    """One traced pass of the learned move, tetrahedron by tetrahedron,
+    against the oracle's FP64 restatement (orc_tet_move_check): the spins and
+    external fields it read, its network outputs (BF16 network, to 3% of
+    their scale), its vMF draws (the FP64 inverse-CDF draws from the same
+    Philox words, to 2e-4), its log Metropolis-Hastings ratio (the FP64
+    ratio with both proposal densities and their normalisations, to the
+    FP32 rounding of its terms), its test uniform (exact), its decision
+    (equal wherever log u is not within the rounding band of log r), its
+    beta (the replica's temperature), and the spins it left."""
+    L, R, seed = 6, 3, 91
+    temps = geometric_ladder(T, 4 * T, R)
+    s = System(L=L, temperatures=temps)
+    e = Engine([s], seed=seed)
+    e.init_random()
+    e.cycle(1, 2, True, 2)
+    e.tet_init(seed=4)
+    w = e.tet_weights()
+    w[OFF_B3 + np.array([3, 7, 11, 15])] = [5.5, 1.0, -3.5, 2.0]  # kappas from ~e^-3.5 to ~e^5.5
+    e.tet_set_weights(w)
+    e.tet_set_proposal(closure)
+    e.tet_sweep(2)  # the traced pass uses counter value 2
+    before = e.get_spins()
+    rec = e.tet_trace_pass(corner, form)
+    after = e.get_spins()
+    L3 = L ** 3
+    t_of_rep = e.temperatures_of_replicas()
+    np.testing.assert_array_equal(rec[:, 0, 55], (1.0 / t_of_rep).astype(np.float32))
+    o = Oracle([s], seed=seed)
+    o.set_spins(before)
+    rec2 = rec.reshape(R * L3, 56)
+    for r in range(R):
+        feats, spins = o.tet_features(r, corner)
+        np.testing.assert_array_equal(rec[r, :, 0:12], spins)
+        np.testing.assert_allclose(rec[r, :, 12:24], 3.0 * feats[:, :12], atol=2e-6)
+        feats[:, 12] = np.log(rec[r, 0, 55]) / 3.0  # beta of the replica (the oracle's is unswapped)
+        net = orc.mlp_forward(w, feats)
+        assert np.abs(rec[r, :, 24:40] - net).max() <= 3e-2 * np.abs(net).max()
+    rep = np.repeat(np.arange(R), L3)
+    cell = np.tile(np.arange(L3), R)
+    chk = orc.tet_move_check(rec2, rep, cell, corner, L3, seed, 2, 1.0, closure)
+    assert np.abs(rec2[:, 40:52] - chk[:, 5:17]).max() <= 2e-4
+    assert np.abs(np.linalg.norm(rec2[:, 40:52].reshape(-1, 4, 3), axis=-1) - 1).max() < 1e-5
+    np.testing.assert_array_equal(rec2[:, 54].astype(np.float64), chk[:, 1])
+    # tolerance: FP32 rounding of the ratio's terms
+    beta = rec2[:, 55].astype(np.float64)
+    kap = np.exp(np.clip(rec2[:, 24:40].reshape(-1, 4, 4)[:, :, 3], -4, 6)).sum(axis=1)
+    hmag = np.linalg.norm(rec2[:, 12:24].reshape(-1, 4, 3), axis=-1).sum(axis=1)
+    scale = 2 * beta * (6 + hmag) + 2 * kap + (4 * beta * (3 + hmag) if closure else 0)
+    tol = 4e-6 * scale + 1e-5
+    dev = np.abs(rec2[:, 52] - chk[:, 0])
+    assert np.all(dev <= tol), (dev.max(), np.argmax(dev - tol))
+    u = rec2[:, 54].astype(np.float64)
+    clear = np.abs(np.log(u) - chk[:, 0]) > tol
+    assert clear.mean() > 0.99
+    np.testing.assert_array_equal(rec2[clear, 53], chk[clear, 2])
+    acc = rec2[:, 53] > 0.5
+    assert 0 < acc.sum() < len(acc)  # both outcomes occur
+    a = after[:, 4 * corner:4 * corner + 4, :, :3].transpose(0, 2, 1, 3).reshape(R * L3, 12)
+    b = before[:, 4 * corner:4 * corner + 4, :, :3].transpose(0, 2, 1, 3).reshape(R * L3, 12)
+    np.testing.assert_array_equal(a[acc], rec2[acc, 40:52])
+    np.testing.assert_array_equal(a[~acc], b[~acc])
