@@ -546,7 +546,7 @@ void free_all(pyro_ctx* c) {
                   c->d_energy,      c->d_mag,          c->d_rep_sys,     c->d_rep_local,
                   c->d_obs_segs,    c->d_partials,     c->d_sweep,       c->d_scratch_u64,
                   c->d_history,     c->d_history_count, c->d_obs_generic,
-                  c->d_sq_s1,       c->d_sq_s2,        c->d_sq_s3,       c->d_sq_tw,
+                  c->d_sq_s1,       c->d_sq_s2,        c->d_sq_tw,
                   c->d_sq_out,      c->d_exch,         c->d_submag,      c->d_order,
                   c->d_wave,        c->d_wave_status};
   for (void* p : ptrs)
@@ -1774,34 +1774,65 @@ int pyro_structure_factor(pyro_ctx* ctx, int system, int replica, int G, int str
   if (replica < -1 || replica >= sd.n_rep)
     return fail(ctx, PYRO_ERR_ARG, "structure_factor: replica out of range");
   PYRO_CK(cudaSetDevice(ctx->device));
-  const int L = sd.L;
-  const size_t G3 = (size_t)G * G * G;
-  int rc = grow(ctx, &ctx->d_sq_s1, &ctx->sq_s1, (size_t)48 * L * L * G);
-  if (!rc) rc = grow(ctx, &ctx->d_sq_s2, &ctx->sq_s2, (size_t)48 * L * G * G);
-  if (!rc) rc = grow(ctx, &ctx->d_sq_s3, &ctx->sq_s3, (size_t)48 * G3);
-  if (!rc) rc = grow(ctx, &ctx->d_sq_tw, &ctx->sq_tw, (size_t)4 * L);
-  if (!rc) rc = grow(ctx, (double2**)&ctx->d_sq_out, &ctx->sq_out, (G3 + 1) / 2);
-  if (rc) return rc;
-  std::vector<double2> tw(4 * L);
-  for (int j = 0; j < 4 * L; ++j) {
-    const double ang = -2.0 * M_PI * (double)j / (4.0 * L);
-    tw[j] = make_double2(std::cos(ang), std::sin(ang));
+  if (!ctx->sq_ready) {
+    PYRO_CK(sq_prepare());
+    ctx->sq_ready = true;
   }
-  PYRO_CK(cudaMemcpyAsync(ctx->d_sq_tw, tw.data(), sizeof(double2) * tw.size(),
-                          cudaMemcpyHostToDevice, ctx->stream));
-  PYRO_CK(cudaMemsetAsync(ctx->d_sq_out, 0, sizeof(double) * G3, ctx->stream));
+  const int L = sd.L;
+  int g = L, b = stride;  // gcd(L, stride)
+  while (b) {
+    const int t = g % b;
+    g = b;
+    b = t;
+  }
   SqParams p;
   p.L = L;
   p.G = G;
   p.stride = stride;
-  p.tw = ctx->d_sq_tw;
+  p.Lf = L / g;
+  p.R = std::min(G, p.Lf);
+  p.residues = G > p.Lf ? 1 : 0;
   for (int s = 0; s < 16; ++s) site_pos4(s, &p.pos4[3 * s]);
   const int r0 = replica < 0 ? 0 : replica, r1 = replica < 0 ? sd.n_rep : replica + 1;
   p.inv_n_norm = 1.0 / ((double)16 * sd.L3 * (double)(r1 - r0));
-  for (int r = r0; r < r1; ++r) {
-    launch_structure_factor_replica(ctx->d_spins + sd.spin_off + (long long)r * 16 * sd.L3, p,
-                                    ctx->d_sq_s1, ctx->d_sq_s2, ctx->d_sq_s3, ctx->d_sq_out,
-                                    ctx->stream);
+  // replicas per launch sequence: at most 1 GiB of scratch (at least one replica)
+  const size_t per_rep = sq_scratch_per_replica(p);
+  const int batch = (int)std::max<size_t>(1, std::min<size_t>(r1 - r0, (1ull << 30) / per_rep));
+  const size_t G3 = (size_t)G * G * G;
+  // d_sq_s1: scratch; d_sq_tw: 4L basis-phase roots, then the Lf DFT roots;
+  // d_sq_s2: the R steps (ints)
+  int rc = grow(ctx, &ctx->d_sq_s1, &ctx->sq_s1, (per_rep * batch + 15) / 16);
+  if (!rc) rc = grow(ctx, &ctx->d_sq_tw, &ctx->sq_tw, (size_t)4 * L + p.Lf);
+  if (!rc) rc = grow(ctx, &ctx->d_sq_s2, &ctx->sq_s2, (size_t)(p.R + 3) / 4);
+  if (!rc) rc = grow(ctx, (double2**)&ctx->d_sq_out, &ctx->sq_out, (G3 + 1) / 2);
+  if (rc) return rc;
+  std::vector<double2> tw(4 * L + p.Lf);
+  for (int j = 0; j < 4 * L; ++j) {
+    const double ang = -2.0 * M_PI * (double)j / (4.0 * L);
+    tw[j] = make_double2(std::cos(ang), std::sin(ang));
+  }
+  for (int j = 0; j < p.Lf; ++j) {
+    const double ang = -2.0 * M_PI * (double)j / (double)p.Lf;
+    tw[4 * L + j] = make_double2(std::cos(ang), std::sin(ang));
+  }
+  std::vector<int> steps(p.R);
+  const long long sred = stride / g;
+  for (int k = 0; k < p.R; ++k) {
+    const long long w = p.residues ? k : k - G / 2;
+    const long long v = (sred * w) % p.Lf;
+    steps[k] = (int)(v < 0 ? v + p.Lf : v);
+  }
+  PYRO_CK(cudaMemcpyAsync(ctx->d_sq_tw, tw.data(), sizeof(double2) * tw.size(),
+                          cudaMemcpyHostToDevice, ctx->stream));
+  PYRO_CK(cudaMemcpyAsync(ctx->d_sq_s2, steps.data(), sizeof(int) * steps.size(),
+                          cudaMemcpyHostToDevice, ctx->stream));
+  PYRO_CK(cudaMemsetAsync(ctx->d_sq_out, 0, sizeof(double) * G3, ctx->stream));
+  p.tw4 = ctx->d_sq_tw;
+  for (int r = r0; r < r1; r += batch) {
+    const int n = std::min(batch, r1 - r);
+    launch_structure_factor(ctx->d_spins + sd.spin_off + (long long)r * 16 * sd.L3, n, p,
+                            ctx->d_sq_tw + 4 * L, (const int*)ctx->d_sq_s2, ctx->d_sq_s1,
+                            ctx->d_sq_out, ctx->stream);
     PYRO_CK_LAUNCH();
   }
   PYRO_CK(cudaMemcpyAsync(out, ctx->d_sq_out, sizeof(double) * G3, cudaMemcpyDeviceToHost,

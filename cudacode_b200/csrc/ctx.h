@@ -130,10 +130,10 @@ struct pyro_ctx {
   // Structure-factor scratch, grown on demand.
   double2* d_sq_s1 = nullptr;
   double2* d_sq_s2 = nullptr;
-  double2* d_sq_s3 = nullptr;
   double2* d_sq_tw = nullptr;
   double* d_sq_out = nullptr;
-  size_t sq_s1 = 0, sq_s2 = 0, sq_s3 = 0, sq_tw = 0, sq_out = 0;
+  size_t sq_s1 = 0, sq_s2 = 0, sq_tw = 0, sq_out = 0;
+  bool sq_ready = false;  // DFT kernels' shared-memory limit raised
 
   pyro::TetState* tet = nullptr;
 
