@@ -548,9 +548,18 @@ void free_all(pyro_ctx* c) {
                   c->d_history,     c->d_history_count, c->d_obs_generic,
                   c->d_sq_s1,       c->d_sq_s2,        c->d_sq_tw,
                   c->d_sq_out,      c->d_exch,         c->d_submag,      c->d_order,
-                  c->d_wave,        c->d_wave_status};
+                  c->d_wave,        c->d_wave_status,  c->d_snap,        c->d_snap_temp_of_rep,
+                  c->d_snap_rep_of_temp, c->d_snap_energy, c->d_snap_mag};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  if (c->snap_stream) cudaStreamDestroy(c->snap_stream);
+  if (c->snap_start) cudaEventDestroy(c->snap_start);
+  if (c->snap_done) cudaEventDestroy(c->snap_done);
+  c->snap_stream = nullptr;
+  c->snap_start = c->snap_done = nullptr;
+  c->d_snap = nullptr;
+  c->snap_taken = false;
+  c->measure_snapshot = 0;
   if (c->h_wave_status) cudaFreeHost(c->h_wave_status);
   c->h_wave_status = nullptr;
   c->d_wave = nullptr;
@@ -974,6 +983,12 @@ int pyro_set_stream(pyro_ctx* ctx, void* cuda_stream) {
 
 int pyro_set_option(pyro_ctx* ctx, int option, int value) {
   if (!ctx) return PYRO_ERR_ARG;
+  if (option == PYRO_OPT_MEASURE_SNAPSHOT) {  // no kernel schedule depends on it
+    if (value != 0 && value != 1) return fail(ctx, PYRO_ERR_ARG, "measure snapshot option is 0 or 1");
+    if (value && !ctx->snap_taken) return fail(ctx, PYRO_ERR_STATE, "no snapshot taken yet");
+    ctx->measure_snapshot = value;
+    return PYRO_OK;
+  }
   PYRO_CK(cudaSetDevice(ctx->device));
   PYRO_CK(cudaStreamSynchronize(ctx->stream));
   if (option == PYRO_OPT_J1_KERNEL) {
@@ -1044,6 +1059,7 @@ int pyro_get_option(pyro_ctx* ctx, int option, int* value) {
     case PYRO_OPT_TET_GROUPED: *value = ctx->tet_grouped; break;
     case PYRO_OPT_FUSED_OBS: *value = ctx->fused_obs; break;
     case PYRO_OPT_WAVE_STALL: *value = ctx->wave_stall_item; break;
+    case PYRO_OPT_MEASURE_SNAPSHOT: *value = ctx->measure_snapshot; break;
     case PYRO_OPT_J1_SITE_MODE:
       *value = (ctx->j1_metro_site_mode ? 1 : 0) | (ctx->j1_or_site_mode ? 2 : 0);
       break;
@@ -1155,6 +1171,41 @@ int pyro_synchronize(pyro_ctx* ctx) {
   PYRO_CK(cudaSetDevice(ctx->device));
   PYRO_CK(cudaStreamSynchronize(ctx->stream));
   return check_wave_status(ctx);
+}
+
+int pyro_snapshot(pyro_ctx* ctx) {
+  if (!ctx) return PYRO_ERR_ARG;
+  PYRO_CK(cudaSetDevice(ctx->device));
+  if (!ctx->snap_stream) {
+    PYRO_CK(cudaStreamCreateWithFlags(&ctx->snap_stream, cudaStreamNonBlocking));
+    PYRO_CK(cudaEventCreateWithFlags(&ctx->snap_start, cudaEventDisableTiming));
+    PYRO_CK(cudaEventCreateWithFlags(&ctx->snap_done, cudaEventDisableTiming));
+    PYRO_CK(alloc(&ctx->d_snap, (size_t)ctx->n_spins));
+    PYRO_CK(alloc(&ctx->d_snap_temp_of_rep, (size_t)ctx->total_temps));
+    PYRO_CK(alloc(&ctx->d_snap_rep_of_temp, (size_t)ctx->total_temps));
+    PYRO_CK(alloc(&ctx->d_snap_energy, (size_t)ctx->total_reps));
+    PYRO_CK(alloc(&ctx->d_snap_mag, (size_t)3 * ctx->total_reps));
+  }
+  // The copy starts when the context stream reaches this point, after any
+  // measurement of the previous snapshot (same measurement stream); the
+  // context stream's next update waits until the copy has read the spins.
+  cudaStream_t ms = ctx->snap_stream;
+  PYRO_CK(cudaEventRecord(ctx->snap_start, ctx->stream));
+  PYRO_CK(cudaStreamWaitEvent(ms, ctx->snap_start, 0));
+  PYRO_CK(cudaMemcpyAsync(ctx->d_snap, ctx->d_spins, sizeof(float4) * (size_t)ctx->n_spins,
+                          cudaMemcpyDeviceToDevice, ms));
+  PYRO_CK(cudaMemcpyAsync(ctx->d_snap_temp_of_rep, ctx->d_temp_of_rep,
+                          sizeof(int) * ctx->total_temps, cudaMemcpyDeviceToDevice, ms));
+  PYRO_CK(cudaMemcpyAsync(ctx->d_snap_rep_of_temp, ctx->d_rep_of_temp,
+                          sizeof(int) * ctx->total_temps, cudaMemcpyDeviceToDevice, ms));
+  PYRO_CK(cudaMemcpyAsync(ctx->d_snap_energy, ctx->d_energy, sizeof(double) * ctx->total_reps,
+                          cudaMemcpyDeviceToDevice, ms));
+  PYRO_CK(cudaMemcpyAsync(ctx->d_snap_mag, ctx->d_mag, sizeof(double) * 3 * ctx->total_reps,
+                          cudaMemcpyDeviceToDevice, ms));
+  PYRO_CK(cudaEventRecord(ctx->snap_done, ms));
+  PYRO_CK(cudaStreamWaitEvent(ctx->stream, ctx->snap_done, 0));
+  ctx->snap_taken = true;
+  return PYRO_OK;
 }
 
 int pyro_system_info(const pyro_ctx* ctx, int system, int* L, int* n_sites, int* n_replicas,
@@ -1414,6 +1465,17 @@ int pyro_last_observables(pyro_ctx* ctx, int system, double* energy, double* mag
     return fail(ctx, PYRO_ERR_ARG, "last_observables: bad system");
   PYRO_CK(cudaSetDevice(ctx->device));
   const SysDev& s = ctx->sys[system];
+  if (ctx->measure_snapshot) {  // the energies the snapshot's cycle computed
+    const cudaStream_t st = ctx->snap_stream;
+    if (energy)
+      PYRO_CK(cudaMemcpyAsync(energy, ctx->d_snap_energy + s.rep_ctx_base,
+                              sizeof(double) * s.n_rep, cudaMemcpyDeviceToHost, st));
+    if (magnetisation3)
+      PYRO_CK(cudaMemcpyAsync(magnetisation3, ctx->d_snap_mag + 3 * s.rep_ctx_base,
+                              sizeof(double) * 3 * s.n_rep, cudaMemcpyDeviceToHost, st));
+    PYRO_CK(cudaStreamSynchronize(st));
+    return PYRO_OK;
+  }
   if (energy)
     PYRO_CK(cudaMemcpyAsync(energy, ctx->d_energy + s.rep_ctx_base, sizeof(double) * s.n_rep,
                             cudaMemcpyDeviceToHost, ctx->stream));
@@ -1453,9 +1515,10 @@ int pyro_get_temperatures(pyro_ctx* ctx, int system, double* temperature_of_repl
   const SysDev& s = ctx->sys[system];
   std::vector<int> t(s.n_temp);
   PYRO_CK(cudaSetDevice(ctx->device));
-  PYRO_CK(cudaMemcpyAsync(t.data(), ctx->d_temp_of_rep + s.temp_base, sizeof(int) * s.n_temp,
-                          cudaMemcpyDeviceToHost, ctx->stream));
-  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  const cudaStream_t st = measure_stream(ctx);
+  PYRO_CK(cudaMemcpyAsync(t.data(), measure_temp_of_rep(ctx) + s.temp_base,
+                          sizeof(int) * s.n_temp, cudaMemcpyDeviceToHost, st));
+  PYRO_CK(cudaStreamSynchronize(st));
   for (int g = 0; g < s.n_temp; ++g) temperature_of_replica[g] = ctx->ladders[system][t[g]];
   return PYRO_OK;
 }
@@ -1466,9 +1529,10 @@ int pyro_get_permutation(pyro_ctx* ctx, int system, int* replica_of_temperature)
     return fail(ctx, PYRO_ERR_ARG, "get_permutation: bad system or null pointer");
   const SysDev& s = ctx->sys[system];
   PYRO_CK(cudaSetDevice(ctx->device));
-  PYRO_CK(cudaMemcpyAsync(replica_of_temperature, ctx->d_rep_of_temp + s.temp_base,
-                          sizeof(int) * s.n_temp, cudaMemcpyDeviceToHost, ctx->stream));
-  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  const cudaStream_t st = measure_stream(ctx);
+  PYRO_CK(cudaMemcpyAsync(replica_of_temperature, measure_rep_of_temp(ctx) + s.temp_base,
+                          sizeof(int) * s.n_temp, cudaMemcpyDeviceToHost, st));
+  PYRO_CK(cudaStreamSynchronize(st));
   return PYRO_OK;
 }
 
@@ -1774,6 +1838,7 @@ int pyro_structure_factor(pyro_ctx* ctx, int system, int replica, int G, int str
   if (replica < -1 || replica >= sd.n_rep)
     return fail(ctx, PYRO_ERR_ARG, "structure_factor: replica out of range");
   PYRO_CK(cudaSetDevice(ctx->device));
+  const cudaStream_t st = measure_stream(ctx);
   if (!ctx->sq_ready) {
     PYRO_CK(sq_prepare());
     ctx->sq_ready = true;
@@ -1823,21 +1888,20 @@ int pyro_structure_factor(pyro_ctx* ctx, int system, int replica, int G, int str
     steps[k] = (int)(v < 0 ? v + p.Lf : v);
   }
   PYRO_CK(cudaMemcpyAsync(ctx->d_sq_tw, tw.data(), sizeof(double2) * tw.size(),
-                          cudaMemcpyHostToDevice, ctx->stream));
+                          cudaMemcpyHostToDevice, st));
   PYRO_CK(cudaMemcpyAsync(ctx->d_sq_s2, steps.data(), sizeof(int) * steps.size(),
-                          cudaMemcpyHostToDevice, ctx->stream));
-  PYRO_CK(cudaMemsetAsync(ctx->d_sq_out, 0, sizeof(double) * G3, ctx->stream));
+                          cudaMemcpyHostToDevice, st));
+  PYRO_CK(cudaMemsetAsync(ctx->d_sq_out, 0, sizeof(double) * G3, st));
   p.tw4 = ctx->d_sq_tw;
   for (int r = r0; r < r1; r += batch) {
     const int n = std::min(batch, r1 - r);
-    launch_structure_factor(ctx->d_spins + sd.spin_off + (long long)r * 16 * sd.L3, n, p,
+    launch_structure_factor(measure_spins(ctx) + sd.spin_off + (long long)r * 16 * sd.L3, n, p,
                             ctx->d_sq_tw + 4 * L, (const int*)ctx->d_sq_s2, ctx->d_sq_s1,
-                            ctx->d_sq_out, ctx->stream);
+                            ctx->d_sq_out, st);
     PYRO_CK_LAUNCH();
   }
-  PYRO_CK(cudaMemcpyAsync(out, ctx->d_sq_out, sizeof(double) * G3, cudaMemcpyDeviceToHost,
-                          ctx->stream));
-  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  PYRO_CK(cudaMemcpyAsync(out, ctx->d_sq_out, sizeof(double) * G3, cudaMemcpyDeviceToHost, st));
+  PYRO_CK(cudaStreamSynchronize(st));
   return PYRO_OK;
 }
 

@@ -137,6 +137,20 @@ struct pyro_ctx {
 
   pyro::TetState* tet = nullptr;
 
+  // Measurement snapshot (pyro_snapshot): copies of every system's spins, of
+  // the replica <-> temperature maps and of the last cycle's FP64 energies
+  // and magnetisations, taken on snap_stream; with measure_snapshot set the
+  // measurement calls read them there while later cycles run.
+  float4* d_snap = nullptr;
+  int* d_snap_temp_of_rep = nullptr;
+  int* d_snap_rep_of_temp = nullptr;
+  double* d_snap_energy = nullptr;
+  double* d_snap_mag = nullptr;
+  cudaStream_t snap_stream = nullptr;
+  cudaEvent_t snap_start = nullptr, snap_done = nullptr;
+  bool snap_taken = false;
+  int measure_snapshot = 0;
+
   // Per-sublattice magnetisation partials, grown on demand (exchange.cu).
   double* d_submag = nullptr;
   size_t submag_cap = 0;
@@ -159,6 +173,21 @@ inline bool j1_sweepable(const SysDev& s) {
 inline int fail(pyro_ctx* c, int code, const std::string& msg) {
   if (c) c->err = msg;
   return code;
+}
+
+// What the measurement calls read: the live state on the context stream,
+// or (measure_snapshot) the last pyro_snapshot on the measurement stream.
+inline const float4* measure_spins(const pyro_ctx* c) {
+  return c->measure_snapshot ? c->d_snap : c->d_spins;
+}
+inline cudaStream_t measure_stream(const pyro_ctx* c) {
+  return c->measure_snapshot ? c->snap_stream : c->stream;
+}
+inline const int* measure_temp_of_rep(const pyro_ctx* c) {
+  return c->measure_snapshot ? c->d_snap_temp_of_rep : c->d_temp_of_rep;
+}
+inline const int* measure_rep_of_temp(const pyro_ctx* c) {
+  return c->measure_snapshot ? c->d_snap_rep_of_temp : c->d_rep_of_temp;
 }
 
 // Drops the captured cycle graphs and rebuilds the pass schedules (after a

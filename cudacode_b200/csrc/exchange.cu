@@ -262,16 +262,16 @@ int pyro_sublattice_magnetisation(pyro_ctx* ctx, int system, double* out) {
   }
   double* partials = ctx->d_submag;
   double* d_out = ctx->d_submag + (size_t)s.n_rep * 16 * chunks * 3;
-  plane_sum_kernel<<<dim3(chunks, 16, s.n_rep), kMagThreads, 0, ctx->stream>>>(
-      ctx->d_spins + s.spin_off, s.L3, chunks, partials);
+  const cudaStream_t st = measure_stream(ctx);
+  plane_sum_kernel<<<dim3(chunks, 16, s.n_rep), kMagThreads, 0, st>>>(
+      measure_spins(ctx) + s.spin_off, s.L3, chunks, partials);
   PYRO_CK_LAUNCH();
-  sublattice_finalise_kernel<<<(s.n_rep * 12 + 127) / 128, 128, 0, ctx->stream>>>(partials, s.n_rep,
-                                                                                chunks, d_out);
+  sublattice_finalise_kernel<<<(s.n_rep * 12 + 127) / 128, 128, 0, st>>>(partials, s.n_rep,
+                                                                       chunks, d_out);
   PYRO_CK_LAUNCH();
   ctx->launches += 2;
-  PYRO_CK(cudaMemcpyAsync(out, d_out, sizeof(double) * 12 * s.n_rep, cudaMemcpyDeviceToHost,
-                          ctx->stream));
-  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  PYRO_CK(cudaMemcpyAsync(out, d_out, sizeof(double) * 12 * s.n_rep, cudaMemcpyDeviceToHost, st));
+  PYRO_CK(cudaStreamSynchronize(st));
   return PYRO_OK;
 }
 

@@ -182,18 +182,18 @@ int pyro_order_parameters(pyro_ctx* ctx, int system, double* out) {
   if (rc) return rc;
   double* part = reinterpret_cast<double*>(ctx->d_order);
   double* d_out = part + n_part;
-  order_partials_kernel<<<dim3(chunks, s.n_rep), kOrdThreads, 0, ctx->stream>>>(
-      ctx->d_spins + s.spin_off, s.L3, chunks, part);
+  const cudaStream_t st = measure_stream(ctx);
+  order_partials_kernel<<<dim3(chunks, s.n_rep), kOrdThreads, 0, st>>>(
+      measure_spins(ctx) + s.spin_off, s.L3, chunks, part);
   PYRO_CK_LAUNCH();
-  order_finalise_kernel<<<(int)((n_out + 127) / 128), 128, 0, ctx->stream>>>(part, s.n_rep, chunks,
-                                                                          d_out);
+  order_finalise_kernel<<<(int)((n_out + 127) / 128), 128, 0, st>>>(part, s.n_rep, chunks, d_out);
   PYRO_CK_LAUNCH();
   ctx->launches += 2;
   std::string buf;
   buf.resize(sizeof(double) * n_out);
   double* h = reinterpret_cast<double*>(&buf[0]);
-  PYRO_CK(cudaMemcpyAsync(h, d_out, sizeof(double) * n_out, cudaMemcpyDeviceToHost, ctx->stream));
-  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  PYRO_CK(cudaMemcpyAsync(h, d_out, sizeof(double) * n_out, cudaMemcpyDeviceToHost, st));
+  PYRO_CK(cudaStreamSynchronize(st));
   for (int r = 0; r < s.n_rep; ++r) {
     const double* p = h + (size_t)r * kOrdPart;
     double* o = out + (size_t)r * kOrdQ;
@@ -221,12 +221,13 @@ int pyro_ising_configuration(pyro_ctx* ctx, int system, int replica, int* out) {
   int rc = grow_scratch(ctx, sizeof(int) * (size_t)s.L3);
   if (rc) return rc;
   int* d = reinterpret_cast<int*>(ctx->d_order);
-  ising_kernel<<<(s.L3 + 255) / 256, 256, 0, ctx->stream>>>(
-      ctx->d_spins + s.spin_off + (long long)replica * 16 * s.L3, s.L3, d);
+  const cudaStream_t st = measure_stream(ctx);
+  ising_kernel<<<(s.L3 + 255) / 256, 256, 0, st>>>(
+      measure_spins(ctx) + s.spin_off + (long long)replica * 16 * s.L3, s.L3, d);
   PYRO_CK_LAUNCH();
   ctx->launches += 1;
-  PYRO_CK(cudaMemcpyAsync(out, d, sizeof(int) * s.L3, cudaMemcpyDeviceToHost, ctx->stream));
-  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  PYRO_CK(cudaMemcpyAsync(out, d, sizeof(int) * s.L3, cudaMemcpyDeviceToHost, st));
+  PYRO_CK(cudaStreamSynchronize(st));
   return PYRO_OK;
 }
 

@@ -87,6 +87,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "pyro_set_stream": (i, [P, P]),
         "pyro_get_stream": (P, [P]),
         "pyro_synchronize": (i, [P]),
+        "pyro_snapshot": (i, [P]),
         "pyro_system_info": (i, [P, i, pi, pi, pi, pi]),
         "pyro_init_random": (i, [P]),
         "pyro_set_spins": (i, [P, i, pf]),
@@ -291,6 +292,7 @@ class Engine:
     OPT_TET_GROUPED = 11
     OPT_FUSED_OBS = 12
     OPT_WAVE_STALL = 13
+    OPT_MEASURE_SNAPSHOT = 14
 
     def set_option(self, option: int, value: int) -> None:
         self._ck(self.lib.pyro_set_option(self.ctx, option, value))
@@ -315,6 +317,10 @@ class Engine:
 
     def synchronize(self) -> None:
         self._ck(self.lib.pyro_synchronize(self.ctx))
+
+    def snapshot(self) -> None:
+        """Queues a measurement snapshot (pyro_snapshot)."""
+        self._ck(self.lib.pyro_snapshot(self.ctx))
 
     def info(self, system: int = 0) -> dict:
         L, n, r, c = C.c_int(), C.c_int(), C.c_int(), C.c_int()

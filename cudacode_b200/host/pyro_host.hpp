@@ -113,6 +113,34 @@ inline void ParallelTempering(Device& d, int OverRelaxation, int McSteps,
   d.check(pyro_get_temperatures(d.ctx(), 0, Temperatures.data()));
 }
 
+// ApplyParallelTemperingDuringMeasure (MonteCarlo.cu:613-657): queues
+// McSteps sweeps and one exchange without waiting for them.
+inline void ParallelTemperingAsync(Device& d, int OverRelaxation, int McSteps) {
+  d.check(pyro_cycle(d.ctx(), McSteps, McSteps * OverRelaxation, 1, 1));
+}
+
+// ExtractConfigurationsFromMonteCarlo (Pyrochlore.cu:1608-1617): a
+// measurement snapshot of the state the queued Monte Carlo reaches; the
+// Monte Carlo queued after it runs while the snapshot is measured.
+inline void ExtractConfigurationsFromMonteCarlo(Device& d) { d.check(pyro_snapshot(d.ctx())); }
+
+// Measurement calls read the last snapshot (on) or the live state (off).
+inline void MeasureSnapshot(Device& d, bool on) {
+  d.check(pyro_set_option(d.ctx(), PYRO_OPT_MEASURE_SNAPSHOT, on ? 1 : 0));
+}
+
+// Energies the cycle of the measured state computed, per configuration slot.
+inline void CycleEnergies(Device& d, std::vector<double>& Energies) {
+  Energies.resize(d.replicas());
+  d.check(pyro_last_observables(d.ctx(), 0, Energies.data(), nullptr));
+}
+
+// Temperature of each configuration slot in the measured state.
+inline void SlotTemperatures(Device& d, std::vector<double>& Temperatures) {
+  Temperatures.resize(d.replicas());
+  d.check(pyro_get_temperatures(d.ctx(), 0, Temperatures.data()));
+}
+
 // CalculateSolidAngle(device, OR, McSteps, ratio, Temperatures, CosThetaSolid)
 // (MonteCarlo.cu:371-426): cone width of every temperature for `ratio`
 // acceptance.

@@ -192,10 +192,19 @@ void run(const Options& o, int rep, const std::string& series) {
   std::vector<double> e_row(2 * nT), op_row(10 * nT), dchi_row(10 * nT), q_row(3 * nT),
       sz_row(nT), szs_row(nT), mag_row(nT);
   std::vector<int> slot(nT, 0);  // replica holding temperature t
+  // Measure cycle m from a snapshot while cycle m + 1 runs on the GPU.
+  pyro_host::ParallelTemperingAsync(dev, o.over_relaxation, o.mc_steps_pt);
+  pyro_host::ExtractConfigurationsFromMonteCarlo(dev);
   for (int m = 0; m < o.n_measures; ++m) {
-    pyro_host::ParallelTempering(dev, o.over_relaxation, o.mc_steps_pt, temps, energies);
+    if (m + 1 < o.n_measures)
+      pyro_host::ParallelTemperingAsync(dev, o.over_relaxation, o.mc_steps_pt);
+    pyro_host::MeasureSnapshot(dev, true);
+    pyro_host::CycleEnergies(dev, energies);
+    pyro_host::SlotTemperatures(dev, temps);
     if (fm || o.magnetization) pyro_host::MagnetizationG(dev, o.gxy, o.gz, M);
     if (need_op) pyro_host::OrderParameters(dev, op);
+    pyro_host::MeasureSnapshot(dev, false);
+    if (m + 1 < o.n_measures) pyro_host::ExtractConfigurationsFromMonteCarlo(dev);
     for (size_t r = 0; r < temps.size(); ++r)
       for (int t = 0; t < nT; ++t)
         if (temps[r] == T[t]) slot[t] = (int)r;

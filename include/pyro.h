@@ -143,6 +143,15 @@ int pyro_neighbour_table(int site, int* out120);
  * partly updated. -1 (default) is normal operation. Used to test the
  * bounded waits without a device fault. */
 #define PYRO_OPT_WAVE_STALL 13
+/* PYRO_OPT_MEASURE_SNAPSHOT: 1 makes the measurement calls
+ * (pyro_last_observables, pyro_get_temperatures, pyro_get_permutation,
+ * pyro_order_parameters, pyro_sublattice_magnetisation,
+ * pyro_structure_factor, pyro_ising_configuration) read the last
+ * pyro_snapshot on the context's measurement stream, so they run while the
+ * Monte Carlo calls queued after the snapshot proceed on the context
+ * stream; 0 (default) reads the live state on the context stream. Needs a
+ * snapshot first (else PYRO_ERR_STATE). Changes no kernel schedule. */
+#define PYRO_OPT_MEASURE_SNAPSHOT 14
 int pyro_set_option(pyro_ctx* ctx, int option, int value);
 int pyro_get_option(pyro_ctx* ctx, int option, int* value);
 /* Autotuner: times every kernel variant (per-pass generic, per-pass J1,
@@ -160,6 +169,18 @@ void* pyro_get_stream(const pyro_ctx* ctx);
 /* Wait for all work queued by the context. Replaces SynchronizeJobs
  * (MonteCarlo.cu:230-245). */
 int pyro_synchronize(pyro_ctx* ctx);
+/* Measurement snapshot. Replaces ExtractConfigurationsFromMonteCarlo
+ * (Pyrochlore.cu:1608-1617), which copies the working spins into a
+ * measurement buffer so that the next Monte Carlo block runs while the
+ * previous one is measured (ApplyParallelTemperingDuringMeasure,
+ * MonteCarlo.cu:613-657). Queues, at the current point of the context
+ * stream, a device copy of every system's spins, of the replica <->
+ * temperature maps and of the last cycle's FP64 energies and
+ * magnetisations, on the context's measurement stream; the context stream's
+ * next work waits only for that copy (a few hundred microseconds for
+ * gigabytes of spins). Returns without waiting; the first call allocates the
+ * snapshot buffers. Not allowed during a stream capture. */
+int pyro_snapshot(pyro_ctx* ctx);
 
 /* Sizes of one system, and the number of colour classes its sweep uses
  * (4 for J1 only, 16 when J2/J3 are present). */
