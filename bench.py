@@ -647,6 +647,81 @@ def run_learned(args):
     return 0
 
 
+def learned_leg(cycles: int = 60000, warmup: int = 2000) -> dict:
+    """The second half of the metric, compact: energy ESS/s at T=0.05 of the
+    learned method against the plain method, each at a fixed schedule chosen
+    beforehand by the full learned workload (`--workload learned`): plain
+    3 Metropolis + 1 over-relaxation sweeps per exchange (the plain method's
+    best), learned 2 tetrahedron sweeps per exchange. L=16 (65,536 sites),
+    8 temperatures geometric in [0.05, 0.5]; the network trained on the GPU
+    on 2^20 tetrahedra from the plain chains; chains of `cycles` exchange
+    cycles each, device time by CUDA events, tau_int by Sokal windowing."""
+    import torch
+
+    from cudacode_b200 import stats
+    from cudacode_b200.engine import Engine, System, geometric_ladder
+
+    Ll, nT = 16, 8
+    temps = geometric_ladder(0.05, 0.5, nT)
+    eng = Engine([System(L=Ll, temperatures=temps)], seed=SEED + 3)
+    stream = torch.cuda.Stream()
+    eng.set_stream(stream.cuda_stream)
+    eng.init_random()
+    eng.tune_cone(0.5, 20, 5, 1)
+    eng.cycle(3, 1, True, warmup)
+    eng.tet_init(seed=7, sample_capacity=1 << 20)
+    n_samples = 0
+    while n_samples < (1 << 20):
+        eng.cycle(3, 1, True, 25)
+        n_samples += eng.tet_collect(1)
+    t0 = time.perf_counter()
+    eng.tet_train(1500, 4096, 2e-3)
+    eng.tet_train(4500, 4096, 5e-4)
+    loss = eng.tet_train(3000, 4096, 2e-4)
+    train_s = time.perf_counter() - t0
+    choice = eng.autotune(3, 1, 5)
+    n = 16 * Ll ** 3
+
+    def chain(n_metro, n_or, n_tet):
+        run = (lambda k: eng.cycle(n_metro, n_or, True, k)) if n_tet == 0 else \
+            (lambda k: eng.cycle_tet(n_metro, n_or, n_tet, True, k))
+        run(warmup)
+        eng.enable_history(cycles)
+        eng.tet_reset_acceptance()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        run(cycles)
+        b.record(stream)
+        torch.cuda.synchronize()
+        sec = a.elapsed_time(b) / 1e3
+        h = eng.history()
+        tau = stats.tau_int(h[:, 0])
+        means = [stats.mean_error(h[:, t] / n) for t in range(nT)]
+        out = {"schedule": {"metropolis": n_metro, "overrelax": n_or, "tetrahedron": n_tet},
+               "us_per_cycle": 1e6 * sec / cycles, "tau_int_T0.05": tau,
+               "ess_per_s_T0.05": cycles / (2 * tau) / sec, "E_per_site": means}
+        if n_tet:
+            acc, prop = eng.tet_acceptance()
+            out["tet_acceptance_T0.05"] = float(acc[0] / max(prop[0], 1))
+        return out
+
+    plain = chain(3, 1, 0)
+    learned = chain(0, 0, 2)
+    agree = [abs(p[0] - q[0]) / max(float(np.hypot(p[1], q[1])), 1e-30)
+             for p, q in zip(plain["E_per_site"], learned["E_per_site"])]
+    eng.close()
+    return {"metric": "energy ESS/s at T=0.05, learned proposal vs the plain method at its best "
+                      "schedule",
+            "ratio_vs_plain_best_schedule": learned["ess_per_s_T0.05"] / plain["ess_per_s_T0.05"],
+            "plain": plain, "learned": learned, "cycles_per_chain": cycles,
+            "energy_agreement_sigma_max": max(agree),
+            "config": {"workload": "L=16 (65,536 sites), J1=1 AFM, 8 temperatures geometric in "
+                                   "[0.05, 0.5]", "training_samples": n_samples,
+                       "train_seconds": train_s, "loss_last": loss,
+                       "autotune_choice_plain": choice}}
+
+
 WAVE_PROFILE = os.path.join(ROOT, "profiles", "wave_kernel_L32_R64.md")
 
 
@@ -711,6 +786,8 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the learned-proposal ESS/s leg of the default line")
     ap.add_argument("--dry-run", action="store_true",
                     help="check the launcher only: ranks meet over gloo, no GPU work")
     ap.add_argument("--L", type=int, default=L, help="lattice size (profiling cases)")
@@ -903,6 +980,9 @@ def main():
     cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu, parity = cpu_baseline_and_parity(options)
+    learned = None
+    if rank == 0 and world == 1 and not args.no_learned:
+        learned = learned_leg()
 
     if rank == 0:
         line = {
@@ -935,6 +1015,7 @@ def main():
                     "traffic": profiled_traffic() if (L, R_PER_GPU) == (32, 64) else None}},
             "cpu_baseline": cpu,
             "parity": parity,
+            "learned": learned,
             "e2e": {"value": e2e_value, "unit": "updates/ns",
                     "h2d_bytes_per_step": 4 * len(temps),
                     "d2h_bytes_per_step": 8 * R_PER_GPU + 24 * R_PER_GPU},

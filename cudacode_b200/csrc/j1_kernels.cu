@@ -745,52 +745,62 @@ template <bool kExch, int kForms>
 __global__ void __launch_bounds__(kJ1Threads, kForms == 3 ? 4 : 2)
     j1_wave_kernel(const J1WaveParams w) {
   constexpr bool kMetroSite = (kForms & 1) != 0, kOrSite = (kForms & 2) != 0;
-  __shared__ int s_item;
+  __shared__ int s_info[5];  // item (or -1), replica, pass, chunk, sub-item
+  __shared__ unsigned int s_need;
   __shared__ double red[4][kJ1Threads / 32];
-  if (threadIdx.x == 0) s_item = (int)atomicAdd(w.queue, 1u);
-  __syncthreads();
-  const int item = s_item;
-  if (item >= w.n_items) return;
   const int nq = w.n_chunks;
   const int n_passes = 4 * (w.n_metro + w.n_or);  // colour passes; pass n_passes: observables
-  // Items per chunk before pass k (cum) and of pass k (sub): the Metropolis
-  // passes come first, then the over-relaxation passes, then (with_obs) one
-  // observables item per chunk.
-  const int m_items = 4 * w.n_metro * w.sub_metro;
-  const int c_items = m_items + 4 * w.n_or * w.sub_or;
-  // item -> (replica group g, pass k, position j, replica, sub-item f)
-  const int per_group = w.group * nq * (c_items + (w.with_obs ? 1 : 0));
-  const int g = item / per_group;
-  const int local = item - g * per_group;
-  const int r0 = g * w.group;
-  const int cnt = min(w.group, w.pass.n_rep - r0);
-  const int per_unit = cnt * nq;
-  const int u = local / per_unit;
-  int k, cum, sub;
-  if (u < m_items) {
-    sub = w.sub_metro;
-    k = u / sub;
-    cum = k * sub;
-  } else if (u < c_items) {
-    sub = w.sub_or;
-    k = 4 * w.n_metro + (u - m_items) / sub;
-    cum = m_items + (k - 4 * w.n_metro) * sub;
-  } else {
-    sub = 1;
-    k = n_passes;
-    cum = c_items;
+  if (threadIdx.x == 0) {
+    // One thread takes the ticket and decodes it:
+    // item -> (replica group g, pass k, position j, replica, sub-item f).
+    // Items per chunk before pass k (cum) and of pass k (sub): the
+    // Metropolis passes come first, then the over-relaxation passes, then
+    // (with_obs) one observables item per chunk.
+    const int item = (int)atomicAdd(w.queue, 1u);
+    s_info[0] = item < w.n_items ? item : -1;
+    if (item < w.n_items) {
+      const int m_items = 4 * w.n_metro * w.sub_metro;
+      const int c_items = m_items + 4 * w.n_or * w.sub_or;
+      const int per_group = w.group * nq * (c_items + (w.with_obs ? 1 : 0));
+      const int g = item / per_group;
+      const int local = item - g * per_group;
+      const int r0 = g * w.group;
+      const int cnt = min(w.group, w.pass.n_rep - r0);
+      const int per_unit = cnt * nq;
+      const int u = local / per_unit;
+      int k, cum, sub;
+      if (u < m_items) {
+        sub = w.sub_metro;
+        k = u / sub;
+        cum = k * sub;
+      } else if (u < c_items) {
+        sub = w.sub_or;
+        k = 4 * w.n_metro + (u - m_items) / sub;
+        cum = m_items + (k - 4 * w.n_metro) * sub;
+      } else {
+        sub = 1;
+        k = n_passes;
+        cum = c_items;
+      }
+      const int wi = local - per_unit * cum;
+      const int tt = wi / sub;
+      const int j = tt / cnt;
+      s_info[1] = r0 + (tt - j * cnt);
+      s_info[2] = k;
+      s_info[3] = (int)(((long long)j + (long long)w.dep * k) % nq);
+      s_info[4] = wi - tt * sub;  // FCC corner of a site-form pass
+      s_need = (unsigned int)cum;
+    }
   }
-  const int wi = local - per_unit * cum;
-  const int f = wi % sub;  // FCC corner of a site-form pass
-  const int tt = wi / sub;
-  const int rep = r0 + tt % cnt;
-  const int j = tt / cnt;
-  const int q = (int)(((long long)j + (long long)w.dep * k) % nq);
+  __syncthreads();
+  const int item = s_info[0];
+  if (item < 0) return;
+  const int rep = s_info[1], k = s_info[2], q = s_info[3], f = s_info[4];
   // Wait until pass k - 1 is complete on every chunk holding a neighbour.
   int failed = 0;
   if (k > 0) {
     const int n_dep = 2 * w.dep + 1 >= nq ? nq : 2 * w.dep + 1;
-    const unsigned int need = (unsigned int)cum;
+    const unsigned int need = s_need;
     const unsigned int* row = w.progress + (long long)rep * nq;
     for (int d = threadIdx.x; d < n_dep; d += blockDim.x) {
       int qq = n_dep == nq ? d : q - w.dep + d;
