@@ -254,6 +254,52 @@ int queue_wave(pyro_ctx* ctx, int n_metro, int n_or, bool with_obs) {
   return PYRO_OK;
 }
 
+// The skewed multi-group launches run the J1 systems of a cycle without
+// learned sweeps.
+bool use_skew_kernel(const pyro_ctx* ctx, int n_metro, int n_or, int n_tet) {
+  return ctx->cycle_kernel == 3 && ctx->use_j1_kernel && !ctx->j1_sys.empty() && n_tet == 0 &&
+         n_metro + n_or > 0;
+}
+
+// Skewed launches per J1 system: replica groups of PYRO_OPT_REPLICA_GROUP
+// (0: 2), about PYRO_OPT_CHAINS groups in flight per launch.
+int queue_skew(pyro_ctx* ctx, int n_metro, int n_or, bool with_obs) {
+  const int forms = (ctx->j1_metro_site_mode ? 1 : 0) | (ctx->j1_or_site_mode ? 2 : 0);
+  for (int si : ctx->j1_sys) {
+    const SysDev& s = ctx->sys[si];
+    J1SkewParams sp;
+    std::memset(&sp, 0, sizeof sp);
+    J1WaveParams& w = sp.w;
+    w.pass = j1_params(ctx, si, 0);
+    w.n_metro = n_metro;
+    w.n_or = n_or;
+    w.group = std::min(ctx->rep_group > 0 ? ctx->rep_group : 2, s.n_rep);
+    w.n_chunks = j1_blocks_per_replica(s.L3);
+    w.with_obs = with_obs && s.exch < 0 ? 1 : 0;
+    w.obs.spins = ctx->d_spins + s.spin_off;
+    w.obs.L = s.L;
+    w.obs.L3 = s.L3;
+    w.obs.n_rep = s.n_rep;
+    w.obs.rcpL = 1.0f / (float)s.L;
+    w.obs.J1 = s.J64[0];
+    w.obs.partials = ctx->d_partials;
+    w.obs.partial_begin = ctx->obs_segs[si].partial_begin;
+    w.sub_metro = (forms & 1) ? 4 : 1;
+    w.sub_or = (forms & 2) ? 4 : 1;
+    w.stall_item = -1;
+    sp.n_groups = (s.n_rep + w.group - 1) / w.group;
+    const int passes = skew_passes(w);
+    const int in_flight = std::max(1, ctx->n_chains);
+    sp.stagger = std::max(1, (passes + in_flight - 1) / in_flight);
+    const int launches = sp.stagger * (sp.n_groups - 1) + passes;
+    for (int t = 0; t < launches; ++t) {
+      sp.t = t;
+      PYRO_CK(launch_j1_skew(sp, forms, ctx->stream));
+    }
+  }
+  return PYRO_OK;
+}
+
 // Queues the copy of the work-queue kernel's status word to pinned host
 // memory (read by wave_status_result after the stream synchronised).
 int queue_wave_status(pyro_ctx* ctx) {
@@ -412,13 +458,15 @@ bool j1_grouped_path(const pyro_ctx* ctx) {
 int queue_cycle_body(pyro_ctx* ctx, int n_metro, int n_or, bool with_obs, int n_tet = 0) {
   int rc = check_cluster(ctx);
   if (rc) return rc;
-  if (use_wave_kernel(ctx, n_metro, n_or, n_tet)) {
-    // other systems on their usual kernels, then one launch per J1 system
+  const bool skew = use_skew_kernel(ctx, n_metro, n_or, n_tet);
+  if (skew || use_wave_kernel(ctx, n_metro, n_or, n_tet)) {
+    // other systems on their usual kernels, then the J1 systems' launches
     if (!ctx->gen_groups.empty())
       rc = queue_grouped(ctx, n_metro, n_or, false, true, with_obs, 0);
     else
       rc = queue_generic_sweeps(ctx, n_metro, n_or);
-    if (rc == PYRO_OK) rc = queue_wave(ctx, n_metro, n_or, with_obs);
+    if (rc == PYRO_OK)
+      rc = skew ? queue_skew(ctx, n_metro, n_or, with_obs) : queue_wave(ctx, n_metro, n_or, with_obs);
     if (rc == PYRO_OK && with_obs) rc = queue_observables(ctx, /*skip_j1=*/true);
     return rc;
   }
@@ -1023,7 +1071,7 @@ int pyro_set_option(pyro_ctx* ctx, int option, int value) {
     ctx->j1_metro_site_mode = (value & 1) != 0;
     ctx->j1_or_site_mode = (value & 2) != 0;
   } else if (option == PYRO_OPT_CYCLE_KERNEL) {
-    if (value < 0 || value > 2) return fail(ctx, PYRO_ERR_ARG, "cycle kernel option is 0, 1 or 2");
+    if (value < 0 || value > 3) return fail(ctx, PYRO_ERR_ARG, "cycle kernel option is 0..3");
     ctx->cycle_kernel = value;
     ctx->cluster_checked = false;
   } else if (option == PYRO_OPT_WAVE_STALL) {
@@ -1094,7 +1142,11 @@ int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen)
                            // the work-queue cycle kernel: forms, replica groups
                            {1, 2, 16, 3, 2, 1, 0}, {1, 2, 16, 3, 4, 1, 0}, {1, 2, 16, 3, 8, 1, 0},
                            {1, 2, 16, 3, 16, 1, 0}, {1, 2, 16, 3, 0, 1, 0}, {1, 2, 16, 1, 4, 1, 0},
-                           {1, 2, 16, 1, 8, 1, 0}, {1, 2, 16, 2, 8, 1, 0}};
+                           {1, 2, 16, 1, 8, 1, 0}, {1, 2, 16, 2, 8, 1, 0},
+                           // skewed multi-group launches: forms, group size, groups in flight
+                           {1, 3, 16, 3, 2, 4, 0}, {1, 3, 16, 3, 2, 8, 0}, {1, 3, 16, 3, 1, 8, 0},
+                           {1, 3, 16, 3, 4, 4, 0}, {1, 3, 16, 1, 2, 4, 0}, {1, 3, 16, 1, 2, 8, 0},
+                           {1, 3, 16, 1, 4, 4, 0}, {1, 3, 16, 3, 4, 2, 0}};
     vs.insert(vs.end(), std::begin(j1v), std::end(j1v));
     n_j1 = (int)vs.size();
   }
@@ -1139,7 +1191,7 @@ int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen)
     int rc = apply(v);
     if (rc) continue;
     if (v.cyc == 1 && (ctx->cycle_kernel != 1 || ctx->cluster_size != v.cs)) continue;
-    if (v.cyc == 2 && ctx->cycle_kernel != 2) continue;
+    if (v.cyc >= 2 && ctx->cycle_kernel != v.cyc) continue;
     if ((rc = pyro_cycle(ctx, n_metro, n_or, swap, 1))) return rc;  // build the graph
     float ms = 1e30f;
     for (int rep = 0; rep < 2; ++rep) {  // best of two timings

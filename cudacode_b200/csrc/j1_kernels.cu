@@ -20,6 +20,8 @@
 // MagnetizationGPU (277-342) by sums over tetrahedra.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "../../include/pyro_math.h"
 #include "j1_kernels.cuh"
 
@@ -840,6 +842,60 @@ __global__ void __launch_bounds__(kJ1Threads, kForms == 3 ? 4 : 2)
   if (threadIdx.x == 0 && item != w.stall_item)
     release_add_gpu(w.progress + (long long)rep * nq + q, 1u);
 }
+
+// Skewed launches (see J1SkewParams): launch t runs pass t - stagger g of
+// every replica group g that has one, all of them independent (different
+// replicas); consecutive passes of a group are ordered by the stream. The
+// CTA's item comes from blockIdx.x across the groups of the launch, group by
+// group, then (replica, chunk, sub-item) as in the work-queue kernel.
+template <bool kExch, int kForms>
+__global__ void __launch_bounds__(kJ1Threads, kForms == 3 ? 4 : 2)
+    j1_skew_kernel(const J1SkewParams sp) {
+  constexpr bool kMetroSite = (kForms & 1) != 0, kOrSite = (kForms & 2) != 0;
+  pass_prologue();
+  const J1WaveParams& w = sp.w;
+  __shared__ int s_info[4];  // replica, pass, chunk, sub-item
+  __shared__ double red[4][kJ1Threads / 32];
+  const int nq = w.n_chunks;
+  const int n_passes = 4 * (w.n_metro + w.n_or);
+  if (threadIdx.x == 0) {
+    int b = blockIdx.x;
+    int g = skew_first_group(sp);
+    for (;; ++g) {
+      const int k = sp.t - sp.stagger * g;
+      const int cnt = min(w.group, w.pass.n_rep - g * w.group);
+      const int sub = skew_sub(w, k);
+      const int items = cnt * nq * sub;
+      if (b < items) {
+        const int tt = b / sub;
+        const int r = tt % cnt;
+        s_info[0] = g * w.group + r;
+        s_info[1] = k;
+        s_info[2] = tt / cnt;
+        s_info[3] = b - tt * sub;
+        break;
+      }
+      b -= items;
+    }
+  }
+  __syncthreads();
+  const int rep = s_info[0], k = s_info[1], q = s_info[2], f = s_info[3];
+  if (k == n_passes) {  // the group's observables, in the layout of j1_observables_kernel
+    const float4* rb = w.pass.spins + (long long)rep * 16 * w.pass.L3;
+    wave_observables(rb, q * kJ1Threads + threadIdx.x, w.pass.L, w.pass.L3, w.pass.rcpL, w.obs.J1,
+                     red, w.obs.partials + w.obs.partial_begin + (long long)rep * nq + q);
+    return;
+  }
+  const int sweep_idx = k >> 2;
+  const bool metro = sweep_idx < w.n_metro;
+  const unsigned long long sweep_add = (unsigned long long)sweep_idx;
+  switch (k & 3) {
+    case 0: wave_item<0, kExch, kMetroSite, kOrSite>(w, rep, q, f, metro, sweep_add); break;
+    case 1: wave_item<1, kExch, kMetroSite, kOrSite>(w, rep, q, f, metro, sweep_add); break;
+    case 2: wave_item<2, kExch, kMetroSite, kOrSite>(w, rep, q, f, metro, sweep_add); break;
+    default: wave_item<3, kExch, kMetroSite, kOrSite>(w, rep, q, f, metro, sweep_add); break;
+  }
+}
 }  // namespace
 
 namespace {
@@ -947,6 +1003,37 @@ WaveKernel wave_kernel(bool exch, int forms) {
 cudaError_t launch_j1_wave(const J1WaveParams& p, int forms, cudaStream_t st) {
   wave_kernel(p.pass.exch != 0, forms)<<<p.n_items, kJ1Threads, 0, st>>>(p);
   return cudaGetLastError();
+}
+
+int j1_skew_items(const J1SkewParams& sp) {
+  const J1WaveParams& w = sp.w;
+  int total = 0;
+  for (int g = skew_first_group(sp); g <= skew_last_group(sp); ++g) {
+    const int cnt = std::min(w.group, w.pass.n_rep - g * w.group);
+    total += cnt * w.n_chunks * skew_sub(w, sp.t - sp.stagger * g);
+  }
+  return total;
+}
+
+cudaError_t launch_j1_skew(const J1SkewParams& sp, int forms, cudaStream_t st) {
+  using SkewKernel = void (*)(const J1SkewParams);
+  static const SkewKernel k[2][4] = {
+      {j1_skew_kernel<false, 0>, j1_skew_kernel<false, 1>, j1_skew_kernel<false, 2>,
+       j1_skew_kernel<false, 3>},
+      {j1_skew_kernel<true, 0>, j1_skew_kernel<true, 1>, j1_skew_kernel<true, 2>,
+       j1_skew_kernel<true, 3>}};
+  const int items = j1_skew_items(sp);
+  if (items <= 0) return cudaSuccess;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(items, 1, 1);
+  cfg.blockDim = dim3(kJ1Threads, 1, 1);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = sp.w.pass.pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k[sp.w.pass.exch ? 1 : 0][forms & 3], sp);
 }
 
 cudaError_t j1_cycle_prepare(int cluster_size, int* max_active_clusters) {

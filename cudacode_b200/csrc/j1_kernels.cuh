@@ -103,6 +103,40 @@ struct J1WaveParams {
 // forms: bit 0 Metropolis passes in the site form, bit 1 over-relaxation
 // passes in the site form.
 cudaError_t launch_j1_wave(const J1WaveParams& p, int forms, cudaStream_t st);
+
+// A cycle of one J1 system as skewed launches: replica group g (of w.group
+// replicas) runs its pass k (k < 4 (n_metro + n_or): colour passes; k ==
+// 4 (n_metro + n_or), with w.with_obs: its energy partials) in launch
+// t = stagger g + k, so every launch holds the passes of about
+// passes / stagger groups at once (one launch fills the GPU; their spins
+// stay in L2) and needs no synchronisation inside: its items belong to
+// different replicas, and consecutive passes of a group are in consecutive
+// launches of one stream. Items and their code are the work-queue kernel's
+// (w.queue, w.progress and w.status are unused).
+struct J1SkewParams {
+  J1WaveParams w;
+  int t;         // launch index, 0 .. stagger (n_groups - 1) + passes - 1
+  int stagger;   // launches between the starts of consecutive groups
+  int n_groups;  // ceil(n_rep / group)
+};
+__host__ __device__ inline int skew_passes(const J1WaveParams& w) {
+  return 4 * (w.n_metro + w.n_or) + (w.with_obs ? 1 : 0);
+}
+__host__ __device__ inline int skew_sub(const J1WaveParams& w, int k) {
+  return k < 4 * w.n_metro ? w.sub_metro : (k < 4 * (w.n_metro + w.n_or) ? w.sub_or : 1);
+}
+__host__ __device__ inline int skew_first_group(const J1SkewParams& sp) {
+  const int lag = sp.t - (skew_passes(sp.w) - 1);
+  const int g = lag <= 0 ? 0 : (lag + sp.stagger - 1) / sp.stagger;
+  return g;
+}
+__host__ __device__ inline int skew_last_group(const J1SkewParams& sp) {
+  const int g = sp.t / sp.stagger;
+  return g < sp.n_groups - 1 ? g : sp.n_groups - 1;
+}
+// Items (CTAs) of launch sp.t.
+int j1_skew_items(const J1SkewParams& sp);
+cudaError_t launch_j1_skew(const J1SkewParams& sp, int forms, cudaStream_t st);
 // Dependency half-width in chunks for lattice size L.
 int j1_wave_dep(int L);
 

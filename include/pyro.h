@@ -86,8 +86,12 @@ int pyro_neighbour_table(int site, int* out120);
  * the chunks that hold its neighbours (per-chunk counters, released and
  * acquired at GPU scope, every wait bounded; a wait that runs out makes the
  * next pyro_synchronize return PYRO_ERR_TIMEOUT). PYRO_OPT_J1_SITE_MODE
- * chooses its pass forms. Calls other than pyro_cycle use the per-pass
- * kernels. PYRO_OPT_CLUSTER_SIZE: CTAs per cluster (2, 4, 8, 16; the
+ * chooses its pass forms. 3 runs them as skewed launches: replica group g
+ * (PYRO_OPT_REPLICA_GROUP replicas, 0 = 2) runs its pass k in launch
+ * s g + k, with s chosen so that about PYRO_OPT_CHAINS groups are in flight
+ * in every launch; a launch's items belong to different replicas and need
+ * no synchronisation, and its groups' spins stay in L2. Calls other than
+ * pyro_cycle use the per-pass kernels. PYRO_OPT_CLUSTER_SIZE: CTAs per cluster (2, 4, 8, 16; the
  * context falls back to the largest size that can be resident).
  * Identical results in every mode. */
 #define PYRO_OPT_CYCLE_KERNEL 2
@@ -106,7 +110,8 @@ int pyro_neighbour_table(int site, int* out120);
  * replicas in every pass), keeping a group's spins in L2. Identical results. */
 #define PYRO_OPT_REPLICA_GROUP 6
 /* PYRO_OPT_CHAINS: 1..8 concurrent streams (parallel branches of the cycle
- * graph) the replica groups are dealt to. Identical results. */
+ * graph) the replica groups are dealt to; with PYRO_OPT_CYCLE_KERNEL 3, the
+ * replica groups in flight in one launch. Identical results. */
 #define PYRO_OPT_CHAINS 7
 /* PYRO_OPT_GROUP_MB: run the generic (J2/J3) colour passes over groups of
  * replicas of about this many MB, all sweeps of a group before the next,

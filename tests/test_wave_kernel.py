@@ -121,3 +121,35 @@ def test_wave_wait_that_runs_out_reports_timeout_and_the_context_recovers(tmp_pa
     o.cycle(1, 2, True, 3)
     assert np.array_equal(e.get_spins(), o.get_spins())
     assert np.array_equal(e.permutation(), o.permutation())
+
+
+@pytest.mark.parametrize("L,R,forms,group,in_flight,n_metro,n_or", [
+    (12, 6, 3, 2, 4, 1, 4),    # the benchmark's cycle shape, partial last chunk
+    (16, 5, 1, 2, 2, 1, 3),    # cell-form over-relaxation, uneven last group
+    (8, 7, 0, 3, 8, 2, 1),     # both cell form, more groups in flight than passes allow
+    (20, 4, 3, 1, 3, 3, 0),    # Metropolis only, groups of one replica
+    (9, 3, 2, 4, 2, 0, 2),     # over-relaxation only, one group
+])
+def test_skewed_launches_bit_exact(L, R, forms, group, in_flight, n_metro, n_or):
+    temps = geometric_ladder(0.05, 1.5, R)
+    e, o = pair([System(L=L, temperatures=temps)], renorm_every=3)
+    e.set_option(e.OPT_CYCLE_KERNEL, 3)
+    e.set_option(e.OPT_J1_SITE_MODE, forms)
+    e.set_option(e.OPT_REPLICA_GROUP, group)
+    e.set_option(e.OPT_CHAINS, in_flight)
+    e.init_random()
+    o.init_random()
+    cones = np.linspace(-0.6, 0.8, R).astype(np.float32)
+    e.set_cone(cones)
+    o.set_cone(cones)
+    e.enable_history(8)
+    e.cycle(n_metro, n_or, True, 4)
+    h = o.cycle(n_metro, n_or, True, 4, record=True)
+    assert np.array_equal(e.get_spins(), o.get_spins())
+    assert np.array_equal(e.permutation(), o.permutation())
+    assert np.array_equal(e.acceptance()[0], o.acceptance()[0])
+    np.testing.assert_allclose(e.history(), h, rtol=1e-12, atol=1e-9)
+    E0, M0 = e.last_observables()
+    E1, M1 = o.observables()
+    np.testing.assert_allclose(E0, E1, rtol=1e-12, atol=1e-9)
+    np.testing.assert_allclose(M0, M1, rtol=1e-12, atol=1e-9)
