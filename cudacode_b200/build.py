@@ -46,7 +46,7 @@ def _newer(target: str, sources: list[str]) -> bool:
 
 
 def _deps() -> list[str]:
-    out = []
+    out = [os.path.abspath(__file__)]  # flag changes rebuild too
     for d in (CSRC, os.path.join(ROOT, "include")):
         for f in os.listdir(d):
             if f.endswith((".cu", ".cuh", ".h", ".cpp", ".hpp")):
