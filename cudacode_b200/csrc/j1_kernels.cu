@@ -696,7 +696,7 @@ __device__ __forceinline__ void release_add_gpu(unsigned int* p, unsigned int v)
 
 // One work item: colour B of pass k on chunk q of replica rep, sub-item f
 // (FCC corner in the site form, unused in the cell form).
-template <int B, bool kExch, bool kMetroSite, bool kOrSite>
+template <int B, bool kExch, bool kMetroSite, bool kOrSite, int kLd = kLdCoherent>
 __device__ __forceinline__ void wave_item(const J1WaveParams& w, int rep, int q, int f,
                                           bool metro, unsigned long long sweep_add) {
   const J1PassParams& p = w.pass;
@@ -712,14 +712,14 @@ __device__ __forceinline__ void wave_item(const J1WaveParams& w, int rep, int q,
   if (cell < p.L3) {
     if (metro) {
       if (kMetroSite)
-        acc = site_item<B, true, kExch, kLdCoherent>(p, rep, f, cell, beta, cosmax, sweep_add);
+        acc = site_item<B, true, kExch, kLd>(p, rep, f, cell, beta, cosmax, sweep_add);
       else
-        acc = cell_pass<B, true, kExch, kLdCoherent>(p, rep, cell, beta, cosmax, sweep_add);
+        acc = cell_pass<B, true, kExch, kLd>(p, rep, cell, beta, cosmax, sweep_add);
     } else {
       if (kOrSite)
-        site_item<B, false, kExch, kLdCoherent>(p, rep, f, cell, beta, cosmax, sweep_add);
+        site_item<B, false, kExch, kLd>(p, rep, f, cell, beta, cosmax, sweep_add);
       else
-        cell_pass<B, false, kExch, kLdCoherent>(p, rep, cell, beta, cosmax, sweep_add);
+        cell_pass<B, false, kExch, kLd>(p, rep, cell, beta, cosmax, sweep_add);
     }
   }
   if (metro) block_accept(p, t, acc);
@@ -843,13 +843,23 @@ __global__ void __launch_bounds__(kJ1Threads, kForms == 3 ? 4 : 2)
     release_add_gpu(w.progress + (long long)rep * nq + q, 1u);
 }
 
+// Resident CTAs per SM of the skewed launches with both passes in the site
+// form (their register bound).
+#ifndef PYRO_SKEW_SITE_BLOCKS
+#define PYRO_SKEW_SITE_BLOCKS 4
+#endif
+constexpr int kSkewSiteBlocks = PYRO_SKEW_SITE_BLOCKS;
+
 // Skewed launches (see J1SkewParams): launch t runs pass t - stagger g of
 // every replica group g that has one, all of them independent (different
 // replicas); consecutive passes of a group are ordered by the stream. The
 // CTA's item comes from blockIdx.x across the groups of the launch, group by
-// group, then (replica, chunk, sub-item) as in the work-queue kernel.
+// group, then (replica, chunk, sub-item) as in the work-queue kernel. Within a
+// launch nothing that an item reads is written (its own pass writes one
+// colour, which no item of the launch reads), so the loads take the
+// read-only path like the per-pass kernels'.
 template <bool kExch, int kForms>
-__global__ void __launch_bounds__(kJ1Threads, kForms == 3 ? 4 : 2)
+__global__ void __launch_bounds__(kJ1Threads, kForms == 3 ? kSkewSiteBlocks : 2)
     j1_skew_kernel(const J1SkewParams sp) {
   constexpr bool kMetroSite = (kForms & 1) != 0, kOrSite = (kForms & 2) != 0;
   pass_prologue();
@@ -890,10 +900,10 @@ __global__ void __launch_bounds__(kJ1Threads, kForms == 3 ? 4 : 2)
   const bool metro = sweep_idx < w.n_metro;
   const unsigned long long sweep_add = (unsigned long long)sweep_idx;
   switch (k & 3) {
-    case 0: wave_item<0, kExch, kMetroSite, kOrSite>(w, rep, q, f, metro, sweep_add); break;
-    case 1: wave_item<1, kExch, kMetroSite, kOrSite>(w, rep, q, f, metro, sweep_add); break;
-    case 2: wave_item<2, kExch, kMetroSite, kOrSite>(w, rep, q, f, metro, sweep_add); break;
-    default: wave_item<3, kExch, kMetroSite, kOrSite>(w, rep, q, f, metro, sweep_add); break;
+    case 0: wave_item<0, kExch, kMetroSite, kOrSite, kLdNc>(w, rep, q, f, metro, sweep_add); break;
+    case 1: wave_item<1, kExch, kMetroSite, kOrSite, kLdNc>(w, rep, q, f, metro, sweep_add); break;
+    case 2: wave_item<2, kExch, kMetroSite, kOrSite, kLdNc>(w, rep, q, f, metro, sweep_add); break;
+    default: wave_item<3, kExch, kMetroSite, kOrSite, kLdNc>(w, rep, q, f, metro, sweep_add); break;
   }
 }
 }  // namespace
