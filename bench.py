@@ -722,18 +722,25 @@ def learned_leg(cycles: int = 60000, warmup: int = 2000) -> dict:
                        "autotune_choice_plain": choice}}
 
 
-WAVE_PROFILE = os.path.join(ROOT, "profiles", "wave_kernel_L32_R64.md")
+STEP_PROFILE = os.path.join(ROOT, "profiles", "pt_step_L32_R64_instructions.md")
 
 
-def profiled_instructions():
-    """Warp instructions per spin update of the work-queue cycle kernel, from
-    its committed ncu summary (line 'warp_instructions_per_update: X')."""
+def profiled_instructions(kernel_desc: dict):
+    """Warp instructions per spin update of one step of the timed schedule,
+    from the committed ncu summary of that schedule (lines 'schedule: k=v
+    ...' and 'warp_instructions_per_update: X'); None when the summary is of
+    another schedule."""
     try:
-        with open(WAVE_PROFILE) as f:
+        sched, ipu = None, None
+        with open(STEP_PROFILE) as f:
             for line in f:
-                if line.startswith("warp_instructions_per_update:"):
-                    return float(line.split(":", 1)[1])
-    except OSError:
+                if line.startswith("schedule:"):
+                    sched = dict(kv.split("=") for kv in line.split(":", 1)[1].split())
+                elif line.startswith("warp_instructions_per_update:"):
+                    ipu = float(line.split(":", 1)[1])
+        if sched and ipu and all(str(kernel_desc.get(k)) == v for k, v in sched.items()):
+            return ipu
+    except (OSError, ValueError):
         pass
     return None
 
@@ -946,7 +953,7 @@ def main():
     step_updates = R_PER_GPU * 16 * L ** 3 * (N_METRO + N_OR)  # per GPU
     achieved = step_updates * sched_bytes / (step_ms * 1e-3) / 1e9
     wave = kernel_desc["cycle_kernel"] == 2
-    ipu = profiled_instructions() if (wave and (L, R_PER_GPU) == (32, 64)) else None
+    ipu = profiled_instructions(kernel_desc) if (L, R_PER_GPU) == (32, 64) else None
     props = torch.cuda.get_device_properties(local)
     issue = None
     if ipu and clocks.get("sm_mhz"):
@@ -955,7 +962,8 @@ def main():
                  "warp_instructions_per_update": ipu,
                  "frac": ipu * step_updates / issue_slots,
                  "sm_mhz": clocks["sm_mhz"], "sms": props.multi_processor_count,
-                 "source": "profiles/wave_kernel_L32_R64.md (ncu smsp__inst_executed.sum)"}
+                 "source": "profiles/pt_step_L32_R64_instructions.md (ncu "
+                           "smsp__inst_executed.sum over one step's launches)"}
 
     # The streaming form of the same passes, for comparison: one launch per
     # colour pass over all replicas, 80 algorithmic bytes per update.
