@@ -43,7 +43,9 @@ class EngineBackend:
 
     The engine queues on its own stream and the collective on torch's
     current stream; each hand-over makes the receiving stream wait for the
-    other (no host synchronisation)."""
+    other (no host synchronisation). On a CPU device (a host stand-in for
+    the engine, used by the tests) the calls are synchronous and there is
+    nothing to order."""
 
     def __init__(self, engine: Engine, device: torch.device):
         self.engine = engine
@@ -63,11 +65,13 @@ class EngineBackend:
     def local_energies(self) -> torch.Tensor:
         # the cycle computed them at its end: copy, do not recompute
         self.engine.last_observables_device(self._e.data_ptr())
-        torch.cuda.current_stream(self.device).wait_stream(self._engine_stream())
+        if self.device.type == "cuda":
+            torch.cuda.current_stream(self.device).wait_stream(self._engine_stream())
         return self._e
 
     def swap_global(self, all_energies: torch.Tensor, parity: int) -> None:
-        self._engine_stream().wait_stream(torch.cuda.current_stream(self.device))
+        if self.device.type == "cuda":
+            self._engine_stream().wait_stream(torch.cuda.current_stream(self.device))
         self.engine.pt_swap_global(all_energies.data_ptr(), parity)
 
 

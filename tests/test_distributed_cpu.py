@@ -6,6 +6,7 @@ oracle standing in for the engine: the two half-ladder ranks must reproduce
 the unsharded run of the whole ladder bit for bit, spins and temperature
 labels. A planted mistake (one rank contributing its energies in the wrong
 replica order) must break it."""
+import ctypes
 import os
 import socket
 
@@ -42,13 +43,43 @@ class OracleBackend:
         self.o.pt_swap_global(all_energies.numpy(), parity)
 
 
+class FakeEngine:
+    """Host stand-in for cudacode_b200.engine.Engine with exactly the calls
+    that EngineBackend makes (energies passed by pointer, as the engine's
+    device calls take them), backed by the oracle (test infrastructure)."""
+
+    def __init__(self, oracle, system, reversed_energies=False):
+        self.o = oracle
+        self.systems = [system]
+        self.reversed_energies = reversed_energies
+        self._e = None
+
+    def stream_handle(self):
+        return 0
+
+    def cycle(self, n_metro, n_or, do_swap, n_cycles):
+        assert not do_swap and n_cycles == 1
+        self.o.metropolis_sweep(n_metro)
+        self.o.overrelax_sweep(n_or)
+        self._e = np.ascontiguousarray(self.o.observables()[0])  # the cycle's own energies
+
+    def last_observables_device(self, e_ptr, m_ptr=0, system=0):
+        e = self._e[::-1].copy() if self.reversed_energies else self._e  # planted mistake
+        ctypes.memmove(e_ptr, e.ctypes.data, e.nbytes)
+
+    def pt_swap_global(self, e_all_ptr, parity=-1, system=0):
+        n = len(self.systems[0].temperatures)
+        e = np.ctypeslib.as_array((ctypes.c_double * n).from_address(e_all_ptr)).copy()
+        self.o.pt_swap_global(e, parity)
+
+
 def free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
         return s.getsockname()[1]
 
 
-def run_rank(rank, world, port, out_dir, scrambled):
+def run_rank(rank, world, port, out_dir, scrambled, engine_backend=False):
     from oracle.binding import Oracle
 
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
@@ -59,7 +90,14 @@ def run_rank(rank, world, port, out_dir, scrambled):
                threads=1)
     o.init_random()
     o.set_cone(np.linspace(-0.5, 0.8, N_T).astype(np.float32))
-    pt = ShardedPT(OracleBackend(o, scrambled=scrambled and rank == 1), N_T)
+    if engine_backend:  # the engine's backend class over a host stand-in of the engine
+        from cudacode_b200.distributed import EngineBackend
+        system = System(L=L, temperatures=temps, n_replicas=cnt, replica_offset=off)
+        backend = EngineBackend(FakeEngine(o, system, reversed_energies=scrambled and rank == 1),
+                                torch.device("cpu"))
+    else:
+        backend = OracleBackend(o, scrambled=scrambled and rank == 1)
+    pt = ShardedPT(backend, N_T)
     for _ in range(CYCLES):
         pt.cycle(1, 2)
     np.save(os.path.join(out_dir, f"spins{rank}.npy"), o.get_spins())
@@ -83,10 +121,11 @@ def reference_run():
     return o.get_spins(), o.permutation()
 
 
-def launch(tmp_path, scrambled):
+def launch(tmp_path, scrambled, engine_backend=False):
     ctx = mp.get_context("spawn")
     port = free_port()
-    procs = [ctx.Process(target=run_rank, args=(r, 2, port, str(tmp_path), scrambled)) for r in range(2)]
+    procs = [ctx.Process(target=run_rank, args=(r, 2, port, str(tmp_path), scrambled,
+                                                engine_backend)) for r in range(2)]
     for p in procs:
         p.start()
     for p in procs:
@@ -116,4 +155,18 @@ def test_two_ranks_reproduce_the_unsharded_ladder(tmp_path):
 def test_planted_energy_order_mistake_is_detected(tmp_path):
     spins, perms = launch(tmp_path, scrambled=True)
     ref_spins, ref_perm = reference_run()
+    assert not (np.array_equal(perms[0], ref_perm) and np.array_equal(spins, ref_spins))
+
+
+def test_engine_backend_ordering_over_two_ranks(tmp_path):
+    """EngineBackend (energies of the cycle copied by pointer, gathered,
+    handed to the global exchange) over two gloo ranks, with a host stand-in
+    for the engine: the unsharded ladder bit for bit; a rank that hands over
+    its energies in the wrong order is detected."""
+    spins, perms = launch(tmp_path, scrambled=False, engine_backend=True)
+    ref_spins, ref_perm = reference_run()
+    assert np.array_equal(perms[0], perms[1])
+    assert np.array_equal(perms[0], ref_perm)
+    assert np.array_equal(spins, ref_spins)
+    spins, perms = launch(tmp_path, scrambled=True, engine_backend=True)
     assert not (np.array_equal(perms[0], ref_perm) and np.array_equal(spins, ref_spins))
