@@ -1119,6 +1119,7 @@ int pyro_get_option(pyro_ctx* ctx, int option, int* value) {
 // Times each kernel variant on `cycles` real cycles (they advance the chain:
 // every variant computes the same updates) and keeps the fastest.
 int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen) {
+  NvtxRange nvtx_range("pyro_autotune");
   if (!ctx) return PYRO_ERR_ARG;
   if (cycles < 1 || n_metro < 0 || n_or < 0 || n_metro + n_or < 1)
     return fail(ctx, PYRO_ERR_ARG, "autotune: need cycles >= 1 and at least one sweep");
@@ -1226,6 +1227,7 @@ int pyro_synchronize(pyro_ctx* ctx) {
 }
 
 int pyro_snapshot(pyro_ctx* ctx) {
+  NvtxRange nvtx_range("pyro_snapshot");
   if (!ctx) return PYRO_ERR_ARG;
   PYRO_CK(cudaSetDevice(ctx->device));
   if (!ctx->snap_stream) {
@@ -1363,6 +1365,7 @@ int pyro_get_spins_device(pyro_ctx* ctx, int system, float* dev_xyzw) {
 }
 
 static int run_sweeps(pyro_ctx* ctx, int n, bool metro) {
+  NvtxRange nvtx_range("pyro_sweeps");
   if (!ctx) return PYRO_ERR_ARG;
   if (n < 0) return fail(ctx, PYRO_ERR_ARG, "n_sweeps must be >= 0");
   if (n == 0) return PYRO_OK;
@@ -1541,6 +1544,7 @@ int pyro_last_observables(pyro_ctx* ctx, int system, double* energy, double* mag
 }
 
 int pyro_observables(pyro_ctx* ctx, int system, double* energy, double* magnetisation3) {
+  NvtxRange nvtx_range("pyro_observables");
   if (!ctx) return PYRO_ERR_ARG;
   if (system < 0 || system >= (int)ctx->sys.size())
     return fail(ctx, PYRO_ERR_ARG, "observables: bad system");
@@ -1751,6 +1755,7 @@ static bool tet_in_groups(const pyro_ctx* ctx) {
 }
 
 static int run_cycles(pyro_ctx* ctx, int n_metro, int n_or, int n_tet, int do_swap, int n_cycles) {
+  NvtxRange nvtx_range("pyro_cycle");
   if (!ctx) return PYRO_ERR_ARG;
   if (n_metro < 0 || n_or < 0 || n_tet < 0 || n_cycles < 0)
     return fail(ctx, PYRO_ERR_ARG, "cycle: counts must be >= 0");
@@ -1881,6 +1886,7 @@ static int grow(pyro_ctx* ctx, double2** p, size_t* cap, size_t n) {
 }
 
 int pyro_structure_factor(pyro_ctx* ctx, int system, int replica, int G, int stride, double* out) {
+  NvtxRange nvtx_range("pyro_structure_factor");
   if (!ctx) return PYRO_ERR_ARG;
   if (system < 0 || system >= (int)ctx->sys.size() || !out)
     return fail(ctx, PYRO_ERR_ARG, "structure_factor: bad system or null pointer");

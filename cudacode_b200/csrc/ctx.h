@@ -8,6 +8,8 @@
 #include <utility>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/pyro.h"
 #include "kernels.cuh"
 #include "lattice.h"
@@ -169,6 +171,15 @@ inline bool j1_only(const SysDev& s) { return s.n_colours == 4 && s.shells == 1 
 inline bool j1_sweepable(const SysDev& s) {
   return s.n_colours == 4 && (j1_only(s) || (s.exch >= 0 && (s.shells & ~1) == 0));
 }
+
+// NVTX range around a C-ABI call (header-only NVTX 3: inert unless a
+// profiler attaches), so timelines show cycles, measurements and training.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 inline int fail(pyro_ctx* c, int code, const std::string& msg) {
   if (c) c->err = msg;

@@ -243,6 +243,7 @@ int pyro_reference_gtensor(double gxy, double gz, double* g36) {
 }
 
 int pyro_sublattice_magnetisation(pyro_ctx* ctx, int system, double* out) {
+  NvtxRange nvtx_range("pyro_sublattice_magnetisation");
   if (!ctx || !out) return PYRO_ERR_ARG;
   if (system < 0 || system >= (int)ctx->sys.size())
     return fail(ctx, PYRO_ERR_ARG, "sublattice_magnetisation: no such system");

@@ -170,6 +170,7 @@ int grow_scratch(pyro_ctx* ctx, size_t need) {
 extern "C" {
 
 int pyro_order_parameters(pyro_ctx* ctx, int system, double* out) {
+  NvtxRange nvtx_range("pyro_order_parameters");
   if (!ctx || !out) return PYRO_ERR_ARG;
   if (system < 0 || system >= (int)ctx->sys.size())
     return fail(ctx, PYRO_ERR_ARG, "order_parameters: no such system");

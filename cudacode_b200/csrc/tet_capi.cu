@@ -346,6 +346,7 @@ int pyro_tet_trace_pass(pyro_ctx* ctx, int system, int corner, int form, float* 
 }
 
 int pyro_tet_sweep(pyro_ctx* ctx, int n_sweeps) {
+  NvtxRange nvtx_range("pyro_tet_sweep");
   int rc = need_tet(ctx);
   if (rc) return rc;
   if (n_sweeps < 0) return fail(ctx, PYRO_ERR_ARG, "tet_sweep: n_sweeps must be >= 0");
@@ -442,6 +443,7 @@ int pyro_tet_samples(pyro_ctx* ctx, float* features, float* targets, long long m
 }
 
 int pyro_tet_train(pyro_ctx* ctx, int steps, int batch, float lr, double* mean_loss) {
+  NvtxRange nvtx_range("pyro_tet_train");
   int rc = need_tet(ctx);
   if (rc) return rc;
   TetState* t = ctx->tet;
