@@ -916,6 +916,7 @@ int pyro_create(const pyro_config* cfg, pyro_ctx** out) {
     s.n_rep = d.n_replicas;
     s.rep_global = d.replica_offset;
     s.rep_key = temp_base + d.replica_offset;
+    s.swap_key = i;
     s.rep_ctx_base = rep_ctx;
     s.temp_base = temp_base;
     s.n_temp = d.n_temperatures;
@@ -1224,6 +1225,20 @@ int pyro_synchronize(pyro_ctx* ctx) {
   PYRO_CK(cudaSetDevice(ctx->device));
   PYRO_CK(cudaStreamSynchronize(ctx->stream));
   return check_wave_status(ctx);
+}
+
+int pyro_set_system_keys(pyro_ctx* ctx, int system, int key_base, int swap_key) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (system < 0 || system >= (int)ctx->sys.size() || key_base < 0 || swap_key < 0)
+    return fail(ctx, PYRO_ERR_ARG, "set_system_keys: bad system or negative key");
+  PYRO_CK(cudaSetDevice(ctx->device));
+  PYRO_CK(cudaStreamSynchronize(ctx->stream));
+  SysDev& s = ctx->sys[system];
+  s.rep_key = key_base + s.rep_global;
+  s.swap_key = swap_key;
+  PYRO_CK(cudaMemcpy(ctx->d_sys, ctx->sys.data(), sizeof(SysDev) * ctx->sys.size(),
+                     cudaMemcpyHostToDevice));
+  return rebuild_schedule(ctx);  // the captured cycles hold the old keys
 }
 
 int pyro_snapshot(pyro_ctx* ctx) {

@@ -373,7 +373,7 @@ __global__ void exchange_kernel(const ExchangeParams p) {
       const double ea = p.energy_is_global ? p.energy[ga] : p.energy[sd.rep_ctx_base + ga];
       const double eb = p.energy_is_global ? p.energy[gb] : p.energy[sd.rep_ctx_base + gb];
       uint32_t r[4];
-      pyro_philox((uint32_t)t, (uint32_t)count, (uint32_t)si, PYRO_PURPOSE_SWAP, p.seed_lo,
+      pyro_philox((uint32_t)t, (uint32_t)count, (uint32_t)sd.swap_key, PYRO_PURPOSE_SWAP, p.seed_lo,
                   p.seed_hi, r);
       const double u = pyro_uniform53(r[0], r[1]);
       const int acc =

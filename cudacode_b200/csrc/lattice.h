@@ -145,6 +145,7 @@ struct SysDev {
   int n_rep;           // replicas held
   int rep_global;      // global replica id of replica 0 within the system's ladder
   int rep_key;         // Philox replica word of replica 0 (unique across systems)
+  int swap_key;        // Philox word of the system's exchanges (its index, unique)
   int rep_ctx_base;    // index of replica 0 in the context-wide per-replica arrays
   int temp_base;       // offset of this system's temperature arrays
   int n_temp;          // ladder size

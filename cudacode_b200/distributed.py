@@ -17,6 +17,12 @@ TrySwapingTemperatures MonteCarlo.cu:105-172).
 The driver only needs an object with ``sweeps(n_metro, n_or)``,
 ``local_energies() -> tensor`` and ``swap_global(all_energies, parity)``;
 :class:`EngineBackend` binds it to the CUDA engine.
+
+Many independent systems (the batched configuration) shard whole systems
+instead: :func:`deal_systems` gives each rank a set of systems of about equal
+work, every rank runs its own engine with its own exchanges and no
+collective, and :func:`gather_system_results` collects per-system results on
+every rank at the end, in the global system order.
 """
 from __future__ import annotations
 
@@ -108,3 +114,61 @@ def make_engine_shard(L: int, temperatures, world: int, rank: int, seed: int, de
     offset, count = shard(len(temperatures), world, rank)
     return Engine([System(L=L, temperatures=list(temperatures), n_replicas=count,
                           replica_offset=offset, **couplings)], seed=seed, device=device)
+
+
+def deal_systems(sizes, world: int, rank: int) -> list[int]:
+    """Indices of the systems held by `rank`: greedy by decreasing size
+    (sites x replicas) onto the least loaded rank, ties to the lowest rank,
+    so the ranks' work differs by at most one system. The same on every rank."""
+    if len(sizes) < world:
+        raise ValueError(f"{len(sizes)} systems cannot be spread over {world} ranks")
+    load = [0] * world
+    owner = [0] * len(sizes)
+    for i in sorted(range(len(sizes)), key=lambda i: (-sizes[i], i)):
+        r = min(range(world), key=lambda k: (load[k], k))
+        owner[i] = r
+        load[r] += sizes[i]
+    return [i for i in range(len(sizes)) if owner[i] == rank]
+
+
+def gather_system_results(local: dict, n_systems: int, group=None) -> list:
+    """{global system index: result} of every rank -> list over all systems
+    (on every rank; one object gather at the end of a run)."""
+    if not dist.is_initialized():
+        out = [None] * n_systems
+        for i, v in local.items():
+            out[i] = v
+        return out
+    parts = [None] * dist.get_world_size(group)
+    dist.all_gather_object(parts, local, group=group)
+    out = [None] * n_systems
+    for part in parts:
+        for i, v in part.items():
+            out[i] = v
+    return out
+
+
+def system_keys(systems) -> list[tuple[int, int]]:
+    """(key_base, swap_key) of every system in the full set: the Philox keys
+    each has in a context holding all of them."""
+    keys, base = [], 0
+    for i, sy in enumerate(systems):
+        keys.append((base, i))
+        base += len(sy.temperatures)
+    return keys
+
+
+def make_system_shard(systems, world: int, rank: int, seed: int, device: int = 0,
+                      factory=None, **kwargs):
+    """This rank's share of independent systems (deal_systems) in one context
+    whose Philox keys are those of the full set, so each system's chain is
+    the one an unsharded run gives. Returns (context, global indices).
+    `factory` builds the context (default: the CUDA engine)."""
+    sizes = [sy.n_sites * sy.replicas() for sy in systems]
+    local = deal_systems(sizes, world, rank)
+    make = factory or (lambda sys_list: Engine(sys_list, seed=seed, device=device, **kwargs))
+    ctx = make([systems[i] for i in local])
+    keys = system_keys(systems)
+    for j, gi in enumerate(local):
+        ctx.set_system_keys(j, *keys[gi])
+    return ctx, local

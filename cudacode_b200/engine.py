@@ -88,6 +88,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "pyro_get_stream": (P, [P]),
         "pyro_synchronize": (i, [P]),
         "pyro_snapshot": (i, [P]),
+        "pyro_set_system_keys": (i, [P, i, i, i]),
         "pyro_system_info": (i, [P, i, pi, pi, pi, pi]),
         "pyro_init_random": (i, [P]),
         "pyro_set_spins": (i, [P, i, pf]),
@@ -317,6 +318,10 @@ class Engine:
 
     def synchronize(self) -> None:
         self._ck(self.lib.pyro_synchronize(self.ctx))
+
+    def set_system_keys(self, system: int, key_base: int, swap_key: int) -> None:
+        """Philox keys of a system (pyro_set_system_keys)."""
+        self._ck(self.lib.pyro_set_system_keys(self.ctx, system, key_base, swap_key))
 
     def snapshot(self) -> None:
         """Queues a measurement snapshot (pyro_snapshot)."""

@@ -174,6 +174,15 @@ void* pyro_get_stream(const pyro_ctx* ctx);
 /* Wait for all work queued by the context. Replaces SynchronizeJobs
  * (MonteCarlo.cu:230-245). */
 int pyro_synchronize(pyro_ctx* ctx);
+/* Philox keys of one system: its replica r draws with the replica word
+ * key_base + replica_offset + r and its exchanges with the word swap_key.
+ * By default key_base is the number of temperatures of the systems before it
+ * in the context and swap_key its index, so that no two systems share a
+ * stream; a context holding a subset of a larger set of independent systems
+ * (one rank's share, see cudacode_b200/distributed.py) sets each system's
+ * keys to those it has in the full set and reproduces its chain bit for
+ * bit. Synchronises the context stream; drops the captured cycles. */
+int pyro_set_system_keys(pyro_ctx* ctx, int system, int key_base, int swap_key);
 /* Measurement snapshot. Replaces ExtractConfigurationsFromMonteCarlo
  * (Pyrochlore.cu:1608-1617), which copies the working spins into a
  * measurement buffer so that the next Monte Carlo block runs while the

@@ -57,6 +57,7 @@ def load() -> C.CDLL:
         "orc_mlp_forward": (None, [pf, pf, i, pd]),
         "orc_mlp_gradient": (None, [pf, pf, pf, i, pd, pd]),
         "orc_tet_features": (None, [P, i, i, i, pf, pf]),
+        "orc_set_system_keys": (None, [P, i, i, i]),
         "orc_tet_move_check": (None, [pf, i, pi, pi, i, i, C.c_uint64, C.c_uint64, d, i, pd]),
         "orc_neighbours": (None, [i, pi]),
         "orc_philox": (None, [pu32, pu32, pu32]),
@@ -116,6 +117,9 @@ class Oracle:
 
     def init_random(self):
         self.lib.orc_init_random(self.h)
+
+    def set_system_keys(self, system, key_base, swap_key):
+        self.lib.orc_set_system_keys(self.h, system, key_base, swap_key)
 
     def get_spins(self, system=0):
         out = np.empty(self.spin_shape(system), dtype=np.float32)

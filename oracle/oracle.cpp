@@ -120,6 +120,7 @@ std::array<std::array<Nbr, 30>, 16> build_geometry() {
 
 struct Sys {
   int L, L3, R, off, nT, n_colours, temp_base, rep_key, shells;
+  int swap_key;  // Philox word of the system's exchanges
   double J[4];
   bool exch = false;  // bond matrices replace the isotropic J1 shell
   float A[16][9] = {}, f[4][3] = {};
@@ -417,7 +418,7 @@ int exchange(Oracle& o, int si, const double* E_global, int parity) {
   for (int t = parity; t + 1 < S.nT; t += 2) {
     const int ga = o.rep_of_temp[S.temp_base + t], gb = o.rep_of_temp[S.temp_base + t + 1];
     uint32_t r[4];
-    pyro_philox((uint32_t)t, (uint32_t)count, (uint32_t)si, PYRO_PURPOSE_SWAP,
+    pyro_philox((uint32_t)t, (uint32_t)count, (uint32_t)S.swap_key, PYRO_PURPOSE_SWAP,
                 (uint32_t)(o.seed & 0xffffffffu), (uint32_t)(o.seed >> 32), r);
     const double u = pyro_uniform53(r[0], r[1]);
     const int acc = pyro_swap_accept(1.0 / S.T[t], 1.0 / S.T[t + 1], E_global[ga], E_global[gb], u);
@@ -464,6 +465,7 @@ void* orc_create(int n_sys, const int* L, const int* n_rep, const int* rep_off, 
     S.T.assign(temps_concat + tb, temps_concat + tb + S.nT);
     S.temp_base = tb;
     S.rep_key = tb + S.off;
+    S.swap_key = i;
     S.spin_off = spin_off;
     spin_off += (size_t)S.R * 16 * S.L3;
     for (int t = 0; t < S.nT; ++t) {
@@ -485,6 +487,13 @@ void* orc_create(int n_sys, const int* L, const int* n_rep, const int* rep_off, 
 }
 
 void orc_destroy(void* p) { delete (Oracle*)p; }
+
+// The engine's pyro_set_system_keys.
+void orc_set_system_keys(void* p, int si, int key_base, int swap_key) {
+  Sys& S = ((Oracle*)p)->sys[si];
+  S.rep_key = key_base + S.off;
+  S.swap_key = swap_key;
+}
 
 int orc_set_threads(int n) {
   if (n > 0) omp_set_num_threads(n);

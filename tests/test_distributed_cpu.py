@@ -170,3 +170,68 @@ def test_engine_backend_ordering_over_two_ranks(tmp_path):
     assert np.array_equal(spins, ref_spins)
     spins, perms = launch(tmp_path, scrambled=True, engine_backend=True)
     assert not (np.array_equal(perms[0], ref_perm) and np.array_equal(spins, ref_spins))
+
+
+BATCH = [(3, 4, 0.0), (4, 3, 0.05), (3, 2, -0.04), (5, 2, 0.0), (4, 5, 0.02)]  # L, temps, J2
+
+
+def batch_systems():
+    return [System(L=L, temperatures=geometric_ladder(0.1, 1.5, n), J2=j2)
+            for L, n, j2 in BATCH]
+
+
+def run_system_rank(rank, world, port, out_dir):
+    from cudacode_b200.distributed import gather_system_results, make_system_shard
+    from oracle.binding import Oracle
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    systems = batch_systems()
+    o, local = make_system_shard(systems, world, rank, seed=SEED,
+                                 factory=lambda s: Oracle(s, seed=SEED, threads=1))
+    o.init_random()
+    o.cycle(1, 2, True, CYCLES)
+    mine = {gi: (o.get_spins(j), o.permutation(j)) for j, gi in enumerate(local)}
+    allres = gather_system_results(mine, len(systems))
+    if rank == 0:
+        np.save(os.path.join(out_dir, "batch.npy"),
+                np.array([np.concatenate([r[0].ravel(), r[1].astype(np.float32)])
+                          for r in allres], dtype=object), allow_pickle=True)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_deal_systems_balances_and_covers():
+    from cudacode_b200.distributed import deal_systems
+    sizes = [5, 1, 4, 4, 2, 7, 3]
+    parts = [deal_systems(sizes, 3, r) for r in range(3)]
+    assert sorted(sum(parts, [])) == list(range(7))
+    loads = [sum(sizes[i] for i in p) for p in parts]
+    assert max(loads) - min(loads) <= max(sizes)
+    with pytest.raises(ValueError):
+        deal_systems([1], 2, 0)
+
+
+def test_systems_dealt_over_two_ranks_reproduce_the_whole_batch(tmp_path):
+    """Independent systems shared out over two gloo ranks, each rank one
+    context with the full set's Philox keys and no collective until the
+    final gather: every system's spins and permutation equal the
+    single-context run's bit for bit."""
+    from oracle.binding import Oracle
+
+    ctx = mp.get_context("spawn")
+    port = free_port()
+    procs = [ctx.Process(target=run_system_rank, args=(r, 2, port, str(tmp_path)))
+             for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=180)
+        assert p.exitcode == 0
+    got = np.load(tmp_path / "batch.npy", allow_pickle=True)
+    o = Oracle(batch_systems(), seed=SEED, threads=1)
+    o.init_random()
+    o.cycle(1, 2, True, CYCLES)
+    for i in range(len(BATCH)):
+        want = np.concatenate([o.get_spins(i).ravel(), o.permutation(i).astype(np.float32)])
+        assert np.array_equal(got[i], want), i

@@ -533,3 +533,24 @@ def test_spins_in_the_reference_layout():
     assert np.all(back[..., 3] == 0.0)
     with pytest.raises(ValueError):
         e.set_spins_planar(v[:, :2])
+
+
+def test_a_subset_of_systems_with_the_full_sets_keys_reproduces_their_chains():
+    """One rank's share of independent systems: a context holding systems 1
+    and 3 of a batch, with the Philox keys they have in the whole batch
+    (pyro_set_system_keys), reproduces their chains bit for bit."""
+    from cudacode_b200.distributed import system_keys
+    systems = [System(L=L, temperatures=geometric_ladder(0.1, 1.5, n), J2=j2)
+               for L, n, j2 in [(4, 3, 0.0), (5, 4, 0.05), (6, 2, 0.0), (8, 3, 0.0)]]
+    full = Engine(systems, seed=31)
+    full.init_random()
+    full.cycle(1, 3, True, 5)
+    keys = system_keys(systems)
+    part = Engine([systems[1], systems[3]], seed=31)
+    for j, gi in enumerate((1, 3)):
+        part.set_system_keys(j, *keys[gi])
+    part.init_random()
+    part.cycle(1, 3, True, 5)
+    for j, gi in enumerate((1, 3)):
+        assert np.array_equal(part.get_spins(j), full.get_spins(gi)), gi
+        assert np.array_equal(part.permutation(j), full.permutation(gi)), gi
