@@ -82,9 +82,15 @@ def test_cli_anisotropic_model_matches_python_engine(tmp_path):
 
 
 @pytest.mark.gpu
-def test_cli_statistics_files_match_python_engine(tmp_path):
-    from cudacode_b200.engine import (Engine, System, geometric_ladder, reference_exchange,
+def test_cli_statistics_files_match_the_oracle(tmp_path):
+    """The statistics files of the CLI's measurement loop (measured from
+    snapshots while the next cycle runs) against the same chain run by the
+    host oracle and measured on the host: the oracle's FP64 energies, order
+    parameters and sublattice sums of its spins (the chains are identical bit
+    for bit, so the files must agree to FP64 rounding)."""
+    from cudacode_b200.engine import (System, geometric_ladder, reference_exchange,
                                       reference_field, reference_gtensor)
+    from oracle.binding import Oracle
 
     args = ["--nx", "3", "--NumberOfTemperatures", "4", "--TMin", "0.2", "--TMax", "2.0",
             "--LogScale", "--OverRelaxation", "1", "--ThermalizationSteps", "5",
@@ -100,7 +106,7 @@ def test_cli_statistics_files_match_python_engine(tmp_path):
     assert (tmp_path / "series.dat.1").exists()
     temps = geometric_ladder(0.2, 2.0, 4)
     J = (-0.09 / 0.29, -0.22 / 0.29, -1.00, 0.0)
-    e = Engine([System(L=3, temperatures=temps, J1=0.0)], seed=5, renorm_every=100)
+    e = Oracle([System(L=3, temperatures=temps, J1=0.0)], seed=5, renorm_every=100)
     e.set_exchange(reference_exchange(*J), reference_field(1.0, 1.0, [1.0, 0.0, 1.0]))
     e.init_random()
     e.tune_cone(0.5, 50, 10, 1)
@@ -113,7 +119,9 @@ def test_cli_statistics_files_match_python_engine(tmp_path):
         E, _ = e.observables()
         perm = e.permutation()  # replica of each temperature
         q = e.order_parameters()[perm]
-        Mg = np.einsum("bik,rbk->ri", g, e.sublattice_magnetisation())[perm]
+        spins = e.get_spins()[..., :3].astype(np.float64)      # [replica][site][cell][xyz]
+        sub = spins.reshape(len(temps), 4, 4, -1, 3).sum(axis=(1, 3))  # site = 4 f + b
+        Mg = np.einsum("bik,rbk->ri", g, sub)[perm]
         rows["E"].append(np.stack([E[perm], E[perm] ** 2], axis=1))
         sq = np.stack([q[:, 0] ** 2, (q[:, 1:3] ** 2).sum(1), (q[:, 3:6] ** 2).sum(1),
                        (q[:, 6:9] ** 2).sum(1), (q[:, 9:12] ** 2).sum(1)], axis=1)

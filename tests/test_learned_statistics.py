@@ -6,8 +6,9 @@ The engine trains its network on configurations of its plain chains, then
 runs parallel-tempering cycles of 1 Metropolis + 1 over-relaxation + 2
 learned sweeps; the oracle runs the plain method (1 Metropolis + 1
 over-relaxation sweep per exchange) with FP64 spins, independently seeded,
-in a host thread at the same time. Energy per site and specific heat at
-T = 0.05 must agree within 3 sigma (errors from the integrated
+in a host thread at the same time. The plain method on the GPU runs the
+same length. Energy per site and specific heat at T = 0.05 of both GPU
+chains must agree with the oracle's within 3 sigma (errors from the integrated
 autocorrelation time for E, from a 20-block jackknife for C); the deviation
 in sigma is printed for comparison with the 2 sigma that the learned method
 is required to meet on average."""
@@ -64,6 +65,14 @@ def test_learned_chain_agrees_with_the_fp64_oracle_at_L16_T005():
     e.cycle_tet(1, 1, 2, True, N_MEAS)
     h_gpu = e.history()[:, 0]
     acc, prop = e.tet_acceptance()
+    # the plain method on the GPU (1 M + 1 OR per exchange), same length
+    pl = Engine([s], seed=503)
+    pl.init_random()
+    pl.tune_cone(0.5, 10, 5, 1)
+    pl.cycle(1, 1, True, N_BURN)
+    pl.enable_history(N_MEAS)
+    pl.cycle(1, 1, True, N_MEAS)
+    h_plain = pl.history()[:, 0]
     th.join()
     h_host = host["h"]
     m1, s1 = stats.mean_error(h_gpu / n)
@@ -75,6 +84,14 @@ def test_learned_chain_agrees_with_the_fp64_oracle_at_L16_T005():
     print(f"T=0.05: E/N learned {m1:.6f}+-{s1:.6f}, FP64 oracle {m2:.6f}+-{s2:.6f} "
           f"({dev_e:.2f} sigma); C/N learned {c1:.4f}+-{u1:.4f}, oracle {c2:.4f}+-{u2:.4f} "
           f"({dev_c:.2f} sigma); learned acceptance {acc[0] / prop[0]:.3f}")
+    m3, s3 = stats.mean_error(h_plain / n)
+    c3, u3 = c_and_error(h_plain, temps[0], n)
+    dev_pe = abs(m3 - m2) / np.hypot(s3, s2)
+    dev_pc = abs(c3 - c2) / np.hypot(u3, u2)
+    print(f"T=0.05: plain GPU chain E/N {m3:.6f}+-{s3:.6f} ({dev_pe:.2f} sigma), "
+          f"C/N {c3:.4f}+-{u3:.4f} ({dev_pc:.2f} sigma) against the FP64 oracle")
     assert acc[0] > 0
     assert dev_e < 3.0, (m1, s1, m2, s2)
     assert dev_c < 3.0, (c1, u1, c2, u2)
+    assert dev_pe < 3.0, (m3, s3, m2, s2)
+    assert dev_pc < 3.0, (c3, u3, c2, u2)
