@@ -174,7 +174,7 @@ class ClockSampler:
 
 
 KERNEL_OPTIONS = ("J1_KERNEL", "CYCLE_KERNEL", "CLUSTER_SIZE", "J1_SITE_MODE", "REPLICA_GROUP",
-                  "CHAINS", "PDL", "FUSED_OBS")
+                  "CHAINS", "PDL", "FUSED_OBS", "J1_FIXED_L")
 
 
 def cpu_baseline_and_parity(kernel_options: dict, cycles: int = 6):
@@ -816,6 +816,9 @@ def main():
     ap.add_argument("--group", type=int, default=4)
     ap.add_argument("--chains", type=int, default=2)
     ap.add_argument("--site-mode", type=int, default=3)
+    ap.add_argument("--fixed-l", type=int, default=1, choices=[0, 1],
+                    help="1: per-pass J1 kernels compiled for L = 16 / 32 (default); "
+                         "0: the run-time-L kernels")
     args = ap.parse_args()
     rc = relaunch_under_torchrun(args)
     if rc is not None:
@@ -862,6 +865,7 @@ def main():
     cones = np.full(len(temps), 0.3, dtype=np.float32)
     eng.set_cone(cones)
     variant = None
+    eng.set_option(eng.OPT_J1_FIXED_L, args.fixed_l)
     if args.kernel == "auto":
         # the autotuner's cycles are untimed warm-up Monte Carlo steps; on a
         # shard (one of several ranks) it runs them without the local
@@ -882,7 +886,8 @@ def main():
                    "j1_kernel": options["J1_KERNEL"],
                    "replica_group": options["REPLICA_GROUP"],
                    "chains": options["CHAINS"],
-                   "j1_site_mode": options["J1_SITE_MODE"], "autotune_choice": variant}
+                   "j1_site_mode": options["J1_SITE_MODE"],
+                   "j1_fixed_l": options["J1_FIXED_L"], "autotune_choice": variant}
     if world > 1:
         from cudacode_b200.distributed import EngineBackend, ShardedPT
         pt = ShardedPT(EngineBackend(eng, torch.device(f"cuda:{local}")), R_PER_GPU * n_gpus)

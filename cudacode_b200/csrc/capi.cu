@@ -78,6 +78,7 @@ J1PassParams j1_params(pyro_ctx* ctx, int si, unsigned long long off) {
   p.renorm_every = ctx->renorm_every;
   p.exch = s.exch >= 0 ? 1 : 0;
   p.pdl = ctx->pdl;
+  p.fixed_l = ctx->j1_fixed_l;
   std::memset(p.xa, 0, sizeof p.xa);
   std::memset(p.xf, 0, sizeof p.xf);
   if (s.exch >= 0) {
@@ -1078,6 +1079,9 @@ int pyro_set_option(pyro_ctx* ctx, int option, int value) {
   } else if (option == PYRO_OPT_WAVE_STALL) {
     if (value < -1) return fail(ctx, PYRO_ERR_ARG, "stall item is -1 (off) or an item index");
     ctx->wave_stall_item = value;
+  } else if (option == PYRO_OPT_J1_FIXED_L) {
+    if (value != 0 && value != 1) return fail(ctx, PYRO_ERR_ARG, "fixed-L option is 0 or 1");
+    ctx->j1_fixed_l = value;
   } else if (option == PYRO_OPT_CLUSTER_SIZE) {
     if (value < 1 || value > 16) return fail(ctx, PYRO_ERR_ARG, "cluster size is 1..16");
     ctx->cluster_size = value;
@@ -1109,6 +1113,7 @@ int pyro_get_option(pyro_ctx* ctx, int option, int* value) {
     case PYRO_OPT_FUSED_OBS: *value = ctx->fused_obs; break;
     case PYRO_OPT_WAVE_STALL: *value = ctx->wave_stall_item; break;
     case PYRO_OPT_MEASURE_SNAPSHOT: *value = ctx->measure_snapshot; break;
+    case PYRO_OPT_J1_FIXED_L: *value = ctx->j1_fixed_l; break;
     case PYRO_OPT_J1_SITE_MODE:
       *value = (ctx->j1_metro_site_mode ? 1 : 0) | (ctx->j1_or_site_mode ? 2 : 0);
       break;

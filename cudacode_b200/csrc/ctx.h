@@ -78,6 +78,7 @@ struct pyro_ctx {
   // one site per thread (true) or the 4 sites of a cell per thread.
   bool j1_metro_site_mode = true;
   bool j1_or_site_mode = false;
+  int j1_fixed_l = 1;  // fixed-L per-pass kernels for L = 16, 32 (PYRO_OPT_J1_FIXED_L)
   // Cycle kernel for J1 systems: 0 per-pass launches, 1 cluster-resident,
   // 2 the work-queue kernel (one launch per system per cycle).
   int cycle_kernel = 0;

@@ -151,26 +151,37 @@ __device__ __forceinline__ void site_field(const float4* __restrict__ rep, const
 // The update of site S given its spin and field: Metropolis (Philox, cone,
 // exp) or over-relaxation, optional renormalisation, store. Returns 1 if a
 // Metropolis move was accepted.
+// `own` = S L3 + cell, the site's index in its replica (its Philox counter).
+template <bool kMetro>
+__device__ __forceinline__ float4 updated_spin(uint32_t own, pyro_vec3 sp, pyro_vec3 h,
+                                               float beta, float cosmax, uint32_t rkey,
+                                               uint32_t sweep32, bool renorm, uint32_t seed_lo,
+                                               uint32_t seed_hi, int* acc) {
+  pyro_vec3 out;
+  if (kMetro) {
+    uint32_t r[4];
+    pyro_philox(own, rkey, sweep32, PYRO_PURPOSE_METRO, seed_lo, seed_hi, r);
+    const pyro_vec3 prop = pyro_cone_proposal(sp, cosmax, pyro_uniform(r[0]), pyro_uniform(r[1]));
+    const float dE = pyro_delta_e(h, sp, prop);
+    *acc = pyro_metropolis_accept(dE, beta, pyro_uniform(r[2]));
+    out = *acc ? prop : sp;
+  } else {
+    *acc = 0;
+    out = pyro_overrelax(sp, h);
+  }
+  if (renorm) out = pyro_renormalise(out);
+  return make_float4(out.x, out.y, out.z, 0.0f);
+}
+
 template <int S, bool kMetro>
 __device__ __forceinline__ int site_update(float4* __restrict__ rep, int cell, int L3,
                                            pyro_vec3 sp, pyro_vec3 h, float beta, float cosmax,
                                            uint32_t rkey, uint32_t sweep32, bool renorm,
                                            uint32_t seed_lo, uint32_t seed_hi) {
   const int own = S * L3 + cell;
-  pyro_vec3 out;
-  int acc = 0;
-  if (kMetro) {
-    uint32_t r[4];
-    pyro_philox((uint32_t)own, rkey, sweep32, PYRO_PURPOSE_METRO, seed_lo, seed_hi, r);
-    const pyro_vec3 prop = pyro_cone_proposal(sp, cosmax, pyro_uniform(r[0]), pyro_uniform(r[1]));
-    const float dE = pyro_delta_e(h, sp, prop);
-    acc = pyro_metropolis_accept(dE, beta, pyro_uniform(r[2]));
-    out = acc ? prop : sp;
-  } else {
-    out = pyro_overrelax(sp, h);
-  }
-  if (renorm) out = pyro_renormalise(out);
-  rep[own] = make_float4(out.x, out.y, out.z, 0.0f);
+  int acc;
+  rep[own] = updated_spin<kMetro>((uint32_t)own, sp, h, beta, cosmax, rkey, sweep32, renorm,
+                                  seed_lo, seed_hi, &acc);
   return acc;
 }
 
@@ -183,6 +194,159 @@ __device__ __forceinline__ int update_site(float4* __restrict__ rep, const CellF
   site_field<S, kLd, kExch>(rep, f, cell, L3, J1, p, &sp, &h);
   return site_update<S, kMetro>(rep, cell, L3, sp, h, beta, cosmax, rkey, sweep32, renorm, seed_lo,
                                 seed_hi);
+}
+
+// ---------------------------------------------------------------------------
+// Addressing with the lattice size fixed at compile time (L = 2^kLog2L,
+// isotropic J1 systems with L = 16 or 32, which the per-pass launches pick
+// by L). The thread's cell is decoded with shifts; the base pointer is its
+// cell in site plane 8 of its replica, so the plane of a neighbour is a
+// compile-time offset of at most 8 planes (8 L^3 x 16 B = 4 MiB at L = 32)
+// that the load carries as an immediate; the wrapped offsets of the
+// neighbouring columns, rows and planes are selected once per thread, so a
+// neighbour cell costs one add and one pointer, shared by all loads from
+// that cell (7 distinct cells per colour pass). The loads, their order and
+// the update arithmetic are those of the run-time form: results are
+// identical.
+template <int kLog2L>
+struct FixedCell {
+  static constexpr int kL = 1 << kLog2L;
+  static constexpr int kL3 = 1 << (3 * kLog2L);
+  float4* mid;              // the thread's cell in site plane 8 of its replica
+  int xo[3], yo[3], zo[3];  // cell offsets of the previous / same / next column, row, plane
+};
+
+template <int kLog2L>
+__device__ __forceinline__ FixedCell<kLog2L> fixed_cell(float4* rb, int cell) {
+  constexpr int L = FixedCell<kLog2L>::kL, L2 = L * L;
+  const int x = cell & (L - 1), y = (cell >> kLog2L) & (L - 1), z = cell >> (2 * kLog2L);
+  FixedCell<kLog2L> c;
+  c.mid = rb + 8 * FixedCell<kLog2L>::kL3 + cell;
+  c.xo[0] = x == 0 ? L - 1 : -1;
+  c.xo[1] = 0;
+  c.xo[2] = x == L - 1 ? 1 - L : 1;
+  c.yo[0] = y == 0 ? (L - 1) * L : -L;
+  c.yo[1] = 0;
+  c.yo[2] = y == L - 1 ? (1 - L) * L : L;
+  c.zo[0] = z == 0 ? (L - 1) * L2 : -L2;
+  c.zo[1] = 0;
+  c.zo[2] = z == L - 1 ? (1 - L) * L2 : L2;
+  return c;
+}
+
+// Site s of the thread's cell (read-only path, or through L2 for the
+// thread's own stores of the same launch).
+template <int s, int kLog2L, int kLd = kLdNc>
+__device__ __forceinline__ float4 fixed_own(const FixedCell<kLog2L>& c) {
+  return load_spin<kLd>(c.mid + (s - 8) * FixedCell<kLog2L>::kL3);
+}
+
+template <int S, int K, int kLog2L>
+__device__ __forceinline__ float4 fixed_neighbour(const FixedCell<kLog2L>& c) {
+  constexpr NbrEntry e = j1_neighbour(S, K);
+  static_assert(e.t >= 0, "neighbour table");
+  const float4* pc = c.mid + (c.zo[e.dz + 1] + c.yo[e.dy + 1] + c.xo[e.dx + 1]);
+  return __ldg(pc + (e.t - 8) * FixedCell<kLog2L>::kL3);
+}
+
+// Spin and local field of site S (the arithmetic of site_field).
+template <int S, int kLog2L>
+__device__ __forceinline__ void fixed_site_field(const FixedCell<kLog2L>& c, float J1,
+                                                 pyro_vec3* sp, pyro_vec3* h) {
+  const float4 sv = fixed_own<S, kLog2L>(c);
+  const float4 n0 = fixed_neighbour<S, 0, kLog2L>(c);
+  const float4 n1 = fixed_neighbour<S, 1, kLog2L>(c);
+  const float4 n2 = fixed_neighbour<S, 2, kLog2L>(c);
+  const float4 n3 = fixed_neighbour<S, 3, kLog2L>(c);
+  const float4 n4 = fixed_neighbour<S, 4, kLog2L>(c);
+  const float4 n5 = fixed_neighbour<S, 5, kLog2L>(c);
+  h->x = J1 * (((((n0.x + n1.x) + n2.x) + n3.x) + n4.x) + n5.x);
+  h->y = J1 * (((((n0.y + n1.y) + n2.y) + n3.y) + n4.y) + n5.y);
+  h->z = J1 * (((((n0.z + n1.z) + n2.z) + n3.z) + n4.z) + n5.z);
+  sp->x = sv.x;
+  sp->y = sv.y;
+  sp->z = sv.z;
+}
+
+template <int S, bool kMetro, int kLog2L>
+__device__ __forceinline__ int fixed_site_update(const FixedCell<kLog2L>& c, int cell,
+                                                 pyro_vec3 sp, pyro_vec3 h, float beta,
+                                                 float cosmax, uint32_t rkey, uint32_t sweep32,
+                                                 bool renorm, uint32_t seed_lo,
+                                                 uint32_t seed_hi) {
+  constexpr int L3 = FixedCell<kLog2L>::kL3;
+  int acc;
+  c.mid[(S - 8) * L3] = updated_spin<kMetro>((uint32_t)(S * L3 + cell), sp, h, beta, cosmax,
+                                             rkey, sweep32, renorm, seed_lo, seed_hi, &acc);
+  return acc;
+}
+
+// Sweep number, renormalisation flag and Philox replica word of a pass.
+struct PassWords {
+  uint32_t rkey, sw;
+  bool renorm;
+};
+__device__ __forceinline__ PassWords pass_words(const J1PassParams& p, int rep,
+                                                unsigned long long sweep_add = 0) {
+  const unsigned long long sweep =
+      (p.sweep_ctr ? *p.sweep_ctr : 0ull) + p.sweep_off + sweep_add;
+  PassWords w;
+  w.renorm = p.renorm_every > 0 && ((sweep + 1) % (unsigned long long)p.renorm_every) == 0;
+  w.rkey = (uint32_t)(p.rep_key + rep);
+  w.sw = (uint32_t)sweep;
+  return w;
+}
+
+// Cell form of a colour-B pass with fixed L (as cell_pass).
+template <int B, bool kMetro, int kLog2L>
+__device__ __forceinline__ int fixed_cell_pass(const J1PassParams& p, int rep, int cell,
+                                               float beta, float cosmax) {
+  const FixedCell<kLog2L> c =
+      fixed_cell<kLog2L>(p.spins + (long long)rep * 16 * FixedCell<kLog2L>::kL3, cell);
+  const PassWords w = pass_words(p, rep);
+  pyro_vec3 s0, h0, s1, h1, s2, h2, s3, h3;
+  fixed_site_field<B, kLog2L>(c, p.J1, &s0, &h0);
+  fixed_site_field<4 + B, kLog2L>(c, p.J1, &s1, &h1);
+  fixed_site_field<8 + B, kLog2L>(c, p.J1, &s2, &h2);
+  fixed_site_field<12 + B, kLog2L>(c, p.J1, &s3, &h3);
+  int acc = 0;
+  acc += fixed_site_update<B, kMetro, kLog2L>(c, cell, s0, h0, beta, cosmax, w.rkey, w.sw,
+                                              w.renorm, p.seed_lo, p.seed_hi);
+  acc += fixed_site_update<4 + B, kMetro, kLog2L>(c, cell, s1, h1, beta, cosmax, w.rkey, w.sw,
+                                                  w.renorm, p.seed_lo, p.seed_hi);
+  acc += fixed_site_update<8 + B, kMetro, kLog2L>(c, cell, s2, h2, beta, cosmax, w.rkey, w.sw,
+                                                  w.renorm, p.seed_lo, p.seed_hi);
+  acc += fixed_site_update<12 + B, kMetro, kLog2L>(c, cell, s3, h3, beta, cosmax, w.rkey, w.sw,
+                                                   w.renorm, p.seed_lo, p.seed_hi);
+  return acc;
+}
+
+template <int S, bool kMetro, int kLog2L>
+__device__ __forceinline__ int fixed_update_site(const J1PassParams& p, int rep, int cell,
+                                                 float beta, float cosmax) {
+  const FixedCell<kLog2L> c =
+      fixed_cell<kLog2L>(p.spins + (long long)rep * 16 * FixedCell<kLog2L>::kL3, cell);
+  const PassWords w = pass_words(p, rep);
+  pyro_vec3 sp, h;
+  fixed_site_field<S, kLog2L>(c, p.J1, &sp, &h);
+  return fixed_site_update<S, kMetro, kLog2L>(c, cell, sp, h, beta, cosmax, w.rkey, w.sw,
+                                              w.renorm, p.seed_lo, p.seed_hi);
+}
+
+// Site form with fixed L (as site_item).
+template <int B, bool kMetro, int kLog2L>
+__device__ __forceinline__ int fixed_site_item(const J1PassParams& p, int rep, int f, int cell,
+                                               float beta, float cosmax) {
+  switch (f) {
+    case 0:
+      return fixed_update_site<B, kMetro, kLog2L>(p, rep, cell, beta, cosmax);
+    case 1:
+      return fixed_update_site<4 + B, kMetro, kLog2L>(p, rep, cell, beta, cosmax);
+    case 2:
+      return fixed_update_site<8 + B, kMetro, kLog2L>(p, rep, cell, beta, cosmax);
+    default:
+      return fixed_update_site<12 + B, kMetro, kLog2L>(p, rep, cell, beta, cosmax);
+  }
 }
 
 // Start of a per-pass kernel: the grid this launch may overlap (programmatic
@@ -245,8 +409,10 @@ __device__ __forceinline__ void block_accept(const J1PassParams& p, int t, int a
   }
 }
 
-template <int B, bool kMetro, bool kExch>
+// kLog2L > 0: the fixed-L addressing (isotropic J1 systems of L = 2^kLog2L).
+template <int B, bool kMetro, bool kExch, int kLog2L = 0>
 __global__ void __launch_bounds__(kJ1Threads) j1_pass_kernel(const J1PassParams p) {
+  static_assert(kLog2L == 0 || !kExch, "fixed-L form is isotropic only");
   pass_prologue();
   const int rep = blockIdx.y;
   const int cell = blockIdx.x * kJ1Threads + threadIdx.x;
@@ -259,7 +425,10 @@ __global__ void __launch_bounds__(kJ1Threads) j1_pass_kernel(const J1PassParams 
     cosmax = p.cosmax[p.temp_base + t];
   }
   int acc = 0;
-  if (cell < p.L3) acc = cell_pass<B, kMetro, kExch>(p, rep, cell, beta, cosmax);
+  if (cell < p.L3) {
+    if constexpr (kLog2L > 0) acc = fixed_cell_pass<B, kMetro, kLog2L>(p, rep, cell, beta, cosmax);
+    else acc = cell_pass<B, kMetro, kExch>(p, rep, cell, beta, cosmax);
+  }
   if (kMetro) block_accept(p, t, acc);
 }
 
@@ -299,8 +468,9 @@ __device__ __forceinline__ int site_item(const J1PassParams& p, int rep, int f, 
 // S = 4 f + B is uniform in a CTA), blockIdx.z the replica. Fewer live
 // registers than the cell-per-thread form, hence more warps in flight; the
 // Metropolis pass (Philox, cone, exp) is latency-bound without them.
-template <int B, bool kMetro, bool kExch>
+template <int B, bool kMetro, bool kExch, int kLog2L = 0>
 __global__ void __launch_bounds__(kJ1Threads) j1_site_pass_kernel(const J1PassParams p) {
+  static_assert(kLog2L == 0 || !kExch, "fixed-L form is isotropic only");
   pass_prologue();
   const int f = blockIdx.y;
   const int rep = blockIdx.z;
@@ -314,7 +484,10 @@ __global__ void __launch_bounds__(kJ1Threads) j1_site_pass_kernel(const J1PassPa
     cosmax = p.cosmax[p.temp_base + t];
   }
   int acc = 0;
-  if (cell < p.L3) acc = site_item<B, kMetro, kExch>(p, rep, f, cell, beta, cosmax);
+  if (cell < p.L3) {
+    if constexpr (kLog2L > 0) acc = fixed_site_item<B, kMetro, kLog2L>(p, rep, f, cell, beta, cosmax);
+    else acc = site_item<B, kMetro, kExch>(p, rep, f, cell, beta, cosmax);
+  }
   if (kMetro) {
     const int n = __syncthreads_count(acc);
     if (threadIdx.x == 0 && n > 0)
@@ -494,13 +667,54 @@ __device__ __forceinline__ void last_item(const J1PassParams& p, const J1ObsPara
   if (threadIdx.x == 0) o.partials[slot] = r;
 }
 
+// corner3_observables with the fixed-L addressing (same loads, same sums).
+template <int F, int kLog2L>
+__device__ __forceinline__ void fixed_corner3_observables(const FixedCell<kLog2L>& c, double* e,
+                                                          double* mx, double* my, double* mz) {
+  constexpr int S = 4 * F + 3;
+  const float4 s0 = fixed_own<4 * F + 0, kLog2L>(c);
+  const float4 s1 = fixed_own<4 * F + 1, kLog2L>(c);
+  const float4 s2 = fixed_own<4 * F + 2, kLog2L>(c);
+  const float4 s3 = fixed_own<S, kLog2L, kLdL2>(c);  // this thread's own store
+  const float4 d1 = fixed_neighbour<S, j1_down_index(S, 0), kLog2L>(c);
+  const float4 d2 = fixed_neighbour<S, j1_down_index(S, 1), kLog2L>(c);
+  const float4 d3 = fixed_neighbour<S, j1_down_index(S, 2), kLog2L>(c);
+  *e += tet_energy(s0, s1, s2, s3) + tet_energy(s3, d1, d2, d3);
+  *mx += (double)s0.x + s1.x + s2.x + s3.x;
+  *my += (double)s0.y + s1.y + s2.y + s3.y;
+  *mz += (double)s0.z + s1.z + s2.z + s3.z;
+}
+
+// last_item with the fixed-L addressing.
+template <bool kMetro, int kLog2L>
+__device__ __forceinline__ void fixed_last_item(const J1PassParams& p, const J1ObsParams& o,
+                                                int rep, int cell, float beta, float cosmax,
+                                                int t, double (*red)[kJ1Threads / 32],
+                                                long long slot) {
+  int acc = 0;
+  double e = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+  if (cell < p.L3) {
+    acc = fixed_cell_pass<3, kMetro, kLog2L>(p, rep, cell, beta, cosmax);
+    const FixedCell<kLog2L> c =
+        fixed_cell<kLog2L>(p.spins + (long long)rep * 16 * FixedCell<kLog2L>::kL3, cell);
+    fixed_corner3_observables<0, kLog2L>(c, &e, &mx, &my, &mz);
+    fixed_corner3_observables<1, kLog2L>(c, &e, &mx, &my, &mz);
+    fixed_corner3_observables<2, kLog2L>(c, &e, &mx, &my, &mz);
+    fixed_corner3_observables<3, kLog2L>(c, &e, &mx, &my, &mz);
+    e *= o.J1;
+  }
+  if (kMetro) block_accept(p, t, acc);
+  const double4 r = block_observables(e, mx, my, mz, red);
+  if (threadIdx.x == 0) o.partials[slot] = r;
+}
+
 // The last pass of a cycle (colour 3, cell form, isotropic J1) fused with
 // the FP64 energy and magnetisation partials of the state it leaves: the
 // same updates as j1_pass_kernel<3, kMetro, false>, then each cell's eight
 // tetrahedra from spins the pass just loaded (L1/L2), instead of a separate
 // observables kernel reading the lattice again. Partials in the layout of
 // j1_observables_kernel (one per CTA of kJ1Threads cells).
-template <bool kMetro>
+template <bool kMetro, int kLog2L = 0>
 __global__ void __launch_bounds__(kJ1Threads) j1_last_pass_kernel(const J1PassParams p,
                                                                   const J1ObsParams o) {
   pass_prologue();
@@ -515,8 +729,11 @@ __global__ void __launch_bounds__(kJ1Threads) j1_last_pass_kernel(const J1PassPa
     beta = p.beta[p.temp_base + t];
     cosmax = p.cosmax[p.temp_base + t];
   }
-  last_item<kMetro, kLdNc>(p, o, rep, cell, beta, cosmax, t, 0ull, red,
-                          o.partial_begin + (long long)rep * gridDim.x + blockIdx.x);
+  const long long slot = o.partial_begin + (long long)rep * gridDim.x + blockIdx.x;
+  if constexpr (kLog2L > 0)
+    fixed_last_item<kMetro, kLog2L>(p, o, rep, cell, beta, cosmax, t, red, slot);
+  else
+    last_item<kMetro, kLdNc>(p, o, rep, cell, beta, cosmax, t, 0ull, red, slot);
 }
 
 // One site update of the cluster kernel: site S of `cell`, neighbours read
@@ -925,39 +1142,48 @@ void launch_pass(Kernel k, dim3 grid, const J1PassParams& p, cudaStream_t st) {
 }
 }  // namespace
 
+// log2 L of the fixed-L kernels for this pass (0: the run-time form).
+int j1_fixed_log2(const J1PassParams& p) {
+  if (p.exch || p.fixed_l == 0) return 0;
+  if (p.L == 32) return 5;
+  if (p.L == 16) return 4;
+  return 0;
+}
+
 void launch_j1_pass(const J1PassParams& p, int colour, bool metro, bool site_per_thread,
                     cudaStream_t st) {
   const dim3 grid((p.L3 + kJ1Threads - 1) / kJ1Threads, p.n_rep);
   const dim3 sgrid((p.L3 + kJ1Threads - 1) / kJ1Threads, 4, p.n_rep);
-#define PYRO_J1_CASE(B, X)                                                            \
+#define PYRO_J1_CASE(B, X, G)                                                         \
   case B:                                                                             \
     if (site_per_thread) {                                                            \
-      if (metro) launch_pass(j1_site_pass_kernel<B, true, X>, sgrid, p, st);          \
-      else launch_pass(j1_site_pass_kernel<B, false, X>, sgrid, p, st);               \
+      if (metro) launch_pass(j1_site_pass_kernel<B, true, X, G>, sgrid, p, st);       \
+      else launch_pass(j1_site_pass_kernel<B, false, X, G>, sgrid, p, st);            \
     } else {                                                                          \
-      if (metro) launch_pass(j1_pass_kernel<B, true, X>, grid, p, st);                \
-      else launch_pass(j1_pass_kernel<B, false, X>, grid, p, st);                     \
+      if (metro) launch_pass(j1_pass_kernel<B, true, X, G>, grid, p, st);             \
+      else launch_pass(j1_pass_kernel<B, false, X, G>, grid, p, st);                  \
     }                                                                                 \
     break;
-  if (p.exch) {
-    switch (colour) {
-      PYRO_J1_CASE(0, true)
-      PYRO_J1_CASE(1, true)
-      PYRO_J1_CASE(2, true)
-      PYRO_J1_CASE(3, true)
-      default:
-        break;
-    }
-  } else {
-    switch (colour) {
-      PYRO_J1_CASE(0, false)
-      PYRO_J1_CASE(1, false)
-      PYRO_J1_CASE(2, false)
-      PYRO_J1_CASE(3, false)
-      default:
-        break;
-    }
+#define PYRO_J1_COLOURS(X, G) \
+  switch (colour) {           \
+    PYRO_J1_CASE(0, X, G)     \
+    PYRO_J1_CASE(1, X, G)     \
+    PYRO_J1_CASE(2, X, G)     \
+    PYRO_J1_CASE(3, X, G)     \
+    default:                  \
+      break;                  \
   }
+  const int lg = j1_fixed_log2(p);
+  if (p.exch) {
+    PYRO_J1_COLOURS(true, 0)
+  } else if (lg == 5) {
+    PYRO_J1_COLOURS(false, 5)
+  } else if (lg == 4) {
+    PYRO_J1_COLOURS(false, 4)
+  } else {
+    PYRO_J1_COLOURS(false, 0)
+  }
+#undef PYRO_J1_COLOURS
 #undef PYRO_J1_CASE
 }
 
@@ -973,8 +1199,17 @@ void launch_j1_last_pass(const J1PassParams& p, const J1ObsParams& o, bool metro
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = p.pdl ? 1 : 0;
-  if (metro) cudaLaunchKernelEx(&cfg, j1_last_pass_kernel<true>, p, o);
-  else cudaLaunchKernelEx(&cfg, j1_last_pass_kernel<false>, p, o);
+  const int lg = j1_fixed_log2(p);
+  if (lg == 5) {
+    if (metro) cudaLaunchKernelEx(&cfg, j1_last_pass_kernel<true, 5>, p, o);
+    else cudaLaunchKernelEx(&cfg, j1_last_pass_kernel<false, 5>, p, o);
+  } else if (lg == 4) {
+    if (metro) cudaLaunchKernelEx(&cfg, j1_last_pass_kernel<true, 4>, p, o);
+    else cudaLaunchKernelEx(&cfg, j1_last_pass_kernel<false, 4>, p, o);
+  } else {
+    if (metro) cudaLaunchKernelEx(&cfg, j1_last_pass_kernel<true>, p, o);
+    else cudaLaunchKernelEx(&cfg, j1_last_pass_kernel<false>, p, o);
+  }
 }
 
 void launch_j1_observables(const J1ObsParams& p, cudaStream_t st) {

@@ -36,6 +36,9 @@ struct J1PassParams {
   // previous kernel of its stream drains; it waits (griddepcontrol.wait)
   // before its first global memory access.
   int pdl;
+  // Per-pass launches of isotropic systems with L = 16 or 32 use kernels
+  // compiled for that L (shift decode, compile-time plane offsets) when set.
+  int fixed_l;
 };
 
 // FP64 energy (by tetrahedra) and magnetisation partials of one J1 system;
@@ -139,6 +142,10 @@ int j1_skew_items(const J1SkewParams& sp);
 cudaError_t launch_j1_skew(const J1SkewParams& sp, int forms, cudaStream_t st);
 // Dependency half-width in chunks for lattice size L.
 int j1_wave_dep(int L);
+
+// log2 L of the fixed-L per-pass kernels that launch_j1_pass and
+// launch_j1_last_pass use for `p` (0: the run-time-L kernels).
+int j1_fixed_log2(const J1PassParams& p);
 
 // site_per_thread: one site per thread (more warps in flight) instead of the
 // 4 sites of a cell per thread; identical results.

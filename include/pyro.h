@@ -157,6 +157,11 @@ int pyro_neighbour_table(int site, int* out120);
  * stream; 0 (default) reads the live state on the context stream. Needs a
  * snapshot first (else PYRO_ERR_STATE). Changes no kernel schedule. */
 #define PYRO_OPT_MEASURE_SNAPSHOT 14
+/* PYRO_OPT_J1_FIXED_L: 1 (default) runs the per-pass kernels of isotropic
+ * J1 systems with L = 16 or 32 in forms compiled for that L (cell decode by
+ * shifts, neighbour planes as compile-time offsets: fewer instructions per
+ * update); 0 uses the run-time-L kernels for every L. Identical results. */
+#define PYRO_OPT_J1_FIXED_L 15
 int pyro_set_option(pyro_ctx* ctx, int option, int value);
 int pyro_get_option(pyro_ctx* ctx, int option, int* value);
 /* Autotuner: times every kernel variant (per-pass generic, per-pass J1,
