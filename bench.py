@@ -725,21 +725,25 @@ def learned_leg(cycles: int = 60000, warmup: int = 2000) -> dict:
 STEP_PROFILE = os.path.join(ROOT, "profiles", "pt_step_L32_R64_instructions.md")
 
 
-def profiled_instructions(kernel_desc: dict):
-    """Warp instructions per spin update of one step of the timed schedule,
-    from the committed ncu summary of that schedule (lines 'schedule: k=v
-    ...' and 'warp_instructions_per_update: X'); None when the summary is of
-    another schedule."""
+def profiled_step(kernel_desc: dict):
+    """Per-update figures of one step of the timed kernels, from the committed
+    ncu summary of those kernels (lines 'schedule: k=v ...',
+    'warp_instructions_per_update: X', 'l2_bytes_per_update: Y',
+    'l2_peak_gbs: Z'); None when the summary is of other kernels."""
     try:
-        sched, ipu = None, None
+        sched, vals = None, {}
         with open(STEP_PROFILE) as f:
             for line in f:
                 if line.startswith("schedule:"):
                     sched = dict(kv.split("=") for kv in line.split(":", 1)[1].split())
-                elif line.startswith("warp_instructions_per_update:"):
-                    ipu = float(line.split(":", 1)[1])
-        if sched and ipu and all(str(kernel_desc.get(k)) == v for k, v in sched.items()):
-            return ipu
+                else:
+                    for key in ("warp_instructions_per_update", "l2_bytes_per_update",
+                                "l2_peak_gbs"):
+                        if line.startswith(key + ":"):
+                            vals[key] = float(line.split(":", 1)[1])
+        if sched and len(vals) == 3 and all(str(kernel_desc.get(k)) == v
+                                            for k, v in sched.items()):
+            return vals
     except (OSError, ValueError):
         pass
     return None
@@ -815,7 +819,11 @@ def main():
                          "pass forms --site-mode")
     ap.add_argument("--group", type=int, default=4)
     ap.add_argument("--chains", type=int, default=2)
-    ap.add_argument("--site-mode", type=int, default=3)
+    ap.add_argument("--site-mode", type=int, default=None,
+                    help="J1 pass forms (bit 0 Metropolis, bit 1 over-relaxation one site "
+                         "per thread) for --kernel grouped / wave (wave default 3)")
+    ap.add_argument("--cluster-size", type=int, default=None,
+                    help="CTAs per cluster of --kernel cluster (default: the engine's)")
     ap.add_argument("--fixed-l", type=int, default=1, choices=[0, 1],
                     help="1: per-pass J1 kernels compiled for L = 16 / 32 (default); "
                          "0: the run-time-L kernels")
@@ -874,11 +882,15 @@ def main():
         variant = eng.autotune(N_METRO, N_OR, 16)
     else:
         eng.set_option(eng.OPT_CYCLE_KERNEL, {"cluster": 1, "wave": 2}.get(args.kernel, 0))
+        if args.kernel == "cluster" and args.cluster_size is not None:
+            eng.set_option(eng.OPT_CLUSTER_SIZE, args.cluster_size)
         if args.kernel in ("grouped", "wave"):
             eng.set_option(eng.OPT_REPLICA_GROUP, args.group)
         if args.kernel == "grouped":
             eng.set_option(eng.OPT_CHAINS, args.chains)
         if args.kernel == "wave":
+            eng.set_option(eng.OPT_J1_SITE_MODE, 3 if args.site_mode is None else args.site_mode)
+        elif args.kernel == "grouped" and args.site_mode is not None:
             eng.set_option(eng.OPT_J1_SITE_MODE, args.site_mode)
     options = {n: eng.get_option(getattr(Engine, "OPT_" + n)) for n in KERNEL_OPTIONS}
     kernel_desc = {"cycle_kernel": options["CYCLE_KERNEL"],
@@ -949,26 +961,34 @@ def main():
     # Roofline of the timed step. With the work-queue kernel (or replica
     # groups) a replica stays in L2 for all 20 passes of its cycle, so the
     # step's algorithmic HBM bytes are one read and one write of every spin
-    # per cycle: 32 B per 5 updates. The binding resource is instruction
-    # issue: warp instructions per update (ncu, committed summary) times the
-    # updates, over 4 schedulers x the SMs x the sampled SM clock x the time.
+    # per cycle: 32 B per 5 updates. The binding block reports the step's
+    # instruction-issue fraction (warp instructions per update from the
+    # committed ncu summary, times the updates, over 4 schedulers x the SMs x
+    # the sampled SM clock x the time) and its L2 fraction (L2 bytes per
+    # update from the same summary over the L2 peak).
     l2_resident = (kernel_desc["replica_group"] > 0 or kernel_desc["cycle_kernel"] > 0)
     sched_bytes = 32.0 / (N_METRO + N_OR) if l2_resident else float(BYTES_PER_UPDATE_PASS)
     step_ms = ms / args.steps
     step_updates = R_PER_GPU * 16 * L ** 3 * (N_METRO + N_OR)  # per GPU
     achieved = step_updates * sched_bytes / (step_ms * 1e-3) / 1e9
     wave = kernel_desc["cycle_kernel"] == 2
-    ipu = profiled_instructions(kernel_desc) if (L, R_PER_GPU) == (32, 64) else None
+    prof = profiled_step(kernel_desc) if (L, R_PER_GPU) == (32, 64) else None
     props = torch.cuda.get_device_properties(local)
-    issue = None
-    if ipu and clocks.get("sm_mhz"):
+    binding = None
+    if prof and clocks.get("sm_mhz"):
         issue_slots = props.multi_processor_count * 4 * clocks["sm_mhz"] * 1e6 * step_ms * 1e-3
-        issue = {"resource": "warp-instruction issue (4 schedulers per SM)",
-                 "warp_instructions_per_update": ipu,
-                 "frac": ipu * step_updates / issue_slots,
-                 "sm_mhz": clocks["sm_mhz"], "sms": props.multi_processor_count,
-                 "source": "profiles/pt_step_L32_R64_instructions.md (ncu "
-                           "smsp__inst_executed.sum over one step's launches)"}
+        ipu = prof["warp_instructions_per_update"]
+        l2_gbs = step_updates * prof["l2_bytes_per_update"] / (step_ms * 1e-3) / 1e9
+        binding = {
+            "resource": "the chains of dependent colour-pass launches (neither instruction "
+                        "issue nor L2 bandwidth saturates)",
+            "issue": {"warp_instructions_per_update": ipu,
+                      "frac": ipu * step_updates / issue_slots,
+                      "sm_mhz": clocks["sm_mhz"], "sms": props.multi_processor_count},
+            "l2": {"bytes_per_update": prof["l2_bytes_per_update"], "achieved_gbs": l2_gbs,
+                   "peak_gbs": prof["l2_peak_gbs"], "frac": l2_gbs / prof["l2_peak_gbs"]},
+            "source": "profiles/pt_step_L32_R64_instructions.md (ncu smsp__inst_executed.sum "
+                      "over one step's launches; lts__t_bytes.sum per launch)"}
 
     # The streaming form of the same passes, for comparison: one launch per
     # colour pass over all replicas, 80 algorithmic bytes per update.
@@ -1014,10 +1034,10 @@ def main():
                 "bytes_per_update": sched_bytes, "updates_per_launch": step_updates,
                 "ms_per_launch": step_ms,
                 "traffic": None,
-                "binding": issue,
+                "binding": binding,
                 "note": ("HBM is not the bound of this schedule: each replica group stays in L2 "
                          "for its cycle, so HBM sees one read and one write per spin per cycle; "
-                         "the binding resource is instruction issue (binding.frac)"
+                         "binding gives the step's instruction-issue and L2 fractions"
                          if l2_resident else "every pass streams the lattice from HBM"),
                 "streaming_pass": {
                     "what": "j1_pass_kernel<colour, over-relaxation> streaming from HBM, one "

@@ -1153,7 +1153,10 @@ int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen)
                            // skewed multi-group launches: forms, group size, groups in flight
                            {1, 3, 16, 3, 2, 4, 0}, {1, 3, 16, 3, 2, 8, 0}, {1, 3, 16, 3, 1, 8, 0},
                            {1, 3, 16, 3, 4, 4, 0}, {1, 3, 16, 1, 2, 4, 0}, {1, 3, 16, 1, 2, 8, 0},
-                           {1, 3, 16, 1, 4, 4, 0}, {1, 3, 16, 3, 4, 2, 0}};
+                           {1, 3, 16, 1, 4, 4, 0}, {1, 3, 16, 3, 4, 2, 0},
+                           // Metropolis passes in the cell form too (fixed-L kernels)
+                           {1, 0, 16, 0, 2, 4, 0}, {1, 0, 16, 0, 4, 2, 0}, {1, 0, 16, 0, 3, 3, 0},
+                           {1, 0, 16, 0, 1, 8, 0}};
     vs.insert(vs.end(), std::begin(j1v), std::end(j1v));
     n_j1 = (int)vs.size();
   }

@@ -241,25 +241,25 @@ __device__ __forceinline__ float4 fixed_own(const FixedCell<kLog2L>& c) {
   return load_spin<kLd>(c.mid + (s - 8) * FixedCell<kLog2L>::kL3);
 }
 
-template <int S, int K, int kLog2L>
+template <int S, int K, int kLog2L, int kLd = kLdNc>
 __device__ __forceinline__ float4 fixed_neighbour(const FixedCell<kLog2L>& c) {
   constexpr NbrEntry e = j1_neighbour(S, K);
   static_assert(e.t >= 0, "neighbour table");
   const float4* pc = c.mid + (c.zo[e.dz + 1] + c.yo[e.dy + 1] + c.xo[e.dx + 1]);
-  return __ldg(pc + (e.t - 8) * FixedCell<kLog2L>::kL3);
+  return load_spin<kLd>(pc + (e.t - 8) * FixedCell<kLog2L>::kL3);
 }
 
 // Spin and local field of site S (the arithmetic of site_field).
-template <int S, int kLog2L>
+template <int S, int kLog2L, int kLd = kLdNc>
 __device__ __forceinline__ void fixed_site_field(const FixedCell<kLog2L>& c, float J1,
                                                  pyro_vec3* sp, pyro_vec3* h) {
-  const float4 sv = fixed_own<S, kLog2L>(c);
-  const float4 n0 = fixed_neighbour<S, 0, kLog2L>(c);
-  const float4 n1 = fixed_neighbour<S, 1, kLog2L>(c);
-  const float4 n2 = fixed_neighbour<S, 2, kLog2L>(c);
-  const float4 n3 = fixed_neighbour<S, 3, kLog2L>(c);
-  const float4 n4 = fixed_neighbour<S, 4, kLog2L>(c);
-  const float4 n5 = fixed_neighbour<S, 5, kLog2L>(c);
+  const float4 sv = fixed_own<S, kLog2L, kLd>(c);
+  const float4 n0 = fixed_neighbour<S, 0, kLog2L, kLd>(c);
+  const float4 n1 = fixed_neighbour<S, 1, kLog2L, kLd>(c);
+  const float4 n2 = fixed_neighbour<S, 2, kLog2L, kLd>(c);
+  const float4 n3 = fixed_neighbour<S, 3, kLog2L, kLd>(c);
+  const float4 n4 = fixed_neighbour<S, 4, kLog2L, kLd>(c);
+  const float4 n5 = fixed_neighbour<S, 5, kLog2L, kLd>(c);
   h->x = J1 * (((((n0.x + n1.x) + n2.x) + n3.x) + n4.x) + n5.x);
   h->y = J1 * (((((n0.y + n1.y) + n2.y) + n3.y) + n4.y) + n5.y);
   h->z = J1 * (((((n0.z + n1.z) + n2.z) + n3.z) + n4.z) + n5.z);
@@ -297,6 +297,29 @@ __device__ __forceinline__ PassWords pass_words(const J1PassParams& p, int rep,
   return w;
 }
 
+// The four colour-B sites of a cell with fixed L: loads of all four before
+// the first store (as cell_pass).
+template <int B, bool kMetro, int kLog2L, int kLd = kLdNc>
+__device__ __forceinline__ int fixed_cell_sites(const FixedCell<kLog2L>& c, int cell, float J1,
+                                                float beta, float cosmax, const PassWords& w,
+                                                uint32_t seed_lo, uint32_t seed_hi) {
+  pyro_vec3 s0, h0, s1, h1, s2, h2, s3, h3;
+  fixed_site_field<B, kLog2L, kLd>(c, J1, &s0, &h0);
+  fixed_site_field<4 + B, kLog2L, kLd>(c, J1, &s1, &h1);
+  fixed_site_field<8 + B, kLog2L, kLd>(c, J1, &s2, &h2);
+  fixed_site_field<12 + B, kLog2L, kLd>(c, J1, &s3, &h3);
+  int acc = 0;
+  acc += fixed_site_update<B, kMetro, kLog2L>(c, cell, s0, h0, beta, cosmax, w.rkey, w.sw,
+                                              w.renorm, seed_lo, seed_hi);
+  acc += fixed_site_update<4 + B, kMetro, kLog2L>(c, cell, s1, h1, beta, cosmax, w.rkey, w.sw,
+                                                  w.renorm, seed_lo, seed_hi);
+  acc += fixed_site_update<8 + B, kMetro, kLog2L>(c, cell, s2, h2, beta, cosmax, w.rkey, w.sw,
+                                                  w.renorm, seed_lo, seed_hi);
+  acc += fixed_site_update<12 + B, kMetro, kLog2L>(c, cell, s3, h3, beta, cosmax, w.rkey, w.sw,
+                                                   w.renorm, seed_lo, seed_hi);
+  return acc;
+}
+
 // Cell form of a colour-B pass with fixed L (as cell_pass).
 template <int B, bool kMetro, int kLog2L>
 __device__ __forceinline__ int fixed_cell_pass(const J1PassParams& p, int rep, int cell,
@@ -304,21 +327,8 @@ __device__ __forceinline__ int fixed_cell_pass(const J1PassParams& p, int rep, i
   const FixedCell<kLog2L> c =
       fixed_cell<kLog2L>(p.spins + (long long)rep * 16 * FixedCell<kLog2L>::kL3, cell);
   const PassWords w = pass_words(p, rep);
-  pyro_vec3 s0, h0, s1, h1, s2, h2, s3, h3;
-  fixed_site_field<B, kLog2L>(c, p.J1, &s0, &h0);
-  fixed_site_field<4 + B, kLog2L>(c, p.J1, &s1, &h1);
-  fixed_site_field<8 + B, kLog2L>(c, p.J1, &s2, &h2);
-  fixed_site_field<12 + B, kLog2L>(c, p.J1, &s3, &h3);
-  int acc = 0;
-  acc += fixed_site_update<B, kMetro, kLog2L>(c, cell, s0, h0, beta, cosmax, w.rkey, w.sw,
-                                              w.renorm, p.seed_lo, p.seed_hi);
-  acc += fixed_site_update<4 + B, kMetro, kLog2L>(c, cell, s1, h1, beta, cosmax, w.rkey, w.sw,
-                                                  w.renorm, p.seed_lo, p.seed_hi);
-  acc += fixed_site_update<8 + B, kMetro, kLog2L>(c, cell, s2, h2, beta, cosmax, w.rkey, w.sw,
-                                                  w.renorm, p.seed_lo, p.seed_hi);
-  acc += fixed_site_update<12 + B, kMetro, kLog2L>(c, cell, s3, h3, beta, cosmax, w.rkey, w.sw,
-                                                   w.renorm, p.seed_lo, p.seed_hi);
-  return acc;
+  return fixed_cell_sites<B, kMetro, kLog2L>(c, cell, p.J1, beta, cosmax, w, p.seed_lo,
+                                             p.seed_hi);
 }
 
 template <int S, bool kMetro, int kLog2L>
@@ -777,6 +787,77 @@ __device__ __forceinline__ void cluster_barrier() {
   asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
 }
 
+// End of a cluster cycle: the replica's acceptance count (one atomic per CTA)
+// and, when p.partials is set, the observables partials of the final state
+// in the chunks and reduction order of j1_observables_kernel (thread group q
+// of the CTA handles chunk oc). Every thread of the cluster calls it after
+// the last pass's barrier.
+__device__ __forceinline__ void cluster_cycle_tail(
+    const J1CycleParams& p, int rep, int rank, int t, int acc,
+    double (*red)[4][kJ1Threads / 32], int* warp_acc) {
+  const int csize = p.cluster_size;
+  const int L = p.pass.L, L3 = p.pass.L3;
+  const float rcpL = p.pass.rcpL;
+  const float4* rb = p.pass.spins + (long long)rep * 16 * L3;
+  if (p.n_metro > 0) {
+    int v = acc;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) warp_acc[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int s = 0;
+      for (int w = 0; w < kJ1CycleThreads / 32; ++w) s += warp_acc[w];
+      if (s > 0) atomicAdd(p.pass.accepted + p.pass.temp_base + t, (unsigned long long)s);
+    }
+  }
+  if (p.partials) {
+    constexpr int kGroups = kJ1CycleThreads / kJ1Threads;
+    const int q = threadIdx.x / kJ1Threads;
+    const int lt = threadIdx.x - q * kJ1Threads;
+    const int n_obs = (L3 + kJ1Threads - 1) / kJ1Threads;
+    for (int base_c = rank * kGroups; base_c < n_obs; base_c += csize * kGroups) {
+      const int oc = base_c + q;
+      const int cell = oc * kJ1Threads + lt;
+      double e = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+      if (oc < n_obs && cell < L3) {
+        int x, y, z;
+        decode_cell(cell, L, rcpL, &x, &y, &z);
+        const CellFrame f = make_frame(x, y, z, L);
+        cell_corner<0, true>(rb, f, cell, L3, &e, &mx, &my, &mz);
+        cell_corner<1, true>(rb, f, cell, L3, &e, &mx, &my, &mz);
+        cell_corner<2, true>(rb, f, cell, L3, &e, &mx, &my, &mz);
+        cell_corner<3, true>(rb, f, cell, L3, &e, &mx, &my, &mz);
+        e *= p.J1_64;
+      }
+      e = warp_sum_d(e);
+      mx = warp_sum_d(mx);
+      my = warp_sum_d(my);
+      mz = warp_sum_d(mz);
+      const int w = lt >> 5, lane = lt & 31;
+      if (lane == 0) {
+        red[q][0][w] = e;
+        red[q][1][w] = mx;
+        red[q][2][w] = my;
+        red[q][3][w] = mz;
+      }
+      __syncthreads();
+      if (lt == 0 && oc < n_obs) {
+        double4 o = make_double4(0.0, 0.0, 0.0, 0.0);
+        for (int ww = 0; ww < kJ1Threads / 32; ++ww) {
+          o.x += red[q][0][ww];
+          o.y += red[q][1][ww];
+          o.z += red[q][2][ww];
+          o.w += red[q][3][ww];
+        }
+        o.x *= 2.0;
+        p.partials[p.partial_begin + (long long)rep * n_obs + oc] = o;
+      }
+      __syncthreads();
+    }
+  }
+}
+
 // A whole cycle for one replica per thread-block cluster: n_metro Metropolis
 // then n_or over-relaxation sweeps, each sweep 4 colour passes separated by a
 // cluster barrier, then (optionally) the observables partials of the final
@@ -832,65 +913,84 @@ __global__ void __launch_bounds__(kJ1CycleThreads, 1)
       cluster_barrier();
     }
   }
-  if (p.n_metro > 0) {
-    int v = acc;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0) warp_acc[threadIdx.x >> 5] = v;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int s = 0;
-      for (int w = 0; w < kJ1CycleThreads / 32; ++w) s += warp_acc[w];
-      if (s > 0) atomicAdd(p.pass.accepted + p.pass.temp_base + t, (unsigned long long)s);
+  cluster_cycle_tail(p, rep, rank, t, acc, red, warp_acc);
+}
+
+// The four colour-b sites of one cell in a fixed-L cluster cycle: loads
+// through L1 (coherent after the barrier's acquire), all four sites' loads
+// before the first store.
+template <bool kMetro, int kLog2L>
+__device__ __forceinline__ int cluster_fixed_cell(int b, const FixedCell<kLog2L>& c, int cell,
+                                                  float J1, float beta, float cosmax,
+                                                  const PassWords& w, uint32_t seed_lo,
+                                                  uint32_t seed_hi) {
+  switch (b) {
+    case 0:
+      return fixed_cell_sites<0, kMetro, kLog2L, kLdCoherent>(c, cell, J1, beta, cosmax, w,
+                                                              seed_lo, seed_hi);
+    case 1:
+      return fixed_cell_sites<1, kMetro, kLog2L, kLdCoherent>(c, cell, J1, beta, cosmax, w,
+                                                              seed_lo, seed_hi);
+    case 2:
+      return fixed_cell_sites<2, kMetro, kLog2L, kLdCoherent>(c, cell, J1, beta, cosmax, w,
+                                                              seed_lo, seed_hi);
+    default:
+      return fixed_cell_sites<3, kMetro, kLog2L, kLdCoherent>(c, cell, J1, beta, cosmax, w,
+                                                              seed_lo, seed_hi);
+  }
+}
+
+// The cluster cycle with L = 2^kLog2L fixed at compile time (isotropic J1,
+// L = 16 or 32): every colour pass in the cell form (a thread updates the
+// four sites of the colour in each of its cells, chunks of kJ1CycleThreads
+// cells dealt to the CTAs of the cluster), the fixed-L addressing, and loads
+// through L1: the cluster barrier between passes releases each CTA's stores
+// and acquires the others', so the memory model orders the next pass's loads
+// after them and the L1 serves the neighbour reuse within a pass. Same
+// updates in the same order per site as the per-pass kernels.
+template <int kLog2L>
+__global__ void __launch_bounds__(kJ1CycleThreads, 1)
+    j1_cycle_cluster_fixed_kernel(const J1CycleParams p) {
+  __shared__ double red[kJ1CycleThreads / kJ1Threads][4][kJ1Threads / 32];
+  __shared__ int warp_acc[kJ1CycleThreads / 32];
+  constexpr int L3 = FixedCell<kLog2L>::kL3;
+  const int csize = p.cluster_size;
+  const int rep = blockIdx.x / csize;
+  const int rank = blockIdx.x - rep * csize;
+  const int g = p.pass.rep_global + rep;
+  const int t = p.pass.temp_of_rep[p.pass.temp_base + g];
+  const float beta = p.pass.beta[p.pass.temp_base + t];
+  const float cosmax = p.pass.cosmax[p.pass.temp_base + t];
+  float4* rb = p.pass.spins + (long long)rep * 16 * L3;
+  const unsigned long long base =
+      (p.pass.sweep_ctr ? *p.pass.sweep_ctr : 0ull) + p.pass.sweep_off;
+  PassWords w;
+  w.rkey = (uint32_t)(p.pass.rep_key + rep);
+  int acc = 0;
+  const int n_sweeps = p.n_metro + p.n_or;
+  for (int k = 0; k < n_sweeps; ++k) {
+    const unsigned long long sweep = base + (unsigned long long)k;
+    w.renorm = p.pass.renorm_every > 0 &&
+               ((sweep + 1) % (unsigned long long)p.pass.renorm_every) == 0;
+    w.sw = (uint32_t)sweep;
+    const bool metro = k < p.n_metro;
+#pragma unroll 1
+    for (int b = 0; b < 4; ++b) {
+#pragma unroll 1
+      for (int cell = rank * kJ1CycleThreads + threadIdx.x; cell < L3;
+           cell += csize * kJ1CycleThreads) {
+        const FixedCell<kLog2L> c = fixed_cell<kLog2L>(rb, cell);
+        if (metro)
+          acc += cluster_fixed_cell<true, kLog2L>(b, c, cell, p.pass.J1, beta, cosmax, w,
+                                                  p.pass.seed_lo, p.pass.seed_hi);
+        else
+          cluster_fixed_cell<false, kLog2L>(b, c, cell, p.pass.J1, beta, cosmax, w,
+                                            p.pass.seed_lo, p.pass.seed_hi);
+      }
+      cluster_barrier();
     }
   }
-  if (p.partials) {
-    // Same 256-cell chunks and reduction order as j1_observables_kernel:
-    // thread group q of the CTA handles observables chunk oc.
-    constexpr int kGroups = kJ1CycleThreads / kJ1Threads;
-    const int q = threadIdx.x / kJ1Threads;
-    const int lt = threadIdx.x - q * kJ1Threads;
-    const int n_obs = (L3 + kJ1Threads - 1) / kJ1Threads;
-    for (int base_c = rank * kGroups; base_c < n_obs; base_c += csize * kGroups) {
-      const int oc = base_c + q;
-      const int cell = oc * kJ1Threads + lt;
-      double e = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
-      if (oc < n_obs && cell < L3) {
-        int x, y, z;
-        decode_cell(cell, L, rcpL, &x, &y, &z);
-        const CellFrame f = make_frame(x, y, z, L);
-        cell_corner<0, true>(rb, f, cell, L3, &e, &mx, &my, &mz);
-        cell_corner<1, true>(rb, f, cell, L3, &e, &mx, &my, &mz);
-        cell_corner<2, true>(rb, f, cell, L3, &e, &mx, &my, &mz);
-        cell_corner<3, true>(rb, f, cell, L3, &e, &mx, &my, &mz);
-        e *= p.J1_64;
-      }
-      e = warp_sum_d(e);
-      mx = warp_sum_d(mx);
-      my = warp_sum_d(my);
-      mz = warp_sum_d(mz);
-      const int w = lt >> 5, lane = lt & 31;
-      if (lane == 0) {
-        red[q][0][w] = e;
-        red[q][1][w] = mx;
-        red[q][2][w] = my;
-        red[q][3][w] = mz;
-      }
-      __syncthreads();
-      if (lt == 0 && oc < n_obs) {
-        double4 o = make_double4(0.0, 0.0, 0.0, 0.0);
-        for (int ww = 0; ww < kJ1Threads / 32; ++ww) {
-          o.x += red[q][0][ww];
-          o.y += red[q][1][ww];
-          o.z += red[q][2][ww];
-          o.w += red[q][3][ww];
-        }
-        o.x *= 2.0;
-        p.partials[p.partial_begin + (long long)rep * n_obs + oc] = o;
-      }
-      __syncthreads();
-    }
-  }
+  cluster_cycle_tail(p, rep, rank, t, acc, red, warp_acc);
 }
 
 
@@ -1281,11 +1381,15 @@ cudaError_t launch_j1_skew(const J1SkewParams& sp, int forms, cudaStream_t st) {
   return cudaLaunchKernelEx(&cfg, k[sp.w.pass.exch ? 1 : 0][forms & 3], sp);
 }
 
-cudaError_t j1_cycle_prepare(int cluster_size, int* max_active_clusters) {
-  *max_active_clusters = 0;
-  cudaError_t e = cudaFuncSetAttribute(j1_cycle_cluster_kernel,
-                                       cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-  if (e != cudaSuccess) return e;
+namespace {
+using CycleKernel = void (*)(const J1CycleParams);
+CycleKernel cycle_kernel_for(int log2L) {
+  if (log2L == 5) return j1_cycle_cluster_fixed_kernel<5>;
+  if (log2L == 4) return j1_cycle_cluster_fixed_kernel<4>;
+  return j1_cycle_cluster_kernel;
+}
+
+cudaError_t cycle_occupancy(void (*kern)(const J1CycleParams), int cluster_size, int* n) {
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1296,7 +1400,25 @@ cudaError_t j1_cycle_prepare(int cluster_size, int* max_active_clusters) {
   cfg.blockDim = dim3(kJ1CycleThreads, 1, 1);
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaOccupancyMaxActiveClusters(max_active_clusters, j1_cycle_cluster_kernel, &cfg);
+  return cudaOccupancyMaxActiveClusters(n, kern, &cfg);
+}
+}  // namespace
+
+cudaError_t j1_cycle_prepare(int cluster_size, int* max_active_clusters) {
+  *max_active_clusters = 0;
+  int least = 1 << 30;
+  for (int lg : {0, 4, 5}) {
+    const CycleKernel kern = cycle_kernel_for(lg);
+    cudaError_t e =
+        cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+    int n = 0;
+    e = cycle_occupancy(kern, cluster_size, &n);
+    if (e != cudaSuccess) return e;
+    least = std::min(least, n);
+  }
+  *max_active_clusters = least;
+  return cudaSuccess;
 }
 
 cudaError_t launch_j1_cycle(const J1CycleParams& p, cudaStream_t st) {
@@ -1312,7 +1434,7 @@ cudaError_t launch_j1_cycle(const J1CycleParams& p, cudaStream_t st) {
   cfg.stream = st;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, j1_cycle_cluster_kernel, p);
+  return cudaLaunchKernelEx(&cfg, cycle_kernel_for(j1_fixed_log2(p.pass)), p);
 }
 
 }  // namespace pyro

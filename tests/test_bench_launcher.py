@@ -41,3 +41,21 @@ def test_world_size_must_match_gpus():
     r = run(["--gpus", "2", "--dry-run"], {"WORLD_SIZE": "3", "RANK": "0"})
     assert r.returncode == 2
     assert "WORLD_SIZE=3" in r.stderr
+
+
+def test_step_profile_matches_the_timed_kernels_only():
+    """The committed step summary gives the issue and L2 figures for the
+    kernels it was measured on, and nothing for other kernel choices."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", BENCH)
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    desc = {"cycle_kernel": 0, "cluster_size": 16, "j1_kernel": 1, "replica_group": 4,
+            "chains": 2, "j1_site_mode": 1, "j1_fixed_l": 1, "autotune_choice": 4}
+    prof = bench.profiled_step(desc)
+    assert prof is not None
+    assert 1.0 < prof["warp_instructions_per_update"] < 10.0
+    assert 10.0 < prof["l2_bytes_per_update"] < 400.0
+    assert prof["l2_peak_gbs"] > 1000.0
+    assert bench.profiled_step(dict(desc, j1_fixed_l=0)) is None
+    assert bench.profiled_step(dict(desc, j1_site_mode=3)) is None

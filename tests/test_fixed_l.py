@@ -88,3 +88,30 @@ def test_fixed_L32_shard_against_oracle():
     o.cycle(1, 2, False, 2)
     assert np.array_equal(e.get_spins(), o.get_spins())
     assert np.array_equal(e.acceptance()[0], o.acceptance()[0])
+
+
+@pytest.mark.parametrize("L,cluster", [(16, 16), (16, 4), (32, 16), (32, 8), (32, 2)])
+def test_fixed_cluster_cycle_against_oracle(L, cluster):
+    """The cluster-resident cycle kernel with the fixed-L cell form (loads
+    through L1 between cluster barriers), chained with exchanges."""
+    temps = geometric_ladder(0.03, 1.8, 5)
+    s = System(L=L, temperatures=temps)
+    e = Engine([s], seed=2024 + L, renorm_every=4)
+    e.set_option(e.OPT_CYCLE_KERNEL, 1)
+    e.set_option(e.OPT_CLUSTER_SIZE, cluster)
+    assert e.get_option(e.OPT_CYCLE_KERNEL) == 1
+    o = Oracle([s], seed=2024 + L, renorm_every=4)
+    e.init_random()
+    o.init_random()
+    cones = np.linspace(-0.6, 0.9, len(temps)).astype(np.float32)
+    e.set_cone(cones)
+    o.set_cone(cones)
+    e.cycle(1, 4, True, 3)
+    o.cycle(1, 4, True, 3)
+    assert np.array_equal(e.get_spins(), o.get_spins()), "bit-exact contract"
+    assert np.array_equal(e.permutation(), o.permutation())
+    assert np.array_equal(e.acceptance()[0], o.acceptance()[0])
+    E0, M0 = e.last_observables()
+    E1, M1 = o.observables()
+    np.testing.assert_allclose(E0, E1, rtol=1e-12, atol=1e-9)
+    np.testing.assert_allclose(M0, M1, rtol=1e-12, atol=1e-9)
