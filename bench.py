@@ -727,23 +727,25 @@ STEP_PROFILE = os.path.join(ROOT, "profiles", "pt_step_L32_R64_instructions.md")
 
 def profiled_step(kernel_desc: dict):
     """Per-update figures of one step of the timed kernels, from the committed
-    ncu summary of those kernels (lines 'schedule: k=v ...',
+    ncu summary (blocks of lines 'schedule: k=v ...', then
     'warp_instructions_per_update: X', 'l2_bytes_per_update: Y',
-    'l2_peak_gbs: Z'); None when the summary is of other kernels."""
+    'l2_peak_gbs: Z'); None when no block is of the timed kernels."""
+    keys = ("warp_instructions_per_update", "l2_bytes_per_update", "l2_peak_gbs")
     try:
-        sched, vals = None, {}
+        blocks = []
         with open(STEP_PROFILE) as f:
             for line in f:
                 if line.startswith("schedule:"):
                     sched = dict(kv.split("=") for kv in line.split(":", 1)[1].split())
-                else:
-                    for key in ("warp_instructions_per_update", "l2_bytes_per_update",
-                                "l2_peak_gbs"):
+                    blocks.append((sched, {}))
+                elif blocks:
+                    for key in keys:
                         if line.startswith(key + ":"):
-                            vals[key] = float(line.split(":", 1)[1])
-        if sched and len(vals) == 3 and all(str(kernel_desc.get(k)) == v
-                                            for k, v in sched.items()):
-            return vals
+                            blocks[-1][1][key] = float(line.split(":", 1)[1])
+        for sched, vals in blocks:
+            if len(vals) == len(keys) and all(str(kernel_desc.get(k)) == v
+                                              for k, v in sched.items()):
+                return vals
     except (OSError, ValueError):
         pass
     return None

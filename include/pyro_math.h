@@ -55,14 +55,6 @@
 
 typedef struct { float x, y, z; } pyro_vec3;
 
-PYRO_HD uint32_t pyro_mulhi32(uint32_t a, uint32_t b) {
-#if defined(__CUDA_ARCH__)
-  return __umulhi(a, b);
-#else
-  return (uint32_t)(((uint64_t)a * (uint64_t)b) >> 32);
-#endif
-}
-
 PYRO_HD float pyro_u2f(uint32_t u) {
 #if defined(__CUDA_ARCH__)
   return __uint_as_float(u);
@@ -90,8 +82,10 @@ PYRO_HD void pyro_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
 #pragma unroll
 #endif
   for (int round = 0; round < 10; ++round) {
-    const uint32_t lo0 = 0xD2511F53u * c0, hi0 = pyro_mulhi32(0xD2511F53u, c0);
-    const uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = pyro_mulhi32(0xCD9E8D57u, c2);
+    /* each 32x32 -> 64-bit product once, both halves from it */
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+    const uint32_t lo0 = (uint32_t)p0, hi0 = (uint32_t)(p0 >> 32);
+    const uint32_t lo1 = (uint32_t)p1, hi1 = (uint32_t)(p1 >> 32);
     const uint32_t n0 = hi1 ^ c1 ^ k0;
     const uint32_t n2 = hi0 ^ c3 ^ k1;
     c0 = n0;

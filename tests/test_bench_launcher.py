@@ -57,5 +57,8 @@ def test_step_profile_matches_the_timed_kernels_only():
     assert 1.0 < prof["warp_instructions_per_update"] < 10.0
     assert 10.0 < prof["l2_bytes_per_update"] < 400.0
     assert prof["l2_peak_gbs"] > 1000.0
+    cell = bench.profiled_step(dict(desc, j1_site_mode=0))
+    assert cell is not None
+    assert cell["warp_instructions_per_update"] < prof["warp_instructions_per_update"]
     assert bench.profiled_step(dict(desc, j1_fixed_l=0)) is None
     assert bench.profiled_step(dict(desc, j1_site_mode=3)) is None
