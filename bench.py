@@ -363,7 +363,13 @@ def run_batched(args):
     eng.init_random()
     for k, sy in enumerate(systems):
         eng.set_cone(np.full(len(sy.temperatures), 0.3, dtype=np.float32), k)
-    choice = eng.autotune(1, 4, 2)
+    if args.kernel == "wave":
+        # the work-queue launch over every system (one per cycle)
+        eng.set_option(eng.OPT_CYCLE_KERNEL, 2)
+        eng.set_option(eng.OPT_GROUP_MB, args.group_mb or 0)
+        choice = None
+    else:
+        choice = eng.autotune(1, 4, 2)
     eng.cycle(1, 4, True, args.warmup)
     steps = args.steps if args.steps != 300 else 20
     sec = _timed(stream, lambda: eng.cycle(1, 4, True, steps))
@@ -824,6 +830,9 @@ def main():
     ap.add_argument("--site-mode", type=int, default=None,
                     help="J1 pass forms (bit 0 Metropolis, bit 1 over-relaxation one site "
                          "per thread) for --kernel grouped / wave (wave default 3)")
+    ap.add_argument("--group-mb", type=int, default=None,
+                    help="--workload batched --kernel wave: MB of spins per work-queue group "
+                         "(0: one group)")
     ap.add_argument("--cluster-size", type=int, default=None,
                     help="CTAs per cluster of --kernel cluster (default: the engine's)")
     ap.add_argument("--fixed-l", type=int, default=1, choices=[0, 1],

@@ -24,7 +24,7 @@ CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libpyro.so")
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 
-ENGINE_SOURCES = ["kernels.cu", "j1_kernels.cu", "far_kernels.cu", "sq_kernels.cu", "tet_mlp.cu", "smem_kernels.cu",
+ENGINE_SOURCES = ["kernels.cu", "j1_kernels.cu", "far_kernels.cu", "gen_wave.cu", "sq_kernels.cu", "tet_mlp.cu", "smem_kernels.cu",
                   "capi.cu",
                   "tet_capi.cu", "checkpoint.cu", "lattice.cpp", "noalloc.cu", "exchange.cu", "order.cu", "tet_umma.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

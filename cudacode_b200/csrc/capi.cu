@@ -255,6 +255,146 @@ int queue_wave(pyro_ctx* ctx, int n_metro, int n_or, bool with_obs) {
   return PYRO_OK;
 }
 
+// The work-queue kernel of 16-colour systems runs, with PYRO_OPT_CYCLE_KERNEL
+// 2, the systems off the nearest-neighbour path when every one of them is an
+// isotropic 16-colour system (J2 or J3 set, no bond matrices).
+bool use_gen_wave(const pyro_ctx* ctx, int n_metro, int n_or, int n_tet) {
+  if (ctx->cycle_kernel != 2 || n_tet != 0 || n_metro + n_or <= 0) return false;
+  bool any = false;
+  for (int i = 0; i < (int)ctx->sys.size(); ++i) {
+    if (std::find(ctx->j1_sys.begin(), ctx->j1_sys.end(), i) != ctx->j1_sys.end()) continue;
+    const SysDev& s = ctx->sys[i];
+    if (s.n_colours != 16 || s.exch >= 0) return false;
+    any = true;
+  }
+  return any;
+}
+
+// Units (system, replica) of the 16-colour systems in groups of about
+// PYRO_OPT_GROUP_MB MB of spins (one group when 0), their progress counters
+// and the queue (allocated outside any capture).
+int prepare_gen_wave(pyro_ctx* ctx) {
+  std::vector<GenWaveUnit> units;
+  std::vector<GenWaveGroup> groups;
+  const double budget = ctx->gen_group_mb > 0 ? (double)ctx->gen_group_mb * 1048576.0 : 1e300;
+  double bytes = 0.0;
+  int prog = 0;
+  for (int i = 0; i < (int)ctx->sys.size(); ++i) {
+    if (std::find(ctx->j1_sys.begin(), ctx->j1_sys.end(), i) != ctx->j1_sys.end()) continue;
+    const SysDev& s = ctx->sys[i];
+    const double per_rep = 16.0 * 16.0 * s.L3;
+    const int nq = (s.L3 + kPassThreads - 1) / kPassThreads;
+    for (int r = 0; r < s.n_rep; ++r) {
+      if (groups.empty() || (bytes > 0.0 && bytes + per_rep > budget)) {
+        GenWaveGroup g;
+        g.unit_begin = (int)units.size();
+        g.n_units = 0;
+        g.chunks = 0;
+        g.chunk_prefix = 0;
+        groups.push_back(g);
+        bytes = 0.0;
+      }
+      GenWaveGroup& g = groups.back();
+      GenWaveUnit u;
+      u.sys = i;
+      u.rep = r;
+      u.n_chunks = nq;
+      u.dep = (2 * s.L * s.L + kPassThreads - 1) / kPassThreads + 1;
+      u.prog_off = prog;
+      u.chunk_begin = g.chunks;
+      units.push_back(u);
+      g.n_units += 1;
+      g.chunks += nq;
+      prog += nq;
+      bytes += per_rep;
+    }
+  }
+  if (units.empty()) return fail(ctx, PYRO_ERR_STATE, "work queue: no 16-colour systems");
+  if (units.size() > ctx->gwave_units_cap) {
+    if (ctx->d_gwave_units) cudaFree(ctx->d_gwave_units);
+    ctx->d_gwave_units = nullptr;
+    ctx->gwave_units_cap = 0;
+    PYRO_CK(alloc(&ctx->d_gwave_units, units.size()));
+    ctx->gwave_units_cap = units.size();
+  }
+  if (groups.size() > ctx->gwave_groups_cap) {
+    if (ctx->d_gwave_groups) cudaFree(ctx->d_gwave_groups);
+    ctx->d_gwave_groups = nullptr;
+    ctx->gwave_groups_cap = 0;
+    PYRO_CK(alloc(&ctx->d_gwave_groups, groups.size()));
+    ctx->gwave_groups_cap = groups.size();
+  }
+  const size_t words = kWaveTicketWords + (size_t)prog;
+  if (words > ctx->gwave_words) {
+    if (ctx->d_gwave) cudaFree(ctx->d_gwave);
+    ctx->d_gwave = nullptr;
+    ctx->gwave_words = 0;
+    PYRO_CK(alloc(&ctx->d_gwave, words));
+    ctx->gwave_words = words;
+  }
+  long long chunks = 0;
+  for (auto& g : groups) {
+    g.chunk_prefix = (int)chunks;
+    chunks += g.chunks;
+  }
+  std::vector<int> chunk_unit;
+  chunk_unit.reserve((size_t)chunks);
+  for (int ui = 0; ui < (int)units.size(); ++ui)
+    for (int q = 0; q < units[ui].n_chunks; ++q) chunk_unit.push_back(ui);
+  if (chunk_unit.size() > ctx->gwave_chunk_cap) {
+    if (ctx->d_gwave_chunk_unit) cudaFree(ctx->d_gwave_chunk_unit);
+    ctx->d_gwave_chunk_unit = nullptr;
+    ctx->gwave_chunk_cap = 0;
+    PYRO_CK(alloc(&ctx->d_gwave_chunk_unit, chunk_unit.size()));
+    ctx->gwave_chunk_cap = chunk_unit.size();
+  }
+  PYRO_CK(cudaMemcpy(ctx->d_gwave_chunk_unit, chunk_unit.data(), sizeof(int) * chunk_unit.size(),
+                     cudaMemcpyHostToDevice));
+  ctx->gwave_n_groups = (int)groups.size();
+  ctx->gwave_chunks = chunks;
+  PYRO_CK(cudaMemcpy(ctx->d_gwave_units, units.data(), sizeof(GenWaveUnit) * units.size(),
+                     cudaMemcpyHostToDevice));
+  PYRO_CK(cudaMemcpy(ctx->d_gwave_groups, groups.data(), sizeof(GenWaveGroup) * groups.size(),
+                     cudaMemcpyHostToDevice));
+  if (!ctx->d_wave_status) {
+    PYRO_CK(cudaHostAlloc((void**)&ctx->h_wave_status, sizeof(int), cudaHostAllocDefault));
+    *ctx->h_wave_status = 0;
+    PYRO_CK(alloc(&ctx->d_wave_status, 1));
+    PYRO_CK(cudaMemset(ctx->d_wave_status, 0, sizeof(int)));
+  }
+  return PYRO_OK;
+}
+
+// One work-queue launch for the 16-colour systems: n_metro + n_or sweeps
+// (their energies come from the observables kernel after it).
+int queue_gen_wave(pyro_ctx* ctx, int n_metro, int n_or) {
+  if (!ctx->d_gwave || !ctx->d_wave_status) return fail(ctx, PYRO_ERR_STATE, "work queue not prepared");
+  const long long item = 16ll * (n_metro + n_or) * ctx->gwave_chunks;
+  if (item > 0x7fffffffll) return fail(ctx, PYRO_ERR_ARG, "work-queue kernel: too many items");
+  PYRO_CK(cudaMemsetAsync(ctx->d_gwave, 0, ctx->gwave_words * sizeof(unsigned int), ctx->stream));
+  GenWaveParams w;
+  std::memset(&w, 0, sizeof w);
+  w.pass = pass_params(ctx, 0);
+  w.pass.segs = nullptr;
+  w.pass.nseg = 0;
+  w.pass.sweep_off = 0;
+  w.pass.pdl = 0;
+  w.units = ctx->d_gwave_units;
+  w.groups = ctx->d_gwave_groups;
+  w.chunk_unit = ctx->d_gwave_chunk_unit;
+  w.n_groups = ctx->gwave_n_groups;
+  w.n_metro = n_metro;
+  w.n_or = n_or;
+  w.queue = ctx->d_gwave;
+  w.progress = ctx->d_gwave + kWaveTicketWords;
+  w.status = ctx->d_wave_status;
+  w.n_items = (int)item;
+  w.spin_limit = ctx->wave_stall_item >= 0 ? 4096u : (1u << 20);
+  w.stall_item = ctx->wave_stall_item;
+  PYRO_CK(launch_gen_wave(w, ctx->stream));
+  return PYRO_OK;
+}
+
 // The skewed multi-group launches run the J1 systems of a cycle without
 // learned sweeps.
 bool use_skew_kernel(const pyro_ctx* ctx, int n_metro, int n_or, int n_tet) {
@@ -460,15 +600,22 @@ int queue_cycle_body(pyro_ctx* ctx, int n_metro, int n_or, bool with_obs, int n_
   int rc = check_cluster(ctx);
   if (rc) return rc;
   const bool skew = use_skew_kernel(ctx, n_metro, n_or, n_tet);
-  if (skew || use_wave_kernel(ctx, n_metro, n_or, n_tet)) {
-    // other systems on their usual kernels, then the J1 systems' launches
-    if (!ctx->gen_groups.empty())
+  const bool j1_wave = use_wave_kernel(ctx, n_metro, n_or, n_tet);
+  const bool gen_wave = use_gen_wave(ctx, n_metro, n_or, n_tet);
+  if (skew || j1_wave || gen_wave) {
+    // the 16-colour systems in their work-queue launch, or the other systems
+    // on their usual kernels; then the J1 systems' launches
+    if (gen_wave)
+      rc = queue_gen_wave(ctx, n_metro, n_or);
+    else if (!ctx->gen_groups.empty())
       rc = queue_grouped(ctx, n_metro, n_or, false, true, with_obs, 0);
     else
       rc = queue_generic_sweeps(ctx, n_metro, n_or);
-    if (rc == PYRO_OK)
+    if (rc == PYRO_OK && (skew || j1_wave))
       rc = skew ? queue_skew(ctx, n_metro, n_or, with_obs) : queue_wave(ctx, n_metro, n_or, with_obs);
-    if (rc == PYRO_OK && with_obs) rc = queue_observables(ctx, /*skip_j1=*/true);
+    else if (rc == PYRO_OK && !ctx->j1_sys.empty())
+      rc = PYRO_ERR_STATE;  // J1 systems take the J1 work queue whenever the 16-colour ones do
+    if (rc == PYRO_OK && with_obs) rc = queue_observables(ctx, /*skip_j1=*/skew || j1_wave);
     return rc;
   }
   const bool cyc = use_cycle_kernel(ctx);
@@ -598,7 +745,8 @@ void free_all(pyro_ctx* c) {
                   c->d_sq_s1,       c->d_sq_s2,        c->d_sq_tw,
                   c->d_sq_out,      c->d_exch,         c->d_submag,      c->d_order,
                   c->d_wave,        c->d_wave_status,  c->d_snap,        c->d_snap_temp_of_rep,
-                  c->d_snap_rep_of_temp, c->d_snap_energy, c->d_snap_mag};
+                  c->d_snap_rep_of_temp, c->d_snap_energy, c->d_snap_mag,
+                  c->d_gwave_units, c->d_gwave_groups, c->d_gwave, c->d_gwave_chunk_unit};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->snap_stream) cudaStreamDestroy(c->snap_stream);
@@ -614,6 +762,11 @@ void free_all(pyro_ctx* c) {
   c->d_wave = nullptr;
   c->d_wave_status = nullptr;
   c->wave_words = 0;
+  c->d_gwave_units = nullptr;
+  c->d_gwave_groups = nullptr;
+  c->d_gwave = nullptr;
+  c->d_gwave_chunk_unit = nullptr;
+  c->gwave_units_cap = c->gwave_groups_cap = c->gwave_words = c->gwave_chunk_cap = 0;
   for (auto* p : c->d_pass_segs)
     if (p) cudaFree(p);
   c->d_pass_segs.clear();
@@ -1164,7 +1317,10 @@ int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen)
     const int base = vs.size();  // filled with the best J1 knobs after stage 1
     const Variant gv[] = {{1, 0, 16, 1, 0, 1, 0},  {1, 0, 16, 1, 0, 1, 24}, {1, 0, 16, 1, 0, 1, 40},
                           {1, 0, 16, 1, 0, 1, 64}, {1, 0, 16, 1, 0, 2, 24}, {1, 0, 16, 1, 0, 2, 40},
-                          {1, 0, 16, 1, 0, 3, 24}};
+                          {1, 0, 16, 1, 0, 3, 24},
+                          // the work queue over every 16-colour system (contexts without J1
+                          // systems: with them, stage 2 keeps the J1 winner's cycle kernel)
+                          {1, 2, 16, 1, 0, 1, 0},  {1, 2, 16, 1, 0, 1, 24}, {1, 2, 16, 1, 0, 1, 64}};
     vs.insert(vs.end(), std::begin(gv), std::end(gv));
     (void)base;
   }
@@ -1797,6 +1953,7 @@ static int run_cycles(pyro_ctx* ctx, int n_metro, int n_or, int n_tet, int do_sw
     int rc = check_cluster(ctx);  // sets kernel attributes: not inside a capture
     if (rc) return rc;
     if (use_wave_kernel(ctx, n_metro, n_or, n_tet) && (rc = prepare_wave(ctx))) return rc;
+    if (use_gen_wave(ctx, n_metro, n_or, n_tet) && (rc = prepare_gen_wave(ctx))) return rc;
     PYRO_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     ctx->defer_finalise = true;  // the exchange kernel below finalises the observables
     if (n_tet == 0) {

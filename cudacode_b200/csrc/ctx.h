@@ -11,6 +11,7 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include "../../include/pyro.h"
+#include "gen_wave.cuh"
 #include "kernels.cuh"
 #include "lattice.h"
 
@@ -90,6 +91,17 @@ struct pyro_ctx {
   int* d_wave_status = nullptr;
   int* h_wave_status = nullptr;  // pinned copy, read after a synchronising call
   int wave_stall_item = -1;
+  // Work-queue kernel of the 16-colour systems (same option): its units and
+  // groups, and a queue ticket (padded) plus one progress counter per (unit,
+  // chunk), zeroed before each launch.
+  pyro::GenWaveUnit* d_gwave_units = nullptr;
+  pyro::GenWaveGroup* d_gwave_groups = nullptr;
+  int* d_gwave_chunk_unit = nullptr;
+  size_t gwave_chunk_cap = 0;
+  unsigned int* d_gwave = nullptr;
+  size_t gwave_units_cap = 0, gwave_groups_cap = 0, gwave_words = 0;
+  int gwave_n_groups = 0;
+  long long gwave_chunks = 0;  // chunks of one pass over every unit
   int smem_kernel = 1;
   int rep_group = 0;    // per-pass J1 kernels over groups of this many replicas (0: all)
   int gen_group_mb = 0; // generic kernels over groups of replicas of about this many MB (0: off)

@@ -17,64 +17,10 @@
 
 #include "../../include/pyro_math.h"
 #include "far_kernels.cuh"
+#include "far_update.cuh"
 
 namespace pyro {
 namespace {
-
-struct Frame3 {
-  int zo[3], yo[3], xo[3];
-};
-
-__device__ __forceinline__ Frame3 frame_of(int cell, int L, float rcpL) {
-  int q = (int)((float)cell * rcpL);
-  int r = cell - q * L;
-  if (r < 0) { --q; r += L; } else if (r >= L) { ++q; r -= L; }
-  int q2 = (int)((float)q * rcpL);
-  int r2 = q - q2 * L;
-  if (r2 < 0) { --q2; r2 += L; } else if (r2 >= L) { ++q2; r2 -= L; }
-  const int x = r, y = r2, z = q2, L2 = L * L;
-  Frame3 f;
-  f.xo[0] = x == 0 ? L - 1 : x - 1;
-  f.xo[1] = x;
-  f.xo[2] = x == L - 1 ? 0 : x + 1;
-  f.yo[0] = (y == 0 ? L - 1 : y - 1) * L;
-  f.yo[1] = y * L;
-  f.yo[2] = (y == L - 1 ? 0 : y + 1) * L;
-  f.zo[0] = (z == 0 ? L - 1 : z - 1) * L2;
-  f.zo[1] = z * L2;
-  f.zo[2] = (z == L - 1 ? 0 : z + 1) * L2;
-  return f;
-}
-
-template <int S, int K>
-__device__ __forceinline__ float4 nb(const float4* __restrict__ rep, const Frame3& f, int L3) {
-  constexpr NbrEntry e = far_neighbour(S, K);
-  static_assert(e.t >= 0, "neighbour table");
-  return __ldg(rep + f.zo[e.dz + 1] + f.yo[e.dy + 1] + f.xo[e.dx + 1] + e.t * L3);
-}
-
-// Sum of neighbours K0..K1-1 of site S in canonical order (first value, then
-// left-to-right adds), as shell_sum of the generic kernel.
-template <int S, int K, int K1>
-__device__ __forceinline__ void add_rest(const float4* __restrict__ rep, const Frame3& f, int L3,
-                                         float3& a) {
-  if constexpr (K < K1) {
-    const float4 v = nb<S, K>(rep, f, L3);
-    a.x = a.x + v.x;
-    a.y = a.y + v.y;
-    a.z = a.z + v.z;
-    add_rest<S, K + 1, K1>(rep, f, L3, a);
-  }
-}
-
-template <int S, int K0, int K1>
-__device__ __forceinline__ float3 shell_sum_c(const float4* __restrict__ rep, const Frame3& f,
-                                              int L3) {
-  const float4 v0 = nb<S, K0>(rep, f, L3);
-  float3 a = make_float3(v0.x, v0.y, v0.z);
-  add_rest<S, K0 + 1, K1>(rep, f, L3, a);
-  return a;
-}
 
 template <typename Seg>
 __device__ __forceinline__ int find_seg(const Seg* segs, int nseg, int block) {
@@ -100,59 +46,12 @@ __global__ void __launch_bounds__(kFarThreads) far_pass_kernel(const PassParams 
   const int rep_in_seg = rel / sg.blocks_per_rep;
   const int rep = sg.rep_begin + rep_in_seg;
   const int cell = (rel - rep_in_seg * sg.blocks_per_rep) * kFarThreads + threadIdx.x;
-  const int L3 = sd.L3;
   int accepted = 0;
   int tslot = 0;
   if (kMetro) tslot = p.temp_of_rep[sd.temp_base + sd.rep_global + rep];
-  if (cell < L3) {
-    const Frame3 fr = frame_of(cell, sd.L, sd.rcpL);
-    float4* rb = p.spins + sd.spin_off + (long long)rep * 16 * L3;
-    const int own = S * L3 + cell;
-    const float3 a1 = shell_sum_c<S, 0, 6>(rb, fr, L3);
-    pyro_vec3 h;
-    h.x = sd.J1 * a1.x;
-    h.y = sd.J1 * a1.y;
-    h.z = sd.J1 * a1.z;
-    if (sd.shells & 2) {
-      const float3 a = shell_sum_c<S, 6, 18>(rb, fr, L3);
-      h.x = fmaf(sd.J2, a.x, h.x);
-      h.y = fmaf(sd.J2, a.y, h.y);
-      h.z = fmaf(sd.J2, a.z, h.z);
-    }
-    if (sd.shells & 4) {
-      const float3 a = shell_sum_c<S, 18, 24>(rb, fr, L3);
-      h.x = fmaf(sd.J3a, a.x, h.x);
-      h.y = fmaf(sd.J3a, a.y, h.y);
-      h.z = fmaf(sd.J3a, a.z, h.z);
-    }
-    if (sd.shells & 8) {
-      const float3 a = shell_sum_c<S, 24, 30>(rb, fr, L3);
-      h.x = fmaf(sd.J3b, a.x, h.x);
-      h.y = fmaf(sd.J3b, a.y, h.y);
-      h.z = fmaf(sd.J3b, a.z, h.z);
-    }
-    const float4 sv = rb[own];
-    pyro_vec3 sp;
-    sp.x = sv.x;
-    sp.y = sv.y;
-    sp.z = sv.z;
+  if (cell < sd.L3) {
     const unsigned long long sweep = (p.sweep_ctr ? *p.sweep_ctr : 0ull) + p.sweep_off;
-    pyro_vec3 out;
-    if (kMetro) {
-      const float beta = p.beta[sd.temp_base + tslot];
-      const float cosmax = p.cosmax[sd.temp_base + tslot];
-      uint32_t r[4];
-      pyro_philox((uint32_t)own, (uint32_t)(sd.rep_key + rep), (uint32_t)sweep, PYRO_PURPOSE_METRO,
-                  p.seed_lo, p.seed_hi, r);
-      const pyro_vec3 prop = pyro_cone_proposal(sp, cosmax, pyro_uniform(r[0]), pyro_uniform(r[1]));
-      accepted = pyro_metropolis_accept(pyro_delta_e(h, sp, prop), beta, pyro_uniform(r[2]));
-      out = accepted ? prop : sp;
-    } else {
-      out = pyro_overrelax(sp, h);
-    }
-    if (p.renorm_every > 0 && ((sweep + 1) % (unsigned long long)p.renorm_every) == 0)
-      out = pyro_renormalise(out);
-    rb[own] = make_float4(out.x, out.y, out.z, 0.0f);
+    accepted = far::site_update<S, kMetro>(p, sd, rep, cell, sweep, tslot);
   }
   if (kMetro) {
     const int n = __syncthreads_count(accepted);

@@ -86,7 +86,12 @@ int pyro_neighbour_table(int site, int* out120);
  * the chunks that hold its neighbours (per-chunk counters, released and
  * acquired at GPU scope, every wait bounded; a wait that runs out makes the
  * next pyro_synchronize return PYRO_ERR_TIMEOUT). PYRO_OPT_J1_SITE_MODE
- * chooses its pass forms. 3 runs them as skewed launches: replica group g
+ * chooses its pass forms. With 2, when every other system is an isotropic
+ * 16-colour system (J2 or J3 set), their sweeps of a pyro_cycle run as one
+ * more work-queue launch over all of them: units (system, replica) in
+ * groups of about PYRO_OPT_GROUP_MB MB (0: one group), items of one 16-colour
+ * pass of a 256-cell chunk, the same waits and bounds; their energies come
+ * from the observables kernel after it. 3 runs them as skewed launches: replica group g
  * (PYRO_OPT_REPLICA_GROUP replicas, 0 = 2) runs its pass k in launch
  * s g + k, with s chosen so that about PYRO_OPT_CHAINS groups are in flight
  * in every launch; a launch's items belong to different replicas and need

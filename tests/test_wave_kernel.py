@@ -153,3 +153,84 @@ def test_skewed_launches_bit_exact(L, R, forms, group, in_flight, n_metro, n_or)
     E1, M1 = o.observables()
     np.testing.assert_allclose(E0, E1, rtol=1e-12, atol=1e-9)
     np.testing.assert_allclose(M0, M1, rtol=1e-12, atol=1e-9)
+
+
+def batched_16_colour(n=5, seed=3):
+    rng = np.random.default_rng(seed)
+    systems = []
+    for i in range(n):
+        L = int(rng.choice([4, 6, 9, 12, 16]))
+        R = int(rng.integers(2, 5))
+        systems.append(System(L=L, temperatures=geometric_ladder(0.05, 1.5, R),
+                              J2=float(rng.uniform(-0.1, 0.1)), J3=float(rng.uniform(-0.1, 0.1))))
+    return systems
+
+
+@pytest.mark.parametrize("group_mb,n_metro,n_or", [(0, 1, 2), (1, 1, 3), (3, 2, 1), (0, 0, 2)])
+def test_work_queue_of_16_colour_systems_bit_exact(group_mb, n_metro, n_or):
+    """The batched 16-colour systems as one work-queue launch per cycle:
+    uneven L (one chunk per replica up to 16 chunks with a dependency window
+    narrower than the replica), groups of about group_mb MB, against the
+    oracle bit for bit."""
+    systems = batched_16_colour()
+    e, o = pair(systems, seed=31, renorm_every=3)
+    e.set_option(e.OPT_CYCLE_KERNEL, 2)
+    e.set_option(e.OPT_GROUP_MB, group_mb)
+    e.init_random()
+    o.init_random()
+    for k, sy in enumerate(systems):
+        c = np.linspace(-0.6, 0.8, len(sy.temperatures)).astype(np.float32)
+        e.set_cone(c, k)
+        o.set_cone(c, k)
+    e.cycle(n_metro, n_or, True, 3)
+    o.cycle(n_metro, n_or, True, 3)
+    for k in range(len(systems)):
+        assert np.array_equal(e.get_spins(k), o.get_spins(k)), k
+        assert np.array_equal(e.permutation(k), o.permutation(k)), k
+        assert np.array_equal(e.acceptance(k)[0], o.acceptance(k)[0]), k
+        np.testing.assert_allclose(e.last_observables(k)[0], o.observables(k)[0], rtol=1e-12,
+                                   atol=1e-9)
+
+
+def test_work_queue_skips_contexts_with_bond_matrix_systems():
+    """An anisotropic system off the nearest-neighbour path keeps the 16-colour
+    systems on their per-pass kernels: same chains."""
+    systems = batched_16_colour(3, seed=9)
+    e, o = pair(systems, seed=4)
+    sym = np.array([[0.1, 0.02, 0.0], [0.02, -0.05, 0.01], [0.0, 0.01, 0.03]])
+    A = np.tile(np.eye(3), (4, 4, 1, 1)) + sym
+    e.set_exchange(A, system=1)
+    o.set_exchange(A, system=1)
+    e.set_option(e.OPT_CYCLE_KERNEL, 2)
+    e.init_random()
+    o.init_random()
+    e.cycle(1, 1, True, 2)
+    o.cycle(1, 1, True, 2)
+    for k in range(len(systems)):
+        assert np.array_equal(e.get_spins(k), o.get_spins(k)), k
+
+
+def test_work_queue_of_16_colour_systems_wait_that_runs_out(tmp_path):
+    systems = batched_16_colour(3, seed=12)
+    e, o = pair(systems, seed=23)
+    e.set_option(e.OPT_CYCLE_KERNEL, 2)
+    e.init_random()
+    o.init_random()
+    e.cycle(1, 1, True, 1)
+    o.cycle(1, 1, True, 1)
+    ck = str(tmp_path / "before.ck")
+    e.save_checkpoint(ck)
+    # item 1 (a pass-0 item) never reports completion: the pass-1 items that
+    # need its chunk give up after 4096 polls
+    e.set_option(e.OPT_WAVE_STALL, 1)
+    e.cycle(1, 1, True, 1)
+    with pytest.raises(PyroError) as err:
+        e.synchronize()
+    assert err.value.code == PYRO_ERR_TIMEOUT
+    e.synchronize()
+    e.set_option(e.OPT_WAVE_STALL, -1)
+    e.load_checkpoint(ck)
+    e.cycle(1, 1, True, 2)
+    o.cycle(1, 1, True, 2)
+    for k in range(len(systems)):
+        assert np.array_equal(e.get_spins(k), o.get_spins(k)), k
