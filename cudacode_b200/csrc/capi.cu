@@ -1722,6 +1722,57 @@ int pyro_last_observables(pyro_ctx* ctx, int system, double* energy, double* mag
   return wave_status_result(ctx);
 }
 
+namespace {
+// True for page-locked host memory that the device can copy from or to
+// asynchronously.
+bool pinned_host(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+}  // namespace
+
+int pyro_set_cone_async(pyro_ctx* ctx, int system, const float* pinned_cosmax) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (system < 0 || system >= (int)ctx->sys.size() || !pinned_cosmax)
+    return fail(ctx, PYRO_ERR_ARG, "set_cone_async: bad system or null pointer");
+  PYRO_CK(cudaSetDevice(ctx->device));
+  if (!pinned_host(pinned_cosmax))
+    return fail(ctx, PYRO_ERR_ARG, "set_cone_async: the buffer is not pinned host memory");
+  const SysDev& s = ctx->sys[system];
+  for (int t = 0; t < s.n_temp; ++t)
+    if (!(pinned_cosmax[t] >= -1.0f && pinned_cosmax[t] < 1.0f))
+      return fail(ctx, PYRO_ERR_ARG, "set_cone_async: cos(theta_max) must lie in [-1, 1)");
+  PYRO_CK(cudaMemcpyAsync(ctx->d_cosmax + s.temp_base, pinned_cosmax, sizeof(float) * s.n_temp,
+                          cudaMemcpyHostToDevice, ctx->stream));
+  return PYRO_OK;
+}
+
+int pyro_last_observables_async(pyro_ctx* ctx, int system, double* pinned_energy,
+                                double* pinned_magnetisation3) {
+  if (!ctx) return PYRO_ERR_ARG;
+  if (system < 0 || system >= (int)ctx->sys.size())
+    return fail(ctx, PYRO_ERR_ARG, "last_observables_async: bad system");
+  if (ctx->measure_snapshot)
+    return fail(ctx, PYRO_ERR_STATE, "last_observables_async: not in the snapshot mode");
+  PYRO_CK(cudaSetDevice(ctx->device));
+  if ((pinned_energy && !pinned_host(pinned_energy)) ||
+      (pinned_magnetisation3 && !pinned_host(pinned_magnetisation3)))
+    return fail(ctx, PYRO_ERR_ARG, "last_observables_async: a buffer is not pinned host memory");
+  const SysDev& s = ctx->sys[system];
+  if (pinned_energy)
+    PYRO_CK(cudaMemcpyAsync(pinned_energy, ctx->d_energy + s.rep_ctx_base,
+                            sizeof(double) * s.n_rep, cudaMemcpyDeviceToHost, ctx->stream));
+  if (pinned_magnetisation3)
+    PYRO_CK(cudaMemcpyAsync(pinned_magnetisation3, ctx->d_mag + 3 * s.rep_ctx_base,
+                            sizeof(double) * 3 * s.n_rep, cudaMemcpyDeviceToHost, ctx->stream));
+  return PYRO_OK;
+}
+
 int pyro_observables(pyro_ctx* ctx, int system, double* energy, double* magnetisation3) {
   NvtxRange nvtx_range("pyro_observables");
   if (!ctx) return PYRO_ERR_ARG;

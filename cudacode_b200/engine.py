@@ -133,6 +133,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "pyro_tet_forward": (i, [P, pf, i, pf]),
         "pyro_tet_forward_device": (i, [P, C.c_void_p, i, C.c_void_p]),
         "pyro_last_observables_device": (i, [P, i, C.c_void_p, C.c_void_p]),
+        "pyro_set_cone_async": (i, [P, i, C.c_void_p]),
+        "pyro_last_observables_async": (i, [P, i, C.c_void_p, C.c_void_p]),
         "pyro_last_observables": (i, [P, i, pd, pd]),
         "pyro_tet_set_forward": (i, [P, i]),
         "pyro_tet_gradient": (i, [P, pf, pf, i, pf, pd]),
@@ -484,6 +486,26 @@ class Engine:
         self._ck(self.lib.pyro_last_observables(self.ctx, system, _ptr(e, C.c_double),
                                                 _ptr(m, C.c_double)))
         return e, m
+
+    def set_cone_async(self, pinned_cosmax, system: int = 0) -> None:
+        """Queue the cone widths from pinned host memory (a float32 array of
+        the system's temperatures, e.g. a pinned torch tensor's numpy view);
+        it must stay unchanged until synchronize() returns."""
+        a = pinned_cosmax
+        if a.dtype != np.float32 or not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("set_cone_async: a contiguous float32 array is needed")
+        self._ck(self.lib.pyro_set_cone_async(self.ctx, system, a.ctypes.data))
+
+    def last_observables_async(self, pinned_energy, pinned_mag=None, system: int = 0) -> None:
+        """Queue the copy of the last cycle's energies (and magnetisations) to
+        pinned host arrays (float64, n and (n, 3)); read them after
+        synchronize()."""
+        for a in (pinned_energy, pinned_mag):
+            if a is not None and (a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]):
+                raise ValueError("last_observables_async: contiguous float64 arrays are needed")
+        self._ck(self.lib.pyro_last_observables_async(
+            self.ctx, system, pinned_energy.ctypes.data,
+            None if pinned_mag is None else pinned_mag.ctypes.data))
 
     def last_observables_device(self, e_ptr: int, m_ptr: int = 0, system: int = 0) -> None:
         """Energies (and magnetisations) of the last cycle, without recomputing."""

@@ -265,6 +265,17 @@ int pyro_last_observables_device(pyro_ctx* ctx, int system, double* dev_energy,
 /* The same to host memory (synchronous). */
 int pyro_last_observables(pyro_ctx* ctx, int system, double* energy, double* magnetisation3);
 
+/* Stream-ordered forms with host buffers, for drivers that queue the next
+ * step before reading the last one: the copy is queued on the context's
+ * stream and the call returns at once. The buffers must be pinned host
+ * memory (cudaHostAlloc or cudaHostRegister; else PYRO_ERR_ARG); the cone
+ * widths are checked when the call is made and must not change, and the
+ * observables must not be read, until pyro_synchronize has returned. Not in
+ * the PYRO_OPT_MEASURE_SNAPSHOT mode (PYRO_ERR_STATE). */
+int pyro_set_cone_async(pyro_ctx* ctx, int system, const float* pinned_cosmax);
+int pyro_last_observables_async(pyro_ctx* ctx, int system, double* pinned_energy,
+                                double* pinned_magnetisation3);
+
 /* Temperatures. temperature_of_replica: T of each configuration slot (the
  * reference's permuted `Temperatures` vector); replica_of_temperature: the
  * inverse map. Global indices (all n_temperatures entries). */
