@@ -713,7 +713,22 @@ def learned_leg(cycles: int = 60000, warmup: int = 2000) -> dict:
         return out
 
     plain = chain(3, 1, 0)
+    # the learned cycle at its own best replica grouping (the autotuner times
+    # plain cycles only): a few groupings timed on untimed warm-up cycles;
+    # every grouping gives the same chain
+    tet_timing = {}
+    for group, chains in ((0, 1), (8, 1), (4, 2), (2, 4), (1, 8), (2, 2)):
+        eng.set_option(eng.OPT_REPLICA_GROUP, group)
+        eng.set_option(eng.OPT_CHAINS, chains)
+        eng.cycle_tet(0, 0, 2, True, 20)
+        torch.cuda.synchronize()
+        tet_timing[(group, chains)] = _timed(stream, lambda: eng.cycle_tet(0, 0, 2, True, 200))
+    tet_best = min(tet_timing, key=tet_timing.get)
+    eng.set_option(eng.OPT_REPLICA_GROUP, tet_best[0])
+    eng.set_option(eng.OPT_CHAINS, tet_best[1])
     learned = chain(0, 0, 2)
+    learned["replica_group_chains"] = list(tet_best)
+    learned["groupings_us_per_cycle"] = {f"{g}x{c}": 1e6 * t / 200 for (g, c), t in tet_timing.items()}
     agree = [abs(p[0] - q[0]) / max(float(np.hypot(p[1], q[1])), 1e-30)
              for p, q in zip(plain["E_per_site"], learned["E_per_site"])]
     eng.close()
