@@ -441,6 +441,18 @@ __device__ __forceinline__ int pass_cell() {
   }
 }
 
+// The cell of this thread in a fixed-L site-form CTA that holds all four
+// corners: kJ1Threads / 4 cells per corner, a tile of L x kTy x 1 cells,
+// the same tile for every corner group of the CTA.
+template <int kLog2L>
+__device__ __forceinline__ int corner_tile_cell() {
+  constexpr int L = 1 << kLog2L, kCells = kJ1Threads / 4, kTy = kCells / L, kTilesY = L / kTy;
+  static_assert(L * kTy == kCells && L % kTy == 0, "tile");
+  const int t = threadIdx.x & (kCells - 1);
+  const int ty = blockIdx.x % kTilesY, z = blockIdx.x / kTilesY;
+  return (z * L + ty * kTy + (t >> kLog2L)) * L + (t & (L - 1));
+}
+
 // kLog2L > 0: the fixed-L addressing (isotropic J1 systems of L = 2^kLog2L).
 template <int B, bool kMetro, bool kExch, int kLog2L = 0>
 __global__ void __launch_bounds__(kJ1Threads) j1_pass_kernel(const J1PassParams p) {
@@ -500,13 +512,25 @@ __device__ __forceinline__ int site_item(const J1PassParams& p, int rep, int f, 
 // S = 4 f + B is uniform in a CTA), blockIdx.z the replica. Fewer live
 // registers than the cell-per-thread form, hence more warps in flight; the
 // Metropolis pass (Philox, cone, exp) is latency-bound without them.
+//
+// With L fixed (kLog2L > 0) a CTA holds all four corners of a tile of
+// kJ1Threads / 4 cells instead (corner f = warps 2f, 2f + 1; blockIdx.y = 0):
+// its four corner groups together read every site plane of the tile's
+// cells, so the neighbours one corner's sites read in the tile are spins
+// another corner group has loaded (L1), which a CTA of one corner misses.
 template <int B, bool kMetro, bool kExch, int kLog2L = 0>
 __global__ void __launch_bounds__(kJ1Threads) j1_site_pass_kernel(const J1PassParams p) {
   static_assert(kLog2L == 0 || !kExch, "fixed-L form is isotropic only");
   pass_prologue();
-  const int f = blockIdx.y;
+  int f, cell;
+  if constexpr (kLog2L > 0) {
+    f = threadIdx.x / (kJ1Threads / 4);  // warp-uniform
+    cell = corner_tile_cell<kLog2L>();
+  } else {
+    f = blockIdx.y;
+    cell = pass_cell<0>();
+  }
   const int rep = blockIdx.z;
-  const int cell = pass_cell<kLog2L>();
   const int g = p.rep_global + rep;
   float beta = 0.0f, cosmax = 0.0f;
   int t = 0;
@@ -1275,7 +1299,9 @@ int j1_fixed_log2(const J1PassParams& p) {
 void launch_j1_pass(const J1PassParams& p, int colour, bool metro, bool site_per_thread,
                     cudaStream_t st) {
   const dim3 grid((p.L3 + kJ1Threads - 1) / kJ1Threads, p.n_rep);
-  const dim3 sgrid((p.L3 + kJ1Threads - 1) / kJ1Threads, 4, p.n_rep);
+  // site form: CTAs of one corner, or (fixed L) of all four corners of a tile
+  const dim3 sgrid = j1_fixed_log2(p) > 0 ? dim3(4 * p.L3 / kJ1Threads, 1, p.n_rep)
+                                          : dim3((p.L3 + kJ1Threads - 1) / kJ1Threads, 4, p.n_rep);
 #define PYRO_J1_CASE(B, X, G)                                                         \
   case B:                                                                             \
     if (site_per_thread) {                                                            \
