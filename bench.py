@@ -174,7 +174,7 @@ class ClockSampler:
 
 
 KERNEL_OPTIONS = ("J1_KERNEL", "CYCLE_KERNEL", "CLUSTER_SIZE", "J1_SITE_MODE", "REPLICA_GROUP",
-                  "CHAINS", "PDL", "FUSED_OBS", "J1_FIXED_L")
+                  "CHAINS", "PDL", "FUSED_OBS", "J1_FIXED_L", "CHAIN_STAGGER")
 
 
 def cpu_baseline_and_parity(kernel_options: dict, cycles: int = 6):
@@ -850,6 +850,9 @@ def main():
                          "(0: one group)")
     ap.add_argument("--cluster-size", type=int, default=None,
                     help="CTAs per cluster of --kernel cluster (default: the engine's)")
+    ap.add_argument("--stagger", type=int, default=None,
+                    help="--kernel grouped: each odd chain starts after the preceding chain's first "
+                         "N passes")
     ap.add_argument("--fixed-l", type=int, default=1, choices=[0, 1],
                     help="1: per-pass J1 kernels compiled for L = 16 / 32 (default); "
                          "0: the run-time-L kernels")
@@ -918,6 +921,8 @@ def main():
             eng.set_option(eng.OPT_J1_SITE_MODE, 3 if args.site_mode is None else args.site_mode)
         elif args.kernel == "grouped" and args.site_mode is not None:
             eng.set_option(eng.OPT_J1_SITE_MODE, args.site_mode)
+        if args.kernel == "grouped" and args.stagger is not None:
+            eng.set_option(eng.OPT_CHAIN_STAGGER, args.stagger)
     options = {n: eng.get_option(getattr(Engine, "OPT_" + n)) for n in KERNEL_OPTIONS}
     kernel_desc = {"cycle_kernel": options["CYCLE_KERNEL"],
                    "cluster_size": options["CLUSTER_SIZE"],
@@ -925,7 +930,8 @@ def main():
                    "replica_group": options["REPLICA_GROUP"],
                    "chains": options["CHAINS"],
                    "j1_site_mode": options["J1_SITE_MODE"],
-                   "j1_fixed_l": options["J1_FIXED_L"], "autotune_choice": variant}
+                   "j1_fixed_l": options["J1_FIXED_L"],
+                   "chain_stagger": options["CHAIN_STAGGER"], "autotune_choice": variant}
     if world > 1:
         from cudacode_b200.distributed import EngineBackend, ShardedPT
         pt = ShardedPT(EngineBackend(eng, torch.device(f"cuda:{local}")), R_PER_GPU * n_gpus)

@@ -500,6 +500,28 @@ int queue_grouped(pyro_ctx* ctx, int n_metro, int n_or, bool j1_grouped, bool ge
     PYRO_CK(cudaEventRecord(ctx->fork_event, ctx->stream));
     for (int c = 0; c < chains; ++c) PYRO_CK(cudaStreamWaitEvent(ctx->chain_stream[c], ctx->fork_event, 0));
   }
+  // staggered start: each odd chain c waits for chain c - 1's first
+  // `stagger` passes (recorded when chain c - 1 has queued them)
+  // (at most one group's passes: chain c - 1's first group is queued before
+  // chain c's, so the event is recorded before it is waited on)
+  const int stagger = chains > 1 ? std::min(ctx->chain_stagger, 4 * (n_metro + n_or)) : 0;
+  int chain_passes[kMaxChains] = {};
+  bool chain_started[kMaxChains] = {};
+  auto before_pass = [&](int c) -> int {
+    if (stagger > 0 && (c & 1) && !chain_started[c])
+      PYRO_CK(cudaStreamWaitEvent(ctx->chain_stream[c], ctx->stagger_event[c - 1], 0));
+    chain_started[c] = true;
+    return PYRO_OK;
+  };
+  auto after_pass = [&](int c) -> int {
+    if (stagger > 0 && !(c & 1) && c + 1 < chains && ++chain_passes[c] == stagger)
+      PYRO_CK(cudaEventRecord(ctx->stagger_event[c], ctx->chain_stream[c]));
+    return PYRO_OK;
+  };
+  if (stagger > 0)
+    for (int c = 0; c + 1 < chains; c += 2)
+      if (!ctx->stagger_event[c])
+        PYRO_CK(cudaEventCreateWithFlags(&ctx->stagger_event[c], cudaEventDisableTiming));
   int gi = 0;
   if (j1_grouped) {
     for (int si : ctx->j1_sys) {
@@ -523,6 +545,7 @@ int queue_grouped(pyro_ctx* ctx, int n_metro, int n_or, bool j1_grouped, bool ge
         const bool last_metro = n_or == 0;
         const bool fuse = ctx->fused_obs && with_obs && s.exch < 0 && n_tet == 0 && n_sw > 0 &&
                           !(last_metro ? ctx->j1_metro_site_mode : ctx->j1_or_site_mode);
+        const int ch = chains > 1 ? (gi % chains) : 0;
         for (int k = 0; k < n_sw; ++k) {
           const bool metro = k < n_metro;
           for (int colour = 0; colour < 4; ++colour) {
@@ -531,12 +554,14 @@ int queue_grouped(pyro_ctx* ctx, int n_metro, int n_or, bool j1_grouped, bool ge
             p.n_rep = cnt;
             p.rep_global += r0;
             p.rep_key += r0;
+            if (int rc = before_pass(ch)) return rc;
             if (fuse && k == n_sw - 1 && colour == 3)
               launch_j1_last_pass(p, jp, metro, st);
             else
               launch_j1_pass(p, colour, metro,
                              metro ? ctx->j1_metro_site_mode : ctx->j1_or_site_mode, st);
             PYRO_CK_LAUNCH();
+            if (int rc = after_pass(ch)) return rc;
           }
         }
         if (n_tet > 0) {
@@ -728,8 +753,10 @@ void free_all(pyro_ctx* c) {
   for (int i = 0; i < kMaxChains; ++i) {
     if (c->chain_stream[i]) cudaStreamDestroy(c->chain_stream[i]);
     if (c->chain_event[i]) cudaEventDestroy(c->chain_event[i]);
+    if (c->stagger_event[i]) cudaEventDestroy(c->stagger_event[i]);
     c->chain_stream[i] = nullptr;
     c->chain_event[i] = nullptr;
+    c->stagger_event[i] = nullptr;
   }
   if (c->fork_event) cudaEventDestroy(c->fork_event);
   c->fork_event = nullptr;
@@ -1232,6 +1259,9 @@ int pyro_set_option(pyro_ctx* ctx, int option, int value) {
   } else if (option == PYRO_OPT_WAVE_STALL) {
     if (value < -1) return fail(ctx, PYRO_ERR_ARG, "stall item is -1 (off) or an item index");
     ctx->wave_stall_item = value;
+  } else if (option == PYRO_OPT_CHAIN_STAGGER) {
+    if (value < 0) return fail(ctx, PYRO_ERR_ARG, "chain stagger must be >= 0");
+    ctx->chain_stagger = value;
   } else if (option == PYRO_OPT_J1_FIXED_L) {
     if (value != 0 && value != 1) return fail(ctx, PYRO_ERR_ARG, "fixed-L option is 0 or 1");
     ctx->j1_fixed_l = value;
@@ -1267,6 +1297,7 @@ int pyro_get_option(pyro_ctx* ctx, int option, int* value) {
     case PYRO_OPT_WAVE_STALL: *value = ctx->wave_stall_item; break;
     case PYRO_OPT_MEASURE_SNAPSHOT: *value = ctx->measure_snapshot; break;
     case PYRO_OPT_J1_FIXED_L: *value = ctx->j1_fixed_l; break;
+    case PYRO_OPT_CHAIN_STAGGER: *value = ctx->chain_stagger; break;
     case PYRO_OPT_J1_SITE_MODE:
       *value = (ctx->j1_metro_site_mode ? 1 : 0) | (ctx->j1_or_site_mode ? 2 : 0);
       break;
@@ -1282,7 +1313,7 @@ int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen)
   if (!ctx) return PYRO_ERR_ARG;
   if (cycles < 1 || n_metro < 0 || n_or < 0 || n_metro + n_or < 1)
     return fail(ctx, PYRO_ERR_ARG, "autotune: need cycles >= 1 and at least one sweep");
-  struct Variant { int j1, cyc, cs, site, group, chains, gen_mb; };
+  struct Variant { int j1, cyc, cs, site, group, chains, gen_mb, stagger; };
   bool any_j1 = false, any_gen = false;
   for (const auto& s : ctx->sys) {
     if (j1_sweepable(s)) any_j1 = true;
@@ -1309,7 +1340,10 @@ int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen)
                            {1, 3, 16, 1, 4, 4, 0}, {1, 3, 16, 3, 4, 2, 0},
                            // Metropolis passes in the cell form too (fixed-L kernels)
                            {1, 0, 16, 0, 2, 4, 0}, {1, 0, 16, 0, 4, 2, 0}, {1, 0, 16, 0, 3, 3, 0},
-                           {1, 0, 16, 0, 1, 8, 0}};
+                           {1, 0, 16, 0, 1, 8, 0},
+                           // odd chains started one Metropolis sweep after their partner
+                           {1, 0, 16, 1, 2, 4, 0, 4}, {1, 0, 16, 1, 2, 4, 0, 8}, {1, 0, 16, 1, 3, 3, 0, 4},
+                           {1, 0, 16, 1, 1, 8, 0, 4}, {1, 0, 16, 0, 2, 4, 0, 4}};
     vs.insert(vs.end(), std::begin(j1v), std::end(j1v));
     n_j1 = (int)vs.size();
   }
@@ -1336,6 +1370,7 @@ int pyro_autotune(pyro_ctx* ctx, int n_metro, int n_or, int cycles, int* chosen)
     if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_REPLICA_GROUP, v.group);
     if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_CHAINS, v.chains);
     if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_GROUP_MB, v.gen_mb);
+    if (!rc) rc = pyro_set_option(ctx, PYRO_OPT_CHAIN_STAGGER, v.stagger);
     if (!rc) rc = check_cluster(ctx);
     return rc;
   };

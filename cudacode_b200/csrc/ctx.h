@@ -121,6 +121,10 @@ struct pyro_ctx {
   int n_chains = 1;     // concurrent streams the replica groups are dealt to
   cudaStream_t chain_stream[pyro::kMaxChains] = {};
   cudaEvent_t chain_event[pyro::kMaxChains] = {};
+  // PYRO_OPT_CHAIN_STAGGER: each odd chain starts after the preceding
+  // chain's first chain_stagger passes (0: all chains start together)
+  int chain_stagger = 0;
+  cudaEvent_t stagger_event[pyro::kMaxChains] = {};
   cudaEvent_t fork_event = nullptr;  // cycles without exchange of L <= 8 systems in shared memory
   int cluster_size = 16;
   bool cluster_checked = false;

@@ -297,6 +297,7 @@ class Engine:
     OPT_WAVE_STALL = 13
     OPT_MEASURE_SNAPSHOT = 14
     OPT_J1_FIXED_L = 15
+    OPT_CHAIN_STAGGER = 16
 
     def set_option(self, option: int, value: int) -> None:
         self._ck(self.lib.pyro_set_option(self.ctx, option, value))

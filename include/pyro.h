@@ -167,6 +167,12 @@ int pyro_neighbour_table(int site, int* out120);
  * shifts, neighbour planes as compile-time offsets: fewer instructions per
  * update); 0 uses the run-time-L kernels for every L. Identical results. */
 #define PYRO_OPT_J1_FIXED_L 15
+/* PYRO_OPT_CHAIN_STAGGER: with replica groups on PYRO_OPT_CHAINS > 1
+ * chains, each odd chain c starts its first group after chain c - 1 has run
+ * its first `value` colour passes (at most one group's; 0, default: all
+ * chains start together), so the Metropolis phases of a chain pair do not
+ * coincide. Identical results. */
+#define PYRO_OPT_CHAIN_STAGGER 16
 int pyro_set_option(pyro_ctx* ctx, int option, int value);
 int pyro_get_option(pyro_ctx* ctx, int option, int* value);
 /* Autotuner: times every kernel variant (per-pass generic, per-pass J1,

@@ -115,3 +115,28 @@ def test_fixed_cluster_cycle_against_oracle(L, cluster):
     E1, M1 = o.observables()
     np.testing.assert_allclose(E0, E1, rtol=1e-12, atol=1e-9)
     np.testing.assert_allclose(M0, M1, rtol=1e-12, atol=1e-9)
+
+
+@pytest.mark.parametrize("stagger", [2, 4, 9])
+def test_staggered_chains_give_the_same_chain(stagger):
+    """Odd chains starting after their partner's first passes change only
+    the timing: spins, permutation and energies as with simultaneous chains
+    and as the oracle's."""
+    temps = geometric_ladder(0.03, 1.5, 8)
+    s = System(L=16, temperatures=temps)
+    e = Engine([s], seed=606)
+    o = Oracle([s], seed=606)
+    e.set_option(e.OPT_REPLICA_GROUP, 1)
+    e.set_option(e.OPT_CHAINS, 4)
+    e.set_option(e.OPT_CHAIN_STAGGER, stagger)
+    assert e.get_option(e.OPT_CHAIN_STAGGER) == stagger
+    e.init_random()
+    o.init_random()
+    cones = np.linspace(-0.7, 0.9, len(temps)).astype(np.float32)
+    e.set_cone(cones)
+    o.set_cone(cones)
+    e.cycle(1, 3, True, 3)
+    o.cycle(1, 3, True, 3)
+    assert np.array_equal(e.get_spins(), o.get_spins())
+    assert np.array_equal(e.permutation(), o.permutation())
+    np.testing.assert_allclose(e.last_observables()[0], o.observables()[0], rtol=1e-12, atol=1e-9)
