@@ -978,7 +978,7 @@ def main():
     # copies are queued on the engine's stream (pyro_set_cone_async,
     # pyro_last_observables_async), so step k + 1 is queued while step k
     # runs, and the wall clock ends when every step's results are on the host.
-    e2e_steps = 0 if args.no_e2e else max(10, args.steps // 4)
+    e2e_steps = 0 if args.no_e2e else max(40, args.steps)
     n_loc = R_PER_GPU
     cones_h = torch.from_numpy(cones).pin_memory()
     e_h = torch.empty((max(e2e_steps, 1), n_loc), dtype=torch.float64).pin_memory()
