@@ -190,6 +190,47 @@ __device__ __forceinline__ unsigned long long j1_pass_smem(float4* lat, float J1
   return acc;
 }
 
+// Twice the FP64 energy of an isotropic J1-only replica of fixed L from its
+// tetrahedra (this thread's share): every bond lies in exactly one
+// tetrahedron, and a tetrahedron's bonds sum to (|sum S|^2 - sum |S|^2) / 2.
+// Each cell holds its four up-tetrahedra (sites 4F..4F+3) and the four down-
+// tetrahedra through its sublattice-0 sites 4F. Same value as energy2_share
+// up to FP64 rounding, from 8 tetrahedra per cell instead of 6 neighbours
+// per site.
+__device__ __forceinline__ double tet_pairs(float4 a, float4 b, float4 c, float4 d) {
+  const double mx = (double)a.x + b.x + c.x + d.x;
+  const double my = (double)a.y + b.y + c.y + d.y;
+  const double mz = (double)a.z + b.z + c.z + d.z;
+  const double n2 = (double)a.x * a.x + (double)a.y * a.y + (double)a.z * a.z +
+                    (double)b.x * b.x + (double)b.y * b.y + (double)b.z * b.z +
+                    (double)c.x * c.x + (double)c.y * c.y + (double)c.z * c.z +
+                    (double)d.x * d.x + (double)d.y * d.y + (double)d.z * d.z;
+  return mx * mx + my * my + mz * mz - n2;  // twice the sum of the pair products
+}
+
+template <int L, int F>
+__device__ __forceinline__ double j1_cell_corner2(const float4* lat, int cell, int x, int y, int z) {
+  constexpr int L3 = L * L * L, S = 4 * F;
+  const float4 s0 = lat[S * L3 + cell], s1 = lat[(S + 1) * L3 + cell],
+               s2 = lat[(S + 2) * L3 + cell], s3 = lat[(S + 3) * L3 + cell];
+  const float4 d1 = lat[j1_nbr<L, S, j1_down_index(S, 0)>(x, y, z)];
+  const float4 d2 = lat[j1_nbr<L, S, j1_down_index(S, 1)>(x, y, z)];
+  const float4 d3 = lat[j1_nbr<L, S, j1_down_index(S, 2)>(x, y, z)];
+  return tet_pairs(s0, s1, s2, s3) + tet_pairs(s0, d1, d2, d3);
+}
+
+template <int L>
+__device__ double j1_energy2_share(const float4* lat, double J1) {
+  constexpr int L3 = L * L * L;
+  double e = 0.0;
+  for (int cell = threadIdx.x; cell < L3; cell += blockDim.x) {
+    const int x = cell % L, y = (cell / L) % L, z = cell / (L * L);
+    e += j1_cell_corner2<L, 0>(lat, cell, x, y, z) + j1_cell_corner2<L, 1>(lat, cell, x, y, z) +
+         j1_cell_corner2<L, 2>(lat, cell, x, y, z) + j1_cell_corner2<L, 3>(lat, cell, x, y, z);
+  }
+  return J1 * e;  // = sum over sites of S_i . h_i, as energy2_share
+}
+
 // Spin-independent part of a Metropolis update: the Philox words of the
 // site and the cone geometry they give (cos, sin of the polar angle, the
 // azimuth's cos and sin, the acceptance uniform), exactly as
@@ -386,7 +427,9 @@ __global__ void __launch_bounds__(kSmemThreads) smem_cycles_kernel(const SmemCyc
     }
     if (p.history) {
       // FP64 energy of the cycle's final state: E = 1/2 sum_i S_i . h_i
-      const double e = energy2_share(lat, tab, sd, p.exch, L, L3, n);
+      double e;
+      if constexpr (kL > 0) e = j1_energy2_share<kL>(lat, sd.J64[0]);
+      else e = energy2_share(lat, tab, sd, p.exch, L, L3, n);
       const double tot = block_sum(e, red);
       if (threadIdx.x == 0) {
         const unsigned long long row = (hist0 + c) % (unsigned long long)p.history_cap;
@@ -396,7 +439,10 @@ __global__ void __launch_bounds__(kSmemThreads) smem_cycles_kernel(const SmemCyc
   }
   for (int i = threadIdx.x; i < n; i += blockDim.x) g[i] = lat[i];
   if (p.energy) {  // observables of the final state, as the per-pass path leaves them
-    const double e = block_sum(energy2_share(lat, tab, sd, p.exch, L, L3, n), red);
+    double e2;
+    if constexpr (kL > 0) e2 = j1_energy2_share<kL>(lat, sd.J64[0]);
+    else e2 = energy2_share(lat, tab, sd, p.exch, L, L3, n);
+    const double e = block_sum(e2, red);
     double mx = 0.0, my = 0.0, mz = 0.0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
       mx += lat[i].x;

@@ -372,7 +372,8 @@ def test_structure_factor_matches_direct_sum(L, G, stride, replica):
                                         sel.shape[0], rel=1e-9)
 
 
-@pytest.mark.parametrize("L,J2,J3", [(4, 0.0, 0.0), (8, 0.0, 0.0), (5, 0.06, -0.04)])
+@pytest.mark.parametrize("L,J2,J3", [(4, 0.0, 0.0), (8, 0.0, 0.0), (5, 0.06, -0.04), (3, 0.0, 0.0),
+                                     (6, 0.0, 0.0), (7, 0.0, 0.0)])
 def test_shared_memory_cycles_bit_exact(L, J2, J3):
     temps = geometric_ladder(0.1, 1.0, 3)
     e, o = pair([System(L=L, temperatures=temps, J2=J2, J3=J3)], renorm_every=4)
