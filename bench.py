@@ -351,7 +351,7 @@ def run_batched(args):
 
     rng = np.random.default_rng(12345 + 3)
     systems = []
-    for _ in range(256):
+    for _ in range(args.systems):
         Ls = int(rng.choice([8, 12, 16, 20, 24]))
         nT = int(rng.integers(16, 33))
         j2, j3 = rng.uniform(-0.1, 0.1, 2)
@@ -379,7 +379,7 @@ def run_batched(args):
     print(json.dumps({
         "metric": "spin-updates/ns", "workload": "batched", "value": updates / (sec * 1e9),
         "unit": "updates/ns", "ms_per_step": 1e3 * sec / steps, "steps": steps,
-        "spins": spins, "systems": 256, "autotune_choice": choice,
+        "spins": spins, "systems": args.systems, "autotune_choice": choice,
         "roofline": roofline,
         "config": {"workload": "256 systems, L in {8,12,16,20,24}, 16-32 replicas each, ladders "
                                "in [0.05, 1.5], J2, J3 in [-0.1, 0.1], 1 M + 4 OR + exchange"}}),
@@ -845,6 +845,8 @@ def main():
     ap.add_argument("--site-mode", type=int, default=None,
                     help="J1 pass forms (bit 0 Metropolis, bit 1 over-relaxation one site "
                          "per thread) for --kernel grouped / wave (wave default 3)")
+    ap.add_argument("--systems", type=int, default=256,
+                    help="--workload batched: number of systems (256 in the configuration)")
     ap.add_argument("--group-mb", type=int, default=None,
                     help="--workload batched --kernel wave: MB of spins per work-queue group "
                          "(0: one group)")
