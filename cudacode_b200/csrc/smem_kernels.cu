@@ -294,6 +294,102 @@ __device__ __forceinline__ int j1_metro_pass_drawn(float4* lat, float J1, float 
   }
 }
 
+// Lattices whose colour classes have at most one site per thread
+// (4 L^3 <= kSmemThreads): a thread's corner k and cell never change, so the
+// shared-memory indices of its site's 6 neighbours and its own spin, for
+// each of the 4 colours, are computed once per launch. The passes then run
+// one code body per colour and no address arithmetic.
+struct SiteIdx {
+  int n[4][7];  // per colour b: neighbours 0..5 of site 4 k + b, then the site itself
+};
+
+template <int L, int S>
+__device__ __forceinline__ void site_idx(int* out, int x, int y, int z, int cell) {
+  out[0] = j1_nbr<L, S, 0>(x, y, z);
+  out[1] = j1_nbr<L, S, 1>(x, y, z);
+  out[2] = j1_nbr<L, S, 2>(x, y, z);
+  out[3] = j1_nbr<L, S, 3>(x, y, z);
+  out[4] = j1_nbr<L, S, 4>(x, y, z);
+  out[5] = j1_nbr<L, S, 5>(x, y, z);
+  out[6] = S * L * L * L + cell;
+}
+
+template <int L, int B>
+__device__ __forceinline__ void colour_idx(int* out, int k, int x, int y, int z, int cell) {
+  switch (k) {
+    case 0: site_idx<L, B>(out, x, y, z, cell); break;
+    case 1: site_idx<L, 4 + B>(out, x, y, z, cell); break;
+    case 2: site_idx<L, 8 + B>(out, x, y, z, cell); break;
+    default: site_idx<L, 12 + B>(out, x, y, z, cell); break;
+  }
+}
+
+template <int L>
+__device__ __forceinline__ SiteIdx make_site_idx(int k, int cell) {
+  const int x = cell % L, y = (cell / L) % L, z = cell / (L * L);
+  SiteIdx t;
+  colour_idx<L, 0>(t.n[0], k, x, y, z, cell);
+  colour_idx<L, 1>(t.n[1], k, x, y, z, cell);
+  colour_idx<L, 2>(t.n[2], k, x, y, z, cell);
+  colour_idx<L, 3>(t.n[3], k, x, y, z, cell);
+  return t;
+}
+
+// One site update from precomputed indices (the arithmetic of
+// j1_site_smem / j1_metro_drawn).
+template <bool kMetro>
+__device__ __forceinline__ int idx_update(float4* lat, const int* ix, float J1, float beta,
+                                          const MetroDraw& d, bool renorm) {
+  const float4 n0 = lat[ix[0]], n1 = lat[ix[1]], n2 = lat[ix[2]], n3 = lat[ix[3]],
+               n4 = lat[ix[4]], n5 = lat[ix[5]];
+  pyro_vec3 h;
+  h.x = J1 * (((((n0.x + n1.x) + n2.x) + n3.x) + n4.x) + n5.x);
+  h.y = J1 * (((((n0.y + n1.y) + n2.y) + n3.y) + n4.y) + n5.y);
+  h.z = J1 * (((((n0.z + n1.z) + n2.z) + n3.z) + n4.z) + n5.z);
+  const float4 sv = lat[ix[6]];
+  pyro_vec3 sp;
+  sp.x = sv.x;
+  sp.y = sv.y;
+  sp.z = sv.z;
+  pyro_vec3 out;
+  int a = 0;
+  if (kMetro) {
+    const pyro_vec3 prop = pyro_about_axis(sp, d.ct, d.st, d.cp, d.sp);
+    a = pyro_metropolis_accept(pyro_delta_e(h, sp, prop), beta, d.u3);
+    out = a ? prop : sp;
+  } else {
+    out = pyro_overrelax(sp, h);
+  }
+  if (renorm) out = pyro_renormalise(out);
+  lat[ix[6]] = make_float4(out.x, out.y, out.z, 0.0f);
+  return a;
+}
+
+// A sweep of a small lattice from precomputed indices (4 L^3 <= kSmemThreads).
+template <int L, bool kMetro>
+__device__ __forceinline__ unsigned long long idx_sweep(float4* lat, const SiteIdx& t, int k,
+                                                        int cell, float J1, float beta,
+                                                        float cosmax, uint32_t rkey,
+                                                        uint32_t sweep32, bool renorm,
+                                                        uint32_t seed_lo, uint32_t seed_hi) {
+  constexpr int L3 = L * L * L;
+  const bool active = threadIdx.x < 4 * L3;
+  MetroDraw d[4];
+  if (kMetro) {
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+      d[b] = metro_draw((uint32_t)((4 * k + b) * L3 + cell), rkey, sweep32, cosmax, seed_lo,
+                        seed_hi);
+  }
+  unsigned long long acc = 0;
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    if (active) acc += idx_update<kMetro>(lat, t.n[b], J1, beta, d[b], renorm);
+    __syncthreads();
+  }
+  return acc;
+}
+
 template <int L, bool kMetro>
 __device__ __forceinline__ unsigned long long j1_sweep_smem(float4* lat, float J1, float beta,
                                                             float cosmax, uint32_t rkey,
@@ -355,13 +451,24 @@ __global__ void __launch_bounds__(kSmemThreads) smem_cycles_kernel(const SmemCyc
   const int per_cycle = p.n_metro + p.n_or;
   __syncthreads();
   unsigned long long acc = 0;
+  constexpr bool kIdx = kL > 0 && 4 * kL * kL * kL <= kSmemThreads;
+  const int my_k = kIdx ? (int)threadIdx.x / (kL * kL * kL > 0 ? kL * kL * kL : 1) : 0;
+  const int my_cell = kIdx ? (int)threadIdx.x - my_k * kL * kL * kL : 0;
+  SiteIdx site_ix;
+  if constexpr (kIdx) site_ix = make_site_idx<kL>(my_k < 4 ? my_k : 0, my_cell);
   for (int c = 0; c < p.n_cycles; ++c) {
     for (int k = 0; k < per_cycle; ++k) {
       const unsigned long long sweep = base + (unsigned long long)c * per_cycle + k;
       const bool metro = k < p.n_metro;
       const bool renorm =
           p.renorm_every > 0 && ((sweep + 1) % (unsigned long long)p.renorm_every) == 0;
-      if constexpr (kL > 0) {
+      if constexpr (kIdx) {
+        acc += metro ? idx_sweep<kL, true>(lat, site_ix, my_k, my_cell, sd.J1, beta, cosmax,
+                                           rkey, (uint32_t)sweep, renorm, p.seed_lo, p.seed_hi)
+                     : idx_sweep<kL, false>(lat, site_ix, my_k, my_cell, sd.J1, beta, cosmax,
+                                            rkey, (uint32_t)sweep, renorm, p.seed_lo,
+                                            p.seed_hi);
+      } else if constexpr (kL > 0) {
         acc += metro ? j1_sweep_smem<kL, true>(lat, sd.J1, beta, cosmax, rkey, (uint32_t)sweep,
                                                renorm, p.seed_lo, p.seed_hi)
                      : j1_sweep_smem<kL, false>(lat, sd.J1, beta, cosmax, rkey, (uint32_t)sweep,
